@@ -1,0 +1,358 @@
+"""Benchmark of the block-sparse contraction path (btod_contract2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ltg|reference]
+                    [--workload ladder-large|ladder-split|ladder-small|ring] [--mode plain|...]
+
+One step = one btod_contract2::perform over the whole synthetic workload.
+value   = algorithmic FP64 flops / device time, inputs resident in HBM
+          (effective FP64 TFLOP/s; flops = sum over non-zero C blocks and
+          coalesced pairs of 2*|C block|*K, the reference's get_cost x 2000);
+e2e     = same flops / time of the C-ABI call sequence with host buffers:
+          H2D of both operand arenas, the contraction, D2H of the result.
+N > 1 runs independent replicas (the path does not shard); value sums ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "ladder-large": "LADDER_LARGE",
+    "ladder-split": "LADDER_SPLIT",
+    "ladder-small": "LADDER_SMALL",
+    "ladder-ccd": "LADDER_CCD",
+    "ring": "RING_D2H",
+    "ring-small": "RING_D2H_SMALL",
+}
+MODES = {"plain": 0, "ozaki-bf16": 1, "ozaki-fp8": 2, "ozaki-int8": 3}
+FP64_NOMINAL = 40.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ltg", choices=["ltg", "reference"])
+    p.add_argument("--workload", default="ladder-large", choices=sorted(WORKLOADS))
+    p.add_argument("--mode", default="plain", choices=sorted(MODES))
+    p.add_argument("--nslices", type=int, default=0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(name):
+    from libtensor_b200 import spec as S
+    cfg = getattr(S, WORKLOADS[name])
+    a = cfg.t_spec()
+    b = cfg.v_spec() if hasattr(cfg, "v_spec") else cfg.w_spec()
+    return cfg, a, b
+
+
+def contraction_of(cfg):
+    from libtensor_b200.core import contraction2
+    c = cfg.contraction
+    contr = contraction2(c["n"], c["m"], c["k"], c["permc"])
+    for p in c["pairs"]:
+        contr.contract(*p)
+    return contr
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- reference
+
+def build_reference(a_spec, b_spec, cfg, A_host, A_bt, B_host, B_bt):
+    from oracle import refapi as R
+    ra, rb = R.RefBT(a_spec), R.RefBT(b_spec)
+    for t, host, r in ((A_bt, A_host, ra), (B_bt, B_host, rb)):
+        for bidx, blk in t.blocks(host):
+            r.set_block(bidx, blk)
+    c = cfg.contraction
+    op = R.RefContract2(c["n"], c["m"], c["k"], c["permc"], c["pairs"], ra, rb, 1.0, 1.0, cfg.kc)
+    rc = op.make_result()
+    return ra, rb, op, rc
+
+
+def time_reference(op, rc, steps, warmup, budget_s=30.0):
+    """Times the reference's perform() (wall clock); returns (seconds/step, runs)."""
+    from oracle import refapi as R
+    R.set_threads(os.cpu_count() or 1)
+    for _ in range(warmup):
+        op.perform(rc)
+    ts = []
+    t_start = time.perf_counter()
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        op.perform(rc)
+        ts.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s:
+            break
+    return float(np.median(ts)), len(ts)
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from libtensor_b200.core import Context, block_tensor
+    from oracle import refapi as R
+    cfg, a_spec, b_spec = workload(args.workload)
+    metric, unit = metric_name(), "TFLOP/s"
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libltref.so was not built"}))
+        return
+    hctx = Context(-1)
+    A, B = block_tensor(hctx, a_spec), block_tensor(hctx, b_spec)
+    ah, bh = A.fill_seeded_host(11, cfg.t_scale), B.fill_seeded_host(23, cfg.v_scale)
+    from libtensor_b200.core import btod_contract2
+    A.mark_nonzero(); B.mark_nonzero()
+    plan = btod_contract2(contraction_of(cfg), A, B, kc=cfg.kc)
+    flops = plan.flops()
+    ra, rb, op, rc = build_reference(a_spec, b_spec, cfg, ah, A, bh, B)
+    sec, runs = time_reference(op, rc, args.steps, min(args.warmup, 1), budget_s=120.0)
+    v = flops / sec / 1e12
+    out = {"metric": metric, "value": v, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
+           "steps": runs, "warmup": min(args.warmup, 1), "ms_per_step": sec * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, symmetrised)",
+           "config": config_of(args, cfg, flops),
+           "cpu_baseline": {"value": v, "unit": unit, "cores": os.cpu_count(), "kind": "reference",
+                            "sample": f"full workload, {runs} perform() calls, median"},
+           "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def metric_name():
+    return "btod_contract2 eff. FP64 TFLOP/s: split-prec vs plain DMMA @ rel err<=1e-12"
+
+
+def config_of(args, cfg, flops):
+    return {"workload": f"{cfg.name} ({args.workload})", "mode": args.mode, "nslices": args.nslices,
+            "o": cfg.o, "v": cfg.v, "algorithmic_flops": flops,
+            "l2": "inputs larger than L2 (no flush)" if args.workload in ("ladder-large", "ladder-split", "ring", "ladder-ccd") else "small inputs, L2-resident"}
+
+
+# ---------------------------------------------------------------- ltg arm
+
+def measure_fp64_peak(torch, dev):
+    """cuBLAS DGEMM 8192^3 (best of 3): the FP64 denominator of the roofline."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def ltg_arm(args):
+    import torch
+    import torch.distributed as dist
+    from libtensor_b200.core import Context, block_tensor, btod_contract2
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    cfg, a_spec, b_spec = workload(args.workload)
+    mode = MODES[args.mode]
+    ctx = Context(local)
+    A, B = block_tensor(ctx, a_spec), block_tensor(ctx, b_spec)
+    A.fill_seeded(11, cfg.t_scale)
+    B.fill_seeded(23, cfg.v_scale)
+    op = btod_contract2(contraction_of(cfg), A, B, kc=cfg.kc)
+    C = op.make_result()
+    flops = op.flops()
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ctx.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        op.perform(C, mode=mode, nslices=args.nslices)
+    barrier()
+
+    # ---- device-resident timing
+    clocks = ClockSampler(local)
+    clocks.start()
+    n0 = ctx.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        op.perform(C, mode=mode, nslices=args.nslices)
+    e1.record(stream)
+    barrier()
+    launches = ctx.launch_count() - n0
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * flops / (ms * 1e-3) / 1e12
+
+    # ---- end-to-end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        ha = torch.empty(max(1, A.nelems), dtype=torch.float64, pin_memory=True)
+        hb = torch.empty(max(1, B.nelems), dtype=torch.float64, pin_memory=True)
+        hc = torch.empty(max(1, C.nelems), dtype=torch.float64, pin_memory=True)
+        A.download_async(ha.data_ptr()); B.download_async(hb.data_ptr())
+        ctx.synchronize()
+        for _ in range(2):
+            A.upload_async(ha.data_ptr()); B.upload_async(hb.data_ptr())
+            op.perform(C, mode=mode, nslices=args.nslices)
+            C.download_async(hc.data_ptr())
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            A.upload_async(ha.data_ptr()); B.upload_async(hb.data_ptr())
+            op.perform(C, mode=mode, nslices=args.nslices)
+            C.download_async(hc.data_ptr())
+        f1.record(stream)
+        barrier()
+        ems = f0.elapsed_time(f1) / args.steps
+        if world > 1:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * flops / (ems * 1e-3) / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": 8 * (A.nelems + B.nelems), "d2h_bytes_per_step": 8 * C.nelems,
+               "ms_per_step": ems}
+        del ha, hb, hc
+
+    # ---- roofline of the dominant kernel (the contraction is the whole step)
+    peak = measure_fp64_peak(torch, dev) if rank == 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(f"{args.workload}:{args.mode}")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cfg, a_spec, b_spec, A, B, flops)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    achieved = flops / (ms * 1e-3) / 1e12
+    out = {"metric": metric_name(), "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+           "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, symmetrised; no public dataset)",
+           "config": config_of(args, cfg, flops),
+           "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak if peak else None, "traffic": traffic,
+                        "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU (FP64 tensor path); "
+                                       f"nominal {FP64_NOMINAL} TFLOP/s"},
+           "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+    print(json.dumps(out))
+
+
+def cpu_baseline(cfg, a_spec, b_spec, A, B, flops):
+    try:
+        from oracle import refapi as R
+        if not R.available():
+            return None
+        ah, bh = A.download(), B.download()
+        ra, rb, op, rc = build_reference(a_spec, b_spec, cfg, ah, A, bh, B)
+        sec, runs = time_reference(op, rc, 2, 0, budget_s=30.0)
+        return {"value": flops / sec / 1e12, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"full workload, {runs} perform() call(s) of the reference built from its sources "
+                          f"(OpenBLAS, 1 BLAS thread x {os.cpu_count()} libutil threads, one batch per operand)",
+                "ms_per_step": sec * 1e3}
+    except Exception as e:   # the baseline is reported, never required
+        return {"value": None, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"failed: {e}"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ltg_arm(args)
+
+
+if __name__ == "__main__":
+    main()

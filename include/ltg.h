@@ -1,0 +1,197 @@
+/*
+ * ltg.h -- C ABI of the B200 block-tensor contraction path.
+ *
+ * This is the drop-in boundary for libtensor's block-sparse contraction hot
+ * path.  Each entry point replaces one reference interface (cited per
+ * function).  Conventions:
+ *   - every function returns an int status: LTG_OK (0) or an LTG_ERR_* code;
+ *     ltg_last_error() gives a message for the calling thread;
+ *   - no C++ exceptions cross this boundary;
+ *   - handles are opaque; plain pointers and sizes only;
+ *   - permutations use the reference's convention (libtensor/core/permutation.h):
+ *     perm[i] is the position in the source sequence of the element that lands
+ *     at position i;
+ *   - one CUDA stream per context; calls are asynchronous on that stream
+ *     unless stated otherwise; ltg_ctx_synchronize() waits for it.
+ */
+#ifndef LTG_H
+#define LTG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    LTG_OK = 0,
+    LTG_ERR_BAD_ARG = 1,
+    LTG_ERR_BAD_DIMS = 2,        /* libtensor::bad_dimensions */
+    LTG_ERR_SYMMETRY = 3,        /* libtensor::symmetry_violation / bad_symmetry */
+    LTG_ERR_UNSUPPORTED = 4,
+    LTG_ERR_OOM = 5,
+    LTG_ERR_CUDA = 6,
+    LTG_ERR_TIMEOUT = 7,         /* a bounded device wait gave up */
+    LTG_ERR_STATE = 8
+};
+
+/* Contraction arithmetic (ltg_contract2 mode). */
+enum {
+    LTG_MODE_PLAIN_FP64 = 0,     /* FP64 DMMA tensor-core contraction (drop-in) */
+    LTG_MODE_OZAKI_BF16 = 1,     /* split-precision: BF16 slices, FP32 accumulate */
+    LTG_MODE_OZAKI_FP8 = 2,      /* split-precision: FP8 E4M3 slices, FP32 accumulate */
+    LTG_MODE_OZAKI_INT8 = 3      /* split-precision: INT8 slices, INT32 accumulate */
+};
+
+typedef struct ltg_ctx ltg_ctx;
+typedef struct ltg_bt ltg_bt;
+typedef struct ltg_plan ltg_plan;
+typedef struct ltg_graph ltg_graph;
+
+/* Block tensor description: block index space plus symmetry.
+ * Symmetry elements are applied in the order perm, part, label (the order in
+ * which libtensor::symmetry<N,T>::insert() receives them).                  */
+typedef struct ltg_bt_spec {
+    int32_t order;                  /* 1..8 */
+    const int64_t *dims;            /* [order] extents */
+    const int32_t *nsplit;          /* [order] number of split points per dim */
+    const int64_t *splits;          /* concatenated split positions */
+    /* se_perm generators (libtensor/symmetry/se_perm.h:28) */
+    int32_t nperm;
+    const int32_t *perm;            /* [nperm*order] */
+    const double *perm_coeff;       /* [nperm] +1 symmetric, -1 antisymmetric */
+    /* se_part (libtensor/symmetry/se_part.h:32), forbidden partitions only */
+    int32_t has_part;
+    const int64_t *part_pdims;      /* [order] partitions per dim (1 = none) */
+    int64_t npart_forbidden;
+    const int64_t *part_forbidden;  /* [npart_forbidden*order] partition indices */
+    /* se_label (libtensor/symmetry/se_label.h:37) for abelian (XOR) tables */
+    int32_t has_label;
+    int32_t label_nirrep;           /* 1, 2, 4 or 8 */
+    const int32_t *labels;          /* concatenated per-dim block labels, -1 = none */
+    int32_t label_nintr;
+    const int32_t *label_intr;      /* allowed intrinsic labels (OR) */
+} ltg_bt_spec;
+
+const char *ltg_last_error(void);
+int ltg_version(void);
+
+/* ---- context --------------------------------------------------------- */
+int ltg_ctx_create(int device, ltg_ctx **out);
+int ltg_ctx_destroy(ltg_ctx *ctx);
+int ltg_ctx_synchronize(ltg_ctx *ctx);
+/* Underlying cudaStream_t of the context (for event timing by callers). */
+int ltg_ctx_stream(ltg_ctx *ctx, void **stream);
+/* Host threads used for schedule construction (libutil::thread_pool role). */
+int ltg_ctx_set_host_threads(ltg_ctx *ctx, int nthreads);
+/* Number of device kernels launched by this context so far. */
+int ltg_ctx_launch_count(ltg_ctx *ctx, int64_t *count);
+
+/* ---- block tensors (libtensor/block_tensor/block_tensor.h:22) --------- */
+int ltg_bt_create(ltg_ctx *ctx, const ltg_bt_spec *spec, ltg_bt **out);
+/* New tensor with the block index space and symmetry of `a` permuted by
+ * `perm` (so_permute; the result space of btod_copy(a, perm)). */
+int ltg_bt_create_permuted(ltg_bt *a, const int32_t *perm, ltg_bt **out);
+int ltg_bt_destroy(ltg_bt *bt);
+/* Canonical allowed blocks: count and packed arena size in elements. */
+int ltg_bt_info(const ltg_bt *bt, int32_t *order, int64_t *nblocks, int64_t *nelems);
+/* Per canonical block: absolute block index, arena offset, element count. */
+int ltg_bt_blocks(const ltg_bt *bt, int64_t *abs_idx, int64_t *offset, int64_t *size);
+/* Block-index dims (number of blocks per dimension). */
+int ltg_bt_bidims(const ltg_bt *bt, int64_t *bidims);
+/* Extents of the block with block index bidx
+ * (block_index_space::get_block_dims). */
+int ltg_bt_block_dims(const ltg_bt *bt, const int64_t *bidx, int64_t *dims);
+/* Non-zero canonical blocks (req_nonzero_blocks,
+ * gen_block_tensor/gen_block_tensor_ctrl.h:100). Returns the count in *n. */
+int ltg_bt_nonzero(const ltg_bt *bt, int64_t *abs_idx, int64_t cap, int64_t *n);
+/* Orbit of a block: canonical index, transform canonical->block, allowed
+ * (libtensor/core/orbit.h). Returns allowed (0/1) in *allowed. */
+int ltg_bt_orbit(const ltg_bt *bt, int64_t abs_idx, int64_t *canonical,
+                 int32_t *perm, double *coeff, int32_t *allowed);
+/* Whole-arena transfer of all canonical blocks in ltg_bt_blocks order
+ * (synchronous).  Upload marks every block non-zero. */
+int ltg_bt_upload(ltg_bt *bt, const double *host);
+int ltg_bt_download(ltg_bt *bt, double *host);
+/* Single-block transfer (req_block / ret_block). */
+int ltg_bt_upload_block(ltg_bt *bt, const int64_t *bidx, const double *data);
+int ltg_bt_download_block(ltg_bt *bt, const int64_t *bidx, double *data);
+/* Asynchronous whole-arena transfer on the context stream (pinned host
+ * memory recommended). */
+int ltg_bt_upload_async(ltg_bt *bt, const double *host);
+int ltg_bt_download_async(ltg_bt *bt, double *host);
+/* Zero every block and mark all blocks zero (btod_set(0)). */
+int ltg_bt_set_zero(ltg_bt *bt);
+/* Mark all canonical blocks non-zero without touching data. */
+int ltg_bt_mark_nonzero(ltg_bt *bt);
+/* Make one canonical block zero (gen_block_tensor_ctrl::req_zero_block,
+ * gen_block_tensor/gen_block_tensor_ctrl.h): its data is cleared and it
+ * leaves the non-zero list. */
+int ltg_bt_zero_block(ltg_bt *bt, const int64_t *bidx);
+/* Device fill of all canonical blocks with the seeded, symmetrised test
+ * distribution of ltg_seeded_value() (one launch). */
+int ltg_bt_fill_seeded(ltg_bt *bt, uint64_t seed, double scale);
+/* Host fill with bit-identical values (multi-threaded CPU). */
+int ltg_bt_fill_seeded_host(const ltg_bt *bt, uint64_t seed, double scale, double *host);
+/* Raw device pointer of the arena. */
+int ltg_bt_device_ptr(ltg_bt *bt, double **ptr);
+
+/* ---- btod_contract2 (libtensor/block_tensor/btod_contract2.h:29-140) -- */
+/* Builds the contraction of a (order N+K) and b (order M+K): permc is the
+ * result permutation (contraction2(permc)), pairs[2*K] the contracted index
+ * pairs (contraction2::contract(ia, ib)).  Schedule construction runs here
+ * (gen_bto_contract2::make_schedule). */
+int ltg_contract2_create(ltg_ctx *ctx, int32_t n, int32_t m, int32_t k,
+                         const int32_t *permc, const int32_t *pairs,
+                         ltg_bt *a, ltg_bt *b, ltg_plan **out);
+/* Creates an empty result tensor with the derived block index space and
+ * symmetry (btod_contract2::get_bis / get_symmetry). */
+int ltg_contract2_make_result(ltg_plan *plan, ltg_bt **c);
+/* Non-zero canonical C blocks (get_schedule). */
+int ltg_plan_schedule(ltg_plan *plan, int64_t *abs_idx, int64_t cap, int64_t *n);
+/* Coalesced pair list of schedule entry i: per pair
+ * {aia, acia, perm_a[NA], coeff_a bits, aib, acib, perm_b[NB], coeff_b bits}
+ * as int64 (coefficients as raw IEEE-754 bits). */
+int ltg_plan_pairs(ltg_plan *plan, int64_t i, int64_t *out, int64_t cap, int64_t *npairs);
+/* Algorithmic flops: sum over C blocks and pairs of 2*|C block|*K. */
+int ltg_plan_flops(ltg_plan *plan, double *flops);
+/* perform(): C = kc * contr(ka*A, kb*B) (add == 0), or C += d * ... (add).
+ * nslices is the slice count of the split-precision modes (ignored by
+ * LTG_MODE_PLAIN_FP64). */
+int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices,
+                  double ka, double kb, double kc, int32_t add, double d);
+int ltg_plan_destroy(ltg_plan *plan);
+
+/* ---- btod_copy / btod_add / btod_dotprod ------------------------------ */
+/* b = c * perm(a)  or  b += d * c * perm(a)   (btod_copy.h:38-115) */
+int ltg_copy(ltg_bt *a, const int32_t *perm, double c, ltg_bt *b,
+             int32_t add, double d);
+/* b = sum_t c_t * perm_t(a_t)  or  b += d * sum ...  (btod_add.h:38-131) */
+int ltg_add(int32_t nterms, ltg_bt *const *a, const int32_t *perms,
+            const double *coeffs, ltg_bt *b, int32_t add, double d);
+/* <perma(a), permb(b)> over the full tensor (btod_dotprod.h:35-70);
+ * synchronous, result in *out. */
+int ltg_dotprod(ltg_bt *a, const int32_t *perma, ltg_bt *b,
+                const int32_t *permb, double *out);
+/* Asynchronous form: result left in device memory at *dev_out. */
+int ltg_dotprod_async(ltg_bt *a, const int32_t *perma, ltg_bt *b,
+                      const int32_t *permb, double *dev_out);
+/* a *= c  (btod_scale) */
+int ltg_scale(ltg_bt *a, double c);
+/* a[i,j,a,b] /= (e_i + e_j - e_a - e_b) style denominator over a 4-index
+ * tensor: divides every element by (sum of eps over the index positions with
+ * sign +1 for the first `nocc` dims and -1 for the rest).  eps is a device or
+ * host array per dim concatenated (dims[0]+...+dims[3]). */
+int ltg_denominator(ltg_bt *a, const double *eps_host, int32_t nocc);
+
+/* ---- CUDA graphs over a context's stream ------------------------------ */
+int ltg_graph_begin(ltg_ctx *ctx);
+int ltg_graph_end(ltg_ctx *ctx, ltg_graph **out);
+int ltg_graph_launch(ltg_graph *g);
+int ltg_graph_destroy(ltg_graph *g);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LTG_H */

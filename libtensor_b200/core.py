@@ -1,0 +1,347 @@
+"""Python face of the C ABI, named after the reference's operations.
+
+    ctx = Context(0)
+    t = block_tensor(ctx, spec); t.fill_seeded(seed)
+    contr = contraction2(2, 2, 2); contr.contract(2, 2); contr.contract(3, 3)
+    op = btod_contract2(contr, t, v, kc=0.5)
+    r = op.make_result(); op.perform(r)            # r = 0.5 * contr(t, v)
+    op.perform(r, 1.0)                             # r += ...
+    btod_copy(t, perm, c).perform(u)
+    btod_add(x, p1, c1).add_op(x, p2, c2).perform(y)
+    e = btod_dotprod(a, None, b, None).calculate()
+
+Every call goes through libltg.so; nothing here computes tensor data.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import check, lib
+from .spec import BTSpec
+
+MODE_PLAIN_FP64 = _capi.MODE_PLAIN_FP64
+MODE_OZAKI_BF16 = _capi.MODE_OZAKI_BF16
+MODE_OZAKI_FP8 = _capi.MODE_OZAKI_FP8
+MODE_OZAKI_INT8 = _capi.MODE_OZAKI_INT8
+
+
+def _i32(vals):
+    return (C.c_int32 * max(1, len(vals)))(*vals)
+
+
+def _perm(p, n):
+    return None if p is None else _i32(list(p))
+
+
+class Context:
+    """One device (device >= 0) or a host-only context (device = -1) for
+    schedules and orbit queries without a GPU."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().ltg_ctx_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def synchronize(self):
+        check(lib().ltg_ctx_synchronize(self.h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib().ltg_ctx_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        check(lib().ltg_ctx_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def set_host_threads(self, n: int):
+        check(lib().ltg_ctx_set_host_threads(self.h, n))
+
+    def close(self):
+        if self.h:
+            check(lib().ltg_ctx_destroy(self.h))
+            self.h = None
+
+    # graphs
+    def graph_begin(self):
+        check(lib().ltg_graph_begin(self.h))
+
+    def graph_end(self) -> "Graph":
+        g = C.c_void_p()
+        check(lib().ltg_graph_end(self.h, C.byref(g)))
+        return Graph(g)
+
+
+class Graph:
+    def __init__(self, h):
+        self.h = h
+
+    def launch(self):
+        check(lib().ltg_graph_launch(self.h))
+
+    def close(self):
+        if self.h:
+            check(lib().ltg_graph_destroy(self.h))
+            self.h = None
+
+
+class block_tensor:
+    """Canonical blocks of a symmetric block tensor in one device arena."""
+
+    def __init__(self, ctx: Context, spec: Optional[BTSpec] = None, _handle=None):
+        self.ctx = ctx
+        self.spec = spec
+        if _handle is None:
+            s = spec.to_ltg()
+            h = C.c_void_p()
+            check(lib().ltg_bt_create(ctx.h, C.byref(s), C.byref(h)))
+            self.h = h
+        else:
+            self.h = _handle
+        order, nb, ne = C.c_int32(), C.c_int64(), C.c_int64()
+        check(lib().ltg_bt_info(self.h, C.byref(order), C.byref(nb), C.byref(ne)))
+        self.order, self.nblocks, self.nelems = order.value, nb.value, ne.value
+        self.abs_idx = np.zeros(max(1, self.nblocks), np.int64)
+        self.offsets = np.zeros(max(1, self.nblocks), np.int64)
+        self.sizes = np.zeros(max(1, self.nblocks), np.int64)
+        check(lib().ltg_bt_blocks(self.h, self.abs_idx.ctypes.data_as(_capi.c_i64p),
+                                  self.offsets.ctypes.data_as(_capi.c_i64p),
+                                  self.sizes.ctypes.data_as(_capi.c_i64p)))
+        self.abs_idx = self.abs_idx[:self.nblocks]
+        self.offsets = self.offsets[:self.nblocks]
+        self.sizes = self.sizes[:self.nblocks]
+        bd = np.zeros(self.order, np.int64)
+        check(lib().ltg_bt_bidims(self.h, bd.ctypes.data_as(_capi.c_i64p)))
+        self.bidims = [int(x) for x in bd]
+
+    def permuted(self, perm) -> "block_tensor":
+        h = C.c_void_p()
+        check(lib().ltg_bt_create_permuted(self.h, _i32(list(perm)), C.byref(h)))
+        return block_tensor(self.ctx, None, _handle=h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(lib().ltg_bt_destroy(self.h))
+            self.h = None
+
+    # ----------------------------------------------------------- queries
+    def block_index(self, aidx: int) -> List[int]:
+        out, a = [], int(aidx)
+        for d in reversed(self.bidims):
+            out.append(a % d)
+            a //= d
+        return out[::-1]
+
+    def abs_index(self, bidx: Sequence[int]) -> int:
+        a = 0
+        for d, b in zip(self.bidims, bidx):
+            a = a * d + int(b)
+        return a
+
+    def nonzero(self) -> List[int]:
+        n = C.c_int64()
+        buf = np.zeros(max(1, self.nblocks), np.int64)
+        check(lib().ltg_bt_nonzero(self.h, buf.ctypes.data_as(_capi.c_i64p), len(buf), C.byref(n)))
+        return [int(x) for x in buf[:n.value]]
+
+    def orbit(self, aidx: int):
+        canon, coeff, allowed = C.c_int64(), C.c_double(), C.c_int32()
+        perm = (C.c_int32 * self.order)()
+        check(lib().ltg_bt_orbit(self.h, aidx, C.byref(canon), perm, C.byref(coeff), C.byref(allowed)))
+        return canon.value, list(perm), coeff.value, bool(allowed.value)
+
+    def block_dims(self, bidx) -> tuple:
+        out = (C.c_int64 * self.order)()
+        check(lib().ltg_bt_block_dims(self.h, (C.c_int64 * self.order)(*bidx), out))
+        return tuple(int(x) for x in out)
+
+    # ----------------------------------------------------------- data
+    def upload(self, arena: np.ndarray):
+        a = np.ascontiguousarray(arena, dtype=np.float64)
+        assert a.size >= self.nelems
+        check(lib().ltg_bt_upload(self.h, a.ctypes.data_as(_capi.c_dblp)))
+
+    def download(self) -> np.ndarray:
+        a = np.zeros(max(1, self.nelems), np.float64)
+        check(lib().ltg_bt_download(self.h, a.ctypes.data_as(_capi.c_dblp)))
+        return a[:self.nelems]
+
+    def upload_async(self, ptr: int):
+        check(lib().ltg_bt_upload_async(self.h, C.c_void_p(ptr)))
+
+    def download_async(self, ptr: int):
+        check(lib().ltg_bt_download_async(self.h, C.c_void_p(ptr)))
+
+    def set_block(self, bidx, data: np.ndarray):
+        b = np.ascontiguousarray(data, dtype=np.float64)
+        check(lib().ltg_bt_upload_block(self.h, (C.c_int64 * self.order)(*bidx), b.ctypes.data_as(_capi.c_dblp)))
+
+    def get_block(self, bidx, shape) -> np.ndarray:
+        out = np.zeros(int(np.prod(shape)), np.float64)
+        check(lib().ltg_bt_download_block(self.h, (C.c_int64 * self.order)(*bidx), out.ctypes.data_as(_capi.c_dblp)))
+        return out.reshape(shape)
+
+    def set_zero(self):
+        check(lib().ltg_bt_set_zero(self.h))
+
+    def mark_nonzero(self):
+        check(lib().ltg_bt_mark_nonzero(self.h))
+
+    def zero_block(self, bidx):
+        check(lib().ltg_bt_zero_block(self.h, (C.c_int64 * self.order)(*bidx)))
+
+    def fill_seeded(self, seed: int, scale: float = 1.0):
+        check(lib().ltg_bt_fill_seeded(self.h, seed, scale))
+
+    def fill_seeded_host(self, seed: int, scale: float = 1.0) -> np.ndarray:
+        a = np.zeros(max(1, self.nelems), np.float64)
+        check(lib().ltg_bt_fill_seeded_host(self.h, seed, scale, a.ctypes.data_as(_capi.c_dblp)))
+        return a[:self.nelems]
+
+    def device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib().ltg_bt_device_ptr(self.h, C.byref(p)))
+        return p.value or 0
+
+    def scale(self, c: float):
+        check(lib().ltg_scale(self.h, c))
+
+    def denominator(self, eps: np.ndarray, nocc: int = 2):
+        e = np.ascontiguousarray(eps, dtype=np.float64)
+        check(lib().ltg_denominator(self.h, e.ctypes.data_as(_capi.c_dblp), nocc))
+
+    def blocks(self, arena: np.ndarray):
+        """Yields (block index, ndarray view) of every canonical block."""
+        for s in range(self.nblocks):
+            bidx = self.block_index(self.abs_idx[s])
+            shape = self.block_dims(bidx)
+            yield bidx, arena[self.offsets[s]:self.offsets[s] + self.sizes[s]].reshape(shape)
+
+
+class contraction2:
+    """contraction2<N,M,K>(permc) + contract(ia, ib) (libtensor/core/contraction2.h:48)."""
+
+    def __init__(self, n: int, m: int, k: int, permc: Optional[Sequence[int]] = None):
+        self.n, self.m, self.k = n, m, k
+        self.permc = list(permc) if permc is not None else list(range(n + m))
+        self.pairs = []
+
+    def contract(self, ia: int, ib: int):
+        self.pairs.append((ia, ib))
+        return self
+
+
+class btod_contract2:
+    """btod_contract2<N,M,K>(contr, A, ka, B, kb, kc) (btod_contract2.h:29-140)."""
+
+    def __init__(self, contr: contraction2, a: block_tensor, b: block_tensor,
+                 ka: float = 1.0, kb: float = 1.0, kc: float = 1.0):
+        self.contr, self.a, self.b = contr, a, b
+        self.ka, self.kb, self.kc = ka, kb, kc
+        h = C.c_void_p()
+        pairs = [v for p in contr.pairs for v in p]
+        check(lib().ltg_contract2_create(a.ctx.h, contr.n, contr.m, contr.k, _i32(contr.permc),
+                                         _i32(pairs), a.h, b.h, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(lib().ltg_plan_destroy(self.h))
+            self.h = None
+
+    def get_schedule(self) -> List[int]:
+        n = C.c_int64()
+        check(lib().ltg_plan_schedule(self.h, None, 0, C.byref(n)))
+        buf = np.zeros(max(1, n.value), np.int64)
+        check(lib().ltg_plan_schedule(self.h, buf.ctypes.data_as(_capi.c_i64p), len(buf), C.byref(n)))
+        return [int(x) for x in buf[:n.value]]
+
+    def pairs(self, i: int):
+        """Coalesced pairs of schedule entry i:
+        [(aia, acia, perm_a, coeff_a, aib, acib, perm_b, coeff_b), ...]."""
+        na, nb = self.contr.n + self.contr.k, self.contr.m + self.contr.k
+        rec = 2 + na + 1 + 2 + nb + 1
+        n = C.c_int64()
+        check(lib().ltg_plan_pairs(self.h, i, None, 0, C.byref(n)))
+        buf = np.zeros(max(1, n.value * rec), np.int64)
+        check(lib().ltg_plan_pairs(self.h, i, buf.ctypes.data_as(_capi.c_i64p), len(buf), C.byref(n)))
+        return decode_pairs(buf[:n.value * rec], na, nb)
+
+    def flops(self) -> float:
+        f = C.c_double()
+        check(lib().ltg_plan_flops(self.h, C.byref(f)))
+        return f.value
+
+    def make_result(self) -> block_tensor:
+        h = C.c_void_p()
+        check(lib().ltg_contract2_make_result(self.h, C.byref(h)))
+        return block_tensor(self.a.ctx, None, _handle=h)
+
+    def perform(self, c: block_tensor, d: Optional[float] = None, mode: int = MODE_PLAIN_FP64,
+                nslices: int = 0):
+        check(lib().ltg_contract2(self.h, c.h, mode, nslices, self.ka, self.kb, self.kc,
+                                  0 if d is None else 1, 0.0 if d is None else d))
+
+
+def decode_pairs(buf, na, nb):
+    rec = 2 + na + 1 + 2 + nb + 1
+    out = []
+    for k in range(len(buf) // rec):
+        o = buf[k * rec:(k + 1) * rec]
+        ca = float(np.frombuffer(np.int64(o[2 + na]).tobytes(), np.float64)[0])
+        q = o[3 + na:]
+        cb = float(np.frombuffer(np.int64(q[2 + nb]).tobytes(), np.float64)[0])
+        out.append((int(o[0]), int(o[1]), tuple(int(x) for x in o[2:2 + na]), ca,
+                    int(q[0]), int(q[1]), tuple(int(x) for x in q[2:2 + nb]), cb))
+    return out
+
+
+class btod_copy:
+    """btod_copy<N>(A, perm, c).perform(B[, d]) (btod_copy.h:38-115)."""
+
+    def __init__(self, a: block_tensor, perm: Optional[Sequence[int]] = None, c: float = 1.0):
+        self.a, self.perm, self.c = a, perm, c
+
+    def perform(self, b: block_tensor, d: Optional[float] = None):
+        check(lib().ltg_copy(self.a.h, _perm(self.perm, self.a.order), self.c, b.h,
+                             0 if d is None else 1, 0.0 if d is None else d))
+
+
+class btod_add:
+    """btod_add<N>(A, perm, c).add_op(...).perform(B[, d]) (btod_add.h:38-131)."""
+
+    def __init__(self, a: block_tensor, perm: Optional[Sequence[int]] = None, c: float = 1.0):
+        self.ops = [(a, perm, c)]
+
+    def add_op(self, a: block_tensor, perm: Optional[Sequence[int]] = None, c: float = 1.0):
+        self.ops.append((a, perm, c))
+        return self
+
+    def perform(self, b: block_tensor, d: Optional[float] = None):
+        n = b.order
+        hs = (C.c_void_p * len(self.ops))(*[o[0].h.value if isinstance(o[0].h, C.c_void_p) else o[0].h for o in self.ops])
+        perms = []
+        for _, p, _ in self.ops:
+            perms += list(p) if p is not None else list(range(n))
+        cs = (C.c_double * len(self.ops))(*[o[2] for o in self.ops])
+        check(lib().ltg_add(len(self.ops), hs, _i32(perms), cs, b.h, 0 if d is None else 1,
+                            0.0 if d is None else d))
+
+
+class btod_dotprod:
+    """btod_dotprod<N>(A, permA, B, permB).calculate() (btod_dotprod.h:35-70)."""
+
+    def __init__(self, a: block_tensor, perma, b: block_tensor, permb):
+        self.a, self.pa, self.b, self.pb = a, perma, b, permb
+
+    def calculate(self) -> float:
+        out = C.c_double()
+        check(lib().ltg_dotprod(self.a.h, _perm(self.pa, self.a.order), self.b.h,
+                                _perm(self.pb, self.b.order), C.byref(out)))
+        return out.value

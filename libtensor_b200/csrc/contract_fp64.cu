@@ -1,0 +1,288 @@
+// Plain FP64 grouped block-pair contraction on the B200 FP64 tensor path
+// (mma.sync m16n8k8 .f64, "DMMA").
+//
+// Replaces, for every non-zero canonical C block of a btod_contract2
+// schedule, the per-block tod_contract2 call chain
+// (libtensor/dense_tensor/impl/tod_contract2_impl.h:104-393): the perma/permb
+// staging copies, the dgemm (linalg_cblas_level3.C:18-58) and the permc
+// permute-add.  Here one persistent launch walks all (C block, m-tile,
+// n-tile) work items; each work item accumulates every coalesced pair of its
+// C block in registers, so there are no temporaries and no atomics.
+//
+// The index permutation of a pair is folded into the tile loader: the
+// element (m, k) of the matricised A block lives at
+//   a_off + sum_i digit_i(m) * ma_str[i] + sum_j digit_j(k) * ka_str[j]
+// (mixed-radix digits over the fused sub-dimensions), computed once per tile
+// row and once per k column per stage, and copied with cp.async (zero-filled
+// outside the block).  Shared-memory tiles keep k contiguous with the k index
+// permuted inside every group of 8 so that one 16-byte shared load returns
+// both k and k+4, which is exactly the pair an m16n8k8 f64 fragment needs.
+#include "ltg_device.cuh"
+
+namespace ltg {
+namespace {
+
+__device__ __forceinline__ int kperm8(int kk) {
+    return (kk & ~7) | ((kk & 3) << 1) | ((kk >> 2) & 1);
+}
+
+__device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_t *ext,
+                                                const int32_t *str) {
+    int64_t off = 0;
+    for (int i = n - 1; i >= 0; i--) {
+        int32_t e = ext[i];
+        int32_t q = lin / e;
+        off += (int64_t)(lin - q * e) * str[i];
+        lin = q;
+    }
+    return off;
+}
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" :: "r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template<int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N)); }
+
+__device__ __forceinline__ void dmma_16x8x8(double *d, const double *a, const double *b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+template<int BM_, int BN_, int BK_, int WM_, int WN_, int STAGES_>
+struct TileCfg {
+    static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_, STAGES = STAGES_;
+    static constexpr int kWarpsM = BM / WM, kWarpsN = BN / WN;
+    static constexpr int kThreads = kWarpsM * kWarpsN * 32;
+    static constexpr int kLd = BK + 8;          // padded row stride in doubles
+    static constexpr int kMT = WM / 16, kNT = WN / 8;
+    static constexpr int kStageA = BM * kLd, kStageB = BN * kLd;
+    static constexpr size_t kSmem = (size_t)STAGES * (kStageA + kStageB) * sizeof(double)
+                                  + (size_t)(BM + BN) * sizeof(int64_t);
+    static_assert(kThreads % BK == 0, "loader assumes a fixed k column per thread");
+    static_assert((BM * BK) % kThreads == 0 && (BN * BK) % kThreads == 0, "tile/threads");
+};
+
+template<class C>
+__device__ __forceinline__ void load_stage(double *sA, double *sB, const int64_t *rowA,
+    const int64_t *rowB, const double *__restrict__ A, const double *__restrict__ B,
+    const DTask &t, int k0) {
+    const int tid = threadIdx.x;
+    const int kk = tid % C::BK;
+    const int k = k0 + kk;
+    const bool kin = k < t.K;
+    int64_t koa = 0, kob = 0;
+    if (kin) {
+        koa = mixed_offset(k, t.nk, t.kext, t.ka_str);
+        kob = mixed_offset(k, t.nk, t.kext, t.kb_str);
+    }
+    const int col = kperm8(kk);
+    constexpr int kRowsPerPass = C::kThreads / C::BK;
+#pragma unroll
+    for (int r0 = 0; r0 < C::BM; r0 += kRowsPerPass) {
+        int r = r0 + tid / C::BK;
+        int64_t ro = rowA[r];
+        bool p = kin && ro >= 0;
+        cp_async8(&sA[r * C::kLd + col], p ? (const void *)(A + ro + koa) : (const void *)A, p);
+    }
+#pragma unroll
+    for (int r0 = 0; r0 < C::BN; r0 += kRowsPerPass) {
+        int r = r0 + tid / C::BK;
+        int64_t ro = rowB[r];
+        bool p = kin && ro >= 0;
+        cp_async8(&sB[r * C::kLd + col], p ? (const void *)(B + ro + kob) : (const void *)B, p);
+    }
+}
+
+template<class C>
+__global__ void __launch_bounds__(C::kThreads, 1)
+contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
+                     const DItem *__restrict__ items, int32_t nitems, int32_t *counter,
+                     const double *__restrict__ A, const double *__restrict__ B,
+                     double *__restrict__ Cp, int32_t add) {
+    extern __shared__ __align__(16) double smem[];
+    double *sA = smem;
+    double *sB = smem + C::STAGES * C::kStageA;
+    int64_t *rowA = reinterpret_cast<int64_t *>(sB + C::STAGES * C::kStageB);
+    int64_t *rowB = rowA + C::BM;
+    __shared__ int32_t s_item;
+    __shared__ __align__(16) DTask s_task;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int wm = warp / C::kWarpsN, wn = warp % C::kWarpsN;
+
+    while (true) {
+        if (tid == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= nitems) break;
+        const DItem item = items[it];
+        const DCBlock &cb = cblks[item.cblk];
+        const int M = cb.M, N = cb.N;
+
+        double acc[C::kMT][C::kNT][4];
+#pragma unroll
+        for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+            for (int j = 0; j < C::kNT; j++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
+
+        for (int ti = cb.t_begin; ti < cb.t_end; ti++) {
+            static_assert(sizeof(DTask) % 8 == 0, "task copy granularity");
+            if (tid < (int)(sizeof(DTask) / 8))
+                reinterpret_cast<int64_t *>(&s_task)[tid] =
+                    reinterpret_cast<const int64_t *>(&tasks[ti])[tid];
+            __syncthreads();
+            const DTask &t = s_task;
+            for (int r = tid; r < C::BM; r += C::kThreads) {
+                int m = item.m0 + r;
+                rowA[r] = m < M ? t.a_off + mixed_offset(m, t.nm, t.mext, t.ma_str) : -1;
+            }
+            for (int r = tid; r < C::BN; r += C::kThreads) {
+                int n = item.n0 + r;
+                rowB[r] = n < N ? t.b_off + mixed_offset(n, t.nn, t.next, t.nb_str) : -1;
+            }
+            __syncthreads();
+            const double coef = t.coeff;
+            const bool scale_b = coef != 1.0;
+            const int nkt = (t.K + C::BK - 1) / C::BK;
+
+#pragma unroll
+            for (int s = 0; s < C::STAGES - 1; s++) {
+                if (s < nkt)
+                    load_stage<C>(sA + s * C::kStageA, sB + s * C::kStageB, rowA, rowB, A, B, t, s * C::BK);
+                cp_async_commit();
+            }
+            for (int kt = 0; kt < nkt; kt++) {
+                cp_async_wait<C::STAGES - 2>();
+                __syncthreads();
+                {
+                    int nk = kt + C::STAGES - 1;
+                    if (nk < nkt) {
+                        int st = nk % C::STAGES;
+                        load_stage<C>(sA + st * C::kStageA, sB + st * C::kStageB, rowA, rowB, A, B, t, nk * C::BK);
+                    }
+                    cp_async_commit();
+                }
+                const int st = kt % C::STAGES;
+                const double *tA = sA + st * C::kStageA;
+                const double *tB = sB + st * C::kStageB;
+#pragma unroll
+                for (int ks = 0; ks < C::BK; ks += 8) {
+                    double af[C::kMT][4], bf[C::kNT][2];
+#pragma unroll
+                    for (int i = 0; i < C::kMT; i++) {
+                        const int row = wm * C::WM + i * 16 + g;
+                        double2 lo = *reinterpret_cast<const double2 *>(&tA[row * C::kLd + ks + 2 * t4]);
+                        double2 hi = *reinterpret_cast<const double2 *>(&tA[(row + 8) * C::kLd + ks + 2 * t4]);
+                        af[i][0] = lo.x; af[i][2] = lo.y; af[i][1] = hi.x; af[i][3] = hi.y;
+                    }
+#pragma unroll
+                    for (int j = 0; j < C::kNT; j++) {
+                        const int col = wn * C::WN + j * 8 + g;
+                        double2 v = *reinterpret_cast<const double2 *>(&tB[col * C::kLd + ks + 2 * t4]);
+                        bf[j][0] = scale_b ? v.x * coef : v.x;
+                        bf[j][1] = scale_b ? v.y * coef : v.y;
+                    }
+#pragma unroll
+                    for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+                        for (int j = 0; j < C::kNT; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
+                }
+            }
+            cp_async_wait<0>();
+            __syncthreads();
+        }
+
+        // Epilogue: scaled store (assign) or scaled accumulate (add) into the
+        // canonical C block through its own index mapping.
+        const double scale = cb.scale;
+        int64_t coff_m[C::kMT][2];
+        int64_t coff_n[C::kNT][2];
+#pragma unroll
+        for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int m = item.m0 + wm * C::WM + i * 16 + g + 8 * h;
+                coff_m[i][h] = m < M ? mixed_offset(m, cb.nm, cb.mext, cb.mc_str) : -1;
+            }
+#pragma unroll
+        for (int j = 0; j < C::kNT; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int n = item.n0 + wn * C::WN + j * 8 + 2 * t4 + h;
+                coff_n[j][h] = n < N ? mixed_offset(n, cb.nn, cb.next, cb.nc_str) : -1;
+            }
+        double *Cb = Cp + cb.c_off;
+#pragma unroll
+        for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+            for (int j = 0; j < C::kNT; j++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    int64_t om = coff_m[i][q >> 1], on = coff_n[j][q & 1];
+                    if (om < 0 || on < 0) continue;
+                    double v = scale * acc[i][j][q];
+                    if (add) Cb[om + on] += v;
+                    else Cb[om + on] = v;
+                }
+    }
+}
+
+template<class C>
+cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *items,
+                       int32_t nitems, int32_t *counter, const double *a, const double *b,
+                       double *c, int32_t add, cudaStream_t s) {
+    static bool configured = false;
+    cudaError_t e;
+    if (!configured) {
+        e = cudaFuncSetAttribute(contract_fp64_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)C::kSmem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int grid = nitems < nsm ? nitems : nsm;
+    if (grid < 1) return cudaSuccess;
+    e = cudaMemsetAsync(counter, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) return e;
+    contract_fp64_kernel<C><<<grid, C::kThreads, C::kSmem, s>>>(tasks, cblks, items, nitems, counter,
+                                                               a, b, c, add);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// Tile configurations (BM, BN, BK, warp tile M, warp tile N, stages).
+using Cfg0 = TileCfg<128, 128, 16, 64, 32, 3>;
+using Cfg1 = TileCfg<64, 64, 16, 32, 32, 3>;
+using Cfg2 = TileCfg<64, 128, 16, 32, 32, 3>;
+using Cfg3 = TileCfg<32, 32, 16, 16, 16, 4>;
+
+int tile_cfg_bm(int cfg) { return cfg == 0 ? Cfg0::BM : cfg == 1 ? Cfg1::BM : cfg == 2 ? Cfg2::BM : Cfg3::BM; }
+int tile_cfg_bn(int cfg) { return cfg == 0 ? Cfg0::BN : cfg == 1 ? Cfg1::BN : cfg == 2 ? Cfg2::BN : Cfg3::BN; }
+
+cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
+    const DItem *items, int32_t nitems, int32_t *counter, const double *a,
+    const double *b, double *c, int32_t add, int32_t tile_cfg, cudaStream_t s) {
+    switch (tile_cfg) {
+    case 0: return launch_cfg<Cfg0>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 1: return launch_cfg<Cfg1>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 2: return launch_cfg<Cfg2>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    default: return launch_cfg<Cfg3>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    }
+}
+
+}  // namespace ltg

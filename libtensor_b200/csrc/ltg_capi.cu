@@ -1,0 +1,1023 @@
+// C ABI of the B200 block-tensor path (include/ltg.h).
+//
+// Owns device memory and streams; converts host-engine plans (ltg_host.cpp)
+// into device task arrays and launches the kernels.  No exception crosses
+// the boundary: every entry point returns a status code and records a
+// message for ltg_last_error().
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ltg.h"
+#include "ltg_device.cuh"
+#include "ltg_host.hpp"
+
+namespace ltg {
+int tile_cfg_bm(int cfg);
+int tile_cfg_bn(int cfg);
+}
+
+using namespace ltg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define LTG_CUDA(call)                                                          \
+    do {                                                                        \
+        cudaError_t e_ = (call);                                                \
+        if (e_ != cudaSuccess)                                                  \
+            throw error(e_ == cudaErrorMemoryAllocation ? kErrOom : kErrCuda,   \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
+
+template<class F>
+int guard(F f) {
+    try {
+        f();
+        return kOk;
+    } catch (const error &e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        g_last_error = "host allocation failed";
+        return kErrOom;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return kErrState;
+    }
+}
+
+// Device buffer owned by a context.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { if (p) cudaFree(p); }
+    void alloc(size_t n) {
+        if (n <= bytes && p) return;
+        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+        if (n == 0) return;
+        LTG_CUDA(cudaMalloc(&p, n));
+        bytes = n;
+    }
+    template<class T> T *as() const { return static_cast<T *>(p); }
+};
+
+template<class T>
+void upload_vec(DevBuf &d, const std::vector<T> &v, cudaStream_t s) {
+    d.alloc(v.size() * sizeof(T));
+    if (!v.empty()) {
+        LTG_CUDA(cudaMemcpyAsync(d.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+        LTG_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+}  // namespace
+
+struct ltg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int host_threads = 1;
+    int64_t launches = 0;
+    bool capturing = false;
+    int nsm = 148;
+    DevBuf scratch_counter;      // work-queue counters of persistent launches
+    DevBuf dot_out;              // device scalar for synchronous dot products
+};
+
+static std::atomic<uint64_t> g_bt_uid{1};
+
+struct ltg_bt {
+    ltg_ctx *ctx = nullptr;
+    uint64_t uid = g_bt_uid++;          // never reused (cache keys)
+    BlockTensorHost h;
+    DevBuf arena;
+    DevBuf dir_off, dir_start, dir_ext;   // block directory for fill/denominator
+    bool dir_uploaded = false;
+};
+
+struct ContractExec {
+    // device task arrays bound to one output tensor and coefficient set
+    DevBuf tasks, cblks, items;
+    std::vector<std::pair<int32_t, std::pair<int32_t, int32_t>>> launches;  // cfg -> item range
+    std::vector<std::pair<int64_t, int64_t>> zero_ranges;  // assign mode: blocks not in the schedule
+    std::vector<int64_t> sched_slots;
+};
+
+struct ltg_plan {
+    ltg_ctx *ctx = nullptr;
+    ltg_bt *a = nullptr, *b = nullptr;
+    ContractPlan plan;
+    // cache of device task arrays keyed by (C tensor, ka, kb, kc, add, d)
+    std::map<std::tuple<uint64_t, double, double, double, int, double>,
+             std::unique_ptr<ContractExec>> exec;
+};
+
+struct ltg_graph {
+    ltg_ctx *ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void check_ctx(ltg_ctx *c) { if (!c) throw error(kErrBadArg, "null context"); }
+void check_bt(const ltg_bt *b) { if (!b) throw error(kErrBadArg, "null block tensor"); }
+
+Perm perm_from(int n, const int32_t *p) {
+    Perm r = Perm::identity(n);
+    if (!p) return r;
+    bool seen[kMaxOrder] = {};
+    for (int i = 0; i < n; i++) {
+        if (p[i] < 0 || p[i] >= n || seen[p[i]]) throw error(kErrBadArg, "invalid permutation");
+        seen[p[i]] = true;
+        r.p[i] = (int8_t)p[i];
+    }
+    return r;
+}
+
+void parse_spec(const ltg_bt_spec *s, BlockTensorHost &h) {
+    if (!s) throw error(kErrBadArg, "null spec");
+    const int n = s->order;
+    if (n < 1 || n > kMaxOrder) throw error(kErrBadDims, "order must be 1..8");
+    if (!s->dims) throw error(kErrBadArg, "null dims");
+    h.bis = Bis();
+    h.bis.n = n;
+    int64_t pos = 0;
+    for (int d = 0; d < n; d++) {
+        h.bis.dims[d] = s->dims[d];
+        h.bis.starts[d].clear();
+        h.bis.starts[d].push_back(0);
+        int ns = s->nsplit ? s->nsplit[d] : 0;
+        for (int k = 0; k < ns; k++) h.bis.starts[d].push_back(s->splits[pos++]);
+    }
+    h.bis.finalize();
+    for (int d = 0; d < n; d++) {
+        h.bis.type[d] = d;
+        for (int e = 0; e < d; e++)
+            if (h.bis.dims[e] == h.bis.dims[d] && h.bis.starts[e] == h.bis.starts[d]) { h.bis.type[d] = h.bis.type[e]; break; }
+    }
+    h.sym = Symmetry();
+    for (int g = 0; g < s->nperm; g++) {
+        SePerm e;
+        e.perm = perm_from(n, s->perm + (size_t)g * n);
+        e.coeff = s->perm_coeff ? s->perm_coeff[g] : 1.0;
+        if (e.coeff != 1.0 && e.coeff != -1.0) throw error(kErrSymmetry, "se_perm coefficient must be +1 or -1");
+        // the permutation must map the block index space onto itself
+        // (se_perm::is_valid_bis, libtensor/symmetry/se_perm.h:114-121)
+        if (!h.bis.permuted(e.perm).equals(h.bis)) throw error(kErrSymmetry, "se_perm incompatible with the block index space");
+        h.sym.perm.push_back(e);
+    }
+    (void)perm_group_closure(n, h.sym.perm);   // validates sign consistency
+    if (s->has_part) {
+        SePart p;
+        int64_t np = 1;
+        for (int d = 0; d < n; d++) {
+            p.pdims[d] = s->part_pdims[d];
+            if (p.pdims[d] < 1 || h.bis.bidims[d] % p.pdims[d] != 0)
+                throw error(kErrSymmetry, "block count not divisible by the number of partitions");
+            p.bipdims[d] = h.bis.bidims[d] / p.pdims[d];
+            np *= p.pdims[d];
+        }
+        p.forbidden.assign(np, 0);
+        for (int64_t f = 0; f < s->npart_forbidden; f++) {
+            int64_t a = 0;
+            for (int d = 0; d < n; d++) {
+                int64_t v = s->part_forbidden[f * n + d];
+                if (v < 0 || v >= p.pdims[d]) throw error(kErrBadArg, "forbidden partition index out of range");
+                a = a * p.pdims[d] + v;
+            }
+            p.forbidden[a] = 1;
+        }
+        h.sym.part.push_back(p);
+    }
+    if (s->has_label) {
+        SeLabel l;
+        l.nirrep = s->label_nirrep;
+        if (l.nirrep != 1 && l.nirrep != 2 && l.nirrep != 4 && l.nirrep != 8)
+            throw error(kErrUnsupported, "label tables must be abelian with 1, 2, 4 or 8 irreps");
+        int64_t lp = 0;
+        for (int d = 0; d < n; d++) {
+            l.labels[d].resize(h.bis.bidims[d]);
+            for (int64_t b = 0; b < h.bis.bidims[d]; b++) {
+                int v = s->labels[lp++];
+                if (v >= l.nirrep) throw error(kErrBadArg, "label out of range");
+                l.labels[d][b] = v < 0 ? -1 : v;
+            }
+        }
+        // set_rule(label_set): one single-term product per intrinsic label
+        // covering all dims (libtensor/symmetry/inst/se_label_impl.h:38-54)
+        for (int k = 0; k < s->label_nintr; k++) {
+            LabelTerm t;
+            for (int d = 0; d < n; d++) t.seq[d] = 1;
+            t.intr = s->label_intr[k];
+            l.rule.push_back({t});
+        }
+        h.sym.label.push_back(l);
+    }
+}
+
+void need_dev(const ltg_ctx *c) {
+    if (c->device < 0) throw error(kErrState, "host-only context has no device");
+}
+
+void alloc_arena(ltg_bt *bt) {
+    bt->h.build_directory();
+    if (bt->ctx->device < 0) return;
+    size_t bytes = (size_t)std::max<int64_t>(bt->h.total_elems, 1) * sizeof(double);
+    bt->arena.alloc(bytes);
+    LTG_CUDA(cudaMemsetAsync(bt->arena.p, 0, bytes, bt->ctx->stream));
+    LTG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+}
+
+void upload_directory(ltg_bt *bt) {
+    if (bt->dir_uploaded) return;
+    const BlockTensorHost &h = bt->h;
+    size_t nb = h.blk_abs.size();
+    std::vector<int64_t> st(nb * kDevMaxOrder, 0);
+    std::vector<int32_t> ex(nb * kDevMaxOrder, 1);
+    int64_t bidx[kMaxOrder];
+    for (size_t i = 0; i < nb; i++) {
+        h.bis.unabs(h.blk_abs[i], bidx);
+        for (int d = 0; d < h.bis.n; d++) {
+            st[i * kDevMaxOrder + d] = h.bis.starts[d][bidx[d]];
+            ex[i * kDevMaxOrder + d] = (int32_t)h.bis.block_extent(d, bidx[d]);
+        }
+    }
+    cudaStream_t s = bt->ctx->stream;
+    upload_vec(bt->dir_off, h.blk_off, s);
+    upload_vec(bt->dir_start, st, s);
+    upload_vec(bt->dir_ext, ex, s);
+    bt->dir_uploaded = true;
+}
+
+DGenGroup gen_group(const BlockTensorHost &h) {
+    DGenGroup g;
+    std::memset(&g, 0, sizeof(g));
+    g.order = h.bis.n;
+    std::vector<SePerm> grp = perm_group_closure(h.bis.n, h.sym.perm);
+    if (grp.size() > 48) throw error(kErrUnsupported, "symmetry group too large for the generator");
+    g.ngroup = (int32_t)grp.size();
+    for (size_t e = 0; e < grp.size(); e++) {
+        for (int d = 0; d < kDevMaxOrder; d++) g.perm[e][d] = d < h.bis.n ? grp[e].perm.p[d] : 0;
+        g.coeff[e] = grp[e].coeff > 0 ? 1 : -1;
+    }
+    for (int d = 0; d < h.bis.n; d++) g.dims[d] = h.bis.dims[d];
+    return g;
+}
+
+double two_m32(double scale) { return scale * 2.3283064365386963e-10; }   // scale * 2^-32
+
+// ------------------------------------------------------------ contraction exec
+
+// Tile configuration per C block: the bucket of its (M, N) extents picks one
+// of the compiled tile shapes (an autotuned table may override it).
+int pick_tile(int64_t M, int64_t N) {
+    if (M >= 96 && N >= 96) return 0;
+    if (M >= 48 && N >= 96) return 2;
+    if (M >= 40 && N >= 40) return 1;
+    return 3;
+}
+
+void pack_sub(const SubDims &s, int32_t &n, int32_t *ext, int32_t *str0, int32_t *str1) {
+    if (s.n > kDevMaxSub) throw error(kErrUnsupported, "too many sub-dimensions");
+    n = s.n;
+    for (int i = 0; i < kDevMaxSub; i++) {
+        ext[i] = i < s.n ? s.ext[i] : 1;
+        if (str0) str0[i] = i < s.n ? (int32_t)s.s0[i] : 0;
+        if (str1) str1[i] = i < s.n ? (int32_t)s.s1[i] : 0;
+    }
+}
+
+ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double kc, int add, double d) {
+    auto key = std::make_tuple(c->uid, ka, kb, kc, add, add ? d : 0.0);
+    auto it = pl->exec.find(key);
+    if (it != pl->exec.end()) return it->second.get();
+    if (pl->ctx->capturing) throw error(kErrState, "contraction not prepared before graph capture: call it once outside the capture");
+    std::unique_ptr<ContractExec> ex(new ContractExec());
+    std::vector<GemmTask> tasks;
+    std::vector<CBlockTask> cbt;
+    contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    std::vector<DTask> dt(tasks.size());
+    for (size_t i = 0; i < tasks.size(); i++) {
+        const GemmTask &t = tasks[i];
+        DTask &x = dt[i];
+        std::memset(&x, 0, sizeof(x));
+        x.a_off = t.a_off; x.b_off = t.b_off;
+        x.K = (int32_t)t.k.total();
+        pack_sub(t.k, x.nk, x.kext, x.ka_str, x.kb_str);
+        pack_sub(t.m, x.nm, x.mext, x.ma_str, nullptr);
+        pack_sub(t.n, x.nn, x.next, x.nb_str, nullptr);
+    }
+    std::vector<DCBlock> dc(cbt.size());
+    double post = add ? d : 1.0;
+    for (size_t e = 0; e < cbt.size(); e++) {
+        const CBlockTask &b = cbt[e];
+        DCBlock &x = dc[e];
+        std::memset(&x, 0, sizeof(x));
+        x.c_off = b.c_off;
+        double c0 = b.coeff0 != 0.0 ? b.coeff0 : 1.0;
+        x.scale = c0 * post;
+        x.M = (int32_t)b.M; x.N = (int32_t)b.N;
+        pack_sub(b.cm, x.nm, x.mext, x.mc_str, nullptr);
+        pack_sub(b.cn, x.nn, x.next, x.nc_str, nullptr);
+        x.t_begin = b.t_begin; x.t_end = b.t_end;
+        for (int32_t t = b.t_begin; t < b.t_end; t++) dt[t].coeff = tasks[t].coeff / c0;
+    }
+    // Work items per tile configuration, costliest first (LPT order for the
+    // persistent work queue).
+    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(4);
+    for (size_t e = 0; e < cbt.size(); e++) {
+        int cfg = pick_tile(cbt[e].M, cbt[e].N);
+        int bm = tile_cfg_bm(cfg), bn = tile_cfg_bn(cfg);
+        for (int64_t m0 = 0; m0 < cbt[e].M; m0 += bm)
+            for (int64_t n0 = 0; n0 < cbt[e].N; n0 += bn) {
+                DItem it; it.cblk = (int32_t)e; it.m0 = (int32_t)m0; it.n0 = (int32_t)n0; it.pad = 0;
+                double cost = (double)bm * bn * (cbt[e].kflops + 8.0 * (cbt[e].t_end - cbt[e].t_begin));
+                per_cfg[cfg].push_back({cost, it});
+            }
+    }
+    std::vector<DItem> items;
+    for (int cfg = 0; cfg < 4; cfg++) {
+        auto &v = per_cfg[cfg];
+        if (v.empty()) continue;
+        std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
+        int32_t start = (int32_t)items.size();
+        for (auto &p : v) items.push_back(p.second);
+        ex->launches.push_back({cfg, {start, (int32_t)v.size()}});
+    }
+    cudaStream_t s = pl->ctx->stream;
+    upload_vec(ex->tasks, dt, s);
+    upload_vec(ex->cblks, dc, s);
+    upload_vec(ex->items, items, s);
+    // blocks of C outside the schedule (zeroed in assign mode)
+    std::vector<char> in_sched(c->h.blk_abs.size(), 0);
+    for (int64_t cabs : pl->plan.schedule) {
+        int64_t sl = c->h.slot_of[cabs];
+        in_sched[sl] = 1;
+        ex->sched_slots.push_back(sl);
+    }
+    for (size_t sl = 0; sl < in_sched.size(); sl++) {
+        if (in_sched[sl]) continue;
+        int64_t b0 = c->h.blk_off[sl], b1 = b0 + c->h.blk_size[sl];
+        if (!ex->zero_ranges.empty() && ex->zero_ranges.back().second >= b0 - 3)
+            ex->zero_ranges.back().second = b1;
+        else
+            ex->zero_ranges.push_back({b0, b1});
+    }
+    ContractExec *raw = ex.get();
+    pl->exec[key] = std::move(ex);
+    return raw;
+}
+
+// ------------------------------------------------------------ transfers
+
+// Cached copy/add plans: the first call for a given (operands, permutations,
+// coefficients, destination, mode) builds and uploads the task arrays; later
+// calls, including calls inside a CUDA-graph capture, only launch.
+struct TransferExec {
+    DevBuf jobs, terms, units, srcs;
+    int32_t nunits = 0;
+    std::vector<char> dst_nonzero;
+};
+typedef std::tuple<std::vector<const ltg_bt *>, std::vector<int8_t>, std::vector<double>,
+                   const ltg_bt *, int, double> transfer_key;
+std::mutex g_tr_mtx;
+std::map<transfer_key, std::unique_ptr<TransferExec>> g_tr_cache;
+
+static_assert(sizeof(DJob) == sizeof(TJob), "job layout");
+static_assert(sizeof(DTerm) == sizeof(TTerm), "term layout");
+static_assert(sizeof(DUnit) == sizeof(TUnit), "unit layout");
+
+void run_transfer(ltg_ctx *ctx, const std::vector<ltg_bt *> &srcs, const std::vector<Perm> &perms,
+                  const std::vector<double> &coeffs, ltg_bt *dst, bool add, double d) {
+    transfer_key key;
+    for (size_t t = 0; t < srcs.size(); t++) {
+        if (srcs[t]->ctx != ctx) throw error(kErrBadArg, "operands belong to different contexts");
+        std::get<0>(key).push_back(srcs[t]);
+        for (int i = 0; i < perms[t].n; i++) std::get<1>(key).push_back(perms[t].p[i]);
+    }
+    std::get<2>(key) = coeffs;
+    std::get<3>(key) = dst;
+    std::get<4>(key) = add ? 1 : 0;
+    std::get<5>(key) = add ? d : 0.0;
+    TransferExec *ex = nullptr;
+    cudaStream_t s = ctx->stream;
+    {
+        std::lock_guard<std::mutex> lk(g_tr_mtx);
+        auto it = g_tr_cache.find(key);
+        if (it != g_tr_cache.end()) ex = it->second.get();
+    }
+    if (!ex) {
+        if (ctx->capturing) throw error(kErrState, "copy/add not prepared before graph capture: call it once outside the capture");
+        std::vector<TransferTerm> terms;
+        for (size_t t = 0; t < srcs.size(); t++)
+            terms.push_back(TransferTerm{&srcs[t]->h, perms[t], coeffs[t], (int32_t)t});
+        TransferPlan plan;
+        plan_transfer(terms, dst->h, add, plan);
+        std::unique_ptr<TransferExec> nx(new TransferExec());
+        upload_vec(nx->jobs, plan.jobs, s);
+        upload_vec(nx->terms, plan.terms, s);
+        upload_vec(nx->units, plan.units, s);
+        std::vector<const double *> sp;
+        for (ltg_bt *b : srcs) sp.push_back(b->arena.as<double>());
+        upload_vec(nx->srcs, sp, s);
+        nx->nunits = (int32_t)plan.units.size();
+        nx->dst_nonzero = plan.dst_nonzero;
+        ex = nx.get();
+        std::lock_guard<std::mutex> lk(g_tr_mtx);
+        g_tr_cache[key] = std::move(nx);
+    }
+    LTG_CUDA(launch_transfer(ex->jobs.as<DJob>(), ex->terms.as<DTerm>(), ex->units.as<DUnit>(),
+                             ex->nunits, ex->srcs.as<const double *>(), dst->arena.as<double>(),
+                             add ? 1 : 0, d, s));
+    ctx->launches++;
+    for (size_t sl = 0; sl < ex->dst_nonzero.size(); sl++)
+        dst->h.nonzero[sl] = add ? (dst->h.nonzero[sl] || ex->dst_nonzero[sl]) : ex->dst_nonzero[sl];
+}
+
+void forget_transfer(const ltg_bt *t) {
+    std::lock_guard<std::mutex> lk(g_tr_mtx);
+    for (auto it = g_tr_cache.begin(); it != g_tr_cache.end();) {
+        const auto &v = std::get<0>(it->first);
+        bool hit = std::get<3>(it->first) == t || std::find(v.begin(), v.end(), t) != v.end();
+        if (hit) it = g_tr_cache.erase(it);
+        else ++it;
+    }
+}
+
+// Cached dot-product plans so that repeated (and graph-captured) calls issue
+// only kernel launches.
+struct DotExec {
+    DevBuf jobs, terms, units, partials;
+    int32_t nunits = 0;
+};
+std::mutex g_dot_mtx;
+std::map<std::tuple<const ltg_bt *, const ltg_bt *, std::vector<int8_t>, std::vector<int8_t>>,
+         std::unique_ptr<DotExec>> g_dot_cache;
+
+DotExec *prepare_dot(ltg_bt *a, const Perm &pa, ltg_bt *b, const Perm &pb) {
+    std::vector<int8_t> ka(pa.p, pa.p + pa.n), kb(pb.p, pb.p + pb.n);
+    auto key = std::make_tuple((const ltg_bt *)a, (const ltg_bt *)b, ka, kb);
+    std::lock_guard<std::mutex> lk(g_dot_mtx);
+    auto it = g_dot_cache.find(key);
+    if (it != g_dot_cache.end()) return it->second.get();
+    if (a->ctx->capturing) throw error(kErrState, "dot product not prepared before graph capture");
+    TransferPlan plan;
+    plan_dot(a->h, pa, b->h, pb, plan);
+    std::unique_ptr<DotExec> ex(new DotExec());
+    cudaStream_t s = a->ctx->stream;
+    upload_vec(ex->jobs, plan.jobs, s);
+    upload_vec(ex->terms, plan.terms, s);
+    upload_vec(ex->units, plan.units, s);
+    ex->partials.alloc(std::max<size_t>(plan.units.size(), 1) * sizeof(double));
+    ex->nunits = (int32_t)plan.units.size();
+    DotExec *raw = ex.get();
+    g_dot_cache[key] = std::move(ex);
+    return raw;
+}
+
+void forget_dot(const ltg_bt *t) {
+    std::lock_guard<std::mutex> lk(g_dot_mtx);
+    for (auto it = g_dot_cache.begin(); it != g_dot_cache.end();) {
+        if (std::get<0>(it->first) == t || std::get<1>(it->first) == t) it = g_dot_cache.erase(it);
+        else ++it;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ltg_last_error(void) { return g_last_error.c_str(); }
+int ltg_version(void) { return 100; }
+
+int ltg_ctx_create(int device, ltg_ctx **out) {
+    return guard([&] {
+        if (!out) throw error(kErrBadArg, "null output");
+        std::unique_ptr<ltg_ctx> c(new ltg_ctx());
+        c->device = device;
+        // device < 0: host-only context (schedules, orbits and host fills;
+        // no device memory, every device operation returns LTG_ERR_STATE).
+        if (device >= 0) {
+            LTG_CUDA(cudaSetDevice(device));
+            LTG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            LTG_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+            c->scratch_counter.alloc(64 * sizeof(int32_t));
+            c->dot_out.alloc(sizeof(double));
+        }
+        unsigned hc = std::thread::hardware_concurrency();
+        c->host_threads = hc ? (int)hc : 1;
+        *out = c.release();
+    });
+}
+
+int ltg_ctx_destroy(ltg_ctx *ctx) {
+    return guard([&] {
+        check_ctx(ctx);
+        if (ctx->device >= 0) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaStreamDestroy(ctx->stream);
+        }
+        delete ctx;
+    });
+}
+
+int ltg_ctx_synchronize(ltg_ctx *ctx) {
+    return guard([&] { check_ctx(ctx); if (ctx->device >= 0) LTG_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+int ltg_ctx_stream(ltg_ctx *ctx, void **stream) {
+    return guard([&] { check_ctx(ctx); if (!stream) throw error(kErrBadArg, "null output"); *stream = ctx->stream; });
+}
+
+int ltg_ctx_set_host_threads(ltg_ctx *ctx, int nthreads) {
+    return guard([&] { check_ctx(ctx); ctx->host_threads = nthreads < 1 ? 1 : nthreads; });
+}
+
+int ltg_ctx_launch_count(ltg_ctx *ctx, int64_t *count) {
+    return guard([&] { check_ctx(ctx); if (!count) throw error(kErrBadArg, "null output"); *count = ctx->launches; });
+}
+
+int ltg_bt_create(ltg_ctx *ctx, const ltg_bt_spec *spec, ltg_bt **out) {
+    return guard([&] {
+        check_ctx(ctx);
+        if (!out) throw error(kErrBadArg, "null output");
+        std::unique_ptr<ltg_bt> bt(new ltg_bt());
+        bt->ctx = ctx;
+        parse_spec(spec, bt->h);
+        alloc_arena(bt.get());
+        *out = bt.release();
+    });
+}
+
+int ltg_bt_create_permuted(ltg_bt *a, const int32_t *perm, ltg_bt **out) {
+    return guard([&] {
+        check_bt(a);
+        if (!out) throw error(kErrBadArg, "null output");
+        std::unique_ptr<ltg_bt> bt(new ltg_bt());
+        bt->ctx = a->ctx;
+        Perm p = perm_from(a->h.bis.n, perm);
+        permute_space(a->h.bis, a->h.sym, p, bt->h.bis, bt->h.sym);
+        alloc_arena(bt.get());
+        *out = bt.release();
+    });
+}
+
+int ltg_bt_destroy(ltg_bt *bt) {
+    return guard([&] {
+        check_bt(bt);
+        forget_dot(bt);
+        forget_transfer(bt);
+        if (bt->ctx->device >= 0) cudaStreamSynchronize(bt->ctx->stream);
+        delete bt;
+    });
+}
+
+int ltg_bt_info(const ltg_bt *bt, int32_t *order, int64_t *nblocks, int64_t *nelems) {
+    return guard([&] {
+        check_bt(bt);
+        if (order) *order = bt->h.bis.n;
+        if (nblocks) *nblocks = (int64_t)bt->h.blk_abs.size();
+        if (nelems) *nelems = bt->h.total_elems;
+    });
+}
+
+int ltg_bt_blocks(const ltg_bt *bt, int64_t *abs_idx, int64_t *offset, int64_t *size) {
+    return guard([&] {
+        check_bt(bt);
+        for (size_t i = 0; i < bt->h.blk_abs.size(); i++) {
+            if (abs_idx) abs_idx[i] = bt->h.blk_abs[i];
+            if (offset) offset[i] = bt->h.blk_off[i];
+            if (size) size[i] = bt->h.blk_size[i];
+        }
+    });
+}
+
+int ltg_bt_bidims(const ltg_bt *bt, int64_t *bidims) {
+    return guard([&] {
+        check_bt(bt);
+        for (int d = 0; d < bt->h.bis.n; d++) bidims[d] = bt->h.bis.bidims[d];
+    });
+}
+
+int ltg_bt_block_dims(const ltg_bt *bt, const int64_t *bidx, int64_t *dims) {
+    return guard([&] {
+        check_bt(bt);
+        if (!bidx || !dims) throw error(kErrBadArg, "null argument");
+        for (int d = 0; d < bt->h.bis.n; d++)
+            if (bidx[d] < 0 || bidx[d] >= bt->h.bis.bidims[d]) throw error(kErrBadArg, "block index out of range");
+        bt->h.bis.block_dims(bidx, dims);
+    });
+}
+
+int ltg_bt_nonzero(const ltg_bt *bt, int64_t *abs_idx, int64_t cap, int64_t *n) {
+    return guard([&] {
+        check_bt(bt);
+        int64_t k = 0;
+        for (size_t i = 0; i < bt->h.blk_abs.size(); i++) {
+            if (!bt->h.nonzero[i]) continue;
+            if (abs_idx && k < cap) abs_idx[k] = bt->h.blk_abs[i];
+            k++;
+        }
+        if (n) *n = k;
+    });
+}
+
+int ltg_bt_orbit(const ltg_bt *bt, int64_t abs_idx, int64_t *canonical, int32_t *perm,
+                 double *coeff, int32_t *allowed) {
+    return guard([&] {
+        check_bt(bt);
+        if (abs_idx < 0 || abs_idx >= bt->h.bis.nblocks()) throw error(kErrBadArg, "block index out of range");
+        const OrbitTable &o = bt->h.orbits;
+        if (canonical) *canonical = o.canon[abs_idx];
+        if (perm) for (int d = 0; d < bt->h.bis.n; d++) perm[d] = o.tr[abs_idx].perm.n ? o.tr[abs_idx].perm.p[d] : d;
+        if (coeff) *coeff = o.tr[abs_idx].coeff;
+        if (allowed) *allowed = o.allowed[abs_idx];
+    });
+}
+
+int ltg_bt_upload(ltg_bt *bt, const double *host) {
+    return guard([&] {
+        check_bt(bt);
+        need_dev(bt->ctx);
+        if (!host) throw error(kErrBadArg, "null host buffer");
+        LTG_CUDA(cudaMemcpyAsync(bt->arena.p, host, bt->h.total_elems * sizeof(double), cudaMemcpyHostToDevice, bt->ctx->stream));
+        LTG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+        std::fill(bt->h.nonzero.begin(), bt->h.nonzero.end(), 1);
+    });
+}
+
+int ltg_bt_download(ltg_bt *bt, double *host) {
+    return guard([&] {
+        check_bt(bt);
+        need_dev(bt->ctx);
+        if (!host) throw error(kErrBadArg, "null host buffer");
+        LTG_CUDA(cudaMemcpyAsync(host, bt->arena.p, bt->h.total_elems * sizeof(double), cudaMemcpyDeviceToHost, bt->ctx->stream));
+        LTG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+    });
+}
+
+int ltg_bt_upload_async(ltg_bt *bt, const double *host) {
+    return guard([&] {
+        check_bt(bt);
+        need_dev(bt->ctx);
+        if (!host) throw error(kErrBadArg, "null host buffer");
+        LTG_CUDA(cudaMemcpyAsync(bt->arena.p, host, bt->h.total_elems * sizeof(double), cudaMemcpyHostToDevice, bt->ctx->stream));
+        std::fill(bt->h.nonzero.begin(), bt->h.nonzero.end(), 1);
+    });
+}
+
+int ltg_bt_download_async(ltg_bt *bt, double *host) {
+    return guard([&] {
+        check_bt(bt);
+        need_dev(bt->ctx);
+        if (!host) throw error(kErrBadArg, "null host buffer");
+        LTG_CUDA(cudaMemcpyAsync(host, bt->arena.p, bt->h.total_elems * sizeof(double), cudaMemcpyDeviceToHost, bt->ctx->stream));
+    });
+}
+
+static int64_t slot_of_bidx(const ltg_bt *bt, const int64_t *bidx) {
+    for (int d = 0; d < bt->h.bis.n; d++)
+        if (bidx[d] < 0 || bidx[d] >= bt->h.bis.bidims[d]) throw error(kErrBadArg, "block index out of range");
+    int64_t a = bt->h.bis.abs(bidx);
+    int64_t s = bt->h.slot_of[a];
+    if (s < 0) throw error(kErrSymmetry, "block is not canonical or not allowed by the symmetry");
+    return s;
+}
+
+int ltg_bt_upload_block(ltg_bt *bt, const int64_t *bidx, const double *data) {
+    return guard([&] {
+        check_bt(bt);
+        need_dev(bt->ctx);
+        int64_t s = slot_of_bidx(bt, bidx);
+        LTG_CUDA(cudaMemcpyAsync(bt->arena.as<double>() + bt->h.blk_off[s], data, bt->h.blk_size[s] * sizeof(double), cudaMemcpyHostToDevice, bt->ctx->stream));
+        LTG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+        bt->h.nonzero[s] = 1;
+    });
+}
+
+int ltg_bt_download_block(ltg_bt *bt, const int64_t *bidx, double *data) {
+    return guard([&] {
+        check_bt(bt);
+        need_dev(bt->ctx);
+        int64_t s = slot_of_bidx(bt, bidx);
+        LTG_CUDA(cudaMemcpyAsync(data, bt->arena.as<double>() + bt->h.blk_off[s], bt->h.blk_size[s] * sizeof(double), cudaMemcpyDeviceToHost, bt->ctx->stream));
+        LTG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+    });
+}
+
+int ltg_bt_set_zero(ltg_bt *bt) {
+    return guard([&] {
+        check_bt(bt);
+        need_dev(bt->ctx);
+        LTG_CUDA(cudaMemsetAsync(bt->arena.p, 0, std::max<int64_t>(bt->h.total_elems, 1) * sizeof(double), bt->ctx->stream));
+        std::fill(bt->h.nonzero.begin(), bt->h.nonzero.end(), 0);
+    });
+}
+
+int ltg_bt_zero_block(ltg_bt *bt, const int64_t *bidx) {
+    return guard([&] {
+        check_bt(bt);
+        int64_t s = slot_of_bidx(bt, bidx);
+        if (bt->ctx->device >= 0)
+            LTG_CUDA(cudaMemsetAsync(bt->arena.as<double>() + bt->h.blk_off[s], 0,
+                                     bt->h.blk_size[s] * sizeof(double), bt->ctx->stream));
+        bt->h.nonzero[s] = 0;
+    });
+}
+
+int ltg_bt_mark_nonzero(ltg_bt *bt) {
+    return guard([&] { check_bt(bt); std::fill(bt->h.nonzero.begin(), bt->h.nonzero.end(), 1); });
+}
+
+int ltg_bt_fill_seeded(ltg_bt *bt, uint64_t seed, double scale) {
+    return guard([&] {
+        check_bt(bt);
+        need_dev(bt->ctx);
+        upload_directory(bt);
+        DGenGroup g = gen_group(bt->h);
+        LTG_CUDA(launch_fill_seeded(bt->arena.as<double>(), bt->dir_off.as<int64_t>(), bt->dir_start.as<int64_t>(),
+                                    bt->dir_ext.as<int32_t>(), (int32_t)bt->h.blk_abs.size(), bt->h.bis.n, g, seed,
+                                    two_m32(scale), bt->ctx->stream));
+        bt->ctx->launches++;
+        LTG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+        std::fill(bt->h.nonzero.begin(), bt->h.nonzero.end(), 1);
+    });
+}
+
+int ltg_bt_fill_seeded_host(const ltg_bt *bt, uint64_t seed, double scale, double *host) {
+    return guard([&] {
+        check_bt(bt);
+        if (!host) throw error(kErrBadArg, "null host buffer");
+        DGenGroup g = gen_group(bt->h);
+        const BlockTensorHost &h = bt->h;
+        const double sc = two_m32(scale);
+        int nt = std::max(1, std::min(bt->ctx->host_threads, 64));
+        std::vector<std::thread> th;
+        for (int w = 0; w < nt; w++) {
+            th.emplace_back([&, w] {
+                int64_t bidx[kMaxOrder], ext[kMaxOrder], x[kMaxOrder];
+                for (size_t i = w; i < h.blk_abs.size(); i += nt) {
+                    h.bis.unabs(h.blk_abs[i], bidx);
+                    h.bis.block_dims(bidx, ext);
+                    double *dst = host + h.blk_off[i];
+                    for (int64_t e = 0; e < h.blk_size[i]; e++) {
+                        int64_t r = e;
+                        for (int d = h.bis.n - 1; d >= 0; d--) {
+                            x[d] = h.bis.starts[d][bidx[d]] + r % ext[d];
+                            r /= ext[d];
+                        }
+                        dst[e] = seeded_value(g, seed, sc, x);
+                    }
+                    for (int64_t e = h.blk_size[i]; e < ((h.blk_size[i] + 3) & ~int64_t(3)); e++)
+                        if (h.blk_off[i] + e < h.total_elems) dst[e] = 0.0;
+                }
+            });
+        }
+        for (auto &t : th) t.join();
+    });
+}
+
+int ltg_bt_device_ptr(ltg_bt *bt, double **ptr) {
+    return guard([&] { check_bt(bt); if (!ptr) throw error(kErrBadArg, "null output"); *ptr = bt->arena.as<double>(); });
+}
+
+int ltg_contract2_create(ltg_ctx *ctx, int32_t n, int32_t m, int32_t k, const int32_t *permc,
+                         const int32_t *pairs, ltg_bt *a, ltg_bt *b, ltg_plan **out) {
+    return guard([&] {
+        check_ctx(ctx); check_bt(a); check_bt(b);
+        if (!out) throw error(kErrBadArg, "null output");
+        if (n < 0 || m < 0 || k < 0 || n + m < 1) throw error(kErrBadArg, "invalid contraction orders");
+        if (a->h.bis.n != n + k || b->h.bis.n != m + k) throw error(kErrBadDims, "argument orders do not match the contraction");
+        std::unique_ptr<ltg_plan> pl(new ltg_plan());
+        pl->ctx = ctx; pl->a = a; pl->b = b;
+        Contraction c;
+        c.init(n, m, k, perm_from(n + m, permc));
+        for (int q = 0; q < k; q++) c.contract(pairs[2 * q], pairs[2 * q + 1]);
+        contract2_schedule(c, a->h, b->h, pl->plan, ctx->host_threads);
+        *out = pl.release();
+    });
+}
+
+int ltg_contract2_make_result(ltg_plan *plan, ltg_bt **c) {
+    return guard([&] {
+        if (!plan || !c) throw error(kErrBadArg, "null argument");
+        std::unique_ptr<ltg_bt> bt(new ltg_bt());
+        bt->ctx = plan->ctx;
+        bt->h.bis = plan->plan.bisc;
+        bt->h.sym = plan->plan.symc;
+        alloc_arena(bt.get());
+        *c = bt.release();
+    });
+}
+
+int ltg_plan_schedule(ltg_plan *plan, int64_t *abs_idx, int64_t cap, int64_t *n) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        const auto &s = plan->plan.schedule;
+        for (size_t i = 0; i < s.size() && (int64_t)i < cap; i++) abs_idx[i] = s[i];
+        if (n) *n = (int64_t)s.size();
+    });
+}
+
+int ltg_plan_pairs(ltg_plan *plan, int64_t i, int64_t *out, int64_t cap, int64_t *npairs) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (i < 0 || i >= (int64_t)plan->plan.clst.size()) throw error(kErrBadArg, "schedule index out of range");
+        const auto &lst = plan->plan.clst[i];
+        const int NA = plan->plan.contr.NA(), NB = plan->plan.contr.NB();
+        const int64_t rec = 2 + NA + 1 + 2 + NB + 1;
+        int64_t k = 0;
+        for (const Pair &p : lst) {
+            if ((k + 1) * rec <= cap) {
+                int64_t *o = out + k * rec;
+                o[0] = p.aia; o[1] = p.acia;
+                for (int d = 0; d < NA; d++) o[2 + d] = p.tra.perm.n ? p.tra.perm.p[d] : d;
+                std::memcpy(&o[2 + NA], &p.tra.coeff, 8);
+                int64_t *q = o + 3 + NA;
+                q[0] = p.aib; q[1] = p.acib;
+                for (int d = 0; d < NB; d++) q[2 + d] = p.trb.perm.n ? p.trb.perm.p[d] : d;
+                std::memcpy(&q[2 + NB], &p.trb.coeff, 8);
+            }
+            k++;
+        }
+        if (npairs) *npairs = k;
+    });
+}
+
+int ltg_plan_flops(ltg_plan *plan, double *flops) {
+    return guard([&] { if (!plan || !flops) throw error(kErrBadArg, "null argument"); *flops = plan->plan.flops; });
+}
+
+int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, double ka, double kb,
+                  double kc, int32_t add, double d) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        check_bt(c);
+        need_dev(plan->ctx);
+        if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
+        (void)nslices;
+        if (mode != LTG_MODE_PLAIN_FP64) throw error(kErrUnsupported, "split-precision modes are not built in this library");
+        ltg_ctx *ctx = plan->ctx;
+        cudaStream_t s = ctx->stream;
+        ContractExec *ex = prepare_exec(plan, c, ka, kb, kc, add, d);
+        if (!add)
+            for (auto &r : ex->zero_ranges)
+                LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
+        int slot = 0;
+        for (auto &l : ex->launches) {
+            LTG_CUDA(launch_contract_fp64(ex->tasks.as<DTask>(), ex->cblks.as<DCBlock>(),
+                                          ex->items.as<DItem>() + l.second.first, l.second.second,
+                                          ctx->scratch_counter.as<int32_t>() + (slot++ % 64),
+                                          plan->a->arena.as<double>(), plan->b->arena.as<double>(),
+                                          c->arena.as<double>(), add, l.first, s));
+            ctx->launches++;
+        }
+        if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
+        for (int64_t sl : ex->sched_slots) c->h.nonzero[sl] = 1;
+        if (!ctx->capturing) LTG_CUDA(cudaGetLastError());
+    });
+}
+
+int ltg_plan_destroy(ltg_plan *plan) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (plan->ctx->device >= 0) cudaStreamSynchronize(plan->ctx->stream);
+        delete plan;
+    });
+}
+
+int ltg_copy(ltg_bt *a, const int32_t *perm, double c, ltg_bt *b, int32_t add, double d) {
+    return guard([&] {
+        check_bt(a);
+        need_dev(a->ctx); check_bt(b);
+        run_transfer(a->ctx, {a}, {perm_from(a->h.bis.n, perm)}, {c}, b, add != 0, d);
+    });
+}
+
+int ltg_add(int32_t nterms, ltg_bt *const *a, const int32_t *perms, const double *coeffs, ltg_bt *b,
+            int32_t add, double d) {
+    return guard([&] {
+        check_bt(b);
+        need_dev(b->ctx);
+        if (nterms < 1 || !a || !coeffs) throw error(kErrBadArg, "add needs at least one operand");
+        std::vector<ltg_bt *> srcs;
+        std::vector<Perm> ps;
+        std::vector<double> cs;
+        for (int t = 0; t < nterms; t++) {
+            check_bt(a[t]);
+            srcs.push_back(a[t]);
+            ps.push_back(perm_from(b->h.bis.n, perms ? perms + (size_t)t * b->h.bis.n : nullptr));
+            cs.push_back(coeffs[t]);
+        }
+        run_transfer(b->ctx, srcs, ps, cs, b, add != 0, d);
+    });
+}
+
+int ltg_dotprod_async(ltg_bt *a, const int32_t *perma, ltg_bt *b, const int32_t *permb, double *dev_out) {
+    return guard([&] {
+        check_bt(a);
+        need_dev(a->ctx); check_bt(b);
+        if (a->ctx != b->ctx) throw error(kErrBadArg, "operands belong to different contexts");
+        DotExec *ex = prepare_dot(a, perm_from(a->h.bis.n, perma), b, perm_from(b->h.bis.n, permb));
+        LTG_CUDA(launch_dot(ex->jobs.as<DJob>(), ex->terms.as<DTerm>(), ex->units.as<DUnit>(), ex->nunits,
+                            a->arena.as<double>(), b->arena.as<double>(), ex->partials.as<double>(), dev_out,
+                            a->ctx->stream));
+        a->ctx->launches += 2;
+    });
+}
+
+int ltg_dotprod(ltg_bt *a, const int32_t *perma, ltg_bt *b, const int32_t *permb, double *out) {
+    int st = ltg_dotprod_async(a, perma, b, permb, a ? a->ctx->dot_out.as<double>() : nullptr);
+    if (st != kOk) return st;
+    return guard([&] {
+        if (!out) throw error(kErrBadArg, "null output");
+        LTG_CUDA(cudaMemcpyAsync(out, a->ctx->dot_out.p, sizeof(double), cudaMemcpyDeviceToHost, a->ctx->stream));
+        LTG_CUDA(cudaStreamSynchronize(a->ctx->stream));
+    });
+}
+
+int ltg_scale(ltg_bt *a, double c) {
+    return guard([&] {
+        check_bt(a);
+        need_dev(a->ctx);
+        LTG_CUDA(launch_scale(a->arena.as<double>(), a->h.total_elems, c, a->ctx->stream));
+        a->ctx->launches++;
+    });
+}
+
+int ltg_denominator(ltg_bt *a, const double *eps_host, int32_t nocc) {
+    return guard([&] {
+        check_bt(a);
+        need_dev(a->ctx);
+        if (a->h.bis.n != 4) throw error(kErrUnsupported, "denominator is defined for 4-index tensors");
+        if (a->ctx->capturing) throw error(kErrState, "denominator uploads its orbital energies and cannot run during graph capture");
+        upload_directory(a);
+        int64_t tot = 0;
+        std::vector<int64_t> off(kDevMaxOrder, 0);
+        for (int d = 0; d < 4; d++) { off[d] = tot; tot += a->h.bis.dims[d]; }
+        std::vector<double> eps(eps_host, eps_host + tot);
+        DevBuf de, doff;
+        upload_vec(de, eps, a->ctx->stream);
+        upload_vec(doff, off, a->ctx->stream);
+        LTG_CUDA(launch_denominator(a->arena.as<double>(), a->dir_off.as<int64_t>(), a->dir_start.as<int64_t>(),
+                                    a->dir_ext.as<int32_t>(), (int32_t)a->h.blk_abs.size(), de.as<double>(),
+                                    doff.as<int64_t>(), nocc, a->ctx->stream));
+        a->ctx->launches++;
+        LTG_CUDA(cudaStreamSynchronize(a->ctx->stream));
+    });
+}
+
+int ltg_graph_begin(ltg_ctx *ctx) {
+    return guard([&] {
+        check_ctx(ctx);
+        need_dev(ctx);
+        if (ctx->capturing) throw error(kErrState, "capture already active");
+        LTG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        ctx->capturing = true;
+    });
+}
+
+int ltg_graph_end(ltg_ctx *ctx, ltg_graph **out) {
+    return guard([&] {
+        check_ctx(ctx);
+        if (!ctx->capturing) throw error(kErrState, "no capture active");
+        ctx->capturing = false;
+        std::unique_ptr<ltg_graph> g(new ltg_graph());
+        g->ctx = ctx;
+        LTG_CUDA(cudaStreamEndCapture(ctx->stream, &g->graph));
+        LTG_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+        if (out) *out = g.release();
+    });
+}
+
+int ltg_graph_launch(ltg_graph *g) {
+    return guard([&] {
+        if (!g) throw error(kErrBadArg, "null graph");
+        LTG_CUDA(cudaGraphLaunch(g->exec, g->ctx->stream));
+    });
+}
+
+int ltg_graph_destroy(ltg_graph *g) {
+    return guard([&] {
+        if (!g) throw error(kErrBadArg, "null graph");
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        if (g->graph) cudaGraphDestroy(g->graph);
+        delete g;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+// Device-side data layouts of the B200 block-tensor path and the kernel
+// launchers shared by the C ABI layer.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ltg {
+
+constexpr int kDevMaxSub = 4;     // sub-dimension groups per GEMM axis
+constexpr int kDevMaxOrder = 8;
+
+// ---------------------------------------------------------------- contraction
+
+// One (C block, pair) product:  C[m,n] += coeff * sum_k A[m,k] * B[n,k]
+// with A/B element offsets  a_off + sum_i digit_m[i]*ma_str[i] + sum_j digit_k[j]*ka_str[j].
+// All within-block strides fit 32 bits (a block holds < 2^31 elements).
+struct DTask {
+    int64_t a_off, b_off;
+    double coeff;                 // relative to the owning C block's scale
+    int32_t K;
+    int32_t nk, nm, nn;
+    int32_t kext[kDevMaxSub], ka_str[kDevMaxSub], kb_str[kDevMaxSub];
+    int32_t mext[kDevMaxSub], ma_str[kDevMaxSub];
+    int32_t next[kDevMaxSub], nb_str[kDevMaxSub];
+};
+
+// One canonical C block of the schedule.
+struct DCBlock {
+    int64_t c_off;
+    double scale;                 // kc (and d in add mode) times the first pair's coefficient
+    int32_t M, N;
+    int32_t nm, nn;
+    int32_t mext[kDevMaxSub], mc_str[kDevMaxSub];
+    int32_t next[kDevMaxSub], nc_str[kDevMaxSub];
+    int32_t t_begin, t_end;       // task range
+};
+
+// One CTA work item: an (m, n) tile of a C block.
+struct DItem {
+    int32_t cblk;
+    int32_t m0, n0;
+    int32_t pad;
+};
+
+// ---------------------------------------------------------------- element-wise
+
+constexpr int kMaxTerms = 8;
+
+// One destination block of a copy/add (or one A/B block pair of a dot
+// product): extents of the destination dims and, per term, the source offset
+// and the source stride of every destination dim.
+struct DJob {
+    int64_t dst_off;
+    int32_t ndim, inner;          // inner = ext[ndim-1]
+    int32_t nterms, term0;        // terms[term0 .. term0+nterms)
+    int32_t ext[kDevMaxOrder];
+};
+
+struct DTerm {
+    int64_t src_off;
+    double coeff;
+    int32_t src;                  // source tensor index
+    int32_t pad;
+    int32_t sstr[kDevMaxOrder];
+};
+
+// A contiguous row range of one job processed by one CTA.
+struct DUnit {
+    int32_t job;
+    int32_t pad;
+    int64_t row_begin, row_end;
+};
+
+// ---------------------------------------------------------------- seeded inputs
+
+// Counter-based test-input generator, identical on host and device.
+// g(seed, x) is the centred sum of twelve 32-bit uniforms drawn from
+// splitmix64 (Steele, Lea & Flood, OOPSLA 2014) keyed by the element's
+// linear index in the full dense tensor: an integer in (-6*2^32, 6*2^32) with
+// the variance of N(0,1) * 2^32 (the classic sum-of-12-uniforms normal
+// approximation).  A symmetrised value is sum_{P in G} c_P * g(P x); the
+// final double is that integer times scale * 2^-32, one correctly rounded
+// multiply, so host and device produce the same bits.
+__host__ __device__ inline uint64_t sm64_mix(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+__host__ __device__ inline int64_t seeded_int(uint64_t seed, uint64_t lin) {
+    uint64_t key = sm64_mix(seed);
+    uint64_t s = 0;
+    for (int r = 0; r < 6; r++) {
+        uint64_t h = sm64_mix(key + lin * 6u + (uint64_t)r);
+        s += (h & 0xffffffffULL) + (h >> 32);
+    }
+    return (int64_t)s - (int64_t)(6ULL << 32);
+}
+
+// Symmetry group of the generator (full group closure, perm + coefficient).
+struct DGenGroup {
+    int32_t order;                 // tensor order
+    int32_t ngroup;                // group elements
+    int8_t perm[48][kDevMaxOrder]; // element permutations
+    int8_t coeff[48];              // +1 / -1
+    int64_t dims[kDevMaxOrder];    // full tensor extents
+};
+
+__host__ __device__ inline double seeded_value(const DGenGroup &g, uint64_t seed,
+                                               double scale_2m32, const int64_t *x) {
+    int64_t v = 0;
+    for (int e = 0; e < g.ngroup; e++) {
+        uint64_t lin = 0;
+        for (int d = 0; d < g.order; d++) lin = lin * (uint64_t)g.dims[d] + (uint64_t)x[g.perm[e][d]];
+        int64_t s = seeded_int(seed, lin);
+        v += g.coeff[e] > 0 ? s : -s;
+    }
+#ifdef __CUDA_ARCH__
+    return __dmul_rn((double)v, scale_2m32);
+#else
+    return (double)v * scale_2m32;
+#endif
+}
+
+// ---------------------------------------------------------------- launchers
+
+// Plain FP64 DMMA grouped contraction over all work items.
+cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
+    const DItem *items, int32_t nitems, int32_t *counter, const double *a,
+    const double *b, double *c, int32_t add, int32_t tile_cfg, cudaStream_t s);
+
+// Element-wise transfer kernels.
+cudaError_t launch_transfer(const DJob *jobs, const DTerm *terms, const DUnit *units,
+    int32_t nunits, const double *const *srcs, double *dst, int32_t accumulate,
+    double beta, cudaStream_t s);
+cudaError_t launch_dot(const DJob *jobs, const DTerm *terms, const DUnit *units,
+    int32_t nunits, const double *a, const double *b, double *partials, double *out,
+    cudaStream_t s);
+cudaError_t launch_scale(double *x, int64_t n, double c, cudaStream_t s);
+cudaError_t launch_fill_seeded(double *arena, const int64_t *blk_off,
+    const int64_t *blk_start, const int32_t *blk_ext, int32_t nblk, int32_t order,
+    const DGenGroup &g, uint64_t seed, double scale_2m32, cudaStream_t s);
+cudaError_t launch_denominator(double *arena, const int64_t *blk_off,
+    const int64_t *blk_start, const int32_t *blk_ext, int32_t nblk,
+    const double *eps, const int64_t *eps_off, int32_t nocc, cudaStream_t s);
+
+}  // namespace ltg
