@@ -30,6 +30,7 @@ WORKLOADS = {
     "ladder-split": "LADDER_SPLIT",
     "ladder-small": "LADDER_SMALL",
     "ladder-ccd": "LADDER_CCD",
+    "ladder-prof": "LADDER_PROF",
     "ring": "RING_D2H",
     "ring-small": "RING_D2H_SMALL",
 }

@@ -310,6 +310,20 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     std::vector<GemmTask> tasks;
     std::vector<CBlockTask> cbt;
     contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    // Every address a task can form must lie inside its arena.
+    auto span = [](const SubDims &s, bool second) {
+        int64_t m = 0;
+        for (int i = 0; i < s.n; i++) m += (int64_t)(s.ext[i] - 1) * (second ? s.s1[i] : s.s0[i]);
+        return m;
+    };
+    for (const GemmTask &t : tasks) {
+        int64_t amax = t.a_off + span(t.m, false) + span(t.k, false);
+        int64_t bmax = t.b_off + span(t.n, false) + span(t.k, true);
+        int64_t cmax = t.c_off + span(t.m, true) + span(t.n, true);
+        if (t.a_off < 0 || amax >= pl->a->h.total_elems || t.b_off < 0 || bmax >= pl->b->h.total_elems ||
+            t.c_off < 0 || cmax >= c->h.total_elems)
+            throw error(kErrState, "contraction task addresses outside an operand arena");
+    }
     std::vector<DTask> dt(tasks.size());
     for (size_t i = 0; i < tasks.size(); i++) {
         const GemmTask &t = tasks[i];
@@ -384,6 +398,25 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
 
 // ------------------------------------------------------------ transfers
 
+// Every address a transfer/dot job can form must lie inside its arena.
+void validate_transfer(const TransferPlan &plan, const std::vector<int64_t> &src_sizes, int64_t dst_size) {
+    for (const TJob &j : plan.jobs) {
+        int64_t n = 1;
+        for (int d = 0; d < j.ndim; d++) n *= j.ext[d];
+        if (dst_size >= 0 && (j.dst_off < 0 || j.dst_off + n > dst_size))
+            throw error(kErrState, "transfer destination outside its arena");
+        for (int t = 0; t < j.nterms; t++) {
+            const TTerm &tm = plan.terms[j.term0 + t];
+            int64_t m = tm.src_off;
+            for (int d = 0; d < j.ndim; d++) m += (int64_t)(j.ext[d] - 1) * tm.sstr[d];
+            if (tm.src < 0 || tm.src >= (int)src_sizes.size() || tm.src_off < 0 || m >= src_sizes[tm.src])
+                throw error(kErrState, "transfer source outside its arena");
+        }
+    }
+    for (const TUnit &u : plan.units)
+        if (u.job < 0 || u.job >= (int32_t)plan.jobs.size()) throw error(kErrState, "bad transfer unit");
+}
+
 // Cached copy/add plans: the first call for a given (operands, permutations,
 // coefficients, destination, mode) builds and uploads the task arrays; later
 // calls, including calls inside a CUDA-graph capture, only launch.
@@ -427,6 +460,9 @@ void run_transfer(ltg_ctx *ctx, const std::vector<ltg_bt *> &srcs, const std::ve
             terms.push_back(TransferTerm{&srcs[t]->h, perms[t], coeffs[t], (int32_t)t});
         TransferPlan plan;
         plan_transfer(terms, dst->h, add, plan);
+        std::vector<int64_t> ssz;
+        for (ltg_bt *b : srcs) ssz.push_back(b->h.total_elems);
+        validate_transfer(plan, ssz, dst->h.total_elems);
         std::unique_ptr<TransferExec> nx(new TransferExec());
         upload_vec(nx->jobs, plan.jobs, s);
         upload_vec(nx->terms, plan.terms, s);
@@ -477,6 +513,7 @@ DotExec *prepare_dot(ltg_bt *a, const Perm &pa, ltg_bt *b, const Perm &pb) {
     if (a->ctx->capturing) throw error(kErrState, "dot product not prepared before graph capture");
     TransferPlan plan;
     plan_dot(a->h, pa, b->h, pb, plan);
+    validate_transfer(plan, {a->h.total_elems, b->h.total_elems}, -1);
     std::unique_ptr<DotExec> ex(new DotExec());
     cudaStream_t s = a->ctx->stream;
     upload_vec(ex->jobs, plan.jobs, s);

@@ -196,6 +196,7 @@ LADDER_SMALL = LadderConfig("ladder o=10 v=40", [5], [16, 4])
 LADDER_LARGE = LadderConfig("ladder o=40 v=240", [20], [48, 40, 32])
 LADDER_SPLIT = LadderConfig("ladder o=40 v=240 (64,56)", [20], [64, 56])
 LADDER_CCD = LadderConfig("ladder o=30 v=300", [15], [50, 50, 50])
+LADDER_PROF = LadderConfig("ladder o=40 v=160", [20], [48, 32])   # profiling size (< 1 GB)
 
 D2H_OCC = [6, 2, 3, 1, 5, 2, 3, 1]
 D2H_VIR = [40, 12, 18, 8, 36, 10, 16, 8]
