@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--nslices", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--tile", type=int, default=-1, help="force one tile shape (debug)")
     return p.parse_args()
 
 
@@ -246,6 +248,11 @@ def ltg_arm(args):
         torch.cuda.synchronize()
         ctx.synchronize()
 
+    tiles = None
+    if args.tile >= 0:
+        op.set_tile(args.tile)
+    elif not args.no_autotune:
+        tiles = op.autotune(C, mode=mode, nslices=args.nslices, reps=1)
     for _ in range(max(3, args.warmup)):
         op.perform(C, mode=mode, nslices=args.nslices)
     barrier()
@@ -327,6 +334,8 @@ def ltg_arm(args):
                         "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU (FP64 tensor path); "
                                        f"nominal {FP64_NOMINAL} TFLOP/s"},
            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+    if tiles:
+        out["config"]["autotuned_tiles"] = {f"{m}x{n}": t for (m, n), t in tiles.items()}
     print(json.dumps(out))
 
 

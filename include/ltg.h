@@ -161,6 +161,18 @@ int ltg_plan_flops(ltg_plan *plan, double *flops);
 int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices,
                   double ka, double kb, double kc, int32_t add, double d);
 int ltg_plan_destroy(ltg_plan *plan);
+/* Forces one tile shape for every C block (cfg >= 0) or restores the
+ * automatic choice (-1).  No reference counterpart: the reference hands each
+ * block pair to BLAS. */
+int ltg_contract2_set_tile(ltg_plan *plan, int32_t cfg);
+/* Autotuner: for every distinct C-block shape (M, N) of the plan, costliest
+ * first, times each compiled tile shape on the real contraction (reps calls,
+ * CUDA events) and keeps the fastest.  Overwrites c. */
+int ltg_contract2_autotune(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices,
+                           double ka, double kb, double kc, int32_t reps);
+/* Autotuned table: C-block shape -> tile shape index. */
+int ltg_plan_tiles(ltg_plan *plan, int64_t *m, int64_t *n, int32_t *cfg, int64_t cap,
+                   int64_t *count);
 
 /* ---- btod_copy / btod_add / btod_dotprod ------------------------------ */
 /* b = c * perm(a)  or  b += d * c * perm(a)   (btod_copy.h:38-115) */

@@ -84,6 +84,10 @@ _SIGS = {
     "ltg_contract2": (C.c_int, [c_vp, c_vp, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                 C.c_double, C.c_int32, C.c_double]),
     "ltg_plan_destroy": (C.c_int, [c_vp]),
+    "ltg_contract2_set_tile": (C.c_int, [c_vp, C.c_int32]),
+    "ltg_contract2_autotune": (C.c_int, [c_vp, c_vp, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                         C.c_double, C.c_int32]),
+    "ltg_plan_tiles": (C.c_int, [c_vp, c_i64p, c_i64p, c_i32p, C.c_int64, c_i64p]),
     "ltg_copy": (C.c_int, [c_vp, c_i32p, C.c_double, c_vp, C.c_int32, C.c_double]),
     "ltg_add": (C.c_int, [C.c_int32, C.POINTER(c_vp), c_i32p, c_dblp, c_vp, C.c_int32, C.c_double]),
     "ltg_dotprod": (C.c_int, [c_vp, c_i32p, c_vp, c_i32p, c_dblp]),

@@ -283,6 +283,23 @@ class btod_contract2:
         check(lib().ltg_contract2_make_result(self.h, C.byref(h)))
         return block_tensor(self.a.ctx, None, _handle=h)
 
+    def set_tile(self, cfg: int):
+        check(lib().ltg_contract2_set_tile(self.h, cfg))
+
+    def autotune(self, c: block_tensor, mode: int = MODE_PLAIN_FP64, nslices: int = 0, reps: int = 2):
+        check(lib().ltg_contract2_autotune(self.h, c.h, mode, nslices, self.ka, self.kb, self.kc, reps))
+        return self.tiles()
+
+    def tiles(self):
+        n = C.c_int64()
+        check(lib().ltg_plan_tiles(self.h, None, None, None, 0, C.byref(n)))
+        m = np.zeros(max(1, n.value), np.int64)
+        nn = np.zeros(max(1, n.value), np.int64)
+        cfg = np.zeros(max(1, n.value), np.int32)
+        check(lib().ltg_plan_tiles(self.h, m.ctypes.data_as(_capi.c_i64p), nn.ctypes.data_as(_capi.c_i64p),
+                                   cfg.ctypes.data_as(_capi.c_i32p), n.value, C.byref(n)))
+        return {(int(a), int(b)): int(c) for a, b, c in zip(m[:n.value], nn[:n.value], cfg[:n.value])}
+
     def perform(self, c: block_tensor, d: Optional[float] = None, mode: int = MODE_PLAIN_FP64,
                 nslices: int = 0):
         check(lib().ltg_contract2(self.h, c.h, mode, nslices, self.ka, self.kb, self.kc,

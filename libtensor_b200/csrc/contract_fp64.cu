@@ -5,26 +5,28 @@
 // schedule, the per-block tod_contract2 call chain
 // (libtensor/dense_tensor/impl/tod_contract2_impl.h:104-393): the perma/permb
 // staging copies, the dgemm (linalg_cblas_level3.C:18-58) and the permc
-// permute-add.  Here one persistent launch walks all (C block, m-tile,
-// n-tile) work items; each work item accumulates every coalesced pair of its
-// C block in registers, so there are no temporaries and no atomics.
+// permute-add.  One persistent launch walks all (C block, m-tile, n-tile)
+// work items from a work queue; each work item accumulates every coalesced
+// pair of its C block in registers, so there are no temporaries and no
+// atomics, and every C element is written once.
 //
 // The index permutation of a pair is folded into the tile loader: the
 // element (m, k) of the matricised A block lives at
 //   a_off + sum_i digit_i(m) * ma_str[i] + sum_j digit_j(k) * ka_str[j]
 // (mixed-radix digits over the fused sub-dimensions), computed once per tile
 // row and once per k column per stage, and copied with cp.async (zero-filled
-// outside the block).  Shared-memory tiles keep k contiguous with the k index
-// permuted inside every group of 8 so that one 16-byte shared load returns
-// both k and k+4, which is exactly the pair an m16n8k8 f64 fragment needs.
+// outside the block); 16-byte copies when the pair's k run is contiguous and
+// even-aligned, 8-byte copies otherwise.
+//
+// Fragment k order: the m16n8k8 f64 fragment holds k-slots (t, t+4) of A
+// row g and of B column g in lane (g, t).  Any consistent relabelling of the
+// 8 k values gives the same sum, so slot t carries k = 2t and slot t+4
+// carries k = 2t+1: both operands then read one 16-byte shared-memory word
+// per fragment register pair, from a tile stored in natural k order.
 #include "ltg_device.cuh"
 
 namespace ltg {
 namespace {
-
-__device__ __forceinline__ int kperm8(int kk) {
-    return (kk & ~7) | ((kk & 3) << 1) | ((kk >> 2) & 1);
-}
 
 __device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_t *ext,
                                                 const int32_t *str) {
@@ -43,6 +45,11 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pre
     int sz = pred ? 8 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" :: "r"(s), "l"(gmem), "r"(sz));
 }
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = pred ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(s), "l"(gmem), "r"(sz));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template<int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N)); }
@@ -60,44 +67,61 @@ struct TileCfg {
     static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_, STAGES = STAGES_;
     static constexpr int kWarpsM = BM / WM, kWarpsN = BN / WN;
     static constexpr int kThreads = kWarpsM * kWarpsN * 32;
-    static constexpr int kLd = BK + 8;          // padded row stride in doubles
+    static constexpr int kLd = BK + 8;          // padded row stride in doubles (conflict-free 16B reads)
     static constexpr int kMT = WM / 16, kNT = WN / 8;
     static constexpr int kStageA = BM * kLd, kStageB = BN * kLd;
     static constexpr size_t kSmem = (size_t)STAGES * (kStageA + kStageB) * sizeof(double)
                                   + (size_t)(BM + BN) * sizeof(int64_t);
-    static_assert(kThreads % BK == 0, "loader assumes a fixed k column per thread");
-    static_assert((BM * BK) % kThreads == 0 && (BN * BK) % kThreads == 0, "tile/threads");
+    static_assert(kThreads % BK == 0 && kThreads % (BK / 2) == 0, "loader assumes a fixed k column per thread");
+    static_assert(BM % WM == 0 && BN % WN == 0 && WM % 16 == 0 && WN % 8 == 0, "warp tiling");
+    static_assert(BK % 8 == 0, "k step");
 };
+
+// Copies the (rows x BK) slab starting at k0 of one operand into shared
+// memory.  rowoff[r] < 0 marks rows outside the block (zero fill).
+template<class C, int ROWS>
+__device__ __forceinline__ void load_operand(double *s, const int64_t *rowoff,
+    const double *__restrict__ G, int k0, int K, int nk, const int32_t *kext,
+    const int32_t *kstr, bool vec16) {
+    const int tid = threadIdx.x;
+    if (vec16) {
+        constexpr int kCols = C::BK / 2;
+        constexpr int kRowsPerPass = C::kThreads / kCols;
+        const int kk = (tid % kCols) * 2;
+        const int k = k0 + kk;
+        const bool kin = k < K;          // K is even on this path
+        const int64_t ko = kin ? mixed_offset(k, nk, kext, kstr) : 0;
+#pragma unroll
+        for (int r0 = 0; r0 < ROWS; r0 += kRowsPerPass) {
+            int r = r0 + tid / kCols;
+            if (ROWS % kRowsPerPass != 0 && r >= ROWS) break;
+            int64_t ro = rowoff[r];
+            bool p = kin && ro >= 0;
+            cp_async16(&s[r * C::kLd + kk], p ? (const void *)(G + ro + ko) : (const void *)G, p);
+        }
+    } else {
+        constexpr int kRowsPerPass = C::kThreads / C::BK;
+        const int kk = tid % C::BK;
+        const int k = k0 + kk;
+        const bool kin = k < K;
+        const int64_t ko = kin ? mixed_offset(k, nk, kext, kstr) : 0;
+#pragma unroll
+        for (int r0 = 0; r0 < ROWS; r0 += kRowsPerPass) {
+            int r = r0 + tid / C::BK;
+            if (ROWS % kRowsPerPass != 0 && r >= ROWS) break;
+            int64_t ro = rowoff[r];
+            bool p = kin && ro >= 0;
+            cp_async8(&s[r * C::kLd + kk], p ? (const void *)(G + ro + ko) : (const void *)G, p);
+        }
+    }
+}
 
 template<class C>
 __device__ __forceinline__ void load_stage(double *sA, double *sB, const int64_t *rowA,
     const int64_t *rowB, const double *__restrict__ A, const double *__restrict__ B,
     const DTask &t, int k0) {
-    const int tid = threadIdx.x;
-    const int kk = tid % C::BK;
-    const int k = k0 + kk;
-    const bool kin = k < t.K;
-    int64_t koa = 0, kob = 0;
-    if (kin) {
-        koa = mixed_offset(k, t.nk, t.kext, t.ka_str);
-        kob = mixed_offset(k, t.nk, t.kext, t.kb_str);
-    }
-    const int col = kperm8(kk);
-    constexpr int kRowsPerPass = C::kThreads / C::BK;
-#pragma unroll
-    for (int r0 = 0; r0 < C::BM; r0 += kRowsPerPass) {
-        int r = r0 + tid / C::BK;
-        int64_t ro = rowA[r];
-        bool p = kin && ro >= 0;
-        cp_async8(&sA[r * C::kLd + col], p ? (const void *)(A + ro + koa) : (const void *)A, p);
-    }
-#pragma unroll
-    for (int r0 = 0; r0 < C::BN; r0 += kRowsPerPass) {
-        int r = r0 + tid / C::BK;
-        int64_t ro = rowB[r];
-        bool p = kin && ro >= 0;
-        cp_async8(&sB[r * C::kLd + col], p ? (const void *)(B + ro + kob) : (const void *)B, p);
-    }
+    load_operand<C, C::BM>(sA, rowA, A, k0, t.K, t.nk, t.kext, t.ka_str, t.vec_a != 0);
+    load_operand<C, C::BN>(sB, rowB, B, k0, t.K, t.nk, t.kext, t.kb_str, t.vec_b != 0);
 }
 
 template<class C>
@@ -175,29 +199,36 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
                     cp_async_commit();
                 }
                 const int st = kt % C::STAGES;
-                const double *tA = sA + st * C::kStageA;
-                const double *tB = sB + st * C::kStageB;
-#pragma unroll
-                for (int ks = 0; ks < C::BK; ks += 8) {
-                    double af[C::kMT][4], bf[C::kNT][2];
+                const double *tA = sA + st * C::kStageA + (wm * C::WM + g) * C::kLd + 2 * t4;
+                const double *tB = sB + st * C::kStageB + (wn * C::WN + g) * C::kLd + 2 * t4;
+                double af[2][C::kMT][4], bf[2][C::kNT][2];
+                auto load_frags = [&](int buf, int ks) {
 #pragma unroll
                     for (int i = 0; i < C::kMT; i++) {
-                        const int row = wm * C::WM + i * 16 + g;
-                        double2 lo = *reinterpret_cast<const double2 *>(&tA[row * C::kLd + ks + 2 * t4]);
-                        double2 hi = *reinterpret_cast<const double2 *>(&tA[(row + 8) * C::kLd + ks + 2 * t4]);
-                        af[i][0] = lo.x; af[i][2] = lo.y; af[i][1] = hi.x; af[i][3] = hi.y;
+                        double2 lo = *reinterpret_cast<const double2 *>(tA + (i * 16) * C::kLd + ks);
+                        double2 hi = *reinterpret_cast<const double2 *>(tA + (i * 16 + 8) * C::kLd + ks);
+                        af[buf][i][0] = lo.x; af[buf][i][2] = lo.y; af[buf][i][1] = hi.x; af[buf][i][3] = hi.y;
                     }
 #pragma unroll
                     for (int j = 0; j < C::kNT; j++) {
-                        const int col = wn * C::WN + j * 8 + g;
-                        double2 v = *reinterpret_cast<const double2 *>(&tB[col * C::kLd + ks + 2 * t4]);
-                        bf[j][0] = scale_b ? v.x * coef : v.x;
-                        bf[j][1] = scale_b ? v.y * coef : v.y;
+                        double2 v = *reinterpret_cast<const double2 *>(tB + (j * 8) * C::kLd + ks);
+                        bf[buf][j][0] = v.x;
+                        bf[buf][j][1] = v.y;
+                    }
+                };
+                load_frags(0, 0);
+#pragma unroll
+                for (int ks = 0; ks < C::BK; ks += 8) {
+                    const int cur = (ks / 8) & 1;
+                    if (ks + 8 < C::BK) load_frags(cur ^ 1, ks + 8);
+                    if (scale_b) {
+#pragma unroll
+                        for (int j = 0; j < C::kNT; j++) { bf[cur][j][0] *= coef; bf[cur][j][1] *= coef; }
                     }
 #pragma unroll
                     for (int i = 0; i < C::kMT; i++)
 #pragma unroll
-                        for (int j = 0; j < C::kNT; j++) dmma_16x8x8(acc[i][j], af[i], bf[j]);
+                        for (int j = 0; j < C::kNT; j++) dmma_16x8x8(acc[i][j], af[cur][i], bf[cur][j]);
                 }
             }
             cp_async_wait<0>();
@@ -243,16 +274,16 @@ template<class C>
 cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *items,
                        int32_t nitems, int32_t *counter, const double *a, const double *b,
                        double *c, int32_t add, cudaStream_t s) {
-    static bool configured = false;
+    static int configured_dev = -1;
     cudaError_t e;
-    if (!configured) {
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    if (configured_dev != dev) {
         e = cudaFuncSetAttribute(contract_fp64_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)C::kSmem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured_dev = dev;
     }
-    int dev = 0, nsm = 0;
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     int grid = nitems < nsm ? nitems : nsm;
     if (grid < 1) return cudaSuccess;
@@ -263,16 +294,27 @@ cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *it
     return cudaGetLastError();
 }
 
+// Tile configurations (BM, BN, BK, warp tile M, warp tile N, stages).
+using Cfg0 = TileCfg<128, 128, 16, 64, 32, 4>;
+using Cfg1 = TileCfg<64, 64, 32, 32, 32, 3>;
+using Cfg2 = TileCfg<64, 128, 32, 32, 32, 3>;
+using Cfg3 = TileCfg<32, 32, 32, 16, 16, 3>;
+using Cfg4 = TileCfg<80, 128, 32, 80, 16, 3>;
+using Cfg5 = TileCfg<96, 128, 32, 96, 16, 3>;
+using Cfg6 = TileCfg<48, 128, 32, 48, 16, 3>;
+using Cfg7 = TileCfg<112, 128, 16, 112, 16, 4>;
+
 }  // namespace
 
-// Tile configurations (BM, BN, BK, warp tile M, warp tile N, stages).
-using Cfg0 = TileCfg<128, 128, 16, 64, 32, 3>;
-using Cfg1 = TileCfg<64, 64, 16, 32, 32, 3>;
-using Cfg2 = TileCfg<64, 128, 16, 32, 32, 3>;
-using Cfg3 = TileCfg<32, 32, 16, 16, 16, 4>;
-
-int tile_cfg_bm(int cfg) { return cfg == 0 ? Cfg0::BM : cfg == 1 ? Cfg1::BM : cfg == 2 ? Cfg2::BM : Cfg3::BM; }
-int tile_cfg_bn(int cfg) { return cfg == 0 ? Cfg0::BN : cfg == 1 ? Cfg1::BN : cfg == 2 ? Cfg2::BN : Cfg3::BN; }
+int tile_cfg_count() { return 8; }
+int tile_cfg_bm(int cfg) {
+    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM};
+    return v[cfg];
+}
+int tile_cfg_bn(int cfg) {
+    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN};
+    return v[cfg];
+}
 
 cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     const DItem *items, int32_t nitems, int32_t *counter, const double *a,
@@ -281,7 +323,11 @@ cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     case 0: return launch_cfg<Cfg0>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     case 1: return launch_cfg<Cfg1>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     case 2: return launch_cfg<Cfg2>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    default: return launch_cfg<Cfg3>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 3: return launch_cfg<Cfg3>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 4: return launch_cfg<Cfg4>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 5: return launch_cfg<Cfg5>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 6: return launch_cfg<Cfg6>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    default: return launch_cfg<Cfg7>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     }
 }
 

@@ -22,6 +22,7 @@
 #include "ltg_host.hpp"
 
 namespace ltg {
+int tile_cfg_count();
 int tile_cfg_bm(int cfg);
 int tile_cfg_bn(int cfg);
 }
@@ -119,6 +120,8 @@ struct ContractExec {
 struct ltg_plan {
     ltg_ctx *ctx = nullptr;
     ltg_bt *a = nullptr, *b = nullptr;
+    int forced_tile = -1;         // >= 0: every C block uses this tile shape
+    std::map<std::pair<int64_t, int64_t>, int> tile_override;   // autotuned (M, N) -> shape
     ContractPlan plan;
     // cache of device task arrays keyed by (C tensor, ka, kb, kc, add, d)
     std::map<std::tuple<uint64_t, double, double, double, int, double>,
@@ -282,13 +285,40 @@ double two_m32(double scale) { return scale * 2.3283064365386963e-10; }   // sca
 
 // ------------------------------------------------------------ contraction exec
 
-// Tile configuration per C block: the bucket of its (M, N) extents picks one
-// of the compiled tile shapes (an autotuned table may override it).
+// 16-byte loads of (k, k+1) pairs need a contiguous, even-aligned k run:
+// innermost k stride 1 with even extent, every other k and row stride even
+// and an even base offset.
+int32_t vec16_ok(int64_t off, const SubDims &rows, const SubDims &k, bool second) {
+    if (k.n < 1 || off % 2 != 0) return 0;
+    const int64_t *ks = second ? k.s1 : k.s0;
+    if (ks[k.n - 1] != 1 || k.ext[k.n - 1] % 2 != 0) return 0;
+    for (int i = 0; i < k.n - 1; i++) if (ks[i] % 2 != 0) return 0;
+    for (int i = 0; i < rows.n; i++) if (rows.s0[i] % 2 != 0) return 0;
+    return 1;
+}
+
+// Tile configuration per C block: the (M, N) extents pick the compiled tile
+// shape with the least padded work, weighted by the relative efficiency of
+// the shape (larger tiles reuse more data per load).  An autotuned table
+// (ltg_autotune) overrides the weights with measured rates.
+struct TileShape { int bm, bn; double eff; };
+const TileShape kShapes[8] = {
+    {128, 128, 1.00}, {64, 64, 0.78}, {64, 128, 0.90}, {32, 32, 0.45},
+    {80, 128, 0.97}, {96, 128, 0.98}, {48, 128, 0.85}, {112, 128, 0.99},
+};
+double g_tile_eff[8] = {1.00, 0.78, 0.90, 0.45, 0.97, 0.98, 0.85, 0.99};
+
 int pick_tile(int64_t M, int64_t N) {
-    if (M >= 96 && N >= 96) return 0;
-    if (M >= 48 && N >= 96) return 2;
-    if (M >= 40 && N >= 40) return 1;
-    return 3;
+    int best = 0;
+    double bestc = 1e300;
+    for (int c = 0; c < 8; c++) {
+        const TileShape &s = kShapes[c];
+        double pm = (double)((M + s.bm - 1) / s.bm) * s.bm;
+        double pn = (double)((N + s.bn - 1) / s.bn) * s.bn;
+        double cost = pm * pn / g_tile_eff[c];
+        if (cost < bestc) { bestc = cost; best = c; }
+    }
+    return best;
 }
 
 void pack_sub(const SubDims &s, int32_t &n, int32_t *ext, int32_t *str0, int32_t *str1) {
@@ -334,6 +364,8 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
         pack_sub(t.k, x.nk, x.kext, x.ka_str, x.kb_str);
         pack_sub(t.m, x.nm, x.mext, x.ma_str, nullptr);
         pack_sub(t.n, x.nn, x.next, x.nb_str, nullptr);
+        x.vec_a = vec16_ok(t.a_off, t.m, t.k, false);
+        x.vec_b = vec16_ok(t.b_off, t.n, t.k, true);
     }
     std::vector<DCBlock> dc(cbt.size());
     double post = add ? d : 1.0;
@@ -352,9 +384,11 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     }
     // Work items per tile configuration, costliest first (LPT order for the
     // persistent work queue).
-    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(4);
+    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(8);
     for (size_t e = 0; e < cbt.size(); e++) {
-        int cfg = pick_tile(cbt[e].M, cbt[e].N);
+        int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(cbt[e].M, cbt[e].N);
+        auto ov = pl->tile_override.find({cbt[e].M, cbt[e].N});
+        if (pl->forced_tile < 0 && ov != pl->tile_override.end()) cfg = ov->second;
         int bm = tile_cfg_bm(cfg), bn = tile_cfg_bn(cfg);
         for (int64_t m0 = 0; m0 < cbt[e].M; m0 += bm)
             for (int64_t n0 = 0; n0 < cbt[e].N; n0 += bn) {
@@ -364,7 +398,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
             }
     }
     std::vector<DItem> items;
-    for (int cfg = 0; cfg < 4; cfg++) {
+    for (int cfg = 0; cfg < 8; cfg++) {
         auto &v = per_cfg[cfg];
         if (v.empty()) continue;
         std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
@@ -934,6 +968,85 @@ int ltg_plan_destroy(ltg_plan *plan) {
         if (!plan) throw error(kErrBadArg, "null plan");
         if (plan->ctx->device >= 0) cudaStreamSynchronize(plan->ctx->stream);
         delete plan;
+    });
+}
+
+int ltg_contract2_set_tile(ltg_plan *plan, int32_t cfg) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (cfg < -1 || cfg >= tile_cfg_count()) throw error(kErrBadArg, "tile configuration out of range");
+        plan->forced_tile = cfg;
+        plan->exec.clear();
+    });
+}
+
+int ltg_contract2_autotune(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, double ka,
+                           double kb, double kc, int32_t reps) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        check_bt(c);
+        need_dev(plan->ctx);
+        if (plan->ctx->capturing) throw error(kErrState, "autotuning cannot run during graph capture");
+        if (reps < 1) reps = 1;
+        // Distinct C-block shapes, costliest bucket first.
+        std::vector<GemmTask> tasks;
+        std::vector<CBlockTask> cbt;
+        contract2_tasks(plan->plan, plan->a->h, plan->b->h, c->h, ka, kb, kc, tasks, cbt);
+        std::map<std::pair<int64_t, int64_t>, double> work;
+        for (const CBlockTask &b : cbt) work[{b.M, b.N}] += (double)b.M * b.N * b.kflops;
+        std::vector<std::pair<double, std::pair<int64_t, int64_t>>> order;
+        for (auto &w : work) order.push_back({w.second, w.first});
+        std::sort(order.rbegin(), order.rend());
+        plan->forced_tile = -1;
+        cudaStream_t s = plan->ctx->stream;
+        cudaEvent_t e0, e1;
+        LTG_CUDA(cudaEventCreate(&e0));
+        LTG_CUDA(cudaEventCreate(&e1));
+        auto timed = [&]() {
+            plan->exec.clear();
+            int st = ltg_contract2(plan, c, mode, nslices, ka, kb, kc, 0, 0.0);   // warm + upload
+            if (st != kOk) throw error(st, g_last_error);
+            LTG_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < reps; r++) {
+                st = ltg_contract2(plan, c, mode, nslices, ka, kb, kc, 0, 0.0);
+                if (st != kOk) throw error(st, g_last_error);
+            }
+            LTG_CUDA(cudaEventRecord(e1, s));
+            LTG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            LTG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            return (double)ms;
+        };
+        for (auto &o : order) {
+            auto key = o.second;
+            double best = 1e300;
+            int bestc = pick_tile(key.first, key.second);
+            for (int cfg = 0; cfg < tile_cfg_count(); cfg++) {
+                plan->tile_override[key] = cfg;
+                double ms = timed();
+                if (ms < best) { best = ms; bestc = cfg; }
+            }
+            plan->tile_override[key] = bestc;
+        }
+        plan->exec.clear();
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    });
+}
+
+int ltg_plan_tiles(ltg_plan *plan, int64_t *m, int64_t *n, int32_t *cfg, int64_t cap, int64_t *count) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        int64_t k = 0;
+        for (auto &t : plan->tile_override) {
+            if (k < cap) {
+                if (m) m[k] = t.first.first;
+                if (n) n[k] = t.first.second;
+                if (cfg) cfg[k] = t.second;
+            }
+            k++;
+        }
+        if (count) *count = k;
     });
 }
 

@@ -23,6 +23,7 @@ struct DTask {
     int32_t kext[kDevMaxSub], ka_str[kDevMaxSub], kb_str[kDevMaxSub];
     int32_t mext[kDevMaxSub], ma_str[kDevMaxSub];
     int32_t next[kDevMaxSub], nb_str[kDevMaxSub];
+    int32_t vec_a, vec_b;         // 16-byte loads allowed (contiguous, even-aligned k pairs)
 };
 
 // One canonical C block of the schedule.
@@ -41,6 +42,30 @@ struct DItem {
     int32_t cblk;
     int32_t m0, n0;
     int32_t pad;
+};
+
+// ---------------------------------------------------------------- split precision
+
+// Slice element kinds of the split-precision contraction.
+enum OzKind { kOzInt8 = 0, kOzBf16 = 1, kOzE4m3 = 2 };
+
+// One split operand panel: the matricised view (rows x K) of a canonical
+// block, cut into S integer-valued slices stored row-major (K contiguous)
+// with rows padded to 128 and K padded to one 64-byte k block.
+struct DPanel {
+    int64_t src_off;              // FP64 source block offset (elements)
+    int64_t slice_off;            // byte offset of slice 0 in the slice arena
+    int32_t exp_off;              // first row exponent in the exponent arena
+    int32_t src;                  // 0: A arena, 1: B arena
+    int32_t rows, K, rows_pad, K_pad;
+    int32_t nr, nk;
+    int32_t rext[kDevMaxSub], rstr[kDevMaxSub];
+    int32_t kext[kDevMaxSub], kstr[kDevMaxSub];
+};
+
+struct DOzTask {
+    int32_t pa, pb;               // panels of A and B
+    double coeff;                 // relative coefficient of the pair
 };
 
 // ---------------------------------------------------------------- element-wise
@@ -130,6 +155,21 @@ __host__ __device__ inline double seeded_value(const DGenGroup &g, uint64_t seed
 cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     const DItem *items, int32_t nitems, int32_t *counter, const double *a,
     const double *b, double *c, int32_t add, int32_t tile_cfg, cudaStream_t s);
+
+// Split-precision contraction: FP64 -> slices, then the tcgen05 grouped
+// slice-product kernel with FP64 recombination.  tmaps points to one
+// 128-byte CUtensorMap per panel in device memory.
+cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int32_t max_rows_pad,
+    const double *a, const double *b, uint8_t *slices, int32_t *exps, int32_t S, cudaStream_t s);
+cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const void *tmaps, const DOzTask *tasks,
+    const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps, double *c,
+    int32_t add, int32_t S, int32_t chunk_kb, int32_t *err, cudaStream_t s);
+// Encodes the TMA descriptor of one panel (3D: K_pad, rows_pad, S).
+int oz_encode_tmap(void *tmap, int kind, void *slice_base, int32_t rows_pad, int32_t K_pad,
+                   int32_t S, int32_t box_rows);
+// Per kind: first-slice bits, further-slice bits, element bytes, k elements
+// per 64-byte k block, bound of one slice product.
+void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod);
 
 // Element-wise transfer kernels.
 cudaError_t launch_transfer(const DJob *jobs, const DTerm *terms, const DUnit *units,

@@ -61,6 +61,31 @@ def test_contract_add_matches_reference(gctx, case):
     assert max_rel_block_error(errs) <= TOL
 
 
+@pytest.mark.parametrize("cfg", range(8))
+@pytest.mark.parametrize("case", [CASES[0], CASES[1], CASES[5]], ids=["ladder", "ring", "K=1"])
+def test_every_tile_shape_matches_reference(gctx, case, cfg):
+    A, B, op, rop = _run(gctx, case)
+    op.set_tile(cfg)
+    C = op.make_result()
+    RC = rop.make_result()
+    op.perform(C)
+    rop.perform(RC)
+    errs = block_errors(C, C.download(), RC, None)
+    assert max_rel_block_error(errs) <= TOL
+
+
+def test_autotune_keeps_results(gctx):
+    case = CASES[0]
+    A, B, op, rop = _run(gctx, case)
+    C = op.make_result()
+    table = op.autotune(C, reps=1)
+    assert table and all(0 <= v < 8 for v in table.values())
+    RC = rop.make_result()
+    op.perform(C)
+    rop.perform(RC)
+    assert max_rel_block_error(block_errors(C, C.download(), RC, None)) <= TOL
+
+
 def test_contract_repeat_is_deterministic(gctx):
     case = CASES[0]
     A, B, op, rop = _run(gctx, case)
