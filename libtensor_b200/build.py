@@ -29,8 +29,9 @@ SOURCES = [
     "ltg_capi.cu",
     "contract_fp64.cu",
     "elementwise.cu",
+    "ozaki.cu",
 ]
-OPTIONAL_SOURCES = ["ozaki.cu"]
+OPTIONAL_SOURCES = []
 
 
 def _nvcc():
@@ -78,7 +79,7 @@ def build(verbose=False, force=False):
         for f in [ex.submit(_compile, s, o, verbose) for s, o in jobs]:
             f.result()
     if jobs or not os.path.exists(LIB):
-        cmd = [_nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart", "-lcuda"]
+        cmd = [_nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -117,8 +117,21 @@ struct ContractExec {
     std::vector<int64_t> sched_slots;
 };
 
+// Device arrays of the split-precision path for one (C tensor, coefficients,
+// mode, slice count).
+struct OzExec {
+    int kind = 0, S = 0, chunk_kb = 1, npanels = 0, max_rows_pad = 0, nitems = 0;
+    DevBuf panels, tmaps, slices, exps, tasks, cblks, items, err;
+    std::vector<std::pair<int64_t, int64_t>> zero_ranges;
+    std::vector<int64_t> sched_slots;
+    int32_t *err_host = nullptr;     // pinned copy of the device error word
+    ~OzExec() { if (err_host) cudaFreeHost(err_host); }
+};
+
 struct ltg_plan {
     ltg_ctx *ctx = nullptr;
+    std::map<std::tuple<uint64_t, double, double, double, int, double, int, int>,
+             std::unique_ptr<OzExec>> oz;
     ltg_bt *a = nullptr, *b = nullptr;
     int forced_tile = -1;         // >= 0: every C block uses this tile shape
     std::map<std::pair<int64_t, int64_t>, int> tile_override;   // autotuned (M, N) -> shape
@@ -427,6 +440,138 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     }
     ContractExec *raw = ex.get();
     pl->exec[key] = std::move(ex);
+    return raw;
+}
+
+// ------------------------------------------------------------ split precision
+
+OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, double kb, double kc,
+                      int add, double d) {
+    const int kind = mode == LTG_MODE_OZAKI_INT8 ? kOzInt8 : mode == LTG_MODE_OZAKI_BF16 ? kOzBf16 : kOzE4m3;
+    auto key = std::make_tuple(c->uid, ka, kb, kc, add, add ? d : 0.0, kind, S);
+    auto it = pl->oz.find(key);
+    if (it != pl->oz.end()) return it->second.get();
+    if (pl->ctx->capturing) throw error(kErrState, "contraction not prepared before graph capture: call it once outside the capture");
+    if (S < 1 || S > 8) throw error(kErrBadArg, "slice count must be 1..8");
+    int beta0, beta, esz, kbe;
+    int64_t maxprod;
+    oz_kind_params(kind, &beta0, &beta, &esz, &kbe, &maxprod);
+    std::unique_ptr<OzExec> ex(new OzExec());
+    ex->kind = kind;
+    ex->S = S;
+    // exact accumulation: S * maxprod * Kc below 2^31 (INT32) or 2^24 (FP32)
+    const int64_t lim = kind == kOzInt8 ? ((int64_t)1 << 31) - 1 : ((int64_t)1 << 24) - 1;
+    int64_t kc_elems = lim / ((int64_t)S * maxprod);
+    ex->chunk_kb = (int)std::max<int64_t>(1, std::min<int64_t>(kc_elems / kbe, 1 << 20));
+
+    std::vector<GemmTask> tasks;
+    std::vector<CBlockTask> cbt;
+    contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    // panels, de-duplicated by (operand, block, row mapping, k mapping)
+    std::map<std::vector<int64_t>, int32_t> pidx;
+    std::vector<DPanel> panels;
+    int64_t slice_bytes = 0;
+    int32_t exp_rows = 0;
+    auto panel_of = [&](int src, int64_t off, const SubDims &rows, const SubDims &k, bool kb_second) {
+        std::vector<int64_t> key = {src, off, rows.n, k.n};
+        for (int i = 0; i < rows.n; i++) { key.push_back(rows.ext[i]); key.push_back(rows.s0[i]); }
+        for (int i = 0; i < k.n; i++) { key.push_back(k.ext[i]); key.push_back(kb_second ? k.s1[i] : k.s0[i]); }
+        auto f = pidx.find(key);
+        if (f != pidx.end()) return f->second;
+        DPanel p;
+        std::memset(&p, 0, sizeof(p));
+        p.src = src;
+        p.src_off = off;
+        p.rows = (int32_t)rows.total();
+        p.K = (int32_t)k.total();
+        p.rows_pad = (p.rows + 127) / 128 * 128;
+        p.K_pad = (p.K + kbe - 1) / kbe * kbe;
+        pack_sub(rows, p.nr, p.rext, p.rstr, nullptr);
+        SubDims kk = k;
+        if (kb_second) for (int i = 0; i < kk.n; i++) kk.s0[i] = kk.s1[i];
+        pack_sub(kk, p.nk, p.kext, p.kstr, nullptr);
+        p.slice_off = slice_bytes;
+        slice_bytes += ((int64_t)S * p.rows_pad * p.K_pad * esz + 1023) / 1024 * 1024;
+        p.exp_off = exp_rows;
+        exp_rows += p.rows_pad;
+        int32_t id = (int32_t)panels.size();
+        panels.push_back(p);
+        pidx[key] = id;
+        return id;
+    };
+    std::vector<DOzTask> dt(tasks.size());
+    for (size_t i = 0; i < tasks.size(); i++) {
+        const GemmTask &t = tasks[i];
+        dt[i].pa = panel_of(0, t.a_off, t.m, t.k, false);
+        dt[i].pb = panel_of(1, t.b_off, t.n, t.k, true);
+        if (panels[dt[i].pa].K_pad != panels[dt[i].pb].K_pad) throw error(kErrState, "panel k extents differ");
+    }
+    std::vector<DCBlock> dc(cbt.size());
+    double post = add ? d : 1.0;
+    for (size_t e = 0; e < cbt.size(); e++) {
+        const CBlockTask &b = cbt[e];
+        DCBlock &x = dc[e];
+        std::memset(&x, 0, sizeof(x));
+        x.c_off = b.c_off;
+        double c0 = b.coeff0 != 0.0 ? b.coeff0 : 1.0;
+        x.scale = c0 * post;
+        x.M = (int32_t)b.M; x.N = (int32_t)b.N;
+        pack_sub(b.cm, x.nm, x.mext, x.mc_str, nullptr);
+        pack_sub(b.cn, x.nn, x.next, x.nc_str, nullptr);
+        x.t_begin = b.t_begin; x.t_end = b.t_end;
+        for (int32_t t = b.t_begin; t < b.t_end; t++) dt[t].coeff = tasks[t].coeff / c0;
+    }
+    // (C block, 128 x 64 tile) work items, costliest first, dealt round-robin
+    std::vector<std::pair<double, DItem>> iv;
+    for (size_t e = 0; e < cbt.size(); e++)
+        for (int64_t m0 = 0; m0 < cbt[e].M; m0 += 128)
+            for (int64_t n0 = 0; n0 < cbt[e].N; n0 += 64) {
+                DItem it; it.cblk = (int32_t)e; it.m0 = (int32_t)m0; it.n0 = (int32_t)n0; it.pad = 0;
+                iv.push_back({cbt[e].kflops + 64.0 * (cbt[e].t_end - cbt[e].t_begin), it});
+            }
+    std::stable_sort(iv.begin(), iv.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
+    std::vector<DItem> items;
+    for (auto &p : iv) items.push_back(p.second);
+    for (const DPanel &p : panels) ex->max_rows_pad = std::max(ex->max_rows_pad, p.rows_pad);
+
+    cudaStream_t s = pl->ctx->stream;
+    ex->npanels = (int)panels.size();
+    ex->nitems = (int)items.size();
+    ex->slices.alloc(std::max<int64_t>(slice_bytes, 1024));
+    ex->exps.alloc(std::max<int32_t>(exp_rows, 1) * sizeof(int32_t));
+    // TMA descriptors: A panels load 128-row boxes, B panels 64-row boxes
+    std::vector<uint8_t> maps((size_t)std::max(ex->npanels, 1) * 128, 0);
+    for (int i = 0; i < ex->npanels; i++) {
+        const DPanel &p = panels[i];
+        int r = oz_encode_tmap(maps.data() + (size_t)i * 128, kind, ex->slices.as<uint8_t>() + p.slice_off,
+                               p.rows_pad, p.K_pad, S, p.src == 0 ? 128 : 64);
+        if (r != 0) throw error(kErrCuda, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")");
+    }
+    upload_vec(ex->tmaps, maps, s);
+    upload_vec(ex->panels, panels, s);
+    upload_vec(ex->tasks, dt, s);
+    upload_vec(ex->cblks, dc, s);
+    upload_vec(ex->items, items, s);
+    ex->err.alloc(sizeof(int32_t));
+    LTG_CUDA(cudaMemsetAsync(ex->err.p, 0, sizeof(int32_t), s));
+    LTG_CUDA(cudaMallocHost(&ex->err_host, sizeof(int32_t)));
+    *ex->err_host = 0;
+    // blocks of C outside the schedule (zeroed in assign mode)
+    std::vector<char> in_sched(c->h.blk_abs.size(), 0);
+    for (int64_t cabs : pl->plan.schedule) {
+        int64_t sl = c->h.slot_of[cabs];
+        in_sched[sl] = 1;
+        ex->sched_slots.push_back(sl);
+    }
+    for (size_t sl = 0; sl < in_sched.size(); sl++) {
+        if (in_sched[sl]) continue;
+        int64_t b0 = c->h.blk_off[sl], b1 = b0 + c->h.blk_size[sl];
+        if (!ex->zero_ranges.empty() && ex->zero_ranges.back().second >= b0 - 3) ex->zero_ranges.back().second = b1;
+        else ex->zero_ranges.push_back({b0, b1});
+    }
+    LTG_CUDA(cudaStreamSynchronize(s));
+    OzExec *raw = ex.get();
+    pl->oz[key] = std::move(ex);
     return raw;
 }
 
@@ -940,10 +1085,35 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
         check_bt(c);
         need_dev(plan->ctx);
         if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
-        (void)nslices;
-        if (mode != LTG_MODE_PLAIN_FP64) throw error(kErrUnsupported, "split-precision modes are not built in this library");
         ltg_ctx *ctx = plan->ctx;
         cudaStream_t s = ctx->stream;
+        if (mode != LTG_MODE_PLAIN_FP64) {
+            if (mode < LTG_MODE_OZAKI_BF16 || mode > LTG_MODE_OZAKI_INT8) throw error(kErrBadArg, "unknown mode");
+            int S = nslices > 0 ? nslices : (mode == LTG_MODE_OZAKI_FP8 ? 8 : 7);
+            OzExec *ox = prepare_ozaki(plan, c, mode, S, ka, kb, kc, add, d);
+            if (*ox->err_host != 0) {
+                int code = *ox->err_host;
+                *ox->err_host = 0;
+                throw error(code == kErrTimeout ? kErrTimeout : kErrCuda,
+                            "a bounded device wait of the split-precision kernel gave up");
+            }
+            if (!add)
+                for (auto &r : ox->zero_ranges)
+                    LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
+            LTG_CUDA(launch_oz_split(ox->kind, ox->panels.as<DPanel>(), ox->npanels, ox->max_rows_pad,
+                                     plan->a->arena.as<double>(), plan->b->arena.as<double>(),
+                                     ox->slices.as<uint8_t>(), ox->exps.as<int32_t>(), ox->S, s));
+            LTG_CUDA(launch_oz_gemm(ox->kind, ox->panels.as<DPanel>(), ox->tmaps.p, ox->tasks.as<DOzTask>(),
+                                    ox->cblks.as<DCBlock>(), ox->items.as<DItem>(), ox->nitems,
+                                    ox->exps.as<int32_t>(), c->arena.as<double>(), add, ox->S, ox->chunk_kb,
+                                    ox->err.as<int32_t>(), s));
+            ctx->launches += 2;
+            if (!ctx->capturing)
+                LTG_CUDA(cudaMemcpyAsync(ox->err_host, ox->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
+            for (int64_t sl : ox->sched_slots) c->h.nonzero[sl] = 1;
+            return;
+        }
         ContractExec *ex = prepare_exec(plan, c, ka, kb, kc, add, d);
         if (!add)
             for (auto &r : ex->zero_ranges)

@@ -1,0 +1,541 @@
+// Split-precision ("Ozaki scheme") block-pair contraction on the B200 5th
+// generation tensor cores (tcgen05.mma, accumulators in tensor memory).
+//
+// Same schedule and task list as the plain FP64 path (one work item per
+// (C block, 128-row, 64-column) tile, all coalesced pairs of the C block
+// accumulated before the single FP64 write), but the products run on
+// integer-valued low-precision slices:
+//
+//  1. split (oz_split_kernel): every matricised operand row r of a block is
+//     scaled by its own power of two 2^-e_r (e_r: exponent of the row's
+//     largest magnitude) and cut into S slices of integers by round-to-nearest,
+//       x = 2^(e_r - b0) * sum_s sigma_s * 2^(-b*s),  |sigma_s| <= 2^(b0) or 2^(b-1),
+//     exactly, up to the dropped tail (Ozaki, Ogita, Oishi, Rump 2012; the
+//     per-row power-of-two scaling of Mukunoki et al. 2020).  The permutation
+//     of the block pair is applied here, so the slices are GEMM-ready.
+//  2. slice products (oz_gemm_kernel): the products sigma_sa x sigma_sb with
+//     sa + sb = l (a "level") share one scale, so each level accumulates in its
+//     own TMEM accumulator.  INT8 slices accumulate exactly in INT32; BF16 and
+//     FP8 E4M3 slices accumulate in FP32, exact while every partial sum stays
+//     below 2^24, which the host guarantees by draining every chunk_kb k blocks.
+//  3. recombination: after each pair (or chunk) the epilogue warps read the
+//     level accumulators from TMEM and add
+//       coeff * 2^(e_r + e_c - 2 b0) * sum_l 2^(-b l) * acc_l
+//     into FP64 registers; the C tile is written once, in FP64.
+// Only levels l <= S-1 are formed: S(S+1)/2 slice products per k step.
+//
+// Warp roles (192 threads): warps 0-3 epilogue (TMEM lanes 0-127, one C row
+// per thread), warp 4 TMA producer, warp 5 MMA issuer.  Operand tiles move
+// with cp.async.bulk.tensor (64-byte swizzled rows, no multicast); every
+// mbarrier wait is bounded and reports LTG_ERR_TIMEOUT through *err.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+#include "ltg_device.cuh"
+
+namespace ltg {
+
+void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod) {
+    switch (kind) {
+    case kOzInt8: *beta0 = 6; *beta = 7; *esz = 1; *kbe = 64; *maxprod = 64 * 64; break;
+    case kOzBf16: *beta0 = 6; *beta = 7; *esz = 2; *kbe = 32; *maxprod = 64 * 64; break;
+    default:      *beta0 = 4; *beta = 5; *esz = 1; *kbe = 64; *maxprod = 16 * 16; break;
+    }
+}
+
+namespace {
+
+constexpr int kBM = 128;              // C rows per tile (TMEM lanes)
+constexpr int kBN = 64;               // C columns per tile (TMEM columns per level)
+constexpr int kRowBytes = 64;         // k-block row length in shared memory
+constexpr int kATile = kBM * kRowBytes;   // 8 KB per A slice per stage
+constexpr int kBTile = kBN * kRowBytes;   // 4 KB per B slice per stage
+constexpr int kThreads = 192;
+constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s per barrier wait
+
+__device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_t *ext,
+                                                const int32_t *str) {
+    int64_t off = 0;
+    for (int i = n - 1; i >= 0; i--) {
+        int32_t e = ext[i];
+        int32_t q = lin / e;
+        off += (int64_t)(lin - q * e) * str[i];
+        lin = q;
+    }
+    return off;
+}
+
+// ---------------------------------------------------------------- split
+
+template<int KIND>
+__device__ __forceinline__ void store_slice(uint8_t *base, int64_t idx, double v) {
+    if (KIND == kOzInt8) {
+        reinterpret_cast<int8_t *>(base)[idx] = (int8_t)(int)v;
+    } else if (KIND == kOzBf16) {
+        reinterpret_cast<__nv_bfloat16 *>(base)[idx] = __float2bfloat16_rn((float)v);
+    } else {
+        __nv_fp8_e4m3 q((float)v);
+        reinterpret_cast<__nv_fp8_e4m3 *>(base)[idx] = q;
+    }
+}
+
+template<int KIND>
+__global__ void __launch_bounds__(256)
+oz_split_kernel(const DPanel *__restrict__ panels, int32_t npanels,
+                const double *__restrict__ A, const double *__restrict__ B,
+                uint8_t *__restrict__ slices, int32_t *__restrict__ exps, int32_t S,
+                int32_t beta0, int32_t beta, int32_t esz) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int p = blockIdx.y; p < npanels; p += gridDim.y) {
+        const DPanel &P = panels[p];
+        const double *src = P.src ? B : A;
+        uint8_t *base = slices + P.slice_off;
+        const int64_t sstride = (int64_t)P.rows_pad * P.K_pad;      // elements per slice
+        for (int r = blockIdx.x * 8 + warp; r < P.rows_pad; r += gridDim.x * 8) {
+            if (r >= P.rows) {
+                for (int s = 0; s < S; s++)
+                    for (int k = lane; k < P.K_pad; k += 32)
+                        store_slice<KIND>(base, s * sstride + (int64_t)r * P.K_pad + k, 0.0);
+                if (lane == 0) exps[P.exp_off + r] = 0;
+                continue;
+            }
+            const int64_t ro = P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
+            double mx = 0.0;
+            for (int k = lane; k < P.K; k += 32)
+                mx = fmax(mx, fabs(src[ro + mixed_offset(k, P.nk, P.kext, P.kstr)]));
+            for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            int e = 0;
+            if (mx > 0.0) frexp(mx, &e);            // mx = f * 2^e, f in [0.5, 1)
+            if (lane == 0) exps[P.exp_off + r] = e;
+            const double up = ldexp(1.0, beta);
+            for (int k = lane; k < P.K_pad; k += 32) {
+                double x = k < P.K ? src[ro + mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
+                double t = ldexp(x, beta0 - e);     // |t| < 2^beta0, exact
+                for (int s = 0; s < S; s++) {
+                    double sg = rint(t);
+                    store_slice<KIND>(base, s * sstride + (int64_t)r * P.K_pad + k, sg);
+                    t = (t - sg) * up;               // exact (Sterbenz) and a power-of-two scale
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- tcgen05 helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.shared::cta.b64 st, [%0]; }" :: "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }"
+                 :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for the phase with the given parity to complete, for at most
+// kWaitNs of wall time (try_wait itself may suspend the thread, so the bound
+// is on time, not on iterations); false on timeout or when another role
+// aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    const uint32_t a = smem_u32(bar);
+    uint64_t t0 = 0;
+    for (uint32_t i = 0;; i++) {
+        uint32_t done;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+        if ((i & 63) == 63) {
+            if (*abort) return false;
+            const uint64_t t = global_ns();
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > kWaitNs) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, uint64_t *bar,
+                                            int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];"
+        :: "r"(smem_u32(dst)), "l"(tmap), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+// K-major, 64-byte-swizzled shared-memory matrix descriptor: 8-row swizzle
+// atoms of 64-byte rows, atoms 512 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)1 << 16;                           // leading byte offset (unused, 16 B)
+    d |= (uint64_t)(512 >> 4) << 32;                  // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
+    d |= (uint64_t)4 << 61;                           // layout: 64-byte swizzle
+    return d;
+}
+
+template<int KIND>
+__device__ __forceinline__ uint32_t instr_desc() {
+    // D format: S32 for int8, F32 otherwise; A/B formats; K-major A and B;
+    // N = 64, M = 128.
+    uint32_t c_fmt = KIND == kOzInt8 ? 2u : 1u;
+    uint32_t ab_fmt = KIND == kOzInt8 ? 1u : (KIND == kOzBf16 ? 1u : 0u);
+    return (c_fmt << 4) | (ab_fmt << 7) | (ab_fmt << 10) | ((uint32_t)(kBN >> 3) << 17) |
+           ((uint32_t)(kBM >> 4) << 24);
+}
+
+template<int KIND>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                     uint32_t accumulate) {
+    if (KIND == kOzInt8) {
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0;\n"
+                     "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; }"
+                     :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+    } else if (KIND == kOzBf16) {
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0;\n"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p; }"
+                     :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+    } else {
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0;\n"
+                     "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p; }"
+                     :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+    }
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t *v) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                   "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr) : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// ---------------------------------------------------------------- slice products
+
+template<int KIND>
+__global__ void __launch_bounds__(kThreads, 1)
+oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tmaps,
+               const DOzTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
+               const DItem *__restrict__ items, int32_t nitems, const int32_t *__restrict__ exps,
+               double *__restrict__ Cp, int32_t add, int32_t S, int32_t stages, int32_t chunk_kb,
+               int32_t beta0, int32_t beta, int32_t kbe, int32_t *err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-byte aligned stage buffers: [stage][A slices | B slices]
+    uint8_t *smem = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int stage_bytes = S * (kATile + kBTile);
+    __shared__ __align__(8) uint64_t full_bar[8], empty_bar[8], accf_bar, acce_bar, drain_bar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < stages; i++) { mbar_init(&full_bar[i], 1); mbar_init(&empty_bar[i], 1); }
+        mbar_init(&accf_bar, 1);
+        mbar_init(&acce_bar, 4);
+        mbar_init(&drain_bar, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;"
+                     :: "r"(smem_u32(&tmem_base_s)) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_s;
+
+    if (warp == 4) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            int st = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            int armed_parity[8];
+            for (int i = 0; i < 8; i++) armed_parity[i] = -1;
+            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+                const DItem item = items[it];
+                const DCBlock &cb = cblks[item.cblk];
+                for (int ti = cb.t_begin; ti < cb.t_end && ok; ti++) {
+                    const DOzTask t = tasks[ti];
+                    const DPanel &pa = panels[t.pa];
+                    const void *ma = tmaps + (size_t)t.pa * 128;
+                    const void *mb = tmaps + (size_t)t.pb * 128;
+                    const int nkb = pa.K_pad / kbe;
+                    for (int kb = 0; kb < nkb; kb++) {
+                        if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s)) { ok = false; break; }
+                        uint8_t *sa = smem + st * stage_bytes;
+                        uint8_t *sb = sa + S * kATile;
+                        mbar_expect_tx(&full_bar[st], (uint32_t)stage_bytes);
+                        for (int s = 0; s < S; s++) {
+                            tma_load_3d(sa + s * kATile, ma, &full_bar[st], kb * kbe, item.m0, s);
+                            tma_load_3d(sb + s * kBTile, mb, &full_bar[st], kb * kbe, item.n0, s);
+                        }
+                        armed_parity[st] = (int)ph;
+                        if (++st == stages) { st = 0; ph ^= 1; }
+                    }
+                }
+            }
+            if (!ok) {
+                abort_s = 1;
+                atomicExch(err, 7);
+                // let the copies already in flight land before the CTA exits
+                volatile int never = 0;
+                for (int i = 0; i < stages; i++)
+                    if (armed_parity[i] >= 0) (void)mbar_wait(&full_bar[i], (uint32_t)armed_parity[i], &never);
+            }
+        }
+    } else if (warp == 5) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc<KIND>();
+            int st = 0;
+            uint32_t ph = 0, accph = 0;
+            int ndrain = 0;
+            bool ok = true;
+            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+                const DItem item = items[it];
+                const DCBlock &cb = cblks[item.cblk];
+                for (int ti = cb.t_begin; ti < cb.t_end && ok; ti++) {
+                    const DOzTask t = tasks[ti];
+                    const int nkb = panels[t.pa].K_pad / kbe;
+                    for (int kb0 = 0; kb0 < nkb && ok; kb0 += chunk_kb) {
+                        // the accumulators are free once the previous drain was read
+                        if (ndrain > 0) {
+                            if (!mbar_wait(&acce_bar, accph, &abort_s)) { ok = false; break; }
+                            accph ^= 1;
+                        }
+                        tc_fence_after();
+                        const int kb1 = min(nkb, kb0 + chunk_kb);
+                        for (int kb = kb0; kb < kb1; kb++) {
+                            if (!mbar_wait(&full_bar[st], ph, &abort_s)) { ok = false; break; }
+                            tc_fence_after();
+                            const uint32_t a0 = smem_u32(smem + st * stage_bytes);
+                            const uint32_t b0 = a0 + S * kATile;
+#pragma unroll 1
+                            for (int kk = 0; kk < kRowBytes / 32; kk++) {
+#pragma unroll 1
+                                for (int l = 0; l < S; l++) {
+#pragma unroll 1
+                                    for (int sa = 0; sa <= l; sa++) {
+                                        const int sb = l - sa;
+                                        const uint64_t ad = smem_desc_sw64(a0 + sa * kATile + kk * 32);
+                                        const uint64_t bd = smem_desc_sw64(b0 + sb * kBTile + kk * 32);
+                                        const uint32_t accum = (kb > kb0 || kk > 0 || sa > 0) ? 1u : 0u;
+                                        umma<KIND>(tmem + (uint32_t)(l * kBN), ad, bd, idesc, accum);
+                                    }
+                                }
+                            }
+                            umma_commit(&empty_bar[st]);       // frees the stage when these MMAs finish
+                            if (++st == stages) { st = 0; ph ^= 1; }
+                        }
+                        umma_commit(&accf_bar);                // accumulators ready for the epilogue
+                        ndrain++;
+                    }
+                }
+            }
+            if (!ok) {
+                abort_s = 1;
+                atomicExch(err, 7);
+                // the MMAs already issued must finish before TMEM is freed
+                volatile int never = 0;
+                umma_commit(&drain_bar);
+                (void)mbar_wait(&drain_bar, 0, &never);
+            }
+        }
+    } else {
+        // ------------------------------------------------ epilogue (warps 0-3)
+        const int row = warp * 32 + lane;                 // TMEM lane == tile row
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+        uint32_t accph = 0;
+        bool ok = true;
+        for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+            const DItem item = items[it];
+            const DCBlock &cb = cblks[item.cblk];
+            double acc[kBN];
+#pragma unroll
+            for (int j = 0; j < kBN; j++) acc[j] = 0.0;
+            const int m = item.m0 + row;
+            for (int ti = cb.t_begin; ti < cb.t_end && ok; ti++) {
+                const DOzTask t = tasks[ti];
+                const DPanel &pa = panels[t.pa];
+                const DPanel &pb = panels[t.pb];
+                const int nkb = pa.K_pad / kbe;
+                const double f = ldexp(t.coeff, exps[pa.exp_off + m] - 2 * beta0);
+                const int32_t *eb = exps + pb.exp_off + item.n0;
+                for (int kb0 = 0; kb0 < nkb; kb0 += chunk_kb) {
+                    // warp-uniform outcome: tcgen05.ld below is .sync.aligned
+                    ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar, accph, &abort_s));
+                    if (!ok) break;
+                    accph ^= 1;
+                    tc_fence_after();
+#pragma unroll
+                    for (int c = 0; c < kBN / 8; c++) {
+                        double sum[8];
+#pragma unroll
+                        for (int j = 0; j < 8; j++) sum[j] = 0.0;
+                        double w = 1.0;
+                        for (int l = 0; l < S; l++) {
+                            uint32_t v[8];
+                            tmem_ld8(lane_base + (uint32_t)(l * kBN + c * 8), v);
+                            tmem_wait_ld();
+#pragma unroll
+                            for (int j = 0; j < 8; j++) {
+                                double x = KIND == kOzInt8 ? (double)(int32_t)v[j] : (double)__uint_as_float(v[j]);
+                                sum[j] += w * x;
+                            }
+                            w = ldexp(w, -beta);
+                        }
+#pragma unroll
+                        for (int j = 0; j < 8; j++) acc[c * 8 + j] += ldexp(f, eb[c * 8 + j]) * sum[j];
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acce_bar);
+                }
+            }
+            if (!ok) break;
+            // FP64 write of the finished tile row
+            if (m < cb.M) {
+                const int64_t orow = cb.c_off + mixed_offset(m, cb.nm, cb.mext, cb.mc_str);
+#pragma unroll
+                for (int j = 0; j < kBN; j++) {
+                    const int n = item.n0 + j;
+                    if (n < cb.N) {
+                        double *dst = Cp + orow + mixed_offset(n, cb.nn, cb.next, cb.nc_str);
+                        const double v = cb.scale * acc[j];
+                        if (add) *dst += v;
+                        else *dst = v;
+                    }
+                }
+            }
+        }
+        if (!ok) { abort_s = 1; atomicExch(err, 7); }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" :: "r"(tmem) : "memory");
+    }
+}
+
+int g_nsm = 0;
+
+}  // namespace
+
+cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int32_t max_rows_pad,
+                            const double *a, const double *b, uint8_t *slices, int32_t *exps,
+                            int32_t S, cudaStream_t s) {
+    if (npanels <= 0) return cudaSuccess;
+    int beta0, beta, esz, kbe;
+    int64_t mp;
+    oz_kind_params(kind, &beta0, &beta, &esz, &kbe, &mp);
+    dim3 grid((max_rows_pad + 7) / 8, npanels < 65535 ? npanels : 65535);
+    if (kind == kOzInt8)
+        oz_split_kernel<kOzInt8><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta, esz);
+    else if (kind == kOzBf16)
+        oz_split_kernel<kOzBf16><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta, esz);
+    else
+        oz_split_kernel<kOzE4m3><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta, esz);
+    return cudaGetLastError();
+}
+
+template<int KIND>
+static cudaError_t launch_gemm_t(const DPanel *panels, const void *tmaps, const DOzTask *tasks,
+                                 const DCBlock *cblks, const DItem *items, int32_t nitems,
+                                 const int32_t *exps, double *c, int32_t add, int32_t S,
+                                 int32_t chunk_kb, int32_t *err, cudaStream_t s) {
+    int beta0, beta, esz, kbe;
+    int64_t mp;
+    oz_kind_params(KIND, &beta0, &beta, &esz, &kbe, &mp);
+    const int stage_bytes = S * (kATile + kBTile);
+    int stages = (200 * 1024) / stage_bytes;
+    if (stages > 4) stages = 4;
+    if (stages < 2) return cudaErrorInvalidValue;
+    // At least 120 KB so that a second CTA never shares the SM: each CTA
+    // holds all 512 TMEM columns.
+    size_t smem = (size_t)stages * stage_bytes + 1024;
+    if (smem < 120 * 1024) smem = 120 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (g_nsm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
+    }
+    int grid = nitems < g_nsm ? nitems : g_nsm;
+    if (grid < 1) return cudaSuccess;
+    oz_gemm_kernel<KIND><<<grid, kThreads, smem, s>>>(panels, static_cast<const uint8_t *>(tmaps), tasks, cblks,
+                                                     items, nitems, exps, c, add, S, stages, chunk_kb, beta0,
+                                                     beta, kbe, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const void *tmaps, const DOzTask *tasks,
+                           const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps,
+                           double *c, int32_t add, int32_t S, int32_t chunk_kb, int32_t *err,
+                           cudaStream_t s) {
+    if (S < 1 || S > 8) return cudaErrorInvalidValue;
+    if (kind == kOzInt8)
+        return launch_gemm_t<kOzInt8>(panels, tmaps, tasks, cblks, items, nitems, exps, c, add, S, chunk_kb, err, s);
+    if (kind == kOzBf16)
+        return launch_gemm_t<kOzBf16>(panels, tmaps, tasks, cblks, items, nitems, exps, c, add, S, chunk_kb, err, s);
+    return launch_gemm_t<kOzE4m3>(panels, tmaps, tasks, cblks, items, nitems, exps, c, add, S, chunk_kb, err, s);
+}
+
+int oz_encode_tmap(void *tmap, int kind, void *slice_base, int32_t rows_pad, int32_t K_pad, int32_t S,
+                   int32_t box_rows) {
+    int beta0, beta, esz, kbe;
+    int64_t mp;
+    oz_kind_params(kind, &beta0, &beta, &esz, &kbe, &mp);
+    CUtensorMapDataType dt = kind == kOzBf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    cuuint64_t dims[3] = {(cuuint64_t)K_pad, (cuuint64_t)rows_pad, (cuuint64_t)S};
+    cuuint64_t strides[2] = {(cuuint64_t)K_pad * esz, (cuuint64_t)rows_pad * K_pad * esz};
+    cuuint32_t box[3] = {(cuuint32_t)kbe, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    // The driver entry point is looked up at run time so that the library
+    // also loads on hosts without a GPU driver.
+    typedef CUresult (*encode_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static encode_fn encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return -1;
+        encode = reinterpret_cast<encode_fn>(fn);
+    }
+    CUresult r = encode(reinterpret_cast<CUtensorMap *>(tmap), dt, 3, slice_base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : (int)r;
+}
+
+}  // namespace ltg

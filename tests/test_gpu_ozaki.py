@@ -1,0 +1,73 @@
+"""GPU checks of the split-precision (Ozaki) contraction on tcgen05 tensor
+cores: same non-zero C blocks as the reference and every C block within the
+stated relative error (block max-norm) of the reference's FP64 result."""
+import numpy as np
+import pytest
+
+from libtensor_b200.core import (Context, MODE_OZAKI_BF16, MODE_OZAKI_FP8, MODE_OZAKI_INT8,
+                                 btod_contract2, contraction2)
+from oracle import refapi as R
+from tests.cases import cases
+from tests.helpers import block_errors, max_rel_block_error, seeded_pair
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")]
+
+CASES = [c for c in cases() if not c.symmetry_error]
+
+# (mode, slices, bound on the block-relative error).  INT8 slices carry 7
+# bits (6 for the first), BF16 slices are given the same 7 bits (exact
+# partial sums in FP32), FP8 E4M3 slices 5 bits (4 for the first); the bounds
+# are a few units of the dropped tail 2^-(b0 + b(S-1)) times sqrt(K).
+MODES = [
+    (MODE_OZAKI_INT8, 7, 1e-12),
+    (MODE_OZAKI_INT8, 6, 1e-10),
+    (MODE_OZAKI_INT8, 3, 1e-4),
+    (MODE_OZAKI_BF16, 7, 1e-12),
+    (MODE_OZAKI_FP8, 8, 1e-9),
+]
+
+
+@pytest.fixture(scope="module")
+def gctx():
+    c = Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("mode,S,tol", MODES, ids=[f"mode{m}-S{s}" for m, s, _ in MODES])
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_split_precision_matches_reference(gctx, case, mode, S, tol):
+    A, ra, _ = seeded_pair(gctx, case.a, 11, case.a_scale, case.zero_a)
+    B, rb, _ = seeded_pair(gctx, case.b, 23, case.b_scale)
+    contr = contraction2(case.n, case.m, case.k, case.permc)
+    for p in case.pairs:
+        contr.contract(*p)
+    op = btod_contract2(contr, A, B, case.ka, case.kb, case.kc)
+    rop = R.RefContract2(case.n, case.m, case.k, case.permc, case.pairs, ra, rb, case.ka, case.kb, case.kc)
+    C = op.make_result()
+    RC = rop.make_result()
+    op.perform(C, mode=mode, nslices=S)
+    gctx.synchronize()
+    rop.perform(RC)
+    assert C.nonzero() == RC.nonzero()
+    errs = block_errors(C, C.download(), RC, None)
+    err = max_rel_block_error(errs)
+    print(f"{case.name} mode={mode} S={S}: max block rel err {err:.3e}")
+    assert err <= tol, sorted(errs, key=lambda e: -e[1])[:3]
+
+
+def test_split_precision_add_mode(gctx):
+    case = CASES[0]
+    A, ra, _ = seeded_pair(gctx, case.a, 3, case.a_scale)
+    B, rb, _ = seeded_pair(gctx, case.b, 4, case.b_scale)
+    contr = contraction2(case.n, case.m, case.k, case.permc)
+    for p in case.pairs:
+        contr.contract(*p)
+    op = btod_contract2(contr, A, B, case.ka, case.kb, case.kc)
+    rop = R.RefContract2(case.n, case.m, case.k, case.permc, case.pairs, ra, rb, case.ka, case.kb, case.kc)
+    C, RC = op.make_result(), rop.make_result()
+    op.perform(C)
+    rop.perform(RC)
+    op.perform(C, 0.5, mode=MODE_OZAKI_INT8, nslices=7)
+    rop.perform(RC, 0.5)
+    assert max_rel_block_error(block_errors(C, C.download(), RC, None)) <= 1e-12
