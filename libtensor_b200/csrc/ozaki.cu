@@ -26,8 +26,9 @@
 //
 // Warp roles (192 threads): warps 0-3 epilogue (TMEM lanes 0-127, one C row
 // per thread), warp 4 TMA producer, warp 5 MMA issuer.  Operand tiles move
-// with cp.async.bulk.tensor (64-byte swizzled rows, no multicast); every
-// mbarrier wait is bounded and reports LTG_ERR_TIMEOUT through *err.
+// with cp.async.bulk.tensor in 32-byte swizzled k blocks (one MMA k step per
+// pipeline stage, so even 8 slices leave room for 4 stages); no multicast.
+// Every mbarrier wait is bounded in time and reports through *err.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -36,11 +37,12 @@
 
 namespace ltg {
 
+// k elements per 32-byte k block: 32 for 8-bit slices, 16 for BF16.
 void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod) {
     switch (kind) {
-    case kOzInt8: *beta0 = 6; *beta = 7; *esz = 1; *kbe = 64; *maxprod = 64 * 64; break;
-    case kOzBf16: *beta0 = 6; *beta = 7; *esz = 2; *kbe = 32; *maxprod = 64 * 64; break;
-    default:      *beta0 = 4; *beta = 5; *esz = 1; *kbe = 64; *maxprod = 16 * 16; break;
+    case kOzInt8: *beta0 = 6; *beta = 7; *esz = 1; *kbe = 32; *maxprod = 64 * 64; break;
+    case kOzBf16: *beta0 = 6; *beta = 7; *esz = 2; *kbe = 16; *maxprod = 64 * 64; break;
+    default:      *beta0 = 4; *beta = 5; *esz = 1; *kbe = 32; *maxprod = 16 * 16; break;
     }
 }
 
@@ -48,10 +50,11 @@ namespace {
 
 constexpr int kBM = 128;              // C rows per tile (TMEM lanes)
 constexpr int kBN = 64;               // C columns per tile (TMEM columns per level)
-constexpr int kRowBytes = 64;         // k-block row length in shared memory
-constexpr int kATile = kBM * kRowBytes;   // 8 KB per A slice per stage
-constexpr int kBTile = kBN * kRowBytes;   // 4 KB per B slice per stage
+constexpr int kRowBytes = 32;         // k-block row length in shared memory (one MMA k step)
+constexpr int kATile = kBM * kRowBytes;   // 4 KB per A slice per stage
+constexpr int kBTile = kBN * kRowBytes;   // 2 KB per B slice per stage
 constexpr int kThreads = 192;
+constexpr int kMaxStages = 8;
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s per barrier wait
 
 __device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_t *ext,
@@ -68,54 +71,94 @@ __device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_
 
 // ---------------------------------------------------------------- split
 
-template<int KIND>
-__device__ __forceinline__ void store_slice(uint8_t *base, int64_t idx, double v) {
-    if (KIND == kOzInt8) {
-        reinterpret_cast<int8_t *>(base)[idx] = (int8_t)(int)v;
-    } else if (KIND == kOzBf16) {
-        reinterpret_cast<__nv_bfloat16 *>(base)[idx] = __float2bfloat16_rn((float)v);
-    } else {
-        __nv_fp8_e4m3 q((float)v);
-        reinterpret_cast<__nv_fp8_e4m3 *>(base)[idx] = q;
+// Four consecutive slice values packed for one store.
+template<int KIND> struct Pack4;
+template<> struct Pack4<kOzInt8> {
+    typedef uint32_t T;
+    __device__ static T pack(const double *v) {
+        return (uint32_t)(uint8_t)(int8_t)(int)v[0] | ((uint32_t)(uint8_t)(int8_t)(int)v[1] << 8) |
+               ((uint32_t)(uint8_t)(int8_t)(int)v[2] << 16) | ((uint32_t)(uint8_t)(int8_t)(int)v[3] << 24);
     }
-}
+};
+template<> struct Pack4<kOzE4m3> {
+    typedef uint32_t T;
+    __device__ static T pack(const double *v) {
+        uint32_t r = 0;
+        for (int i = 0; i < 4; i++) {
+            __nv_fp8_e4m3 q((float)v[i]);
+            r |= (uint32_t)q.__x << (8 * i);
+        }
+        return r;
+    }
+};
+template<> struct Pack4<kOzBf16> {
+    typedef uint2 T;
+    __device__ static T pack(const double *v) {
+        __nv_bfloat16 b[4];
+        for (int i = 0; i < 4; i++) b[i] = __float2bfloat16_rn((float)v[i]);
+        uint2 r;
+        r.x = (uint32_t)__bfloat16_as_ushort(b[0]) | ((uint32_t)__bfloat16_as_ushort(b[1]) << 16);
+        r.y = (uint32_t)__bfloat16_as_ushort(b[2]) | ((uint32_t)__bfloat16_as_ushort(b[3]) << 16);
+        return r;
+    }
+};
 
+// One warp per panel row, four consecutive k per lane; two passes over the
+// row (largest magnitude, then the slices).  Contiguous rows (one k
+// sub-dimension of stride 1) skip the mixed-radix index arithmetic.
 template<int KIND>
 __global__ void __launch_bounds__(256)
 oz_split_kernel(const DPanel *__restrict__ panels, int32_t npanels,
                 const double *__restrict__ A, const double *__restrict__ B,
                 uint8_t *__restrict__ slices, int32_t *__restrict__ exps, int32_t S,
-                int32_t beta0, int32_t beta, int32_t esz) {
+                int32_t beta0, int32_t beta) {
+    typedef typename Pack4<KIND>::T PT;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int p = blockIdx.y; p < npanels; p += gridDim.y) {
         const DPanel &P = panels[p];
         const double *src = P.src ? B : A;
-        uint8_t *base = slices + P.slice_off;
-        const int64_t sstride = (int64_t)P.rows_pad * P.K_pad;      // elements per slice
+        PT *base = reinterpret_cast<PT *>(slices + P.slice_off);
+        const int64_t sstride = (int64_t)P.rows_pad * P.K_pad / 4;     // packs per slice
+        const int64_t rstride = P.K_pad / 4;                            // packs per row
+        const bool contig = P.nk == 1 && P.kstr[0] == 1;
         for (int r = blockIdx.x * 8 + warp; r < P.rows_pad; r += gridDim.x * 8) {
             if (r >= P.rows) {
+                PT z;
+                memset(&z, 0, sizeof(z));
                 for (int s = 0; s < S; s++)
-                    for (int k = lane; k < P.K_pad; k += 32)
-                        store_slice<KIND>(base, s * sstride + (int64_t)r * P.K_pad + k, 0.0);
+                    for (int k4 = lane; k4 < rstride; k4 += 32) base[s * sstride + r * rstride + k4] = z;
                 if (lane == 0) exps[P.exp_off + r] = 0;
                 continue;
             }
-            const int64_t ro = P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
+            const double *row = src + P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
             double mx = 0.0;
-            for (int k = lane; k < P.K; k += 32)
-                mx = fmax(mx, fabs(src[ro + mixed_offset(k, P.nk, P.kext, P.kstr)]));
+            for (int k4 = lane; k4 < rstride; k4 += 32) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int k = 4 * k4 + j;
+                    if (k < P.K) mx = fmax(mx, fabs(row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)]));
+                }
+            }
             for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
             int e = 0;
             if (mx > 0.0) frexp(mx, &e);            // mx = f * 2^e, f in [0.5, 1)
             if (lane == 0) exps[P.exp_off + r] = e;
             const double up = ldexp(1.0, beta);
-            for (int k = lane; k < P.K_pad; k += 32) {
-                double x = k < P.K ? src[ro + mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
-                double t = ldexp(x, beta0 - e);     // |t| < 2^beta0, exact
+            for (int k4 = lane; k4 < rstride; k4 += 32) {
+                double t[4], sg[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int k = 4 * k4 + j;
+                    const double x = k < P.K ? row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
+                    t[j] = ldexp(x, beta0 - e);     // |t| < 2^beta0, exact
+                }
                 for (int s = 0; s < S; s++) {
-                    double sg = rint(t);
-                    store_slice<KIND>(base, s * sstride + (int64_t)r * P.K_pad + k, sg);
-                    t = (t - sg) * up;               // exact (Sterbenz) and a power-of-two scale
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        sg[j] = rint(t[j]);
+                        t[j] = (t[j] - sg[j]) * up;   // exact (Sterbenz), power-of-two scale
+                    }
+                    base[s * sstride + r * rstride + k4] = Pack4<KIND>::pack(sg);
                 }
             }
         }
@@ -168,24 +211,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     }
 }
 
-__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, uint64_t *bar,
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *tmap, uint32_t bar,
                                             int c0, int c1, int c2) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%3, %4, %5}], [%2];"
-        :: "r"(smem_u32(dst)), "l"(tmap), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        :: "r"(dst), "l"(tmap), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
         : "memory");
 }
 
-// K-major, 64-byte-swizzled shared-memory matrix descriptor: 8-row swizzle
-// atoms of 64-byte rows, atoms 512 bytes apart.
-__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
+// K-major, 32-byte-swizzled shared-memory matrix descriptor: 8-row swizzle
+// atoms of 32-byte rows, atoms 256 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc_sw32(uint32_t addr) {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
     d |= (uint64_t)1 << 16;                           // leading byte offset (unused, 16 B)
-    d |= (uint64_t)(512 >> 4) << 32;                  // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)(256 >> 4) << 32;                  // stride byte offset: 8 rows x 32 B
     d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
-    d |= (uint64_t)4 << 61;                           // layout: 64-byte swizzle
+    d |= (uint64_t)6 << 61;                           // layout: 32-byte swizzle
     return d;
 }
 
@@ -234,18 +277,18 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 
 // ---------------------------------------------------------------- slice products
 
-template<int KIND>
+template<int KIND, int S>
 __global__ void __launch_bounds__(kThreads, 1)
 oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tmaps,
                const DOzTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
                const DItem *__restrict__ items, int32_t nitems, const int32_t *__restrict__ exps,
-               double *__restrict__ Cp, int32_t add, int32_t S, int32_t stages, int32_t chunk_kb,
+               double *__restrict__ Cp, int32_t add, int32_t stages, int32_t chunk_kb,
                int32_t beta0, int32_t beta, int32_t kbe, int32_t *err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte aligned stage buffers: [stage][A slices | B slices]
     uint8_t *smem = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const int stage_bytes = S * (kATile + kBTile);
-    __shared__ __align__(8) uint64_t full_bar[8], empty_bar[8], accf_bar, acce_bar, drain_bar;
+    constexpr int kStageBytes = S * (kATile + kBTile);
+    __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar, acce_bar, drain_bar;
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
 
@@ -267,6 +310,7 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base_s;
+    const uint32_t smem0 = smem_u32(smem);
 
     if (warp == 4) {
         // ------------------------------------------------ TMA producer
@@ -274,25 +318,26 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
             int st = 0;
             uint32_t ph = 0;
             bool ok = true;
-            int armed_parity[8];
-            for (int i = 0; i < 8; i++) armed_parity[i] = -1;
+            int armed_parity[kMaxStages];
+            for (int i = 0; i < kMaxStages; i++) armed_parity[i] = -1;
             for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
                 const DItem item = items[it];
                 const DCBlock &cb = cblks[item.cblk];
                 for (int ti = cb.t_begin; ti < cb.t_end && ok; ti++) {
                     const DOzTask t = tasks[ti];
-                    const DPanel &pa = panels[t.pa];
                     const void *ma = tmaps + (size_t)t.pa * 128;
                     const void *mb = tmaps + (size_t)t.pb * 128;
-                    const int nkb = pa.K_pad / kbe;
+                    const int nkb = panels[t.pa].K_pad / kbe;
                     for (int kb = 0; kb < nkb; kb++) {
                         if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s)) { ok = false; break; }
-                        uint8_t *sa = smem + st * stage_bytes;
-                        uint8_t *sb = sa + S * kATile;
-                        mbar_expect_tx(&full_bar[st], (uint32_t)stage_bytes);
+                        const uint32_t sa = smem0 + st * kStageBytes;
+                        const uint32_t sb = sa + S * kATile;
+                        const uint32_t fb = smem_u32(&full_bar[st]);
+                        mbar_expect_tx(&full_bar[st], (uint32_t)kStageBytes);
+#pragma unroll
                         for (int s = 0; s < S; s++) {
-                            tma_load_3d(sa + s * kATile, ma, &full_bar[st], kb * kbe, item.m0, s);
-                            tma_load_3d(sb + s * kBTile, mb, &full_bar[st], kb * kbe, item.n0, s);
+                            tma_load_3d(sa + s * kATile, ma, fb, kb * kbe, item.m0, s);
+                            tma_load_3d(sb + s * kBTile, mb, fb, kb * kbe, item.n0, s);
                         }
                         armed_parity[st] = (int)ph;
                         if (++st == stages) { st = 0; ph ^= 1; }
@@ -320,8 +365,7 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
                 const DItem item = items[it];
                 const DCBlock &cb = cblks[item.cblk];
                 for (int ti = cb.t_begin; ti < cb.t_end && ok; ti++) {
-                    const DOzTask t = tasks[ti];
-                    const int nkb = panels[t.pa].K_pad / kbe;
+                    const int nkb = panels[tasks[ti].pa].K_pad / kbe;
                     for (int kb0 = 0; kb0 < nkb && ok; kb0 += chunk_kb) {
                         // the accumulators are free once the previous drain was read
                         if (ndrain > 0) {
@@ -333,20 +377,20 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
                         for (int kb = kb0; kb < kb1; kb++) {
                             if (!mbar_wait(&full_bar[st], ph, &abort_s)) { ok = false; break; }
                             tc_fence_after();
-                            const uint32_t a0 = smem_u32(smem + st * stage_bytes);
+                            const uint32_t a0 = smem0 + st * kStageBytes;
                             const uint32_t b0 = a0 + S * kATile;
-#pragma unroll 1
-                            for (int kk = 0; kk < kRowBytes / 32; kk++) {
-#pragma unroll 1
-                                for (int l = 0; l < S; l++) {
-#pragma unroll 1
-                                    for (int sa = 0; sa <= l; sa++) {
-                                        const int sb = l - sa;
-                                        const uint64_t ad = smem_desc_sw64(a0 + sa * kATile + kk * 32);
-                                        const uint64_t bd = smem_desc_sw64(b0 + sb * kBTile + kk * 32);
-                                        const uint32_t accum = (kb > kb0 || kk > 0 || sa > 0) ? 1u : 0u;
-                                        umma<KIND>(tmem + (uint32_t)(l * kBN), ad, bd, idesc, accum);
-                                    }
+                            const uint64_t da = smem_desc_sw32(a0), db = smem_desc_sw32(b0);
+                            const uint32_t first = kb == kb0 ? 0u : 1u;
+#pragma unroll
+                            for (int l = 0; l < S; l++) {
+#pragma unroll
+                                for (int sa = 0; sa <= l; sa++) {
+                                    const int sb = l - sa;
+                                    // descriptor start addresses advance in 16-byte units
+                                    umma<KIND>(tmem + (uint32_t)(l * kBN),
+                                               da + (uint64_t)((sa * kATile) >> 4),
+                                               db + (uint64_t)((sb * kBTile) >> 4), idesc,
+                                               sa == 0 ? first : 1u);
                                 }
                             }
                             umma_commit(&empty_bar[st]);       // frees the stage when these MMAs finish
@@ -372,6 +416,10 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
         const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
         uint32_t accph = 0;
         bool ok = true;
+        double lw[S];                                     // 2^(-beta * l)
+        lw[0] = 1.0;
+#pragma unroll
+        for (int l = 1; l < S; l++) lw[l] = ldexp(lw[l - 1], -beta);
         for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
             const DItem item = items[it];
             const DCBlock &cb = cblks[item.cblk];
@@ -394,23 +442,21 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
                     tc_fence_after();
 #pragma unroll
                     for (int c = 0; c < kBN / 8; c++) {
-                        double sum[8];
+                        uint32_t v[S][8];
 #pragma unroll
-                        for (int j = 0; j < 8; j++) sum[j] = 0.0;
-                        double w = 1.0;
-                        for (int l = 0; l < S; l++) {
-                            uint32_t v[8];
-                            tmem_ld8(lane_base + (uint32_t)(l * kBN + c * 8), v);
-                            tmem_wait_ld();
+                        for (int l = 0; l < S; l++) tmem_ld8(lane_base + (uint32_t)(l * kBN + c * 8), v[l]);
+                        tmem_wait_ld();
 #pragma unroll
-                            for (int j = 0; j < 8; j++) {
-                                double x = KIND == kOzInt8 ? (double)(int32_t)v[j] : (double)__uint_as_float(v[j]);
-                                sum[j] += w * x;
+                        for (int j = 0; j < 8; j++) {
+                            double sum = 0.0;
+#pragma unroll
+                            for (int l = S - 1; l >= 0; l--) {
+                                const double x = KIND == kOzInt8 ? (double)(int32_t)v[l][j]
+                                                                 : (double)__uint_as_float(v[l][j]);
+                                sum += lw[l] * x;
                             }
-                            w = ldexp(w, -beta);
+                            acc[c * 8 + j] += ldexp(f, eb[c * 8 + j]) * sum;
                         }
-#pragma unroll
-                        for (int j = 0; j < 8; j++) acc[c * 8 + j] += ldexp(f, eb[c * 8 + j]) * sum[j];
                     }
                     tc_fence_before();
                     __syncwarp();
@@ -446,6 +492,49 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
 
 int g_nsm = 0;
 
+template<int KIND, int S>
+cudaError_t launch_gemm_s(const DPanel *panels, const void *tmaps, const DOzTask *tasks, const DCBlock *cblks,
+                          const DItem *items, int32_t nitems, const int32_t *exps, double *c, int32_t add,
+                          int32_t chunk_kb, int32_t *err, cudaStream_t s) {
+    int beta0, beta, esz, kbe;
+    int64_t mp;
+    oz_kind_params(KIND, &beta0, &beta, &esz, &kbe, &mp);
+    constexpr int stage_bytes = S * (kATile + kBTile);
+    int stages = (200 * 1024) / stage_bytes;
+    if (stages > kMaxStages) stages = kMaxStages;
+    if (stages < 2) return cudaErrorInvalidValue;
+    // At least 120 KB so that a second CTA never shares the SM: each CTA
+    // holds all 512 TMEM columns.
+    size_t smem = (size_t)stages * stage_bytes + 1024;
+    if (smem < 120 * 1024) smem = 120 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<KIND, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    if (g_nsm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
+    }
+    int grid = nitems < g_nsm ? nitems : g_nsm;
+    if (grid < 1) return cudaSuccess;
+    oz_gemm_kernel<KIND, S><<<grid, kThreads, smem, s>>>(panels, static_cast<const uint8_t *>(tmaps), tasks, cblks,
+                                                        items, nitems, exps, c, add, stages, chunk_kb, beta0, beta,
+                                                        kbe, err);
+    return cudaGetLastError();
+}
+
+template<int KIND>
+cudaError_t launch_gemm_k(int S, const DPanel *panels, const void *tmaps, const DOzTask *tasks,
+                          const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps, double *c,
+                          int32_t add, int32_t chunk_kb, int32_t *err, cudaStream_t s) {
+    switch (S) {
+#define CASE_S(n) case n: return launch_gemm_s<KIND, n>(panels, tmaps, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
+    CASE_S(1) CASE_S(2) CASE_S(3) CASE_S(4) CASE_S(5) CASE_S(6) CASE_S(7) CASE_S(8)
+#undef CASE_S
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int32_t max_rows_pad,
@@ -457,42 +546,11 @@ cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int
     oz_kind_params(kind, &beta0, &beta, &esz, &kbe, &mp);
     dim3 grid((max_rows_pad + 7) / 8, npanels < 65535 ? npanels : 65535);
     if (kind == kOzInt8)
-        oz_split_kernel<kOzInt8><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta, esz);
+        oz_split_kernel<kOzInt8><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta);
     else if (kind == kOzBf16)
-        oz_split_kernel<kOzBf16><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta, esz);
+        oz_split_kernel<kOzBf16><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta);
     else
-        oz_split_kernel<kOzE4m3><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta, esz);
-    return cudaGetLastError();
-}
-
-template<int KIND>
-static cudaError_t launch_gemm_t(const DPanel *panels, const void *tmaps, const DOzTask *tasks,
-                                 const DCBlock *cblks, const DItem *items, int32_t nitems,
-                                 const int32_t *exps, double *c, int32_t add, int32_t S,
-                                 int32_t chunk_kb, int32_t *err, cudaStream_t s) {
-    int beta0, beta, esz, kbe;
-    int64_t mp;
-    oz_kind_params(KIND, &beta0, &beta, &esz, &kbe, &mp);
-    const int stage_bytes = S * (kATile + kBTile);
-    int stages = (200 * 1024) / stage_bytes;
-    if (stages > 4) stages = 4;
-    if (stages < 2) return cudaErrorInvalidValue;
-    // At least 120 KB so that a second CTA never shares the SM: each CTA
-    // holds all 512 TMEM columns.
-    size_t smem = (size_t)stages * stage_bytes + 1024;
-    if (smem < 120 * 1024) smem = 120 * 1024;
-    cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    if (g_nsm == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
-    }
-    int grid = nitems < g_nsm ? nitems : g_nsm;
-    if (grid < 1) return cudaSuccess;
-    oz_gemm_kernel<KIND><<<grid, kThreads, smem, s>>>(panels, static_cast<const uint8_t *>(tmaps), tasks, cblks,
-                                                     items, nitems, exps, c, add, S, stages, chunk_kb, beta0,
-                                                     beta, kbe, err);
+        oz_split_kernel<kOzE4m3><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta);
     return cudaGetLastError();
 }
 
@@ -502,10 +560,10 @@ cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const void *tmaps, co
                            cudaStream_t s) {
     if (S < 1 || S > 8) return cudaErrorInvalidValue;
     if (kind == kOzInt8)
-        return launch_gemm_t<kOzInt8>(panels, tmaps, tasks, cblks, items, nitems, exps, c, add, S, chunk_kb, err, s);
+        return launch_gemm_k<kOzInt8>(S, panels, tmaps, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
     if (kind == kOzBf16)
-        return launch_gemm_t<kOzBf16>(panels, tmaps, tasks, cblks, items, nitems, exps, c, add, S, chunk_kb, err, s);
-    return launch_gemm_t<kOzE4m3>(panels, tmaps, tasks, cblks, items, nitems, exps, c, add, S, chunk_kb, err, s);
+        return launch_gemm_k<kOzBf16>(S, panels, tmaps, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
+    return launch_gemm_k<kOzE4m3>(S, panels, tmaps, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
 }
 
 int oz_encode_tmap(void *tmap, int kind, void *slice_base, int32_t rows_pad, int32_t K_pad, int32_t S,
@@ -533,7 +591,7 @@ int oz_encode_tmap(void *tmap, int kind, void *slice_base, int32_t rows_pad, int
         encode = reinterpret_cast<encode_fn>(fn);
     }
     CUresult r = encode(reinterpret_cast<CUtensorMap *>(tmap), dt, 3, slice_base, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? 0 : (int)r;
 }
