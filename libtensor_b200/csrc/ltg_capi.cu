@@ -121,7 +121,7 @@ struct ContractExec {
 // mode, slice count).
 struct OzExec {
     int kind = 0, S = 0, chunk_kb = 1, npanels = 0, max_rows_pad = 0, nitems = 0;
-    DevBuf panels, tmaps, slices, exps, tasks, cblks, items, err;
+    DevBuf panels, slices, exps, tasks, cblks, items, err;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
     int32_t *err_host = nullptr;     // pinned copy of the device error word
@@ -485,7 +485,7 @@ OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, doubl
         p.rows = (int32_t)rows.total();
         p.K = (int32_t)k.total();
         p.rows_pad = (p.rows + 127) / 128 * 128;
-        p.K_pad = (p.K + kbe - 1) / kbe * kbe;
+        p.K_pad = (p.K + 31) / 32 * 32;      // whole 32-element split steps (a multiple of kbe)
         pack_sub(rows, p.nr, p.rext, p.rstr, nullptr);
         SubDims kk = k;
         if (kb_second) for (int i = 0; i < kk.n; i++) kk.s0[i] = kk.s1[i];
@@ -539,15 +539,6 @@ OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, doubl
     ex->nitems = (int)items.size();
     ex->slices.alloc(std::max<int64_t>(slice_bytes, 1024));
     ex->exps.alloc(std::max<int32_t>(exp_rows, 1) * sizeof(int32_t));
-    // TMA descriptors: A panels load 128-row boxes, B panels 64-row boxes
-    std::vector<uint8_t> maps((size_t)std::max(ex->npanels, 1) * 128, 0);
-    for (int i = 0; i < ex->npanels; i++) {
-        const DPanel &p = panels[i];
-        int r = oz_encode_tmap(maps.data() + (size_t)i * 128, kind, ex->slices.as<uint8_t>() + p.slice_off,
-                               p.rows_pad, p.K_pad, S, p.src == 0 ? 128 : 64);
-        if (r != 0) throw error(kErrCuda, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")");
-    }
-    upload_vec(ex->tmaps, maps, s);
     upload_vec(ex->panels, panels, s);
     upload_vec(ex->tasks, dt, s);
     upload_vec(ex->cblks, dc, s);
@@ -1103,7 +1094,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             LTG_CUDA(launch_oz_split(ox->kind, ox->panels.as<DPanel>(), ox->npanels, ox->max_rows_pad,
                                      plan->a->arena.as<double>(), plan->b->arena.as<double>(),
                                      ox->slices.as<uint8_t>(), ox->exps.as<int32_t>(), ox->S, s));
-            LTG_CUDA(launch_oz_gemm(ox->kind, ox->panels.as<DPanel>(), ox->tmaps.p, ox->tasks.as<DOzTask>(),
+            LTG_CUDA(launch_oz_gemm(ox->kind, ox->panels.as<DPanel>(), ox->slices.as<uint8_t>(), ox->tasks.as<DOzTask>(),
                                     ox->cblks.as<DCBlock>(), ox->items.as<DItem>(), ox->nitems,
                                     ox->exps.as<int32_t>(), c->arena.as<double>(), add, ox->S, ox->chunk_kb,
                                     ox->err.as<int32_t>(), s));

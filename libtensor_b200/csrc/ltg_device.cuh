@@ -50,8 +50,9 @@ struct DItem {
 enum OzKind { kOzInt8 = 0, kOzBf16 = 1, kOzE4m3 = 2 };
 
 // One split operand panel: the matricised view (rows x K) of a canonical
-// block, cut into S integer-valued slices stored row-major (K contiguous)
-// with rows padded to 128 and K padded to one 64-byte k block.
+// block, cut into S integer-valued slices stored as shared-memory tile images
+// (per row tile, 32-byte k block and slice), rows padded to 128 and K to 32
+// elements.
 struct DPanel {
     int64_t src_off;              // FP64 source block offset (elements)
     int64_t slice_off;            // byte offset of slice 0 in the slice arena
@@ -156,17 +157,13 @@ cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     const DItem *items, int32_t nitems, int32_t *counter, const double *a,
     const double *b, double *c, int32_t add, int32_t tile_cfg, cudaStream_t s);
 
-// Split-precision contraction: FP64 -> slices, then the tcgen05 grouped
-// slice-product kernel with FP64 recombination.  tmaps points to one
-// 128-byte CUtensorMap per panel in device memory.
+// Split-precision contraction: FP64 -> slice tile images, then the tcgen05
+// grouped slice-product kernel with FP64 recombination.
 cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int32_t max_rows_pad,
     const double *a, const double *b, uint8_t *slices, int32_t *exps, int32_t S, cudaStream_t s);
-cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const void *tmaps, const DOzTask *tasks,
+cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices, const DOzTask *tasks,
     const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps, double *c,
     int32_t add, int32_t S, int32_t chunk_kb, int32_t *err, cudaStream_t s);
-// Encodes the TMA descriptor of one panel (3D: K_pad, rows_pad, S).
-int oz_encode_tmap(void *tmap, int kind, void *slice_base, int32_t rows_pad, int32_t K_pad,
-                   int32_t S, int32_t box_rows);
 // Per kind: first-slice bits, further-slice bits, element bytes, k elements
 // per 64-byte k block, bound of one slice product.
 void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod);

@@ -29,7 +29,6 @@
 // with cp.async.bulk.tensor in 32-byte swizzled k blocks (one MMA k step per
 // pipeline stage, so even 8 slices leave room for 4 stages); no multicast.
 // Every mbarrier wait is bounded in time and reports through *err.
-#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 
@@ -103,9 +102,22 @@ template<> struct Pack4<kOzBf16> {
     }
 };
 
-// One warp per panel row, four consecutive k per lane; two passes over the
-// row (largest magnitude, then the slices).  Contiguous rows (one k
-// sub-dimension of stride 1) skip the mixed-radix index arithmetic.
+// Byte offset of (row r, byte kb_byte of k block kb, slice s) in the tile
+// images of a panel.  Panels are stored as the exact shared-memory images
+// the MMA reads: per (row tile, k block, slice) one TR x 32-byte tile,
+// K-major without swizzle (8-row x 16-byte core matrices, the two 16-byte k
+// halves 128 bytes apart, 8-row groups 256 bytes apart), so one pipeline
+// stage is a single contiguous bulk copy per operand.
+__device__ __forceinline__ int64_t tile_image_offset(int r, int TR, int nkb, int kb, int s, int S,
+                                                     int kb_byte) {
+    const int tile = r / TR, rr = r % TR;
+    return ((int64_t)(tile * nkb + kb) * S + s) * (TR * 32) + (rr >> 3) * 256 + (kb_byte >> 4) * 128 +
+           (rr & 7) * 16 + (kb_byte & 15);
+}
+
+// 32 panel rows per CTA, 8 threads per row, 4 consecutive k per thread; two
+// passes over each row (largest magnitude, then the slices).  Contiguous
+// rows (one k sub-dimension of stride 1) skip the mixed-radix arithmetic.
 template<int KIND>
 __global__ void __launch_bounds__(256)
 oz_split_kernel(const DPanel *__restrict__ panels, int32_t npanels,
@@ -113,52 +125,53 @@ oz_split_kernel(const DPanel *__restrict__ panels, int32_t npanels,
                 uint8_t *__restrict__ slices, int32_t *__restrict__ exps, int32_t S,
                 int32_t beta0, int32_t beta) {
     typedef typename Pack4<KIND>::T PT;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int kEsz = KIND == kOzBf16 ? 2 : 1;
+    constexpr int kKbe = 32 / kEsz;                  // elements per 32-byte k block
+    const int lr = threadIdx.x >> 3;                 // row within the CTA's 32 rows
+    const int c = threadIdx.x & 7;                   // 4-element chunk of a 32-element step
     for (int p = blockIdx.y; p < npanels; p += gridDim.y) {
         const DPanel &P = panels[p];
         const double *src = P.src ? B : A;
-        PT *base = reinterpret_cast<PT *>(slices + P.slice_off);
-        const int64_t sstride = (int64_t)P.rows_pad * P.K_pad / 4;     // packs per slice
-        const int64_t rstride = P.K_pad / 4;                            // packs per row
+        uint8_t *base = slices + P.slice_off;
+        const int TR = P.src ? 64 : 128;             // rows per tile image (MMA N or M)
+        const int nkb = P.K_pad / kKbe;
         const bool contig = P.nk == 1 && P.kstr[0] == 1;
-        for (int r = blockIdx.x * 8 + warp; r < P.rows_pad; r += gridDim.x * 8) {
-            if (r >= P.rows) {
-                PT z;
-                memset(&z, 0, sizeof(z));
-                for (int s = 0; s < S; s++)
-                    for (int k4 = lane; k4 < rstride; k4 += 32) base[s * sstride + r * rstride + k4] = z;
-                if (lane == 0) exps[P.exp_off + r] = 0;
-                continue;
-            }
-            const double *row = src + P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
+        for (int r0 = blockIdx.x * 32; r0 < P.rows_pad; r0 += gridDim.x * 32) {
+            const int r = r0 + lr;
+            const bool valid = r < P.rows;
+            const double *row = src + (valid ? P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
             double mx = 0.0;
-            for (int k4 = lane; k4 < rstride; k4 += 32) {
+            if (valid)
+                for (int k0 = 4 * c; k0 < P.K; k0 += 32)
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int k = 4 * k4 + j;
-                    if (k < P.K) mx = fmax(mx, fabs(row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)]));
-                }
-            }
-            for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                    for (int j = 0; j < 4; j++) {
+                        const int k = k0 + j;
+                        if (k < P.K) mx = fmax(mx, fabs(row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)]));
+                    }
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
             int e = 0;
             if (mx > 0.0) frexp(mx, &e);            // mx = f * 2^e, f in [0.5, 1)
-            if (lane == 0) exps[P.exp_off + r] = e;
+            if (c == 0) exps[P.exp_off + r] = e;
             const double up = ldexp(1.0, beta);
-            for (int k4 = lane; k4 < rstride; k4 += 32) {
+            for (int k0 = 4 * c; k0 < P.K_pad; k0 += 32) {
                 double t[4], sg[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
-                    const int k = 4 * k4 + j;
-                    const double x = k < P.K ? row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
+                    const int k = k0 + j;
+                    const double x = (valid && k < P.K) ? row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
                     t[j] = ldexp(x, beta0 - e);     // |t| < 2^beta0, exact
                 }
+                const int kb = k0 / kKbe, kb_byte = (k0 % kKbe) * kEsz;
                 for (int s = 0; s < S; s++) {
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
                         sg[j] = rint(t[j]);
                         t[j] = (t[j] - sg[j]) * up;   // exact (Sterbenz), power-of-two scale
                     }
-                    base[s * sstride + r * rstride + k4] = Pack4<KIND>::pack(sg);
+                    *reinterpret_cast<PT *>(base + tile_image_offset(r, TR, nkb, kb, s, S, kb_byte)) =
+                        Pack4<KIND>::pack(sg);
                 }
             }
         }
@@ -211,25 +224,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     }
 }
 
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *tmap, uint32_t bar,
-                                            int c0, int c1, int c2) {
+// One contiguous global -> shared bulk copy (16-byte aligned, size a
+// multiple of 16), completing on the stage's mbarrier.  No multicast.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
     asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4, %5}], [%2];"
-        :: "r"(dst), "l"(tmap), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        :: "r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
 }
 
-// K-major, 32-byte-swizzled shared-memory matrix descriptor: 8-row swizzle
-// atoms of 32-byte rows, atoms 256 bytes apart.
-__device__ __forceinline__ uint64_t smem_desc_sw32(uint32_t addr) {
+// K-major shared-memory matrix descriptor without swizzle: 8-row x 16-byte
+// core matrices, the two k halves 128 bytes apart (leading byte offset),
+// 8-row groups 256 bytes apart (stride byte offset).
+__device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t addr) {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
-    d |= (uint64_t)1 << 16;                           // leading byte offset (unused, 16 B)
-    d |= (uint64_t)(256 >> 4) << 32;                  // stride byte offset: 8 rows x 32 B
+    d |= (uint64_t)(128 >> 4) << 16;                  // leading byte offset
+    d |= (uint64_t)(256 >> 4) << 32;                  // stride byte offset
     d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
-    d |= (uint64_t)6 << 61;                           // layout: 32-byte swizzle
-    return d;
+    return d;                                         // layout type 0: no swizzle
 }
 
 template<int KIND>
@@ -260,6 +272,32 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t b
     }
 }
 
+// Same product with the A operand read from tensor memory (a_tmem).
+template<int KIND>
+__device__ __forceinline__ void umma_ts(uint32_t tmem_d, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+    if (KIND == kOzInt8) {
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0;\n"
+                     "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p; }"
+                     :: "r"(tmem_d), "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+    } else if (KIND == kOzBf16) {
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0;\n"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p; }"
+                     :: "r"(tmem_d), "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+    } else {
+        asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0;\n"
+                     "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], [%1], %2, %3, p; }"
+                     :: "r"(tmem_d), "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+    }
+}
+
+// Shared -> tensor memory copy of one 128-row x 32-byte operand tile (row r
+// to TMEM lane r, 8 columns).  Executes in issue order with the MMAs of the
+// same thread, so a single A buffer can be refilled every k step.
+__device__ __forceinline__ void tmem_cp_128x256b(uint32_t taddr, uint64_t sdesc) {
+    asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;" :: "r"(taddr), "l"(sdesc) : "memory");
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  :: "r"(smem_u32(bar)) : "memory");
@@ -279,7 +317,7 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 
 template<int KIND, int S>
 __global__ void __launch_bounds__(kThreads, 1)
-oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tmaps,
+oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ slices,
                const DOzTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
                const DItem *__restrict__ items, int32_t nitems, const int32_t *__restrict__ exps,
                double *__restrict__ Cp, int32_t add, int32_t stages, int32_t chunk_kb,
@@ -288,6 +326,13 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
     // 1024-byte aligned stage buffers: [stage][A slices | B slices]
     uint8_t *smem = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     constexpr int kStageBytes = S * (kATile + kBTile);
+    // A operand from tensor memory (tcgen05.cp of the A slices once per k
+    // step, products reading only B from shared memory) is supported when the
+    // accumulators leave room for it, but measured slower than reading both
+    // operands from shared memory on the ladder workloads (35.1 vs 39.4
+    // effective TFLOP/s at S = 7), so it is off.
+    constexpr bool kATmem = false && (S * kBN + S * 8 <= 512);
+    constexpr int kACol = S * kBN;
     __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar, acce_bar, drain_bar;
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
@@ -325,20 +370,18 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
                 const DCBlock &cb = cblks[item.cblk];
                 for (int ti = cb.t_begin; ti < cb.t_end && ok; ti++) {
                     const DOzTask t = tasks[ti];
-                    const void *ma = tmaps + (size_t)t.pa * 128;
-                    const void *mb = tmaps + (size_t)t.pb * 128;
                     const int nkb = panels[t.pa].K_pad / kbe;
+                    // tile images of this (row tile, k block): all S slices contiguous
+                    const uint8_t *ga = slices + panels[t.pa].slice_off + (int64_t)(item.m0 / kBM) * nkb * S * kATile;
+                    const uint8_t *gb = slices + panels[t.pb].slice_off + (int64_t)(item.n0 / kBN) * nkb * S * kBTile;
                     for (int kb = 0; kb < nkb; kb++) {
                         if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s)) { ok = false; break; }
                         const uint32_t sa = smem0 + st * kStageBytes;
                         const uint32_t sb = sa + S * kATile;
                         const uint32_t fb = smem_u32(&full_bar[st]);
                         mbar_expect_tx(&full_bar[st], (uint32_t)kStageBytes);
-#pragma unroll
-                        for (int s = 0; s < S; s++) {
-                            tma_load_3d(sa + s * kATile, ma, fb, kb * kbe, item.m0, s);
-                            tma_load_3d(sb + s * kBTile, mb, fb, kb * kbe, item.n0, s);
-                        }
+                        bulk_load(sa, ga + (int64_t)kb * S * kATile, S * kATile, fb);
+                        bulk_load(sb, gb + (int64_t)kb * S * kBTile, S * kBTile, fb);
                         armed_parity[st] = (int)ph;
                         if (++st == stages) { st = 0; ph ^= 1; }
                     }
@@ -379,18 +422,31 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
                             tc_fence_after();
                             const uint32_t a0 = smem0 + st * kStageBytes;
                             const uint32_t b0 = a0 + S * kATile;
-                            const uint64_t da = smem_desc_sw32(a0), db = smem_desc_sw32(b0);
+                            const uint64_t da = smem_desc_kmajor(a0), db = smem_desc_kmajor(b0);
                             const uint32_t first = kb == kb0 ? 0u : 1u;
+                            if (kATmem) {
+                                // A slices into tensor memory once per k step; the
+                                // products then read only B from shared memory.
+#pragma unroll
+                                for (int sa = 0; sa < S; sa++)
+                                    tmem_cp_128x256b(tmem + (uint32_t)(kACol + sa * 8),
+                                                     da + (uint64_t)((sa * kATile) >> 4));
+                            }
 #pragma unroll
                             for (int l = 0; l < S; l++) {
 #pragma unroll
                                 for (int sa = 0; sa <= l; sa++) {
                                     const int sb = l - sa;
                                     // descriptor start addresses advance in 16-byte units
-                                    umma<KIND>(tmem + (uint32_t)(l * kBN),
-                                               da + (uint64_t)((sa * kATile) >> 4),
-                                               db + (uint64_t)((sb * kBTile) >> 4), idesc,
-                                               sa == 0 ? first : 1u);
+                                    if (kATmem)
+                                        umma_ts<KIND>(tmem + (uint32_t)(l * kBN), tmem + (uint32_t)(kACol + sa * 8),
+                                                      db + (uint64_t)((sb * kBTile) >> 4), idesc,
+                                                      sa == 0 ? first : 1u);
+                                    else
+                                        umma<KIND>(tmem + (uint32_t)(l * kBN),
+                                                   da + (uint64_t)((sa * kATile) >> 4),
+                                                   db + (uint64_t)((sb * kBTile) >> 4), idesc,
+                                                   sa == 0 ? first : 1u);
                                 }
                             }
                             umma_commit(&empty_bar[st]);       // frees the stage when these MMAs finish
@@ -493,7 +549,7 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ tm
 int g_nsm = 0;
 
 template<int KIND, int S>
-cudaError_t launch_gemm_s(const DPanel *panels, const void *tmaps, const DOzTask *tasks, const DCBlock *cblks,
+cudaError_t launch_gemm_s(const DPanel *panels, const uint8_t *slices, const DOzTask *tasks, const DCBlock *cblks,
                           const DItem *items, int32_t nitems, const int32_t *exps, double *c, int32_t add,
                           int32_t chunk_kb, int32_t *err, cudaStream_t s) {
     int beta0, beta, esz, kbe;
@@ -517,18 +573,17 @@ cudaError_t launch_gemm_s(const DPanel *panels, const void *tmaps, const DOzTask
     }
     int grid = nitems < g_nsm ? nitems : g_nsm;
     if (grid < 1) return cudaSuccess;
-    oz_gemm_kernel<KIND, S><<<grid, kThreads, smem, s>>>(panels, static_cast<const uint8_t *>(tmaps), tasks, cblks,
-                                                        items, nitems, exps, c, add, stages, chunk_kb, beta0, beta,
-                                                        kbe, err);
+    oz_gemm_kernel<KIND, S><<<grid, kThreads, smem, s>>>(panels, slices, tasks, cblks, items, nitems, exps, c, add,
+                                                        stages, chunk_kb, beta0, beta, kbe, err);
     return cudaGetLastError();
 }
 
 template<int KIND>
-cudaError_t launch_gemm_k(int S, const DPanel *panels, const void *tmaps, const DOzTask *tasks,
+cudaError_t launch_gemm_k(int S, const DPanel *panels, const uint8_t *slices, const DOzTask *tasks,
                           const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps, double *c,
                           int32_t add, int32_t chunk_kb, int32_t *err, cudaStream_t s) {
     switch (S) {
-#define CASE_S(n) case n: return launch_gemm_s<KIND, n>(panels, tmaps, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
+#define CASE_S(n) case n: return launch_gemm_s<KIND, n>(panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
     CASE_S(1) CASE_S(2) CASE_S(3) CASE_S(4) CASE_S(5) CASE_S(6) CASE_S(7) CASE_S(8)
 #undef CASE_S
     default: return cudaErrorInvalidValue;
@@ -544,7 +599,7 @@ cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int
     int beta0, beta, esz, kbe;
     int64_t mp;
     oz_kind_params(kind, &beta0, &beta, &esz, &kbe, &mp);
-    dim3 grid((max_rows_pad + 7) / 8, npanels < 65535 ? npanels : 65535);
+    dim3 grid((max_rows_pad + 31) / 32, npanels < 65535 ? npanels : 65535);
     if (kind == kOzInt8)
         oz_split_kernel<kOzInt8><<<grid, 256, 0, s>>>(panels, npanels, a, b, slices, exps, S, beta0, beta);
     else if (kind == kOzBf16)
@@ -554,46 +609,16 @@ cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int
     return cudaGetLastError();
 }
 
-cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const void *tmaps, const DOzTask *tasks,
+cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices, const DOzTask *tasks,
                            const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps,
                            double *c, int32_t add, int32_t S, int32_t chunk_kb, int32_t *err,
                            cudaStream_t s) {
     if (S < 1 || S > 8) return cudaErrorInvalidValue;
     if (kind == kOzInt8)
-        return launch_gemm_k<kOzInt8>(S, panels, tmaps, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
+        return launch_gemm_k<kOzInt8>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
     if (kind == kOzBf16)
-        return launch_gemm_k<kOzBf16>(S, panels, tmaps, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
-    return launch_gemm_k<kOzE4m3>(S, panels, tmaps, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
-}
-
-int oz_encode_tmap(void *tmap, int kind, void *slice_base, int32_t rows_pad, int32_t K_pad, int32_t S,
-                   int32_t box_rows) {
-    int beta0, beta, esz, kbe;
-    int64_t mp;
-    oz_kind_params(kind, &beta0, &beta, &esz, &kbe, &mp);
-    CUtensorMapDataType dt = kind == kOzBf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
-    cuuint64_t dims[3] = {(cuuint64_t)K_pad, (cuuint64_t)rows_pad, (cuuint64_t)S};
-    cuuint64_t strides[2] = {(cuuint64_t)K_pad * esz, (cuuint64_t)rows_pad * K_pad * esz};
-    cuuint32_t box[3] = {(cuuint32_t)kbe, (cuuint32_t)box_rows, 1};
-    cuuint32_t estr[3] = {1, 1, 1};
-    // The driver entry point is looked up at run time so that the library
-    // also loads on hosts without a GPU driver.
-    typedef CUresult (*encode_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-    static encode_fn encode = nullptr;
-    if (!encode) {
-        void *fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn)
-            return -1;
-        encode = reinterpret_cast<encode_fn>(fn);
-    }
-    CUresult r = encode(reinterpret_cast<CUtensorMap *>(tmap), dt, 3, slice_base, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
-                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS ? 0 : (int)r;
+        return launch_gemm_k<kOzBf16>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
+    return launch_gemm_k<kOzE4m3>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
 }
 
 }  // namespace ltg
