@@ -41,17 +41,23 @@ FP64_NOMINAL = 40.0
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=30)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ltg", choices=["ltg", "reference"])
-    p.add_argument("--workload", default="ladder-large", choices=sorted(WORKLOADS))
-    p.add_argument("--mode", default="plain", choices=sorted(MODES))
-    p.add_argument("--nslices", type=int, default=0)
+    # Headline: the split-precision ladder o=40 v=240 (blocks 64/56 per spin)
+    # at <= 1e-12, with the plain FP64 DMMA path timed on the same workload.
+    p.add_argument("--workload", default="ladder-split", choices=sorted(WORKLOADS))
+    p.add_argument("--mode", default="ozaki-int8", choices=sorted(MODES))
+    p.add_argument("--nslices", type=int, default=7)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--no-plain", action="store_true", help="skip the plain-DMMA companion timing")
     p.add_argument("--tile", type=int, default=-1, help="force one tile shape (debug)")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.mode == "plain":
+        a.nslices = 0
+    return a
 
 
 def workload(name):
@@ -90,7 +96,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                 "-lms", "50", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
@@ -251,15 +257,16 @@ def ltg_arm(args):
     tiles = None
     if args.tile >= 0:
         op.set_tile(args.tile)
-    elif not args.no_autotune and mode == 0:
-        tiles = op.autotune(C, mode=mode, nslices=args.nslices, reps=1)
+    elif not args.no_autotune:
+        # tile shapes of the plain FP64 kernel (also the companion timing below)
+        tiles = op.autotune(C, mode=0, nslices=0, reps=1)
+    clocks = ClockSampler(local)
+    clocks.start()            # nvidia-smi needs a moment to start: begin before the warm-up
     for _ in range(max(3, args.warmup)):
         op.perform(C, mode=mode, nslices=args.nslices)
     barrier()
 
     # ---- device-resident timing
-    clocks = ClockSampler(local)
-    clocks.start()
     n0 = ctx.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
@@ -291,6 +298,25 @@ def ltg_arm(args):
                     "against": "plain FP64 DMMA result of the same call (itself within 1e-13 of the "
                                "reference CPU btod_contract2)"}
         Cref.close()
+
+    # plain FP64 DMMA companion on the same workload (the metric's denominator)
+    plain = None
+    if mode != 0 and not args.no_plain:
+        for _ in range(3):
+            op.perform(C, mode=0)
+        barrier()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            op.perform(C, mode=0)
+        p1.record(stream)
+        barrier()
+        pms = p0.elapsed_time(p1) / args.steps
+        if world > 1:
+            t = torch.tensor([pms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pms = float(t.item())
+        plain = {"value": world * flops / (pms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": pms}
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -356,6 +382,9 @@ def ltg_arm(args):
            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
     if tiles:
         out["config"]["autotuned_tiles"] = {f"{m}x{n}": t for (m, n), t in tiles.items()}
+    if plain:
+        out["plain_fp64_dmma"] = plain
+        out["split_vs_plain"] = value / plain["value"]
     if accuracy:
         out["accuracy"] = accuracy
         out["roofline"]["note"] = ("split-precision: achieved is effective FP64 TFLOP/s over the split pass and "
