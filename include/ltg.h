@@ -188,6 +188,20 @@ int ltg_dotprod(ltg_bt *a, const int32_t *perma, ltg_bt *b,
 /* Asynchronous form: result left in device memory at *dev_out. */
 int ltg_dotprod_async(ltg_bt *a, const int32_t *perma, ltg_bt *b,
                       const int32_t *permb, double *dev_out);
+/* Allocation-free dot product sum_i x[i]*y[i] of two device arrays of the
+ * calling thread's current device, run on `stream` (a cudaStream_t; NULL =
+ * default stream); synchronous, result in *out (host).  No reference
+ * counterpart: it serves callers that must not allocate device memory (error
+ * paths after an out-of-memory failure, programs whose memory is reserved by
+ * another allocator, loops that cudaMalloc/cudaFree would stall).  Partial
+ * sums live in one fixed device array per device (16384 partials of 65536
+ * elements each): n is limited to 2^30 elements and larger n returns
+ * LTG_ERR_BAD_ARG.  All calls on a device share that array, so calls that
+ * overlap in time race and must be serialised by the caller.  The first call
+ * on a device also looks up the array's address; make it before any stream
+ * capture on that device.  The sum order depends only on n. */
+int ltg_dot_noalloc(const double *x, const double *y, int64_t n, void *stream,
+                    double *out);
 /* a *= c  (btod_scale) */
 int ltg_scale(ltg_bt *a, double c);
 /* a[i,j,a,b] /= (e_i + e_j - e_a - e_b) style denominator over a 4-index

@@ -92,6 +92,7 @@ _SIGS = {
     "ltg_add": (C.c_int, [C.c_int32, C.POINTER(c_vp), c_i32p, c_dblp, c_vp, C.c_int32, C.c_double]),
     "ltg_dotprod": (C.c_int, [c_vp, c_i32p, c_vp, c_i32p, c_dblp]),
     "ltg_dotprod_async": (C.c_int, [c_vp, c_i32p, c_vp, c_i32p, c_vp]),
+    "ltg_dot_noalloc": (C.c_int, [c_vp, c_vp, C.c_int64, c_vp, c_dblp]),
     "ltg_scale": (C.c_int, [c_vp, C.c_double]),
     "ltg_denominator": (C.c_int, [c_vp, c_dblp, C.c_int32]),
     "ltg_graph_begin": (C.c_int, [c_vp]),

@@ -30,6 +30,7 @@ SOURCES = [
     "contract_fp64.cu",
     "elementwise.cu",
     "ozaki.cu",
+    "noalloc.cu",
 ]
 OPTIONAL_SOURCES = []
 

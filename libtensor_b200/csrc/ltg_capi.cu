@@ -87,6 +87,11 @@ void upload_vec(DevBuf &d, const std::vector<T> &v, cudaStream_t s) {
 
 }  // namespace
 
+namespace ltg {
+// Message for ltg_last_error() from entry points defined in other files.
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}
+
 struct ltg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
