@@ -34,6 +34,9 @@ WORKLOADS = {
     "ring": "RING_D2H",
     "ring-small": "RING_D2H_SMALL",
 }
+# HBM-bound operations (btod_copy / btod_add / btod_dotprod) on the CCD
+# iteration's tensors, o=30 v=300 (blocks 15 / 50,50,50 per spin).
+TRANSFER_WORKLOADS = ("copy-vvvv", "add-x4", "dot-vvvv")
 MODES = {"plain": 0, "ozaki-bf16": 1, "ozaki-fp8": 2, "ozaki-int8": 3}
 FP64_NOMINAL = 40.0
 
@@ -46,7 +49,7 @@ def parse():
     p.add_argument("--impl", default="ltg", choices=["ltg", "reference"])
     # Headline: the split-precision ladder o=40 v=240 (blocks 64/56 per spin)
     # at <= 1e-12, with the plain FP64 DMMA path timed on the same workload.
-    p.add_argument("--workload", default="ladder-split", choices=sorted(WORKLOADS))
+    p.add_argument("--workload", default="ladder-split", choices=sorted(WORKLOADS) + list(TRANSFER_WORKLOADS))
     p.add_argument("--mode", default="ozaki-int8", choices=sorted(MODES))
     p.add_argument("--nslices", type=int, default=7)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -270,11 +273,14 @@ def ltg_arm(args):
     n0 = ctx.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
+    ctx.set_timing(True)          # event pair around every kernel launch of the library
     e0.record(stream)
     for _ in range(args.steps):
         op.perform(C, mode=mode, nslices=args.nslices)
     e1.record(stream)
     barrier()
+    ktimes = ctx.kernel_times()
+    ctx.set_timing(False)
     launches = ctx.launch_count() - n0
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
@@ -354,12 +360,10 @@ def ltg_arm(args):
                "ms_per_step": ems}
         del ha, hb, hc
 
-    # ---- roofline of the dominant kernel (the contraction is the whole step)
-    peak = measure_fp64_peak(torch, dev) if rank == 0 else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(f"{args.workload}:{args.mode}")
+    # ---- roofline of the dominant kernel, timed by events inside the timed region
+    roofline = None
+    if rank == 0:
+        roofline = contraction_roofline(torch, dev, args, flops, ktimes)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -370,15 +374,12 @@ def ltg_arm(args):
         dist.destroy_process_group()
     if rank != 0:
         return
-    achieved = flops / (ms * 1e-3) / 1e12
     out = {"metric": metric_name(), "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, symmetrised; no public dataset)",
-           "config": config_of(args, cfg, flops),
-           "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "frac": achieved / peak if peak else None, "traffic": traffic,
-                        "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU (FP64 tensor path); "
-                                       f"nominal {FP64_NOMINAL} TFLOP/s"},
+           "config": config_of(args, cfg, flops), "roofline": roofline,
+           "kernels": {k: {"launches": n, "ms_total": v, "share": v / sum(x for x, _ in ktimes.values())}
+                       for k, (v, n) in ktimes.items()},
            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
     if tiles:
         out["config"]["autotuned_tiles"] = {f"{m}x{n}": t for (m, n), t in tiles.items()}
@@ -387,9 +388,78 @@ def ltg_arm(args):
         out["split_vs_plain"] = value / plain["value"]
     if accuracy:
         out["accuracy"] = accuracy
-        out["roofline"]["note"] = ("split-precision: achieved is effective FP64 TFLOP/s over the split pass and "
-                                   "the slice products; peak is the FP64 DGEMM rate it replaces")
     print(json.dumps(out))
+
+
+def measure_int8_peak(torch, dev):
+    """cuBLASLt INT8 GEMM 8192^3 (torch._int_mm, best of 3), TOP/s."""
+    n = 8192
+    a = torch.randint(-64, 64, (n, n), dtype=torch.int8, device=dev)
+    b = torch.randint(-64, 64, (n, n), dtype=torch.int8, device=dev)
+    torch._int_mm(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def contraction_roofline(torch, dev, args, flops, ktimes):
+    """Roofline of the kernel with the largest device time in the timed region.
+
+    Plain mode: the DMMA contraction against the live cuBLAS DGEMM rate.
+    Split modes: the slice-product kernel; its algorithmic work is the
+    S(S+1)/2 slice products per FP64 multiply-add of the schedule
+    (2*|C|*K each), against the live dense rate of the slice type."""
+    if not ktimes:
+        return None
+    kname = max(ktimes, key=lambda k: ktimes[k][0])
+    kms, kn = ktimes[kname]
+    sec = kms * 1e-3 / max(1, kn)                       # average launch
+    per_launch = flops * args.steps / max(1, kn)        # algorithmic FP64 flops per launch
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        t = json.load(open(tpath)).get(f"{kname}:{args.workload}:{args.mode}")
+        traffic = t.get("bytes_per_launch") if isinstance(t, dict) else t
+    if kname == "contract_fp64":
+        peak = measure_fp64_peak(torch, dev)
+        ach = per_launch / sec / 1e12
+        return {"bound": "tensor", "kernel": kname, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                "frac": ach / peak, "traffic": traffic, "avg_launch_ms": sec * 1e3,
+                "peak_source": "measured live: cuBLAS DGEMM 8192^3 (FP64 tensor path), "
+                               f"nominal {FP64_NOMINAL} TFLOP/s"}
+    if kname == "oz_gemm":
+        S = args.nslices if args.nslices > 0 else (8 if args.mode == "ozaki-fp8" else 7)
+        prods = S * (S + 1) // 2
+        ach = prods * per_launch / sec / 1e12
+        if args.mode == "ozaki-int8":
+            try:
+                peak, src = measure_int8_peak(torch, dev), "measured live: cuBLASLt INT8 GEMM 8192^3 (torch._int_mm)"
+            except Exception as e:     # no INT8 GEMM in this torch build
+                peak, src = None, f"INT8 GEMM unavailable: {e}"
+            unit = "TFLOP/s"       # INT8 multiply-adds counted as 2 operations, like flops
+        else:
+            mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+                os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
+            bf = float(mp["bf16_tflops"])
+            peak = bf if args.mode == "ozaki-bf16" else 2 * bf
+            src = ("measured bf16 dense (MEASURED_PEAKS.json bf16_tflops)" if args.mode == "ozaki-bf16" else
+                   "2 x measured bf16 dense (FP8 E4M3 is twice the bf16 rate on this part)")
+            unit = "TFLOP/s"
+        return {"bound": "tensor", "kernel": kname, "achieved": ach, "peak": peak, "unit": unit,
+                "frac": ach / peak if peak else None, "traffic": traffic, "avg_launch_ms": sec * 1e3,
+                "slice_products": prods, "effective_fp64_tflops": per_launch / sec / 1e12,
+                "peak_source": src}
+    return {"bound": "hbm", "kernel": kname, "achieved": None, "peak": None, "unit": "GB/s",
+            "frac": None, "traffic": traffic, "avg_launch_ms": sec * 1e3}
 
 
 def cpu_baseline(cfg, a_spec, b_spec, A, B, flops):
@@ -409,9 +479,219 @@ def cpu_baseline(cfg, a_spec, b_spec, A, B, flops):
                 "sample": f"failed: {e}"}
 
 
+# ---------------------------------------------------------------- HBM-bound operations
+
+def hbm_peak():
+    """Measured copy bandwidth of this GPU model (GB/s) and where it came from."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, torch copy)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def transfer_setup(name, ctx):
+    """Operands, the operation and its algorithmic bytes per call."""
+    from libtensor_b200 import spec as S
+    from libtensor_b200.core import block_tensor, btod_add, btod_copy, btod_dotprod
+    cfg = S.LADDER_CCD
+    if name == "copy-vvvv":
+        a = block_tensor(ctx, cfg.v_spec())
+        a.fill_seeded(31, 1.0)
+        b = a.permuted((0, 2, 1, 3))
+        op = btod_copy(a, (0, 2, 1, 3), 1.0)
+        run = lambda: op.perform(b)                       # noqa: E731
+        return dict(srcs=[a], dst=b, run=run, bytes=16 * b.nelems, terms=1,
+                    desc="B = P(0,2,1,3) V, V(a,b,c,d) v=300 antisym ab, cd + spin")
+    if name == "add-x4":
+        x = block_tensor(ctx, cfg.x_spec())
+        x.fill_seeded(32, 1.0)
+        r = block_tensor(ctx, cfg.x_spec())
+        op = btod_add(x, None, 1.0)
+        op.add_op(x, (1, 0, 2, 3), -1.0)
+        op.add_op(x, (0, 1, 3, 2), -0.5)
+        op.add_op(x, (1, 0, 3, 2), 0.5)
+        run = lambda: op.perform(r)                       # noqa: E731
+        return dict(srcs=[x], dst=r, run=run, bytes=(8 * 4 + 8) * r.nelems, terms=4,
+                    desc="r = X - P(ij)X - 0.5 P(ab)X + 0.5 P(ij)P(ab)X, X(i,j,a,b) o=30 v=300 spin blocks")
+    if name == "dot-vvvv":
+        a = block_tensor(ctx, cfg.v_spec())
+        b = block_tensor(ctx, cfg.v_spec())
+        a.fill_seeded(33, 1.0)
+        b.fill_seeded(34, 1.0)
+        op = btod_dotprod(a, None, b, (1, 0, 3, 2))
+        out = {}
+        run = lambda: out.__setitem__("v", op.calculate())   # noqa: E731
+        return dict(srcs=[a, b], dst=None, run=run, bytes=16 * a.nelems, terms=2, out=out, op=op,
+                    desc="<V, P(1,0,3,2) V'>, V v=300 antisym ab, cd + spin")
+    raise ValueError(name)
+
+
+def transfer_arm(args):
+    import torch
+    from libtensor_b200.core import Context
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    ctx = Context(local)
+    w = transfer_setup(args.workload, ctx)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(max(3, args.warmup)):
+        w["run"]()
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    n0 = ctx.launch_count()
+    ctx.set_timing(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        w["run"]()
+    e1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    launches = ctx.launch_count() - n0
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    gbs = world * w["bytes"] / (ms * 1e-3) / 1e9
+    kname = "dot" if args.workload.startswith("dot") else "transfer"
+    kms, kn = kt.get(kname, (0.0, 0))
+    peak, peak_src = hbm_peak()
+    achieved = w["bytes"] * args.steps / (kms * 1e-3) / 1e9 if kms > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(f"{kname}:{args.workload}")
+
+    e2e = None
+    if not args.no_e2e:
+        hs = [torch.empty(max(1, t.nelems), dtype=torch.float64, pin_memory=True) for t in w["srcs"]]
+        hd = torch.empty(max(1, w["dst"].nelems), dtype=torch.float64, pin_memory=True) if w["dst"] else None
+        for t, h in zip(w["srcs"], hs):
+            t.download_async(h.data_ptr())
+        ctx.synchronize()
+
+        def e2e_step():
+            for t, h in zip(w["srcs"], hs):
+                t.upload_async(h.data_ptr())
+            w["run"]()
+            if hd is not None:
+                w["dst"].download_async(hd.data_ptr())
+        for _ in range(2):
+            e2e_step()
+        ctx.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        f1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1) / args.steps
+        h2d = sum(8 * t.nelems for t in w["srcs"])
+        d2h = 8 * w["dst"].nelems if w["dst"] else 8
+        e2e = {"value": world * w["bytes"] / (ems * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ems}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {"metric": f"{args.workload}: algorithmic GB/s", "value": gbs, "unit": "GB/s", "n_gpus": world,
+           "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, symmetrised)",
+           "config": {"workload": f"{args.workload}: {w['desc']}", "algorithmic_bytes": w["bytes"],
+                      "l2": "operands larger than L2 (no flush)"},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak if achieved else None, "traffic": traffic,
+                        "peak_source": peak_src, "kernel": kname},
+           "kernels": {k: {"launches": n, "ms_total": v} for k, (v, n) in kt.items()},
+           "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": None}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = transfer_cpu_baseline(args.workload, w)
+    print(json.dumps(out))
+
+
+def transfer_reference(name, w):
+    """The reference's own btod_copy / btod_add / btod_dotprod on the same
+    canonical blocks; returns (callable, tensors to close)."""
+    from oracle import refapi as R
+    refs = []
+    for t in w["srcs"]:
+        r = R.RefBT(t.spec)
+        host = t.download()
+        for bidx, blk in t.blocks(host):
+            r.set_block(bidx, blk)
+        refs.append(r)
+    if name == "copy-vvvv":
+        from libtensor_b200.spec import permuted_spec
+        rb = R.RefBT(permuted_spec(w["srcs"][0].spec, (0, 2, 1, 3)))
+        return (lambda: R.ref_copy(refs[0], (0, 2, 1, 3), 1.0, rb)), refs + [rb]
+    if name == "add-x4":
+        rr = R.RefBT(w["dst"].spec)
+        x = refs[0]
+        ops = [(x, None, 1.0), (x, (1, 0, 2, 3), -1.0), (x, (0, 1, 3, 2), -0.5), (x, (1, 0, 3, 2), 0.5)]
+        return (lambda: R.ref_add(ops, rr)), refs + [rr]
+    return (lambda: R.ref_dotprod(refs[0], None, refs[1], (1, 0, 3, 2))), refs
+
+
+def transfer_cpu_baseline(name, w, steps=2, budget_s=30.0):
+    try:
+        from oracle import refapi as R
+        if not R.available():
+            return None
+        R.set_threads(os.cpu_count() or 1)
+        fn, refs = transfer_reference(name, w)
+        ts = []
+        t_start = time.perf_counter()
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+            if time.perf_counter() - t_start > budget_s:
+                break
+        for r in refs:
+            r.close()
+        sec = float(np.median(ts))
+        return {"value": w["bytes"] / sec / 1e9, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"full workload, {len(ts)} call(s) of the reference built from its sources",
+                "ms_per_step": sec * 1e3}
+    except Exception as e:
+        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"failed: {e}"}
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload in TRANSFER_WORKLOADS:
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) != 0:
+                return
+            import torch  # noqa: F401  (device context for the operand fill)
+            from libtensor_b200.core import Context
+            ctx = Context(0)
+            w = transfer_setup(args.workload, ctx)
+            b = transfer_cpu_baseline(args.workload, w, steps=args.steps, budget_s=120.0)
+            print(json.dumps({"metric": f"{args.workload}: algorithmic GB/s", "value": b["value"], "unit": "GB/s",
+                              "impl": "reference", "n_gpus": args.gpus, "higher_is_better": True,
+                              "cpu_baseline": b, "e2e": {"value": b["value"], "unit": "GB/s",
+                                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        else:
+            transfer_arm(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         ltg_arm(args)

@@ -86,6 +86,25 @@ int ltg_ctx_stream(ltg_ctx *ctx, void **stream);
 int ltg_ctx_set_host_threads(ltg_ctx *ctx, int nthreads);
 /* Number of device kernels launched by this context so far. */
 int ltg_ctx_launch_count(ltg_ctx *ctx, int64_t *count);
+/* Per-kernel device timing.  While enabled, every kernel launch of the
+ * context (outside graph capture) is bracketed by CUDA events on its stream;
+ * ltg_ctx_kernel_times() waits for the stream and returns, per kernel kind,
+ * the summed device time (ms) and the number of timed launches since timing
+ * was enabled.  Enabling resets the totals.  No reference counterpart (the
+ * reference's libutil timers time host regions). */
+enum {
+    LTG_KERNEL_CONTRACT_FP64 = 0,   /* plain FP64 DMMA contraction */
+    LTG_KERNEL_OZ_SPLIT = 1,        /* split-precision: FP64 -> slices */
+    LTG_KERNEL_OZ_GEMM = 2,         /* split-precision: slice products */
+    LTG_KERNEL_TRANSFER = 3,        /* btod_copy / btod_add */
+    LTG_KERNEL_DOT = 4,             /* btod_dotprod (both passes) */
+    LTG_KERNEL_SCALE = 5,
+    LTG_KERNEL_FILL = 6,            /* seeded fill */
+    LTG_KERNEL_DENOMINATOR = 7,
+    LTG_KERNEL_KINDS = 8
+};
+int ltg_ctx_set_timing(ltg_ctx *ctx, int32_t enable);
+int ltg_ctx_kernel_times(ltg_ctx *ctx, double *ms, int64_t *launches);
 
 /* ---- block tensors (libtensor/block_tensor/block_tensor.h:22) --------- */
 int ltg_bt_create(ltg_ctx *ctx, const ltg_bt_spec *spec, ltg_bt **out);

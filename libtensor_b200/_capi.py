@@ -93,6 +93,8 @@ _SIGS = {
     "ltg_dotprod": (C.c_int, [c_vp, c_i32p, c_vp, c_i32p, c_dblp]),
     "ltg_dotprod_async": (C.c_int, [c_vp, c_i32p, c_vp, c_i32p, c_vp]),
     "ltg_dot_noalloc": (C.c_int, [c_vp, c_vp, C.c_int64, c_vp, c_dblp]),
+    "ltg_ctx_set_timing": (C.c_int, [c_vp, C.c_int32]),
+    "ltg_ctx_kernel_times": (C.c_int, [c_vp, c_dblp, c_i64p]),
     "ltg_scale": (C.c_int, [c_vp, C.c_double]),
     "ltg_denominator": (C.c_int, [c_vp, c_dblp, C.c_int32]),
     "ltg_graph_begin": (C.c_int, [c_vp]),

@@ -60,6 +60,20 @@ class Context:
         check(lib().ltg_ctx_launch_count(self.h, C.byref(n)))
         return n.value
 
+    KERNELS = ("contract_fp64", "oz_split", "oz_gemm", "transfer", "dot", "scale", "fill", "denominator")
+
+    def set_timing(self, enable: bool):
+        """Per-kernel device timing with CUDA events (resets the totals)."""
+        check(lib().ltg_ctx_set_timing(self.h, 1 if enable else 0))
+
+    def kernel_times(self):
+        """{kernel: (total ms, timed launches)} since timing was enabled."""
+        k = len(self.KERNELS)
+        ms = (C.c_double * k)()
+        n = (C.c_int64 * k)()
+        check(lib().ltg_ctx_kernel_times(self.h, ms, n))
+        return {name: (ms[i], n[i]) for i, name in enumerate(self.KERNELS) if n[i]}
+
     def set_host_threads(self, n: int):
         check(lib().ltg_ctx_set_host_threads(self.h, n))
 

@@ -10,85 +10,340 @@
 //
 // Every destination block is written exactly once per launch: all terms of
 // a btod_add are read in the same pass, so the traffic is (8T + 8) bytes per
-// destination element (+8 when accumulating).  Threads run along the
-// innermost destination dimension; when a term reads that dimension with a
-// non-unit stride (a transposition such as P(ab)), a shared-memory tile turns
-// the strided reads into coalesced ones.
+// destination element (+8 when accumulating).  A block is traversed as planes
+// of A rows x B columns (DJob).  In row mode (every term reads the columns with
+// unit stride) each warp takes items of a few thousand elements (a chunk of
+// rows x a segment of columns): the outer digits are found once per item with
+// 32-bit divisions and shared by all terms, and the lanes walk the item's
+// cells (a double, or a double2 where every term is 16-byte aligned) in order,
+// stepping row and column without divisions and carrying several cells so that
+// several independent loads per term are in flight.  A job with a transposing
+// term runs in tiled mode: the CTA stages each tile of a transposing term
+// through shared memory, read along the source's contiguous dim and written
+// along the destination's.
 #include "ltg_device.cuh"
 
 namespace ltg {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+// Cells (one double, or a double2 on the 16-byte path) carried per lane and
+// step in row mode: more cells keep more loads in flight, fewer keep the
+// registers (and so the resident CTAs) of many-term adds.
+template<int NT>
+struct CellUnroll { static constexpr int value = NT <= 2 ? 4 : (NT <= 4 ? 2 : 1); };
 
-__device__ __forceinline__ int64_t outer_base(int64_t row, int nout, const int32_t *ext,
-                                              const int32_t *str) {
-    // decompose row over the outer dims (ext[0..nout)) row-major
-    int64_t off = 0;
-    for (int i = nout - 1; i >= 0; i--) {
-        int64_t e = ext[i];
-        int64_t q = row / e;
-        off += (row - q * e) * str[i];
-        row = q;
-    }
-    return off;
+// Job and term descriptors of the current unit, staged in shared memory.
+template<int NT>
+struct UnitDesc {
+    DJob j;
+    DTerm t[NT];
+};
+
+constexpr int kTile = 64;                 // tiled mode: at most kTile x kTile elements
+constexpr int kTileLd = kTile + 1;        // padded shared-memory row
+constexpr int kTileElems = kTile * kTileLd;
+
+template<int NT>
+__device__ __forceinline__ void stage_unit(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
+                                           int32_t job, UnitDesc<NT> &sd) {
+    __syncthreads();                              // previous unit done with sd and the tiles
+    if (threadIdx.x == 0) sd.j = jobs[job];
+    __syncthreads();
+    if ((int)threadIdx.x < sd.j.nterms && (int)threadIdx.x < NT) sd.t[threadIdx.x] = terms[sd.j.term0 + threadIdx.x];
+    __syncthreads();
 }
 
-// Generic path: threads along the innermost dim (coalesced destination).
+// Destination and per-term source offsets of row a of plane p.
+template<int NT>
+__device__ __forceinline__ void plane_row_bases(const UnitDesc<NT> &sd, uint32_t p, uint32_t a,
+                                                int64_t &dst, int64_t (&src)[NT]) {
+    const DJob &j = sd.j;
+    dst = j.dst_off + (int64_t)a * j.dq;
+#pragma unroll
+    for (int t = 0; t < NT; t++) src[t] = sd.t[t].src_off + (int64_t)a * sd.t[t].sq;
+    for (int o = j.nout - 1; o >= 0; o--) {
+        const uint32_t e = (uint32_t)j.oext[o];
+        const uint32_t q = p / e;
+        const uint32_t dig = p - q * e;
+        p = q;
+        dst += (int64_t)dig * j.odst[o];
+#pragma unroll
+        for (int t = 0; t < NT; t++) src[t] += (int64_t)dig * sd.t[t].osrc[o];
+    }
+}
+
+// Row mode: warp item v = (plane, chunk of ra rows, segment of seg columns),
+// ordered with the segment fastest; bases advanced to the item's first
+// element, extents in na (rows) and nb (columns).
+template<int NT>
+__device__ __forceinline__ void item_bases(const UnitDesc<NT> &sd, uint32_t v, int64_t &dst,
+                                           int64_t (&src)[NT], int &na, int &nb) {
+    const DJob &j = sd.j;
+    const uint32_t h = v % (uint32_t)j.nseg;
+    v /= (uint32_t)j.nseg;
+    const uint32_t rc = v % (uint32_t)j.nra;
+    const uint32_t p = v / (uint32_t)j.nra;
+    const int a0 = (int)rc * j.ra, c0 = (int)h * j.seg;
+    na = min(j.ra, j.A - a0);
+    nb = min(j.seg, j.B - c0);
+    plane_row_bases<NT>(sd, p, (uint32_t)a0, dst, src);
+    dst += c0;
+#pragma unroll
+    for (int t = 0; t < NT; t++) src[t] += (int64_t)c0 * sd.t[t].sb;
+}
+
+// Tiled mode: tile v -> plane, first row and column, extents; bases at the
+// tile's first row (column 0).
+template<int NT>
+__device__ __forceinline__ void tile_bases(const UnitDesc<NT> &sd, uint32_t v, int64_t &dst,
+                                           int64_t (&src)[NT], int &b0, int &na, int &nb) {
+    const DJob &j = sd.j;
+    const uint32_t tb = v % (uint32_t)j.ntb;
+    v /= (uint32_t)j.ntb;
+    const uint32_t ta = v % (uint32_t)j.nta;
+    const uint32_t p = v / (uint32_t)j.nta;
+    const int ta_ext = (j.A + j.nta - 1) / j.nta, tb_ext = (j.B + j.ntb - 1) / j.ntb;
+    const int a0 = (int)ta * ta_ext;
+    b0 = (int)tb * tb_ext;
+    na = min(ta_ext, j.A - a0);
+    nb = min(tb_ext, j.B - b0);
+    plane_row_bases<NT>(sd, p, (uint32_t)a0, dst, src);
+}
+
+// Copy / add: dst = sum_t c_t src_t  or  dst += beta * sum_t c_t src_t, terms
+// summed in their order.
+template<int NT>
 __global__ void __launch_bounds__(kThreads)
 transfer_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
                 const DUnit *__restrict__ units, int32_t nunits,
                 const double *const *__restrict__ srcs, double *__restrict__ dst,
                 int32_t accumulate, double beta) {
+    constexpr int RU = CellUnroll<NT>::value;
+    __shared__ UnitDesc<NT> sd;
+    extern __shared__ double tiles[];             // [max_tiles][kTile][kTileLd]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const DUnit un = units[u];
-        const DJob &j = jobs[un.job];
-        const int inner = j.inner;
-        int tin = kThreads;
-        while (tin / 2 >= inner && tin > 1) tin >>= 1;
-        const int rows_per_pass = kThreads / tin;
-        const int i0 = threadIdx.x % tin;
-        for (int64_t r = un.row_begin + threadIdx.x / tin; r < un.row_end; r += rows_per_pass) {
-            int64_t sb[kMaxTerms];
-            for (int t = 0; t < j.nterms; t++)
-                sb[t] = terms[j.term0 + t].src_off +
-                        outer_base(r, j.ndim - 1, j.ext, terms[j.term0 + t].sstr);
-            double *d = dst + j.dst_off + r * inner;
-            for (int i = i0; i < inner; i += tin) {
-                double v = 0.0;
-                for (int t = 0; t < j.nterms; t++) {
-                    const DTerm &tm = terms[j.term0 + t];
-                    v += tm.coeff * srcs[tm.src][sb[t] + (int64_t)i * tm.sstr[j.ndim - 1]];
+        stage_unit<NT>(jobs, terms, un.job, sd);
+        const int nt = sd.j.nterms;
+        const double *sp[NT];
+        double cf[NT];
+        int32_t sb[NT], sq[NT], ts[NT];
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            sp[t] = t < nt ? srcs[sd.t[t].src] : nullptr;
+            cf[t] = t < nt ? sd.t[t].coeff : 0.0;
+            sb[t] = t < nt ? sd.t[t].sb : 0;
+            sq[t] = t < nt ? sd.t[t].sq : 0;
+            ts[t] = t < nt ? sd.t[t].tslot : -1;
+        }
+        if (sd.j.tiled) {
+            for (int64_t v = un.row_begin; v < un.row_end; v++) {
+                int64_t db, sbase[NT];
+                int b0, na, nb;
+                tile_bases<NT>(sd, (uint32_t)v, db, sbase, b0, na, nb);
+                // transposing terms: coalesced along the rows into shared memory
+                const int nel = na * nb;
+#pragma unroll
+                for (int t = 0; t < NT; t++) {
+                    if (t >= nt) break;
+                    if (ts[t] < 0) continue;
+                    double *T = tiles + ts[t] * kTileElems;
+#pragma unroll 4
+                    for (int i = threadIdx.x; i < nel; i += kThreads) {
+                        const int b = i / na, a = i - b * na;      // rows fastest: coalesced source
+                        T[b * kTileLd + a] = sp[t][sbase[t] + (int64_t)a * sq[t] + (int64_t)(b0 + b) * sb[t]];
+                    }
                 }
-                if (accumulate) d[i] = d[i] + beta * v;
-                else d[i] = v;
+                __syncthreads();
+#pragma unroll 4
+                for (int i = threadIdx.x; i < nel; i += kThreads) {
+                    const int a = i / nb, b = i - a * nb;          // columns fastest: coalesced destination
+                    {
+                        double val = 0.0;
+#pragma unroll
+                        for (int t = 0; t < NT; t++) {
+                            if (t >= nt) break;
+                            const double x = ts[t] >= 0 ? tiles[ts[t] * kTileElems + b * kTileLd + a]
+                                                        : sp[t][sbase[t] + (int64_t)a * sq[t] + (int64_t)(b0 + b) * sb[t]];
+                            val += cf[t] * x;
+                        }
+                        double *d = dst + db + (int64_t)a * sd.j.dq + b0 + b;
+                        if (accumulate) *d = *d + beta * val;
+                        else *d = val;
+                    }
+                }
+                __syncthreads();
+            }
+            continue;
+        }
+        // row mode: each warp walks its items cell by cell, lanes consecutive
+        const int W = sd.j.vec ? 2 : 1;
+        for (int64_t v = un.row_begin + warp; v < un.row_end; v += kWarps) {
+            int64_t db, sbase[NT];
+            int na, nb;
+            item_bases<NT>(sd, (uint32_t)v, db, sbase, na, nb);
+            const int ncell = nb / W, ncells = na * ncell;
+            const int drow = 32 / ncell, dcol = 32 - drow * ncell;
+            int row = lane / ncell, col = lane - row * ncell;
+            for (int e0 = 0; e0 < ncells; e0 += 32 * RU) {
+                int rr[RU], cc[RU];
+                bool ok[RU];
+#pragma unroll
+                for (int k = 0; k < RU; k++) {
+                    ok[k] = e0 + k * 32 + lane < ncells;
+                    rr[k] = row;
+                    cc[k] = col;
+                    row += drow;
+                    col += dcol;
+                    if (col >= ncell) { col -= ncell; row++; }
+                }
+                if (W == 2) {
+                    double2 val[RU];
+#pragma unroll
+                    for (int k = 0; k < RU; k++) val[k] = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int t = 0; t < NT; t++) {
+                        if (t >= nt) break;
+#pragma unroll
+                        for (int k = 0; k < RU; k++) {
+                            if (!ok[k]) continue;
+                            const double2 x = *reinterpret_cast<const double2 *>(
+                                sp[t] + sbase[t] + (int64_t)rr[k] * sq[t] + 2 * cc[k]);
+                            val[k].x += cf[t] * x.x;
+                            val[k].y += cf[t] * x.y;
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < RU; k++) {
+                        if (!ok[k]) continue;
+                        double2 *d = reinterpret_cast<double2 *>(dst + db + (int64_t)rr[k] * sd.j.dq + 2 * cc[k]);
+                        if (accumulate) {
+                            double2 o = *d;
+                            o.x = o.x + beta * val[k].x;
+                            o.y = o.y + beta * val[k].y;
+                            *d = o;
+                        } else {
+                            *d = val[k];
+                        }
+                    }
+                } else {
+                    double val[RU];
+#pragma unroll
+                    for (int k = 0; k < RU; k++) val[k] = 0.0;
+#pragma unroll
+                    for (int t = 0; t < NT; t++) {
+                        if (t >= nt) break;
+#pragma unroll
+                        for (int k = 0; k < RU; k++)
+                            if (ok[k]) val[k] += cf[t] * sp[t][sbase[t] + (int64_t)rr[k] * sq[t] + (int64_t)cc[k] * sb[t]];
+                    }
+#pragma unroll
+                    for (int k = 0; k < RU; k++) {
+                        if (!ok[k]) continue;
+                        double *d = dst + db + (int64_t)rr[k] * sd.j.dq + cc[k];
+                        if (accumulate) *d = *d + beta * val[k];
+                        else *d = val[k];
+                    }
+                }
             }
         }
     }
 }
 
-// Dot product: per unit partial sum, then one fixed-order reduction.
+// Dot product: one partial sum per unit (term 0 carries the orbit weight and
+// both transform signs), then one fixed-order reduction.
 __global__ void __launch_bounds__(kThreads)
 dot_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
            const DUnit *__restrict__ units, int32_t nunits,
            const double *__restrict__ a, const double *__restrict__ b,
            double *__restrict__ partials) {
+    constexpr int RU = CellUnroll<2>::value;
+    __shared__ UnitDesc<2> sd;
     __shared__ double red[kThreads];
+    extern __shared__ double tiles[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const DUnit un = units[u];
-        const DJob &j = jobs[un.job];
-        const DTerm &ta = terms[j.term0], &tb = terms[j.term0 + 1];
-        const int inner = j.inner;
-        int tin = kThreads;
-        while (tin / 2 >= inner && tin > 1) tin >>= 1;
-        const int rows_per_pass = kThreads / tin;
-        const int i0 = threadIdx.x % tin;
+        stage_unit<2>(jobs, terms, un.job, sd);
+        const double *sp[2] = {sd.t[0].src == 0 ? a : b, sd.t[1].src == 0 ? a : b};
+        const int32_t sb[2] = {sd.t[0].sb, sd.t[1].sb}, sq[2] = {sd.t[0].sq, sd.t[1].sq};
+        const int32_t ts[2] = {sd.t[0].tslot, sd.t[1].tslot};
         double s = 0.0;
-        for (int64_t r = un.row_begin + threadIdx.x / tin; r < un.row_end; r += rows_per_pass) {
-            int64_t oa = ta.src_off + outer_base(r, j.ndim - 1, j.ext, ta.sstr);
-            int64_t ob = tb.src_off + outer_base(r, j.ndim - 1, j.ext, tb.sstr);
-            const int64_t sa = ta.sstr[j.ndim - 1], sbb = tb.sstr[j.ndim - 1];
-            for (int i = i0; i < inner; i += tin) s += a[oa + i * sa] * b[ob + i * sbb];
+        if (sd.j.tiled) {
+            for (int64_t v = un.row_begin; v < un.row_end; v++) {
+                int64_t db, sbase[2];
+                int b0, na, nb;
+                tile_bases<2>(sd, (uint32_t)v, db, sbase, b0, na, nb);
+                const int nel = na * nb;
+#pragma unroll
+                for (int t = 0; t < 2; t++) {
+                    if (ts[t] < 0) continue;
+                    double *T = tiles + ts[t] * kTileElems;
+#pragma unroll 4
+                    for (int i = threadIdx.x; i < nel; i += kThreads) {
+                        const int bb = i / na, aa = i - bb * na;
+                        T[bb * kTileLd + aa] = sp[t][sbase[t] + (int64_t)aa * sq[t] + (int64_t)(b0 + bb) * sb[t]];
+                    }
+                }
+                __syncthreads();
+#pragma unroll 4
+                for (int i = threadIdx.x; i < nel; i += kThreads) {
+                    const int aa = i / nb, bb = i - aa * nb;
+                    {
+                        double x[2];
+#pragma unroll
+                        for (int t = 0; t < 2; t++)
+                            x[t] = ts[t] >= 0 ? tiles[ts[t] * kTileElems + bb * kTileLd + aa]
+                                              : sp[t][sbase[t] + (int64_t)aa * sq[t] + (int64_t)(b0 + bb) * sb[t]];
+                        s += x[0] * x[1];
+                    }
+                }
+                __syncthreads();
+            }
+        } else {
+            const int W = sd.j.vec ? 2 : 1;
+            for (int64_t v = un.row_begin + warp; v < un.row_end; v += kWarps) {
+                int64_t db, sbase[2];
+                int na, nb;
+                item_bases<2>(sd, (uint32_t)v, db, sbase, na, nb);
+                const int ncell = nb / W, ncells = na * ncell;
+                const int drow = 32 / ncell, dcol = 32 - drow * ncell;
+                int row = lane / ncell, col = lane - row * ncell;
+                for (int e0 = 0; e0 < ncells; e0 += 32 * RU) {
+                    int rr[RU], cc[RU];
+                    bool ok[RU];
+#pragma unroll
+                    for (int k = 0; k < RU; k++) {
+                        ok[k] = e0 + k * 32 + lane < ncells;
+                        rr[k] = row;
+                        cc[k] = col;
+                        row += drow;
+                        col += dcol;
+                        if (col >= ncell) { col -= ncell; row++; }
+                    }
+                    if (W == 2) {
+#pragma unroll
+                        for (int k = 0; k < RU; k++) {
+                            if (!ok[k]) continue;
+                            const double2 x = *reinterpret_cast<const double2 *>(
+                                sp[0] + sbase[0] + (int64_t)rr[k] * sq[0] + 2 * cc[k]);
+                            const double2 y = *reinterpret_cast<const double2 *>(
+                                sp[1] + sbase[1] + (int64_t)rr[k] * sq[1] + 2 * cc[k]);
+                            s += x.x * y.x;
+                            s += x.y * y.y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < RU; k++)
+                            if (ok[k])
+                                s += sp[0][sbase[0] + (int64_t)rr[k] * sq[0] + (int64_t)cc[k] * sb[0]] *
+                                     sp[1][sbase[1] + (int64_t)rr[k] * sq[1] + (int64_t)cc[k] * sb[1]];
+                    }
+                }
+            }
         }
         red[threadIdx.x] = s;
         __syncthreads();
@@ -96,8 +351,7 @@ dot_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
             if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
             __syncthreads();
         }
-        if (threadIdx.x == 0) partials[u] = red[0] * ta.coeff;
-        __syncthreads();
+        if (threadIdx.x == 0) partials[u] = red[0] * sd.t[0].coeff;
     }
 }
 
@@ -183,20 +437,40 @@ int grid_for(int64_t units) {
 
 }  // namespace
 
-cudaError_t launch_transfer(const DJob *jobs, const DTerm *terms, const DUnit *units,
-                            int32_t nunits, const double *const *srcs, double *dst,
-                            int32_t accumulate, double beta, cudaStream_t s) {
-    if (nunits <= 0) return cudaSuccess;
-    transfer_kernel<<<grid_for(nunits), kThreads, 0, s>>>(jobs, terms, units, nunits, srcs, dst,
-                                                          accumulate, beta);
+template<int NT>
+cudaError_t launch_transfer_nt(const DJob *jobs, const DTerm *terms, const DUnit *units, int32_t nunits,
+                               size_t smem, const double *const *srcs, double *dst, int32_t accumulate,
+                               double beta, cudaStream_t s) {
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(transfer_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    transfer_kernel<NT><<<grid_for(nunits), kThreads, smem, s>>>(jobs, terms, units, nunits, srcs, dst,
+                                                                 accumulate, beta);
     return cudaGetLastError();
 }
 
+cudaError_t launch_transfer(const DJob *jobs, const DTerm *terms, const DUnit *units,
+                            int32_t nunits, int32_t max_terms, int32_t max_tiles,
+                            const double *const *srcs, double *dst, int32_t accumulate, double beta,
+                            cudaStream_t s) {
+    if (nunits <= 0) return cudaSuccess;
+    const size_t smem = (size_t)max_tiles * kTileElems * sizeof(double);
+    if (max_terms <= 1) return launch_transfer_nt<1>(jobs, terms, units, nunits, smem, srcs, dst, accumulate, beta, s);
+    if (max_terms <= 2) return launch_transfer_nt<2>(jobs, terms, units, nunits, smem, srcs, dst, accumulate, beta, s);
+    if (max_terms <= 4) return launch_transfer_nt<4>(jobs, terms, units, nunits, smem, srcs, dst, accumulate, beta, s);
+    if (max_terms <= kMaxTerms)
+        return launch_transfer_nt<kMaxTerms>(jobs, terms, units, nunits, smem, srcs, dst, accumulate, beta, s);
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_dot(const DJob *jobs, const DTerm *terms, const DUnit *units,
-                       int32_t nunits, const double *a, const double *b, double *partials,
-                       double *out, cudaStream_t s) {
+                       int32_t nunits, int32_t max_tiles, const double *a, const double *b,
+                       double *partials, double *out, cudaStream_t s) {
     if (nunits <= 0) return cudaMemsetAsync(out, 0, sizeof(double), s);
-    dot_kernel<<<grid_for(nunits), kThreads, 0, s>>>(jobs, terms, units, nunits, a, b, partials);
+    const size_t smem = (size_t)max_tiles * kTileElems * sizeof(double);
+    dot_kernel<<<grid_for(nunits), kThreads, smem, s>>>(jobs, terms, units, nunits, a, b, partials);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     reduce_kernel<<<1, kThreads, 0, s>>>(partials, nunits, out);

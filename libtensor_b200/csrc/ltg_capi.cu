@@ -92,6 +92,16 @@ namespace ltg {
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 }
 
+// Per-kernel device timing: an event pair around every launch while enabled
+// (outside graph capture), summed on request.
+struct KernelTiming {
+    bool enabled = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> pending;
+    double ms[LTG_KERNEL_KINDS] = {};
+    int64_t count[LTG_KERNEL_KINDS] = {};
+};
+
 struct ltg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -101,6 +111,7 @@ struct ltg_ctx {
     int nsm = 148;
     DevBuf scratch_counter;      // work-queue counters of persistent launches
     DevBuf dot_out;              // device scalar for synchronous dot products
+    KernelTiming timing;
 };
 
 static std::atomic<uint64_t> g_bt_uid{1};
@@ -252,6 +263,52 @@ void parse_spec(const ltg_bt_spec *s, BlockTensorHost &h) {
 
 void need_dev(const ltg_ctx *c) {
     if (c->device < 0) throw error(kErrState, "host-only context has no device");
+}
+
+cudaEvent_t timing_event(ltg_ctx *c) {
+    if (!c->timing.pool.empty()) {
+        cudaEvent_t e = c->timing.pool.back();
+        c->timing.pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    LTG_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+// Brackets the launches of one kernel kind with events when timing is on.
+struct TimedLaunch {
+    ltg_ctx *ctx;
+    int kind;
+    cudaEvent_t e0 = nullptr;
+    TimedLaunch(ltg_ctx *c, int k) : ctx(c), kind(k) {
+        if (c->timing.enabled && !c->capturing) {
+            e0 = timing_event(c);
+            LTG_CUDA(cudaEventRecord(e0, c->stream));
+        }
+    }
+    void done() {
+        if (!e0) return;
+        cudaEvent_t e1 = timing_event(ctx);
+        LTG_CUDA(cudaEventRecord(e1, ctx->stream));
+        ctx->timing.pending.emplace_back(kind, e0, e1);
+        e0 = nullptr;
+    }
+    ~TimedLaunch() { if (e0) ctx->timing.pool.push_back(e0); }
+};
+
+void collect_timing(ltg_ctx *c) {
+    if (c->timing.pending.empty()) return;
+    LTG_CUDA(cudaStreamSynchronize(c->stream));
+    for (auto &p : c->timing.pending) {
+        float ms = 0.f;
+        LTG_CUDA(cudaEventElapsedTime(&ms, std::get<1>(p), std::get<2>(p)));
+        c->timing.ms[std::get<0>(p)] += ms;
+        c->timing.count[std::get<0>(p)]++;
+        c->timing.pool.push_back(std::get<1>(p));
+        c->timing.pool.push_back(std::get<2>(p));
+    }
+    c->timing.pending.clear();
 }
 
 void alloc_arena(ltg_bt *bt) {
@@ -595,9 +652,117 @@ void validate_transfer(const TransferPlan &plan, const std::vector<int64_t> &src
 // Cached copy/add plans: the first call for a given (operands, permutations,
 // coefficients, destination, mode) builds and uploads the task arrays; later
 // calls, including calls inside a CUDA-graph capture, only launch.
+// Device form of a transfer plan: every job seen as planes of A rows x B
+// columns (DJob).  Jobs whose terms all read the columns with unit stride run
+// in row mode (warp items of about kItemElems elements: row chunks x column
+// segments); a job
+// with a transposing term runs in tiled mode, tiles of at most 64x64 whose
+// transposing terms are staged through shared memory.  Units hold about
+// kTransferUnitElems elements.
+struct DeviceTransfer {
+    std::vector<DJob> jobs;
+    std::vector<DTerm> terms;
+    std::vector<DUnit> units;
+    int32_t max_terms = 0, max_tiles = 0;
+};
+constexpr int64_t kTransferUnitElems = 32768;
+constexpr int32_t kItemElems = 4096;       // row mode: elements per warp item (about)
+constexpr int32_t kTileSide = 64;          // largest tile side (elements)
+
+DeviceTransfer device_transfer(const TransferPlan &plan) {
+    DeviceTransfer o;
+    for (const TJob &j : plan.jobs) {
+        const int n = j.ndim, L = n - 1;
+        const TTerm *T = plan.terms.data() + j.term0;
+        // Row dim q: the destination dim that is contiguous in the first
+        // source whose innermost stride is not 1 (a transposition), else the
+        // next-to-innermost dim.
+        int q = -1;
+        bool transposing = false;
+        if (n >= 2) {
+            q = L - 1;
+            for (int t = 0; t < j.nterms; t++) {
+                if (T[t].sstr[L] == 1) continue;
+                transposing = true;
+                for (int d = 0; d < L; d++)
+                    if (T[t].sstr[d] == 1) { q = d; break; }
+                break;
+            }
+        }
+        int64_t dstr[kMaxOrder];
+        int64_t acc = 1;
+        for (int d = n - 1; d >= 0; d--) { dstr[d] = acc; acc *= j.ext[d]; }
+        DJob dj{};
+        dj.dst_off = j.dst_off;
+        dj.nterms = j.nterms;
+        dj.term0 = (int32_t)o.terms.size();
+        dj.A = q >= 0 ? j.ext[q] : 1;
+        dj.B = j.ext[L];
+        dj.dq = q >= 0 ? (int32_t)dstr[q] : 0;
+        for (int d = 0; d < L; d++) {
+            if (d == q) continue;
+            dj.oext[dj.nout] = j.ext[d];
+            dj.odst[dj.nout] = (int32_t)dstr[d];
+            dj.nout++;
+        }
+        dj.tiled = transposing ? 1 : 0;
+        dj.seg = dj.B > kItemElems ? kItemElems : dj.B;
+        dj.nseg = (dj.B + dj.seg - 1) / dj.seg;
+        dj.ra = std::max<int32_t>(1, std::min<int32_t>(dj.A, kItemElems / dj.seg));
+        dj.nra = (dj.A + dj.ra - 1) / dj.ra;
+        bool vec = !transposing && dj.seg % 2 == 0 && dj.B % 2 == 0 && dj.dst_off % 2 == 0 && dj.dq % 2 == 0;
+        for (int k = 0; k < dj.nout; k++) vec = vec && dj.odst[k] % 2 == 0;
+        int32_t ntiles = 0;
+        for (int t = 0; t < j.nterms; t++) {
+            DTerm dt{};
+            dt.src_off = T[t].src_off;
+            dt.coeff = T[t].coeff;
+            dt.src = T[t].src;
+            dt.sq = q >= 0 ? T[t].sstr[q] : 0;
+            dt.sb = T[t].sstr[L];
+            dt.tslot = transposing && dt.sb != 1 ? ntiles++ : -1;
+            int k = 0;
+            for (int d = 0; d < L; d++)
+                if (d != q) dt.osrc[k++] = T[t].sstr[d];
+            vec = vec && dt.sb == 1 && dt.src_off % 2 == 0 && dt.sq % 2 == 0;
+            for (int kk = 0; kk < dj.nout; kk++) vec = vec && dt.osrc[kk] % 2 == 0;
+            o.terms.push_back(dt);
+        }
+        dj.vec = vec ? 1 : 0;
+        dj.nta = (dj.A + kTileSide - 1) / kTileSide;
+        dj.ntb = (dj.B + kTileSide - 1) / kTileSide;
+        o.max_terms = std::max(o.max_terms, j.nterms);
+        o.max_tiles = std::max(o.max_tiles, ntiles);
+        const int32_t ji = (int32_t)o.jobs.size();
+        o.jobs.push_back(dj);
+        int64_t planes = 1;
+        for (int k = 0; k < dj.nout; k++) planes *= dj.oext[k];
+        if (planes * dj.A * (int64_t)dj.B >= (int64_t(1) << 31))
+            throw error(kErrUnsupported, "block too large for one transfer job");
+        int64_t items, per_unit;
+        if (dj.tiled) {
+            items = planes * dj.nta * dj.ntb;
+            const int64_t tile = (int64_t)((dj.A + dj.nta - 1) / dj.nta) * ((dj.B + dj.ntb - 1) / dj.ntb);
+            per_unit = std::max<int64_t>(1, kTransferUnitElems / tile);
+        } else {
+            items = planes * dj.nra * dj.nseg;
+            const int64_t item = (int64_t)dj.ra * dj.seg;
+            per_unit = std::max<int64_t>(8, (kTransferUnitElems / item + 7) / 8 * 8);
+        }
+        for (int64_t r = 0; r < items; r += per_unit) {
+            DUnit u{};
+            u.job = ji;
+            u.row_begin = r;
+            u.row_end = std::min(items, r + per_unit);
+            o.units.push_back(u);
+        }
+    }
+    return o;
+}
+
 struct TransferExec {
     DevBuf jobs, terms, units, srcs;
-    int32_t nunits = 0;
+    int32_t nunits = 0, max_terms = 0, max_tiles = 0;
     std::vector<char> dst_nonzero;
 };
 typedef std::tuple<std::vector<const ltg_bt *>, std::vector<int8_t>, std::vector<double>,
@@ -605,9 +770,6 @@ typedef std::tuple<std::vector<const ltg_bt *>, std::vector<int8_t>, std::vector
 std::mutex g_tr_mtx;
 std::map<transfer_key, std::unique_ptr<TransferExec>> g_tr_cache;
 
-static_assert(sizeof(DJob) == sizeof(TJob), "job layout");
-static_assert(sizeof(DTerm) == sizeof(TTerm), "term layout");
-static_assert(sizeof(DUnit) == sizeof(TUnit), "unit layout");
 
 void run_transfer(ltg_ctx *ctx, const std::vector<ltg_bt *> &srcs, const std::vector<Perm> &perms,
                   const std::vector<double> &coeffs, ltg_bt *dst, bool add, double d) {
@@ -639,21 +801,26 @@ void run_transfer(ltg_ctx *ctx, const std::vector<ltg_bt *> &srcs, const std::ve
         for (ltg_bt *b : srcs) ssz.push_back(b->h.total_elems);
         validate_transfer(plan, ssz, dst->h.total_elems);
         std::unique_ptr<TransferExec> nx(new TransferExec());
-        upload_vec(nx->jobs, plan.jobs, s);
-        upload_vec(nx->terms, plan.terms, s);
-        upload_vec(nx->units, plan.units, s);
+        DeviceTransfer dt = device_transfer(plan);
+        upload_vec(nx->jobs, dt.jobs, s);
+        upload_vec(nx->terms, dt.terms, s);
+        upload_vec(nx->units, dt.units, s);
         std::vector<const double *> sp;
         for (ltg_bt *b : srcs) sp.push_back(b->arena.as<double>());
         upload_vec(nx->srcs, sp, s);
-        nx->nunits = (int32_t)plan.units.size();
+        nx->nunits = (int32_t)dt.units.size();
+        nx->max_terms = dt.max_terms;
+        nx->max_tiles = dt.max_tiles;
         nx->dst_nonzero = plan.dst_nonzero;
         ex = nx.get();
         std::lock_guard<std::mutex> lk(g_tr_mtx);
         g_tr_cache[key] = std::move(nx);
     }
+    TimedLaunch tl(ctx, LTG_KERNEL_TRANSFER);
     LTG_CUDA(launch_transfer(ex->jobs.as<DJob>(), ex->terms.as<DTerm>(), ex->units.as<DUnit>(),
-                             ex->nunits, ex->srcs.as<const double *>(), dst->arena.as<double>(),
+                             ex->nunits, ex->max_terms, ex->max_tiles, ex->srcs.as<const double *>(), dst->arena.as<double>(),
                              add ? 1 : 0, d, s));
+    tl.done();
     ctx->launches++;
     for (size_t sl = 0; sl < ex->dst_nonzero.size(); sl++)
         dst->h.nonzero[sl] = add ? (dst->h.nonzero[sl] || ex->dst_nonzero[sl]) : ex->dst_nonzero[sl];
@@ -673,7 +840,7 @@ void forget_transfer(const ltg_bt *t) {
 // only kernel launches.
 struct DotExec {
     DevBuf jobs, terms, units, partials;
-    int32_t nunits = 0;
+    int32_t nunits = 0, max_tiles = 0;
 };
 std::mutex g_dot_mtx;
 std::map<std::tuple<const ltg_bt *, const ltg_bt *, std::vector<int8_t>, std::vector<int8_t>>,
@@ -691,11 +858,13 @@ DotExec *prepare_dot(ltg_bt *a, const Perm &pa, ltg_bt *b, const Perm &pb) {
     validate_transfer(plan, {a->h.total_elems, b->h.total_elems}, -1);
     std::unique_ptr<DotExec> ex(new DotExec());
     cudaStream_t s = a->ctx->stream;
-    upload_vec(ex->jobs, plan.jobs, s);
-    upload_vec(ex->terms, plan.terms, s);
-    upload_vec(ex->units, plan.units, s);
-    ex->partials.alloc(std::max<size_t>(plan.units.size(), 1) * sizeof(double));
-    ex->nunits = (int32_t)plan.units.size();
+    DeviceTransfer dt = device_transfer(plan);
+    upload_vec(ex->jobs, dt.jobs, s);
+    upload_vec(ex->terms, dt.terms, s);
+    upload_vec(ex->units, dt.units, s);
+    ex->partials.alloc(std::max<size_t>(dt.units.size(), 1) * sizeof(double));
+    ex->nunits = (int32_t)dt.units.size();
+    ex->max_tiles = dt.max_tiles;
     DotExec *raw = ex.get();
     g_dot_cache[key] = std::move(ex);
     return raw;
@@ -741,6 +910,11 @@ int ltg_ctx_destroy(ltg_ctx *ctx) {
         check_ctx(ctx);
         if (ctx->device >= 0) {
             cudaStreamSynchronize(ctx->stream);
+            for (auto &p : ctx->timing.pending) {
+                cudaEventDestroy(std::get<1>(p));
+                cudaEventDestroy(std::get<2>(p));
+            }
+            for (cudaEvent_t e : ctx->timing.pool) cudaEventDestroy(e);
             cudaStreamDestroy(ctx->stream);
         }
         delete ctx;
@@ -761,6 +935,27 @@ int ltg_ctx_set_host_threads(ltg_ctx *ctx, int nthreads) {
 
 int ltg_ctx_launch_count(ltg_ctx *ctx, int64_t *count) {
     return guard([&] { check_ctx(ctx); if (!count) throw error(kErrBadArg, "null output"); *count = ctx->launches; });
+}
+
+int ltg_ctx_set_timing(ltg_ctx *ctx, int32_t enable) {
+    return guard([&] {
+        check_ctx(ctx);
+        need_dev(ctx);
+        collect_timing(ctx);
+        ctx->timing.enabled = enable != 0;
+        if (enable)
+            for (int k = 0; k < LTG_KERNEL_KINDS; k++) { ctx->timing.ms[k] = 0.0; ctx->timing.count[k] = 0; }
+    });
+}
+
+int ltg_ctx_kernel_times(ltg_ctx *ctx, double *ms, int64_t *launches) {
+    return guard([&] {
+        check_ctx(ctx);
+        need_dev(ctx);
+        if (!ms || !launches) throw error(kErrBadArg, "null output");
+        collect_timing(ctx);
+        for (int k = 0; k < LTG_KERNEL_KINDS; k++) { ms[k] = ctx->timing.ms[k]; launches[k] = ctx->timing.count[k]; }
+    });
 }
 
 int ltg_bt_create(ltg_ctx *ctx, const ltg_bt_spec *spec, ltg_bt **out) {
@@ -961,9 +1156,11 @@ int ltg_bt_fill_seeded(ltg_bt *bt, uint64_t seed, double scale) {
         need_dev(bt->ctx);
         upload_directory(bt);
         DGenGroup g = gen_group(bt->h);
+        TimedLaunch tl(bt->ctx, LTG_KERNEL_FILL);
         LTG_CUDA(launch_fill_seeded(bt->arena.as<double>(), bt->dir_off.as<int64_t>(), bt->dir_start.as<int64_t>(),
                                     bt->dir_ext.as<int32_t>(), (int32_t)bt->h.blk_abs.size(), bt->h.bis.n, g, seed,
                                     two_m32(scale), bt->ctx->stream));
+        tl.done();
         bt->ctx->launches++;
         LTG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
         std::fill(bt->h.nonzero.begin(), bt->h.nonzero.end(), 1);
@@ -1096,13 +1293,17 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             if (!add)
                 for (auto &r : ox->zero_ranges)
                     LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
+            TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
             LTG_CUDA(launch_oz_split(ox->kind, ox->panels.as<DPanel>(), ox->npanels, ox->max_rows_pad,
                                      plan->a->arena.as<double>(), plan->b->arena.as<double>(),
                                      ox->slices.as<uint8_t>(), ox->exps.as<int32_t>(), ox->S, s));
+            t_split.done();
+            TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
             LTG_CUDA(launch_oz_gemm(ox->kind, ox->panels.as<DPanel>(), ox->slices.as<uint8_t>(), ox->tasks.as<DOzTask>(),
                                     ox->cblks.as<DCBlock>(), ox->items.as<DItem>(), ox->nitems,
                                     ox->exps.as<int32_t>(), c->arena.as<double>(), add, ox->S, ox->chunk_kb,
                                     ox->err.as<int32_t>(), s));
+            t_gemm.done();
             ctx->launches += 2;
             if (!ctx->capturing)
                 LTG_CUDA(cudaMemcpyAsync(ox->err_host, ox->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -1116,11 +1317,13 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                 LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
         int slot = 0;
         for (auto &l : ex->launches) {
+            TimedLaunch tl(ctx, LTG_KERNEL_CONTRACT_FP64);
             LTG_CUDA(launch_contract_fp64(ex->tasks.as<DTask>(), ex->cblks.as<DCBlock>(),
                                           ex->items.as<DItem>() + l.second.first, l.second.second,
                                           ctx->scratch_counter.as<int32_t>() + (slot++ % 64),
                                           plan->a->arena.as<double>(), plan->b->arena.as<double>(),
                                           c->arena.as<double>(), add, l.first, s));
+            tl.done();
             ctx->launches++;
         }
         if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
@@ -1249,9 +1452,11 @@ int ltg_dotprod_async(ltg_bt *a, const int32_t *perma, ltg_bt *b, const int32_t 
         need_dev(a->ctx); check_bt(b);
         if (a->ctx != b->ctx) throw error(kErrBadArg, "operands belong to different contexts");
         DotExec *ex = prepare_dot(a, perm_from(a->h.bis.n, perma), b, perm_from(b->h.bis.n, permb));
+        TimedLaunch tl(a->ctx, LTG_KERNEL_DOT);
         LTG_CUDA(launch_dot(ex->jobs.as<DJob>(), ex->terms.as<DTerm>(), ex->units.as<DUnit>(), ex->nunits,
-                            a->arena.as<double>(), b->arena.as<double>(), ex->partials.as<double>(), dev_out,
+                            ex->max_tiles, a->arena.as<double>(), b->arena.as<double>(), ex->partials.as<double>(), dev_out,
                             a->ctx->stream));
+        tl.done();
         a->ctx->launches += 2;
     });
 }
@@ -1270,7 +1475,9 @@ int ltg_scale(ltg_bt *a, double c) {
     return guard([&] {
         check_bt(a);
         need_dev(a->ctx);
+        TimedLaunch tl(a->ctx, LTG_KERNEL_SCALE);
         LTG_CUDA(launch_scale(a->arena.as<double>(), a->h.total_elems, c, a->ctx->stream));
+        tl.done();
         a->ctx->launches++;
     });
 }
@@ -1289,9 +1496,11 @@ int ltg_denominator(ltg_bt *a, const double *eps_host, int32_t nocc) {
         DevBuf de, doff;
         upload_vec(de, eps, a->ctx->stream);
         upload_vec(doff, off, a->ctx->stream);
+        TimedLaunch tl(a->ctx, LTG_KERNEL_DENOMINATOR);
         LTG_CUDA(launch_denominator(a->arena.as<double>(), a->dir_off.as<int64_t>(), a->dir_start.as<int64_t>(),
                                     a->dir_ext.as<int32_t>(), (int32_t)a->h.blk_abs.size(), de.as<double>(),
                                     doff.as<int64_t>(), nocc, a->ctx->stream));
+        tl.done();
         a->ctx->launches++;
         LTG_CUDA(cudaStreamSynchronize(a->ctx->stream));
     });

@@ -74,24 +74,37 @@ struct DOzTask {
 constexpr int kMaxTerms = 8;
 
 // One destination block of a copy/add (or one A/B block pair of a dot
-// product): extents of the destination dims and, per term, the source offset
-// and the source stride of every destination dim.
+// product), seen as planes of A rows x B columns: the columns are the
+// innermost destination dim, the rows dim q (the destination dim that is
+// contiguous in a transposing source, else the next-to-innermost dim), and
+// every other dim is an outer dim enumerating the planes.  Row r of the job
+// is plane r / A, row r % A.
 struct DJob {
     int64_t dst_off;
-    int32_t ndim, inner;          // inner = ext[ndim-1]
     int32_t nterms, term0;        // terms[term0 .. term0+nterms)
-    int32_t ext[kDevMaxOrder];
+    int32_t A, B;                 // rows per plane (extent of dim q), columns
+    int32_t dq;                   // destination stride of dim q
+    int32_t nout;                 // outer dims, outermost first
+    int32_t oext[kDevMaxOrder - 2], odst[kDevMaxOrder - 2];
+    int32_t vec;                  // 16-byte accesses valid for every term
+    int32_t seg, nseg;            // row mode: columns per item, column segments per row
+    int32_t ra, nra;              // row mode: rows per item, row chunks per plane
+    int32_t tiled;                // 1: 32x32 tiles staged through shared memory
+    int32_t nta, ntb;             // tiled mode: tiles along the rows and the columns
 };
 
 struct DTerm {
     int64_t src_off;
     double coeff;
     int32_t src;                  // source tensor index
-    int32_t pad;
-    int32_t sstr[kDevMaxOrder];
+    int32_t sq, sb;               // source strides of dim q and of the columns
+    int32_t tslot;                // tiled mode: shared-memory tile of this term, -1: read directly
+    int32_t osrc[kDevMaxOrder - 2];   // source strides of the outer dims
 };
 
-// A contiguous row range of one job processed by one CTA.
+// A range [row_begin, row_end) of one job's work items processed by one CTA:
+// warp items ((plane * nra + chunk) * nseg + segment) in row mode, tiles
+// ((plane * nta + ta) * ntb + tb) in tiled mode.
 struct DUnit {
     int32_t job;
     int32_t pad;
@@ -168,13 +181,14 @@ cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices
 // per 64-byte k block, bound of one slice product.
 void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod);
 
-// Element-wise transfer kernels.
+// Element-wise transfer kernels.  max_terms bounds nterms and max_tiles the
+// shared-memory tiles (transposing terms) of any job.
 cudaError_t launch_transfer(const DJob *jobs, const DTerm *terms, const DUnit *units,
-    int32_t nunits, const double *const *srcs, double *dst, int32_t accumulate,
-    double beta, cudaStream_t s);
+    int32_t nunits, int32_t max_terms, int32_t max_tiles, const double *const *srcs, double *dst,
+    int32_t accumulate, double beta, cudaStream_t s);
 cudaError_t launch_dot(const DJob *jobs, const DTerm *terms, const DUnit *units,
-    int32_t nunits, const double *a, const double *b, double *partials, double *out,
-    cudaStream_t s);
+    int32_t nunits, int32_t max_tiles, const double *a, const double *b, double *partials,
+    double *out, cudaStream_t s);
 cudaError_t launch_scale(double *x, int64_t n, double c, cudaStream_t s);
 cudaError_t launch_fill_seeded(double *arena, const int64_t *blk_off,
     const int64_t *blk_start, const int32_t *blk_ext, int32_t nblk, int32_t order,

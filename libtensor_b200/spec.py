@@ -185,6 +185,15 @@ class LadderConfig:
                       perms=antisym_pairs(4, [(0, 1), (2, 3)]), part_pdims=[2, 2, 2, 2],
                       part_forbidden=spin_forbidden([((0, 1), (2, 3))], 4))
 
+    def x_spec(self) -> BTSpec:
+        """An (o,o,v,v) intermediate before antisymmetrisation: spin blocks
+        only, no permutational symmetry (the input of P(ij)P(ab) in a CC
+        residual)."""
+        so, sv = spin_splits(self.occ_blocks), spin_splits(self.vir_blocks)
+        return BTSpec(dims=[self.o, self.o, self.v, self.v], splits=[so, so, sv, sv],
+                      part_pdims=[2, 2, 2, 2],
+                      part_forbidden=spin_forbidden([((0, 1), (2, 3))], 4))
+
     # contraction2<2,2,2>: contract t.2 with V.2 and t.3 with V.3
     contraction = dict(n=2, m=2, k=2, permc=None, pairs=[(2, 2), (3, 3)])
     kc = 0.5
