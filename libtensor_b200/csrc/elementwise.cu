@@ -41,9 +41,18 @@ struct UnitDesc {
     DTerm t[NT];
 };
 
-constexpr int kTile = 64;                 // tiled mode: at most kTile x kTile elements
-constexpr int kTileLd = kTile + 1;        // padded shared-memory row
-constexpr int kTileElems = kTile * kTileLd;
+// 8-byte asynchronous global -> shared copy (LDGSTS) and the wait for all of
+// this thread's outstanding copies.
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async16(double *smem, const double *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 
 template<int NT>
 __device__ __forceinline__ void stage_unit(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
@@ -112,6 +121,82 @@ __device__ __forceinline__ void tile_bases(const UnitDesc<NT> &sd, uint32_t v, i
     plane_row_bases<NT>(sd, p, (uint32_t)a0, dst, src);
 }
 
+// Tiled mode: per-term constants of the current unit, in registers.
+template<int NT>
+struct TileTerms {
+    const double *src[NT];
+    int32_t sq[NT], sb[NT], mode[NT], off[NT], ld[NT], vec[NT];
+};
+
+template<int NT>
+__device__ __forceinline__ void load_tile_terms(const UnitDesc<NT> &sd, const double *const *srcs,
+                                                TileTerms<NT> &tt) {
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+        const bool on = t < sd.j.nterms;
+        tt.src[t] = on ? srcs[sd.t[t].src] : nullptr;
+        tt.sq[t] = on ? sd.t[t].sq : 0;
+        tt.sb[t] = on ? sd.t[t].sb : 0;
+        tt.mode[t] = on ? sd.t[t].tmode : 0;
+        tt.off[t] = on ? sd.t[t].toff : 0;
+        tt.ld[t] = on ? sd.t[t].tld : 0;
+        tt.vec[t] = on ? sd.t[t].tvec : 0;
+    }
+}
+
+// Copies every term's tile into shared memory, each along its own contiguous
+// direction (columns for layout 0, rows for layout 1; 16-byte copies where
+// the term allows), so that all loads of the tile are in flight at once.
+// Offsets inside a tile fit 32 bits (a block holds < 2^31 elements).
+template<int NT, int THREADS>
+__device__ __forceinline__ void stage_tile(int nt, const TileTerms<NT> &tt, const int64_t (&sbase)[NT],
+                                           int b0, int na, int nb, double *tiles) {
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+        if (t >= nt) break;
+        double *T = tiles + tt.off[t];
+        const double *src = tt.src[t] + sbase[t] + (int64_t)b0 * tt.sb[t];
+        const int sq = tt.sq[t], sb = tt.sb[t], ld = tt.ld[t];
+        if (tt.mode[t] == 0) {
+            if (tt.vec[t]) {
+                const int ncp = nb >> 1, nel = na * ncp;
+                const int da = THREADS / ncp, dc = THREADS - da * ncp;
+                int a = threadIdx.x / ncp, c = threadIdx.x - a * ncp;
+                for (int i = threadIdx.x; i < nel; i += THREADS) {
+                    cp_async16(T + a * ld + 2 * c, src + (a * sq + 2 * c));
+                    a += da; c += dc;
+                    if (c >= ncp) { c -= ncp; a++; }
+                }
+            } else {
+                const int nel = na * nb;
+                const int da = THREADS / nb, dc = THREADS - da * nb;
+                int a = threadIdx.x / nb, c = threadIdx.x - a * nb;
+                for (int i = threadIdx.x; i < nel; i += THREADS) {
+                    cp_async8(T + a * ld + c, src + (a * sq + c * sb));
+                    a += da; c += dc;
+                    if (c >= nb) { c -= nb; a++; }
+                }
+            }
+        } else {
+            const int nel = na * nb;
+            const int dc = THREADS / na, da = THREADS - dc * na;
+            int c = threadIdx.x / na, a = threadIdx.x - c * na;
+            for (int i = threadIdx.x; i < nel; i += THREADS) {
+                cp_async8(T + c * ld + a, src + (a * sq + c * sb));
+                c += dc; a += da;
+                if (a >= na) { a -= na; c++; }
+            }
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+}
+
+template<int NT>
+__device__ __forceinline__ double tile_at(const double *tiles, const TileTerms<NT> &tt, int t, int a, int c) {
+    return tiles[tt.off[t] + (tt.mode[t] == 0 ? a * tt.ld[t] + c : c * tt.ld[t] + a)];
+}
+
 // Copy / add: dst = sum_t c_t src_t  or  dst += beta * sum_t c_t src_t, terms
 // summed in their order.
 template<int NT>
@@ -122,7 +207,6 @@ transfer_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
                 int32_t accumulate, double beta) {
     constexpr int RU = CellUnroll<NT>::value;
     __shared__ UnitDesc<NT> sd;
-    extern __shared__ double tiles[];             // [max_tiles][kTile][kTileLd]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const DUnit un = units[u];
@@ -130,54 +214,13 @@ transfer_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
         const int nt = sd.j.nterms;
         const double *sp[NT];
         double cf[NT];
-        int32_t sb[NT], sq[NT], ts[NT];
+        int32_t sb[NT], sq[NT];
 #pragma unroll
         for (int t = 0; t < NT; t++) {
             sp[t] = t < nt ? srcs[sd.t[t].src] : nullptr;
             cf[t] = t < nt ? sd.t[t].coeff : 0.0;
             sb[t] = t < nt ? sd.t[t].sb : 0;
             sq[t] = t < nt ? sd.t[t].sq : 0;
-            ts[t] = t < nt ? sd.t[t].tslot : -1;
-        }
-        if (sd.j.tiled) {
-            for (int64_t v = un.row_begin; v < un.row_end; v++) {
-                int64_t db, sbase[NT];
-                int b0, na, nb;
-                tile_bases<NT>(sd, (uint32_t)v, db, sbase, b0, na, nb);
-                // transposing terms: coalesced along the rows into shared memory
-                const int nel = na * nb;
-#pragma unroll
-                for (int t = 0; t < NT; t++) {
-                    if (t >= nt) break;
-                    if (ts[t] < 0) continue;
-                    double *T = tiles + ts[t] * kTileElems;
-#pragma unroll 4
-                    for (int i = threadIdx.x; i < nel; i += kThreads) {
-                        const int b = i / na, a = i - b * na;      // rows fastest: coalesced source
-                        T[b * kTileLd + a] = sp[t][sbase[t] + (int64_t)a * sq[t] + (int64_t)(b0 + b) * sb[t]];
-                    }
-                }
-                __syncthreads();
-#pragma unroll 4
-                for (int i = threadIdx.x; i < nel; i += kThreads) {
-                    const int a = i / nb, b = i - a * nb;          // columns fastest: coalesced destination
-                    {
-                        double val = 0.0;
-#pragma unroll
-                        for (int t = 0; t < NT; t++) {
-                            if (t >= nt) break;
-                            const double x = ts[t] >= 0 ? tiles[ts[t] * kTileElems + b * kTileLd + a]
-                                                        : sp[t][sbase[t] + (int64_t)a * sq[t] + (int64_t)(b0 + b) * sb[t]];
-                            val += cf[t] * x;
-                        }
-                        double *d = dst + db + (int64_t)a * sd.j.dq + b0 + b;
-                        if (accumulate) *d = *d + beta * val;
-                        else *d = val;
-                    }
-                }
-                __syncthreads();
-            }
-            continue;
         }
         // row mode: each warp walks its items cell by cell, lanes consecutive
         const int W = sd.j.vec ? 2 : 1;
@@ -253,6 +296,96 @@ transfer_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
     }
 }
 
+// Tiled mode (jobs with a transposing term): one CTA per tile at a time; every
+// term's tile is staged through shared memory, then combined in term order
+// and written along the destination's columns.
+constexpr int kTiledThreads = 512;
+
+template<int NT>
+__global__ void __launch_bounds__(kTiledThreads)
+transfer_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
+                      const DUnit *__restrict__ units, int32_t nunits,
+                      const double *const *__restrict__ srcs, double *__restrict__ dst,
+                      int32_t accumulate, double beta) {
+    __shared__ UnitDesc<NT> sd;
+    extern __shared__ double tiles[];             // one tile per term
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const DUnit un = units[u];
+        stage_unit<NT>(jobs, terms, un.job, sd);
+        const int nt = sd.j.nterms;
+        const int dq = sd.j.dq;
+        TileTerms<NT> tt;
+        load_tile_terms<NT>(sd, srcs, tt);
+        double cf[NT];
+#pragma unroll
+        for (int t = 0; t < NT; t++) cf[t] = t < nt ? sd.t[t].coeff : 0.0;
+        for (int64_t v = un.row_begin; v < un.row_end; v++) {
+            int64_t db, sbase[NT];
+            int b0, na, nb;
+            tile_bases<NT>(sd, (uint32_t)v, db, sbase, b0, na, nb);
+            stage_tile<NT, kTiledThreads>(nt, tt, sbase, b0, na, nb, tiles);
+            double *dtile = dst + db + b0;
+            const int nel = na * nb;
+            const int da = kTiledThreads / nb, dc = kTiledThreads - da * nb;
+            int a = threadIdx.x / nb, c = threadIdx.x - a * nb;
+            for (int i = threadIdx.x; i < nel; i += kTiledThreads) {
+                double val = 0.0;
+#pragma unroll
+                for (int t = 0; t < NT; t++) {
+                    if (t >= nt) break;
+                    val += cf[t] * tile_at<NT>(tiles, tt, t, a, c);
+                }
+                double *d = dtile + (a * dq + c);
+                if (accumulate) *d = *d + beta * val;
+                else *d = val;
+                a += da; c += dc;
+                if (c >= nb) { c -= nb; a++; }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTiledThreads)
+dot_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
+                 const DUnit *__restrict__ units, int32_t nunits,
+                 const double *__restrict__ a, const double *__restrict__ b,
+                 double *__restrict__ partials) {
+    __shared__ UnitDesc<2> sd;
+    __shared__ double red[kTiledThreads];
+    extern __shared__ double tiles[];
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const DUnit un = units[u];
+        stage_unit<2>(jobs, terms, un.job, sd);
+        const double *const ab[2] = {a, b};
+        TileTerms<2> tt;
+        load_tile_terms<2>(sd, ab, tt);
+        double s = 0.0;
+        for (int64_t v = un.row_begin; v < un.row_end; v++) {
+            int64_t db, sbase[2];
+            int b0, na, nb;
+            tile_bases<2>(sd, (uint32_t)v, db, sbase, b0, na, nb);
+            stage_tile<2, kTiledThreads>(2, tt, sbase, b0, na, nb, tiles);
+            const int nel = na * nb;
+            const int da = kTiledThreads / nb, dc = kTiledThreads - da * nb;
+            int aa = threadIdx.x / nb, c = threadIdx.x - aa * nb;
+            for (int i = threadIdx.x; i < nel; i += kTiledThreads) {
+                s += tile_at<2>(tiles, tt, 0, aa, c) * tile_at<2>(tiles, tt, 1, aa, c);
+                aa += da; c += dc;
+                if (c >= nb) { c -= nb; aa++; }
+            }
+            __syncthreads();
+        }
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = kTiledThreads / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) partials[u] = red[0] * sd.t[0].coeff;
+    }
+}
+
 // Dot product: one partial sum per unit (term 0 carries the orbit weight and
 // both transform signs), then one fixed-order reduction.
 __global__ void __launch_bounds__(kThreads)
@@ -263,47 +396,14 @@ dot_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
     constexpr int RU = CellUnroll<2>::value;
     __shared__ UnitDesc<2> sd;
     __shared__ double red[kThreads];
-    extern __shared__ double tiles[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const DUnit un = units[u];
         stage_unit<2>(jobs, terms, un.job, sd);
         const double *sp[2] = {sd.t[0].src == 0 ? a : b, sd.t[1].src == 0 ? a : b};
         const int32_t sb[2] = {sd.t[0].sb, sd.t[1].sb}, sq[2] = {sd.t[0].sq, sd.t[1].sq};
-        const int32_t ts[2] = {sd.t[0].tslot, sd.t[1].tslot};
         double s = 0.0;
-        if (sd.j.tiled) {
-            for (int64_t v = un.row_begin; v < un.row_end; v++) {
-                int64_t db, sbase[2];
-                int b0, na, nb;
-                tile_bases<2>(sd, (uint32_t)v, db, sbase, b0, na, nb);
-                const int nel = na * nb;
-#pragma unroll
-                for (int t = 0; t < 2; t++) {
-                    if (ts[t] < 0) continue;
-                    double *T = tiles + ts[t] * kTileElems;
-#pragma unroll 4
-                    for (int i = threadIdx.x; i < nel; i += kThreads) {
-                        const int bb = i / na, aa = i - bb * na;
-                        T[bb * kTileLd + aa] = sp[t][sbase[t] + (int64_t)aa * sq[t] + (int64_t)(b0 + bb) * sb[t]];
-                    }
-                }
-                __syncthreads();
-#pragma unroll 4
-                for (int i = threadIdx.x; i < nel; i += kThreads) {
-                    const int aa = i / nb, bb = i - aa * nb;
-                    {
-                        double x[2];
-#pragma unroll
-                        for (int t = 0; t < 2; t++)
-                            x[t] = ts[t] >= 0 ? tiles[ts[t] * kTileElems + bb * kTileLd + aa]
-                                              : sp[t][sbase[t] + (int64_t)aa * sq[t] + (int64_t)(b0 + bb) * sb[t]];
-                        s += x[0] * x[1];
-                    }
-                }
-                __syncthreads();
-            }
-        } else {
+        {
             const int W = sd.j.vec ? 2 : 1;
             for (int64_t v = un.row_begin + warp; v < un.row_end; v += kWarps) {
                 int64_t db, sbase[2];
@@ -435,45 +535,58 @@ int grid_for(int64_t units) {
     return g < 1 ? 1 : (int)g;
 }
 
-}  // namespace
-
 template<int NT>
-cudaError_t launch_transfer_nt(const DJob *jobs, const DTerm *terms, const DUnit *units, int32_t nunits,
-                               size_t smem, const double *const *srcs, double *dst, int32_t accumulate,
-                               double beta, cudaStream_t s) {
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(transfer_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
+cudaError_t launch_transfer_nt(const DJob *jobs, const DTerm *terms, const DUnit *units, int32_t nrow,
+                               int32_t ntiled, size_t smem, const double *const *srcs, double *dst,
+                               int32_t accumulate, double beta, cudaStream_t s) {
+    if (nrow > 0)
+        transfer_kernel<NT><<<grid_for(nrow), kThreads, 0, s>>>(jobs, terms, units, nrow, srcs, dst,
+                                                                accumulate, beta);
+    if (ntiled > 0) {
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(transfer_tiled_kernel<NT>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        transfer_tiled_kernel<NT><<<grid_for(ntiled), kTiledThreads, smem, s>>>(
+            jobs, terms, units + nrow, ntiled, srcs, dst, accumulate, beta);
     }
-    transfer_kernel<NT><<<grid_for(nunits), kThreads, smem, s>>>(jobs, terms, units, nunits, srcs, dst,
-                                                                 accumulate, beta);
     return cudaGetLastError();
 }
 
+}  // namespace
+
 cudaError_t launch_transfer(const DJob *jobs, const DTerm *terms, const DUnit *units,
-                            int32_t nunits, int32_t max_terms, int32_t max_tiles,
+                            int32_t nrow, int32_t ntiled, int32_t max_terms, int32_t tile_bytes,
                             const double *const *srcs, double *dst, int32_t accumulate, double beta,
                             cudaStream_t s) {
-    if (nunits <= 0) return cudaSuccess;
-    const size_t smem = (size_t)max_tiles * kTileElems * sizeof(double);
-    if (max_terms <= 1) return launch_transfer_nt<1>(jobs, terms, units, nunits, smem, srcs, dst, accumulate, beta, s);
-    if (max_terms <= 2) return launch_transfer_nt<2>(jobs, terms, units, nunits, smem, srcs, dst, accumulate, beta, s);
-    if (max_terms <= 4) return launch_transfer_nt<4>(jobs, terms, units, nunits, smem, srcs, dst, accumulate, beta, s);
+    if (nrow + ntiled <= 0) return cudaSuccess;
+    const size_t smem = (size_t)tile_bytes;
+    if (max_terms <= 1) return launch_transfer_nt<1>(jobs, terms, units, nrow, ntiled, smem, srcs, dst, accumulate, beta, s);
+    if (max_terms <= 2) return launch_transfer_nt<2>(jobs, terms, units, nrow, ntiled, smem, srcs, dst, accumulate, beta, s);
+    if (max_terms <= 4) return launch_transfer_nt<4>(jobs, terms, units, nrow, ntiled, smem, srcs, dst, accumulate, beta, s);
     if (max_terms <= kMaxTerms)
-        return launch_transfer_nt<kMaxTerms>(jobs, terms, units, nunits, smem, srcs, dst, accumulate, beta, s);
+        return launch_transfer_nt<kMaxTerms>(jobs, terms, units, nrow, ntiled, smem, srcs, dst, accumulate, beta, s);
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_dot(const DJob *jobs, const DTerm *terms, const DUnit *units,
-                       int32_t nunits, int32_t max_tiles, const double *a, const double *b,
+                       int32_t nrow, int32_t ntiled, int32_t tile_bytes, const double *a, const double *b,
                        double *partials, double *out, cudaStream_t s) {
-    if (nunits <= 0) return cudaMemsetAsync(out, 0, sizeof(double), s);
-    const size_t smem = (size_t)max_tiles * kTileElems * sizeof(double);
-    dot_kernel<<<grid_for(nunits), kThreads, smem, s>>>(jobs, terms, units, nunits, a, b, partials);
+    if (nrow + ntiled <= 0) return cudaMemsetAsync(out, 0, sizeof(double), s);
+    if (nrow > 0) dot_kernel<<<grid_for(nrow), kThreads, 0, s>>>(jobs, terms, units, nrow, a, b, partials);
+    if (ntiled > 0) {
+        const size_t smem = (size_t)tile_bytes;
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(dot_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        dot_tiled_kernel<<<grid_for(ntiled), kTiledThreads, smem, s>>>(jobs, terms, units + nrow, ntiled, a, b,
+                                                                          partials + nrow);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    reduce_kernel<<<1, kThreads, 0, s>>>(partials, nunits, out);
+    reduce_kernel<<<1, kThreads, 0, s>>>(partials, nrow + ntiled, out);
     return cudaGetLastError();
 }
 

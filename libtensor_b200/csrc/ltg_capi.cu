@@ -662,15 +662,18 @@ void validate_transfer(const TransferPlan &plan, const std::vector<int64_t> &src
 struct DeviceTransfer {
     std::vector<DJob> jobs;
     std::vector<DTerm> terms;
-    std::vector<DUnit> units;
-    int32_t max_terms = 0, max_tiles = 0;
+    std::vector<DUnit> units;          // row-mode units, then tiled-mode units
+    int32_t nrow = 0, ntiled = 0;
+    int32_t max_terms = 0, tile_bytes = 0;
 };
 constexpr int64_t kTransferUnitElems = 32768;
 constexpr int32_t kItemElems = 4096;       // row mode: elements per warp item (about)
 constexpr int32_t kTileSide = 64;          // largest tile side (elements)
+constexpr int64_t kTileSmemDoubles = 12288; // tiled mode: shared memory for all terms' tiles (96 KiB)
 
-DeviceTransfer device_transfer(const TransferPlan &plan) {
+DeviceTransfer device_transfer(const TransferPlan &plan, int64_t unit_elems = kTransferUnitElems) {
     DeviceTransfer o;
+    std::vector<DUnit> tiled_units;
     for (const TJob &j : plan.jobs) {
         const int n = j.ndim, L = n - 1;
         const TTerm *T = plan.terms.data() + j.term0;
@@ -712,7 +715,14 @@ DeviceTransfer device_transfer(const TransferPlan &plan) {
         dj.nra = (dj.A + dj.ra - 1) / dj.ra;
         bool vec = !transposing && dj.seg % 2 == 0 && dj.B % 2 == 0 && dj.dst_off % 2 == 0 && dj.dq % 2 == 0;
         for (int k = 0; k < dj.nout; k++) vec = vec && dj.odst[k] % 2 == 0;
-        int32_t ntiles = 0;
+        // tiled mode: square-ish tiles of at most kTileSide whose tiles of all
+        // terms fit kTileSmemDoubles; balanced tile extents per dim
+        int32_t side = kTileSide;
+        while (side > 8 && (int64_t)std::max(1, j.nterms) * side * (side + 1) > kTileSmemDoubles) side--;
+        dj.nta = (dj.A + side - 1) / side;
+        dj.ntb = (dj.B + side - 1) / side;
+        const int32_t ta_ext = (dj.A + dj.nta - 1) / dj.nta, tb_ext = (dj.B + dj.ntb - 1) / dj.ntb;
+        int32_t toff = 0;
         for (int t = 0; t < j.nterms; t++) {
             DTerm dt{};
             dt.src_off = T[t].src_off;
@@ -720,19 +730,29 @@ DeviceTransfer device_transfer(const TransferPlan &plan) {
             dt.src = T[t].src;
             dt.sq = q >= 0 ? T[t].sstr[q] : 0;
             dt.sb = T[t].sstr[L];
-            dt.tslot = transposing && dt.sb != 1 ? ntiles++ : -1;
+            if (transposing) {
+                dt.tmode = dt.sb == 1 ? 0 : 1;
+                dt.tld = dt.tmode == 0 ? tb_ext : ta_ext + 1;
+                toff += toff & 1;                        // 16-byte aligned tiles
+                dt.toff = toff;
+                toff += dt.tmode == 0 ? ta_ext * tb_ext : tb_ext * (ta_ext + 1);
+                // 16-byte copies along the columns: every tile row starts even
+                dt.tvec = dt.tmode == 0 && tb_ext % 2 == 0 && dj.B % 2 == 0 && dt.src_off % 2 == 0 &&
+                          dt.sq % 2 == 0 ? 1 : 0;
+            }
             int k = 0;
             for (int d = 0; d < L; d++)
                 if (d != q) dt.osrc[k++] = T[t].sstr[d];
             vec = vec && dt.sb == 1 && dt.src_off % 2 == 0 && dt.sq % 2 == 0;
-            for (int kk = 0; kk < dj.nout; kk++) vec = vec && dt.osrc[kk] % 2 == 0;
+            for (int kk = 0; kk < dj.nout; kk++) {
+                vec = vec && dt.osrc[kk] % 2 == 0;
+                if (dt.osrc[kk] % 2) dt.tvec = 0;
+            }
             o.terms.push_back(dt);
         }
         dj.vec = vec ? 1 : 0;
-        dj.nta = (dj.A + kTileSide - 1) / kTileSide;
-        dj.ntb = (dj.B + kTileSide - 1) / kTileSide;
         o.max_terms = std::max(o.max_terms, j.nterms);
-        o.max_tiles = std::max(o.max_tiles, ntiles);
+        if (transposing) o.tile_bytes = std::max<int32_t>(o.tile_bytes, (toff + 1) * (int32_t)sizeof(double));
         const int32_t ji = (int32_t)o.jobs.size();
         o.jobs.push_back(dj);
         int64_t planes = 1;
@@ -743,26 +763,29 @@ DeviceTransfer device_transfer(const TransferPlan &plan) {
         if (dj.tiled) {
             items = planes * dj.nta * dj.ntb;
             const int64_t tile = (int64_t)((dj.A + dj.nta - 1) / dj.nta) * ((dj.B + dj.ntb - 1) / dj.ntb);
-            per_unit = std::max<int64_t>(1, kTransferUnitElems / tile);
+            per_unit = std::max<int64_t>(1, unit_elems / tile);
         } else {
             items = planes * dj.nra * dj.nseg;
             const int64_t item = (int64_t)dj.ra * dj.seg;
-            per_unit = std::max<int64_t>(8, (kTransferUnitElems / item + 7) / 8 * 8);
+            per_unit = std::max<int64_t>(8, (unit_elems / item + 7) / 8 * 8);
         }
         for (int64_t r = 0; r < items; r += per_unit) {
             DUnit u{};
             u.job = ji;
             u.row_begin = r;
             u.row_end = std::min(items, r + per_unit);
-            o.units.push_back(u);
+            (dj.tiled ? tiled_units : o.units).push_back(u);
         }
     }
+    o.nrow = (int32_t)o.units.size();
+    o.ntiled = (int32_t)tiled_units.size();
+    o.units.insert(o.units.end(), tiled_units.begin(), tiled_units.end());
     return o;
 }
 
 struct TransferExec {
     DevBuf jobs, terms, units, srcs;
-    int32_t nunits = 0, max_terms = 0, max_tiles = 0;
+    int32_t nrow = 0, ntiled = 0, max_terms = 0, tile_bytes = 0;
     std::vector<char> dst_nonzero;
 };
 typedef std::tuple<std::vector<const ltg_bt *>, std::vector<int8_t>, std::vector<double>,
@@ -808,9 +831,10 @@ void run_transfer(ltg_ctx *ctx, const std::vector<ltg_bt *> &srcs, const std::ve
         std::vector<const double *> sp;
         for (ltg_bt *b : srcs) sp.push_back(b->arena.as<double>());
         upload_vec(nx->srcs, sp, s);
-        nx->nunits = (int32_t)dt.units.size();
+        nx->nrow = dt.nrow;
+        nx->ntiled = dt.ntiled;
         nx->max_terms = dt.max_terms;
-        nx->max_tiles = dt.max_tiles;
+        nx->tile_bytes = dt.tile_bytes;
         nx->dst_nonzero = plan.dst_nonzero;
         ex = nx.get();
         std::lock_guard<std::mutex> lk(g_tr_mtx);
@@ -818,7 +842,7 @@ void run_transfer(ltg_ctx *ctx, const std::vector<ltg_bt *> &srcs, const std::ve
     }
     TimedLaunch tl(ctx, LTG_KERNEL_TRANSFER);
     LTG_CUDA(launch_transfer(ex->jobs.as<DJob>(), ex->terms.as<DTerm>(), ex->units.as<DUnit>(),
-                             ex->nunits, ex->max_terms, ex->max_tiles, ex->srcs.as<const double *>(), dst->arena.as<double>(),
+                             ex->nrow, ex->ntiled, ex->max_terms, ex->tile_bytes, ex->srcs.as<const double *>(), dst->arena.as<double>(),
                              add ? 1 : 0, d, s));
     tl.done();
     ctx->launches++;
@@ -840,7 +864,7 @@ void forget_transfer(const ltg_bt *t) {
 // only kernel launches.
 struct DotExec {
     DevBuf jobs, terms, units, partials;
-    int32_t nunits = 0, max_tiles = 0;
+    int32_t nrow = 0, ntiled = 0, tile_bytes = 0;
 };
 std::mutex g_dot_mtx;
 std::map<std::tuple<const ltg_bt *, const ltg_bt *, std::vector<int8_t>, std::vector<int8_t>>,
@@ -858,13 +882,15 @@ DotExec *prepare_dot(ltg_bt *a, const Perm &pa, ltg_bt *b, const Perm &pb) {
     validate_transfer(plan, {a->h.total_elems, b->h.total_elems}, -1);
     std::unique_ptr<DotExec> ex(new DotExec());
     cudaStream_t s = a->ctx->stream;
-    DeviceTransfer dt = device_transfer(plan);
+    // larger units for the dot product: each unit ends in a CTA reduction
+    DeviceTransfer dt = device_transfer(plan, 4 * kTransferUnitElems);
     upload_vec(ex->jobs, dt.jobs, s);
     upload_vec(ex->terms, dt.terms, s);
     upload_vec(ex->units, dt.units, s);
     ex->partials.alloc(std::max<size_t>(dt.units.size(), 1) * sizeof(double));
-    ex->nunits = (int32_t)dt.units.size();
-    ex->max_tiles = dt.max_tiles;
+    ex->nrow = dt.nrow;
+    ex->ntiled = dt.ntiled;
+    ex->tile_bytes = dt.tile_bytes;
     DotExec *raw = ex.get();
     g_dot_cache[key] = std::move(ex);
     return raw;
@@ -1453,8 +1479,8 @@ int ltg_dotprod_async(ltg_bt *a, const int32_t *perma, ltg_bt *b, const int32_t 
         if (a->ctx != b->ctx) throw error(kErrBadArg, "operands belong to different contexts");
         DotExec *ex = prepare_dot(a, perm_from(a->h.bis.n, perma), b, perm_from(b->h.bis.n, permb));
         TimedLaunch tl(a->ctx, LTG_KERNEL_DOT);
-        LTG_CUDA(launch_dot(ex->jobs.as<DJob>(), ex->terms.as<DTerm>(), ex->units.as<DUnit>(), ex->nunits,
-                            ex->max_tiles, a->arena.as<double>(), b->arena.as<double>(), ex->partials.as<double>(), dev_out,
+        LTG_CUDA(launch_dot(ex->jobs.as<DJob>(), ex->terms.as<DTerm>(), ex->units.as<DUnit>(), ex->nrow,
+                            ex->ntiled, ex->tile_bytes, a->arena.as<double>(), b->arena.as<double>(), ex->partials.as<double>(), dev_out,
                             a->ctx->stream));
         tl.done();
         a->ctx->launches += 2;

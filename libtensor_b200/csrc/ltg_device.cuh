@@ -98,8 +98,10 @@ struct DTerm {
     double coeff;
     int32_t src;                  // source tensor index
     int32_t sq, sb;               // source strides of dim q and of the columns
-    int32_t tslot;                // tiled mode: shared-memory tile of this term, -1: read directly
+    int32_t tmode;                // tiled mode: 0 tile stored [row][col], 1 stored [col][row]
     int32_t osrc[kDevMaxOrder - 2];   // source strides of the outer dims
+    int32_t toff, tld;            // tiled mode: tile offset (doubles) in shared memory, leading dim
+    int32_t tvec, pad2;           // tiled mode, layout 0: 16-byte copies valid
 };
 
 // A range [row_begin, row_end) of one job's work items processed by one CTA:
@@ -181,14 +183,16 @@ cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices
 // per 64-byte k block, bound of one slice product.
 void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod);
 
-// Element-wise transfer kernels.  max_terms bounds nterms and max_tiles the
-// shared-memory tiles (transposing terms) of any job.
+// Element-wise transfer kernels.  max_terms bounds nterms and tile_bytes the
+// shared-memory tiles of any tiled-mode job.
+// Units are ordered row-mode units first (nrow of them), then tiled-mode
+// units (ntiled); the dot product leaves one partial sum per unit.
 cudaError_t launch_transfer(const DJob *jobs, const DTerm *terms, const DUnit *units,
-    int32_t nunits, int32_t max_terms, int32_t max_tiles, const double *const *srcs, double *dst,
-    int32_t accumulate, double beta, cudaStream_t s);
+    int32_t nrow, int32_t ntiled, int32_t max_terms, int32_t tile_bytes, const double *const *srcs,
+    double *dst, int32_t accumulate, double beta, cudaStream_t s);
 cudaError_t launch_dot(const DJob *jobs, const DTerm *terms, const DUnit *units,
-    int32_t nunits, int32_t max_tiles, const double *a, const double *b, double *partials,
-    double *out, cudaStream_t s);
+    int32_t nrow, int32_t ntiled, int32_t tile_bytes, const double *a, const double *b,
+    double *partials, double *out, cudaStream_t s);
 cudaError_t launch_scale(double *x, int64_t n, double c, cudaStream_t s);
 cudaError_t launch_fill_seeded(double *arena, const int64_t *blk_off,
     const int64_t *blk_start, const int32_t *blk_ext, int32_t nblk, int32_t order,

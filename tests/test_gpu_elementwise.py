@@ -75,6 +75,35 @@ def test_add_four_permuted_terms(gctx):
     assert max_rel_block_error(errs) <= 1e-15
 
 
+def test_add_eight_transposing_terms(gctx):
+    # 8 terms that all move the innermost index: every term goes through the
+    # shared-memory tiles (more than 48 KiB of them per CTA)
+    spec = BTSpec(dims=[20, 70, 90], splits=[[7], [30], [40, 65]])
+    X, rx, _ = seeded_pair(gctx, spec, 14, 1.0)
+    perms = [(0, 2, 1)] * 4 + [(0, 2, 1)] * 4
+    coeffs = [1.0, -0.5, 0.25, 2.0, -1.0, 0.125, 3.0, -0.75]
+    src = [X] * 8
+    out_spec = BTSpec(dims=[20, 90, 70], splits=[[7], [40, 65], [30]])
+    Y = block_tensor(gctx, out_spec)
+    op = btod_add(src[0], perms[0], coeffs[0])
+    for t in range(1, 8):
+        op.add_op(src[t], perms[t], coeffs[t])
+    op.perform(Y)
+    ry = R.RefBT(out_spec)
+    R.ref_add([(rx, p, c) for p, c in zip(perms, coeffs)], ry)
+    errs = block_errors(Y, Y.download(), ry, None)
+    assert max_rel_block_error(errs) <= 1e-15
+
+
+def test_dotprod_transposed_no_symmetry(gctx):
+    spec = BTSpec(dims=[33, 70, 70], splits=[[16], [20, 45], [20, 45]])
+    A, ra, _ = seeded_pair(gctx, spec, 15, 1.0)
+    B, rb, _ = seeded_pair(gctx, spec, 16, 1.0)
+    v = btod_dotprod(A, None, B, (0, 2, 1)).calculate()
+    rv = R.ref_dotprod(ra, None, rb, (0, 2, 1))
+    assert abs(v - rv) <= 1e-12 * abs(rv), (v, rv)
+
+
 def test_add_into_existing_with_coefficients(gctx):
     spec = S.LADDER_SMALL.t_spec()
     A, ra, _ = seeded_pair(gctx, spec, 8, 1.0)
