@@ -37,7 +37,7 @@ WORKLOADS = {
 # HBM-bound operations (btod_copy / btod_add / btod_dotprod) on the CCD
 # iteration's tensors, o=30 v=300 (blocks 15 / 50,50,50 per spin).
 TRANSFER_WORKLOADS = ("copy-vvvv", "add-x4", "dot-vvvv")
-MODES = {"plain": 0, "ozaki-bf16": 1, "ozaki-fp8": 2, "ozaki-int8": 3}
+MODES = {"plain": 0, "ozaki-bf16": 1, "ozaki-fp8": 2, "ozaki-int8": 3, "ozaki-crt": 4}
 FP64_NOMINAL = 40.0
 
 
@@ -437,10 +437,12 @@ def contraction_roofline(torch, dev, args, flops, ktimes):
                 "peak_source": "measured live: cuBLAS DGEMM 8192^3 (FP64 tensor path), "
                                f"nominal {FP64_NOMINAL} TFLOP/s"}
     if kname == "oz_gemm":
-        S = args.nslices if args.nslices > 0 else (8 if args.mode == "ozaki-fp8" else 7)
-        prods = S * (S + 1) // 2
+        S = args.nslices if args.nslices > 0 else (8 if args.mode == "ozaki-fp8" else (13 if args.mode == "ozaki-crt" else 7))
+        # slice products per FP64 multiply-add: S(S+1)/2 for the slice modes,
+        # one per modulus for the modular mode
+        prods = S if args.mode == "ozaki-crt" else S * (S + 1) // 2
         ach = prods * per_launch / sec / 1e12
-        if args.mode == "ozaki-int8":
+        if args.mode in ("ozaki-int8", "ozaki-crt"):
             try:
                 peak, src = measure_int8_peak(torch, dev), "measured live: cuBLASLt INT8 GEMM 8192^3 (torch._int_mm)"
             except Exception as e:     # no INT8 GEMM in this torch build

@@ -40,7 +40,10 @@ enum {
     LTG_MODE_PLAIN_FP64 = 0,     /* FP64 DMMA tensor-core contraction (drop-in) */
     LTG_MODE_OZAKI_BF16 = 1,     /* split-precision: BF16 slices, FP32 accumulate */
     LTG_MODE_OZAKI_FP8 = 2,      /* split-precision: FP8 E4M3 slices, FP32 accumulate */
-    LTG_MODE_OZAKI_INT8 = 3      /* split-precision: INT8 slices, INT32 accumulate */
+    LTG_MODE_OZAKI_INT8 = 3,     /* split-precision: INT8 slices, INT32 accumulate */
+    LTG_MODE_OZAKI_CRT = 4       /* split-precision: INT8 residues modulo nslices (8..16,
+                                    default 13) coprime moduli, INT32 accumulate,
+                                    Chinese-remainder recombination in FP64 */
 };
 
 typedef struct ltg_ctx ltg_ctx;
@@ -101,7 +104,8 @@ enum {
     LTG_KERNEL_SCALE = 5,
     LTG_KERNEL_FILL = 6,            /* seeded fill */
     LTG_KERNEL_DENOMINATOR = 7,
-    LTG_KERNEL_KINDS = 8
+    LTG_KERNEL_OZ_COMBINE = 8,      /* split-precision: modular recombination */
+    LTG_KERNEL_KINDS = 9
 };
 int ltg_ctx_set_timing(ltg_ctx *ctx, int32_t enable);
 int ltg_ctx_kernel_times(ltg_ctx *ctx, double *ms, int64_t *launches);

@@ -20,7 +20,7 @@ ERRORS = {
     4: "LTG_ERR_UNSUPPORTED", 5: "LTG_ERR_OOM", 6: "LTG_ERR_CUDA",
     7: "LTG_ERR_TIMEOUT", 8: "LTG_ERR_STATE",
 }
-MODE_PLAIN_FP64, MODE_OZAKI_BF16, MODE_OZAKI_FP8, MODE_OZAKI_INT8 = 0, 1, 2, 3
+MODE_PLAIN_FP64, MODE_OZAKI_BF16, MODE_OZAKI_FP8, MODE_OZAKI_INT8, MODE_OZAKI_CRT = 0, 1, 2, 3, 4
 
 
 class ltg_bt_spec(C.Structure):

@@ -31,6 +31,7 @@ SOURCES = [
     "elementwise.cu",
     "ozaki.cu",
     "noalloc.cu",
+    "crt.cu",
 ]
 OPTIONAL_SOURCES = []
 

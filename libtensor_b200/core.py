@@ -27,6 +27,7 @@ MODE_PLAIN_FP64 = _capi.MODE_PLAIN_FP64
 MODE_OZAKI_BF16 = _capi.MODE_OZAKI_BF16
 MODE_OZAKI_FP8 = _capi.MODE_OZAKI_FP8
 MODE_OZAKI_INT8 = _capi.MODE_OZAKI_INT8
+MODE_OZAKI_CRT = _capi.MODE_OZAKI_CRT
 
 
 def _i32(vals):
@@ -60,7 +61,8 @@ class Context:
         check(lib().ltg_ctx_launch_count(self.h, C.byref(n)))
         return n.value
 
-    KERNELS = ("contract_fp64", "oz_split", "oz_gemm", "transfer", "dot", "scale", "fill", "denominator")
+    KERNELS = ("contract_fp64", "oz_split", "oz_gemm", "transfer", "dot", "scale", "fill", "denominator",
+               "oz_combine")
 
     def set_timing(self, enable: bool):
         """Per-kernel device timing with CUDA events (resets the totals)."""

@@ -1,0 +1,585 @@
+// Modular (CRT) split-precision contraction on the tcgen05 INT8 tensor cores.
+//
+// FP64 operands are scaled row by row to integers of P bits and multiplied
+// exactly as their residues modulo L pairwise coprime moduli m_l <= 256
+// (the "integer modular" emulation of Ozaki, Uchino and Imamura, 2024):
+//   1. exponents (crt_exp_kernel): for every operand row, the exponent of its
+//      largest magnitude, combined over all panels that feed the same global
+//      row of C (atomicMax into one table per side of C), so that every pair
+//      of a C block shares the row and column scaling;
+//   2. residues (crt_res_kernel): X = c_p * rint(x * 2^(P - e_row)) (the
+//      pair's integer coefficient c_p folded in on one side), stored as its
+//      balanced residues mod m_l (INT8) in shared-memory tile images;
+//   3. products (crt_gemm_kernel): per C tile and modulus, all pairs and k
+//      blocks accumulate sum_p sum_k A_l * B_l exactly in one INT32 TMEM
+//      accumulator (|sum| < 2^31 is checked on the host); the epilogue warps
+//      reduce it mod m_l to one byte per element while the MMA warp fills the
+//      other accumulator with the next modulus;
+//   4. recombination (crt_combine_kernel): Garner's mixed-radix algorithm
+//      with balanced digits gives the exact integer sum_p c_p A'_p B'_p in
+//      (-M/2, M/2), M = prod m_l (the host chooses P so that it fits), which
+//      is scaled by 2^(e_row + e_col - 2P) and the contraction coefficient in
+//      FP64 and written to C (assign or add).
+// The error is that of rounding each operand to P bits relative to its row's
+// largest element (P about 43 for 13 moduli and K up to a few thousand).
+//
+// Warp roles of the products kernel (192 threads): warps 0-3 epilogue (TMEM
+// lanes 0-127, one tile row per thread), warp 4 bulk-copy producer, warp 5
+// MMA issuer.  Operand tiles are whole tile images moved by 1-D
+// cp.async.bulk (no tensor maps, no multicast); every mbarrier wait is
+// bounded in time and reports through *err.
+#include "ltg_device.cuh"
+
+namespace ltg {
+namespace {
+
+constexpr int kXRows = 128;                         // MMA M (TMEM lanes)
+constexpr int kKB = 32;                             // bytes (INT8 elements) per k block
+constexpr int kXTile = kXRows * kKB;                // 4 KB
+constexpr int kMaxNt = 256;
+constexpr int kStageBytes = 2 * kXTile + kMaxNt * kKB;  // 16 KB: two M tiles and one N tile
+constexpr int kMaxStages = 12;
+constexpr int kGemmThreads = 192;
+constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s per barrier wait
+constexpr double kMagicD = 6755399441055744.0;      // 1.5 * 2^52: round-to-integer constant
+constexpr float kMagicF = 12582912.0f;              // 1.5 * 2^23
+constexpr int32_t kNoExp = -1000000;                // exponent of a row with no non-zero element
+
+__device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_t *ext, const int32_t *str) {
+    int64_t off = 0;
+    for (int i = n - 1; i >= 0; i--) {
+        const int32_t e = ext[i];
+        const int32_t q = lin / e;
+        off += (int64_t)(lin - q * e) * str[i];
+        lin = q;
+    }
+    return off;
+}
+
+// Byte offset of element (row r, k byte kb_byte of k block kb) of modulus l
+// in a panel's tile images: [row tile][k block][modulus] images of TR rows x
+// 32 bytes, K-major core matrices of 8 rows x 16 bytes (the two 16-byte k
+// halves 128 bytes apart, 8-row groups 256 bytes apart).
+__device__ __forceinline__ int64_t image_offset(int r, int TR, int nkb, int kb, int l, int L, int kb_byte) {
+    const int tile = r / TR, rr = r - tile * TR;
+    return ((int64_t)(tile * nkb + kb) * L + l) * (int64_t)(TR * kKB) + (rr >> 3) * 256 +
+           (kb_byte >> 4) * 128 + (rr & 7) * 16 + (kb_byte & 15);
+}
+
+// ---------------------------------------------------------------- exponents
+
+__global__ void crt_fill_kernel(int32_t *p, int32_t n, int32_t v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// 32 rows per CTA, 8 threads per row reading 4 consecutive k per step.
+__global__ void __launch_bounds__(256)
+crt_exp_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const double *__restrict__ A,
+               const double *__restrict__ B, const int32_t *__restrict__ gidx, int32_t *ex, int32_t *ey) {
+    const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
+    for (int p = blockIdx.y; p < npanels; p += gridDim.y) {
+        const DCrtPanel &P = panels[p];
+        const double *src = P.src ? B : A;
+        const bool contig = P.nk == 1 && P.kstr[0] == 1;
+        int32_t *tab = P.side == 0 ? ex : ey;
+        for (int r0 = blockIdx.x * 32; r0 < P.rows; r0 += gridDim.x * 32) {
+            const int r = r0 + lr;
+            const bool valid = r < P.rows;
+            const double *row = src + P.src_off + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
+            double mx = 0.0;
+            if (valid)
+                for (int k0 = 4 * c; k0 < P.K; k0 += 32)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const int k = k0 + j;
+                        if (k < P.K) mx = fmax(mx, fabs(row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)]));
+                    }
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+            if (valid && c == 0 && mx > 0.0) {
+                int e;
+                frexp(mx, &e);                        // mx = f * 2^e, f in [0.5, 1)
+                atomicMax(&tab[gidx[P.g_off + r]], e);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- residues
+
+// Balanced residue (as its low byte) of an integer-valued double |X| < 2^51
+// modulo m, from X - m * rint(X / m) in exact FP64 arithmetic.  The quotient
+// rint(X * (1/m)) is exact: the product's relative error 2^-53 moves X/m by
+// less than 2^-10.5, while X/m mod 1 stays at least 1/(2m) away from 1/2 for
+// odd m; for m = 256 the scaling is exact.  So |r| <= (m-1)/2 for odd m and
+// |r| <= 128 for m = 256, where +128 and -128 share the byte 0x80.
+__device__ __forceinline__ uint32_t residue_fp64(double X, double m, double minv) {
+    const double q = fma(X, minv, kMagicD) - kMagicD;
+    return (uint32_t)__double2loint(fma(-q, m, X) + kMagicD);
+}
+
+// Same from the five 11-bit limbs d of |X| (X < 2^55) in exact FP32
+// arithmetic: s = sum_t d_t (2^(11 t) mod m) < 2^21.1, so rint(s * (1/m)) is
+// again exact (error below 2^-10.5 against a distance of at least 2^-9).
+// sgn is +1 or -1, the sign of X.
+__device__ __forceinline__ uint32_t residue_fp32(const float (&d)[5], float sgn, const int32_t *pw, float m,
+                                                 float minv) {
+    float s = d[0];
+#pragma unroll
+    for (int t = 1; t < 5; t++) s = fmaf(d[t], (float)pw[t - 1], s);
+    const float q = fmaf(s, minv, kMagicF) - kMagicF;
+    const float r = fmaf(-q, m, s) * sgn;
+    return (uint32_t)__float_as_int(r + kMagicF);        // low byte: r mod 256
+}
+
+// Low bytes of four words packed into one.
+__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
+}
+
+// The first L64 moduli use the FP64 pipe, the rest the FP32 pipe, so that
+// both run at once.
+template<int L>
+__global__ void __launch_bounds__(256)
+crt_res_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const double *__restrict__ A,
+               const double *__restrict__ B, const int32_t *__restrict__ gidx, const int32_t *__restrict__ ex,
+               const int32_t *__restrict__ ey, uint8_t *__restrict__ res, const CrtParams cp) {
+    constexpr int L64 = (L + 1) / 2;
+    const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
+    for (int p = blockIdx.y; p < npanels; p += gridDim.y) {
+        const DCrtPanel &P = panels[p];
+        const double *src = P.src ? B : A;
+        const bool contig = P.nk == 1 && P.kstr[0] == 1;
+        const int32_t *tab = P.side == 0 ? ex : ey;
+        uint8_t *base = res + P.res_off;
+        const int TR = P.tr, nkb = P.K_pad / kKB;
+        const double coef = (double)P.coef;
+        for (int r0 = blockIdx.x * 32; r0 < P.rows_pad; r0 += gridDim.x * 32) {
+            const int r = r0 + lr;
+            if (r >= P.rows_pad) continue;           // rows_pad need not be a multiple of 32
+            const bool valid = r < P.rows;
+            const double *row = src + P.src_off + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
+            const int e = valid ? tab[gidx[P.g_off + r]] : kNoExp;
+            // 2^(P - e) as two finite factors
+            const int sh = e > kNoExp ? cp.P - e : 0;
+            const double s1 = ldexp(1.0, sh / 2), s2 = ldexp(1.0, sh - sh / 2);
+            const bool live = valid && e > kNoExp;
+            for (int k0 = 4 * c; k0 < P.K_pad; k0 += 32) {
+                double X[4];
+                float d[4][5];
+                float sgn[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int k = k0 + j;
+                    const double x = (live && k < P.K) ? row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
+                    const double y = (x * s1) * s2;                 // exact, |y| < 2^P
+                    X[j] = ((y + kMagicD) - kMagicD) * coef;        // rint, then the integer coefficient
+                    sgn[j] = X[j] < 0.0 ? -1.0f : 1.0f;
+                    const uint64_t u = (uint64_t)__double_as_longlong(fabs(X[j]) + 4503599627370496.0) &
+                                       ((1ull << 52) - 1);         // |X| as an integer
+#pragma unroll
+                    for (int t = 0; t < 5; t++) d[j][t] = (float)(uint32_t)((u >> (11 * t)) & 2047u);
+                }
+                const int kb = k0 / kKB, kb_byte = k0 % kKB;
+                uint8_t *dst0 = base + image_offset(r, TR, nkb, kb, 0, L, kb_byte);
+                const int64_t lstride = (int64_t)TR * kKB;          // next modulus image
+#pragma unroll
+                for (int l = 0; l < L; l++) {
+                    uint32_t v[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        v[j] = l < L64 ? residue_fp64(X[j], (double)cp.m[l], cp.minv_d[l])
+                                       : residue_fp32(d[j], sgn[j], cp.pow11[l], (float)cp.m[l], cp.minv_f[l]);
+                    *reinterpret_cast<uint32_t *>(dst0 + l * lstride) = pack4(v[0], v[1], v[2], v[3]);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- tcgen05 helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.shared::cta.b64 st, [%0]; }" :: "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }"
+                 :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for the phase with the given parity (false on timeout or abort).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    const uint32_t a = smem_u32(bar);
+    uint64_t t0 = 0;
+    for (uint32_t i = 0;; i++) {
+        uint32_t done;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+        if ((i & 63) == 63) {
+            if (*abort) return false;
+            const uint64_t t = global_ns();
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > kWaitNs) return false;
+        }
+    }
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+// K-major shared-memory descriptor without swizzle (8-row x 16-byte core
+// matrices; k halves 128 bytes apart, 8-row groups 256 bytes apart).
+__device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)(128 >> 4) << 16;
+    d |= (uint64_t)(256 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+// kind::i8: S32 accumulator, signed INT8 A and B, K-major, M = 128, N = nt.
+__device__ __forceinline__ uint32_t instr_desc_i8(int nt) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nt >> 3) << 17) | ((uint32_t)(kXRows >> 4) << 24);
+}
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+    asm volatile("{ .reg .pred p; setp.ne.b32 p, %4, 0;\n"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; }"
+                 :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *v) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                   "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                   "=r"(v[14]), "=r"(v[15])
+                 : "r"(taddr) : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// ---------------------------------------------------------------- modular products
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict__ res,
+                const DCrtTask *__restrict__ tasks, const DCrtItem *__restrict__ items, int32_t nitems,
+                uint8_t *__restrict__ out, const CrtParams cp, int32_t stages, int32_t *err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], drain_bar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int L = cp.L;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < stages; i++) { mbar_init(&full_bar[i], 1); mbar_init(&empty_bar[i], 1); }
+        for (int b = 0; b < 2; b++) { mbar_init(&accf_bar[b], 1); mbar_init(&acce_bar[b], 4); }
+        mbar_init(&drain_bar, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;"
+                     :: "r"(smem_u32(&tmem_base_s)) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_s;
+    const uint32_t smem0 = smem_u32(smem);
+
+    if (warp == 4) {
+        // ------------------------------------------------ bulk-copy producer
+        if (lane == 0) {
+            int st = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            int armed[kMaxStages];
+            for (int i = 0; i < kMaxStages; i++) armed[i] = -1;
+            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+                const DCrtItem item = items[it];
+                const uint32_t ybytes = (uint32_t)item.nt * kKB;
+                for (int l = 0; l < L && ok; l++) {
+                    for (int ti = item.t_begin; ti < item.t_end && ok; ti++) {
+                        const DCrtTask t = tasks[ti];
+                        const DCrtPanel &X = panels[t.px];
+                        const DCrtPanel &Y = panels[t.py];
+                        const int nkb = X.K_pad / kKB;
+                        const int64_t xt = (int64_t)nkb * L * kXTile;          // one M tile's images
+                        const uint8_t *ga = res + X.res_off + (int64_t)(item.x0 / kXRows) * xt;
+                        const uint8_t *gb = res + Y.res_off + (int64_t)(item.y0 / item.nt) * nkb * L * ybytes;
+                        for (int kb = 0; kb < nkb; kb++) {
+                            if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s)) { ok = false; break; }
+                            const uint32_t sa = smem0 + st * kStageBytes;
+                            const uint32_t fb = smem_u32(&full_bar[st]);
+                            mbar_expect_tx(&full_bar[st], (uint32_t)(item.nx * kXTile) + ybytes);
+                            bulk_load(sa, ga + ((int64_t)kb * L + l) * kXTile, kXTile, fb);
+                            if (item.nx == 2) bulk_load(sa + kXTile, ga + xt + ((int64_t)kb * L + l) * kXTile, kXTile, fb);
+                            bulk_load(sa + 2 * kXTile, gb + ((int64_t)kb * L + l) * ybytes, ybytes, fb);
+                            armed[st] = (int)ph;
+                            if (++st == stages) { st = 0; ph ^= 1; }
+                        }
+                    }
+                }
+            }
+            if (!ok) {
+                abort_s = 1;
+                atomicExch(err, 7);
+                volatile int never = 0;
+                for (int i = 0; i < stages; i++)
+                    if (armed[i] >= 0) (void)mbar_wait(&full_bar[i], (uint32_t)armed[i], &never);
+            }
+        }
+    } else if (warp == 5) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int st = 0;
+            uint32_t ph = 0;
+            uint32_t fills = 0;                      // accumulator fills so far (one per item and modulus)
+            bool ok = true;
+            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+                const DCrtItem item = items[it];
+                const uint32_t idesc = instr_desc_i8(item.nt);
+                for (int l = 0; l < L && ok; l++) {
+                    if (fills > 0) {                 // the epilogue has read the previous fill
+                        if (!mbar_wait(&acce_bar[0], (fills - 1) & 1, &abort_s)) { ok = false; break; }
+                    }
+                    tc_fence_after();
+                    uint32_t acc = 0;
+                    for (int ti = item.t_begin; ti < item.t_end && ok; ti++) {
+                        const int nkb = panels[tasks[ti].px].K_pad / kKB;
+                        for (int kb = 0; kb < nkb; kb++) {
+                            if (!mbar_wait(&full_bar[st], ph, &abort_s)) { ok = false; break; }
+                            tc_fence_after();
+                            const uint32_t a0 = smem0 + st * kStageBytes;
+                            const uint64_t db = smem_desc_kmajor(a0 + 2 * kXTile);
+                            umma_i8(tmem, smem_desc_kmajor(a0), db, idesc, acc);
+                            if (item.nx == 2) umma_i8(tmem + kMaxNt, smem_desc_kmajor(a0 + kXTile), db, idesc, acc);
+                            acc = 1;
+                            umma_commit(&empty_bar[st]);
+                            if (++st == stages) { st = 0; ph ^= 1; }
+                        }
+                    }
+                    if (!ok) break;
+                    umma_commit(&accf_bar[0]);
+                    fills++;
+                }
+            }
+            if (!ok) {
+                abort_s = 1;
+                atomicExch(err, 7);
+                volatile int never = 0;
+                umma_commit(&drain_bar);
+                (void)mbar_wait(&drain_bar, 0, &never);
+            }
+        }
+    } else {
+        // ------------------------------------------------ epilogue (warps 0-3)
+        const int row = warp * 32 + lane;                         // TMEM lane == tile row
+        uint32_t fills = 0;
+        bool ok = true;
+        for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+            const DCrtItem item = items[it];
+            for (int l = 0; l < L; l++) {
+                ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[0], fills & 1, &abort_s));
+                if (!ok) break;
+                tc_fence_after();
+                const double m = (double)cp.m[l], minv = cp.minv_d[l];
+                const int mi = cp.m[l];
+                for (int xh = 0; xh < item.nx; xh++) {
+                    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + xh * kMaxNt;
+                    uint8_t *orow = out + item.res_off + ((int64_t)(l * item.nx + xh) * kXRows + row) * item.nt;
+                    for (int c0 = 0; c0 < item.nt; c0 += 16) {
+                        uint32_t v[16];
+                        tmem_ld16(taddr + (uint32_t)c0, v);
+                        tmem_wait_ld();
+                        uint32_t w[16];
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            // exact quotient (|x| < 2^31): r in [-(m-1)/2, (m-1)/2] or +-128 for m = 256
+                            const double x = (double)(int32_t)v[j];
+                            const double q = fma(x, minv, kMagicD) - kMagicD;
+                            const int r = __double2loint(fma(-q, m, x) + kMagicD);
+                            w[j] = (uint32_t)(r < 0 ? r + mi : r);            // [0, m)
+                        }
+                        *reinterpret_cast<uint4 *>(orow + c0) =
+                            make_uint4(pack4(w[0], w[1], w[2], w[3]), pack4(w[4], w[5], w[6], w[7]),
+                                       pack4(w[8], w[9], w[10], w[11]), pack4(w[12], w[13], w[14], w[15]));
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce_bar[0]);
+                fills++;
+            }
+        }
+        if (!ok) { abort_s = 1; atomicExch(err, 7); }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" :: "r"(tmem) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------- recombination
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+
+constexpr int kCombCols = 16;                       // tile columns staged per pass
+
+// One CTA per work item at a time: residues of 16 columns staged in shared
+// memory, then one thread per element runs Garner and writes C.
+template<int L>
+__global__ void __launch_bounds__(256)
+crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restrict__ items, int32_t nitems,
+                   const DCBlock *__restrict__ cblks, const uint8_t *__restrict__ out,
+                   const int32_t *__restrict__ gidx, const int32_t *__restrict__ ex,
+                   const int32_t *__restrict__ ey, double *__restrict__ C, int32_t add, const CrtParams cp) {
+    __shared__ __align__(16) uint8_t sres[L][kXRows][kCombCols];
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const DCrtItem item = items[it];
+        const DCBlock &cb = cblks[item.cblk];
+        const int xext = cp.swap ? cb.N : cb.M, yext = cp.swap ? cb.M : cb.N;
+        const int yc = min(item.nt, yext - item.y0);
+        const int32_t *gyp = gidx + panels[item.gy].g_off + item.y0;
+        for (int xh = 0; xh < item.nx; xh++)
+        for (int c0 = 0; c0 < yc; c0 += kCombCols) {
+            const int xb = item.x0 + xh * kXRows;                    // first row of this half
+            const int xr = min(kXRows, xext - xb);
+            const int32_t *gxp = gidx + panels[item.gx].g_off + xb;
+            __syncthreads();
+            for (int i = threadIdx.x; i < L * kXRows; i += blockDim.x) {
+                const int l = i / kXRows, r = i - l * kXRows;
+                cp_async16(&sres[l][r][0],
+                           out + item.res_off + ((int64_t)(l * item.nx + xh) * kXRows + r) * item.nt + c0);
+            }
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+            __syncthreads();
+            for (int e = threadIdx.x; e < kXRows * kCombCols; e += blockDim.x) {
+                int r, c;
+                if (cp.swap) { r = e & (kXRows - 1); c = e >> 7; }      // C rows along the tile columns
+                else { c = e & (kCombCols - 1); r = e >> 4; }
+                if (r >= xr || c0 + c >= yc) continue;
+                // Garner: balanced mixed-radix digits v_i of the residues
+                float v[L];
+#pragma unroll
+                for (int i = 0; i < L; i++) {
+                    const float mi = (float)cp.m[i], minv = cp.minv_f[i];
+                    float t = (float)sres[i][r][c];
+#pragma unroll
+                    for (int j = 0; j < i; j++) {
+                        t = (t - v[j]) * (float)cp.inv[i][j];
+                        t = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);   // t mod m_i, |t| <= m_i/2 + 1
+                    }
+                    // exact balanced digit in (-m_i/2, m_i/2]
+                    t = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);
+                    if (t > 0.5f * mi) t -= mi;
+                    if (t <= -0.5f * mi) t += mi;
+                    v[i] = t;
+                }
+                double X = (double)v[L - 1];
+#pragma unroll
+                for (int i = L - 2; i >= 0; i--) X = fma(X, (double)cp.m[i], (double)v[i]);
+                const int gx = gxp[r], gy = gyp[c0 + c];
+                const int e2 = ex[gx] + ey[gy] - 2 * cp.P;
+                const double val = cb.scale * ldexp(X, max(e2, -2200));
+                const int xi = xb + r, yi = item.y0 + c0 + c;
+                const int m = cp.swap ? yi : xi, n = cp.swap ? xi : yi;
+                double *dst = C + cb.c_off + mixed_offset(m, cb.nm, cb.mext, cb.mc_str) +
+                              mixed_offset(n, cb.nn, cb.next, cb.nc_str);
+                if (add) *dst += val;
+                else *dst = val;
+            }
+        }
+    }
+}
+
+int g_crt_nsm = 0;
+
+int num_sms() {
+    if (g_crt_nsm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_crt_nsm, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return g_crt_nsm;
+}
+
+}  // namespace
+
+cudaError_t launch_crt_exponents(const DCrtPanel *panels, int32_t npanels, int32_t max_rows, int32_t nx,
+                                 int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
+                                 int32_t *ey, cudaStream_t s) {
+    if (npanels <= 0) return cudaSuccess;
+    crt_fill_kernel<<<64, 256, 0, s>>>(ex, nx, kNoExp);
+    crt_fill_kernel<<<64, 256, 0, s>>>(ey, ny, kNoExp);
+    dim3 grid((max_rows + 31) / 32, npanels < 65535 ? npanels : 65535);
+    crt_exp_kernel<<<grid, 256, 0, s>>>(panels, npanels, a, b, gidx, ex, ey);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_residues(const DCrtPanel *panels, int32_t npanels, int32_t max_rows,
+                                const double *a, const double *b, const int32_t *gidx, const int32_t *ex,
+                                const int32_t *ey, uint8_t *res, const CrtParams &cp, cudaStream_t s) {
+    if (npanels <= 0) return cudaSuccess;
+    dim3 grid((max_rows + 31) / 32, npanels < 65535 ? npanels : 65535);
+    switch (cp.L) {
+#define CASE_L(n) case n: crt_res_kernel<n><<<grid, 256, 0, s>>>(panels, npanels, a, b, gidx, ex, ey, res, cp); break;
+    CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
+#undef CASE_L
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
+                            const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp,
+                            int32_t *err, cudaStream_t s) {
+    if (nitems <= 0) return cudaSuccess;
+    int stages = (200 * 1024) / kStageBytes;
+    if (stages > kMaxStages) stages = kMaxStages;
+    const size_t smem = (size_t)stages * kStageBytes + 1024;
+    cudaError_t e = cudaFuncSetAttribute(crt_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = nitems < num_sms() ? nitems : num_sms();
+    crt_gemm_kernel<<<grid, kGemmThreads, smem, s>>>(panels, res, tasks, items, nitems, out, cp, stages, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
+                               const DCBlock *cblks, const uint8_t *out, const int32_t *gidx, const int32_t *ex,
+                               const int32_t *ey, double *c, int32_t add, const CrtParams &cp, cudaStream_t s) {
+    if (nitems <= 0) return cudaSuccess;
+    const int grid = nitems < 8 * num_sms() ? nitems : 8 * num_sms();
+    switch (cp.L) {
+#define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, out, gidx, ex, ey, c, add, cp); break;
+    CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
+#undef CASE_L
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace ltg

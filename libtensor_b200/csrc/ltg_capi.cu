@@ -6,6 +6,7 @@
 // message for ltg_last_error().
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -144,10 +145,23 @@ struct OzExec {
     ~OzExec() { if (err_host) cudaFreeHost(err_host); }
 };
 
+// Device arrays of one modular split-precision contraction (crt.cu).
+struct CrtExec {
+    CrtParams cp{};
+    int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0;
+    DevBuf panels, tasks, items, cblks, gidx, ex, ey, res, out, err;
+    std::vector<std::pair<int64_t, int64_t>> zero_ranges;
+    std::vector<int64_t> sched_slots;
+    int32_t *err_host = nullptr;
+    ~CrtExec() { if (err_host) cudaFreeHost(err_host); }
+};
+
 struct ltg_plan {
     ltg_ctx *ctx = nullptr;
     std::map<std::tuple<uint64_t, double, double, double, int, double, int, int>,
              std::unique_ptr<OzExec>> oz;
+    std::map<std::tuple<uint64_t, double, double, double, int, double, int>,
+             std::unique_ptr<CrtExec>> crt;
     ltg_bt *a = nullptr, *b = nullptr;
     int forced_tile = -1;         // >= 0: every C block uses this tile shape
     std::map<std::pair<int64_t, int64_t>, int> tile_override;   // autotuned (M, N) -> shape
@@ -625,6 +639,295 @@ OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, doubl
     LTG_CUDA(cudaStreamSynchronize(s));
     OzExec *raw = ex.get();
     pl->oz[key] = std::move(ex);
+    return raw;
+}
+
+// ------------------------------------------------------------ modular split precision
+
+// Pairwise coprime moduli <= 256, largest first (residues fit INT8).
+const int32_t kCrtModuli[kCrtMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233,
+                                           229, 227, 223, 217, 211, 199, 197, 193};
+
+int32_t mod_inverse(int64_t a, int64_t m) {
+    int64_t t = 0, nt = 1, r = m, nr = ((a % m) + m) % m;
+    while (nr != 0) {
+        int64_t q = r / nr, tmp;
+        tmp = t - q * nt; t = nt; nt = tmp;
+        tmp = r - q * nr; r = nr; nr = tmp;
+    }
+    if (r != 1) throw error(kErrState, "moduli not coprime");
+    return (int32_t)(t < 0 ? t + m : t);
+}
+
+CrtParams crt_params(int L, int P, bool swap) {
+    CrtParams cp{};
+    cp.L = L; cp.P = P; cp.swap = swap ? 1 : 0;
+    for (int i = 0; i < L; i++) {
+        const int32_t m = kCrtModuli[i];
+        cp.m[i] = m;
+        cp.minv_f[i] = 1.0f / (float)m;
+        cp.minv_d[i] = 1.0 / (double)m;
+        for (int j = 0; j < i; j++) cp.inv[i][j] = mod_inverse(kCrtModuli[j], m);
+        int64_t pw = 1;
+        for (int t = 0; t < 4; t++) {
+            pw = (pw * 2048) % m;
+            cp.pow11[i][t] = (int32_t)pw;
+        }
+    }
+    return cp;
+}
+
+// Tile width of the MMA N operand for a panel of `rows` rows: tiles of at
+// most 256 rows, balanced, in multiples of 16.
+int32_t crt_tile_width(int64_t rows) {
+    const int64_t nt = (rows + 255) / 256;
+    const int64_t w = (rows + nt - 1) / nt;
+    return (int32_t)std::min<int64_t>(256, (w + 15) / 16 * 16);
+}
+
+// Global index of every row (or column) of a C block: the C element's dense
+// coordinates over the dims of that side, linearised with full extents.  The
+// exponent tables are indexed by it, so that all panels feeding one row of C
+// share its scaling.
+struct CrtSideMap {
+    std::vector<int> dims;       // C dims of this side
+    std::vector<int64_t> gstr;   // strides of the linearised index
+    int64_t size = 1;
+};
+
+void crt_global_index(const BlockTensorHost &ch, const CrtSideMap &sm, int64_t c_off, const SubDims &sub,
+                      std::map<int64_t, int64_t> &slot_of_off, std::vector<int32_t> &out) {
+    auto f = slot_of_off.find(c_off);
+    if (f == slot_of_off.end()) throw error(kErrState, "C block offset without a slot");
+    const int n = ch.bis.n;
+    int64_t bidx[kMaxOrder], bext[kMaxOrder], bstr[kMaxOrder];
+    ch.bis.unabs(ch.blk_abs[f->second], bidx);
+    ch.bis.block_dims(bidx, bext);
+    int64_t acc = 1;
+    for (int d = n - 1; d >= 0; d--) { bstr[d] = acc; acc *= bext[d]; }
+    const int64_t total = sub.total();
+    out.resize(total);
+    for (int64_t r = 0; r < total; r++) {
+        int64_t off = 0, q = r;
+        for (int i = sub.n - 1; i >= 0; i--) {
+            off += (q % sub.ext[i]) * sub.s1[i];
+            q /= sub.ext[i];
+        }
+        int64_t g = 0;
+        for (size_t k = 0; k < sm.dims.size(); k++) {
+            const int d = sm.dims[k];
+            const int64_t local = (off / bstr[d]) % bext[d];
+            g += (ch.bis.starts[d][bidx[d]] + local) * sm.gstr[k];
+        }
+        out[r] = (int32_t)g;
+    }
+}
+
+CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, double kc, int add, double d) {
+    auto key = std::make_tuple(c->uid, ka, kb, kc, add, add ? d : 0.0, L);
+    auto it = pl->crt.find(key);
+    if (it != pl->crt.end()) return it->second.get();
+    if (pl->ctx->capturing) throw error(kErrState, "contraction not prepared before graph capture: call it once outside the capture");
+    if (L < 8 || L > kCrtMaxModuli) throw error(kErrBadArg, "modulus count must be 8..16");
+    const double kabc = ka * kb * kc;
+    if (kabc == 0.0) throw error(kErrUnsupported, "zero contraction coefficient");
+
+    std::vector<GemmTask> tasks;
+    std::vector<CBlockTask> cbt;
+    contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    const Contraction &ct = pl->plan.contr;
+    const BlockTensorHost &ch = c->h;
+    // C dims of each side: connected to A (rows) or to B (columns)
+    CrtSideMap sm[2];
+    for (int i = 0; i < ct.NC(); i++) sm[ct.conn[i] < ct.NC() + ct.NA() ? 0 : 1].dims.push_back(i);
+    for (int s = 0; s < 2; s++) {
+        sm[s].gstr.resize(sm[s].dims.size());
+        for (int k = (int)sm[s].dims.size() - 1; k >= 0; k--) {
+            sm[s].gstr[k] = sm[s].size;
+            sm[s].size *= ch.bis.dims[sm[s].dims[k]];
+        }
+        if (sm[s].size > ((int64_t)1 << 27)) throw error(kErrUnsupported, "C side too large for the modular scaling tables");
+    }
+    std::map<int64_t, int64_t> slot_of_off;
+    for (size_t sl = 0; sl < ch.blk_off.size(); sl++) slot_of_off[ch.blk_off[sl]] = (int64_t)sl;
+
+    // orientation: the C side with the larger extents goes to the MMA M side
+    // (128-row tiles) when that pads less
+    double pad_keep = 0, pad_swap = 0;
+    for (const CBlockTask &b : cbt) {
+        auto padded = [](int64_t x, int64_t y) {
+            const int32_t nt = crt_tile_width(y);
+            return (double)((x + 127) / 128 * 128) * (double)((y + nt - 1) / nt * nt);
+        };
+        pad_keep += padded(b.M, b.N);
+        pad_swap += padded(b.N, b.M);
+    }
+    const bool swap = pad_swap < pad_keep;
+    // integer coefficients ride on the operand with the smaller arena
+    const int coef_src = pl->a->h.total_elems <= pl->b->h.total_elems ? 0 : 1;
+
+    // panels by (operand, block, row and k mappings, coefficient); one key can
+    // hold several panels when the same rows feed different rows of C
+    std::map<std::vector<int64_t>, std::vector<int32_t>> pidx;
+    std::vector<DCrtPanel> panels;
+    std::vector<int32_t> gidx;
+    int64_t res_bytes = 0;
+    int32_t max_rows = 0;
+    std::vector<int32_t> grow;
+    // panel of operand src (0: A rows = C side 0, 1: B rows = C side 1)
+    auto panel_of = [&](int src, int64_t off, const SubDims &rows, const SubDims &k, bool kb_second, int32_t coef,
+                        int64_t c_off) {
+        const int side = (src == 1) == swap ? 0 : 1;     // 0: MMA M operand
+        std::vector<int64_t> key = {src, off, rows.n, k.n, coef};
+        for (int i = 0; i < rows.n; i++) { key.push_back(rows.ext[i]); key.push_back(rows.s0[i]); }
+        for (int i = 0; i < k.n; i++) { key.push_back(k.ext[i]); key.push_back(kb_second ? k.s1[i] : k.s0[i]); }
+        // global indices of the panel rows, from this C block
+        crt_global_index(ch, sm[src], c_off, rows, slot_of_off, grow);
+        std::vector<int32_t> &cands = pidx[key];
+        for (int32_t id : cands)
+            if (std::equal(grow.begin(), grow.end(), gidx.begin() + panels[id].g_off)) return id;
+        DCrtPanel p;
+        std::memset(&p, 0, sizeof(p));
+        p.src = src;
+        p.side = side;
+        p.src_off = off;
+        p.rows = (int32_t)rows.total();
+        p.K = (int32_t)k.total();
+        p.tr = side == 0 ? 128 : crt_tile_width(p.rows);
+        p.rows_pad = (p.rows + p.tr - 1) / p.tr * p.tr;
+        p.K_pad = (p.K + 31) / 32 * 32;
+        p.coef = coef;
+        pack_sub(rows, p.nr, p.rext, p.rstr, nullptr);
+        SubDims kk = k;
+        if (kb_second) for (int i = 0; i < kk.n; i++) kk.s0[i] = kk.s1[i];
+        pack_sub(kk, p.nk, p.kext, p.kstr, nullptr);
+        p.res_off = res_bytes;
+        res_bytes += ((int64_t)L * p.rows_pad * p.K_pad + 1023) / 1024 * 1024;
+        p.g_off = (int32_t)gidx.size();
+        gidx.insert(gidx.end(), grow.begin(), grow.end());
+        max_rows = std::max(max_rows, p.rows_pad);
+        const int32_t id = (int32_t)panels.size();
+        panels.push_back(p);
+        cands.push_back(id);
+        return id;
+    };
+    std::vector<DCrtTask> dt(tasks.size());
+    int64_t max_sum = 1, max_coef = 1;
+    for (const CBlockTask &b : cbt) {
+        int64_t sum = 0;
+        for (int32_t t = b.t_begin; t < b.t_end; t++) {
+            const GemmTask &g = tasks[t];
+            const double cr = g.coeff / kabc;
+            const int64_t ci = (int64_t)std::llround(cr);
+            if (ci == 0 || std::fabs(cr - (double)ci) > 1e-9 || std::llabs(ci) > 64)
+                throw error(kErrUnsupported, "modular split precision needs small integer pair coefficients");
+            const int32_t ca = coef_src == 0 ? (int32_t)ci : 1, cbf = coef_src == 1 ? (int32_t)ci : 1;
+            const int32_t pa = panel_of(0, g.a_off, g.m, g.k, false, ca, b.c_off);
+            const int32_t pb = panel_of(1, g.b_off, g.n, g.k, true, cbf, b.c_off);
+            if (panels[pa].K_pad != panels[pb].K_pad) throw error(kErrState, "panel k extents differ");
+            dt[t].px = swap ? pb : pa;
+            dt[t].py = swap ? pa : pb;
+            sum += std::llabs(ci) * (int64_t)g.k.total();
+            max_coef = std::max<int64_t>(max_coef, std::llabs(ci));
+        }
+        max_sum = std::max(max_sum, sum);
+    }
+    // exact INT32 accumulation of |residue| <= 128 products, and the CRT range
+    if (max_sum * 128 * 128 >= ((int64_t)1 << 31))
+        throw error(kErrUnsupported, "contraction too long for exact modular accumulation");
+    double log2M = 0;
+    for (int i = 0; i < L; i++) log2M += std::log2((double)kCrtModuli[i]);
+    // |c * x * 2^(P - e)| < 2^50 keeps every residue computation exact (the
+    // FP64 round-to-integer trick needs magnitudes below 2^51)
+    const int pcap = 50 - (int)std::ceil(std::log2((double)max_coef));
+    const int P = std::min(pcap, (int)std::floor((log2M - 1.0 - std::log2((double)max_sum)) / 2.0));
+    if (P < 24) throw error(kErrUnsupported, "too few moduli for this contraction");
+
+    std::unique_ptr<CrtExec> ex(new CrtExec());
+    ex->cp = crt_params(L, P, swap);
+    ex->nx = (int32_t)sm[swap ? 1 : 0].size;
+    ex->ny = (int32_t)sm[swap ? 0 : 1].size;
+
+    std::vector<DCBlock> dc(cbt.size());
+    const double post = (add ? d : 1.0) * kabc;
+    for (size_t e = 0; e < cbt.size(); e++) {
+        const CBlockTask &b = cbt[e];
+        DCBlock &x = dc[e];
+        std::memset(&x, 0, sizeof(x));
+        x.c_off = b.c_off;
+        x.scale = post;
+        x.M = (int32_t)b.M; x.N = (int32_t)b.N;
+        pack_sub(b.cm, x.nm, x.mext, x.mc_str, nullptr);
+        pack_sub(b.cn, x.nn, x.next, x.nc_str, nullptr);
+        x.t_begin = b.t_begin; x.t_end = b.t_end;
+    }
+    // work items: 128 x nt tiles, costliest first
+    std::vector<std::pair<double, DCrtItem>> iv;
+    int64_t out_bytes = 0;
+    for (size_t e = 0; e < cbt.size(); e++) {
+        const CBlockTask &b = cbt[e];
+        if (b.t_end <= b.t_begin) continue;
+        const DCrtTask &t0 = dt[b.t_begin];
+        const int32_t nt = panels[t0.py].tr;
+        const int64_t xext = swap ? b.N : b.M, yext = swap ? b.M : b.N;
+        for (int64_t x0 = 0; x0 < xext; x0 += 256)
+            for (int64_t y0 = 0; y0 < yext; y0 += nt) {
+                DCrtItem it;
+                std::memset(&it, 0, sizeof(it));
+                it.cblk = (int32_t)e;
+                it.x0 = (int32_t)x0; it.y0 = (int32_t)y0;
+                it.nt = nt;
+                it.nx = x0 + 128 < xext ? 2 : 1;
+                it.t_begin = b.t_begin; it.t_end = b.t_end;
+                it.gx = t0.px; it.gy = t0.py;
+                it.res_off = out_bytes;
+                out_bytes += (int64_t)L * it.nx * 128 * nt;
+                iv.push_back({b.kflops * nt * it.nx, it});
+            }
+    }
+    std::stable_sort(iv.begin(), iv.end(), [](const std::pair<double, DCrtItem> &x, const std::pair<double, DCrtItem> &y) {
+        return x.first > y.first;
+    });
+    std::vector<DCrtItem> items;
+    for (auto &q : iv) items.push_back(q.second);
+    // every pair of an item shares the tile width of its N operand
+    for (const DCrtItem &it : items)
+        for (int32_t t = it.t_begin; t < it.t_end; t++)
+            if (panels[dt[t].py].tr != it.nt || panels[dt[t].px].tr != 128)
+                throw error(kErrState, "inconsistent tile widths within a C block");
+
+    cudaStream_t s = pl->ctx->stream;
+    ex->npanels = (int32_t)panels.size();
+    ex->nitems = (int32_t)items.size();
+    ex->max_rows = max_rows;
+    ex->res.alloc(std::max<int64_t>(res_bytes, 1024));
+    ex->out.alloc(std::max<int64_t>(out_bytes, 1024));
+    ex->ex.alloc(std::max<int64_t>(ex->nx, 1) * sizeof(int32_t));
+    ex->ey.alloc(std::max<int64_t>(ex->ny, 1) * sizeof(int32_t));
+    upload_vec(ex->panels, panels, s);
+    upload_vec(ex->tasks, dt, s);
+    upload_vec(ex->items, items, s);
+    upload_vec(ex->cblks, dc, s);
+    upload_vec(ex->gidx, gidx, s);
+    ex->err.alloc(sizeof(int32_t));
+    LTG_CUDA(cudaMemsetAsync(ex->err.p, 0, sizeof(int32_t), s));
+    LTG_CUDA(cudaMallocHost(&ex->err_host, sizeof(int32_t)));
+    *ex->err_host = 0;
+    std::vector<char> in_sched(c->h.blk_abs.size(), 0);
+    for (int64_t cabs : pl->plan.schedule) {
+        int64_t sl = c->h.slot_of[cabs];
+        in_sched[sl] = 1;
+        ex->sched_slots.push_back(sl);
+    }
+    for (size_t sl = 0; sl < in_sched.size(); sl++) {
+        if (in_sched[sl]) continue;
+        int64_t b0 = c->h.blk_off[sl], b1 = b0 + c->h.blk_size[sl];
+        if (!ex->zero_ranges.empty() && ex->zero_ranges.back().second >= b0 - 3) ex->zero_ranges.back().second = b1;
+        else ex->zero_ranges.push_back({b0, b1});
+    }
+    LTG_CUDA(cudaStreamSynchronize(s));
+    CrtExec *raw = ex.get();
+    pl->crt[key] = std::move(ex);
     return raw;
 }
 
@@ -1306,6 +1609,43 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
         if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
         ltg_ctx *ctx = plan->ctx;
         cudaStream_t s = ctx->stream;
+        if (mode == LTG_MODE_OZAKI_CRT) {
+            CrtExec *cx = prepare_crt(plan, c, nslices > 0 ? nslices : 13, ka, kb, kc, add, d);
+            if (*cx->err_host != 0) {
+                int code = *cx->err_host;
+                *cx->err_host = 0;
+                throw error(code == kErrTimeout ? kErrTimeout : kErrCuda,
+                            "a bounded device wait of the modular split-precision kernel gave up");
+            }
+            if (!add)
+                for (auto &r : cx->zero_ranges)
+                    LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
+            const double *pa = plan->a->arena.as<double>(), *pb = plan->b->arena.as<double>();
+            TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
+            LTG_CUDA(launch_crt_exponents(cx->panels.as<DCrtPanel>(), cx->npanels, cx->max_rows, cx->nx, cx->ny,
+                                          pa, pb, cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), s));
+            LTG_CUDA(launch_crt_residues(cx->panels.as<DCrtPanel>(), cx->npanels, cx->max_rows, pa, pb,
+                                         cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
+                                         cx->res.as<uint8_t>(), cx->cp, s));
+            t_split.done();
+            TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
+            LTG_CUDA(launch_crt_gemm(cx->panels.as<DCrtPanel>(), cx->res.as<uint8_t>(), cx->tasks.as<DCrtTask>(),
+                                     cx->items.as<DCrtItem>(), cx->nitems, cx->out.as<uint8_t>(), cx->cp,
+                                     cx->err.as<int32_t>(), s));
+            t_gemm.done();
+            TimedLaunch t_comb(ctx, LTG_KERNEL_OZ_COMBINE);
+            LTG_CUDA(launch_crt_combine(cx->panels.as<DCrtPanel>(), cx->items.as<DCrtItem>(), cx->nitems,
+                                        cx->cblks.as<DCBlock>(), cx->out.as<uint8_t>(), cx->gidx.as<int32_t>(),
+                                        cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), c->arena.as<double>(), add,
+                                        cx->cp, s));
+            t_comb.done();
+            ctx->launches += 6;
+            if (!ctx->capturing)
+                LTG_CUDA(cudaMemcpyAsync(cx->err_host, cx->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
+            for (int64_t sl : cx->sched_slots) c->h.nonzero[sl] = 1;
+            return;
+        }
         if (mode != LTG_MODE_PLAIN_FP64) {
             if (mode < LTG_MODE_OZAKI_BF16 || mode > LTG_MODE_OZAKI_INT8) throw error(kErrBadArg, "unknown mode");
             int S = nslices > 0 ? nslices : (mode == LTG_MODE_OZAKI_FP8 ? 8 : 7);

@@ -69,6 +69,59 @@ struct DOzTask {
     double coeff;                 // relative coefficient of the pair
 };
 
+// ---------------------------------------------------------------- CRT (modular) split precision
+
+constexpr int kCrtMaxModuli = 16;
+
+// One operand panel of the modular contraction: the matricised view (rows x K)
+// of a canonical block, with the pair's integer coefficient folded in, scaled
+// row by row to integers and stored as its residues modulo each modulus, in
+// shared-memory tile images (per tile of tr rows, 32-byte k block, modulus).
+struct DCrtPanel {
+    int64_t src_off;              // FP64 source block offset (elements)
+    int64_t res_off;              // byte offset of the tile images
+    int32_t src;                  // 0: A arena, 1: B arena
+    int32_t side;                 // 0: MMA M operand (128-row tiles), 1: MMA N operand
+    int32_t rows, K, rows_pad, K_pad;
+    int32_t tr;                   // rows per tile image (128, or the N tile width)
+    int32_t coef;                 // integer coefficient folded into the residues
+    int32_t g_off;                // first of this panel's rows in the global row-index array
+    int32_t nr, nk;
+    int32_t rext[kDevMaxSub], rstr[kDevMaxSub];
+    int32_t kext[kDevMaxSub], kstr[kDevMaxSub];
+};
+
+struct DCrtTask {
+    int32_t px, py;               // MMA M-side and N-side panels of one pair
+};
+
+// One CTA work item: an (nx * 128) x nt tile of one C block (in MMA
+// orientation: rows from the M-side operand, columns from the N-side
+// operand); the nx <= 2 row tiles share every N-side operand tile.
+struct DCrtItem {
+    int32_t cblk;
+    int32_t x0, y0;               // first M-side row, first N-side row
+    int32_t nt;                   // N tile width (multiple of 16, <= 256)
+    int32_t nx;                   // 128-row tiles (1 or 2)
+    int32_t t_begin, t_end;       // pairs (DCrtTask range)
+    int32_t gx, gy;               // panels whose global row indices label the tile
+    int32_t pad;
+    int64_t res_off;              // residue tile output: [modulus][nx * 128][nt] bytes
+};
+
+// Moduli and the constants of Garner's mixed-radix reconstruction.
+struct CrtParams {
+    int32_t L;                    // number of moduli
+    int32_t P;                    // bits of the scaled integer operands
+    int32_t swap;                 // 1: MMA M side = the C columns (B operand)
+    int32_t pad;
+    int32_t m[kCrtMaxModuli];     // moduli, pairwise coprime, <= 256
+    int32_t inv[kCrtMaxModuli][kCrtMaxModuli];   // inv[i][j] = m_j^-1 mod m_i (j < i)
+    float minv_f[kCrtMaxModuli];  // 1 / m_i
+    double minv_d[kCrtMaxModuli];
+    int32_t pow11[kCrtMaxModuli][4];   // 2^(11 t) mod m_i
+};
+
 // ---------------------------------------------------------------- element-wise
 
 constexpr int kMaxTerms = 8;
@@ -182,6 +235,21 @@ cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices
 // Per kind: first-slice bits, further-slice bits, element bytes, k elements
 // per 64-byte k block, bound of one slice product.
 void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod);
+
+// Modular split precision: exponent pass, residue pass, modular products,
+// Garner recombination into FP64 C.
+cudaError_t launch_crt_exponents(const DCrtPanel *panels, int32_t npanels, int32_t max_rows,
+    int32_t nx, int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
+    int32_t *ey, cudaStream_t s);
+cudaError_t launch_crt_residues(const DCrtPanel *panels, int32_t npanels, int32_t max_rows,
+    const double *a, const double *b, const int32_t *gidx, const int32_t *ex, const int32_t *ey,
+    uint8_t *res, const CrtParams &cp, cudaStream_t s);
+cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
+    const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp, int32_t *err,
+    cudaStream_t s);
+cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
+    const DCBlock *cblks, const uint8_t *out, const int32_t *gidx, const int32_t *ex,
+    const int32_t *ey, double *c, int32_t add, const CrtParams &cp, cudaStream_t s);
 
 // Element-wise transfer kernels.  max_terms bounds nterms and tile_bytes the
 // shared-memory tiles of any tiled-mode job.

@@ -4,7 +4,7 @@ stated relative error (block max-norm) of the reference's FP64 result."""
 import numpy as np
 import pytest
 
-from libtensor_b200.core import (Context, MODE_OZAKI_BF16, MODE_OZAKI_FP8, MODE_OZAKI_INT8,
+from libtensor_b200.core import (Context, MODE_OZAKI_BF16, MODE_OZAKI_CRT, MODE_OZAKI_FP8, MODE_OZAKI_INT8,
                                  btod_contract2, contraction2)
 from oracle import refapi as R
 from tests.cases import cases
@@ -17,13 +17,19 @@ CASES = [c for c in cases() if not c.symmetry_error]
 # (mode, slices, bound on the block-relative error).  INT8 slices carry 7
 # bits (6 for the first), BF16 slices are given the same 7 bits (exact
 # partial sums in FP32), FP8 E4M3 slices 5 bits (4 for the first); the bounds
-# are a few units of the dropped tail 2^-(b0 + b(S-1)) times sqrt(K).
+# are a few units of the dropped tail 2^-(b0 + b(S-1)) times sqrt(K).  The
+# modular mode with L moduli rounds each operand to P bits, P = floor((log2 M
+# - 1 - log2(sum_p |c_p| K_p)) / 2) (M the product of the moduli, at most 45):
+# P = 45 for 13 and 16 moduli on these cases, about 31 for 9.
 MODES = [
     (MODE_OZAKI_INT8, 7, 1e-12),
     (MODE_OZAKI_INT8, 6, 1e-10),
     (MODE_OZAKI_INT8, 3, 1e-3),
     (MODE_OZAKI_BF16, 7, 1e-12),
     (MODE_OZAKI_FP8, 8, 1e-9),
+    (MODE_OZAKI_CRT, 13, 1e-12),
+    (MODE_OZAKI_CRT, 16, 1e-12),
+    (MODE_OZAKI_CRT, 9, 1e-7),
 ]
 
 
@@ -56,7 +62,8 @@ def test_split_precision_matches_reference(gctx, case, mode, S, tol):
     assert err <= tol, sorted(errs, key=lambda e: -e[1])[:3]
 
 
-def test_split_precision_add_mode(gctx):
+@pytest.mark.parametrize("mode,S", [(MODE_OZAKI_INT8, 7), (MODE_OZAKI_CRT, 13)], ids=["int8-S7", "crt-L13"])
+def test_split_precision_add_mode(gctx, mode, S):
     case = CASES[0]
     A, ra, _ = seeded_pair(gctx, case.a, 3, case.a_scale)
     B, rb, _ = seeded_pair(gctx, case.b, 4, case.b_scale)
@@ -68,6 +75,6 @@ def test_split_precision_add_mode(gctx):
     C, RC = op.make_result(), rop.make_result()
     op.perform(C)
     rop.perform(RC)
-    op.perform(C, 0.5, mode=MODE_OZAKI_INT8, nslices=7)
+    op.perform(C, 0.5, mode=mode, nslices=S)
     rop.perform(RC, 0.5)
     assert max_rel_block_error(block_errors(C, C.download(), RC, None)) <= 1e-12
