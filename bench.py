@@ -51,7 +51,8 @@ def parse():
     # at <= 1e-12, with the plain FP64 DMMA path timed on the same workload.
     p.add_argument("--workload", default="ladder-split", choices=sorted(WORKLOADS) + list(TRANSFER_WORKLOADS))
     p.add_argument("--mode", default="ozaki-int8", choices=sorted(MODES))
-    p.add_argument("--nslices", type=int, default=7)
+    p.add_argument("--nslices", type=int, default=None,
+                   help="slices (moduli for ozaki-crt); default 7, 8 for FP8, 13 for the modular mode")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
@@ -60,6 +61,8 @@ def parse():
     a = p.parse_args()
     if a.mode == "plain":
         a.nslices = 0
+    elif a.nslices is None:
+        a.nslices = {"ozaki-fp8": 8, "ozaki-crt": 13}.get(a.mode, 7)
     return a
 
 

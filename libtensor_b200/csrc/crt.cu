@@ -28,6 +28,8 @@
 // MMA issuer.  Operand tiles are whole tile images moved by 1-D
 // cp.async.bulk (no tensor maps, no multicast); every mbarrier wait is
 // bounded in time and reports through *err.
+#include <type_traits>
+
 #include "ltg_device.cuh"
 
 namespace ltg {
@@ -44,6 +46,41 @@ constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s per barrier wait
 constexpr double kMagicD = 6755399441055744.0;      // 1.5 * 2^52: round-to-integer constant
 constexpr float kMagicF = 12582912.0f;              // 1.5 * 2^23
 constexpr int32_t kNoExp = -1000000;                // exponent of a row with no non-zero element
+
+// The moduli (pairwise coprime, <= 256) and the constants derived from them,
+// as compile-time functions so that unrolled loops over the moduli fold them
+// into instruction operands.  The same list is used by the host
+// (kCrtModuli in ltg_capi.cu).
+__host__ __device__ constexpr int32_t crt_modulus(int i) {
+    return i == 0 ? 256 : i == 1 ? 255 : i == 2 ? 253 : i == 3 ? 251 : i == 4 ? 247 : i == 5 ? 241 :
+           i == 6 ? 239 : i == 7 ? 233 : i == 8 ? 229 : i == 9 ? 227 : i == 10 ? 223 : i == 11 ? 217 :
+           i == 12 ? 211 : i == 13 ? 199 : i == 14 ? 197 : 193;
+}
+// m_j^-1 mod m_i (extended Euclid)
+__host__ __device__ constexpr int32_t crt_inverse(int j, int i) {
+    int64_t m = crt_modulus(i), t = 0, nt = 1, r = m, nr = crt_modulus(j) % m;
+    while (nr != 0) {
+        const int64_t q = r / nr;
+        const int64_t t2 = t - q * nt; t = nt; nt = t2;
+        const int64_t r2 = r - q * nr; r = nr; nr = r2;
+    }
+    return (int32_t)(t < 0 ? t + m : t);
+}
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E).
+template<int B, int E>
+struct StaticFor {
+    template<class F>
+    __device__ __forceinline__ static void run(F &&f) {
+        f(std::integral_constant<int, B>());
+        StaticFor<B + 1, E>::run(f);
+    }
+};
+template<int E>
+struct StaticFor<E, E> {
+    template<class F>
+    __device__ __forceinline__ static void run(F &&) {}
+};
 
 __device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_t *ext, const int32_t *str) {
     int64_t off = 0;
@@ -108,29 +145,20 @@ crt_exp_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const doub
 
 // ---------------------------------------------------------------- residues
 
-// Balanced residue (as its low byte) of an integer-valued double |X| < 2^51
-// modulo m, from X - m * rint(X / m) in exact FP64 arithmetic.  The quotient
-// rint(X * (1/m)) is exact: the product's relative error 2^-53 moves X/m by
-// less than 2^-10.5, while X/m mod 1 stays at least 1/(2m) away from 1/2 for
-// odd m; for m = 256 the scaling is exact.  So |r| <= (m-1)/2 for odd m and
-// |r| <= 128 for m = 256, where +128 and -128 share the byte 0x80.
-__device__ __forceinline__ uint32_t residue_fp64(double X, double m, double minv) {
-    const double q = fma(X, minv, kMagicD) - kMagicD;
-    return (uint32_t)__double2loint(fma(-q, m, X) + kMagicD);
-}
-
-// Same from the five 11-bit limbs d of |X| (X < 2^55) in exact FP32
-// arithmetic: s = sum_t d_t (2^(11 t) mod m) < 2^21.1, so rint(s * (1/m)) is
-// again exact (error below 2^-10.5 against a distance of at least 2^-9).
-// sgn is +1 or -1, the sign of X.
-__device__ __forceinline__ uint32_t residue_fp32(const float (&d)[5], float sgn, const int32_t *pw, float m,
-                                                 float minv) {
-    float s = d[0];
-#pragma unroll
-    for (int t = 1; t < 5; t++) s = fmaf(d[t], (float)pw[t - 1], s);
-    const float q = fmaf(s, minv, kMagicF) - kMagicF;
-    const float r = fmaf(-q, m, s) * sgn;
-    return (uint32_t)__float_as_int(r + kMagicF);        // low byte: r mod 256
+// Residue of an integer X (|X| < 2^51, given as a double and as its low 32
+// bits) modulo m, as the low byte of X - m * rint(X / m).  The quotient
+// rint(X * (1/m)) comes out of one FMA against the 1.5 * 2^52 constant (its
+// low word is q mod 2^32) and is exact: the product's relative error 2^-53
+// moves X/m by less than 2^-10.5, while X/m mod 1 stays at least 1/(2m) away
+// from 1/2 for odd m, and the scaling is exact for m = 256.  So the balanced
+// residue r = X - q m lies in [-(m-1)/2, (m-1)/2] (or is +-128 for m = 256,
+// where both share the byte 0x80), and its low byte is (X - q m) mod 2^8,
+// formed in 32-bit integer arithmetic.
+template<int I>
+__device__ __forceinline__ uint32_t residue_byte(double X, uint32_t xlo) {
+    constexpr double minv = 1.0 / (double)crt_modulus(I);
+    const uint32_t qlo = (uint32_t)__double2loint(fma(X, minv, kMagicD));
+    return xlo - qlo * (uint32_t)crt_modulus(I);
 }
 
 // Low bytes of four words packed into one.
@@ -138,14 +166,11 @@ __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, ui
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
-// The first L64 moduli use the FP64 pipe, the rest the FP32 pipe, so that
-// both run at once.
 template<int L>
 __global__ void __launch_bounds__(256)
 crt_res_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const double *__restrict__ A,
                const double *__restrict__ B, const int32_t *__restrict__ gidx, const int32_t *__restrict__ ex,
                const int32_t *__restrict__ ey, uint8_t *__restrict__ res, const CrtParams cp) {
-    constexpr int L64 = (L + 1) / 2;
     const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
     for (int p = blockIdx.y; p < npanels; p += gridDim.y) {
         const DCrtPanel &P = panels[p];
@@ -166,33 +191,32 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const doub
             const double s1 = ldexp(1.0, sh / 2), s2 = ldexp(1.0, sh - sh / 2);
             const bool live = valid && e > kNoExp;
             for (int k0 = 4 * c; k0 < P.K_pad; k0 += 32) {
-                double X[4];
-                float d[4][5];
-                float sgn[4];
+                double x[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const int k = k0 + j;
-                    const double x = (live && k < P.K) ? row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
-                    const double y = (x * s1) * s2;                 // exact, |y| < 2^P
-                    X[j] = ((y + kMagicD) - kMagicD) * coef;        // rint, then the integer coefficient
-                    sgn[j] = X[j] < 0.0 ? -1.0f : 1.0f;
-                    const uint64_t u = (uint64_t)__double_as_longlong(fabs(X[j]) + 4503599627370496.0) &
-                                       ((1ull << 52) - 1);         // |X| as an integer
+                    x[j] = (live && k < P.K) ? row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
+                }
+                uint32_t packed[L];
 #pragma unroll
-                    for (int t = 0; t < 5; t++) d[j][t] = (float)(uint32_t)((u >> (11 * t)) & 2047u);
+                for (int l = 0; l < L; l++) packed[l] = 0;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const double t = (x[j] * s1) * s2 + kMagicD;         // 1.5 * 2^52 + rint(x 2^(P-e))
+                    const double X = (t - kMagicD) * coef;               // the integer coefficient folded in
+                    const uint32_t xlo = (uint32_t)__double2loint(t) * (uint32_t)P.coef;   // X mod 2^32
+                    // byte j of each modulus word takes this element's residue
+                    const uint32_t sel = 0x3210u ^ ((0x4u ^ (uint32_t)j) << (4 * j));
+                    StaticFor<0, L>::run([&](auto ic) {
+                        constexpr int l = decltype(ic)::value;
+                        packed[l] = __byte_perm(packed[l], residue_byte<l>(X, xlo), sel);
+                    });
                 }
                 const int kb = k0 / kKB, kb_byte = k0 % kKB;
                 uint8_t *dst0 = base + image_offset(r, TR, nkb, kb, 0, L, kb_byte);
-                const int64_t lstride = (int64_t)TR * kKB;          // next modulus image
+                const int64_t lstride = (int64_t)TR * kKB;              // next modulus image
 #pragma unroll
-                for (int l = 0; l < L; l++) {
-                    uint32_t v[4];
-#pragma unroll
-                    for (int j = 0; j < 4; j++)
-                        v[j] = l < L64 ? residue_fp64(X[j], (double)cp.m[l], cp.minv_d[l])
-                                       : residue_fp32(d[j], sgn[j], cp.pow11[l], (float)cp.m[l], cp.minv_f[l]);
-                    *reinterpret_cast<uint32_t *>(dst0 + l * lstride) = pack4(v[0], v[1], v[2], v[3]);
-                }
+                for (int l = 0; l < L; l++) *reinterpret_cast<uint32_t *>(dst0 + l * lstride) = packed[l];
             }
         }
     }
@@ -319,12 +343,10 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                 for (int l = 0; l < L && ok; l++) {
                     for (int ti = item.t_begin; ti < item.t_end && ok; ti++) {
                         const DCrtTask t = tasks[ti];
-                        const DCrtPanel &X = panels[t.px];
-                        const DCrtPanel &Y = panels[t.py];
-                        const int nkb = X.K_pad / kKB;
+                        const int nkb = t.nkb;
                         const int64_t xt = (int64_t)nkb * L * kXTile;          // one M tile's images
-                        const uint8_t *ga = res + X.res_off + (int64_t)(item.x0 / kXRows) * xt;
-                        const uint8_t *gb = res + Y.res_off + (int64_t)(item.y0 / item.nt) * nkb * L * ybytes;
+                        const uint8_t *ga = res + t.xres + (int64_t)(item.x0 / kXRows) * xt;
+                        const uint8_t *gb = res + t.yres + (int64_t)(item.y0 / item.nt) * nkb * L * ybytes;
                         for (int kb = 0; kb < nkb; kb++) {
                             if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s)) { ok = false; break; }
                             const uint32_t sa = smem0 + st * kStageBytes;
@@ -364,7 +386,7 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                     tc_fence_after();
                     uint32_t acc = 0;
                     for (int ti = item.t_begin; ti < item.t_end && ok; ti++) {
-                        const int nkb = panels[tasks[ti].px].K_pad / kKB;
+                        const int nkb = tasks[ti].nkb;
                         for (int kb = 0; kb < nkb; kb++) {
                             if (!mbar_wait(&full_bar[st], ph, &abort_s)) { ok = false; break; }
                             tc_fence_after();
@@ -401,7 +423,7 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                 ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[0], fills & 1, &abort_s));
                 if (!ok) break;
                 tc_fence_after();
-                const double m = (double)cp.m[l], minv = cp.minv_d[l];
+                const double minv = cp.minv_d[l];
                 const int mi = cp.m[l];
                 for (int xh = 0; xh < item.nx; xh++) {
                     const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + xh * kMaxNt;
@@ -413,11 +435,14 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                         uint32_t w[16];
 #pragma unroll
                         for (int j = 0; j < 16; j++) {
-                            // exact quotient (|x| < 2^31): r in [-(m-1)/2, (m-1)/2] or +-128 for m = 256
-                            const double x = (double)(int32_t)v[j];
-                            const double q = fma(x, minv, kMagicD) - kMagicD;
-                            const int r = __double2loint(fma(-q, m, x) + kMagicD);
-                            w[j] = (uint32_t)(r < 0 ? r + mi : r);            // [0, m)
+                            // int32 -> double by bits (2^52 * 1.5 + 2^31 + v, exact); the
+                            // quotient q = rint(v / m) is exact (|v| < 2^31), so
+                            // r = v - q m lies in [-(m-1)/2, (m-1)/2] (or +-128 for m = 256)
+                            const double x = __hiloint2double(0x43380000, (int)(v[j] ^ 0x80000000u)) -
+                                             6755401588539392.0;
+                            const int q = __double2loint(fma(x, minv, kMagicD));
+                            const int r = (int)v[j] - q * mi;
+                            w[j] = (uint32_t)(r + ((r >> 31) & mi));           // [0, m)
                         }
                         *reinterpret_cast<uint4 *>(orow + c0) =
                             make_uint4(pack4(w[0], w[1], w[2], w[3]), pack4(w[4], w[5], w[6], w[7]),
@@ -484,24 +509,29 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
                 if (r >= xr || c0 + c >= yc) continue;
                 // Garner: balanced mixed-radix digits v_i of the residues
                 float v[L];
-#pragma unroll
-                for (int i = 0; i < L; i++) {
-                    const float mi = (float)cp.m[i], minv = cp.minv_f[i];
-                    float t = (float)sres[i][r][c];
-#pragma unroll
-                    for (int j = 0; j < i; j++) {
-                        t = (t - v[j]) * (float)cp.inv[i][j];
+                StaticFor<0, L>::run([&](auto ii) {
+                    constexpr int i = decltype(ii)::value;
+                    constexpr float mi = (float)crt_modulus(i), minv = 1.0f / (float)crt_modulus(i);
+                    float t = __int_as_float(0x4B000000 | (int)sres[i][r][c]) - 8388608.0f;
+                    StaticFor<0, i>::run([&](auto jj) {
+                        constexpr int j = decltype(jj)::value;
+                        t = (t - v[j]) * (float)crt_inverse(j, i);
                         t = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);   // t mod m_i, |t| <= m_i/2 + 1
-                    }
+                    });
                     // exact balanced digit in (-m_i/2, m_i/2]
                     t = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);
                     if (t > 0.5f * mi) t -= mi;
                     if (t <= -0.5f * mi) t += mi;
                     v[i] = t;
-                }
-                double X = (double)v[L - 1];
+                });
+                // digits to double by bits (|v| < 2^22): float 1.5*2^23 + v -> int -> double
+                auto digit = [](float f) {
+                    const int iv = __float_as_int(f + kMagicF) - 0x4B400000;
+                    return __hiloint2double(0x43380000, iv ^ (int)0x80000000) - 6755401588539392.0;
+                };
+                double X = digit(v[L - 1]);
 #pragma unroll
-                for (int i = L - 2; i >= 0; i--) X = fma(X, (double)cp.m[i], (double)v[i]);
+                for (int i = L - 2; i >= 0; i--) X = fma(X, (double)crt_modulus(i), digit(v[i]));
                 const int gx = gxp[r], gy = gyp[c0 + c];
                 const int e2 = ex[gx] + ey[gy] - 2 * cp.P;
                 const double val = cb.scale * ldexp(X, max(e2, -2200));

@@ -665,14 +665,8 @@ CrtParams crt_params(int L, int P, bool swap) {
     for (int i = 0; i < L; i++) {
         const int32_t m = kCrtModuli[i];
         cp.m[i] = m;
-        cp.minv_f[i] = 1.0f / (float)m;
         cp.minv_d[i] = 1.0 / (double)m;
-        for (int j = 0; j < i; j++) cp.inv[i][j] = mod_inverse(kCrtModuli[j], m);
-        int64_t pw = 1;
-        for (int t = 0; t < 4; t++) {
-            pw = (pw * 2048) % m;
-            cp.pow11[i][t] = (int32_t)pw;
-        }
+        for (int j = 0; j < i; j++) (void)mod_inverse(kCrtModuli[j], m);   // pairwise coprime
     }
     return cp;
 }
@@ -827,6 +821,10 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
             if (panels[pa].K_pad != panels[pb].K_pad) throw error(kErrState, "panel k extents differ");
             dt[t].px = swap ? pb : pa;
             dt[t].py = swap ? pa : pb;
+            dt[t].xres = panels[dt[t].px].res_off;
+            dt[t].yres = panels[dt[t].py].res_off;
+            dt[t].nkb = panels[pa].K_pad / 32;
+            dt[t].pad = 0;
             sum += std::llabs(ci) * (int64_t)g.k.total();
             max_coef = std::max<int64_t>(max_coef, std::llabs(ci));
         }

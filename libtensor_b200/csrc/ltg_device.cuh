@@ -93,6 +93,9 @@ struct DCrtPanel {
 
 struct DCrtTask {
     int32_t px, py;               // MMA M-side and N-side panels of one pair
+    int64_t xres, yres;           // byte offsets of their tile images
+    int32_t nkb;                  // 32-byte k blocks
+    int32_t pad;
 };
 
 // One CTA work item: an (nx * 128) x nt tile of one C block (in MMA
@@ -109,17 +112,15 @@ struct DCrtItem {
     int64_t res_off;              // residue tile output: [modulus][nx * 128][nt] bytes
 };
 
-// Moduli and the constants of Garner's mixed-radix reconstruction.
+// Moduli of a modular contraction and its scaling (the constants of Garner's
+// reconstruction are compile-time functions of the same moduli in crt.cu).
 struct CrtParams {
     int32_t L;                    // number of moduli
     int32_t P;                    // bits of the scaled integer operands
     int32_t swap;                 // 1: MMA M side = the C columns (B operand)
     int32_t pad;
     int32_t m[kCrtMaxModuli];     // moduli, pairwise coprime, <= 256
-    int32_t inv[kCrtMaxModuli][kCrtMaxModuli];   // inv[i][j] = m_j^-1 mod m_i (j < i)
-    float minv_f[kCrtMaxModuli];  // 1 / m_i
-    double minv_d[kCrtMaxModuli];
-    int32_t pow11[kCrtMaxModuli][4];   // 2^(11 t) mod m_i
+    double minv_d[kCrtMaxModuli]; // 1 / m_i
 };
 
 // ---------------------------------------------------------------- element-wise
