@@ -39,8 +39,10 @@ constexpr int kXRows = 128;                         // MMA M (TMEM lanes)
 constexpr int kKB = 32;                             // bytes (INT8 elements) per k block
 constexpr int kXTile = kXRows * kKB;                // 4 KB
 constexpr int kMaxNt = 256;
-constexpr int kStageBytes = 2 * kXTile + kMaxNt * kKB;  // 16 KB: two M tiles and one N tile
-constexpr int kMaxStages = 12;
+constexpr int kSubBytes = 2 * kXTile + kMaxNt * kKB;    // one k block: two M tiles and one N tile (16 KB)
+constexpr int kKbPerStage = 4;                           // k blocks per pipeline stage
+constexpr int kStageBytes = kKbPerStage * kSubBytes;     // 32 KB
+constexpr int kMaxStages = 8;
 constexpr int kGemmThreads = 192;
 constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s per barrier wait
 constexpr double kMagicD = 6755399441055744.0;      // 1.5 * 2^52: round-to-integer constant
@@ -347,14 +349,18 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                         const int64_t xt = (int64_t)nkb * L * kXTile;          // one M tile's images
                         const uint8_t *ga = res + t.xres + (int64_t)(item.x0 / kXRows) * xt;
                         const uint8_t *gb = res + t.yres + (int64_t)(item.y0 / item.nt) * nkb * L * ybytes;
-                        for (int kb = 0; kb < nkb; kb++) {
+                        for (int kb = 0; kb < nkb; kb += kKbPerStage) {
                             if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s)) { ok = false; break; }
-                            const uint32_t sa = smem0 + st * kStageBytes;
+                            const int nsub = min(kKbPerStage, nkb - kb);
                             const uint32_t fb = smem_u32(&full_bar[st]);
-                            mbar_expect_tx(&full_bar[st], (uint32_t)(item.nx * kXTile) + ybytes);
-                            bulk_load(sa, ga + ((int64_t)kb * L + l) * kXTile, kXTile, fb);
-                            if (item.nx == 2) bulk_load(sa + kXTile, ga + xt + ((int64_t)kb * L + l) * kXTile, kXTile, fb);
-                            bulk_load(sa + 2 * kXTile, gb + ((int64_t)kb * L + l) * ybytes, ybytes, fb);
+                            mbar_expect_tx(&full_bar[st], (uint32_t)nsub * ((uint32_t)(item.nx * kXTile) + ybytes));
+                            for (int j = 0; j < nsub; j++) {
+                                const uint32_t sa = smem0 + st * kStageBytes + j * kSubBytes;
+                                const int64_t img = (int64_t)(kb + j) * L + l;
+                                bulk_load(sa, ga + img * kXTile, kXTile, fb);
+                                if (item.nx == 2) bulk_load(sa + kXTile, ga + xt + img * kXTile, kXTile, fb);
+                                bulk_load(sa + 2 * kXTile, gb + img * ybytes, ybytes, fb);
+                            }
                             armed[st] = (int)ph;
                             if (++st == stages) { st = 0; ph ^= 1; }
                         }
@@ -387,14 +393,17 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                     uint32_t acc = 0;
                     for (int ti = item.t_begin; ti < item.t_end && ok; ti++) {
                         const int nkb = tasks[ti].nkb;
-                        for (int kb = 0; kb < nkb; kb++) {
+                        for (int kb = 0; kb < nkb; kb += kKbPerStage) {
                             if (!mbar_wait(&full_bar[st], ph, &abort_s)) { ok = false; break; }
                             tc_fence_after();
-                            const uint32_t a0 = smem0 + st * kStageBytes;
-                            const uint64_t db = smem_desc_kmajor(a0 + 2 * kXTile);
-                            umma_i8(tmem, smem_desc_kmajor(a0), db, idesc, acc);
-                            if (item.nx == 2) umma_i8(tmem + kMaxNt, smem_desc_kmajor(a0 + kXTile), db, idesc, acc);
-                            acc = 1;
+                            const int nsub = min(kKbPerStage, nkb - kb);
+                            for (int j = 0; j < nsub; j++) {
+                                const uint32_t a0 = smem0 + st * kStageBytes + j * kSubBytes;
+                                const uint64_t db = smem_desc_kmajor(a0 + 2 * kXTile);
+                                umma_i8(tmem, smem_desc_kmajor(a0), db, idesc, acc);
+                                if (item.nx == 2) umma_i8(tmem + kMaxNt, smem_desc_kmajor(a0 + kXTile), db, idesc, acc);
+                                acc = 1;
+                            }
                             umma_commit(&empty_bar[st]);
                             if (++st == stages) { st = 0; ph ^= 1; }
                         }
