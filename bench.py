@@ -48,9 +48,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ltg", choices=["ltg", "reference"])
     # Headline: the split-precision ladder o=40 v=240 (blocks 64/56 per spin)
-    # at <= 1e-12, with the plain FP64 DMMA path timed on the same workload.
+    # at <= 1e-12 (modular INT8 mode, 13 moduli), with the plain FP64 DMMA path
+    # timed on the same workload.
     p.add_argument("--workload", default="ladder-split", choices=sorted(WORKLOADS) + list(TRANSFER_WORKLOADS))
-    p.add_argument("--mode", default="ozaki-int8", choices=sorted(MODES))
+    p.add_argument("--mode", default="ozaki-crt", choices=sorted(MODES))
     p.add_argument("--nslices", type=int, default=None,
                    help="slices (moduli for ozaki-crt); default 7, 8 for FP8, 13 for the modular mode")
     p.add_argument("--no-cpu-baseline", action="store_true")

@@ -492,14 +492,16 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
                    const int32_t *__restrict__ gidx, const int32_t *__restrict__ ex,
                    const int32_t *__restrict__ ey, double *__restrict__ C, int32_t add, const CrtParams cp) {
     __shared__ __align__(16) uint8_t sres[L][kXRows][kCombCols];
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const DCrtItem item = items[it];
+    // units: (item, 128-row half, 16-column chunk), 32 per item
+    for (int u = blockIdx.x; u < nitems * 32; u += gridDim.x) {
+        const DCrtItem item = items[u >> 5];
+        const int xh = (u >> 4) & 1, c0 = (u & 15) * kCombCols;
         const DCBlock &cb = cblks[item.cblk];
         const int xext = cp.swap ? cb.N : cb.M, yext = cp.swap ? cb.M : cb.N;
         const int yc = min(item.nt, yext - item.y0);
+        if (xh >= item.nx || c0 >= yc) continue;                     // uniform over the CTA
         const int32_t *gyp = gidx + panels[item.gy].g_off + item.y0;
-        for (int xh = 0; xh < item.nx; xh++)
-        for (int c0 = 0; c0 < yc; c0 += kCombCols) {
+        {
             const int xb = item.x0 + xh * kXRows;                    // first row of this half
             const int xr = min(kXRows, xext - xb);
             const int32_t *gxp = gidx + panels[item.gx].g_off + xb;
@@ -611,7 +613,7 @@ cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, i
                                const DCBlock *cblks, const uint8_t *out, const int32_t *gidx, const int32_t *ex,
                                const int32_t *ey, double *c, int32_t add, const CrtParams &cp, cudaStream_t s) {
     if (nitems <= 0) return cudaSuccess;
-    const int grid = nitems < 8 * num_sms() ? nitems : 8 * num_sms();
+    const int grid = 32 * nitems < 8 * num_sms() ? 32 * nitems : 8 * num_sms();
     switch (cp.L) {
 #define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, out, gidx, ex, ey, c, add, cp); break;
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
