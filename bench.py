@@ -367,7 +367,8 @@ def ltg_arm(args):
     # ---- roofline of the dominant kernel, timed by events inside the timed region
     roofline = None
     if rank == 0:
-        roofline = contraction_roofline(torch, dev, args, flops, ktimes)
+        split = op.split_bytes(C, mode, args.nslices) if mode != 0 else None
+        roofline = contraction_roofline(torch, dev, args, flops, ktimes, split)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -415,7 +416,7 @@ def measure_int8_peak(torch, dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def contraction_roofline(torch, dev, args, flops, ktimes):
+def contraction_roofline(torch, dev, args, flops, ktimes, split=None):
     """Roofline of the kernel with the largest device time in the timed region.
 
     Plain mode: the DMMA contraction against the live cuBLAS DGEMM rate.
@@ -463,6 +464,16 @@ def contraction_roofline(torch, dev, args, flops, ktimes):
         return {"bound": "tensor", "kernel": kname, "achieved": ach, "peak": peak, "unit": unit,
                 "frac": ach / peak if peak else None, "traffic": traffic, "avg_launch_ms": sec * 1e3,
                 "slice_products": prods, "effective_fp64_tflops": per_launch / sec / 1e12,
+                "peak_source": src}
+    if kname == "oz_split" and split is not None:
+        rb, wb = split
+        peak, src = hbm_peak()
+        ach = (rb + wb) / sec / 1e9
+        return {"bound": "hbm", "kernel": kname, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "traffic": traffic, "avg_launch_ms": sec * 1e3,
+                "algorithmic_bytes": {"read": rb, "write": wb,
+                                      "note": "FP64 operands read by the exponent and residue passes, "
+                                              "residue (or slice) images written"},
                 "peak_source": src}
     return {"bound": "hbm", "kernel": kname, "achieved": None, "peak": None, "unit": "GB/s",
             "frac": None, "traffic": traffic, "avg_launch_ms": sec * 1e3}

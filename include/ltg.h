@@ -183,6 +183,13 @@ int ltg_plan_flops(ltg_plan *plan, double *flops);
  * LTG_MODE_PLAIN_FP64). */
 int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices,
                   double ka, double kb, double kc, int32_t add, double d);
+/* Bytes the split pass(es) of a split-precision mode move for this call:
+ * FP64 operand bytes read (twice for the modular mode: exponent and residue
+ * passes) and slice/residue bytes written.  No reference counterpart (used
+ * for rooflines). */
+int ltg_contract2_split_bytes(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, double ka,
+                              double kb, double kc, int32_t add, double d, int64_t *read_bytes,
+                              int64_t *write_bytes);
 int ltg_plan_destroy(ltg_plan *plan);
 /* Forces one tile shape for every C block (cfg >= 0) or restores the
  * automatic choice (-1).  No reference counterpart: the reference hands each

@@ -93,6 +93,8 @@ _SIGS = {
     "ltg_dotprod": (C.c_int, [c_vp, c_i32p, c_vp, c_i32p, c_dblp]),
     "ltg_dotprod_async": (C.c_int, [c_vp, c_i32p, c_vp, c_i32p, c_vp]),
     "ltg_dot_noalloc": (C.c_int, [c_vp, c_vp, C.c_int64, c_vp, c_dblp]),
+    "ltg_contract2_split_bytes": (C.c_int, [c_vp, c_vp, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                            C.c_double, C.c_int32, C.c_double, c_i64p, c_i64p]),
     "ltg_ctx_set_timing": (C.c_int, [c_vp, C.c_int32]),
     "ltg_ctx_kernel_times": (C.c_int, [c_vp, c_dblp, c_i64p]),
     "ltg_scale": (C.c_int, [c_vp, C.c_double]),

@@ -316,6 +316,14 @@ class btod_contract2:
                                    cfg.ctypes.data_as(_capi.c_i32p), n.value, C.byref(n)))
         return {(int(a), int(b)): int(c) for a, b, c in zip(m[:n.value], nn[:n.value], cfg[:n.value])}
 
+    def split_bytes(self, c: block_tensor, mode: int, nslices: int = 0, d: Optional[float] = None):
+        """(bytes read, bytes written) by the split pass(es) of a split-precision mode."""
+        r, w = C.c_int64(), C.c_int64()
+        check(lib().ltg_contract2_split_bytes(self.h, c.h, mode, nslices, self.ka, self.kb, self.kc,
+                                              0 if d is None else 1, 0.0 if d is None else d,
+                                              C.byref(r), C.byref(w)))
+        return r.value, w.value
+
     def perform(self, c: block_tensor, d: Optional[float] = None, mode: int = MODE_PLAIN_FP64,
                 nslices: int = 0):
         check(lib().ltg_contract2(self.h, c.h, mode, nslices, self.ka, self.kb, self.kc,

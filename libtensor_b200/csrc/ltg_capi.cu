@@ -138,6 +138,7 @@ struct ContractExec {
 // mode, slice count).
 struct OzExec {
     int kind = 0, S = 0, chunk_kb = 1, npanels = 0, max_rows_pad = 0, nitems = 0;
+    int64_t src_elems = 0, slice_bytes = 0;   // operand elements read, slice bytes written
     DevBuf panels, slices, exps, tasks, cblks, items, err;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
@@ -149,6 +150,7 @@ struct OzExec {
 struct CrtExec {
     CrtParams cp{};
     int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0;
+    int64_t src_elems = 0, res_bytes = 0;   // operand elements read per pass, residue bytes written
     DevBuf panels, tasks, items, cblks, gidx, ex, ey, res, out, err;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
@@ -608,7 +610,11 @@ OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, doubl
     std::stable_sort(iv.begin(), iv.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
     std::vector<DItem> items;
     for (auto &p : iv) items.push_back(p.second);
-    for (const DPanel &p : panels) ex->max_rows_pad = std::max(ex->max_rows_pad, p.rows_pad);
+    for (const DPanel &p : panels) {
+        ex->max_rows_pad = std::max(ex->max_rows_pad, p.rows_pad);
+        ex->src_elems += (int64_t)p.rows * p.K;
+        ex->slice_bytes += (int64_t)S * p.rows_pad * p.K_pad * esz;
+    }
 
     cudaStream_t s = pl->ctx->stream;
     ex->npanels = (int)panels.size();
@@ -898,6 +904,10 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     ex->npanels = (int32_t)panels.size();
     ex->nitems = (int32_t)items.size();
     ex->max_rows = max_rows;
+    for (const DCrtPanel &q : panels) {
+        ex->src_elems += (int64_t)q.rows * q.K;
+        ex->res_bytes += (int64_t)L * q.rows_pad * q.K_pad;
+    }
     ex->res.alloc(std::max<int64_t>(res_bytes, 1024));
     ex->out.alloc(std::max<int64_t>(out_bytes, 1024));
     ex->ex.alloc(std::max<int64_t>(ex->nx, 1) * sizeof(int32_t));
@@ -1693,6 +1703,27 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
         if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
         for (int64_t sl : ex->sched_slots) c->h.nonzero[sl] = 1;
         if (!ctx->capturing) LTG_CUDA(cudaGetLastError());
+    });
+}
+
+int ltg_contract2_split_bytes(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, double ka, double kb,
+                              double kc, int32_t add, double d, int64_t *read_bytes, int64_t *write_bytes) {
+    return guard([&] {
+        if (!plan || !read_bytes || !write_bytes) throw error(kErrBadArg, "null argument");
+        check_bt(c);
+        need_dev(plan->ctx);
+        if (mode == LTG_MODE_OZAKI_CRT) {
+            CrtExec *cx = prepare_crt(plan, c, nslices > 0 ? nslices : 13, ka, kb, kc, add, d);
+            *read_bytes = 2 * 8 * cx->src_elems;          // exponent pass and residue pass
+            *write_bytes = cx->res_bytes;
+        } else if (mode >= LTG_MODE_OZAKI_BF16 && mode <= LTG_MODE_OZAKI_INT8) {
+            const int S = nslices > 0 ? nslices : (mode == LTG_MODE_OZAKI_FP8 ? 8 : 7);
+            OzExec *ox = prepare_ozaki(plan, c, mode, S, ka, kb, kc, add, d);
+            *read_bytes = 8 * ox->src_elems;
+            *write_bytes = ox->slice_bytes;
+        } else {
+            throw error(kErrBadArg, "not a split-precision mode");
+        }
     });
 }
 
