@@ -37,6 +37,9 @@ WORKLOADS = {
 # HBM-bound operations (btod_copy / btod_add / btod_dotprod) on the CCD
 # iteration's tensors, o=30 v=300 (blocks 15 / 50,50,50 per spin).
 TRANSFER_WORKLOADS = ("copy-vvvv", "add-x4", "dot-vvvv")
+# One CCD amplitude iteration (copy, ladder, ring, antisymmetrising add,
+# denominator, energy) replayed as one CUDA graph, o=30 v=300.
+GRAPH_WORKLOADS = ("ccd-iter",)
 MODES = {"plain": 0, "ozaki-bf16": 1, "ozaki-fp8": 2, "ozaki-int8": 3, "ozaki-crt": 4}
 FP64_NOMINAL = 40.0
 
@@ -50,7 +53,8 @@ def parse():
     # Headline: the split-precision ladder o=40 v=240 (blocks 64/56 per spin)
     # at <= 1e-12 (modular INT8 mode, 13 moduli), with the plain FP64 DMMA path
     # timed on the same workload.
-    p.add_argument("--workload", default="ladder-split", choices=sorted(WORKLOADS) + list(TRANSFER_WORKLOADS))
+    p.add_argument("--workload", default="ladder-split",
+                   choices=sorted(WORKLOADS) + list(TRANSFER_WORKLOADS) + list(GRAPH_WORKLOADS))
     p.add_argument("--mode", default="ozaki-crt", choices=sorted(MODES))
     p.add_argument("--nslices", type=int, default=None,
                    help="slices (moduli for ozaki-crt); default 7, 8 for FP8, 13 for the modular mode")
@@ -691,8 +695,105 @@ def transfer_cpu_baseline(name, w, steps=2, budget_s=30.0):
                 "sample": f"failed: {e}"}
 
 
+def ccd_arm(args):
+    """CCD iteration graph: value = contraction flops (ladder + ring) per second."""
+    import torch
+    from libtensor_b200.ccd import CCDIteration
+    from libtensor_b200.core import Context
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    ctx = Context(local)
+    mode = MODES[args.mode]
+    it = CCDIteration(ctx, [15], [50, 50, 50], mode, args.nslices)
+    # per-operation device times of one eager iteration
+    it.step()
+    ctx.synchronize()
+    ctx.set_timing(True)
+    n0 = ctx.launch_count()
+    it.step()
+    per_iter = ctx.launch_count() - n0          # kernels in one iteration (and in the graph)
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    it.capture()
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(max(3, args.warmup)):
+        it.launch()
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        it.launch()
+    e1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    energy = it.energy()
+    # end to end: amplitudes uploaded from pinned host memory, the graph, the
+    # energy read back, every step
+    nt = it.t.nelems
+    ht = torch.empty(max(1, nt), dtype=torch.float64, pin_memory=True)
+    he = torch.empty(1, dtype=torch.float64, pin_memory=True)
+    it.t.download_async(ht.data_ptr())
+    ctx.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        it.t.upload_async(ht.data_ptr())
+        it.launch()
+        with torch.cuda.stream(stream):
+            he.copy_(it.energy_dev, non_blocking=True)
+    f1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ems = f0.elapsed_time(f1) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms, ems], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ems = float(t[0].item()), float(t[1].item())
+    flops = it.flops
+    it.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    tot = sum(v for v, _ in kt.values())
+    out = {"metric": "CCD iteration (CUDA graph): contraction TFLOP/s eff. FP64",
+           "value": world * flops / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+           "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, symmetrised)",
+           "config": {"workload": "ccd-iter: o=30 (15 per spin) v=300 (50,50,50 per spin); copy P(0,2,1,3), "
+                                  "ladder, ring, 5-term add, denominator, energy, t <- R; one graph launch per step",
+                      "mode": args.mode, "nslices": args.nslices, "algorithmic_flops": flops,
+                      "l2": "operands larger than L2 (no flush)"},
+           "kernels_eager_iteration": {k: {"launches": n, "ms_total": v, "share": v / tot} for k, (v, n) in kt.items()},
+           "energy": energy,
+           "e2e": {"value": world * flops / (ems * 1e-3) / 1e12, "unit": "TFLOP/s",
+                   "h2d_bytes_per_step": 8 * nt, "d2h_bytes_per_step": 8, "ms_per_step": ems},
+           "gpu_launches": per_iter * args.steps, "clocks": clk, "cpu_baseline": None, "roofline": None}
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
+    if args.workload in GRAPH_WORKLOADS:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the CCD iteration graph has no single reference "
+                              "operation; its steps are timed one by one by the other workloads"}))
+        else:
+            ccd_arm(args)
+        return
     if args.workload in TRANSFER_WORKLOADS:
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) != 0:

@@ -1,0 +1,671 @@
+/*
+ * libtensor_b200/libtensor.h -- C++ operator surface of the B200 block-tensor
+ * contraction path, over the C ABI of ltg.h.
+ *
+ * Mirrors the class templates a libtensor user writes against for this path,
+ * in namespace libtensor, with the same names, argument meaning and error
+ * behaviour (exceptions of the same names):
+ *   index, index_range, dimensions, mask, permutation, scalar_transf,
+ *   block_index_space (libtensor/core/block_index_space.h:144),
+ *   se_perm (libtensor/symmetry/se_perm.h:28), se_part (se_part.h:32),
+ *   se_label (se_label.h:37) for abelian point groups, symmetry,
+ *   block_tensor and block_tensor_ctrl (libtensor/block_tensor/block_tensor.h:22),
+ *   contraction2 (libtensor/core/contraction2.h:48),
+ *   btod_contract2 (libtensor/block_tensor/btod_contract2.h:29),
+ *   btod_copy (btod_copy.h:38), btod_add (btod_add.h:38),
+ *   btod_dotprod (btod_dotprod.h:35).
+ * Differences a user meets:
+ *   - block data lives in GPU memory; blocks are read and written with
+ *     block_tensor_ctrl::get_block / put_block (host buffers) instead of the
+ *     dense_tensor_ctrl data-pointer sessions;
+ *   - symmetry elements are inserted before the first data access or
+ *     operation (the device layout is built from them);
+ *   - se_label supports abelian (XOR) product tables of 1, 2, 4 or 8
+ *     irreducible representations, registered by name with
+ *     register_abelian_table();
+ *   - btod_contract2::set_split_precision() selects the split-precision
+ *     modes of ltg.h (the default is the FP64 drop-in path).
+ * Header-only; link with libltg.so.
+ */
+#ifndef LIBTENSOR_B200_LIBTENSOR_H
+#define LIBTENSOR_B200_LIBTENSOR_H
+
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../ltg.h"
+
+namespace libtensor {
+
+// ---------------------------------------------------------------- exceptions
+
+class exception : public std::runtime_error {
+public:
+    explicit exception(const std::string &what) : std::runtime_error(what) { }
+};
+class bad_parameter : public exception { public: using exception::exception; };
+class bad_dimensions : public exception { public: using exception::exception; };
+class bad_symmetry : public exception { public: using exception::exception; };
+class out_of_bounds : public exception { public: using exception::exception; };
+class device_error : public exception { public: using exception::exception; };
+
+namespace b200 {
+
+// Converts an ltg status into the exception class of the reference.
+inline void check(int st) {
+    if (st == LTG_OK) return;
+    const std::string msg = ltg_last_error();
+    switch (st) {
+    case LTG_ERR_BAD_DIMS: throw bad_dimensions(msg);
+    case LTG_ERR_SYMMETRY: throw bad_symmetry(msg);
+    case LTG_ERR_BAD_ARG: throw bad_parameter(msg);
+    default: throw device_error(msg);
+    }
+}
+
+// The process-wide context of the surface: device 0 unless set_device() is
+// called before the first block tensor is used (device -1: host only, for
+// schedules and symmetry queries without a GPU).
+struct context_holder {
+    int device = 0;
+    ltg_ctx *ctx = nullptr;
+    ~context_holder() { if (ctx) ltg_ctx_destroy(ctx); }
+};
+inline context_holder &holder() {
+    static context_holder h;
+    return h;
+}
+inline void set_device(int device) {
+    if (holder().ctx) throw bad_parameter("set_device: the context is already in use");
+    holder().device = device;
+}
+inline ltg_ctx *context() {
+    context_holder &h = holder();
+    if (!h.ctx) check(ltg_ctx_create(h.device, &h.ctx));
+    return h.ctx;
+}
+
+// Abelian product tables for se_label, by name: XOR of irrep indices.
+inline std::map<std::string, int> &abelian_tables() {
+    static std::map<std::string, int> t;
+    return t;
+}
+}  // namespace b200
+
+// Registers an abelian point-group product table (irreps combine by XOR of
+// their indices, as in D2h and its subgroups) under a name for se_label.
+inline void register_abelian_table(const std::string &id, int nirrep) {
+    if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8)
+        throw bad_parameter("register_abelian_table: 1, 2, 4 or 8 irreps");
+    b200::abelian_tables()[id] = nirrep;
+}
+
+// ---------------------------------------------------------------- index types
+
+template<size_t N>
+class index {
+    size_t m_i[N == 0 ? 1 : N];
+public:
+    index() { for (size_t i = 0; i < N; i++) m_i[i] = 0; }
+    size_t &operator[](size_t i) { return m_i[i]; }
+    const size_t &operator[](size_t i) const { return m_i[i]; }
+    size_t at(size_t i) const { if (i >= N) throw out_of_bounds("index::at"); return m_i[i]; }
+    bool equals(const index<N> &o) const {
+        for (size_t i = 0; i < N; i++) if (m_i[i] != o.m_i[i]) return false;
+        return true;
+    }
+    bool operator==(const index<N> &o) const { return equals(o); }
+    bool operator<(const index<N> &o) const {
+        for (size_t i = 0; i < N; i++) if (m_i[i] != o.m_i[i]) return m_i[i] < o.m_i[i];
+        return false;
+    }
+};
+
+template<size_t N>
+class index_range {
+    index<N> m_begin, m_end;
+public:
+    index_range(const index<N> &begin, const index<N> &end) : m_begin(begin), m_end(end) {
+        for (size_t i = 0; i < N; i++)
+            if (end[i] < begin[i]) throw bad_parameter("index_range: end before begin");
+    }
+    const index<N> &get_begin() const { return m_begin; }
+    const index<N> &get_end() const { return m_end; }
+};
+
+template<size_t N>
+class dimensions {
+    index<N> m_d;
+public:
+    explicit dimensions(const index_range<N> &ir) {
+        for (size_t i = 0; i < N; i++) m_d[i] = ir.get_end()[i] - ir.get_begin()[i] + 1;
+    }
+    size_t get_dim(size_t i) const { return m_d.at(i); }
+    size_t operator[](size_t i) const { return m_d[i]; }
+    size_t get_size() const {
+        size_t n = 1;
+        for (size_t i = 0; i < N; i++) n *= m_d[i];
+        return n;
+    }
+    bool equals(const dimensions<N> &o) const { return m_d.equals(o.m_d); }
+};
+
+template<size_t N>
+class mask {
+    bool m_m[N == 0 ? 1 : N];
+public:
+    mask() { for (size_t i = 0; i < N; i++) m_m[i] = false; }
+    bool &operator[](size_t i) { return m_m[i]; }
+    bool operator[](size_t i) const { return m_m[i]; }
+};
+
+// permutation<N>: element i of a permuted sequence is element p[i] of the
+// original (libtensor/core/permutation.h).
+template<size_t N>
+class permutation {
+    size_t m_p[N == 0 ? 1 : N];
+public:
+    permutation() { for (size_t i = 0; i < N; i++) m_p[i] = i; }
+    permutation<N> &permute(size_t i, size_t j) {
+        if (i >= N || j >= N) throw out_of_bounds("permutation::permute");
+        std::swap(m_p[i], m_p[j]);
+        return *this;
+    }
+    permutation<N> &permute(const permutation<N> &q) {
+        size_t r[N == 0 ? 1 : N];
+        for (size_t i = 0; i < N; i++) r[i] = m_p[q.m_p[i]];
+        for (size_t i = 0; i < N; i++) m_p[i] = r[i];
+        return *this;
+    }
+    permutation<N> &invert() {
+        size_t r[N == 0 ? 1 : N];
+        for (size_t i = 0; i < N; i++) r[m_p[i]] = i;
+        for (size_t i = 0; i < N; i++) m_p[i] = r[i];
+        return *this;
+    }
+    bool is_identity() const {
+        for (size_t i = 0; i < N; i++) if (m_p[i] != i) return false;
+        return true;
+    }
+    size_t operator[](size_t i) const { return m_p[i]; }
+    std::vector<int32_t> to_vector() const { return std::vector<int32_t>(m_p, m_p + N); }
+};
+
+template<typename T>
+class scalar_transf {
+    T m_c;
+public:
+    explicit scalar_transf(T c = T(1)) : m_c(c) { }
+    T get_coeff() const { return m_c; }
+};
+
+// ---------------------------------------------------------------- block index space
+
+template<size_t N>
+class block_index_space {
+    dimensions<N> m_dims;
+    std::vector<size_t> m_splits[N == 0 ? 1 : N];
+public:
+    explicit block_index_space(const dimensions<N> &dims) : m_dims(dims) { }
+    const dimensions<N> &get_dims() const { return m_dims; }
+    // splits every dim set in msk at position pos
+    void split(const mask<N> &msk, size_t pos) {
+        for (size_t i = 0; i < N; i++) {
+            if (!msk[i]) continue;
+            if (pos == 0 || pos >= m_dims[i]) throw out_of_bounds("block_index_space::split");
+            std::vector<size_t> &s = m_splits[i];
+            std::vector<size_t>::iterator it = s.begin();
+            while (it != s.end() && *it < pos) ++it;
+            if (it == s.end() || *it != pos) s.insert(it, pos);
+        }
+    }
+    const std::vector<size_t> &get_splits(size_t dim) const { return m_splits[dim]; }
+    dimensions<N> get_block_index_dims() const {
+        index<N> i1;
+        for (size_t i = 0; i < N; i++) i1[i] = m_splits[i].size();
+        return dimensions<N>(index_range<N>(index<N>(), i1));
+    }
+    index<N> get_block_start(const index<N> &bidx) const {
+        index<N> s;
+        for (size_t i = 0; i < N; i++) s[i] = bidx[i] == 0 ? 0 : m_splits[i].at(bidx[i] - 1);
+        return s;
+    }
+    dimensions<N> get_block_dims(const index<N> &bidx) const {
+        index<N> i1;
+        for (size_t i = 0; i < N; i++) {
+            const size_t b0 = bidx[i] == 0 ? 0 : m_splits[i].at(bidx[i] - 1);
+            const size_t b1 = bidx[i] < m_splits[i].size() ? m_splits[i][bidx[i]] : m_dims[i];
+            i1[i] = b1 - b0 - 1;
+        }
+        return dimensions<N>(index_range<N>(index<N>(), i1));
+    }
+    bool equals(const block_index_space<N> &o) const {
+        if (!m_dims.equals(o.m_dims)) return false;
+        for (size_t i = 0; i < N; i++) if (m_splits[i] != o.m_splits[i]) return false;
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------- symmetry elements
+
+template<size_t N, typename T>
+class se_perm {
+    permutation<N> m_perm;
+    scalar_transf<T> m_tr;
+public:
+    se_perm(const permutation<N> &perm, const scalar_transf<T> &tr) : m_perm(perm), m_tr(tr) {
+        if (perm.is_identity() && tr.get_coeff() != T(1))
+            throw bad_symmetry("se_perm: identity permutation with a non-unit coefficient");
+    }
+    const permutation<N> &get_perm() const { return m_perm; }
+    const scalar_transf<T> &get_transf() const { return m_tr; }
+};
+
+// Partitions of block dims with forbidden partition combinations (the
+// partition maps of the reference's se_part are not supported).
+template<size_t N, typename T>
+class se_part {
+    index<N> m_pdims;
+    std::vector<index<N> > m_forbidden;
+public:
+    se_part(const block_index_space<N> &bis, const mask<N> &msk, size_t npart) {
+        const dimensions<N> bd = bis.get_block_index_dims();
+        for (size_t i = 0; i < N; i++) {
+            m_pdims[i] = msk[i] ? npart : 1;
+            if (msk[i] && (npart == 0 || bd[i] % npart != 0))
+                throw bad_parameter("se_part: partitions must divide the number of blocks");
+        }
+    }
+    se_part(const block_index_space<N> &bis, const dimensions<N> &pdims) {
+        const dimensions<N> bd = bis.get_block_index_dims();
+        for (size_t i = 0; i < N; i++) {
+            m_pdims[i] = pdims[i];
+            if (pdims[i] == 0 || bd[i] % pdims[i] != 0)
+                throw bad_parameter("se_part: partitions must divide the number of blocks");
+        }
+    }
+    void mark_forbidden(const index<N> &pidx) {
+        for (size_t i = 0; i < N; i++)
+            if (pidx[i] >= m_pdims[i]) throw out_of_bounds("se_part::mark_forbidden");
+        m_forbidden.push_back(pidx);
+    }
+    const index<N> &get_pdims() const { return m_pdims; }
+    const std::vector<index<N> > &get_forbidden() const { return m_forbidden; }
+};
+
+typedef size_t label_t;
+
+template<size_t N>
+class block_labeling {
+    std::vector<long> m_labels[N == 0 ? 1 : N];
+public:
+    explicit block_labeling(const dimensions<N> &bidims) {
+        for (size_t i = 0; i < N; i++) m_labels[i].assign(bidims[i], -1);
+    }
+    // labels block blk of every dim set in msk
+    void assign(const mask<N> &msk, size_t blk, label_t label) {
+        for (size_t i = 0; i < N; i++)
+            if (msk[i]) m_labels[i].at(blk) = (long)label;
+    }
+    const std::vector<long> &labels(size_t dim) const { return m_labels[dim]; }
+};
+
+template<size_t N, typename T>
+class se_label {
+    block_labeling<N> m_bl;
+    int m_nirrep;
+    std::set<label_t> m_rule;
+public:
+    se_label(const dimensions<N> &bidims, const std::string &id) : m_bl(bidims) {
+        std::map<std::string, int>::const_iterator it = b200::abelian_tables().find(id);
+        if (it == b200::abelian_tables().end())
+            throw bad_parameter("se_label: product table '" + id + "' is not registered");
+        m_nirrep = it->second;
+    }
+    block_labeling<N> &get_labeling() { return m_bl; }
+    const block_labeling<N> &get_labeling() const { return m_bl; }
+    void set_rule(label_t intr) { m_rule.clear(); m_rule.insert(intr); }
+    void set_rule(const std::set<label_t> &intr) { m_rule = intr; }
+    int get_nirrep() const { return m_nirrep; }
+    const std::set<label_t> &get_rule() const { return m_rule; }
+};
+
+template<size_t N, typename T>
+class symmetry {
+    std::vector<se_perm<N, T> > m_perm;
+    std::vector<se_part<N, T> > m_part;
+    std::vector<se_label<N, T> > m_label;
+public:
+    void insert(const se_perm<N, T> &e) { m_perm.push_back(e); }
+    void insert(const se_part<N, T> &e) {
+        if (!m_part.empty()) throw bad_symmetry("symmetry: one se_part element is supported");
+        m_part.push_back(e);
+    }
+    void insert(const se_label<N, T> &e) {
+        if (!m_label.empty()) throw bad_symmetry("symmetry: one se_label element is supported");
+        m_label.push_back(e);
+    }
+    void clear() { m_perm.clear(); m_part.clear(); m_label.clear(); }
+    const std::vector<se_perm<N, T> > &perms() const { return m_perm; }
+    const std::vector<se_part<N, T> > &parts() const { return m_part; }
+    const std::vector<se_label<N, T> > &labels() const { return m_label; }
+};
+
+// ---------------------------------------------------------------- block tensor
+
+template<size_t N, typename T> class block_tensor_ctrl;
+
+template<size_t N, typename T>
+class block_tensor {
+    static_assert(sizeof(T) == 8, "block tensors of double");
+    friend class block_tensor_ctrl<N, T>;
+    block_index_space<N> m_bis;
+    symmetry<N, T> m_sym;
+    ltg_bt *m_bt = nullptr;
+    block_tensor(const block_tensor &) = delete;
+    block_tensor &operator=(const block_tensor &) = delete;
+public:
+    explicit block_tensor(const block_index_space<N> &bis) : m_bis(bis) { }
+    ~block_tensor() { if (m_bt) ltg_bt_destroy(m_bt); }
+    const block_index_space<N> &get_bis() const { return m_bis; }
+    bool is_bound() const { return m_bt != nullptr; }
+    // The device tensor, built from the index space and symmetry on first use.
+    ltg_bt *handle() {
+        if (m_bt) return m_bt;
+        std::vector<int64_t> dims(N), splits;
+        std::vector<int32_t> nsplit(N), perm, labels, intr;
+        std::vector<double> perm_coeff;
+        std::vector<int64_t> pdims, forb;
+        for (size_t i = 0; i < N; i++) {
+            dims[i] = (int64_t)m_bis.get_dims()[i];
+            nsplit[i] = (int32_t)m_bis.get_splits(i).size();
+            for (size_t x : m_bis.get_splits(i)) splits.push_back((int64_t)x);
+        }
+        for (const se_perm<N, T> &e : m_sym.perms()) {
+            for (size_t i = 0; i < N; i++) perm.push_back((int32_t)e.get_perm()[i]);
+            perm_coeff.push_back((double)e.get_transf().get_coeff());
+        }
+        ltg_bt_spec s = {};
+        s.order = (int32_t)N;
+        s.dims = dims.data();
+        s.nsplit = nsplit.data();
+        s.splits = splits.data();
+        s.nperm = (int32_t)m_sym.perms().size();
+        s.perm = perm.data();
+        s.perm_coeff = perm_coeff.data();
+        if (!m_sym.parts().empty()) {
+            const se_part<N, T> &p = m_sym.parts()[0];
+            for (size_t i = 0; i < N; i++) pdims.push_back((int64_t)p.get_pdims()[i]);
+            for (const index<N> &f : p.get_forbidden())
+                for (size_t i = 0; i < N; i++) forb.push_back((int64_t)f[i]);
+            s.has_part = 1;
+            s.part_pdims = pdims.data();
+            s.npart_forbidden = (int64_t)p.get_forbidden().size();
+            s.part_forbidden = forb.data();
+        }
+        if (!m_sym.labels().empty()) {
+            const se_label<N, T> &l = m_sym.labels()[0];
+            for (size_t i = 0; i < N; i++)
+                for (long v : l.get_labeling().labels(i)) labels.push_back((int32_t)v);
+            for (label_t v : l.get_rule()) intr.push_back((int32_t)v);
+            s.has_label = 1;
+            s.label_nirrep = l.get_nirrep();
+            s.labels = labels.data();
+            s.label_nintr = (int32_t)intr.size();
+            s.label_intr = intr.data();
+        }
+        b200::check(ltg_bt_create(b200::context(), &s, &m_bt));
+        return m_bt;
+    }
+    // Adopts a device tensor with the same index space (results of operations).
+    void adopt(ltg_bt *bt) {
+        if (m_bt) ltg_bt_destroy(m_bt);
+        m_bt = bt;
+    }
+};
+
+template<size_t N, typename T>
+class block_tensor_ctrl {
+    block_tensor<N, T> &m_bt;
+    static std::vector<int64_t> idx64(const index<N> &i) {
+        std::vector<int64_t> v(N);
+        for (size_t k = 0; k < N; k++) v[k] = (int64_t)i[k];
+        return v;
+    }
+    std::vector<index<N> > unpack(const std::vector<int64_t> &abs) {
+        std::vector<int64_t> bd(N);
+        b200::check(ltg_bt_bidims(m_bt.handle(), bd.data()));
+        std::vector<index<N> > out;
+        for (int64_t a : abs) {
+            index<N> i;
+            for (size_t k = N; k-- > 0;) { i[k] = (size_t)(a % bd[k]); a /= bd[k]; }
+            out.push_back(i);
+        }
+        return out;
+    }
+public:
+    explicit block_tensor_ctrl(block_tensor<N, T> &bt) : m_bt(bt) { }
+    symmetry<N, T> &req_symmetry() {
+        if (m_bt.is_bound()) throw bad_symmetry("symmetry is fixed once the tensor holds data");
+        return m_bt.m_sym;
+    }
+    const symmetry<N, T> &req_const_symmetry() const { return m_bt.m_sym; }
+    // canonical, allowed block indices (the orbit list)
+    std::vector<index<N> > req_canonical_blocks() {
+        ltg_bt *h = m_bt.handle();
+        int32_t order;
+        int64_t nb, ne;
+        b200::check(ltg_bt_info(h, &order, &nb, &ne));
+        std::vector<int64_t> abs(nb > 0 ? nb : 1), off(abs.size()), sz(abs.size());
+        b200::check(ltg_bt_blocks(h, abs.data(), off.data(), sz.data()));
+        abs.resize(nb);
+        return unpack(abs);
+    }
+    std::vector<index<N> > req_nonzero_blocks() {
+        ltg_bt *h = m_bt.handle();
+        int64_t n = 0;
+        b200::check(ltg_bt_nonzero(h, nullptr, 0, &n));
+        std::vector<int64_t> abs(n > 0 ? n : 1);
+        b200::check(ltg_bt_nonzero(h, abs.data(), n, &n));
+        abs.resize(n);
+        return unpack(abs);
+    }
+    void put_block(const index<N> &bidx, const T *data) {
+        b200::check(ltg_bt_upload_block(m_bt.handle(), idx64(bidx).data(), data));
+    }
+    void get_block(const index<N> &bidx, T *data) {
+        b200::check(ltg_bt_download_block(m_bt.handle(), idx64(bidx).data(), data));
+    }
+    void req_zero_block(const index<N> &bidx) {
+        b200::check(ltg_bt_zero_block(m_bt.handle(), idx64(bidx).data()));
+    }
+    void req_zero_all_blocks() { b200::check(ltg_bt_set_zero(m_bt.handle())); }
+    // marks every canonical block non-zero without data (schedules on a
+    // host-only context; not in the reference)
+    void mark_nonzero() { b200::check(ltg_bt_mark_nonzero(m_bt.handle())); }
+    // seeded test data (the product's generator; not in the reference)
+    void fill_seeded(uint64_t seed, double scale) {
+        b200::check(ltg_bt_fill_seeded(m_bt.handle(), seed, scale));
+    }
+};
+
+// ---------------------------------------------------------------- contraction2
+
+template<size_t N, size_t M, size_t K>
+class contraction2 {
+    permutation<N + M> m_permc;
+    std::vector<std::pair<size_t, size_t> > m_pairs;
+public:
+    contraction2() { }
+    explicit contraction2(const permutation<N + M> &permc) : m_permc(permc) { }
+    bool is_complete() const { return m_pairs.size() == K; }
+    void contract(size_t ia, size_t ib) {
+        if (is_complete()) throw exception("contraction2::contract: contraction is complete");
+        if (ia >= N + K || ib >= M + K) throw out_of_bounds("contraction2::contract");
+        for (const std::pair<size_t, size_t> &p : m_pairs)
+            if (p.first == ia || p.second == ib) throw bad_parameter("contraction2::contract: index used twice");
+        m_pairs.push_back(std::make_pair(ia, ib));
+    }
+    const permutation<N + M> &get_permc() const { return m_permc; }
+    const std::vector<std::pair<size_t, size_t> > &get_pairs() const { return m_pairs; }
+};
+
+// ---------------------------------------------------------------- operations
+
+template<size_t N, size_t M, size_t K>
+class btod_contract2 {
+    ltg_plan *m_plan = nullptr;
+    double m_ka, m_kb, m_kc;
+    int32_t m_mode = LTG_MODE_PLAIN_FP64, m_nslices = 0;
+    btod_contract2(const btod_contract2 &) = delete;
+    btod_contract2 &operator=(const btod_contract2 &) = delete;
+    void init(const contraction2<N, M, K> &contr, block_tensor<N + K, double> &bta,
+              block_tensor<M + K, double> &btb) {
+        if (!contr.is_complete()) throw bad_parameter("btod_contract2: incomplete contraction");
+        std::vector<int32_t> permc = contr.get_permc().to_vector(), pairs;
+        for (const std::pair<size_t, size_t> &p : contr.get_pairs()) {
+            pairs.push_back((int32_t)p.first);
+            pairs.push_back((int32_t)p.second);
+        }
+        b200::check(ltg_contract2_create(b200::context(), (int32_t)N, (int32_t)M, (int32_t)K, permc.data(),
+                                         pairs.data(), bta.handle(), btb.handle(), &m_plan));
+    }
+    void run(block_tensor<N + M, double> &btc, int32_t add, double d) {
+        if (!add) {
+            // assignment gives C the result symmetry (as the reference's perform does)
+            ltg_bt *c = nullptr;
+            b200::check(ltg_contract2_make_result(m_plan, &c));
+            btc.adopt(c);
+        }
+        b200::check(ltg_contract2(m_plan, btc.handle(), m_mode, m_nslices, m_ka, m_kb, m_kc, add, d));
+    }
+public:
+    btod_contract2(const contraction2<N, M, K> &contr, block_tensor<N + K, double> &bta,
+                   block_tensor<M + K, double> &btb) : m_ka(1.0), m_kb(1.0), m_kc(1.0) {
+        init(contr, bta, btb);
+    }
+    btod_contract2(const contraction2<N, M, K> &contr, block_tensor<N + K, double> &bta, double ka,
+                   block_tensor<M + K, double> &btb, double kb, double kc) : m_ka(ka), m_kb(kb), m_kc(kc) {
+        init(contr, bta, btb);
+    }
+    ~btod_contract2() { if (m_plan) ltg_plan_destroy(m_plan); }
+    // C = contraction (assign)
+    void perform(block_tensor<N + M, double> &btc) { run(btc, 0, 0.0); }
+    // C += d * contraction
+    void perform(block_tensor<N + M, double> &btc, double d) { run(btc, 1, d); }
+    void perform(block_tensor<N + M, double> &btc, const scalar_transf<double> &d) { run(btc, 1, d.get_coeff()); }
+    // non-zero canonical result blocks (get_schedule), as absolute indices
+    std::vector<int64_t> get_schedule() const {
+        int64_t n = 0;
+        b200::check(ltg_plan_schedule(m_plan, nullptr, 0, &n));
+        std::vector<int64_t> v(n > 0 ? n : 1);
+        b200::check(ltg_plan_schedule(m_plan, v.data(), n, &n));
+        v.resize(n);
+        return v;
+    }
+    double get_flops() const {
+        double f = 0;
+        b200::check(ltg_plan_flops(m_plan, &f));
+        return f;
+    }
+    // LTG_MODE_OZAKI_* of ltg.h with its slice (or modulus) count; the
+    // default LTG_MODE_PLAIN_FP64 is the FP64 drop-in path.
+    void set_split_precision(int32_t mode, int32_t nslices) { m_mode = mode; m_nslices = nslices; }
+};
+
+template<size_t N>
+class btod_copy {
+    block_tensor<N, double> &m_a;
+    permutation<N> m_perm;
+    double m_c;
+public:
+    btod_copy(block_tensor<N, double> &bta, double c = 1.0) : m_a(bta), m_c(c) { }
+    btod_copy(block_tensor<N, double> &bta, const permutation<N> &perm, double c = 1.0)
+        : m_a(bta), m_perm(perm), m_c(c) { }
+    // B = c P(A): B takes the permuted space and symmetry of A
+    void perform(block_tensor<N, double> &btb) {
+        ltg_bt *b = nullptr;
+        const std::vector<int32_t> p = m_perm.to_vector();
+        b200::check(ltg_bt_create_permuted(m_a.handle(), p.data(), &b));
+        btb.adopt(b);
+        b200::check(ltg_copy(m_a.handle(), p.data(), m_c, btb.handle(), 0, 0.0));
+    }
+    // B += d c P(A)
+    void perform(block_tensor<N, double> &btb, double d) {
+        const std::vector<int32_t> p = m_perm.to_vector();
+        b200::check(ltg_copy(m_a.handle(), p.data(), m_c, btb.handle(), 1, d));
+    }
+};
+
+template<size_t N>
+class btod_add {
+    std::vector<block_tensor<N, double> *> m_ops;
+    std::vector<permutation<N> > m_perms;
+    std::vector<double> m_coeffs;
+    void call(block_tensor<N, double> &btb, int32_t add, double d) {
+        std::vector<ltg_bt *> hs;
+        std::vector<int32_t> perms;
+        for (size_t t = 0; t < m_ops.size(); t++) {
+            hs.push_back(m_ops[t]->handle());
+            const std::vector<int32_t> p = m_perms[t].to_vector();
+            perms.insert(perms.end(), p.begin(), p.end());
+        }
+        b200::check(ltg_add((int32_t)hs.size(), hs.data(), perms.data(), m_coeffs.data(), btb.handle(), add, d));
+    }
+public:
+    btod_add(block_tensor<N, double> &bt, double c = 1.0) { add_op(bt, c); }
+    btod_add(block_tensor<N, double> &bt, const permutation<N> &perm, double c = 1.0) { add_op(bt, perm, c); }
+    void add_op(block_tensor<N, double> &bt, double c = 1.0) { add_op(bt, permutation<N>(), c); }
+    void add_op(block_tensor<N, double> &bt, const permutation<N> &perm, double c = 1.0) {
+        m_ops.push_back(&bt);
+        m_perms.push_back(perm);
+        m_coeffs.push_back(c);
+    }
+    void perform(block_tensor<N, double> &btb) { call(btb, 0, 0.0); }
+    void perform(block_tensor<N, double> &btb, double d) { call(btb, 1, d); }
+};
+
+template<size_t N>
+class btod_dotprod {
+    struct arg {
+        block_tensor<N, double> *a, *b;
+        permutation<N> pa, pb;
+    };
+    std::vector<arg> m_args;
+public:
+    btod_dotprod(block_tensor<N, double> &bt1, block_tensor<N, double> &bt2) { add_arg(bt1, bt2); }
+    btod_dotprod(block_tensor<N, double> &bt1, const permutation<N> &perm1, block_tensor<N, double> &bt2,
+                 const permutation<N> &perm2) { add_arg(bt1, perm1, bt2, perm2); }
+    void add_arg(block_tensor<N, double> &bt1, block_tensor<N, double> &bt2) {
+        add_arg(bt1, permutation<N>(), bt2, permutation<N>());
+    }
+    void add_arg(block_tensor<N, double> &bt1, const permutation<N> &perm1, block_tensor<N, double> &bt2,
+                 const permutation<N> &perm2) {
+        arg x;
+        x.a = &bt1; x.b = &bt2; x.pa = perm1; x.pb = perm2;
+        m_args.push_back(x);
+    }
+    void calculate(std::vector<double> &v) {
+        v.resize(m_args.size());
+        for (size_t i = 0; i < m_args.size(); i++) {
+            const std::vector<int32_t> pa = m_args[i].pa.to_vector(), pb = m_args[i].pb.to_vector();
+            b200::check(ltg_dotprod(m_args[i].a->handle(), pa.data(), m_args[i].b->handle(), pb.data(), &v[i]));
+        }
+    }
+    double calculate() {
+        std::vector<double> v;
+        calculate(v);
+        return v.at(0);
+    }
+};
+
+}  // namespace libtensor
+
+#endif  // LIBTENSOR_B200_LIBTENSOR_H

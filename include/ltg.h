@@ -236,8 +236,10 @@ int ltg_dot_noalloc(const double *x, const double *y, int64_t n, void *stream,
 int ltg_scale(ltg_bt *a, double c);
 /* a[i,j,a,b] /= (e_i + e_j - e_a - e_b) style denominator over a 4-index
  * tensor: divides every element by (sum of eps over the index positions with
- * sign +1 for the first `nocc` dims and -1 for the rest).  eps is a device or
- * host array per dim concatenated (dims[0]+...+dims[3]). */
+ * sign +1 for the first `nocc` dims and -1 for the rest).  eps is a host array
+ * per dim concatenated (dims[0]+...+dims[3]); it is kept on the device, so a
+ * repeated call with the same eps (also inside a graph capture) only launches.
+ * Asynchronous on the context stream. */
 int ltg_denominator(ltg_bt *a, const double *eps_host, int32_t nocc);
 
 /* ---- CUDA graphs over a context's stream ------------------------------ */

@@ -124,6 +124,11 @@ struct ltg_bt {
     DevBuf arena;
     DevBuf dir_off, dir_start, dir_ext;   // block directory for fill/denominator
     bool dir_uploaded = false;
+    // orbital energies of the last denominator call, kept on the device so
+    // that repeated (and graph-captured) calls only launch
+    std::vector<double> denom_eps;
+    int32_t denom_nocc = -1;
+    DevBuf denom_dev, denom_off;
 };
 
 struct ContractExec {
@@ -1882,22 +1887,26 @@ int ltg_denominator(ltg_bt *a, const double *eps_host, int32_t nocc) {
         check_bt(a);
         need_dev(a->ctx);
         if (a->h.bis.n != 4) throw error(kErrUnsupported, "denominator is defined for 4-index tensors");
-        if (a->ctx->capturing) throw error(kErrState, "denominator uploads its orbital energies and cannot run during graph capture");
-        upload_directory(a);
+        if (!eps_host) throw error(kErrBadArg, "null orbital energies");
         int64_t tot = 0;
         std::vector<int64_t> off(kDevMaxOrder, 0);
         for (int d = 0; d < 4; d++) { off[d] = tot; tot += a->h.bis.dims[d]; }
         std::vector<double> eps(eps_host, eps_host + tot);
-        DevBuf de, doff;
-        upload_vec(de, eps, a->ctx->stream);
-        upload_vec(doff, off, a->ctx->stream);
+        if (eps != a->denom_eps || nocc != a->denom_nocc || !a->dir_uploaded) {
+            if (a->ctx->capturing)
+                throw error(kErrState, "denominator not prepared before graph capture: call it once outside the capture");
+            upload_directory(a);
+            upload_vec(a->denom_dev, eps, a->ctx->stream);
+            upload_vec(a->denom_off, off, a->ctx->stream);
+            a->denom_eps = eps;
+            a->denom_nocc = nocc;
+        }
         TimedLaunch tl(a->ctx, LTG_KERNEL_DENOMINATOR);
         LTG_CUDA(launch_denominator(a->arena.as<double>(), a->dir_off.as<int64_t>(), a->dir_start.as<int64_t>(),
-                                    a->dir_ext.as<int32_t>(), (int32_t)a->h.blk_abs.size(), de.as<double>(),
-                                    doff.as<int64_t>(), nocc, a->ctx->stream));
+                                    a->dir_ext.as<int32_t>(), (int32_t)a->h.blk_abs.size(), a->denom_dev.as<double>(),
+                                    a->denom_off.as<int64_t>(), nocc, a->ctx->stream));
         tl.done();
         a->ctx->launches++;
-        LTG_CUDA(cudaStreamSynchronize(a->ctx->stream));
     });
 }
 

@@ -1,0 +1,138 @@
+// Exercises the C++ operator surface (include/libtensor_b200/libtensor.h) the
+// way a libtensor user writes the ladder contraction
+//   r(i,j,a,b) = 0.5 * sum_cd t(i,j,c,d) V(a,b,c,d)
+// on o = 10 (5 per spin), v = 40 (16 + 4 per spin), antisymmetric pairs and
+// spin partitions (the pattern of tests/block_tensor/btod_contract2_test.C).
+//
+//   surface_test schedule        host only: prints the non-zero C blocks
+//   surface_test compute FILE    on GPU 0: seeded inputs, contraction, copy,
+//                                add and dot products; writes the results to FILE
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "libtensor_b200/libtensor.h"
+
+using namespace libtensor;
+
+namespace {
+
+// POSIX declares a function index() in the global namespace
+using libtensor::index;
+
+// splits of a dim holding alpha blocks then beta blocks
+template<size_t N>
+void split_spin(block_index_space<N> &bis, const mask<N> &m, const std::vector<size_t> &per_spin) {
+    std::vector<size_t> sizes(per_spin);
+    sizes.insert(sizes.end(), per_spin.begin(), per_spin.end());
+    size_t pos = 0;
+    for (size_t k = 0; k + 1 < sizes.size(); k++) {
+        pos += sizes[k];
+        bis.split(m, pos);
+    }
+}
+
+// antisymmetry in (0,1) and (2,3); spin partitions with the number of beta
+// indices in (0,1) equal to that in (2,3)
+void add_symmetry(block_tensor<4, double> &bt, const block_index_space<4> &bis) {
+    block_tensor_ctrl<4, double> ctrl(bt);
+    symmetry<4, double> &sym = ctrl.req_symmetry();
+    permutation<4> p01, p23;
+    p01.permute(0, 1);
+    p23.permute(2, 3);
+    sym.insert(se_perm<4, double>(p01, scalar_transf<double>(-1.0)));
+    sym.insert(se_perm<4, double>(p23, scalar_transf<double>(-1.0)));
+    mask<4> all;
+    for (size_t i = 0; i < 4; i++) all[i] = true;
+    se_part<4, double> part(bis, all, 2);
+    for (size_t x = 0; x < 16; x++) {
+        index<4> p;
+        for (size_t i = 0; i < 4; i++) p[i] = (x >> (3 - i)) & 1;
+        if (p[0] + p[1] != p[2] + p[3]) part.mark_forbidden(p);
+    }
+    sym.insert(part);
+}
+
+block_index_space<4> make_bis(size_t d0, size_t d2, const std::vector<size_t> &s0, const std::vector<size_t> &s2) {
+    index<4> i1;
+    i1[0] = d0 - 1; i1[1] = d0 - 1; i1[2] = d2 - 1; i1[3] = d2 - 1;
+    block_index_space<4> bis(dimensions<4>(index_range<4>(index<4>(), i1)));
+    mask<4> m01, m23;
+    m01[0] = m01[1] = true;
+    m23[2] = m23[3] = true;
+    split_spin(bis, m01, s0);
+    split_spin(bis, m23, s2);
+    return bis;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    using libtensor::index;
+    if (argc < 2) {
+        std::fprintf(stderr, "usage: surface_test schedule | compute FILE\n");
+        return 2;
+    }
+    const std::string mode = argv[1];
+    try {
+        if (mode == "schedule") b200::set_device(-1);
+        const std::vector<size_t> occ = {5}, vir = {16, 4};
+        block_index_space<4> bis_t = make_bis(10, 40, occ, vir), bis_v = make_bis(40, 40, vir, vir);
+        block_tensor<4, double> t(bis_t), v(bis_v);
+        add_symmetry(t, bis_t);
+        add_symmetry(v, bis_v);
+        contraction2<2, 2, 2> contr;
+        contr.contract(2, 2);
+        contr.contract(3, 3);
+        if (mode == "schedule") {
+            block_tensor_ctrl<4, double>(t).mark_nonzero();
+            block_tensor_ctrl<4, double>(v).mark_nonzero();
+            btod_contract2<2, 2, 2> op(contr, t, 1.0, v, 1.0, 0.5);
+            for (int64_t a : op.get_schedule()) std::printf("%lld\n", (long long)a);
+            return 0;
+        }
+        if (mode != "compute" || argc < 3) throw bad_parameter("unknown mode");
+        block_tensor_ctrl<4, double>(t).fill_seeded(11, 0.01);
+        block_tensor_ctrl<4, double>(v).fill_seeded(23, 1.0);
+        btod_contract2<2, 2, 2> op(contr, t, 1.0, v, 1.0, 0.5);
+        block_index_space<4> bis_r = make_bis(10, 40, occ, vir);
+        block_tensor<4, double> r(bis_r);
+        op.perform(r);
+
+        // copy with a permutation, a two-term add and dot products: checked
+        // through <tp,tp> = 0.25 <t,t> and <t,s> = 1.25 <t,t>
+        permutation<4> p0213;
+        p0213.permute(1, 2);
+        block_tensor<4, double> tp(bis_t);      // takes the permuted space on assignment
+        btod_copy<4>(t, p0213, -0.5).perform(tp);
+        block_tensor<4, double> s(bis_t);
+        add_symmetry(s, bis_t);
+        btod_add<4> add(t, 1.0);
+        add.add_op(t, 0.25);
+        add.perform(s);
+        const double dot_tt = btod_dotprod<4>(t, t).calculate();
+        const double dot_ts = btod_dotprod<4>(t, s).calculate();
+        const double dot_pp = btod_dotprod<4>(tp, tp).calculate();
+
+        // the contraction's non-zero blocks in index order, then the dot products
+        FILE *f = std::fopen(argv[2], "wb");
+        if (!f) throw bad_parameter("cannot open output file");
+        block_tensor_ctrl<4, double> c(r);
+        const std::vector<index<4> > blocks = c.req_nonzero_blocks();
+        std::fprintf(f, "%zu\n", blocks.size());
+        for (const index<4> &b : blocks) {
+            const dimensions<4> d = bis_r.get_block_dims(b);
+            std::vector<double> data(d.get_size());
+            c.get_block(b, data.data());
+            std::fprintf(f, "%zu %zu %zu %zu %zu\n", b[0], b[1], b[2], b[3], data.size());
+            for (double x : data) std::fprintf(f, "%.17g\n", x);
+        }
+        std::fprintf(f, "%.17g %.17g %.17g\n", dot_tt, dot_ts, dot_pp);
+        std::fclose(f);
+        std::printf("ok %zu blocks, flops %.6g\n", op.get_schedule().size(), op.get_flops());
+    } catch (const libtensor::exception &e) {
+        std::fprintf(stderr, "libtensor exception: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}
