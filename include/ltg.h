@@ -195,6 +195,22 @@ int ltg_plan_destroy(ltg_plan *plan);
  * automatic choice (-1).  No reference counterpart: the reference hands each
  * block pair to BLAS. */
 int ltg_contract2_set_tile(ltg_plan *plan, int32_t cfg);
+/* Modular mode (LTG_MODE_OZAKI_CRT): enables (default) or disables grouped
+ * products.  When no pair list was shortened by coalescing, C blocks whose row
+ * blocks (C dims taken from A) and column blocks (C dims taken from B) are
+ * linked by the schedule are computed as one product over the union of their
+ * contracted blocks (operand cells that no pair uses stay zero), instead of one
+ * product per C block and pair.  The integer products are exact, so both
+ * forms give identical bits; grouping only changes the tile shapes (blocks of
+ * a few rows, as under point-group symmetry, fill whole tiles).  No reference
+ * counterpart. */
+int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable);
+/* Host-side summary of the grouped products the modular mode would use for
+ * result c: number of groups, C blocks they cover, flops of the grouped
+ * products (padding of the contracted blocks to 4 included) and algorithmic
+ * flops of the blocks they cover.  Needs no device.  Any pointer may be NULL. */
+int ltg_contract2_group_info(ltg_plan *plan, ltg_bt *c, int64_t *ngroups, int64_t *nblocks,
+                             double *grouped_flops, double *block_flops);
 /* Autotuner: for every distinct C-block shape (M, N) of the plan, costliest
  * first, times each compiled tile shape on the real contraction (reps calls,
  * CUDA events) and keeps the fastest.  Overwrites c. */

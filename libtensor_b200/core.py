@@ -302,6 +302,18 @@ class btod_contract2:
     def set_tile(self, cfg: int):
         check(lib().ltg_contract2_set_tile(self.h, cfg))
 
+    def set_grouping(self, enable: bool):
+        """Modular mode: grouped products of small C blocks (default on)."""
+        check(lib().ltg_contract2_set_grouping(self.h, 1 if enable else 0))
+
+    def group_info(self, c: block_tensor):
+        """(groups, C blocks grouped, grouped-product flops, their blocks'
+        algorithmic flops) of the modular mode for result c; host only."""
+        ng, nb = C.c_int64(), C.c_int64()
+        gf, bf = C.c_double(), C.c_double()
+        check(lib().ltg_contract2_group_info(self.h, c.h, C.byref(ng), C.byref(nb), C.byref(gf), C.byref(bf)))
+        return ng.value, nb.value, gf.value, bf.value
+
     def autotune(self, c: block_tensor, mode: int = MODE_PLAIN_FP64, nslices: int = 0, reps: int = 2):
         check(lib().ltg_contract2_autotune(self.h, c.h, mode, nslices, self.ka, self.kb, self.kc, reps))
         return self.tiles()

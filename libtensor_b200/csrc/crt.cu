@@ -182,9 +182,9 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const doub
         uint8_t *base = res + P.res_off;
         const int TR = P.tr, nkb = P.K_pad / kKB;
         const double coef = (double)P.coef;
-        for (int r0 = blockIdx.x * 32; r0 < P.rows_pad; r0 += gridDim.x * 32) {
+        for (int r0 = blockIdx.x * 32; r0 < P.wrows; r0 += gridDim.x * 32) {
             const int r = r0 + lr;
-            if (r >= P.rows_pad) continue;           // rows_pad need not be a multiple of 32
+            if (r >= P.wrows) continue;              // wrows need not be a multiple of 32
             const bool valid = r < P.rows;
             const double *row = src + P.src_off + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
             const int e = valid ? tab[gidx[P.g_off + r]] : kNoExp;
@@ -192,7 +192,7 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const doub
             const int sh = e > kNoExp ? cp.P - e : 0;
             const double s1 = ldexp(1.0, sh / 2), s2 = ldexp(1.0, sh - sh / 2);
             const bool live = valid && e > kNoExp;
-            for (int k0 = 4 * c; k0 < P.K_pad; k0 += 32) {
+            for (int k0 = 4 * c; k0 < P.wk; k0 += 32) {
                 double x[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
@@ -214,8 +214,9 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const doub
                         packed[l] = __byte_perm(packed[l], residue_byte<l>(X, xlo), sel);
                     });
                 }
-                const int kb = k0 / kKB, kb_byte = k0 % kKB;
-                uint8_t *dst0 = base + image_offset(r, TR, nkb, kb, 0, L, kb_byte);
+                const int kk = P.k0 + k0;                                // k0 % 4 == 0: one word
+                const int kb = kk / kKB, kb_byte = kk % kKB;
+                uint8_t *dst0 = base + image_offset(P.r0 + r, TR, nkb, kb, 0, L, kb_byte);
                 const int64_t lstride = (int64_t)TR * kKB;              // next modulus image
 #pragma unroll
                 for (int l = 0; l < L; l++) *reinterpret_cast<uint32_t *>(dst0 + l * lstride) = packed[l];
@@ -488,7 +489,8 @@ constexpr int kCombCols = 16;                       // tile columns staged per p
 template<int L>
 __global__ void __launch_bounds__(256)
 crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restrict__ items, int32_t nitems,
-                   const DCBlock *__restrict__ cblks, const uint8_t *__restrict__ out,
+                   const DCBlock *__restrict__ cblks, const DCrtComp *__restrict__ comps,
+                   const int32_t *__restrict__ ctab, const uint8_t *__restrict__ out,
                    const int32_t *__restrict__ gidx, const int32_t *__restrict__ ex,
                    const int32_t *__restrict__ ey, double *__restrict__ C, int32_t add, const CrtParams cp) {
     __shared__ __align__(16) uint8_t sres[L][kXRows][kCombCols];
@@ -496,8 +498,10 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
     for (int u = blockIdx.x; u < nitems * 32; u += gridDim.x) {
         const DCrtItem item = items[u >> 5];
         const int xh = (u >> 4) & 1, c0 = (u & 15) * kCombCols;
-        const DCBlock &cb = cblks[item.cblk];
-        const int xext = cp.swap ? cb.N : cb.M, yext = cp.swap ? cb.M : cb.N;
+        const DCrtComp *cc = item.comp >= 0 ? &comps[item.comp] : nullptr;
+        const DCBlock *cb1 = cc ? nullptr : &cblks[item.cblk];
+        const int rows = cc ? cc->rows : cb1->M, cols = cc ? cc->cols : cb1->N;
+        const int xext = cp.swap ? cols : rows, yext = cp.swap ? rows : cols;
         const int yc = min(item.nt, yext - item.y0);
         if (xh >= item.nx || c0 >= yc) continue;                     // uniform over the CTA
         const int32_t *gyp = gidx + panels[item.gy].g_off + item.y0;
@@ -545,11 +549,20 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
                 for (int i = L - 2; i >= 0; i--) X = fma(X, (double)crt_modulus(i), digit(v[i]));
                 const int gx = gxp[r], gy = gyp[c0 + c];
                 const int e2 = ex[gx] + ey[gy] - 2 * cp.P;
-                const double val = cb.scale * ldexp(X, max(e2, -2200));
                 const int xi = xb + r, yi = item.y0 + c0 + c;
-                const int m = cp.swap ? yi : xi, n = cp.swap ? xi : yi;
-                double *dst = C + cb.c_off + mixed_offset(m, cb.nm, cb.mext, cb.mc_str) +
-                              mixed_offset(n, cb.nn, cb.next, cb.nc_str);
+                int m = cp.swap ? yi : xi, n = cp.swap ? xi : yi;
+                const DCBlock *cb = cb1;
+                if (cc) {                                // grouped: find the C block of (m, n)
+                    const int rb = ctab[cc->row_off + 2 * m], cbk = ctab[cc->col_off + 2 * n];
+                    const int cell = ctab[cc->cell_off + rb * cc->ncb + cbk];
+                    if (cell < 0) continue;
+                    m = ctab[cc->row_off + 2 * m + 1];
+                    n = ctab[cc->col_off + 2 * n + 1];
+                    cb = &cblks[cell];
+                }
+                const double val = cb->scale * ldexp(X, max(e2, -2200));
+                double *dst = C + cb->c_off + mixed_offset(m, cb->nm, cb->mext, cb->mc_str) +
+                              mixed_offset(n, cb->nn, cb->next, cb->nc_str);
                 if (add) *dst += val;
                 else *dst = val;
             }
@@ -610,12 +623,13 @@ cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const D
 }
 
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
-                               const DCBlock *cblks, const uint8_t *out, const int32_t *gidx, const int32_t *ex,
-                               const int32_t *ey, double *c, int32_t add, const CrtParams &cp, cudaStream_t s) {
+                               const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab,
+                               const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey,
+                               double *c, int32_t add, const CrtParams &cp, cudaStream_t s) {
     if (nitems <= 0) return cudaSuccess;
     const int grid = 32 * nitems < 8 * num_sms() ? 32 * nitems : 8 * num_sms();
     switch (cp.L) {
-#define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, out, gidx, ex, ey, c, add, cp); break;
+#define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, out, gidx, ex, ey, c, add, cp); break;
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
 #undef CASE_L
     default: return cudaErrorInvalidValue;

@@ -154,9 +154,9 @@ struct OzExec {
 // Device arrays of one modular split-precision contraction (crt.cu).
 struct CrtExec {
     CrtParams cp{};
-    int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0;
+    int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0, ngroups = 0;
     int64_t src_elems = 0, res_bytes = 0;   // operand elements read per pass, residue bytes written
-    DevBuf panels, tasks, items, cblks, gidx, ex, ey, res, out, err;
+    DevBuf panels, tasks, items, cblks, comps, ctab, gidx, ex, ey, res, out, err;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
     int32_t *err_host = nullptr;
@@ -171,6 +171,7 @@ struct ltg_plan {
              std::unique_ptr<CrtExec>> crt;
     ltg_bt *a = nullptr, *b = nullptr;
     int forced_tile = -1;         // >= 0: every C block uses this tile shape
+    bool group_products = true;   // modular mode: small C blocks grouped into larger products
     std::map<std::pair<int64_t, int64_t>, int> tile_override;   // autotuned (M, N) -> shape
     ContractPlan plan;
     // cache of device task arrays keyed by (C tensor, ka, kb, kc, add, d)
@@ -728,6 +729,222 @@ void crt_global_index(const BlockTensorHost &ch, const CrtSideMap &sm, int64_t c
     }
 }
 
+// ---- grouped modular products
+//
+// Without coalescing, the pair list of a C block (R, S) (R: its block
+// indices on the C dims taken from A, S: on those taken from B) holds every
+// contracted block index K whose A block (R, K) and B block (K, S) are both
+// non-zero (gen_bto_contract2_clst_builder).  So for any set of row blocks and
+// column blocks, the product of [A(R, K)] (rows R, columns K over the union of
+// the contracted blocks, zero where no pair uses the cell) and [B(K, S)] holds,
+// in cell (R, S), exactly the sum over the pairs of C block (R, S).  The
+// schedule links row and column blocks; each connected set of them becomes one
+// grouped product when its grid is dense enough.
+
+// One operand cell: the canonical block read with the pair's orbit transform,
+// rows = the C dims of its side in C order, k = the contracted dims in the
+// order of A's dims (the same for the A and the B cell of one K).
+struct CrtCell {
+    int64_t off = 0;
+    int32_t coef = 1;
+    SubDims rows, k;              // s0: stride in the operand's canonical block
+};
+
+struct CrtGroupHost {
+    std::vector<int64_t> rkey, skey, kkey;     // row / column / contracted block keys, ascending
+    std::vector<int64_t> rn, sn, kn;           // their extents
+    std::vector<int32_t> rce, sce;             // a C block (cbt index) holding each row / column block
+    std::vector<int32_t> cell;                 // rkey.size() x skey.size(): cbt index or -1
+    std::map<std::pair<int32_t, int32_t>, CrtCell> ac, bc;   // (R, K) -> A cell, (K, S) -> B cell
+};
+
+// Strides fused where contiguous (same linear order), unit extents dropped.
+SubDims fuse_single(int n, const int64_t *ext, const int64_t *str) {
+    SubDims r;
+    for (int i = 0; i < n; i++) {
+        if (ext[i] == 1) continue;
+        if (r.n > 0 && r.s0[r.n - 1] == str[i] * ext[i]) {
+            r.ext[r.n - 1] *= (int32_t)ext[i];
+            r.s0[r.n - 1] = str[i];
+            continue;
+        }
+        if (r.n == kMaxSub) throw error(kErrUnsupported, "too many sub-dimensions");
+        r.ext[r.n] = (int32_t)ext[i]; r.s0[r.n] = str[i]; r.n++;
+    }
+    return r;
+}
+
+int32_t round4(int64_t x) { return (int32_t)((x + 3) / 4 * 4); }
+
+// C dims of each side: connected to A (rows) or to B (columns), and the
+// strides of the linearised global index of each side.
+void crt_side_maps(const Contraction &ct, const BlockTensorHost &ch, CrtSideMap *sm) {
+    for (int i = 0; i < ct.NC(); i++) sm[ct.conn[i] < ct.NC() + ct.NA() ? 0 : 1].dims.push_back(i);
+    for (int s = 0; s < 2; s++) {
+        sm[s].gstr.resize(sm[s].dims.size());
+        for (int k = (int)sm[s].dims.size() - 1; k >= 0; k--) {
+            sm[s].gstr[k] = sm[s].size;
+            sm[s].size *= ch.bis.dims[sm[s].dims[k]];
+        }
+        if (sm[s].size > ((int64_t)1 << 27)) throw error(kErrUnsupported, "C side too large for the modular scaling tables");
+    }
+}
+
+void crt_groups(const ltg_plan *pl, const BlockTensorHost &ch, const CrtSideMap *sm,
+                const std::vector<CBlockTask> &cbt, std::vector<CrtGroupHost> &groups,
+                std::vector<int32_t> &group_of) {
+    const ContractPlan &P = pl->plan;
+    const Contraction &c0 = P.contr;
+    const BlockTensorHost &ah = pl->a->h, &bh = pl->b->h;
+    const int NC = c0.NC(), NA = c0.NA(), NB = c0.NB();
+    const size_t ne = cbt.size();
+    group_of.assign(ne, -1);
+    if (ne < 2) return;
+    // contracted dims of A in A order (the k order of every cell)
+    std::vector<int> kdims;
+    for (int i = 0; i < NA; i++) if (c0.conn[NC + i] >= NC + NA) kdims.push_back(i);
+
+    int64_t ic[kMaxOrder];
+    auto side_key = [&](int s) {
+        int64_t k = 0;
+        for (int d : sm[s].dims) k = k * ch.bis.bidims[d] + ic[d];
+        return k;
+    };
+    std::map<int64_t, int32_t> rid, sid;
+    std::vector<int32_t> er(ne), es(ne);
+    for (size_t e = 0; e < ne; e++) {
+        ch.bis.unabs(P.schedule[e], ic);
+        er[e] = rid.emplace(side_key(0), (int32_t)rid.size()).first->second;
+        es[e] = sid.emplace(side_key(1), (int32_t)sid.size()).first->second;
+    }
+    // connected sets of row blocks (ids 0..nr-1) and column blocks (nr..)
+    const int32_t nr = (int32_t)rid.size();
+    std::vector<int32_t> up(nr + sid.size());
+    for (size_t i = 0; i < up.size(); i++) up[i] = (int32_t)i;
+    auto root = [&](int32_t x) {
+        while (up[x] != x) { up[x] = up[up[x]]; x = up[x]; }
+        return x;
+    };
+    for (size_t e = 0; e < ne; e++) {
+        const int32_t a = root(er[e]), b = root(nr + es[e]);
+        if (a != b) up[a] = b;
+    }
+    std::map<int32_t, std::vector<int32_t>> members;
+    for (size_t e = 0; e < ne; e++) members[root(er[e])].push_back((int32_t)e);
+
+    int64_t ia[kMaxOrder], ib[kMaxOrder], da[kMaxOrder], db[kMaxOrder], sa[kMaxOrder], sb[kMaxOrder];
+    int64_t dc[kMaxOrder];
+    for (auto &mb : members) {
+        const std::vector<int32_t> &blocks = mb.second;
+        if (blocks.size() < 2) continue;
+        CrtGroupHost G;
+        std::map<int64_t, int32_t> rloc, sloc, kloc;
+        std::map<int64_t, int64_t> kext_of;
+        bool ok = true;
+        double work = 0;
+        // keys first (ascending order of each)
+        for (int32_t e : blocks) {
+            ch.bis.unabs(P.schedule[e], ic);
+            rloc.emplace(side_key(0), 0);
+            sloc.emplace(side_key(1), 0);
+            for (const Pair &p : P.clst[e]) {
+                ah.bis.unabs(p.aia, ia);
+                ah.bis.block_dims(ia, da);
+                int64_t kk = 0, kx = 1;
+                for (int d : kdims) { kk = kk * ah.bis.bidims[d] + ia[d]; kx *= da[d]; }
+                kloc.emplace(kk, 0);
+                kext_of[kk] = kx;
+                if (std::fabs(std::fabs(p.tra.coeff) - 1.0) > 0 || std::fabs(std::fabs(p.trb.coeff) - 1.0) > 0) ok = false;
+            }
+            work += 2.0 * (double)cbt[e].M * (double)cbt[e].N * cbt[e].kflops;
+        }
+        if (!ok) continue;
+        for (auto &x : rloc) { x.second = (int32_t)G.rkey.size(); G.rkey.push_back(x.first); }
+        for (auto &x : sloc) { x.second = (int32_t)G.skey.size(); G.skey.push_back(x.first); }
+        for (auto &x : kloc) { x.second = (int32_t)G.kkey.size(); G.kkey.push_back(x.first); G.kn.push_back(kext_of[x.first]); }
+        G.rn.assign(G.rkey.size(), 0); G.sn.assign(G.skey.size(), 0);
+        G.rce.assign(G.rkey.size(), -1); G.sce.assign(G.skey.size(), -1);
+        G.cell.assign(G.rkey.size() * G.skey.size(), -1);
+        for (int32_t e : blocks) {
+            ch.bis.unabs(P.schedule[e], ic);
+            ch.bis.block_dims(ic, dc);
+            const int32_t R = rloc[side_key(0)], S = sloc[side_key(1)];
+            G.rn[R] = cbt[e].M; G.sn[S] = cbt[e].N;
+            G.rce[R] = e; G.sce[S] = e;
+            G.cell[(size_t)R * G.skey.size() + S] = e;
+            for (const Pair &p : P.clst[e]) {
+                // the contraction seen from the canonical blocks, as in contract2_tasks
+                Perm pa = p.tra.perm, pb = p.trb.perm;
+                if (pa.n == 0) pa = Perm::identity(NA);
+                if (pb.n == 0) pb = Perm::identity(NB);
+                const Perm pinv = pa.inverse();
+                Contraction ct = c0;
+                ct.permute_a(pinv);
+                ct.permute_b(pb.inverse());
+                ah.bis.unabs(p.acia, ia); ah.bis.block_dims(ia, da);
+                bh.bis.unabs(p.acib, ib); bh.bis.block_dims(ib, db);
+                int64_t x = 1;
+                for (int i = NA - 1; i >= 0; i--) { sa[i] = x; x *= da[i]; }
+                x = 1;
+                for (int i = NB - 1; i >= 0; i--) { sb[i] = x; x *= db[i]; }
+                int64_t re[kMaxOrder], rs[kMaxOrder], ce[kMaxOrder], cs[kMaxOrder];
+                int nra = 0, nrb = 0;
+                for (int i = 0; i < NC; i++) {
+                    const int64_t t = ct.conn[i];
+                    if (t < NC + NA) {
+                        if (da[t - NC] != dc[i]) throw error(kErrState, "block extent mismatch (A/C)");
+                        re[nra] = dc[i]; rs[nra] = sa[t - NC]; nra++;
+                    } else {
+                        if (db[t - NC - NA] != dc[i]) throw error(kErrState, "block extent mismatch (B/C)");
+                        ce[nrb] = dc[i]; cs[nrb] = sb[t - NC - NA]; nrb++;
+                    }
+                }
+                // contracted dims, ordered by the A dim they stand for
+                int64_t ko[kMaxOrder], ke[kMaxOrder], ksa[kMaxOrder], ksb[kMaxOrder];
+                int nk = 0;
+                for (int i = 0; i < NA; i++) {
+                    const int64_t t = ct.conn[NC + i];
+                    if (t < NC + NA) continue;
+                    if (da[i] != db[t - NC - NA]) throw error(kErrState, "block extent mismatch (A/B)");
+                    ko[nk] = pinv.p[i]; ke[nk] = da[i]; ksa[nk] = sa[i]; ksb[nk] = sb[t - NC - NA]; nk++;
+                }
+                for (int i = 1; i < nk; i++)
+                    for (int j = i; j > 0 && ko[j - 1] > ko[j]; j--) {
+                        std::swap(ko[j - 1], ko[j]); std::swap(ke[j - 1], ke[j]);
+                        std::swap(ksa[j - 1], ksa[j]); std::swap(ksb[j - 1], ksb[j]);
+                    }
+                ah.bis.unabs(p.aia, ia);
+                int64_t kk = 0;
+                for (int d : kdims) kk = kk * ah.bis.bidims[d] + ia[d];
+                const int32_t K = kloc[kk];
+                CrtCell A, B;
+                A.off = ah.blk_off[ah.slot_of[p.acia]];
+                A.coef = (int32_t)std::lround(p.tra.coeff);
+                A.rows = fuse_single(nra, re, rs);
+                A.k = fuse_single(nk, ke, ksa);
+                B.off = bh.blk_off[bh.slot_of[p.acib]];
+                B.coef = (int32_t)std::lround(p.trb.coeff);
+                B.rows = fuse_single(nrb, ce, cs);
+                B.k = fuse_single(nk, ke, ksb);
+                auto ra = G.ac.emplace(std::make_pair(R, K), A);
+                auto rb = G.bc.emplace(std::make_pair(K, S), B);
+                if ((!ra.second && (ra.first->second.off != A.off || ra.first->second.coef != A.coef)) ||
+                    (!rb.second && (rb.first->second.off != B.off || rb.first->second.coef != B.coef)))
+                    throw error(kErrState, "one operand cell read from two different blocks");
+            }
+        }
+        // the grouped product must not do much more work than the blocks
+        int64_t rows = 0, cols = 0, kt = 0;
+        for (int64_t v : G.rn) rows += v;
+        for (int64_t v : G.sn) cols += v;
+        for (int64_t v : G.kn) kt += round4(v);
+        if (2.0 * (double)rows * (double)cols * (double)kt > 1.5 * work) continue;
+        if (rows > ((int64_t)1 << 24) || cols > ((int64_t)1 << 24) || kt > ((int64_t)1 << 24)) continue;
+        for (int32_t e : blocks) group_of[e] = (int32_t)groups.size();
+        groups.push_back(std::move(G));
+    }
+}
+
 CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, double kc, int add, double d) {
     auto key = std::make_tuple(c->uid, ka, kb, kc, add, add ? d : 0.0, L);
     auto it = pl->crt.find(key);
@@ -740,19 +957,9 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     std::vector<GemmTask> tasks;
     std::vector<CBlockTask> cbt;
     contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
-    const Contraction &ct = pl->plan.contr;
     const BlockTensorHost &ch = c->h;
-    // C dims of each side: connected to A (rows) or to B (columns)
     CrtSideMap sm[2];
-    for (int i = 0; i < ct.NC(); i++) sm[ct.conn[i] < ct.NC() + ct.NA() ? 0 : 1].dims.push_back(i);
-    for (int s = 0; s < 2; s++) {
-        sm[s].gstr.resize(sm[s].dims.size());
-        for (int k = (int)sm[s].dims.size() - 1; k >= 0; k--) {
-            sm[s].gstr[k] = sm[s].size;
-            sm[s].size *= ch.bis.dims[sm[s].dims[k]];
-        }
-        if (sm[s].size > ((int64_t)1 << 27)) throw error(kErrUnsupported, "C side too large for the modular scaling tables");
-    }
+    crt_side_maps(pl->plan.contr, ch, sm);
     std::map<int64_t, int64_t> slot_of_off;
     for (size_t sl = 0; sl < ch.blk_off.size(); sl++) slot_of_off[ch.blk_off[sl]] = (int64_t)sl;
 
@@ -770,6 +977,10 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     const bool swap = pad_swap < pad_keep;
     // integer coefficients ride on the operand with the smaller arena
     const int coef_src = pl->a->h.total_elems <= pl->b->h.total_elems ? 0 : 1;
+    // grouped products of small blocks (their pairs carry coefficients +-1)
+    std::vector<CrtGroupHost> groups;
+    std::vector<int32_t> group_of(cbt.size(), -1);
+    if (pl->group_products && !pl->plan.coalesced) crt_groups(pl, ch, sm, cbt, groups, group_of);
 
     // panels by (operand, block, row and k mappings, coefficient); one key can
     // hold several panels when the same rows feed different rows of C
@@ -808,6 +1019,7 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         pack_sub(kk, p.nk, p.kext, p.kstr, nullptr);
         p.res_off = res_bytes;
         res_bytes += ((int64_t)L * p.rows_pad * p.K_pad + 1023) / 1024 * 1024;
+        p.r0 = 0; p.k0 = 0; p.wrows = p.rows_pad; p.wk = p.K_pad;
         p.g_off = (int32_t)gidx.size();
         gidx.insert(gidx.end(), grow.begin(), grow.end());
         max_rows = std::max(max_rows, p.rows_pad);
@@ -817,8 +1029,10 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         return id;
     };
     std::vector<DCrtTask> dt(tasks.size());
+    std::memset(dt.data(), 0, dt.size() * sizeof(DCrtTask));
     int64_t max_sum = 1, max_coef = 1;
-    for (const CBlockTask &b : cbt) {
+    for (size_t e = 0; e < cbt.size(); e++) {
+        const CBlockTask &b = cbt[e];
         int64_t sum = 0;
         for (int32_t t = b.t_begin; t < b.t_end; t++) {
             const GemmTask &g = tasks[t];
@@ -826,6 +1040,9 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
             const int64_t ci = (int64_t)std::llround(cr);
             if (ci == 0 || std::fabs(cr - (double)ci) > 1e-9 || std::llabs(ci) > 64)
                 throw error(kErrUnsupported, "modular split precision needs small integer pair coefficients");
+            sum += std::llabs(ci) * (int64_t)g.k.total();
+            max_coef = std::max<int64_t>(max_coef, std::llabs(ci));
+            if (group_of[e] >= 0) continue;          // computed by its grouped product
             const int32_t ca = coef_src == 0 ? (int32_t)ci : 1, cbf = coef_src == 1 ? (int32_t)ci : 1;
             const int32_t pa = panel_of(0, g.a_off, g.m, g.k, false, ca, b.c_off);
             const int32_t pb = panel_of(1, g.b_off, g.n, g.k, true, cbf, b.c_off);
@@ -836,8 +1053,6 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
             dt[t].yres = panels[dt[t].py].res_off;
             dt[t].nkb = panels[pa].K_pad / 32;
             dt[t].pad = 0;
-            sum += std::llabs(ci) * (int64_t)g.k.total();
-            max_coef = std::max<int64_t>(max_coef, std::llabs(ci));
         }
         max_sum = std::max(max_sum, sum);
     }
@@ -875,7 +1090,7 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     int64_t out_bytes = 0;
     for (size_t e = 0; e < cbt.size(); e++) {
         const CBlockTask &b = cbt[e];
-        if (b.t_end <= b.t_begin) continue;
+        if (b.t_end <= b.t_begin || group_of[e] >= 0) continue;
         const DCrtTask &t0 = dt[b.t_begin];
         const int32_t nt = panels[t0.py].tr;
         const int64_t xext = swap ? b.N : b.M, yext = swap ? b.M : b.N;
@@ -889,11 +1104,118 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
                 it.nx = x0 + 128 < xext ? 2 : 1;
                 it.t_begin = b.t_begin; it.t_end = b.t_end;
                 it.gx = t0.px; it.gy = t0.py;
+                it.comp = -1;
                 it.res_off = out_bytes;
                 out_bytes += (int64_t)L * it.nx * 128 * nt;
                 iv.push_back({b.kflops * nt * it.nx, it});
             }
     }
+    // grouped products: per group one image pair (records, placed after the
+    // panels and pieces the split passes process) written cell by cell by
+    // pieces, one task and its tiles
+    std::vector<DCrtPanel> pieces, records;
+    std::vector<DCrtComp> comps;
+    std::vector<int32_t> ctab;
+    size_t npieces = 0;
+    for (const CrtGroupHost &G : groups) npieces += G.ac.size() + G.bc.size();
+    const int32_t rec_base = (int32_t)(panels.size() + npieces);
+    for (size_t gi = 0; gi < groups.size(); gi++) {
+        const CrtGroupHost &G = groups[gi];
+        std::vector<int32_t> kofs(G.kn.size());
+        int32_t kt = 0;
+        for (size_t k = 0; k < G.kn.size(); k++) { kofs[k] = kt; kt += round4(G.kn[k]); }
+        // one side (0: C rows from A, 1: C columns from B) as an image record
+        auto record = [&](int cside, std::vector<int32_t> &ofs) {
+            const std::vector<int64_t> &ext = cside == 0 ? G.rn : G.sn;
+            const std::vector<int32_t> &ce = cside == 0 ? G.rce : G.sce;
+            DCrtPanel r;
+            std::memset(&r, 0, sizeof(r));
+            r.src = cside;
+            r.side = (cside == 1) == swap ? 0 : 1;
+            int64_t tot = 0;
+            ofs.resize(ext.size());
+            for (size_t b = 0; b < ext.size(); b++) { ofs[b] = (int32_t)tot; tot += ext[b]; }
+            r.rows = (int32_t)tot;
+            r.K = kt;
+            r.K_pad = (kt + 31) / 32 * 32;
+            r.tr = r.side == 0 ? 128 : crt_tile_width(r.rows);
+            r.rows_pad = (r.rows + r.tr - 1) / r.tr * r.tr;
+            r.res_off = res_bytes;
+            res_bytes += ((int64_t)L * r.rows_pad * r.K_pad + 1023) / 1024 * 1024;
+            r.g_off = (int32_t)gidx.size();
+            for (size_t b = 0; b < ext.size(); b++) {
+                const CBlockTask &cb = cbt[ce[b]];
+                crt_global_index(ch, sm[cside], cb.c_off, cside == 0 ? cb.cm : cb.cn, slot_of_off, grow);
+                gidx.insert(gidx.end(), grow.begin(), grow.end());
+            }
+            records.push_back(r);
+            return rec_base + (int32_t)records.size() - 1;
+        };
+        std::vector<int32_t> rofs, sofs;
+        const int32_t rrec = record(0, rofs), srec = record(1, sofs);
+        const DCrtPanel &RR = records[rrec - rec_base], &SR = records[srec - rec_base];
+        auto piece = [&](const DCrtPanel &rec, int src, const CrtCell &cl, int32_t r0, int64_t nrow, int32_t k) {
+            DCrtPanel q = rec;
+            q.src = src;
+            q.src_off = cl.off;
+            q.rows = (int32_t)nrow;
+            q.K = (int32_t)G.kn[k];
+            q.coef = cl.coef;
+            q.g_off = rec.g_off + r0;
+            pack_sub(cl.rows, q.nr, q.rext, q.rstr, nullptr);
+            pack_sub(cl.k, q.nk, q.kext, q.kstr, nullptr);
+            if (cl.rows.total() != nrow || cl.k.total() != G.kn[k]) throw error(kErrState, "grouped cell extents");
+            q.r0 = r0; q.k0 = kofs[k]; q.wrows = q.rows; q.wk = round4(q.K);
+            max_rows = std::max(max_rows, q.wrows);
+            pieces.push_back(q);
+        };
+        for (const auto &x : G.ac) piece(RR, 0, x.second, rofs[x.first.first], G.rn[x.first.first], x.first.second);
+        for (const auto &x : G.bc) piece(SR, 1, x.second, sofs[x.first.second], G.sn[x.first.second], x.first.first);
+        // C placement tables
+        DCrtComp cc;
+        cc.rows = RR.rows; cc.cols = SR.rows; cc.ncb = (int32_t)G.skey.size();
+        cc.row_off = (int32_t)ctab.size();
+        for (size_t b = 0; b < G.rn.size(); b++)
+            for (int64_t i = 0; i < G.rn[b]; i++) { ctab.push_back((int32_t)b); ctab.push_back((int32_t)i); }
+        cc.col_off = (int32_t)ctab.size();
+        for (size_t b = 0; b < G.sn.size(); b++)
+            for (int64_t i = 0; i < G.sn[b]; i++) { ctab.push_back((int32_t)b); ctab.push_back((int32_t)i); }
+        cc.cell_off = (int32_t)ctab.size();
+        ctab.insert(ctab.end(), G.cell.begin(), G.cell.end());
+        comps.push_back(cc);
+        // the product and its tiles
+        const int32_t xrec = swap ? srec : rrec, yrec = swap ? rrec : srec;
+        const DCrtPanel &XR = records[xrec - rec_base], &YR = records[yrec - rec_base];
+        DCrtTask tk;
+        std::memset(&tk, 0, sizeof(tk));
+        tk.px = xrec; tk.py = yrec;
+        tk.xres = XR.res_off; tk.yres = YR.res_off;
+        tk.nkb = XR.K_pad / 32;
+        const int32_t ti = (int32_t)dt.size();
+        dt.push_back(tk);
+        const int32_t nt = YR.tr;
+        for (int64_t x0 = 0; x0 < XR.rows; x0 += 256)
+            for (int64_t y0 = 0; y0 < YR.rows; y0 += nt) {
+                DCrtItem it;
+                std::memset(&it, 0, sizeof(it));
+                it.cblk = -1;
+                it.comp = (int32_t)gi;
+                it.x0 = (int32_t)x0; it.y0 = (int32_t)y0;
+                it.nt = nt;
+                it.nx = x0 + 128 < XR.rows ? 2 : 1;
+                it.t_begin = ti; it.t_end = ti + 1;
+                it.gx = xrec; it.gy = yrec;
+                it.res_off = out_bytes;
+                out_bytes += (int64_t)L * it.nx * 128 * nt;
+                iv.push_back({(double)kt * nt * it.nx, it});
+            }
+    }
+    const int32_t nsplit = (int32_t)(panels.size() + pieces.size());   // panels the split passes process
+    panels.insert(panels.end(), pieces.begin(), pieces.end());
+    panels.insert(panels.end(), records.begin(), records.end());
+    if (gidx.size() > ((size_t)1 << 31) - 1 || ctab.size() > ((size_t)1 << 31) - 1)
+        throw error(kErrUnsupported, "modular plan index tables too large");
+
     std::stable_sort(iv.begin(), iv.end(), [](const std::pair<double, DCrtItem> &x, const std::pair<double, DCrtItem> &y) {
         return x.first > y.first;
     });
@@ -902,18 +1224,22 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     // every pair of an item shares the tile width of its N operand
     for (const DCrtItem &it : items)
         for (int32_t t = it.t_begin; t < it.t_end; t++)
-            if (panels[dt[t].py].tr != it.nt || panels[dt[t].px].tr != 128)
+            if (panels[dt[t].py].tr != it.nt || panels[dt[t].px].tr != 128 || panels[dt[t].px].K_pad != panels[dt[t].py].K_pad)
                 throw error(kErrState, "inconsistent tile widths within a C block");
 
     cudaStream_t s = pl->ctx->stream;
-    ex->npanels = (int32_t)panels.size();
+    ex->npanels = nsplit;
     ex->nitems = (int32_t)items.size();
+    ex->ngroups = (int32_t)groups.size();
     ex->max_rows = max_rows;
-    for (const DCrtPanel &q : panels) {
+    for (int32_t i = 0; i < nsplit; i++) {
+        const DCrtPanel &q = panels[i];
         ex->src_elems += (int64_t)q.rows * q.K;
-        ex->res_bytes += (int64_t)L * q.rows_pad * q.K_pad;
+        ex->res_bytes += (int64_t)L * q.wrows * q.wk;
     }
     ex->res.alloc(std::max<int64_t>(res_bytes, 1024));
+    // cells of grouped images that no piece writes stay zero
+    LTG_CUDA(cudaMemsetAsync(ex->res.p, 0, std::max<int64_t>(res_bytes, 1024), s));
     ex->out.alloc(std::max<int64_t>(out_bytes, 1024));
     ex->ex.alloc(std::max<int64_t>(ex->nx, 1) * sizeof(int32_t));
     ex->ey.alloc(std::max<int64_t>(ex->ny, 1) * sizeof(int32_t));
@@ -922,6 +1248,10 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     upload_vec(ex->items, items, s);
     upload_vec(ex->cblks, dc, s);
     upload_vec(ex->gidx, gidx, s);
+    if (comps.empty()) comps.resize(1);
+    if (ctab.empty()) ctab.resize(1);
+    upload_vec(ex->comps, comps, s);
+    upload_vec(ex->ctab, ctab, s);
     ex->err.alloc(sizeof(int32_t));
     LTG_CUDA(cudaMemsetAsync(ex->err.p, 0, sizeof(int32_t), s));
     LTG_CUDA(cudaMallocHost(&ex->err_host, sizeof(int32_t)));
@@ -1648,7 +1978,8 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             t_gemm.done();
             TimedLaunch t_comb(ctx, LTG_KERNEL_OZ_COMBINE);
             LTG_CUDA(launch_crt_combine(cx->panels.as<DCrtPanel>(), cx->items.as<DCrtItem>(), cx->nitems,
-                                        cx->cblks.as<DCBlock>(), cx->out.as<uint8_t>(), cx->gidx.as<int32_t>(),
+                                        cx->cblks.as<DCBlock>(), cx->comps.as<DCrtComp>(), cx->ctab.as<int32_t>(),
+                                        cx->out.as<uint8_t>(), cx->gidx.as<int32_t>(),
                                         cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), c->arena.as<double>(), add,
                                         cx->cp, s));
             t_comb.done();
@@ -1746,6 +2077,47 @@ int ltg_contract2_set_tile(ltg_plan *plan, int32_t cfg) {
         if (cfg < -1 || cfg >= tile_cfg_count()) throw error(kErrBadArg, "tile configuration out of range");
         plan->forced_tile = cfg;
         plan->exec.clear();
+    });
+}
+
+int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
+        plan->group_products = enable != 0;
+        plan->crt.clear();
+    });
+}
+
+int ltg_contract2_group_info(ltg_plan *plan, ltg_bt *c, int64_t *ngroups, int64_t *nblocks,
+                             double *grouped_flops, double *block_flops) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        check_bt(c);
+        if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
+        std::vector<GemmTask> tasks;
+        std::vector<CBlockTask> cbt;
+        contract2_tasks(plan->plan, plan->a->h, plan->b->h, c->h, 1.0, 1.0, 1.0, tasks, cbt);
+        CrtSideMap sm[2];
+        crt_side_maps(plan->plan.contr, c->h, sm);
+        std::vector<CrtGroupHost> groups;
+        std::vector<int32_t> group_of(cbt.size(), -1);
+        if (plan->group_products && !plan->plan.coalesced) crt_groups(plan, c->h, sm, cbt, groups, group_of);
+        int64_t nb = 0;
+        double bf = 0, gf = 0;
+        for (size_t e = 0; e < cbt.size(); e++)
+            if (group_of[e] >= 0) { nb++; bf += 2.0 * (double)cbt[e].M * (double)cbt[e].N * cbt[e].kflops; }
+        for (const CrtGroupHost &G : groups) {
+            double r = 0, cl = 0, k = 0;
+            for (int64_t v : G.rn) r += (double)v;
+            for (int64_t v : G.sn) cl += (double)v;
+            for (int64_t v : G.kn) k += (double)round4(v);
+            gf += 2.0 * r * cl * k;
+        }
+        if (ngroups) *ngroups = (int64_t)groups.size();
+        if (nblocks) *nblocks = nb;
+        if (grouped_flops) *grouped_flops = gf;
+        if (block_flops) *block_flops = bf;
     });
 }
 

@@ -89,6 +89,12 @@ struct DCrtPanel {
     int32_t nr, nk;
     int32_t rext[kDevMaxSub], rstr[kDevMaxSub];
     int32_t kext[kDevMaxSub], kstr[kDevMaxSub];
+    // Placement in the tile images: rows [r0, r0 + wrows) and k [k0, k0 + wk)
+    // are written (the padding included; k0 and wk multiples of 4).  A panel
+    // of its own has r0 = k0 = 0, wrows = rows_pad, wk = K_pad; a piece of a
+    // grouped panel writes its cell of the group's images, whose geometry
+    // (tr, K_pad) it carries.
+    int32_t r0, k0, wrows, wk;
 };
 
 struct DCrtTask {
@@ -108,8 +114,21 @@ struct DCrtItem {
     int32_t nx;                   // 128-row tiles (1 or 2)
     int32_t t_begin, t_end;       // pairs (DCrtTask range)
     int32_t gx, gy;               // panels whose global row indices label the tile
-    int32_t pad;
+    int32_t comp;                 // grouped product (DCrtComp) or -1 for one C block (cblk)
     int64_t res_off;              // residue tile output: [modulus][nx * 128][nt] bytes
+};
+
+// A grouped product: C blocks whose row blocks (C dims taken from A) and
+// column blocks (C dims taken from B) form one dense grid, computed as one
+// product over the union of their contracted blocks.  Row m of the group is
+// (row block, row within the block) = tab[row_off + 2m], tab[row_off + 2m + 1];
+// columns likewise at col_off; tab[cell_off + R * ncb + S] is the C block
+// (DCBlock index) of row block R and column block S, or -1 when that block is
+// not computed by this contraction.
+struct DCrtComp {
+    int32_t rows, cols;           // C rows (side of A) and columns (side of B)
+    int32_t ncb;                  // column blocks
+    int32_t row_off, col_off, cell_off;
 };
 
 // Moduli of a modular contraction and its scaling (the constants of Garner's
@@ -249,8 +268,9 @@ cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const D
     const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp, int32_t *err,
     cudaStream_t s);
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
-    const DCBlock *cblks, const uint8_t *out, const int32_t *gidx, const int32_t *ex,
-    const int32_t *ey, double *c, int32_t add, const CrtParams &cp, cudaStream_t s);
+    const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab, const uint8_t *out,
+    const int32_t *gidx, const int32_t *ex, const int32_t *ey, double *c, int32_t add,
+    const CrtParams &cp, cudaStream_t s);
 
 // Element-wise transfer kernels.  max_terms bounds nterms and tile_bytes the
 // shared-memory tiles of any tiled-mode job.

@@ -657,6 +657,7 @@ void contract2_schedule(const Contraction &c, const BlockTensorHost &a,
     plan.schedule.clear();
     plan.clst.clear();
     plan.flops = 0;
+    plan.coalesced = false;
     int64_t ic[kMaxOrder], ia[kMaxOrder], ib[kMaxOrder], ik[kMaxOrder];
     int64_t da[kMaxOrder], dc[kMaxOrder];
     std::list<Pair> lst;
@@ -679,7 +680,9 @@ void contract2_schedule(const Contraction &c, const BlockTensorHost &a,
             lst.push_back(p);
         }
         if (lst.empty()) continue;
+        const size_t before = lst.size();
         coalesce(c, lst);
+        if (lst.size() != before) plan.coalesced = true;
         if (lst.empty()) continue;
         plan.schedule.push_back(cabs);
         plan.clst.emplace_back(lst.begin(), lst.end());

@@ -295,6 +295,7 @@ struct ContractPlan {
     std::vector<int64_t> schedule;                 // non-zero canonical C blocks
     std::vector<std::vector<Pair>> clst;           // coalesced pairs per schedule entry
     double flops = 0;                              // algorithmic flops (2*|C|*K per pair)
+    bool coalesced = false;                        // some pair list was shortened by coalescing
 };
 
 // Derives the result block index space and symmetry

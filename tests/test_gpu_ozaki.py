@@ -78,3 +78,22 @@ def test_split_precision_add_mode(gctx, mode, S):
     op.perform(C, 0.5, mode=mode, nslices=S)
     rop.perform(RC, 0.5)
     assert max_rel_block_error(block_errors(C, C.download(), RC, None)) <= 1e-12
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_crt_grouped_products_are_bit_identical(gctx, case):
+    """The modular products are exact integers, so computing small C blocks as
+    grouped products gives the same bits as one product per block and pair."""
+    A, _, _ = seeded_pair(gctx, case.a, 5, case.a_scale, case.zero_a)
+    B, _, _ = seeded_pair(gctx, case.b, 6, case.b_scale)
+    contr = contraction2(case.n, case.m, case.k, case.permc)
+    for p in case.pairs:
+        contr.contract(*p)
+    op = btod_contract2(contr, A, B, case.ka, case.kb, case.kc)
+    C1, C2 = op.make_result(), op.make_result()
+    op.perform(C1, mode=MODE_OZAKI_CRT, nslices=13)
+    op.set_grouping(False)
+    op.perform(C2, mode=MODE_OZAKI_CRT, nslices=13)
+    op.set_grouping(True)
+    gctx.synchronize()
+    assert np.array_equal(C1.download().view(np.uint64), C2.download().view(np.uint64))
