@@ -69,6 +69,28 @@ __host__ __device__ constexpr int32_t crt_inverse(int j, int i) {
     return (int32_t)(t < 0 ? t + m : t);
 }
 
+// Balanced representative of x mod m, in (-m/2, m/2].
+__host__ __device__ constexpr int32_t crt_balanced(int64_t x, int32_t m) {
+    const int64_t y = ((x % m) + m) % m;
+    return (int32_t)(y > m / 2 ? y - m : y);
+}
+__host__ __device__ constexpr bool crt_odd_moduli() {
+    for (int i = 1; i < 16; i++)
+        if (crt_modulus(i) % 2 == 0) return false;
+    return true;
+}
+static_assert(crt_odd_moduli(), "the single-reduction Garner digits need odd moduli after m_0");
+// Garner's digit i as one linear form: the recurrence t <- (t - v_j) m_j^-1
+// (mod m_i), j = 0..i-1, started at t = r_i, expands to
+//   v_i = r_i * prod_{j<i} m_j^-1 - sum_{j<i} v_j * prod_{k=j..i-1} m_k^-1  (mod m_i),
+// so the digit costs i multiply-adds and one reduction.  The products are
+// taken balanced (|.| <= 128).
+__host__ __device__ constexpr int32_t crt_garner_d(int j, int i) {
+    int64_t p = 1;
+    for (int k = j; k < i; k++) p = p * crt_inverse(k, i) % crt_modulus(i);
+    return crt_balanced(p, crt_modulus(i));
+}
+
 // Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E).
 template<int B, int E>
 struct StaticFor {
@@ -105,42 +127,110 @@ __device__ __forceinline__ int64_t image_offset(int r, int TR, int nkb, int kb, 
            (kb_byte >> 4) * 128 + (rr & 7) * 16 + (kb_byte & 15);
 }
 
-// ---------------------------------------------------------------- exponents
+// ---------------------------------------------------------------- split passes
+//
+// Work units (built on the host): rows [r0, r0 + nrows) of one panel, all of
+// its k, in one of two thread mappings:
+//  - rows (long k): 32 rows, 8 threads per row, each reading 4 consecutive k
+//    per step along the row; the row maximum is reduced over the 8 threads;
+//  - tiles (short k, e.g. the cells of grouped products): core tiles of 8 rows
+//    x 16 k, the shape of one 128-byte core matrix of a residue image (lane l
+//    takes row l / 4 and the 4 consecutive k of group l % 4), spread over the
+//    CTA's warps, so that short rows still fill the warps.
+// When a panel's k dims are not one contiguous run, their offsets come from a
+// shared-memory table built once per unit (no divisions per element).
+
+constexpr int kSplitThreads = 256;
+constexpr int kSplitWarps = kSplitThreads / 32;
+constexpr int kKoffMax = 4096;                      // k offsets tabulated per unit
+constexpr int kUnitRowsMax = 256;                   // rows per unit (bound of the host's units)
+constexpr int kUnitRowMap = 0, kUnitTileMap = 1;    // thread mapping of a unit (units[].w)
 
 __global__ void crt_fill_kernel(int32_t *p, int32_t n, int32_t v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
 
-// 32 rows per CTA, 8 threads per row reading 4 consecutive k per step.
-__global__ void __launch_bounds__(256)
-crt_exp_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const double *__restrict__ A,
-               const double *__restrict__ B, const int32_t *__restrict__ gidx, int32_t *ex, int32_t *ey) {
-    const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
-    for (int p = blockIdx.y; p < npanels; p += gridDim.y) {
-        const DCrtPanel &P = panels[p];
-        const double *src = P.src ? B : A;
-        const bool contig = P.nk == 1 && P.kstr[0] == 1;
+// k offset mode of a panel: 0 contiguous, 1 tabulated in koff, 2 computed.
+__device__ __forceinline__ int koff_setup(const DCrtPanel &P, int32_t *koff) {
+    const int mode = (P.nk == 1 && P.kstr[0] == 1) ? 0 : (P.K <= kKoffMax ? 1 : 2);
+    if (mode == 1)
+        for (int k = threadIdx.x; k < P.K; k += blockDim.x) koff[k] = (int32_t)mixed_offset(k, P.nk, P.kext, P.kstr);
+    return mode;
+}
+__device__ __forceinline__ int64_t koffset(const DCrtPanel &P, int mode, const int32_t *koff, int k) {
+    return mode == 0 ? k : (mode == 1 ? koff[k] : mixed_offset(k, P.nk, P.kext, P.kstr));
+}
+
+__global__ void __launch_bounds__(kSplitThreads)
+crt_exp_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ units, int32_t nunits,
+               const double *__restrict__ A, const double *__restrict__ B, const int32_t *__restrict__ gidx,
+               int32_t *ex, int32_t *ey) {
+    __shared__ int32_t koff[kKoffMax];
+    __shared__ int32_t rexp[kUnitRowsMax];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lrow = lane >> 2, kq = lane & 3;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int4 un = units[u];
+        const DCrtPanel &P = panels[un.x];
+        // shared memory is used by tabulated k offsets and the tile mapping
+        // (both uniform over the CTA); the first barrier keeps the previous
+        // unit's readers (a grid smaller than the unit count) apart
+        const bool shared = (P.nk != 1 || P.kstr[0] != 1) || un.w == kUnitTileMap;
+        if (shared) __syncthreads();
+        const int mode = koff_setup(P, koff);
+        if (un.w == kUnitTileMap)
+            for (int i = threadIdx.x; i < un.z; i += blockDim.x) rexp[i] = kNoExp;
+        if (shared) __syncthreads();
+        const double *src = (P.src ? B : A) + P.src_off;
         int32_t *tab = P.side == 0 ? ex : ey;
-        for (int r0 = blockIdx.x * 32; r0 < P.rows; r0 += gridDim.x * 32) {
-            const int r = r0 + lr;
-            const bool valid = r < P.rows;
-            const double *row = src + P.src_off + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
+        if (un.w == kUnitRowMap) {
+            const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
+            const int r = un.y + lr;
+            const bool valid = lr < un.z && r < P.rows;
+            const double *row = src + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
             double mx = 0.0;
             if (valid)
                 for (int k0 = 4 * c; k0 < P.K; k0 += 32)
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const int k = k0 + j;
-                        if (k < P.K) mx = fmax(mx, fabs(row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)]));
-                    }
+                    for (int j = 0; j < 4; j++)
+                        if (k0 + j < P.K) mx = fmax(mx, fabs(row[koffset(P, mode, koff, k0 + j)]));
             mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
             mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
             mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
             if (valid && c == 0 && mx > 0.0) {
                 int e;
-                frexp(mx, &e);                        // mx = f * 2^e, f in [0.5, 1)
+                frexp(mx, &e);
                 atomicMax(&tab[gidx[P.g_off + r]], e);
             }
+            continue;
+        }
+        const int nkt = (P.K + 15) >> 4;
+        const int ntile = ((un.z + 7) >> 3) * nkt;
+        int cur = -1;
+        const double *row = src;
+        for (int t = warp; t < ntile; t += kSplitWarps) {
+            const int rg = t / nkt, kt = t - rg * nkt;
+            const int rl = rg * 8 + lrow, r = un.y + rl;
+            const bool valid = rl < un.z && r < P.rows;
+            double mx = 0.0;
+            if (valid) {
+                if (r != cur) { row = src + mixed_offset(r, P.nr, P.rext, P.rstr); cur = r; }
+                const int k0 = kt * 16 + kq * 4;
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (k0 + j < P.K) mx = fmax(mx, fabs(row[koffset(P, mode, koff, k0 + j)]));
+            }
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+            if (valid && kq == 0 && mx > 0.0) {
+                int e;
+                frexp(mx, &e);                                 // mx = f * 2^e, f in [0.5, 1)
+                atomicMax(&rexp[rl], e);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < un.z; i += blockDim.x) {
+            const int r = un.y + i;
+            if (r < P.rows && rexp[i] > kNoExp) atomicMax(&tab[gidx[P.g_off + r]], rexp[i]);
         }
     }
 }
@@ -169,58 +259,87 @@ __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, ui
 }
 
 template<int L>
-__global__ void __launch_bounds__(256)
-crt_res_kernel(const DCrtPanel *__restrict__ panels, int32_t npanels, const double *__restrict__ A,
-               const double *__restrict__ B, const int32_t *__restrict__ gidx, const int32_t *__restrict__ ex,
-               const int32_t *__restrict__ ey, uint8_t *__restrict__ res, const CrtParams cp) {
-    const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
-    for (int p = blockIdx.y; p < npanels; p += gridDim.y) {
-        const DCrtPanel &P = panels[p];
-        const double *src = P.src ? B : A;
-        const bool contig = P.nk == 1 && P.kstr[0] == 1;
+__global__ void __launch_bounds__(kSplitThreads)
+crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ units, int32_t nunits,
+               const double *__restrict__ A, const double *__restrict__ B, const int32_t *__restrict__ gidx,
+               const int32_t *__restrict__ ex, const int32_t *__restrict__ ey, uint8_t *__restrict__ res,
+               const CrtParams cp) {
+    __shared__ int32_t koff[kKoffMax];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lrow = lane >> 2, kq = lane & 3;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int4 un = units[u];
+        const DCrtPanel &P = panels[un.x];
+        const bool shared = P.nk != 1 || P.kstr[0] != 1;      // tabulated k offsets (uniform)
+        if (shared) __syncthreads();                         // the previous unit's readers are done
+        const int mode = koff_setup(P, koff);
+        if (shared) __syncthreads();
+        const double *src = (P.src ? B : A) + P.src_off;
         const int32_t *tab = P.side == 0 ? ex : ey;
         uint8_t *base = res + P.res_off;
         const int TR = P.tr, nkb = P.K_pad / kKB;
         const double coef = (double)P.coef;
-        for (int r0 = blockIdx.x * 32; r0 < P.wrows; r0 += gridDim.x * 32) {
-            const int r = r0 + lr;
-            if (r >= P.wrows) continue;              // wrows need not be a multiple of 32
+        const int64_t lstride = (int64_t)TR * kKB;            // next modulus image
+        int cur = -1;
+        const double *row = src;
+        double s1 = 0.0, s2 = 0.0;
+        bool live = false;
+        // row r's offset and scaling, kept while the thread stays on it
+        auto set_row = [&](int r) {
+            cur = r;
             const bool valid = r < P.rows;
-            const double *row = src + P.src_off + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
+            row = src + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
             const int e = valid ? tab[gidx[P.g_off + r]] : kNoExp;
             // 2^(P - e) as two finite factors
             const int sh = e > kNoExp ? cp.P - e : 0;
-            const double s1 = ldexp(1.0, sh / 2), s2 = ldexp(1.0, sh - sh / 2);
-            const bool live = valid && e > kNoExp;
-            for (int k0 = 4 * c; k0 < P.wk; k0 += 32) {
-                double x[4];
+            s1 = ldexp(1.0, sh / 2);
+            s2 = ldexp(1.0, sh - sh / 2);
+            live = valid && e > kNoExp;
+        };
+        // residues of k0..k0+3 of row r (k0 % 4 == 0) into the images
+        auto put4 = [&](int r, int k0) {
+            double x[4];
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int k = k0 + j;
-                    x[j] = (live && k < P.K) ? row[contig ? k : mixed_offset(k, P.nk, P.kext, P.kstr)] : 0.0;
-                }
-                uint32_t packed[L];
-#pragma unroll
-                for (int l = 0; l < L; l++) packed[l] = 0;
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const double t = (x[j] * s1) * s2 + kMagicD;         // 1.5 * 2^52 + rint(x 2^(P-e))
-                    const double X = (t - kMagicD) * coef;               // the integer coefficient folded in
-                    const uint32_t xlo = (uint32_t)__double2loint(t) * (uint32_t)P.coef;   // X mod 2^32
-                    // byte j of each modulus word takes this element's residue
-                    const uint32_t sel = 0x3210u ^ ((0x4u ^ (uint32_t)j) << (4 * j));
-                    StaticFor<0, L>::run([&](auto ic) {
-                        constexpr int l = decltype(ic)::value;
-                        packed[l] = __byte_perm(packed[l], residue_byte<l>(X, xlo), sel);
-                    });
-                }
-                const int kk = P.k0 + k0;                                // k0 % 4 == 0: one word
-                const int kb = kk / kKB, kb_byte = kk % kKB;
-                uint8_t *dst0 = base + image_offset(P.r0 + r, TR, nkb, kb, 0, L, kb_byte);
-                const int64_t lstride = (int64_t)TR * kKB;              // next modulus image
-#pragma unroll
-                for (int l = 0; l < L; l++) *reinterpret_cast<uint32_t *>(dst0 + l * lstride) = packed[l];
+            for (int j = 0; j < 4; j++) {
+                const int k = k0 + j;
+                x[j] = (live && k < P.K) ? row[koffset(P, mode, koff, k)] : 0.0;
             }
+            uint32_t packed[L];
+#pragma unroll
+            for (int l = 0; l < L; l++) packed[l] = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const double tt = (x[j] * s1) * s2 + kMagicD;         // 1.5 * 2^52 + rint(x 2^(P-e))
+                const double X = (tt - kMagicD) * coef;               // the integer coefficient folded in
+                const uint32_t xlo = (uint32_t)__double2loint(tt) * (uint32_t)P.coef;   // X mod 2^32
+                // byte j of each modulus word takes this element's residue
+                const uint32_t sel = 0x3210u ^ ((0x4u ^ (uint32_t)j) << (4 * j));
+                StaticFor<0, L>::run([&](auto ic) {
+                    constexpr int l = decltype(ic)::value;
+                    packed[l] = __byte_perm(packed[l], residue_byte<l>(X, xlo), sel);
+                });
+            }
+            const int kk = P.k0 + k0;                                // a multiple of 4: one word
+            uint8_t *dst0 = base + image_offset(P.r0 + r, TR, nkb, kk / kKB, 0, L, kk % kKB);
+#pragma unroll
+            for (int l = 0; l < L; l++) *reinterpret_cast<uint32_t *>(dst0 + l * lstride) = packed[l];
+        };
+        if (un.w == kUnitRowMap) {
+            const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
+            const int r = un.y + lr;
+            if (lr >= un.z || r >= P.wrows) continue;
+            set_row(r);
+            for (int k0 = 4 * c; k0 < P.wk; k0 += 32) put4(r, k0);
+            continue;
+        }
+        const int nkt = (P.wk + 15) >> 4;
+        const int ntile = ((un.z + 7) >> 3) * nkt;
+        for (int t = warp; t < ntile; t += kSplitWarps) {
+            const int rg = t / nkt, kt = t - rg * nkt;
+            const int rl = rg * 8 + lrow, r = un.y + rl;
+            const int k0 = kt * 16 + kq * 4;
+            if (rl >= un.z || r >= P.wrows || k0 >= P.wk) continue;
+            if (r != cur) set_row(r);
+            put4(r, k0);
         }
     }
 }
@@ -522,22 +641,28 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
                 if (cp.swap) { r = e & (kXRows - 1); c = e >> 7; }      // C rows along the tile columns
                 else { c = e & (kCombCols - 1); r = e >> 4; }
                 if (r >= xr || c0 + c >= yc) continue;
-                // Garner: balanced mixed-radix digits v_i of the residues
+                // Garner: balanced mixed-radix digits v_i of the residues.  Every
+                // quantity is an integer below 2^19 in magnitude (|r_i D| <=
+                // 255 * 128, |v_j D| <= 128 * 128, at most 15 terms), so FP32
+                // holds it exactly; the quotient rint(t / m_i) from one FMA is
+                // exact for odd m_i (t / m_i stays 1/(2 m_i) away from a half
+                // integer, far above the product's rounding), which leaves t
+                // in [-(m_i - 1)/2, (m_i - 1)/2].
                 float v[L];
                 StaticFor<0, L>::run([&](auto ii) {
                     constexpr int i = decltype(ii)::value;
-                    constexpr float mi = (float)crt_modulus(i), minv = 1.0f / (float)crt_modulus(i);
-                    float t = __int_as_float(0x4B000000 | (int)sres[i][r][c]) - 8388608.0f;
-                    StaticFor<0, i>::run([&](auto jj) {
-                        constexpr int j = decltype(jj)::value;
-                        t = (t - v[j]) * (float)crt_inverse(j, i);
-                        t = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);   // t mod m_i, |t| <= m_i/2 + 1
-                    });
-                    // exact balanced digit in (-m_i/2, m_i/2]
-                    t = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);
-                    if (t > 0.5f * mi) t -= mi;
-                    if (t <= -0.5f * mi) t += mi;
-                    v[i] = t;
+                    const float ri = __int_as_float(0x4B000000 | (int)sres[i][r][c]) - 8388608.0f;
+                    if constexpr (i == 0) {
+                        v[0] = ri >= 128.0f ? ri - 256.0f : ri;             // m_0 = 256: the byte itself
+                    } else {
+                        constexpr float mi = (float)crt_modulus(i), minv = 1.0f / (float)crt_modulus(i);
+                        float t = ri * (float)crt_garner_d(0, i);
+                        StaticFor<0, i>::run([&](auto jj) {
+                            constexpr int j = decltype(jj)::value;
+                            t = fmaf(-v[j], (float)crt_garner_d(j, i), t);
+                        });
+                        v[i] = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);
+                    }
                 });
                 // digits to double by bits (|v| < 2^22): float 1.5*2^23 + v -> int -> double
                 auto digit = [](float f) {
@@ -583,24 +708,24 @@ int num_sms() {
 
 }  // namespace
 
-cudaError_t launch_crt_exponents(const DCrtPanel *panels, int32_t npanels, int32_t max_rows, int32_t nx,
+cudaError_t launch_crt_exponents(const DCrtPanel *panels, const int4 *units, int32_t nunits, int32_t nx,
                                  int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
                                  int32_t *ey, cudaStream_t s) {
-    if (npanels <= 0) return cudaSuccess;
+    if (nunits <= 0) return cudaSuccess;
     crt_fill_kernel<<<64, 256, 0, s>>>(ex, nx, kNoExp);
     crt_fill_kernel<<<64, 256, 0, s>>>(ey, ny, kNoExp);
-    dim3 grid((max_rows + 31) / 32, npanels < 65535 ? npanels : 65535);
-    crt_exp_kernel<<<grid, 256, 0, s>>>(panels, npanels, a, b, gidx, ex, ey);
+    const int grid = nunits;                               // one unit per CTA
+    crt_exp_kernel<<<grid, kSplitThreads, 0, s>>>(panels, units, nunits, a, b, gidx, ex, ey);
     return cudaGetLastError();
 }
 
-cudaError_t launch_crt_residues(const DCrtPanel *panels, int32_t npanels, int32_t max_rows,
+cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int32_t nunits,
                                 const double *a, const double *b, const int32_t *gidx, const int32_t *ex,
                                 const int32_t *ey, uint8_t *res, const CrtParams &cp, cudaStream_t s) {
-    if (npanels <= 0) return cudaSuccess;
-    dim3 grid((max_rows + 31) / 32, npanels < 65535 ? npanels : 65535);
+    if (nunits <= 0) return cudaSuccess;
+    const int grid = nunits;                               // one unit per CTA
     switch (cp.L) {
-#define CASE_L(n) case n: crt_res_kernel<n><<<grid, 256, 0, s>>>(panels, npanels, a, b, gidx, ex, ey, res, cp); break;
+#define CASE_L(n) case n: crt_res_kernel<n><<<grid, kSplitThreads, 0, s>>>(panels, units, nunits, a, b, gidx, ex, ey, res, cp); break;
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
 #undef CASE_L
     default: return cudaErrorInvalidValue;

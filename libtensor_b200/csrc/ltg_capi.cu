@@ -154,9 +154,9 @@ struct OzExec {
 // Device arrays of one modular split-precision contraction (crt.cu).
 struct CrtExec {
     CrtParams cp{};
-    int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0, ngroups = 0;
+    int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0, ngroups = 0, nunits = 0;
     int64_t src_elems = 0, res_bytes = 0;   // operand elements read per pass, residue bytes written
-    DevBuf panels, tasks, items, cblks, comps, ctab, gidx, ex, ey, res, out, err;
+    DevBuf panels, units, tasks, items, cblks, comps, ctab, gidx, ex, ey, res, out, err;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
     int32_t *err_host = nullptr;
@@ -1019,7 +1019,8 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         pack_sub(kk, p.nk, p.kext, p.kstr, nullptr);
         p.res_off = res_bytes;
         res_bytes += ((int64_t)L * p.rows_pad * p.K_pad + 1023) / 1024 * 1024;
-        p.r0 = 0; p.k0 = 0; p.wrows = p.rows_pad; p.wk = p.K_pad;
+        // the padding rows and k of the image stay zero from the buffer's clearing
+        p.r0 = 0; p.k0 = 0; p.wrows = p.rows; p.wk = round4(p.K);
         p.g_off = (int32_t)gidx.size();
         gidx.insert(gidx.end(), grow.begin(), grow.end());
         max_rows = std::max(max_rows, p.rows_pad);
@@ -1237,6 +1238,18 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         ex->src_elems += (int64_t)q.rows * q.K;
         ex->res_bytes += (int64_t)L * q.wrows * q.wk;
     }
+    // split-pass units: 32 rows of a panel with long k (8 threads per row), or
+    // about 64 core tiles (8 rows x 16 k, at most 256 rows) of one with short k
+    std::vector<int4> units;
+    for (int32_t i = 0; i < nsplit; i++) {
+        const bool rowmap = panels[i].wk >= 128;
+        const int32_t nkt = (panels[i].wk + 15) / 16;
+        const int32_t ru = rowmap ? 32 : 8 * std::max(1, std::min(32, 64 / std::max(1, nkt)));
+        for (int32_t r0 = 0; r0 < panels[i].wrows; r0 += ru)
+            units.push_back(make_int4(i, r0, std::min(ru, panels[i].wrows - r0), rowmap ? 0 : 1));
+    }
+    ex->nunits = (int32_t)units.size();
+    upload_vec(ex->units, units, s);
     ex->res.alloc(std::max<int64_t>(res_bytes, 1024));
     // cells of grouped images that no piece writes stay zero
     LTG_CUDA(cudaMemsetAsync(ex->res.p, 0, std::max<int64_t>(res_bytes, 1024), s));
@@ -1965,9 +1978,10 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                     LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
             const double *pa = plan->a->arena.as<double>(), *pb = plan->b->arena.as<double>();
             TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
-            LTG_CUDA(launch_crt_exponents(cx->panels.as<DCrtPanel>(), cx->npanels, cx->max_rows, cx->nx, cx->ny,
-                                          pa, pb, cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), s));
-            LTG_CUDA(launch_crt_residues(cx->panels.as<DCrtPanel>(), cx->npanels, cx->max_rows, pa, pb,
+            LTG_CUDA(launch_crt_exponents(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, cx->nx,
+                                          cx->ny, pa, pb, cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(),
+                                          cx->ey.as<int32_t>(), s));
+            LTG_CUDA(launch_crt_residues(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, pa, pb,
                                          cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
                                          cx->res.as<uint8_t>(), cx->cp, s));
             t_split.done();

@@ -258,10 +258,12 @@ void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t
 
 // Modular split precision: exponent pass, residue pass, modular products,
 // Garner recombination into FP64 C.
-cudaError_t launch_crt_exponents(const DCrtPanel *panels, int32_t npanels, int32_t max_rows,
+// Split passes work on units (panel, first row, rows, unused): at most 256
+// rows of one panel.
+cudaError_t launch_crt_exponents(const DCrtPanel *panels, const int4 *units, int32_t nunits,
     int32_t nx, int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
     int32_t *ey, cudaStream_t s);
-cudaError_t launch_crt_residues(const DCrtPanel *panels, int32_t npanels, int32_t max_rows,
+cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int32_t nunits,
     const double *a, const double *b, const int32_t *gidx, const int32_t *ex, const int32_t *ey,
     uint8_t *res, const CrtParams &cp, cudaStream_t s);
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
