@@ -603,17 +603,24 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 
 constexpr int kCombCols = 16;                       // tile columns staged per pass
 
-// One CTA per work item at a time: residues of 16 columns staged in shared
-// memory, then one thread per element runs Garner and writes C.
+// Units (work item, 128-row half, 16-column chunk): the residues of the
+// unit staged in shared memory together with, per tile row and column, its
+// exponent and its part of the C offset (one C block: the offsets of its row
+// and column; grouped products: the block and coordinates, combined with the
+// C block's strides per element); then one thread per element runs Garner
+// and writes C.
 template<int L>
 __global__ void __launch_bounds__(256)
 crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restrict__ items, int32_t nitems,
                    const DCBlock *__restrict__ cblks, const DCrtComp *__restrict__ comps,
-                   const int32_t *__restrict__ ctab, const uint8_t *__restrict__ out,
-                   const int32_t *__restrict__ gidx, const int32_t *__restrict__ ex,
-                   const int32_t *__restrict__ ey, double *__restrict__ C, int32_t add, const CrtParams cp) {
+                   const int32_t *__restrict__ ctab, const DCrtCell *__restrict__ cells,
+                   const uint8_t *__restrict__ out, const int32_t *__restrict__ gidx,
+                   const int32_t *__restrict__ ex, const int32_t *__restrict__ ey, double *__restrict__ C,
+                   int32_t add, double scale, const CrtParams cp) {
     __shared__ __align__(16) uint8_t sres[L][kXRows][kCombCols];
-    // units: (item, 128-row half, 16-column chunk), 32 per item
+    __shared__ int64_t soff[kXRows + kCombCols];               // one C block: row / column offsets
+    __shared__ int32_t sexp[kXRows + kCombCols];               // exponents of tile rows / columns
+    __shared__ int32_t sco[kXRows + kCombCols][1 + kCrtSideDims];   // grouped: block, coordinates
     for (int u = blockIdx.x; u < nitems * 32; u += gridDim.x) {
         const DCrtItem item = items[u >> 5];
         const int xh = (u >> 4) & 1, c0 = (u & 15) * kCombCols;
@@ -623,74 +630,87 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
         const int xext = cp.swap ? cols : rows, yext = cp.swap ? rows : cols;
         const int yc = min(item.nt, yext - item.y0);
         if (xh >= item.nx || c0 >= yc) continue;                     // uniform over the CTA
-        const int32_t *gyp = gidx + panels[item.gy].g_off + item.y0;
-        {
-            const int xb = item.x0 + xh * kXRows;                    // first row of this half
-            const int xr = min(kXRows, xext - xb);
-            const int32_t *gxp = gidx + panels[item.gx].g_off + xb;
-            __syncthreads();
-            for (int i = threadIdx.x; i < L * kXRows; i += blockDim.x) {
-                const int l = i / kXRows, r = i - l * kXRows;
-                cp_async16(&sres[l][r][0],
-                           out + item.res_off + ((int64_t)(l * item.nx + xh) * kXRows + r) * item.nt + c0);
-            }
-            asm volatile("cp.async.wait_all;\n" ::: "memory");
-            __syncthreads();
-            for (int e = threadIdx.x; e < kXRows * kCombCols; e += blockDim.x) {
-                int r, c;
-                if (cp.swap) { r = e & (kXRows - 1); c = e >> 7; }      // C rows along the tile columns
-                else { c = e & (kCombCols - 1); r = e >> 4; }
-                if (r >= xr || c0 + c >= yc) continue;
-                // Garner: balanced mixed-radix digits v_i of the residues.  Every
-                // quantity is an integer below 2^19 in magnitude (|r_i D| <=
-                // 255 * 128, |v_j D| <= 128 * 128, at most 15 terms), so FP32
-                // holds it exactly; the quotient rint(t / m_i) from one FMA is
-                // exact for odd m_i (t / m_i stays 1/(2 m_i) away from a half
-                // integer, far above the product's rounding), which leaves t
-                // in [-(m_i - 1)/2, (m_i - 1)/2].
-                float v[L];
-                StaticFor<0, L>::run([&](auto ii) {
-                    constexpr int i = decltype(ii)::value;
-                    const float ri = __int_as_float(0x4B000000 | (int)sres[i][r][c]) - 8388608.0f;
-                    if constexpr (i == 0) {
-                        v[0] = ri >= 128.0f ? ri - 256.0f : ri;             // m_0 = 256: the byte itself
-                    } else {
-                        constexpr float mi = (float)crt_modulus(i), minv = 1.0f / (float)crt_modulus(i);
-                        float t = ri * (float)crt_garner_d(0, i);
-                        StaticFor<0, i>::run([&](auto jj) {
-                            constexpr int j = decltype(jj)::value;
-                            t = fmaf(-v[j], (float)crt_garner_d(j, i), t);
-                        });
-                        v[i] = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);
-                    }
-                });
-                // digits to double by bits (|v| < 2^22): float 1.5*2^23 + v -> int -> double
-                auto digit = [](float f) {
-                    const int iv = __float_as_int(f + kMagicF) - 0x4B400000;
-                    return __hiloint2double(0x43380000, iv ^ (int)0x80000000) - 6755401588539392.0;
-                };
-                double X = digit(v[L - 1]);
+        const int xb = item.x0 + xh * kXRows;                        // first row of this half
+        const int xr = min(kXRows, xext - xb);
+        __syncthreads();                                             // the previous unit is done
+        for (int i = threadIdx.x; i < L * kXRows; i += blockDim.x) {
+            const int l = i / kXRows, r = i - l * kXRows;
+            cp_async16(&sres[l][r][0], out + item.res_off + ((int64_t)(l * item.nx + xh) * kXRows + r) * item.nt + c0);
+        }
+        for (int i = threadIdx.x; i < kXRows + kCombCols; i += blockDim.x) {
+            const bool isx = i < kXRows;
+            const int j = isx ? i : i - kXRows;
+            if (isx ? j >= xr : c0 + j >= yc) continue;
+            const int idx = isx ? xb + j : item.y0 + c0 + j;           // tile row / column
+            sexp[i] = isx ? ex[gidx[panels[item.gx].g_off + idx]] : ey[gidx[panels[item.gy].g_off + idx]];
+            const bool crow = isx != (cp.swap != 0);                  // a row of C (side of A)
+            if (cc) {
+                const int32_t *e = ctab + (crow ? cc->row_off : cc->col_off) + (1 + kCrtSideDims) * idx;
 #pragma unroll
-                for (int i = L - 2; i >= 0; i--) X = fma(X, (double)crt_modulus(i), digit(v[i]));
-                const int gx = gxp[r], gy = gyp[c0 + c];
-                const int e2 = ex[gx] + ey[gy] - 2 * cp.P;
-                const int xi = xb + r, yi = item.y0 + c0 + c;
-                int m = cp.swap ? yi : xi, n = cp.swap ? xi : yi;
-                const DCBlock *cb = cb1;
-                if (cc) {                                // grouped: find the C block of (m, n)
-                    const int rb = ctab[cc->row_off + 2 * m], cbk = ctab[cc->col_off + 2 * n];
-                    const int cell = ctab[cc->cell_off + rb * cc->ncb + cbk];
-                    if (cell < 0) continue;
-                    m = ctab[cc->row_off + 2 * m + 1];
-                    n = ctab[cc->col_off + 2 * n + 1];
-                    cb = &cblks[cell];
-                }
-                const double val = cb->scale * ldexp(X, max(e2, -2200));
-                double *dst = C + cb->c_off + mixed_offset(m, cb->nm, cb->mext, cb->mc_str) +
-                              mixed_offset(n, cb->nn, cb->next, cb->nc_str);
-                if (add) *dst += val;
-                else *dst = val;
+                for (int k = 0; k <= kCrtSideDims; k++) sco[i][k] = e[k];
+            } else {
+                soff[i] = crow ? mixed_offset(idx, cb1->nm, cb1->mext, cb1->mc_str)
+                               : mixed_offset(idx, cb1->nn, cb1->next, cb1->nc_str);
             }
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+        for (int e = threadIdx.x; e < kXRows * kCombCols; e += blockDim.x) {
+            int r, c;
+            if (cp.swap) { r = e & (kXRows - 1); c = e >> 7; }      // C rows along the tile columns
+            else { c = e & (kCombCols - 1); r = e >> 4; }
+            if (r >= xr || c0 + c >= yc) continue;
+            int64_t off;
+            if (cc) {                                                // grouped: the C block of (r, c)
+                const int32_t *cx = sco[r], *cy = sco[kXRows + c];
+                const int32_t *cm = cp.swap ? cy : cx, *cn = cp.swap ? cx : cy;
+                const int cell = ctab[cc->cell_off + cm[0] * cc->ncb + cn[0]];
+                if (cell < 0) continue;
+                const DCrtCell &cl = cells[cell];
+                off = cl.c_off;
+#pragma unroll
+                for (int k = 0; k < kCrtSideDims; k++) off += (int64_t)cm[1 + k] * cl.ms[k] + (int64_t)cn[1 + k] * cl.ns[k];
+            } else {
+                off = cb1->c_off + soff[r] + soff[kXRows + c];
+            }
+            // Garner: balanced mixed-radix digits v_i of the residues.  Every
+            // quantity is an integer below 2^19 in magnitude (|r_i D| <=
+            // 255 * 128, |v_j D| <= 128 * 128, at most 15 terms), so FP32
+            // holds it exactly; the quotient rint(t / m_i) from one FMA is
+            // exact for odd m_i (t / m_i stays 1/(2 m_i) away from a half
+            // integer, far above the product's rounding), which leaves t
+            // in [-(m_i - 1)/2, (m_i - 1)/2].
+            float v[L];
+            StaticFor<0, L>::run([&](auto ii) {
+                constexpr int i = decltype(ii)::value;
+                const float ri = __int_as_float(0x4B000000 | (int)sres[i][r][c]) - 8388608.0f;
+                if constexpr (i == 0) {
+                    v[0] = ri >= 128.0f ? ri - 256.0f : ri;             // m_0 = 256: the byte itself
+                } else {
+                    constexpr float mi = (float)crt_modulus(i), minv = 1.0f / (float)crt_modulus(i);
+                    float t = ri * (float)crt_garner_d(0, i);
+                    StaticFor<0, i>::run([&](auto jj) {
+                        constexpr int j = decltype(jj)::value;
+                        t = fmaf(-v[j], (float)crt_garner_d(j, i), t);
+                    });
+                    v[i] = fmaf(-(fmaf(t, minv, kMagicF) - kMagicF), mi, t);
+                }
+            });
+            // digits to double by bits (|v| < 2^22): float 1.5*2^23 + v -> int -> double
+            auto digit = [](float f) {
+                const int iv = __float_as_int(f + kMagicF) - 0x4B400000;
+                return __hiloint2double(0x43380000, iv ^ (int)0x80000000) - 6755401588539392.0;
+            };
+            double X = digit(v[L - 1]);
+#pragma unroll
+            for (int i = L - 2; i >= 0; i--) X = fma(X, (double)crt_modulus(i), digit(v[i]));
+            // 2^(e_row + e_col - 2P) from its bits (a row without exponent has X = 0)
+            const int e2 = sexp[r] + sexp[kXRows + c] - 2 * cp.P;
+            const double p2 = e2 < -1022 ? 0.0 : __hiloint2double((min(e2, 1023) + 1023) << 20, 0);
+            const double val = scale * (X * p2);
+            double *dst = C + off;
+            if (add) *dst += val;
+            else *dst = val;
         }
     }
 }
@@ -749,12 +769,13 @@ cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const D
 
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
                                const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab,
-                               const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey,
-                               double *c, int32_t add, const CrtParams &cp, cudaStream_t s) {
+                               const DCrtCell *cells, const uint8_t *out, const int32_t *gidx,
+                               const int32_t *ex, const int32_t *ey, double *c, int32_t add, double scale,
+                               const CrtParams &cp, cudaStream_t s) {
     if (nitems <= 0) return cudaSuccess;
     const int grid = 32 * nitems < 8 * num_sms() ? 32 * nitems : 8 * num_sms();
     switch (cp.L) {
-#define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, out, gidx, ex, ey, c, add, cp); break;
+#define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, c, add, scale, cp); break;
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
 #undef CASE_L
     default: return cudaErrorInvalidValue;

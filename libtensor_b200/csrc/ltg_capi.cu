@@ -156,7 +156,8 @@ struct CrtExec {
     CrtParams cp{};
     int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0, ngroups = 0, nunits = 0;
     int64_t src_elems = 0, res_bytes = 0;   // operand elements read per pass, residue bytes written
-    DevBuf panels, units, tasks, items, cblks, comps, ctab, gidx, ex, ey, res, out, err;
+    double scale = 1.0;                     // kc (and d in add mode) times the pair coefficients' scale
+    DevBuf panels, units, tasks, items, cblks, comps, ctab, cells, gidx, ex, ey, res, out, err;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
     int32_t *err_host = nullptr;
@@ -800,6 +801,7 @@ void crt_groups(const ltg_plan *pl, const BlockTensorHost &ch, const CrtSideMap 
     const size_t ne = cbt.size();
     group_of.assign(ne, -1);
     if (ne < 2) return;
+    if (sm[0].dims.size() > (size_t)kCrtSideDims || sm[1].dims.size() > (size_t)kCrtSideDims) return;
     // contracted dims of A in A order (the k order of every cell)
     std::vector<int> kdims;
     for (int i = 0; i < NA; i++) if (c0.conn[NC + i] >= NC + NA) kdims.push_back(i);
@@ -1116,6 +1118,7 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     // pieces, one task and its tiles
     std::vector<DCrtPanel> pieces, records;
     std::vector<DCrtComp> comps;
+    std::vector<DCrtCell> cells;
     std::vector<int32_t> ctab;
     size_t npieces = 0;
     for (const CrtGroupHost &G : groups) npieces += G.ac.size() + G.bc.size();
@@ -1172,17 +1175,44 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         };
         for (const auto &x : G.ac) piece(RR, 0, x.second, rofs[x.first.first], G.rn[x.first.first], x.first.second);
         for (const auto &x : G.bc) piece(SR, 1, x.second, sofs[x.first.second], G.sn[x.first.second], x.first.first);
-        // C placement tables
+        // C placement tables: per row (column) its block and its coordinates
+        // on the C dims of its side; per C block its offset and strides
         DCrtComp cc;
         cc.rows = RR.rows; cc.cols = SR.rows; cc.ncb = (int32_t)G.skey.size();
+        int64_t ic[kMaxOrder], dcb[kMaxOrder], scb[kMaxOrder];
+        auto side_entries = [&](int cside, const std::vector<int64_t> &ext, const std::vector<int32_t> &ce) {
+            const std::vector<int> &dims = sm[cside].dims;
+            for (size_t b = 0; b < ext.size(); b++) {
+                ch.bis.unabs(pl->plan.schedule[ce[b]], ic);
+                ch.bis.block_dims(ic, dcb);
+                for (int64_t i = 0; i < ext[b]; i++) {
+                    int32_t co[kCrtSideDims] = {0, 0, 0, 0};
+                    int64_t q = i;
+                    for (int k = (int)dims.size() - 1; k >= 0; k--) { co[k] = (int32_t)(q % dcb[dims[k]]); q /= dcb[dims[k]]; }
+                    ctab.push_back((int32_t)b);
+                    for (int k = 0; k < kCrtSideDims; k++) ctab.push_back(co[k]);
+                }
+            }
+        };
         cc.row_off = (int32_t)ctab.size();
-        for (size_t b = 0; b < G.rn.size(); b++)
-            for (int64_t i = 0; i < G.rn[b]; i++) { ctab.push_back((int32_t)b); ctab.push_back((int32_t)i); }
+        side_entries(0, G.rn, G.rce);
         cc.col_off = (int32_t)ctab.size();
-        for (size_t b = 0; b < G.sn.size(); b++)
-            for (int64_t i = 0; i < G.sn[b]; i++) { ctab.push_back((int32_t)b); ctab.push_back((int32_t)i); }
+        side_entries(1, G.sn, G.sce);
         cc.cell_off = (int32_t)ctab.size();
-        ctab.insert(ctab.end(), G.cell.begin(), G.cell.end());
+        for (int32_t e : G.cell) {
+            if (e < 0) { ctab.push_back(-1); continue; }
+            DCrtCell cl;
+            std::memset(&cl, 0, sizeof(cl));
+            cl.c_off = cbt[e].c_off;
+            ch.bis.unabs(pl->plan.schedule[e], ic);
+            ch.bis.block_dims(ic, dcb);
+            int64_t x = 1;
+            for (int d = ch.bis.n - 1; d >= 0; d--) { scb[d] = x; x *= dcb[d]; }
+            for (size_t k = 0; k < sm[0].dims.size(); k++) cl.ms[k] = (int32_t)scb[sm[0].dims[k]];
+            for (size_t k = 0; k < sm[1].dims.size(); k++) cl.ns[k] = (int32_t)scb[sm[1].dims[k]];
+            ctab.push_back((int32_t)cells.size());
+            cells.push_back(cl);
+        }
         comps.push_back(cc);
         // the product and its tiles
         const int32_t xrec = swap ? srec : rrec, yrec = swap ? rrec : srec;
@@ -1263,8 +1293,11 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     upload_vec(ex->gidx, gidx, s);
     if (comps.empty()) comps.resize(1);
     if (ctab.empty()) ctab.resize(1);
+    if (cells.empty()) cells.resize(1);
     upload_vec(ex->comps, comps, s);
     upload_vec(ex->ctab, ctab, s);
+    upload_vec(ex->cells, cells, s);
+    ex->scale = post;
     ex->err.alloc(sizeof(int32_t));
     LTG_CUDA(cudaMemsetAsync(ex->err.p, 0, sizeof(int32_t), s));
     LTG_CUDA(cudaMallocHost(&ex->err_host, sizeof(int32_t)));
@@ -1993,9 +2026,9 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             TimedLaunch t_comb(ctx, LTG_KERNEL_OZ_COMBINE);
             LTG_CUDA(launch_crt_combine(cx->panels.as<DCrtPanel>(), cx->items.as<DCrtItem>(), cx->nitems,
                                         cx->cblks.as<DCBlock>(), cx->comps.as<DCrtComp>(), cx->ctab.as<int32_t>(),
-                                        cx->out.as<uint8_t>(), cx->gidx.as<int32_t>(),
+                                        cx->cells.as<DCrtCell>(), cx->out.as<uint8_t>(), cx->gidx.as<int32_t>(),
                                         cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), c->arena.as<double>(), add,
-                                        cx->cp, s));
+                                        cx->scale, cx->cp, s));
             t_comb.done();
             ctx->launches += 6;
             if (!ctx->capturing)

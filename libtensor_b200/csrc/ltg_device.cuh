@@ -121,14 +121,22 @@ struct DCrtItem {
 // A grouped product: C blocks whose row blocks (C dims taken from A) and
 // column blocks (C dims taken from B) form one dense grid, computed as one
 // product over the union of their contracted blocks.  Row m of the group is
-// (row block, row within the block) = tab[row_off + 2m], tab[row_off + 2m + 1];
-// columns likewise at col_off; tab[cell_off + R * ncb + S] is the C block
-// (DCBlock index) of row block R and column block S, or -1 when that block is
-// not computed by this contraction.
+// tab[row_off + 5m .. +4] = (row block, its coordinates on the row dims, unused
+// ones 0); columns likewise at col_off; tab[cell_off + R * ncb + S] is the
+// DCrtCell of row block R and column block S, or -1 when that block is not
+// computed by this contraction.
 struct DCrtComp {
     int32_t rows, cols;           // C rows (side of A) and columns (side of B)
     int32_t ncb;                  // column blocks
     int32_t row_off, col_off, cell_off;
+};
+// Grouped products: a C block of a group, its offset and the C strides of
+// its row dims (the C dims taken from A, in C order) and column dims; the row
+// entries of DCrtComp give a row's block and its coordinates on those dims.
+constexpr int kCrtSideDims = 4;
+struct DCrtCell {
+    int64_t c_off;
+    int32_t ms[kCrtSideDims], ns[kCrtSideDims];
 };
 
 // Moduli of a modular contraction and its scaling (the constants of Garner's
@@ -270,9 +278,9 @@ cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const D
     const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp, int32_t *err,
     cudaStream_t s);
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
-    const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab, const uint8_t *out,
-    const int32_t *gidx, const int32_t *ex, const int32_t *ey, double *c, int32_t add,
-    const CrtParams &cp, cudaStream_t s);
+    const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab, const DCrtCell *cells,
+    const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey, double *c,
+    int32_t add, double scale, const CrtParams &cp, cudaStream_t s);
 
 // Element-wise transfer kernels.  max_terms bounds nterms and tile_bytes the
 // shared-memory tiles of any tiled-mode job.
