@@ -63,6 +63,8 @@ def parse():
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-DMMA companion timing")
     p.add_argument("--tile", type=int, default=-1, help="force one tile shape (debug)")
+    p.add_argument("--crt-rows", type=int, default=0, choices=[0, 128, 256],
+                   help="modular mode: rows of the products kernel's work items (0: default, 256)")
     a = p.parse_args()
     if a.mode == "plain":
         a.nslices = 0
@@ -266,6 +268,8 @@ def ltg_arm(args):
         ctx.synchronize()
 
     tiles = None
+    if args.crt_rows:
+        op.set_crt_rows(args.crt_rows)
     if args.tile >= 0:
         op.set_tile(args.tile)
     elif not args.no_autotune:

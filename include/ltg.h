@@ -205,6 +205,12 @@ int ltg_contract2_set_tile(ltg_plan *plan, int32_t cfg);
  * a few rows, as under point-group symmetry, fill whole tiles).  No reference
  * counterpart. */
 int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable);
+/* Modular mode: rows of the products kernel's work items, 256 (two MMA
+ * tiles sharing each operand tile of the other side; also 0, the default) or
+ * 128 (one MMA tile; the epilogue of one modulus overlaps the products of the
+ * next, at twice the operand traffic per product).  Both give identical bits.
+ * No reference counterpart. */
+int ltg_contract2_set_crt_rows(ltg_plan *plan, int32_t rows);
 /* Host-side summary of the grouped products the modular mode would use for
  * result c: number of groups, C blocks they cover, flops of the grouped
  * products (padding of the contracted blocks to 4 included) and algorithmic

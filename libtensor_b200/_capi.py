@@ -87,6 +87,7 @@ _SIGS = {
     "ltg_contract2_set_tile": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_set_grouping": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_group_info": (C.c_int, [c_vp, c_vp, c_i64p, c_i64p, c_dblp, c_dblp]),
+    "ltg_contract2_set_crt_rows": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_autotune": (C.c_int, [c_vp, c_vp, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                          C.c_double, C.c_int32]),
     "ltg_plan_tiles": (C.c_int, [c_vp, c_i64p, c_i64p, c_i32p, C.c_int64, c_i64p]),

@@ -306,6 +306,10 @@ class btod_contract2:
         """Modular mode: grouped products of small C blocks (default on)."""
         check(lib().ltg_contract2_set_grouping(self.h, 1 if enable else 0))
 
+    def set_crt_rows(self, rows: int):
+        """Modular mode: rows of the products kernel's work items (128, 256; 0 default = 256)."""
+        check(lib().ltg_contract2_set_crt_rows(self.h, rows))
+
     def group_info(self, c: block_tensor):
         """(groups, C blocks grouped, grouped-product flops, their blocks'
         algorithmic flops) of the modular mode for result c; host only."""

@@ -13,8 +13,9 @@
 //   3. products (crt_gemm_kernel): per C tile and modulus, all pairs and k
 //      blocks accumulate sum_p sum_k A_l * B_l exactly in one INT32 TMEM
 //      accumulator (|sum| < 2^31 is checked on the host); the epilogue warps
-//      reduce it mod m_l to one byte per element while the MMA warp fills the
-//      other accumulator with the next modulus;
+//      reduce it mod m_l to one byte per element; items of one 128-row tile
+//      alternate between two accumulator slots, so that the MMA warp fills
+//      one with the next modulus while the epilogue drains the other;
 //   4. recombination (crt_combine_kernel): Garner's mixed-radix algorithm
 //      with balanced digits gives the exact integer sum_p c_p A'_p B'_p in
 //      (-M/2, M/2), M = prod m_l (the host chooses P so that it fits), which
@@ -23,9 +24,9 @@
 // The error is that of rounding each operand to P bits relative to its row's
 // largest element (P about 43 for 13 moduli and K up to a few thousand).
 //
-// Warp roles of the products kernel (192 threads): warps 0-3 epilogue (TMEM
-// lanes 0-127, one tile row per thread), warp 4 bulk-copy producer, warp 5
-// MMA issuer.  Operand tiles are whole tile images moved by 1-D
+// Warp roles of the products kernel (320 threads): warps 0-7 epilogue (two
+// per TMEM lane quarter, one tile row per thread, alternate 16-column
+// chunks), warp 8 bulk-copy producer, warp 9 MMA issuer.  Operand tiles are whole tile images moved by 1-D
 // cp.async.bulk (no tensor maps, no multicast); every mbarrier wait is
 // bounded in time and reports through *err.
 #include <type_traits>
@@ -43,7 +44,8 @@ constexpr int kSubBytes = 2 * kXTile + kMaxNt * kKB;    // one k block: two M ti
 constexpr int kKbPerStage = 4;                           // k blocks per pipeline stage
 constexpr int kStageBytes = kKbPerStage * kSubBytes;     // 32 KB
 constexpr int kMaxStages = 8;
-constexpr int kGemmThreads = 192;
+constexpr int kEpiWarps = 8;                        // two per TMEM lane quarter
+constexpr int kGemmThreads = 32 * (kEpiWarps + 2);  // + bulk-copy producer + MMA issuer
 constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s per barrier wait
 constexpr double kMagicD = 6755399441055744.0;      // 1.5 * 2^52: round-to-integer constant
 constexpr float kMagicF = 12582912.0f;              // 1.5 * 2^23
@@ -435,7 +437,7 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
     const int L = cp.L;
     if (threadIdx.x == 0) {
         for (int i = 0; i < stages; i++) { mbar_init(&full_bar[i], 1); mbar_init(&empty_bar[i], 1); }
-        for (int b = 0; b < 2; b++) { mbar_init(&accf_bar[b], 1); mbar_init(&acce_bar[b], 4); }
+        for (int b = 0; b < 2; b++) { mbar_init(&accf_bar[b], 1); mbar_init(&acce_bar[b], kEpiWarps); }
         mbar_init(&drain_bar, 1);
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -451,7 +453,7 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
     const uint32_t tmem = tmem_base_s;
     const uint32_t smem0 = smem_u32(smem);
 
-    if (warp == 4) {
+    if (warp == kEpiWarps) {
         // ------------------------------------------------ bulk-copy producer
         if (lane == 0) {
             int st = 0;
@@ -495,21 +497,28 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                     if (armed[i] >= 0) (void)mbar_wait(&full_bar[i], (uint32_t)armed[i], &never);
             }
         }
-    } else if (warp == 5) {
+    } else if (warp == kEpiWarps + 1) {
         // ------------------------------------------------ MMA issuer
         if (lane == 0) {
             int st = 0;
             uint32_t ph = 0;
-            uint32_t fills = 0;                      // accumulator fills so far (one per item and modulus)
+            uint32_t uses[2] = {0, 0};               // fills of each accumulator slot so far
+            int rr = 0;                              // slot of the next one-tile fill
             bool ok = true;
             for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
                 const DCrtItem item = items[it];
                 const uint32_t idesc = instr_desc_i8(item.nt);
                 for (int l = 0; l < L && ok; l++) {
-                    if (fills > 0) {                 // the epilogue has read the previous fill
-                        if (!mbar_wait(&acce_bar[0], (fills - 1) & 1, &abort_s)) { ok = false; break; }
+                    // a two-tile fill takes both slots, a one-tile fill slot rr
+                    const int s0 = item.nx == 2 ? 0 : rr;
+                    // the epilogue has read the slots' previous fills
+                    if (uses[s0] > 0 && !mbar_wait(&acce_bar[s0], (uses[s0] - 1) & 1, &abort_s)) { ok = false; break; }
+                    if (item.nx == 2 && uses[1] > 0 && !mbar_wait(&acce_bar[1], (uses[1] - 1) & 1, &abort_s)) {
+                        ok = false;
+                        break;
                     }
                     tc_fence_after();
+                    const uint32_t d0 = tmem + (uint32_t)(s0 * kMaxNt);
                     uint32_t acc = 0;
                     for (int ti = item.t_begin; ti < item.t_end && ok; ti++) {
                         const int nkb = tasks[ti].nkb;
@@ -520,7 +529,7 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                             for (int j = 0; j < nsub; j++) {
                                 const uint32_t a0 = smem0 + st * kStageBytes + j * kSubBytes;
                                 const uint64_t db = smem_desc_kmajor(a0 + 2 * kXTile);
-                                umma_i8(tmem, smem_desc_kmajor(a0), db, idesc, acc);
+                                umma_i8(d0, smem_desc_kmajor(a0), db, idesc, acc);
                                 if (item.nx == 2) umma_i8(tmem + kMaxNt, smem_desc_kmajor(a0 + kXTile), db, idesc, acc);
                                 acc = 1;
                             }
@@ -529,8 +538,10 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                         }
                     }
                     if (!ok) break;
-                    umma_commit(&accf_bar[0]);
-                    fills++;
+                    umma_commit(&accf_bar[s0]);
+                    uses[s0]++;
+                    if (item.nx == 2) { umma_commit(&accf_bar[1]); uses[1]++; }
+                    else rr ^= 1;
                 }
             }
             if (!ok) {
@@ -542,22 +553,28 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
             }
         }
     } else {
-        // ------------------------------------------------ epilogue (warps 0-3)
-        const int row = warp * 32 + lane;                         // TMEM lane == tile row
-        uint32_t fills = 0;
+        // ------------------------------------------------ epilogue (warps 0-7)
+        // warp w reads TMEM lanes 32 (w % 4) .. + 31 (the lane quarter a warp
+        // may access) and every other 16-column chunk, starting at 16 (w / 4)
+        const int quarter = warp & 3, chunk0 = (warp >> 2) * 16;
+        const int row = quarter * 32 + lane;                      // TMEM lane == tile row
+        uint32_t uses[2] = {0, 0};                                // same slot sequence as the MMA warp
+        int rr = 0;
         bool ok = true;
         for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
             const DCrtItem item = items[it];
             for (int l = 0; l < L; l++) {
-                ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[0], fills & 1, &abort_s));
+                const int s0 = item.nx == 2 ? 0 : rr;
+                ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[s0], uses[s0] & 1, &abort_s));
+                if (ok && item.nx == 2) ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[1], uses[1] & 1, &abort_s));
                 if (!ok) break;
                 tc_fence_after();
                 const double minv = cp.minv_d[l];
                 const int mi = cp.m[l];
                 for (int xh = 0; xh < item.nx; xh++) {
-                    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + xh * kMaxNt;
+                    const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)((s0 + xh) * kMaxNt);
                     uint8_t *orow = out + item.res_off + ((int64_t)(l * item.nx + xh) * kXRows + row) * item.nt;
-                    for (int c0 = 0; c0 < item.nt; c0 += 16) {
+                    for (int c0 = chunk0; c0 < item.nt; c0 += 32) {
                         uint32_t v[16];
                         tmem_ld16(taddr + (uint32_t)c0, v);
                         tmem_wait_ld();
@@ -580,8 +597,13 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&acce_bar[0]);
-                fills++;
+                if (lane == 0) {
+                    mbar_arrive(&acce_bar[s0]);
+                    if (item.nx == 2) mbar_arrive(&acce_bar[1]);
+                }
+                uses[s0]++;
+                if (item.nx == 2) uses[1]++;
+                else rr ^= 1;
             }
         }
         if (!ok) { abort_s = 1; atomicExch(err, 7); }
@@ -731,9 +753,9 @@ int num_sms() {
 cudaError_t launch_crt_exponents(const DCrtPanel *panels, const int4 *units, int32_t nunits, int32_t nx,
                                  int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
                                  int32_t *ey, cudaStream_t s) {
-    if (nunits <= 0) return cudaSuccess;
     crt_fill_kernel<<<64, 256, 0, s>>>(ex, nx, kNoExp);
     crt_fill_kernel<<<64, 256, 0, s>>>(ey, ny, kNoExp);
+    if (nunits <= 0) return cudaGetLastError();
     const int grid = nunits;                               // one unit per CTA
     crt_exp_kernel<<<grid, kSplitThreads, 0, s>>>(panels, units, nunits, a, b, gidx, ex, ey);
     return cudaGetLastError();

@@ -173,6 +173,7 @@ struct ltg_plan {
     ltg_bt *a = nullptr, *b = nullptr;
     int forced_tile = -1;         // >= 0: every C block uses this tile shape
     bool group_products = true;   // modular mode: small C blocks grouped into larger products
+    int crt_rows = 0;             // modular mode: work-item rows (128, 256; 0 default)
     std::map<std::pair<int64_t, int64_t>, int> tile_override;   // autotuned (M, N) -> shape
     ContractPlan plan;
     // cache of device task arrays keyed by (C tensor, ka, kb, kc, add, d)
@@ -1088,30 +1089,19 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         pack_sub(b.cn, x.nn, x.next, x.nc_str, nullptr);
         x.t_begin = b.t_begin; x.t_end = b.t_end;
     }
-    // work items: 128 x nt tiles, costliest first
-    std::vector<std::pair<double, DCrtItem>> iv;
-    int64_t out_bytes = 0;
+    // products (one per C block or grouped product), cut into work items below
+    struct Prod {
+        int32_t cblk, comp, t_begin, t_end, gx, gy, nt;
+        int64_t xext, yext;
+        double kw;                    // contracted length (work per tile element)
+    };
+    std::vector<Prod> prods;
     for (size_t e = 0; e < cbt.size(); e++) {
         const CBlockTask &b = cbt[e];
         if (b.t_end <= b.t_begin || group_of[e] >= 0) continue;
         const DCrtTask &t0 = dt[b.t_begin];
-        const int32_t nt = panels[t0.py].tr;
-        const int64_t xext = swap ? b.N : b.M, yext = swap ? b.M : b.N;
-        for (int64_t x0 = 0; x0 < xext; x0 += 256)
-            for (int64_t y0 = 0; y0 < yext; y0 += nt) {
-                DCrtItem it;
-                std::memset(&it, 0, sizeof(it));
-                it.cblk = (int32_t)e;
-                it.x0 = (int32_t)x0; it.y0 = (int32_t)y0;
-                it.nt = nt;
-                it.nx = x0 + 128 < xext ? 2 : 1;
-                it.t_begin = b.t_begin; it.t_end = b.t_end;
-                it.gx = t0.px; it.gy = t0.py;
-                it.comp = -1;
-                it.res_off = out_bytes;
-                out_bytes += (int64_t)L * it.nx * 128 * nt;
-                iv.push_back({b.kflops * nt * it.nx, it});
-            }
+        prods.push_back({(int32_t)e, -1, b.t_begin, b.t_end, t0.px, t0.py, panels[t0.py].tr,
+                         swap ? b.N : b.M, swap ? b.M : b.N, b.kflops});
     }
     // grouped products: per group one image pair (records, placed after the
     // panels and pieces the split passes process) written cell by cell by
@@ -1224,23 +1214,32 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         tk.nkb = XR.K_pad / 32;
         const int32_t ti = (int32_t)dt.size();
         dt.push_back(tk);
-        const int32_t nt = YR.tr;
-        for (int64_t x0 = 0; x0 < XR.rows; x0 += 256)
-            for (int64_t y0 = 0; y0 < YR.rows; y0 += nt) {
+        prods.push_back({-1, (int32_t)gi, ti, ti + 1, xrec, yrec, YR.tr, XR.rows, YR.rows, (double)kt});
+    }
+    // work items: tiles of 256 (two MMA tiles sharing each N-side tile; the
+    // default) or 128 rows (one MMA tile; its accumulator slots alternate, so
+    // the epilogue of one modulus overlaps the products of the next, but every
+    // N-side tile is loaded per 128 rows, which makes the products bound by
+    // L2 bandwidth on this part) by nt columns, costliest first
+    const int64_t xstep = pl->crt_rows == 128 ? 128 : 256;
+    std::vector<std::pair<double, DCrtItem>> iv;
+    int64_t out_bytes = 0;
+    for (const Prod &q : prods)
+        for (int64_t x0 = 0; x0 < q.xext; x0 += xstep)
+            for (int64_t y0 = 0; y0 < q.yext; y0 += q.nt) {
                 DCrtItem it;
                 std::memset(&it, 0, sizeof(it));
-                it.cblk = -1;
-                it.comp = (int32_t)gi;
+                it.cblk = q.cblk;
+                it.comp = q.comp;
                 it.x0 = (int32_t)x0; it.y0 = (int32_t)y0;
-                it.nt = nt;
-                it.nx = x0 + 128 < XR.rows ? 2 : 1;
-                it.t_begin = ti; it.t_end = ti + 1;
-                it.gx = xrec; it.gy = yrec;
+                it.nt = q.nt;
+                it.nx = xstep == 256 && x0 + 128 < q.xext ? 2 : 1;
+                it.t_begin = q.t_begin; it.t_end = q.t_end;
+                it.gx = q.gx; it.gy = q.gy;
                 it.res_off = out_bytes;
-                out_bytes += (int64_t)L * it.nx * 128 * nt;
-                iv.push_back({(double)kt * nt * it.nx, it});
+                out_bytes += (int64_t)L * it.nx * 128 * q.nt;
+                iv.push_back({q.kw * q.nt * it.nx, it});
             }
-    }
     const int32_t nsplit = (int32_t)(panels.size() + pieces.size());   // panels the split passes process
     panels.insert(panels.end(), pieces.begin(), pieces.end());
     panels.insert(panels.end(), records.begin(), records.end());
@@ -2030,7 +2029,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                                         cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), c->arena.as<double>(), add,
                                         cx->scale, cx->cp, s));
             t_comb.done();
-            ctx->launches += 6;
+            ctx->launches += 2 + (cx->nunits > 0 ? 2 : 0) + (cx->nitems > 0 ? 2 : 0);
             if (!ctx->capturing)
                 LTG_CUDA(cudaMemcpyAsync(cx->err_host, cx->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
             if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
@@ -2132,6 +2131,16 @@ int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable) {
         if (!plan) throw error(kErrBadArg, "null plan");
         if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
         plan->group_products = enable != 0;
+        plan->crt.clear();
+    });
+}
+
+int ltg_contract2_set_crt_rows(ltg_plan *plan, int32_t rows) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (rows != 0 && rows != 128 && rows != 256) throw error(kErrBadArg, "work-item rows must be 0, 128 or 256");
+        if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
+        plan->crt_rows = rows;
         plan->crt.clear();
     });
 }

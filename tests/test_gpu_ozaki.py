@@ -97,3 +97,30 @@ def test_crt_grouped_products_are_bit_identical(gctx, case):
     op.set_grouping(True)
     gctx.synchronize()
     assert np.array_equal(C1.download().view(np.uint64), C2.download().view(np.uint64))
+
+
+def _crt_variants(gctx, case, seeds, setters):
+    """Results of the modular mode (13 moduli) under each setting of a plan
+    switch, as raw bits."""
+    A, _, _ = seeded_pair(gctx, case.a, seeds[0], case.a_scale, case.zero_a)
+    B, _, _ = seeded_pair(gctx, case.b, seeds[1], case.b_scale)
+    contr = contraction2(case.n, case.m, case.k, case.permc)
+    for p in case.pairs:
+        contr.contract(*p)
+    op = btod_contract2(contr, A, B, case.ka, case.kb, case.kc)
+    out = []
+    for setter in setters:
+        C = op.make_result()
+        setter(op)
+        op.perform(C, mode=MODE_OZAKI_CRT, nslices=13)
+        gctx.synchronize()
+        out.append(C.download().view(np.uint64))
+    return out
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_crt_item_rows_are_bit_identical(gctx, case):
+    """Work items of 128 rows (alternating accumulator slots) and of 256 rows
+    (two MMA tiles per item) compute the same exact integers."""
+    out = _crt_variants(gctx, case, (7, 8), [lambda op: op.set_crt_rows(128), lambda op: op.set_crt_rows(256)])
+    assert np.array_equal(out[0], out[1])
