@@ -32,6 +32,7 @@ SOURCES = [
     "ozaki.cu",
     "noalloc.cu",
     "crt.cu",
+    "group.cu",
 ]
 OPTIONAL_SOURCES = []
 

@@ -131,9 +131,21 @@ struct ltg_bt {
     DevBuf denom_dev, denom_off;
 };
 
+// Grouped products of the plain FP64 path (the groups of crt_groups): the
+// operand cells of every group gathered into dense panels in buf, one DMMA
+// product per group into a dense result in buf, scattered into the C blocks.
+struct PlainGroups {
+    int32_t ngroups = 0, nunits = 0, nsunits = 0;
+    double scale = 1.0;                       // ka kb kc (and d in add mode)
+    DevBuf buf, pieces, units, sunits, comps, res_off, ctab, cells;
+    DevBuf tasks, cblks, items;               // DMMA work over buf
+    std::vector<std::pair<int32_t, std::pair<int32_t, int32_t>>> launches;   // cfg -> item range
+};
+
 struct ContractExec {
     // device task arrays bound to one output tensor and coefficient set
     DevBuf tasks, cblks, items;
+    std::unique_ptr<PlainGroups> groups;      // grouped small blocks, if any
     std::vector<std::pair<int32_t, std::pair<int32_t, int32_t>>> launches;  // cfg -> item range
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;  // assign mode: blocks not in the schedule
     std::vector<int64_t> sched_slots;
@@ -430,6 +442,12 @@ void pack_sub(const SubDims &s, int32_t &n, int32_t *ext, int32_t *str0, int32_t
     }
 }
 
+void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &cbt, double kabc, double post,
+                        std::vector<int32_t> &group_of, PlainGroups &pg);
+std::vector<std::pair<int64_t, int64_t>> plain_group_shapes(ltg_plan *pl, ltg_bt *c,
+                                                           const std::vector<CBlockTask> &cbt,
+                                                           std::vector<int32_t> &group_of);
+
 ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double kc, int add, double d) {
     auto key = std::make_tuple(c->uid, ka, kb, kc, add, add ? d : 0.0);
     auto it = pl->exec.find(key);
@@ -481,10 +499,18 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
         x.t_begin = b.t_begin; x.t_end = b.t_end;
         for (int32_t t = b.t_begin; t < b.t_end; t++) dt[t].coeff = tasks[t].coeff / c0;
     }
+    // small blocks computed as grouped products
+    std::vector<int32_t> group_of(cbt.size(), -1);
+    if (pl->group_products && !pl->plan.coalesced) {
+        ex->groups.reset(new PlainGroups());
+        build_plain_groups(pl, c, cbt, ka * kb * kc, post, group_of, *ex->groups);
+        if (ex->groups->ngroups == 0) ex->groups.reset();
+    }
     // Work items per tile configuration, costliest first (LPT order for the
     // persistent work queue).
     std::vector<std::vector<std::pair<double, DItem>>> per_cfg(8);
     for (size_t e = 0; e < cbt.size(); e++) {
+        if (group_of[e] >= 0) continue;
         int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(cbt[e].M, cbt[e].N);
         auto ov = pl->tile_override.find({cbt[e].M, cbt[e].N});
         if (pl->forced_tile < 0 && ov != pl->tile_override.end()) cfg = ov->second;
@@ -948,6 +974,204 @@ void crt_groups(const ltg_plan *pl, const BlockTensorHost &ch, const CrtSideMap 
     }
 }
 
+// C placement tables of a group: per row (column) its block and its
+// coordinates on the C dims of its side; per C block of the grid its offset
+// and C strides (DCrtComp, DCrtCell).
+DCrtComp crt_group_tables(const ltg_plan *pl, const BlockTensorHost &ch, const CrtSideMap *sm,
+                          const std::vector<CBlockTask> &cbt, const CrtGroupHost &G,
+                          std::vector<int32_t> &ctab, std::vector<DCrtCell> &cells) {
+    DCrtComp cc;
+    cc.rows = 0; cc.cols = 0;
+    for (int64_t v : G.rn) cc.rows += (int32_t)v;
+    for (int64_t v : G.sn) cc.cols += (int32_t)v;
+    cc.ncb = (int32_t)G.skey.size();
+    int64_t ic[kMaxOrder], dcb[kMaxOrder], scb[kMaxOrder];
+    auto side_entries = [&](int cside, const std::vector<int64_t> &ext, const std::vector<int32_t> &ce) {
+        const std::vector<int> &dims = sm[cside].dims;
+        for (size_t b = 0; b < ext.size(); b++) {
+            ch.bis.unabs(pl->plan.schedule[ce[b]], ic);
+            ch.bis.block_dims(ic, dcb);
+            for (int64_t i = 0; i < ext[b]; i++) {
+                int32_t co[kCrtSideDims] = {0, 0, 0, 0};
+                int64_t q = i;
+                for (int k = (int)dims.size() - 1; k >= 0; k--) { co[k] = (int32_t)(q % dcb[dims[k]]); q /= dcb[dims[k]]; }
+                ctab.push_back((int32_t)b);
+                for (int k = 0; k < kCrtSideDims; k++) ctab.push_back(co[k]);
+            }
+        }
+    };
+    cc.row_off = (int32_t)ctab.size();
+    side_entries(0, G.rn, G.rce);
+    cc.col_off = (int32_t)ctab.size();
+    side_entries(1, G.sn, G.sce);
+    cc.cell_off = (int32_t)ctab.size();
+    for (int32_t e : G.cell) {
+        if (e < 0) { ctab.push_back(-1); continue; }
+        DCrtCell cl;
+        std::memset(&cl, 0, sizeof(cl));
+        cl.c_off = cbt[e].c_off;
+        ch.bis.unabs(pl->plan.schedule[e], ic);
+        ch.bis.block_dims(ic, dcb);
+        int64_t x = 1;
+        for (int d = ch.bis.n - 1; d >= 0; d--) { scb[d] = x; x *= dcb[d]; }
+        for (size_t k = 0; k < sm[0].dims.size(); k++) cl.ms[k] = (int32_t)scb[sm[0].dims[k]];
+        for (size_t k = 0; k < sm[1].dims.size(); k++) cl.ns[k] = (int32_t)scb[sm[1].dims[k]];
+        ctab.push_back((int32_t)cells.size());
+        cells.push_back(cl);
+    }
+    return cc;
+}
+
+// Dense layout of one group for the plain path (element offsets in buf, all
+// multiples of 4): A panel rows x kt, B panel cols x kt, result rows x cols.
+struct PlainGroupLayout {
+    int64_t rows = 0, cols = 0, kt = 0, aoff = 0, boff = 0, coff = 0;
+    std::vector<int64_t> rofs, sofs, kofs;
+};
+
+bool plain_group_layout(const CrtGroupHost &G, int64_t &off, PlainGroupLayout &lay) {
+    lay.rofs.clear(); lay.sofs.clear(); lay.kofs.clear();
+    lay.rows = lay.cols = lay.kt = 0;
+    for (int64_t v : G.rn) { lay.rofs.push_back(lay.rows); lay.rows += v; }
+    for (int64_t v : G.sn) { lay.sofs.push_back(lay.cols); lay.cols += v; }
+    for (int64_t v : G.kn) { lay.kofs.push_back(lay.kt); lay.kt += round4(v); }
+    const int64_t lim = ((int64_t)1 << 31) - 1;
+    if (lay.rows * lay.kt > lim || lay.cols * lay.kt > lim || lay.rows * lay.cols > lim) return false;
+    auto r4 = [](int64_t x) { return (x + 3) / 4 * 4; };
+    lay.aoff = off; off += r4(lay.rows * lay.kt);
+    lay.boff = off; off += r4(lay.cols * lay.kt);
+    lay.coff = off; off += r4(lay.rows * lay.cols);
+    return true;
+}
+
+std::vector<std::pair<int64_t, int64_t>> plain_group_shapes(ltg_plan *pl, ltg_bt *c,
+                                                           const std::vector<CBlockTask> &cbt,
+                                                           std::vector<int32_t> &group_of) {
+    std::vector<std::pair<int64_t, int64_t>> shapes;
+    group_of.assign(cbt.size(), -1);
+    if (!pl->group_products || pl->plan.coalesced) return shapes;
+    CrtSideMap sm[2];
+    crt_side_maps(pl->plan.contr, c->h, sm);
+    std::vector<CrtGroupHost> groups;
+    crt_groups(pl, c->h, sm, cbt, groups, group_of);
+    int64_t off = 0;
+    PlainGroupLayout lay;
+    for (const CrtGroupHost &G : groups) {
+        if (!plain_group_layout(G, off, lay)) { group_of.assign(cbt.size(), -1); return {}; }
+        shapes.push_back({lay.rows, lay.cols});
+    }
+    return shapes;
+}
+
+void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &cbt, double kabc, double post,
+                        std::vector<int32_t> &group_of, PlainGroups &pg) {
+    CrtSideMap sm[2];
+    crt_side_maps(pl->plan.contr, c->h, sm);
+    std::vector<CrtGroupHost> groups;
+    crt_groups(pl, c->h, sm, cbt, groups, group_of);
+    if (groups.empty()) return;
+    std::vector<DGather> pieces;
+    std::vector<int4> units;
+    std::vector<int2> sunits;
+    std::vector<DCrtComp> comps;
+    std::vector<int32_t> ctab;
+    std::vector<DCrtCell> cells;
+    std::vector<int64_t> res_off;
+    std::vector<DTask> dt;
+    std::vector<DCBlock> dc;
+    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(8);
+    int64_t off = 0;
+    PlainGroupLayout lay;
+    for (size_t gi = 0; gi < groups.size(); gi++) {
+        const CrtGroupHost &G = groups[gi];
+        if (!plain_group_layout(G, off, lay)) { group_of.assign(cbt.size(), -1); return; }
+        auto piece = [&](int src, const CrtCell &cl, int64_t dst_off, int64_t nrow, int64_t K) {
+            DGather q;
+            std::memset(&q, 0, sizeof(q));
+            q.src = src;
+            q.src_off = cl.off;
+            q.dst_off = dst_off;
+            q.rows = (int32_t)nrow;
+            q.K = (int32_t)K;
+            q.ld = (int32_t)lay.kt;
+            q.coef = cl.coef;
+            pack_sub(cl.rows, q.nr, q.rext, q.rstr, nullptr);
+            pack_sub(cl.k, q.nk, q.kext, q.kstr, nullptr);
+            if (cl.rows.total() != nrow || cl.k.total() != K) throw error(kErrState, "grouped cell extents");
+            const int32_t ru = (int32_t)std::max<int64_t>(8, std::min<int64_t>(256, 4096 / std::max<int64_t>(1, K)));
+            for (int32_t r0 = 0; r0 < q.rows; r0 += ru)
+                units.push_back(make_int4((int32_t)pieces.size(), r0, std::min(ru, q.rows - r0), 0));
+            pieces.push_back(q);
+        };
+        for (const auto &x : G.ac)
+            piece(0, x.second, lay.aoff + lay.rofs[x.first.first] * lay.kt + lay.kofs[x.first.second],
+                  G.rn[x.first.first], G.kn[x.first.second]);
+        for (const auto &x : G.bc)
+            piece(1, x.second, lay.boff + lay.sofs[x.first.second] * lay.kt + lay.kofs[x.first.first],
+                  G.sn[x.first.second], G.kn[x.first.first]);
+        comps.push_back(crt_group_tables(pl, c->h, sm, cbt, G, ctab, cells));
+        res_off.push_back(lay.coff);
+        for (int64_t m = 0; m < lay.rows; m++) sunits.push_back(make_int2((int32_t)gi, (int32_t)m));
+        // the dense product: result[m][n] = sum_k A[m][k] B[n][k]
+        DTask t;
+        std::memset(&t, 0, sizeof(t));
+        t.a_off = lay.aoff; t.b_off = lay.boff; t.coeff = 1.0;
+        t.K = (int32_t)lay.kt;
+        t.nk = 1; t.kext[0] = (int32_t)lay.kt; t.ka_str[0] = 1; t.kb_str[0] = 1;
+        t.nm = 1; t.mext[0] = (int32_t)lay.rows; t.ma_str[0] = (int32_t)lay.kt;
+        t.nn = 1; t.next[0] = (int32_t)lay.cols; t.nb_str[0] = (int32_t)lay.kt;
+        for (int i = 1; i < kDevMaxSub; i++) { t.kext[i] = 1; t.mext[i] = 1; t.next[i] = 1; }
+        t.vec_a = 1; t.vec_b = 1;                 // offsets and kt are multiples of 4
+        DCBlock b;
+        std::memset(&b, 0, sizeof(b));
+        b.c_off = lay.coff; b.scale = 1.0;
+        b.M = (int32_t)lay.rows; b.N = (int32_t)lay.cols;
+        b.nm = 1; b.mext[0] = (int32_t)lay.rows; b.mc_str[0] = (int32_t)lay.cols;
+        b.nn = 1; b.next[0] = (int32_t)lay.cols; b.nc_str[0] = 1;
+        for (int i = 1; i < kDevMaxSub; i++) { b.mext[i] = 1; b.next[i] = 1; }
+        b.t_begin = (int32_t)dt.size(); b.t_end = b.t_begin + 1;
+        dt.push_back(t);
+        int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(lay.rows, lay.cols);
+        auto ov = pl->tile_override.find({lay.rows, lay.cols});
+        if (pl->forced_tile < 0 && ov != pl->tile_override.end()) cfg = ov->second;
+        const int bm = tile_cfg_bm(cfg), bn = tile_cfg_bn(cfg);
+        for (int64_t m0 = 0; m0 < lay.rows; m0 += bm)
+            for (int64_t n0 = 0; n0 < lay.cols; n0 += bn) {
+                DItem it; it.cblk = (int32_t)dc.size(); it.m0 = (int32_t)m0; it.n0 = (int32_t)n0; it.pad = 0;
+                per_cfg[cfg].push_back({(double)bm * bn * (double)lay.kt, it});
+            }
+        dc.push_back(b);
+    }
+    std::vector<DItem> items;
+    for (int cfg = 0; cfg < 8; cfg++) {
+        auto &v = per_cfg[cfg];
+        if (v.empty()) continue;
+        std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
+        const int32_t start = (int32_t)items.size();
+        for (auto &q : v) items.push_back(q.second);
+        pg.launches.push_back({cfg, {start, (int32_t)v.size()}});
+    }
+    cudaStream_t s = pl->ctx->stream;
+    pg.ngroups = (int32_t)groups.size();
+    pg.nunits = (int32_t)units.size();
+    pg.nsunits = (int32_t)sunits.size();
+    pg.scale = kabc * post;
+    pg.buf.alloc(std::max<int64_t>(off, 4) * (int64_t)sizeof(double));
+    // cells that no pair uses stay zero
+    LTG_CUDA(cudaMemsetAsync(pg.buf.p, 0, std::max<int64_t>(off, 4) * sizeof(double), s));
+    if (cells.empty()) cells.resize(1);
+    upload_vec(pg.pieces, pieces, s);
+    upload_vec(pg.units, units, s);
+    upload_vec(pg.sunits, sunits, s);
+    upload_vec(pg.comps, comps, s);
+    upload_vec(pg.res_off, res_off, s);
+    upload_vec(pg.ctab, ctab, s);
+    upload_vec(pg.cells, cells, s);
+    upload_vec(pg.tasks, dt, s);
+    upload_vec(pg.cblks, dc, s);
+    upload_vec(pg.items, items, s);
+}
+
 CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, double kc, int add, double d) {
     auto key = std::make_tuple(c->uid, ka, kb, kc, add, add ? d : 0.0, L);
     auto it = pl->crt.find(key);
@@ -1165,45 +1389,7 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         };
         for (const auto &x : G.ac) piece(RR, 0, x.second, rofs[x.first.first], G.rn[x.first.first], x.first.second);
         for (const auto &x : G.bc) piece(SR, 1, x.second, sofs[x.first.second], G.sn[x.first.second], x.first.first);
-        // C placement tables: per row (column) its block and its coordinates
-        // on the C dims of its side; per C block its offset and strides
-        DCrtComp cc;
-        cc.rows = RR.rows; cc.cols = SR.rows; cc.ncb = (int32_t)G.skey.size();
-        int64_t ic[kMaxOrder], dcb[kMaxOrder], scb[kMaxOrder];
-        auto side_entries = [&](int cside, const std::vector<int64_t> &ext, const std::vector<int32_t> &ce) {
-            const std::vector<int> &dims = sm[cside].dims;
-            for (size_t b = 0; b < ext.size(); b++) {
-                ch.bis.unabs(pl->plan.schedule[ce[b]], ic);
-                ch.bis.block_dims(ic, dcb);
-                for (int64_t i = 0; i < ext[b]; i++) {
-                    int32_t co[kCrtSideDims] = {0, 0, 0, 0};
-                    int64_t q = i;
-                    for (int k = (int)dims.size() - 1; k >= 0; k--) { co[k] = (int32_t)(q % dcb[dims[k]]); q /= dcb[dims[k]]; }
-                    ctab.push_back((int32_t)b);
-                    for (int k = 0; k < kCrtSideDims; k++) ctab.push_back(co[k]);
-                }
-            }
-        };
-        cc.row_off = (int32_t)ctab.size();
-        side_entries(0, G.rn, G.rce);
-        cc.col_off = (int32_t)ctab.size();
-        side_entries(1, G.sn, G.sce);
-        cc.cell_off = (int32_t)ctab.size();
-        for (int32_t e : G.cell) {
-            if (e < 0) { ctab.push_back(-1); continue; }
-            DCrtCell cl;
-            std::memset(&cl, 0, sizeof(cl));
-            cl.c_off = cbt[e].c_off;
-            ch.bis.unabs(pl->plan.schedule[e], ic);
-            ch.bis.block_dims(ic, dcb);
-            int64_t x = 1;
-            for (int d = ch.bis.n - 1; d >= 0; d--) { scb[d] = x; x *= dcb[d]; }
-            for (size_t k = 0; k < sm[0].dims.size(); k++) cl.ms[k] = (int32_t)scb[sm[0].dims[k]];
-            for (size_t k = 0; k < sm[1].dims.size(); k++) cl.ns[k] = (int32_t)scb[sm[1].dims[k]];
-            ctab.push_back((int32_t)cells.size());
-            cells.push_back(cl);
-        }
-        comps.push_back(cc);
+        comps.push_back(crt_group_tables(pl, ch, sm, cbt, G, ctab, cells));
         // the product and its tiles
         const int32_t xrec = swap ? srec : rrec, yrec = swap ? rrec : srec;
         const DCrtPanel &XR = records[xrec - rec_base], &YR = records[yrec - rec_base];
@@ -2072,6 +2258,25 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             for (auto &r : ex->zero_ranges)
                 LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
         int slot = 0;
+        PlainGroups *pg = ex->groups.get();
+        if (pg) {
+            TimedLaunch tg(ctx, LTG_KERNEL_TRANSFER);
+            LTG_CUDA(launch_gather_cells(pg->pieces.as<DGather>(), pg->units.as<int4>(), pg->nunits,
+                                         plan->a->arena.as<double>(), plan->b->arena.as<double>(),
+                                         pg->buf.as<double>(), s));
+            tg.done();
+            ctx->launches++;
+            for (auto &l : pg->launches) {
+                TimedLaunch tl(ctx, LTG_KERNEL_CONTRACT_FP64);
+                LTG_CUDA(launch_contract_fp64(pg->tasks.as<DTask>(), pg->cblks.as<DCBlock>(),
+                                              pg->items.as<DItem>() + l.second.first, l.second.second,
+                                              ctx->scratch_counter.as<int32_t>() + (slot++ % 64),
+                                              pg->buf.as<double>(), pg->buf.as<double>(), pg->buf.as<double>(),
+                                              0, l.first, s));
+                tl.done();
+                ctx->launches++;
+            }
+        }
         for (auto &l : ex->launches) {
             TimedLaunch tl(ctx, LTG_KERNEL_CONTRACT_FP64);
             LTG_CUDA(launch_contract_fp64(ex->tasks.as<DTask>(), ex->cblks.as<DCBlock>(),
@@ -2080,6 +2285,14 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                                           plan->a->arena.as<double>(), plan->b->arena.as<double>(),
                                           c->arena.as<double>(), add, l.first, s));
             tl.done();
+            ctx->launches++;
+        }
+        if (pg) {
+            TimedLaunch ts(ctx, LTG_KERNEL_TRANSFER);
+            LTG_CUDA(launch_scatter_groups(pg->comps.as<DCrtComp>(), pg->res_off.as<int64_t>(), pg->ctab.as<int32_t>(),
+                                           pg->cells.as<DCrtCell>(), pg->sunits.as<int2>(), pg->nsunits,
+                                           pg->buf.as<double>(), c->arena.as<double>(), pg->scale, add, s));
+            ts.done();
             ctx->launches++;
         }
         if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
@@ -2190,7 +2403,14 @@ int ltg_contract2_autotune(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nsli
         std::vector<CBlockTask> cbt;
         contract2_tasks(plan->plan, plan->a->h, plan->b->h, c->h, ka, kb, kc, tasks, cbt);
         std::map<std::pair<int64_t, int64_t>, double> work;
-        for (const CBlockTask &b : cbt) work[{b.M, b.N}] += (double)b.M * b.N * b.kflops;
+        std::vector<int32_t> group_of;
+        const std::vector<std::pair<int64_t, int64_t>> gshapes =
+            mode == LTG_MODE_PLAIN_FP64 ? plain_group_shapes(plan, c, cbt, group_of)
+                                        : std::vector<std::pair<int64_t, int64_t>>();
+        if (group_of.size() != cbt.size()) group_of.assign(cbt.size(), -1);
+        for (size_t e = 0; e < cbt.size(); e++)
+            if (group_of[e] < 0) work[{cbt[e].M, cbt[e].N}] += (double)cbt[e].M * cbt[e].N * cbt[e].kflops;
+        for (const auto &g : gshapes) work[g] += (double)g.first * g.second;
         std::vector<std::pair<double, std::pair<int64_t, int64_t>>> order;
         for (auto &w : work) order.push_back({w.second, w.first});
         std::sort(order.rbegin(), order.rend());

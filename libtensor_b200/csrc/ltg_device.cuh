@@ -150,6 +150,18 @@ struct CrtParams {
     double minv_d[kCrtMaxModuli]; // 1 / m_i
 };
 
+// One operand cell of a grouped plain product: rows x K elements of a
+// canonical block (row and k mappings of the pair's orbit transform, times
+// coef) copied to buf[dst_off + r * ld + k].
+struct DGather {
+    int64_t src_off, dst_off;
+    int32_t src;                  // 0: A arena, 1: B arena
+    int32_t rows, K, ld, coef;
+    int32_t nr, nk, pad;
+    int32_t rext[kDevMaxSub], rstr[kDevMaxSub];
+    int32_t kext[kDevMaxSub], kstr[kDevMaxSub];
+};
+
 // ---------------------------------------------------------------- element-wise
 
 constexpr int kMaxTerms = 8;
@@ -281,6 +293,15 @@ cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, i
     const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab, const DCrtCell *cells,
     const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey, double *c,
     int32_t add, double scale, const CrtParams &cp, cudaStream_t s);
+
+// Grouped plain products: operand cells into dense group panels (units:
+// piece, first row, rows), and the dense group results into the C blocks
+// (units: group, result row).
+cudaError_t launch_gather_cells(const DGather *pieces, const int4 *units, int32_t nunits,
+    const double *a, const double *b, double *buf, cudaStream_t s);
+cudaError_t launch_scatter_groups(const DCrtComp *comps, const int64_t *res_off, const int32_t *ctab,
+    const DCrtCell *cells, const int2 *units, int32_t nunits, const double *buf, double *c,
+    double scale, int32_t add, cudaStream_t s);
 
 // Element-wise transfer kernels.  max_terms bounds nterms and tile_bytes the
 // shared-memory tiles of any tiled-mode job.

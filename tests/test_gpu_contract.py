@@ -95,3 +95,22 @@ def test_contract_repeat_is_deterministic(gctx):
     op.perform(C)
     x2 = C.download()
     assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_grouped_products_match_per_block(gctx, case):
+    """Small blocks computed as grouped dense products (gathered panels, one
+    DMMA product per group, scattered into the C blocks) agree with one
+    product per C block and pair, in assign and add mode."""
+    A, B, op, _ = _run(gctx, case, 31, 32)
+    out = []
+    for grouped in (True, False):
+        op.set_grouping(grouped)
+        C = op.make_result()
+        op.perform(C)
+        op.perform(C, 0.5)
+        gctx.synchronize()
+        out.append(C.download())
+    op.set_grouping(True)
+    scale = float(np.max(np.abs(out[1]))) if out[1].size else 1.0
+    assert float(np.max(np.abs(out[0] - out[1]))) <= TOL * max(scale, 1e-300)
