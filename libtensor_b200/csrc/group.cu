@@ -3,9 +3,9 @@
 // see crt_groups in ltg_capi.cu).
 //  - gather_cells_kernel: every operand cell (a canonical block read through
 //    the pair's orbit transform, times its sign) copied into its place in a
-//    dense group panel (rows x k, k contiguous), a warp per row and the lanes
-//    along k; non-contiguous k offsets come from a shared-memory table built
-//    once per unit;
+//    dense group panel (rows x k, k contiguous), the unit's (row, k) pairs
+//    spread over the CTA with k fastest; non-contiguous k offsets come from a
+//    shared-memory table built once per unit;
 //  - scatter_groups_kernel: the dense group result (C rows x C columns of the
 //    group) written into the C blocks of the grid (assign or add), through
 //    the same placement tables as the modular mode's recombination.
@@ -35,7 +35,6 @@ __global__ void __launch_bounds__(kGatherThreads)
 gather_cells_kernel(const DGather *__restrict__ pieces, const int4 *__restrict__ units, int32_t nunits,
                     const double *__restrict__ A, const double *__restrict__ B, double *__restrict__ buf) {
     __shared__ int32_t koff[kGatherKoff];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const int4 un = units[u];
         const DGather &P = pieces[un.x];
@@ -48,13 +47,16 @@ gather_cells_kernel(const DGather *__restrict__ pieces, const int4 *__restrict__
         }
         const double *src = (P.src ? B : A) + P.src_off;
         const double coef = (double)P.coef;
-        for (int r = un.y + warp; r < un.y + un.z; r += kGatherThreads / 32) {
-            const double *row = src + gmixed(r, P.nr, P.rext, P.rstr);
-            double *dst = buf + P.dst_off + (int64_t)r * P.ld;
-            for (int k = lane; k < P.K; k += 32) {
-                const int64_t ko = contig ? k : (tab ? koff[k] : gmixed(k, P.nk, P.kext, P.kstr));
-                dst[k] = coef * row[ko];
-            }
+        // the unit's (row, k) pairs flattened over the CTA, k fastest
+        const int n = un.z * P.K;
+        int cur = -1;
+        const double *row = src;
+        for (int i = threadIdx.x; i < n; i += kGatherThreads) {
+            const int rl = i / P.K, k = i - rl * P.K;
+            const int r = un.y + rl;
+            if (r != cur) { cur = r; row = src + gmixed(r, P.nr, P.rext, P.rstr); }
+            const int64_t ko = contig ? k : (tab ? koff[k] : gmixed(k, P.nk, P.kext, P.kstr));
+            buf[P.dst_off + (int64_t)r * P.ld + k] = coef * row[ko];
         }
     }
 }

@@ -1082,6 +1082,23 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
     std::vector<std::vector<std::pair<double, DItem>>> per_cfg(8);
     int64_t off = 0;
     PlainGroupLayout lay;
+    // one tile shape for all groups (one launch, one tail): that of the
+    // costliest group
+    int gcfg = -1;
+    {
+        int64_t o2 = 0;
+        double best = -1;
+        for (const CrtGroupHost &G : groups) {
+            if (!plain_group_layout(G, o2, lay)) { group_of.assign(cbt.size(), -1); return; }
+            const double w = (double)lay.rows * lay.cols * lay.kt;
+            if (w > best) {
+                best = w;
+                gcfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(lay.rows, lay.cols);
+                auto ov = pl->tile_override.find({lay.rows, lay.cols});
+                if (pl->forced_tile < 0 && ov != pl->tile_override.end()) gcfg = ov->second;
+            }
+        }
+    }
     for (size_t gi = 0; gi < groups.size(); gi++) {
         const CrtGroupHost &G = groups[gi];
         if (!plain_group_layout(G, off, lay)) { group_of.assign(cbt.size(), -1); return; }
@@ -1098,7 +1115,7 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
             pack_sub(cl.rows, q.nr, q.rext, q.rstr, nullptr);
             pack_sub(cl.k, q.nk, q.kext, q.kstr, nullptr);
             if (cl.rows.total() != nrow || cl.k.total() != K) throw error(kErrState, "grouped cell extents");
-            const int32_t ru = (int32_t)std::max<int64_t>(8, std::min<int64_t>(256, 4096 / std::max<int64_t>(1, K)));
+            const int32_t ru = (int32_t)std::max<int64_t>(1, std::min<int64_t>(1024, 4096 / std::max<int64_t>(1, K)));
             for (int32_t r0 = 0; r0 < q.rows; r0 += ru)
                 units.push_back(make_int4((int32_t)pieces.size(), r0, std::min(ru, q.rows - r0), 0));
             pieces.push_back(q);
@@ -1131,9 +1148,7 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
         for (int i = 1; i < kDevMaxSub; i++) { b.mext[i] = 1; b.next[i] = 1; }
         b.t_begin = (int32_t)dt.size(); b.t_end = b.t_begin + 1;
         dt.push_back(t);
-        int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(lay.rows, lay.cols);
-        auto ov = pl->tile_override.find({lay.rows, lay.cols});
-        if (pl->forced_tile < 0 && ov != pl->tile_override.end()) cfg = ov->second;
+        const int cfg = gcfg;
         const int bm = tile_cfg_bm(cfg), bn = tile_cfg_bn(cfg);
         for (int64_t m0 = 0; m0 < lay.rows; m0 += bm)
             for (int64_t n0 = 0; n0 < lay.cols; n0 += bn) {
