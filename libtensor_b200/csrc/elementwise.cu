@@ -48,6 +48,12 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Waits for all of this thread's copy groups but the newest (pending = 1) or all.
+__device__ __forceinline__ void cp_async_wait_pending(bool one) {
+    if (one) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
 
 __device__ __forceinline__ void cp_async16(double *smem, const double *gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -144,13 +150,16 @@ __device__ __forceinline__ void load_tile_terms(const UnitDesc<NT> &sd, const do
     }
 }
 
-// Copies every term's tile into shared memory, each along its own contiguous
-// direction (columns for layout 0, rows for layout 1; 16-byte copies where
-// the term allows), so that all loads of the tile are in flight at once.
-// Offsets inside a tile fit 32 bits (a block holds < 2^31 elements).
+// Issues the copies of every term's tile into shared memory, each along its
+// own contiguous direction (columns for layout 0, rows for layout 1; 16-byte
+// copies where the term allows), so that all loads of the tile are in flight
+// at once.  Offsets inside a tile fit 32 bits (a block holds < 2^31 elements).
 template<int NT, int THREADS>
-__device__ __forceinline__ void stage_tile(int nt, const TileTerms<NT> &tt, const int64_t (&sbase)[NT],
+__device__ __forceinline__ void issue_tile(int nt, const TileTerms<NT> &tt, const int64_t (&sbase)[NT],
                                            int b0, int na, int nb, double *tiles) {
+    // each thread keeps one position along the copied direction and walks
+    // the other by pointer increments (threads beyond a whole number of
+    // lines stay idle)
 #pragma unroll
     for (int t = 0; t < NT; t++) {
         if (t >= nt) break;
@@ -159,43 +168,41 @@ __device__ __forceinline__ void stage_tile(int nt, const TileTerms<NT> &tt, cons
         const int sq = tt.sq[t], sb = tt.sb[t], ld = tt.ld[t];
         if (tt.mode[t] == 0) {
             if (tt.vec[t]) {
-                const int ncp = nb >> 1, nel = na * ncp;
-                const int da = THREADS / ncp, dc = THREADS - da * ncp;
-                int a = threadIdx.x / ncp, c = threadIdx.x - a * ncp;
-                for (int i = threadIdx.x; i < nel; i += THREADS) {
-                    cp_async16(T + a * ld + 2 * c, src + (a * sq + 2 * c));
-                    a += da; c += dc;
-                    if (c >= ncp) { c -= ncp; a++; }
+                const int ncp = nb >> 1, da = THREADS / ncp;
+                const int a0 = threadIdx.x / ncp, c = threadIdx.x - a0 * ncp;
+                if (a0 < da) {
+                    double *d = T + a0 * ld + 2 * c;
+                    const double *g = src + (int64_t)a0 * sq + 2 * c;
+                    for (int a = a0; a < na; a += da, d += da * ld, g += (int64_t)da * sq) cp_async16(d, g);
                 }
             } else {
-                const int nel = na * nb;
-                const int da = THREADS / nb, dc = THREADS - da * nb;
-                int a = threadIdx.x / nb, c = threadIdx.x - a * nb;
-                for (int i = threadIdx.x; i < nel; i += THREADS) {
-                    cp_async8(T + a * ld + c, src + (a * sq + c * sb));
-                    a += da; c += dc;
-                    if (c >= nb) { c -= nb; a++; }
+                const int da = THREADS / nb;
+                const int a0 = threadIdx.x / nb, c = threadIdx.x - a0 * nb;
+                if (a0 < da) {
+                    double *d = T + a0 * ld + c;
+                    const double *g = src + (int64_t)a0 * sq + (int64_t)c * sb;
+                    for (int a = a0; a < na; a += da, d += da * ld, g += (int64_t)da * sq) cp_async8(d, g);
                 }
             }
         } else {
-            const int nel = na * nb;
-            const int dc = THREADS / na, da = THREADS - dc * na;
-            int c = threadIdx.x / na, a = threadIdx.x - c * na;
-            for (int i = threadIdx.x; i < nel; i += THREADS) {
-                cp_async8(T + c * ld + a, src + (a * sq + c * sb));
-                c += dc; a += da;
-                if (a >= na) { a -= na; c++; }
+            const int dc = THREADS / na;
+            const int c0 = threadIdx.x / na, a = threadIdx.x - c0 * na;
+            if (c0 < dc) {
+                double *d = T + c0 * ld + a;
+                const double *g = src + (int64_t)a * sq + (int64_t)c0 * sb;
+                for (int c = c0; c < nb; c += dc, d += dc * ld, g += (int64_t)dc * sb) cp_async8(d, g);
             }
         }
     }
-    cp_async_wait_all();
-    __syncthreads();
 }
 
+// One tile of the unit: destination and source bases, first column, extents.
 template<int NT>
-__device__ __forceinline__ double tile_at(const double *tiles, const TileTerms<NT> &tt, int t, int a, int c) {
-    return tiles[tt.off[t] + (tt.mode[t] == 0 ? a * tt.ld[t] + c : c * tt.ld[t] + a)];
-}
+struct TileGeo {
+    int64_t db, sbase[NT];
+    int b0, na, nb;
+};
+
 
 // Copy / add: dst = sum_t c_t src_t  or  dst += beta * sum_t c_t src_t, terms
 // summed in their order.
@@ -300,15 +307,21 @@ transfer_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
 // term's tile is staged through shared memory, then combined in term order
 // and written along the destination's columns.
 constexpr int kTiledThreads = 512;
+// Dynamic shared memory of a double-buffered tiled CTA: two CTAs of 512
+// threads share an SM, so tiles are double-buffered only while both CTAs'
+// sets fit; larger tiles run single-buffered and overlap across the CTAs.
+constexpr size_t kTileSmemLimit = 110 * 1024;
 
 template<int NT>
-__global__ void __launch_bounds__(kTiledThreads)
+__global__ void __launch_bounds__(kTiledThreads, NT <= 4 ? 2 : 1)
 transfer_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
                       const DUnit *__restrict__ units, int32_t nunits,
                       const double *const *__restrict__ srcs, double *__restrict__ dst,
-                      int32_t accumulate, double beta) {
+                      int32_t accumulate, double beta, int32_t stride) {
     __shared__ UnitDesc<NT> sd;
-    extern __shared__ double tiles[];             // one tile per term
+    // one tile per term; two such sets `stride` doubles apart when stride > 0,
+    // so that the next tile's copies are in flight while this one is written
+    extern __shared__ double tiles[];
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const DUnit un = units[u];
         stage_unit<NT>(jobs, terms, un.job, sd);
@@ -319,41 +332,61 @@ transfer_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ t
         double cf[NT];
 #pragma unroll
         for (int t = 0; t < NT; t++) cf[t] = t < nt ? sd.t[t].coeff : 0.0;
-        for (int64_t v = un.row_begin; v < un.row_end; v++) {
-            int64_t db, sbase[NT];
-            int b0, na, nb;
-            tile_bases<NT>(sd, (uint32_t)v, db, sbase, b0, na, nb);
-            stage_tile<NT, kTiledThreads>(nt, tt, sbase, b0, na, nb, tiles);
-            double *dtile = dst + db + b0;
-            const int nel = na * nb;
-            const int da = kTiledThreads / nb, dc = kTiledThreads - da * nb;
-            int a = threadIdx.x / nb, c = threadIdx.x - a * nb;
-            for (int i = threadIdx.x; i < nel; i += kTiledThreads) {
-                double val = 0.0;
+        TileGeo<NT> g;
+        tile_bases<NT>(sd, (uint32_t)un.row_begin, g.db, g.sbase, g.b0, g.na, g.nb);
+        issue_tile<NT, kTiledThreads>(nt, tt, g.sbase, g.b0, g.na, g.nb, tiles);
+        cp_async_commit();                                   // the first tile's copies: a group of their own
+        int i = 0;
+        for (int64_t v = un.row_begin; v < un.row_end; v++, i++) {
+            const bool next = v + 1 < un.row_end;
+            TileGeo<NT> gn;
+            if (next) tile_bases<NT>(sd, (uint32_t)(v + 1), gn.db, gn.sbase, gn.b0, gn.na, gn.nb);
+            if (stride > 0 && next) issue_tile<NT, kTiledThreads>(nt, tt, gn.sbase, gn.b0, gn.na, gn.nb, tiles + ((i + 1) & 1) * stride);
+            cp_async_commit();
+            cp_async_wait_pending(stride > 0);               // this tile's copies have landed
+            __syncthreads();
+            const double *cur = tiles + (stride > 0 ? (i & 1) * stride : 0);
+            const int b0 = g.b0, na = g.na, nb = g.nb;
+            // a fixed column per thread, rows by pointer increments
+            const int da = kTiledThreads / nb;
+            const int a0 = threadIdx.x / nb, c = threadIdx.x - a0 * nb;
+            if (a0 < da) {
+                double *d = dst + g.db + b0 + (int64_t)a0 * dq + c;
+                const double *p[NT];
+                int step[NT];
 #pragma unroll
                 for (int t = 0; t < NT; t++) {
-                    if (t >= nt) break;
-                    val += cf[t] * tile_at<NT>(tiles, tt, t, a, c);
+                    const bool m0 = tt.mode[t] == 0;
+                    p[t] = cur + tt.off[t] + (m0 ? a0 * tt.ld[t] + c : c * tt.ld[t] + a0);
+                    step[t] = m0 ? da * tt.ld[t] : da;
                 }
-                double *d = dtile + (a * dq + c);
-                if (accumulate) *d = *d + beta * val;
-                else *d = val;
-                a += da; c += dc;
-                if (c >= nb) { c -= nb; a++; }
+                for (int a = a0; a < na; a += da, d += (int64_t)da * dq) {
+                    double val = 0.0;
+#pragma unroll
+                    for (int t = 0; t < NT; t++) {
+                        if (t >= nt) break;
+                        val += cf[t] * *p[t];
+                        p[t] += step[t];
+                    }
+                    if (accumulate) *d = *d + beta * val;
+                    else *d = val;
+                }
             }
-            __syncthreads();
+            __syncthreads();                                 // done with this tile's buffer
+            if (stride == 0 && next) issue_tile<NT, kTiledThreads>(nt, tt, gn.sbase, gn.b0, gn.na, gn.nb, tiles);
+            g = gn;
         }
     }
 }
 
-__global__ void __launch_bounds__(kTiledThreads)
+__global__ void __launch_bounds__(kTiledThreads, 2)
 dot_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
                  const DUnit *__restrict__ units, int32_t nunits,
                  const double *__restrict__ a, const double *__restrict__ b,
-                 double *__restrict__ partials) {
+                 double *__restrict__ partials, int32_t stride) {
     __shared__ UnitDesc<2> sd;
     __shared__ double red[kTiledThreads];
-    extern __shared__ double tiles[];
+    extern __shared__ double tiles[];             // as in transfer_tiled_kernel
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const DUnit un = units[u];
         stage_unit<2>(jobs, terms, un.job, sd);
@@ -361,20 +394,41 @@ dot_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
         TileTerms<2> tt;
         load_tile_terms<2>(sd, ab, tt);
         double s = 0.0;
-        for (int64_t v = un.row_begin; v < un.row_end; v++) {
-            int64_t db, sbase[2];
-            int b0, na, nb;
-            tile_bases<2>(sd, (uint32_t)v, db, sbase, b0, na, nb);
-            stage_tile<2, kTiledThreads>(2, tt, sbase, b0, na, nb, tiles);
-            const int nel = na * nb;
-            const int da = kTiledThreads / nb, dc = kTiledThreads - da * nb;
-            int aa = threadIdx.x / nb, c = threadIdx.x - aa * nb;
-            for (int i = threadIdx.x; i < nel; i += kTiledThreads) {
-                s += tile_at<2>(tiles, tt, 0, aa, c) * tile_at<2>(tiles, tt, 1, aa, c);
-                aa += da; c += dc;
-                if (c >= nb) { c -= nb; aa++; }
+        TileGeo<2> g;
+        tile_bases<2>(sd, (uint32_t)un.row_begin, g.db, g.sbase, g.b0, g.na, g.nb);
+        issue_tile<2, kTiledThreads>(2, tt, g.sbase, g.b0, g.na, g.nb, tiles);
+        cp_async_commit();
+        int it = 0;
+        for (int64_t v = un.row_begin; v < un.row_end; v++, it++) {
+            const bool next = v + 1 < un.row_end;
+            TileGeo<2> gn;
+            if (next) tile_bases<2>(sd, (uint32_t)(v + 1), gn.db, gn.sbase, gn.b0, gn.na, gn.nb);
+            if (stride > 0 && next) issue_tile<2, kTiledThreads>(2, tt, gn.sbase, gn.b0, gn.na, gn.nb, tiles + ((it + 1) & 1) * stride);
+            cp_async_commit();
+            cp_async_wait_pending(stride > 0);
+            __syncthreads();
+            const double *cur = tiles + (stride > 0 ? (it & 1) * stride : 0);
+            const int na = g.na, nb = g.nb;
+            const int da = kTiledThreads / nb;
+            const int a0 = threadIdx.x / nb, c = threadIdx.x - a0 * nb;
+            if (a0 < da) {
+                const double *p[2];
+                int step[2];
+#pragma unroll
+                for (int t = 0; t < 2; t++) {
+                    const bool m0 = tt.mode[t] == 0;
+                    p[t] = cur + tt.off[t] + (m0 ? a0 * tt.ld[t] + c : c * tt.ld[t] + a0);
+                    step[t] = m0 ? da * tt.ld[t] : da;
+                }
+                for (int aa = a0; aa < na; aa += da) {
+                    s += *p[0] * *p[1];
+                    p[0] += step[0];
+                    p[1] += step[1];
+                }
             }
             __syncthreads();
+            if (stride == 0 && next) issue_tile<2, kTiledThreads>(2, tt, gn.sbase, gn.b0, gn.na, gn.nb, tiles);
+            g = gn;
         }
         red[threadIdx.x] = s;
         __syncthreads();
@@ -527,6 +581,14 @@ denom_kernel(double *__restrict__ arena, const int64_t *__restrict__ blk_off,
     }
 }
 
+// Doubles between the two tile sets of a double-buffered tiled launch (a
+// multiple of 16, keeping 16-byte copies aligned), or 0 when two sets of
+// `smem` bytes do not fit.
+int32_t tile_stride(size_t smem) {
+    const size_t st = (smem / sizeof(double) + 15) / 16 * 16;
+    return 2 * st * sizeof(double) <= kTileSmemLimit ? (int32_t)st : 0;
+}
+
 int grid_for(int64_t units) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -543,13 +605,16 @@ cudaError_t launch_transfer_nt(const DJob *jobs, const DTerm *terms, const DUnit
         transfer_kernel<NT><<<grid_for(nrow), kThreads, 0, s>>>(jobs, terms, units, nrow, srcs, dst,
                                                                 accumulate, beta);
     if (ntiled > 0) {
-        if (smem > 48 * 1024) {
+        // two tile sets when they fit (double buffering), else one
+        const int32_t stride = tile_stride(smem);
+        const size_t bytes = stride > 0 ? 2 * (size_t)stride * sizeof(double) : smem;
+        if (bytes > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(transfer_tiled_kernel<NT>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
             if (e != cudaSuccess) return e;
         }
-        transfer_tiled_kernel<NT><<<grid_for(ntiled), kTiledThreads, smem, s>>>(
-            jobs, terms, units + nrow, ntiled, srcs, dst, accumulate, beta);
+        transfer_tiled_kernel<NT><<<grid_for(ntiled), kTiledThreads, bytes, s>>>(
+            jobs, terms, units + nrow, ntiled, srcs, dst, accumulate, beta, stride);
     }
     return cudaGetLastError();
 }
@@ -577,12 +642,14 @@ cudaError_t launch_dot(const DJob *jobs, const DTerm *terms, const DUnit *units,
     if (nrow > 0) dot_kernel<<<grid_for(nrow), kThreads, 0, s>>>(jobs, terms, units, nrow, a, b, partials);
     if (ntiled > 0) {
         const size_t smem = (size_t)tile_bytes;
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(dot_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const int32_t stride = tile_stride(smem);
+        const size_t bytes = stride > 0 ? 2 * (size_t)stride * sizeof(double) : smem;
+        if (bytes > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(dot_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
             if (e != cudaSuccess) return e;
         }
-        dot_tiled_kernel<<<grid_for(ntiled), kTiledThreads, smem, s>>>(jobs, terms, units + nrow, ntiled, a, b,
-                                                                          partials + nrow);
+        dot_tiled_kernel<<<grid_for(ntiled), kTiledThreads, bytes, s>>>(jobs, terms, units + nrow, ntiled, a, b,
+                                                                          partials + nrow, stride);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
