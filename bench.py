@@ -44,6 +44,24 @@ MODES = {"plain": 0, "ozaki-bf16": 1, "ozaki-fp8": 2, "ozaki-int8": 3, "ozaki-cr
 FP64_NOMINAL = 40.0
 
 
+def max_over_ranks(values, device, world):
+    """Per-rank times -> their maximum over all ranks (every rank gets it).
+    Replicas run independently; the job's time is that of the slowest rank."""
+    if world <= 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def replica_rate(work_per_rank, ms, world):
+    """Whole-job rate of `world` replicas that each did `work_per_rank` in at
+    most `ms` milliseconds (units of work per second)."""
+    return world * work_per_rank / (ms * 1e-3)
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -329,17 +347,10 @@ def ltg_arm(args):
             op.perform(C, mode=0)
         p1.record(stream)
         barrier()
-        pms = p0.elapsed_time(p1) / args.steps
-        if world > 1:
-            t = torch.tensor([pms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            pms = float(t.item())
-        plain = {"value": world * flops / (pms * 1e-3) / 1e12, "unit": "TFLOP/s", "ms_per_step": pms}
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * flops / (ms * 1e-3) / 1e12
+        pms = max_over_ranks([p0.elapsed_time(p1) / args.steps], dev, world)[0]
+        plain = {"value": replica_rate(flops, pms, world) / 1e12, "unit": "TFLOP/s", "ms_per_step": pms}
+    ms = max_over_ranks([ms], dev, world)[0]
+    value = replica_rate(flops, ms, world) / 1e12
 
     # ---- end-to-end through the C ABI with pinned host buffers
     e2e = None
@@ -362,12 +373,8 @@ def ltg_arm(args):
             C.download_async(hc.data_ptr())
         f1.record(stream)
         barrier()
-        ems = f0.elapsed_time(f1) / args.steps
-        if world > 1:
-            t = torch.tensor([ems], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": world * flops / (ems * 1e-3) / 1e12, "unit": "TFLOP/s",
+        ems = max_over_ranks([f0.elapsed_time(f1) / args.steps], dev, world)[0]
+        e2e = {"value": replica_rate(flops, ems, world) / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": 8 * (A.nelems + B.nelems), "d2h_bytes_per_step": 8 * C.nelems,
                "ms_per_step": ems}
         del ha, hb, hc
@@ -585,12 +592,8 @@ def transfer_arm(args):
     launches = ctx.launch_count() - n0
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    gbs = world * w["bytes"] / (ms * 1e-3) / 1e9
+    ms = max_over_ranks([ms], dev, world)[0]
+    gbs = replica_rate(w["bytes"], ms, world) / 1e9
     kname = "dot" if args.workload.startswith("dot") else "transfer"
     kms, kn = kt.get(kname, (0.0, 0))
     peak, peak_src = hbm_peak()
@@ -624,10 +627,10 @@ def transfer_arm(args):
         f1.record(stream)
         ctx.synchronize()
         torch.cuda.synchronize()
-        ems = f0.elapsed_time(f1) / args.steps
+        ems = max_over_ranks([f0.elapsed_time(f1) / args.steps], dev, world)[0]
         h2d = sum(8 * t.nelems for t in w["srcs"])
         d2h = 8 * w["dst"].nelems if w["dst"] else 8
-        e2e = {"value": world * w["bytes"] / (ems * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+        e2e = {"value": replica_rate(w["bytes"], ems, world) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": ems}
     if world > 1:
         import torch.distributed as dist
@@ -759,11 +762,7 @@ def ccd_arm(args):
     ctx.synchronize()
     torch.cuda.synchronize()
     ems = f0.elapsed_time(f1) / args.steps
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms, ems], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ems = float(t[0].item()), float(t[1].item())
+    ms, ems = max_over_ranks([ms, ems], dev, world)
     flops = it.flops
     it.close()
     if world > 1:
@@ -774,7 +773,7 @@ def ccd_arm(args):
         return
     tot = sum(v for v, _ in kt.values())
     out = {"metric": "CCD iteration (CUDA graph): contraction TFLOP/s eff. FP64",
-           "value": world * flops / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+           "value": replica_rate(flops, ms, world) / 1e12, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, symmetrised)",
            "config": {"workload": "ccd-iter: o=30 (15 per spin) v=300 (50,50,50 per spin); copy P(0,2,1,3), "
@@ -783,7 +782,7 @@ def ccd_arm(args):
                       "l2": "operands larger than L2 (no flush)"},
            "kernels_eager_iteration": {k: {"launches": n, "ms_total": v, "share": v / tot} for k, (v, n) in kt.items()},
            "energy": energy,
-           "e2e": {"value": world * flops / (ems * 1e-3) / 1e12, "unit": "TFLOP/s",
+           "e2e": {"value": replica_rate(flops, ems, world) / 1e12, "unit": "TFLOP/s",
                    "h2d_bytes_per_step": 8 * nt, "d2h_bytes_per_step": 8, "ms_per_step": ems},
            "gpu_launches": per_iter * args.steps, "clocks": clk, "cpu_baseline": None, "roofline": None}
     print(json.dumps(out))
