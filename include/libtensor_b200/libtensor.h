@@ -13,7 +13,11 @@
  *   contraction2 (libtensor/core/contraction2.h:48),
  *   btod_contract2 (libtensor/block_tensor/btod_contract2.h:29),
  *   btod_copy (btod_copy.h:38), btod_add (btod_add.h:38),
- *   btod_dotprod (btod_dotprod.h:35).
+ *   btod_dotprod (btod_dotprod.h:35),
+ *   and the letter interface over them (libtensor/expr/iface/letter.h,
+ *   label.h, expr_rhs.h; operators/contract.h, plus_minus.h,
+ *   multiply_divide.h, dot_product.h): letter, label, operator|, btensor,
+ *   t(i|j|a|b) = expression, +=, -=, contract, dot_product.
  * Differences a user meets:
  *   - block data lives in GPU memory; blocks are read and written with
  *     block_tensor_ctrl::get_block / put_block (host buffers) instead of the
@@ -30,6 +34,7 @@
 #ifndef LIBTENSOR_B200_LIBTENSOR_H
 #define LIBTENSOR_B200_LIBTENSOR_H
 
+#include <array>
 #include <cstddef>
 #include <cstdint>
 #include <map>
@@ -173,6 +178,16 @@ class permutation {
     size_t m_p[N == 0 ? 1 : N];
 public:
     permutation() { for (size_t i = 0; i < N; i++) m_p[i] = i; }
+    // from the sequence p[0..N) (a permutation of 0..N-1)
+    explicit permutation(const std::vector<size_t> &p) {
+        if (p.size() != N) throw bad_parameter("permutation: wrong length");
+        std::vector<char> seen(N, 0);
+        for (size_t i = 0; i < N; i++) {
+            if (p[i] >= N || seen[p[i]]) throw bad_parameter("permutation: not a permutation");
+            seen[p[i]] = 1;
+            m_p[i] = p[i];
+        }
+    }
     permutation<N> &permute(size_t i, size_t j) {
         if (i >= N || j >= N) throw out_of_bounds("permutation::permute");
         std::swap(m_p[i], m_p[j]);
@@ -361,6 +376,8 @@ public:
 // ---------------------------------------------------------------- block tensor
 
 template<size_t N, typename T> class block_tensor_ctrl;
+template<size_t N> class label;
+template<size_t N> class labeled_btensor;
 
 template<size_t N, typename T>
 class block_tensor {
@@ -429,6 +446,8 @@ public:
         if (m_bt) ltg_bt_destroy(m_bt);
         m_bt = bt;
     }
+    // t(i|j|a|b): the tensor labelled for the letter interface (defined below)
+    template<size_t M> labeled_btensor<M> operator()(const label<M> &l);
 };
 
 template<size_t N, typename T>
@@ -665,6 +684,302 @@ public:
         return v.at(0);
     }
 };
+
+
+// ---------------------------------------------------------------- letter interface
+//
+// The expression layer libtensor users write (libtensor/expr/iface/letter.h,
+// label.h; libtensor/expr/operators/contract.h, dot_product.h, plus_minus.h,
+// multiply_divide.h):
+//     letter i, j, a, b, c, d;
+//     r(i|j|a|b) = 0.5 * contract(c|d, t(i|j|c|d), v(a|b|c|d));
+//     r(i|j|a|b) += x(i|j|a|b) - x(j|i|a|b);
+//     double e = dot_product(t(i|j|a|b), r(i|j|a|b));
+// An assignment evaluates its terms directly with the operations above: each
+// contraction term with one btod_contract2 (the first term assigns, the rest
+// add), all tensor terms together with one btod_add.  Contraction operands
+// are (scaled) tensors; the result must not appear on the right-hand side.
+
+// Letters are told apart by identity (address).
+class letter {
+public:
+    letter() { }
+    letter(const letter &) = delete;
+    letter &operator=(const letter &) = delete;
+};
+
+template<size_t N>
+class label {
+    std::array<const letter *, N> m_l;
+public:
+    label() { m_l.fill(nullptr); }
+    explicit label(const letter &l) { static_assert(N == 1, "one letter"); m_l[0] = &l; }
+    const letter &letter_at(size_t i) const { return *m_l.at(i); }
+    const letter *ptr(size_t i) const { return m_l[i]; }
+    bool contains(const letter &l) const {
+        for (size_t i = 0; i < N; i++) if (m_l[i] == &l) return true;
+        return false;
+    }
+    size_t index_of(const letter &l) const {
+        for (size_t i = 0; i < N; i++) if (m_l[i] == &l) return i;
+        throw bad_parameter("label: letter not found");
+    }
+    template<size_t M> friend class label;
+    template<size_t M> label<M + 1> append(const letter &l) const;
+    friend inline label<2> operator|(const letter &l1, const letter &l2);
+    template<size_t M> friend label<M + 1> operator|(const label<M> &e, const letter &l);
+};
+
+inline label<2> operator|(const letter &l1, const letter &l2) {
+    if (&l1 == &l2) throw bad_parameter("operator|: repeated letter");
+    label<2> r;
+    r.m_l[0] = &l1;
+    r.m_l[1] = &l2;
+    return r;
+}
+
+template<size_t N>
+label<N + 1> operator|(const label<N> &e, const letter &l) {
+    if (e.contains(l)) throw bad_parameter("operator|: repeated letter");
+    label<N + 1> r;
+    for (size_t i = 0; i < N; i++) r.m_l[i] = e.m_l[i];
+    r.m_l[N] = &l;
+    return r;
+}
+
+// btensor<N> is the block tensor of double
+template<size_t N, typename T = double>
+using btensor = block_tensor<N, T>;
+
+namespace expr_detail {
+
+// Permutation taking a tensor labelled `from` to the order of `to`:
+// result index d comes from source index perm[d].
+template<size_t N>
+permutation<N> align(const label<N> &from, const label<N> &to) {
+    std::vector<size_t> v(N);
+    for (size_t d = 0; d < N; d++) v[d] = from.index_of(to.letter_at(d));
+    return permutation<N>(v);
+}
+
+// One term of an expression of order N.
+template<size_t N>
+struct term {
+    double coeff = 1.0;
+    virtual ~term() { }
+    virtual bool uses(const void *bt) const = 0;
+    virtual term *scaled(double f) const = 0;
+    // contraction terms: evaluate into c (assign, or add d times the term)
+    virtual bool is_contraction() const = 0;
+    virtual void contract_into(block_tensor<N, double> &c, const label<N> &lc, bool add, double d) const = 0;
+};
+
+template<size_t N>
+struct tensor_term : term<N> {
+    block_tensor<N, double> *bt;
+    label<N> lab;
+    tensor_term(block_tensor<N, double> &t, const label<N> &l) : bt(&t), lab(l) { }
+    bool uses(const void *p) const override { return p == (const void *)bt; }
+    term<N> *scaled(double f) const override {
+        tensor_term *r = new tensor_term(*this);
+        r->coeff *= f;
+        return r;
+    }
+    bool is_contraction() const override { return false; }
+    void contract_into(block_tensor<N, double> &, const label<N> &, bool, double) const override {
+        throw exception("tensor term evaluated as a contraction");
+    }
+};
+
+}  // namespace expr_detail
+
+// Right-hand side of order N: a sum of (scaled) tensor and contraction terms.
+template<size_t N, typename T = double>
+class expr_rhs {
+    static_assert(sizeof(T) == 8, "expressions of double");
+public:
+    std::vector<std::shared_ptr<expr_detail::term<N> > > terms;
+    expr_rhs() { }
+    explicit expr_rhs(expr_detail::term<N> *t) { terms.emplace_back(t); }
+    // the single tensor of a (scaled) tensor expression
+    const expr_detail::tensor_term<N> &as_tensor(const char *what) const {
+        const expr_detail::tensor_term<N> *t =
+            terms.size() == 1 ? dynamic_cast<const expr_detail::tensor_term<N> *>(terms[0].get()) : nullptr;
+        if (!t) throw bad_parameter(std::string(what) + ": operands must be (scaled) tensors");
+        return *t;
+    }
+};
+
+template<size_t N>
+class labeled_btensor {
+    block_tensor<N, double> &m_bt;
+    label<N> m_label;
+    void evaluate(const expr_rhs<N> &e, bool add, double sign) {
+        for (const auto &t : e.terms)
+            if (t->uses(&m_bt)) throw bad_parameter("letter interface: the result appears on the right-hand side");
+        bool written = add;
+        for (const auto &t : e.terms)
+            if (t->is_contraction()) {
+                t->contract_into(m_bt, m_label, written, sign);
+                written = true;
+            }
+        std::unique_ptr<btod_add<N> > sum;
+        for (const auto &t : e.terms) {
+            if (t->is_contraction()) continue;
+            const expr_detail::tensor_term<N> &x = static_cast<const expr_detail::tensor_term<N> &>(*t);
+            const permutation<N> p = expr_detail::align(x.lab, m_label);
+            if (!sum) sum.reset(new btod_add<N>(*x.bt, p, x.coeff));
+            else sum->add_op(*x.bt, p, x.coeff);
+        }
+        if (sum) {
+            if (written) sum->perform(m_bt, sign);
+            else if (sign == 1.0) sum->perform(m_bt);
+            else {
+                // assignment of a negated sum: C = 0 - ... is C += -sum after zeroing
+                b200::check(ltg_bt_set_zero(m_bt.handle()));
+                sum->perform(m_bt, sign);
+            }
+        }
+    }
+public:
+    labeled_btensor(block_tensor<N, double> &bt, const label<N> &l) : m_bt(bt), m_label(l) { }
+    block_tensor<N, double> &get_btensor() const { return m_bt; }
+    const label<N> &get_label() const { return m_label; }
+    operator expr_rhs<N>() const { return expr_rhs<N>(new expr_detail::tensor_term<N>(m_bt, m_label)); }
+    labeled_btensor &operator=(const expr_rhs<N> &e) { evaluate(e, false, 1.0); return *this; }
+    labeled_btensor &operator=(const labeled_btensor &o) { evaluate(expr_rhs<N>(o), false, 1.0); return *this; }
+    labeled_btensor &operator+=(const expr_rhs<N> &e) { evaluate(e, true, 1.0); return *this; }
+    labeled_btensor &operator-=(const expr_rhs<N> &e) { evaluate(e, true, -1.0); return *this; }
+};
+
+template<size_t N, typename T>
+template<size_t M>
+labeled_btensor<M> block_tensor<N, T>::operator()(const label<M> &l) {
+    static_assert(M == N, "a label needs one letter per tensor index");
+    return labeled_btensor<M>(*this, l);
+}
+
+// sums and scalar multiples
+template<size_t N>
+expr_rhs<N> operator+(const expr_rhs<N> &a, const expr_rhs<N> &b) {
+    expr_rhs<N> r(a);
+    r.terms.insert(r.terms.end(), b.terms.begin(), b.terms.end());
+    return r;
+}
+template<size_t N>
+expr_rhs<N> operator*(double f, const expr_rhs<N> &a) {
+    expr_rhs<N> r;
+    for (const auto &t : a.terms) r.terms.emplace_back(t->scaled(f));
+    return r;
+}
+template<size_t N> expr_rhs<N> operator*(const expr_rhs<N> &a, double f) { return f * a; }
+template<size_t N> expr_rhs<N> operator-(const expr_rhs<N> &a) { return -1.0 * a; }
+template<size_t N> expr_rhs<N> operator-(const expr_rhs<N> &a, const expr_rhs<N> &b) { return a + (-1.0 * b); }
+template<size_t N> expr_rhs<N> operator+(const labeled_btensor<N> &a, const labeled_btensor<N> &b) { return expr_rhs<N>(a) + expr_rhs<N>(b); }
+template<size_t N> expr_rhs<N> operator-(const labeled_btensor<N> &a, const labeled_btensor<N> &b) { return expr_rhs<N>(a) - expr_rhs<N>(b); }
+template<size_t N> expr_rhs<N> operator+(const expr_rhs<N> &a, const labeled_btensor<N> &b) { return a + expr_rhs<N>(b); }
+template<size_t N> expr_rhs<N> operator-(const expr_rhs<N> &a, const labeled_btensor<N> &b) { return a - expr_rhs<N>(b); }
+template<size_t N> expr_rhs<N> operator+(const labeled_btensor<N> &a, const expr_rhs<N> &b) { return expr_rhs<N>(a) + b; }
+template<size_t N> expr_rhs<N> operator-(const labeled_btensor<N> &a, const expr_rhs<N> &b) { return expr_rhs<N>(a) - b; }
+template<size_t N> expr_rhs<N> operator*(double f, const labeled_btensor<N> &a) { return f * expr_rhs<N>(a); }
+template<size_t N> expr_rhs<N> operator*(const labeled_btensor<N> &a, double f) { return f * expr_rhs<N>(a); }
+template<size_t N> expr_rhs<N> operator-(const labeled_btensor<N> &a) { return -1.0 * expr_rhs<N>(a); }
+
+namespace b200 {
+// Arithmetic of the letter interface's contractions (ltg.h modes; default
+// LTG_MODE_PLAIN_FP64, the FP64 drop-in path).
+struct expr_precision { int32_t mode = LTG_MODE_PLAIN_FP64, nslices = 0; };
+inline expr_precision &letter_precision() { static expr_precision p; return p; }
+inline void set_letter_precision(int32_t mode, int32_t nslices) {
+    letter_precision().mode = mode;
+    letter_precision().nslices = nslices;
+}
+}  // namespace b200
+
+namespace expr_detail {
+
+// contraction of A (order NA) and B (order NB) over K letters
+template<size_t NA, size_t NB, size_t K>
+struct contract_term : term<NA + NB - 2 * K> {
+    static constexpr size_t NC = NA + NB - 2 * K;
+    block_tensor<NA, double> *a;
+    block_tensor<NB, double> *b;
+    label<NA> la;
+    label<NB> lb;
+    label<K> lk;
+    contract_term(const tensor_term<NA> &x, const tensor_term<NB> &y, const label<K> &k)
+        : a(x.bt), b(y.bt), la(x.lab), lb(y.lab), lk(k) {
+        this->coeff = x.coeff * y.coeff;
+        for (size_t i = 0; i < K; i++)
+            if (!la.contains(lk.letter_at(i)) || !lb.contains(lk.letter_at(i)))
+                throw bad_parameter("contract: a contracted letter is missing from an operand");
+    }
+    bool uses(const void *p) const override { return p == (const void *)a || p == (const void *)b; }
+    term<NC> *scaled(double f) const override {
+        contract_term *r = new contract_term(*this);
+        r->coeff *= f;
+        return r;
+    }
+    bool is_contraction() const override { return true; }
+    void contract_into(block_tensor<NC, double> &c, const label<NC> &lc, bool add, double d) const override {
+        // natural result order: A's free letters, then B's (contraction2)
+        std::vector<const letter *> nat;
+        for (size_t i = 0; i < NA; i++) if (!lk.contains(la.letter_at(i))) nat.push_back(la.ptr(i));
+        for (size_t i = 0; i < NB; i++) if (!lk.contains(lb.letter_at(i))) nat.push_back(lb.ptr(i));
+        if (nat.size() != NC) throw bad_parameter("contract: uncontracted letters do not match the result");
+        std::vector<size_t> pc(NC);
+        for (size_t dd = 0; dd < NC; dd++) {
+            size_t k = NC;
+            for (size_t q = 0; q < NC; q++) if (nat[q] == lc.ptr(dd)) k = q;
+            if (k == NC) throw bad_parameter("contract: result letter not produced by the contraction");
+            pc[dd] = k;
+        }
+        contraction2<NA - K, NB - K, K> contr{permutation<NC>(pc)};
+        for (size_t i = 0; i < K; i++) contr.contract(la.index_of(lk.letter_at(i)), lb.index_of(lk.letter_at(i)));
+        btod_contract2<NA - K, NB - K, K> op(contr, *a, 1.0, *b, 1.0, this->coeff);
+        op.set_split_precision(b200::letter_precision().mode, b200::letter_precision().nslices);
+        if (add) op.perform(c, d);
+        else if (d == 1.0) op.perform(c);
+        else {
+            op.perform(c);
+            b200::check(ltg_scale(c.handle(), d));
+        }
+    }
+};
+
+}  // namespace expr_detail
+
+// contract(letters, A(...), B(...)) (libtensor/expr/operators/contract.h)
+template<size_t K, size_t NA, size_t NB>
+expr_rhs<NA + NB - 2 * K> contract(const label<K> &lk, const expr_rhs<NA> &a, const expr_rhs<NB> &b) {
+    static_assert(K >= 1 && K <= NA && K <= NB && NA + NB > 2 * K, "contraction orders");
+    return expr_rhs<NA + NB - 2 * K>(new expr_detail::contract_term<NA, NB, K>(a.as_tensor("contract"),
+                                                                               b.as_tensor("contract"), lk));
+}
+template<size_t NA, size_t NB>
+expr_rhs<NA + NB - 2> contract(const letter &l, const expr_rhs<NA> &a, const expr_rhs<NB> &b) {
+    return contract(label<1>(l), a, b);
+}
+template<size_t K, size_t NA, size_t NB>
+expr_rhs<NA + NB - 2 * K> contract(const label<K> &lk, const labeled_btensor<NA> &a, const labeled_btensor<NB> &b) {
+    return contract(lk, expr_rhs<NA>(a), expr_rhs<NB>(b));
+}
+template<size_t NA, size_t NB>
+expr_rhs<NA + NB - 2> contract(const letter &l, const labeled_btensor<NA> &a, const labeled_btensor<NB> &b) {
+    return contract(label<1>(l), expr_rhs<NA>(a), expr_rhs<NB>(b));
+}
+
+// dot_product(A(...), B(...)) (libtensor/expr/operators/dot_product.h)
+template<size_t N>
+double dot_product(const expr_rhs<N> &a, const expr_rhs<N> &b) {
+    const expr_detail::tensor_term<N> &x = a.as_tensor("dot_product"), &y = b.as_tensor("dot_product");
+    return x.coeff * y.coeff *
+           btod_dotprod<N>(*x.bt, permutation<N>(), *y.bt, expr_detail::align(y.lab, x.lab)).calculate();
+}
+template<size_t N>
+double dot_product(const labeled_btensor<N> &a, const labeled_btensor<N> &b) {
+    return dot_product(expr_rhs<N>(a), expr_rhs<N>(b));
+}
 
 }  // namespace libtensor
 

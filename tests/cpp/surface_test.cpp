@@ -7,6 +7,8 @@
 //   surface_test schedule        host only: prints the non-zero C blocks
 //   surface_test compute FILE    on GPU 0: seeded inputs, contraction, copy,
 //                                add and dot products; writes the results to FILE
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -65,6 +67,31 @@ block_index_space<4> make_bis(size_t d0, size_t d2, const std::vector<size_t> &s
     return bis;
 }
 
+block_index_space<2> make_bis2(size_t d, const std::vector<size_t> &s) {
+    index<2> i1;
+    i1[0] = d - 1; i1[1] = d - 1;
+    block_index_space<2> bis(dimensions<2>(index_range<2>(index<2>(), i1)));
+    mask<2> m;
+    m[0] = m[1] = true;
+    split_spin(bis, m, s);
+    return bis;
+}
+
+// largest |x - f y| over the canonical blocks of x (same index space)
+template<size_t N>
+double max_diff(block_tensor<N, double> &x, block_tensor<N, double> &y, double f, const block_index_space<N> &bis) {
+    block_tensor_ctrl<N, double> cx(x), cy(y);
+    double m = 0.0;
+    for (const index<N> &b : cx.req_canonical_blocks()) {
+        const dimensions<N> d = bis.get_block_dims(b);
+        std::vector<double> u(d.get_size()), w(d.get_size());
+        cx.get_block(b, u.data());
+        cy.get_block(b, w.data());
+        for (size_t k = 0; k < u.size(); k++) m = std::max(m, std::fabs(u[k] - f * w[k]));
+    }
+    return m;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -114,6 +141,37 @@ int main(int argc, char **argv) {
         const double dot_ts = btod_dotprod<4>(t, s).calculate();
         const double dot_pp = btod_dotprod<4>(tp, tp).calculate();
 
+        // the letter interface: the same operations written as expressions,
+        // against the operations written out
+        letter i, j, a, b, c1, d1;
+        block_tensor<4, double> rl(bis_r), ra(bis_r);
+        rl(i|j|a|b) = 0.5 * contract(c1|d1, t(i|j|c1|d1), v(a|b|c1|d1));
+        add_symmetry(ra, bis_r);
+        ra(i|j|a|b) = r(i|j|a|b) - r(j|i|a|b);                // = 2 r (r is antisymmetric in i, j)
+        const double dl_tt = dot_product(t(i|j|a|b), t(i|j|a|b));
+        const double dl_tp = dot_product(t(i|j|a|b), t(j|i|a|b));   // = -<t,t>
+        block_index_space<2> bis_f = make_bis2(40, vir);
+        block_tensor<2, double> fl(bis_f), fe(bis_f);
+        fl(a|b) = contract(i|j|c1, t(i|j|a|c1), t(i|j|b|c1));
+        contraction2<1, 1, 3> c3;
+        c3.contract(0, 0);
+        c3.contract(1, 1);
+        c3.contract(3, 3);
+        btod_contract2<1, 1, 3>(c3, t, t).perform(fe);
+        block_tensor<4, double> gl(bis_r), ge(bis_r);
+        gl(i|j|a|b) = contract(c1, t(i|j|a|c1), fl(c1|b));
+        contraction2<3, 1, 1> c1c;
+        c1c.contract(3, 0);
+        btod_contract2<3, 1, 1>(c1c, t, fe).perform(ge);
+        block_tensor<4, double> hl(bis_r);
+        add_symmetry(hl, bis_r);
+        hl(i|j|a|b) = r(i|j|a|b);
+        hl(i|j|a|b) -= 0.5 * r(i|j|a|b);                      // = r / 2
+        const double diffs[] = {max_diff(rl, r, 1.0, bis_r), max_diff(ra, r, 2.0, bis_r),
+                                std::fabs(dl_tt - dot_tt), std::fabs(dl_tp + dot_tt),
+                                max_diff(fl, fe, 1.0, bis_f), max_diff(gl, ge, 1.0, bis_r),
+                                max_diff(hl, r, 0.5, bis_r)};
+
         // the contraction's non-zero blocks in index order, then the dot products
         FILE *f = std::fopen(argv[2], "wb");
         if (!f) throw bad_parameter("cannot open output file");
@@ -128,6 +186,8 @@ int main(int argc, char **argv) {
             for (double x : data) std::fprintf(f, "%.17g\n", x);
         }
         std::fprintf(f, "%.17g %.17g %.17g\n", dot_tt, dot_ts, dot_pp);
+        for (double x : diffs) std::fprintf(f, "%.17g ", x);
+        std::fprintf(f, "\n");
         std::fclose(f);
         std::printf("ok %zu blocks, flops %.6g\n", op.get_schedule().size(), op.get_flops());
     } catch (const libtensor::exception &e) {
