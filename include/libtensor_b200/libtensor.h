@@ -716,6 +716,7 @@ public:
     explicit label(const letter &l) { static_assert(N == 1, "one letter"); m_l[0] = &l; }
     const letter &letter_at(size_t i) const { return *m_l.at(i); }
     const letter *ptr(size_t i) const { return m_l[i]; }
+    void set(size_t i, const letter *l) { m_l.at(i) = l; }
     bool contains(const letter &l) const {
         for (size_t i = 0; i < N; i++) if (m_l[i] == &l) return true;
         return false;
@@ -762,6 +763,25 @@ permutation<N> align(const label<N> &from, const label<N> &to) {
     return permutation<N>(v);
 }
 
+// Letter pairs exchanged by a (anti)symmetrizer.
+struct letter_swap {
+    std::vector<std::pair<const letter *, const letter *> > pairs;
+    const letter *map(const letter *l) const {
+        for (const auto &p : pairs) {
+            if (l == p.first) return p.second;
+            if (l == p.second) return p.first;
+        }
+        return l;
+    }
+};
+
+template<size_t N>
+label<N> relabel(const label<N> &l, const letter_swap &sw) {
+    label<N> r = l;
+    for (size_t i = 0; i < N; i++) r.set(i, sw.map(l.ptr(i)));
+    return r;
+}
+
 // One term of an expression of order N.
 template<size_t N>
 struct term {
@@ -769,6 +789,8 @@ struct term {
     virtual ~term() { }
     virtual bool uses(const void *bt) const = 0;
     virtual term *scaled(double f) const = 0;
+    // the term with the letters of sw exchanged (the permuted term P E)
+    virtual term *swapped(const letter_swap &sw) const = 0;
     // contraction terms: evaluate into c (assign, or add d times the term)
     virtual bool is_contraction() const = 0;
     virtual void contract_into(block_tensor<N, double> &c, const label<N> &lc, bool add, double d) const = 0;
@@ -783,6 +805,11 @@ struct tensor_term : term<N> {
     term<N> *scaled(double f) const override {
         tensor_term *r = new tensor_term(*this);
         r->coeff *= f;
+        return r;
+    }
+    term<N> *swapped(const letter_swap &sw) const override {
+        tensor_term *r = new tensor_term(*this);
+        r->lab = relabel(lab, sw);
         return r;
     }
     bool is_contraction() const override { return false; }
@@ -810,27 +837,97 @@ public:
     }
 };
 
+namespace expr_detail {
+
+// E + sign P E for the letter exchange P: holds E (evaluated with the
+// target's letters; contraction terms of E once, into a temporary)
+template<size_t N>
+struct symm_term : term<N> {
+    expr_rhs<N> sub;
+    letter_swap sw;
+    double sign;
+    symm_term(const expr_rhs<N> &e, const letter_swap &s, double sg) : sub(e), sw(s), sign(sg) { }
+    bool uses(const void *p) const override {
+        for (const auto &t : sub.terms) if (t->uses(p)) return true;
+        return false;
+    }
+    term<N> *scaled(double f) const override {
+        symm_term *r = new symm_term(*this);
+        r->coeff *= f;
+        return r;
+    }
+    term<N> *swapped(const letter_swap &s2) const override {
+        expr_rhs<N> e;
+        for (const auto &t : sub.terms) e.terms.emplace_back(t->swapped(s2));
+        letter_swap s = sw;
+        for (auto &p : s.pairs) p = std::make_pair(s2.map(p.first), s2.map(p.second));
+        symm_term *r = new symm_term(e, s, sign);
+        r->coeff = this->coeff;
+        return r;
+    }
+    bool is_contraction() const override { return false; }
+    void contract_into(block_tensor<N, double> &, const label<N> &, bool, double) const override {
+        throw exception("symmetrizer evaluated as a contraction");
+    }
+};
+
+}  // namespace expr_detail
+
 template<size_t N>
 class labeled_btensor {
     block_tensor<N, double> &m_bt;
     label<N> m_label;
+    // The terms as contractions into the result and a flat list of (scaled)
+    // tensor terms; symmetrizers are expanded, their contraction terms
+    // evaluated once into temporaries kept in `temps`.
+    void flatten(const expr_rhs<N> &e, double f, std::vector<std::shared_ptr<expr_detail::term<N> > > &contr,
+                 std::vector<expr_detail::tensor_term<N> > &tens,
+                 std::vector<std::unique_ptr<block_tensor<N, double> > > &temps) {
+        for (const auto &t : e.terms) {
+            if (t->is_contraction()) { contr.emplace_back(t->scaled(f)); continue; }
+            if (const expr_detail::tensor_term<N> *x = dynamic_cast<const expr_detail::tensor_term<N> *>(t.get())) {
+                tens.push_back(*x);
+                tens.back().coeff *= f;
+                continue;
+            }
+            const expr_detail::symm_term<N> &y = dynamic_cast<const expr_detail::symm_term<N> &>(*t);
+            std::vector<std::shared_ptr<expr_detail::term<N> > > sc;
+            std::vector<expr_detail::tensor_term<N> > st;
+            flatten(y.sub, 1.0, sc, st, temps);
+            if (!sc.empty()) {
+                temps.emplace_back(new block_tensor<N, double>(m_bt.get_bis()));
+                block_tensor<N, double> &tmp = *temps.back();
+                for (size_t k = 0; k < sc.size(); k++) sc[k]->contract_into(tmp, m_label, k > 0, 1.0);
+                st.push_back(expr_detail::tensor_term<N>(tmp, m_label));
+            }
+            for (const expr_detail::tensor_term<N> &x : st) {
+                tens.push_back(x);
+                tens.back().coeff *= f * y.coeff;
+                tens.push_back(x);
+                tens.back().lab = expr_detail::relabel(x.lab, y.sw);
+                tens.back().coeff *= f * y.coeff * y.sign;
+            }
+        }
+    }
     void evaluate(const expr_rhs<N> &e, bool add, double sign) {
         for (const auto &t : e.terms)
             if (t->uses(&m_bt)) throw bad_parameter("letter interface: the result appears on the right-hand side");
+        std::vector<std::shared_ptr<expr_detail::term<N> > > contr;
+        std::vector<expr_detail::tensor_term<N> > tens;
+        std::vector<std::unique_ptr<block_tensor<N, double> > > temps;
+        flatten(e, 1.0, contr, tens, temps);
         bool written = add;
-        for (const auto &t : e.terms)
-            if (t->is_contraction()) {
-                t->contract_into(m_bt, m_label, written, sign);
-                written = true;
-            }
+        for (const auto &t : contr) {
+            t->contract_into(m_bt, m_label, written, sign);
+            written = true;
+        }
         std::unique_ptr<btod_add<N> > sum;
-        for (const auto &t : e.terms) {
-            if (t->is_contraction()) continue;
-            const expr_detail::tensor_term<N> &x = static_cast<const expr_detail::tensor_term<N> &>(*t);
+        for (const expr_detail::tensor_term<N> &x : tens) {
             const permutation<N> p = expr_detail::align(x.lab, m_label);
             if (!sum) sum.reset(new btod_add<N>(*x.bt, p, x.coeff));
             else sum->add_op(*x.bt, p, x.coeff);
         }
+        if (!sum && !written) b200::check(ltg_bt_set_zero(m_bt.handle()));
         if (sum) {
             if (written) sum->perform(m_bt, sign);
             else if (sign == 1.0) sum->perform(m_bt);
@@ -920,6 +1017,14 @@ struct contract_term : term<NA + NB - 2 * K> {
         r->coeff *= f;
         return r;
     }
+    term<NC> *swapped(const letter_swap &sw) const override {
+        for (size_t i = 0; i < K; i++)
+            if (sw.map(lk.ptr(i)) != lk.ptr(i)) throw bad_parameter("symm/asymm: a contracted letter is exchanged");
+        contract_term *r = new contract_term(*this);
+        r->la = relabel(la, sw);
+        r->lb = relabel(lb, sw);
+        return r;
+    }
     bool is_contraction() const override { return true; }
     void contract_into(block_tensor<NC, double> &c, const label<NC> &lc, bool add, double d) const override {
         // natural result order: A's free letters, then B's (contraction2)
@@ -980,6 +1085,56 @@ template<size_t N>
 double dot_product(const labeled_btensor<N> &a, const labeled_btensor<N> &b) {
     return dot_product(expr_rhs<N>(a), expr_rhs<N>(b));
 }
+
+// symm / asymm (libtensor/expr/operators/symm_asymm.h): E + P E and E - P E,
+// P exchanging the letters of l1 with those of l2 (pairwise, simultaneously)
+template<size_t N, size_t M>
+expr_rhs<N> symm(const label<M> &l1, const label<M> &l2, const expr_rhs<N> &e) {
+    expr_detail::letter_swap sw;
+    for (size_t i = 0; i < M; i++) sw.pairs.push_back(std::make_pair(l1.ptr(i), l2.ptr(i)));
+    return expr_rhs<N>(new expr_detail::symm_term<N>(e, sw, 1.0));
+}
+template<size_t N, size_t M>
+expr_rhs<N> asymm(const label<M> &l1, const label<M> &l2, const expr_rhs<N> &e) {
+    expr_detail::letter_swap sw;
+    for (size_t i = 0; i < M; i++) sw.pairs.push_back(std::make_pair(l1.ptr(i), l2.ptr(i)));
+    return expr_rhs<N>(new expr_detail::symm_term<N>(e, sw, -1.0));
+}
+template<size_t N>
+expr_rhs<N> symm(const letter &l1, const letter &l2, const expr_rhs<N> &e) { return symm(label<1>(l1), label<1>(l2), e); }
+template<size_t N>
+expr_rhs<N> asymm(const letter &l1, const letter &l2, const expr_rhs<N> &e) { return asymm(label<1>(l1), label<1>(l2), e); }
+template<size_t N, size_t M>
+expr_rhs<N> symm(const label<M> &l1, const label<M> &l2, const labeled_btensor<N> &e) { return symm(l1, l2, expr_rhs<N>(e)); }
+template<size_t N, size_t M>
+expr_rhs<N> asymm(const label<M> &l1, const label<M> &l2, const labeled_btensor<N> &e) { return asymm(l1, l2, expr_rhs<N>(e)); }
+template<size_t N>
+expr_rhs<N> symm(const letter &l1, const letter &l2, const labeled_btensor<N> &e) { return symm(l1, l2, expr_rhs<N>(e)); }
+template<size_t N>
+expr_rhs<N> asymm(const letter &l1, const letter &l2, const labeled_btensor<N> &e) { return asymm(l1, l2, expr_rhs<N>(e)); }
+
+// btod_symmetrize2 (libtensor/block_tensor/btod_symmetrize2.h:19-60) over a
+// tensor: B = A + P(A) (symm) or A - P(A), P exchanging indexes i1 and i2.
+// The reference wraps another operation; here the operand is its result.
+template<size_t N>
+class btod_symmetrize2 {
+    block_tensor<N, double> &m_a;
+    permutation<N> m_p;
+    double m_sign;
+public:
+    btod_symmetrize2(block_tensor<N, double> &bta, size_t i1, size_t i2, bool symm)
+        : m_a(bta), m_sign(symm ? 1.0 : -1.0) { m_p.permute(i1, i2); }
+    void perform(block_tensor<N, double> &btb) {
+        btod_add<N> op(m_a, 1.0);
+        op.add_op(m_a, m_p, m_sign);
+        op.perform(btb);
+    }
+    void perform(block_tensor<N, double> &btb, double d) {
+        btod_add<N> op(m_a, 1.0);
+        op.add_op(m_a, m_p, m_sign);
+        op.perform(btb, d);
+    }
+};
 
 }  // namespace libtensor
 

@@ -167,10 +167,18 @@ int main(int argc, char **argv) {
         add_symmetry(hl, bis_r);
         hl(i|j|a|b) = r(i|j|a|b);
         hl(i|j|a|b) -= 0.5 * r(i|j|a|b);                      // = r / 2
+        // symmetrizers: symm over a pair of index pairs, asymm of a contraction
+        // against btod_symmetrize2 of the contraction written out
+        block_tensor<4, double> ys(bis_r), gs(bis_r), gse(bis_r);
+        add_symmetry(ys, bis_r);
+        ys(i|j|a|b) = symm(i|a, j|b, r(i|j|a|b));             // = 2 r
+        gs(i|j|a|b) = asymm(a, b, contract(c1, t(i|j|a|c1), fl(c1|b)));
+        btod_symmetrize2<4>(ge, 2, 3, false).perform(gse);
         const double diffs[] = {max_diff(rl, r, 1.0, bis_r), max_diff(ra, r, 2.0, bis_r),
                                 std::fabs(dl_tt - dot_tt), std::fabs(dl_tp + dot_tt),
                                 max_diff(fl, fe, 1.0, bis_f), max_diff(gl, ge, 1.0, bis_r),
-                                max_diff(hl, r, 0.5, bis_r)};
+                                max_diff(hl, r, 0.5, bis_r), max_diff(ys, r, 2.0, bis_r),
+                                max_diff(gs, gse, 1.0, bis_r)};
 
         // the contraction's non-zero blocks in index order, then the dot products
         FILE *f = std::fopen(argv[2], "wb");

@@ -61,7 +61,7 @@ def test_surface_compute_matches_golden(exe, tmp_path):
     assert abs(dot_pp - 0.25 * dot_tt) <= 1e-13 * dot_tt
     # letter interface against the operations written out: the ladder, an
     # antisymmetrising difference, dot products (one permuted), K = 3 and
-    # K = 1 contractions, assignment then -=
+    # K = 1 contractions, assignment then -=, symmetrizers
     d = [float(x) for x in lines[pos + 1].split()]
     rmax = max(float(np.max(np.abs(v))) for v in gold.values())
     assert d[0] == 0.0                                  # the same plan and kernels
@@ -69,3 +69,5 @@ def test_surface_compute_matches_golden(exe, tmp_path):
     assert d[2] <= 1e-13 * dot_tt and d[3] <= 1e-13 * dot_tt
     assert d[4] == 0.0 and d[5] == 0.0
     assert d[6] <= 1e-15 * rmax
+    assert d[7] <= 1e-15 * rmax                         # symm(i|a, j|b, r) = 2 r
+    assert d[8] == 0.0                                  # asymm(a, b, contraction) = btod_symmetrize2
