@@ -556,12 +556,16 @@ class btod_contract2 {
         b200::check(ltg_contract2_create(b200::context(), (int32_t)N, (int32_t)M, (int32_t)K, permc.data(),
                                          pairs.data(), bta.handle(), btb.handle(), &m_plan));
     }
+    ltg_bt *m_adopted = nullptr;     // the result tensor the last assignment created
     void run(block_tensor<N + M, double> &btc, int32_t add, double d) {
-        if (!add) {
-            // assignment gives C the result symmetry (as the reference's perform does)
+        if (!add && !(btc.is_bound() && btc.handle() == m_adopted)) {
+            // assignment gives C the result symmetry (as the reference's perform
+            // does); repeated assignments to the same result reuse it, so
+            // that they can be captured in a graph
             ltg_bt *c = nullptr;
             b200::check(ltg_contract2_make_result(m_plan, &c));
             btc.adopt(c);
+            m_adopted = c;
         }
         b200::check(ltg_contract2(m_plan, btc.handle(), m_mode, m_nslices, m_ka, m_kb, m_kc, add, d));
     }
@@ -604,16 +608,20 @@ class btod_copy {
     block_tensor<N, double> &m_a;
     permutation<N> m_perm;
     double m_c;
+    ltg_bt *m_adopted = nullptr;     // as in btod_contract2
 public:
     btod_copy(block_tensor<N, double> &bta, double c = 1.0) : m_a(bta), m_c(c) { }
     btod_copy(block_tensor<N, double> &bta, const permutation<N> &perm, double c = 1.0)
         : m_a(bta), m_perm(perm), m_c(c) { }
     // B = c P(A): B takes the permuted space and symmetry of A
     void perform(block_tensor<N, double> &btb) {
-        ltg_bt *b = nullptr;
         const std::vector<int32_t> p = m_perm.to_vector();
-        b200::check(ltg_bt_create_permuted(m_a.handle(), p.data(), &b));
-        btb.adopt(b);
+        if (!(btb.is_bound() && btb.handle() == m_adopted)) {
+            ltg_bt *b = nullptr;
+            b200::check(ltg_bt_create_permuted(m_a.handle(), p.data(), &b));
+            btb.adopt(b);
+            m_adopted = b;
+        }
         b200::check(ltg_copy(m_a.handle(), p.data(), m_c, btb.handle(), 0, 0.0));
     }
     // B += d c P(A)
@@ -983,6 +991,28 @@ template<size_t N> expr_rhs<N> operator*(const labeled_btensor<N> &a, double f) 
 template<size_t N> expr_rhs<N> operator-(const labeled_btensor<N> &a) { return -1.0 * expr_rhs<N>(a); }
 
 namespace b200 {
+
+// CUDA graph of a sequence of operations (ltg_graph_begin/end/launch): run
+// every operation once before the capture (their plans are built then), capture
+// the sequence, then launch it as often as needed.
+class graph {
+    ltg_graph *m_g = nullptr;
+public:
+    explicit graph(ltg_graph *g) : m_g(g) { }
+    graph(graph &&o) noexcept : m_g(o.m_g) { o.m_g = nullptr; }
+    graph(const graph &) = delete;
+    graph &operator=(const graph &) = delete;
+    ~graph() { if (m_g) ltg_graph_destroy(m_g); }
+    void launch() { check(ltg_graph_launch(m_g)); }
+};
+inline void begin_capture() { check(ltg_graph_begin(context())); }
+inline graph end_capture() {
+    ltg_graph *g = nullptr;
+    check(ltg_graph_end(context(), &g));
+    return graph(g);
+}
+inline void synchronize() { check(ltg_ctx_synchronize(context())); }
+
 // Arithmetic of the letter interface's contractions (ltg.h modes; default
 // LTG_MODE_PLAIN_FP64, the FP64 drop-in path).
 struct expr_precision { int32_t mode = LTG_MODE_PLAIN_FP64, nslices = 0; };

@@ -71,3 +71,4 @@ def test_surface_compute_matches_golden(exe, tmp_path):
     assert d[6] <= 1e-15 * rmax
     assert d[7] <= 1e-15 * rmax                         # symm(i|a, j|b, r) = 2 r
     assert d[8] == 0.0                                  # asymm(a, b, contraction) = btod_symmetrize2
+    assert d[9] == 0.0                                  # graph replay = eager operations
