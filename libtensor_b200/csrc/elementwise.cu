@@ -154,9 +154,28 @@ __device__ __forceinline__ void load_tile_terms(const UnitDesc<NT> &sd, const do
 // own contiguous direction (columns for layout 0, rows for layout 1; 16-byte
 // copies where the term allows), so that all loads of the tile are in flight
 // at once.  Offsets inside a tile fit 32 bits (a block holds < 2^31 elements).
+// Per-thread positions of the tile mappings for extents (na, nb): threads
+// along the columns (da rows apart), along column pairs, or along the rows
+// (dc columns apart).  Recomputed only when a tile's extents change.
+template<int THREADS>
+struct TileMap {
+    int na = -1, nb = -1;
+    int da, a0, c;           // columns: row step, first row, column
+    int vda, va0, vc;        // column pairs
+    int dc, c0, ar;          // rows: column step, first column, row
+    __device__ __forceinline__ void update(int na_, int nb_) {
+        if (na_ == na && nb_ == nb) return;
+        na = na_; nb = nb_;
+        da = THREADS / nb; a0 = threadIdx.x / nb; c = threadIdx.x - a0 * nb;
+        const int ncp = nb >> 1 > 0 ? nb >> 1 : 1;
+        vda = THREADS / ncp; va0 = threadIdx.x / ncp; vc = threadIdx.x - va0 * ncp;
+        dc = THREADS / na; c0 = threadIdx.x / na; ar = threadIdx.x - c0 * na;
+    }
+};
+
 template<int NT, int THREADS>
 __device__ __forceinline__ void issue_tile(int nt, const TileTerms<NT> &tt, const int64_t (&sbase)[NT],
-                                           int b0, int na, int nb, double *tiles) {
+                                           int b0, int na, int nb, const TileMap<THREADS> &m, double *tiles) {
     // each thread keeps one position along the copied direction and walks
     // the other by pointer increments (threads beyond a whole number of
     // lines stay idle)
@@ -168,29 +187,23 @@ __device__ __forceinline__ void issue_tile(int nt, const TileTerms<NT> &tt, cons
         const int sq = tt.sq[t], sb = tt.sb[t], ld = tt.ld[t];
         if (tt.mode[t] == 0) {
             if (tt.vec[t]) {
-                const int ncp = nb >> 1, da = THREADS / ncp;
-                const int a0 = threadIdx.x / ncp, c = threadIdx.x - a0 * ncp;
-                if (a0 < da) {
-                    double *d = T + a0 * ld + 2 * c;
-                    const double *g = src + (int64_t)a0 * sq + 2 * c;
-                    for (int a = a0; a < na; a += da, d += da * ld, g += (int64_t)da * sq) cp_async16(d, g);
+                if (m.va0 < m.vda) {
+                    double *d = T + m.va0 * ld + 2 * m.vc;
+                    const double *g = src + (int64_t)m.va0 * sq + 2 * m.vc;
+                    for (int a = m.va0; a < na; a += m.vda, d += m.vda * ld, g += (int64_t)m.vda * sq) cp_async16(d, g);
                 }
             } else {
-                const int da = THREADS / nb;
-                const int a0 = threadIdx.x / nb, c = threadIdx.x - a0 * nb;
-                if (a0 < da) {
-                    double *d = T + a0 * ld + c;
-                    const double *g = src + (int64_t)a0 * sq + (int64_t)c * sb;
-                    for (int a = a0; a < na; a += da, d += da * ld, g += (int64_t)da * sq) cp_async8(d, g);
+                if (m.a0 < m.da) {
+                    double *d = T + m.a0 * ld + m.c;
+                    const double *g = src + (int64_t)m.a0 * sq + (int64_t)m.c * sb;
+                    for (int a = m.a0; a < na; a += m.da, d += m.da * ld, g += (int64_t)m.da * sq) cp_async8(d, g);
                 }
             }
         } else {
-            const int dc = THREADS / na;
-            const int c0 = threadIdx.x / na, a = threadIdx.x - c0 * na;
-            if (c0 < dc) {
-                double *d = T + c0 * ld + a;
-                const double *g = src + (int64_t)a * sq + (int64_t)c0 * sb;
-                for (int c = c0; c < nb; c += dc, d += dc * ld, g += (int64_t)dc * sb) cp_async8(d, g);
+            if (m.c0 < m.dc) {
+                double *d = T + m.c0 * ld + m.ar;
+                const double *g = src + (int64_t)m.ar * sq + (int64_t)m.c0 * sb;
+                for (int c = m.c0; c < nb; c += m.dc, d += m.dc * ld, g += (int64_t)m.dc * sb) cp_async8(d, g);
             }
         }
     }
@@ -312,6 +325,16 @@ constexpr int kTiledThreads = 512;
 // sets fit; larger tiles run single-buffered and overlap across the CTAs.
 constexpr size_t kTileSmemLimit = 110 * 1024;
 
+// Geometry of the unit's tiles: computed by one thread, two tiles ahead, in
+// a ring of three shared slots (current, copies in flight, next).
+template<int NT>
+__device__ __forceinline__ void geo_ahead(const UnitDesc<NT> &sd, int64_t v, int64_t end, TileGeo<NT> *ring, int slot) {
+    if (threadIdx.x == 0 && v < end) {
+        TileGeo<NT> &g = ring[slot];
+        tile_bases<NT>(sd, (uint32_t)v, g.db, g.sbase, g.b0, g.na, g.nb);
+    }
+}
+
 template<int NT>
 __global__ void __launch_bounds__(kTiledThreads, NT <= 4 ? 2 : 1)
 transfer_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
@@ -319,9 +342,11 @@ transfer_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ t
                       const double *const *__restrict__ srcs, double *__restrict__ dst,
                       int32_t accumulate, double beta, int32_t stride) {
     __shared__ UnitDesc<NT> sd;
+    __shared__ TileGeo<NT> ring[3];
     // one tile per term; two such sets `stride` doubles apart when stride > 0,
     // so that the next tile's copies are in flight while this one is written
     extern __shared__ double tiles[];
+    TileMap<kTiledThreads> tm;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const DUnit un = units[u];
         stage_unit<NT>(jobs, terms, un.job, sd);
@@ -332,24 +357,33 @@ transfer_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ t
         double cf[NT];
 #pragma unroll
         for (int t = 0; t < NT; t++) cf[t] = t < nt ? sd.t[t].coeff : 0.0;
-        TileGeo<NT> g;
-        tile_bases<NT>(sd, (uint32_t)un.row_begin, g.db, g.sbase, g.b0, g.na, g.nb);
-        issue_tile<NT, kTiledThreads>(nt, tt, g.sbase, g.b0, g.na, g.nb, tiles);
+        geo_ahead<NT>(sd, un.row_begin, un.row_end, ring, 0);
+        geo_ahead<NT>(sd, un.row_begin + 1, un.row_end, ring, 1);
+        __syncthreads();
+        {
+            const TileGeo<NT> &g0 = ring[0];
+            tm.update(g0.na, g0.nb);
+            issue_tile<NT, kTiledThreads>(nt, tt, g0.sbase, g0.b0, g0.na, g0.nb, tm, tiles);
+        }
         cp_async_commit();                                   // the first tile's copies: a group of their own
         int i = 0;
         for (int64_t v = un.row_begin; v < un.row_end; v++, i++) {
             const bool next = v + 1 < un.row_end;
-            TileGeo<NT> gn;
-            if (next) tile_bases<NT>(sd, (uint32_t)(v + 1), gn.db, gn.sbase, gn.b0, gn.na, gn.nb);
-            if (stride > 0 && next) issue_tile<NT, kTiledThreads>(nt, tt, gn.sbase, gn.b0, gn.na, gn.nb, tiles + ((i + 1) & 1) * stride);
+            const TileGeo<NT> &gn = ring[(i + 1) % 3];
+            if (stride > 0 && next) {
+                tm.update(gn.na, gn.nb);
+                issue_tile<NT, kTiledThreads>(nt, tt, gn.sbase, gn.b0, gn.na, gn.nb, tm, tiles + ((i + 1) & 1) * stride);
+            }
             cp_async_commit();
             cp_async_wait_pending(stride > 0);               // this tile's copies have landed
             __syncthreads();
+            geo_ahead<NT>(sd, v + 2, un.row_end, ring, (i + 2) % 3);
             const double *cur = tiles + (stride > 0 ? (i & 1) * stride : 0);
+            const TileGeo<NT> &g = ring[i % 3];
             const int b0 = g.b0, na = g.na, nb = g.nb;
+            tm.update(na, nb);
             // a fixed column per thread, rows by pointer increments
-            const int da = kTiledThreads / nb;
-            const int a0 = threadIdx.x / nb, c = threadIdx.x - a0 * nb;
+            const int da = tm.da, a0 = tm.a0, c = tm.c;
             if (a0 < da) {
                 double *d = dst + g.db + b0 + (int64_t)a0 * dq + c;
                 const double *p[NT];
@@ -372,9 +406,11 @@ transfer_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ t
                     else *d = val;
                 }
             }
-            __syncthreads();                                 // done with this tile's buffer
-            if (stride == 0 && next) issue_tile<NT, kTiledThreads>(nt, tt, gn.sbase, gn.b0, gn.na, gn.nb, tiles);
-            g = gn;
+            __syncthreads();                                 // done with this tile's buffer and slot
+            if (stride == 0 && next) {
+                tm.update(gn.na, gn.nb);
+                issue_tile<NT, kTiledThreads>(nt, tt, gn.sbase, gn.b0, gn.na, gn.nb, tm, tiles);
+            }
         }
     }
 }
@@ -385,8 +421,10 @@ dot_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
                  const double *__restrict__ a, const double *__restrict__ b,
                  double *__restrict__ partials, int32_t stride) {
     __shared__ UnitDesc<2> sd;
+    __shared__ TileGeo<2> ring[3];
     __shared__ double red[kTiledThreads];
     extern __shared__ double tiles[];             // as in transfer_tiled_kernel
+    TileMap<kTiledThreads> tm;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const DUnit un = units[u];
         stage_unit<2>(jobs, terms, un.job, sd);
@@ -394,23 +432,32 @@ dot_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
         TileTerms<2> tt;
         load_tile_terms<2>(sd, ab, tt);
         double s = 0.0;
-        TileGeo<2> g;
-        tile_bases<2>(sd, (uint32_t)un.row_begin, g.db, g.sbase, g.b0, g.na, g.nb);
-        issue_tile<2, kTiledThreads>(2, tt, g.sbase, g.b0, g.na, g.nb, tiles);
+        geo_ahead<2>(sd, un.row_begin, un.row_end, ring, 0);
+        geo_ahead<2>(sd, un.row_begin + 1, un.row_end, ring, 1);
+        __syncthreads();
+        {
+            const TileGeo<2> &g0 = ring[0];
+            tm.update(g0.na, g0.nb);
+            issue_tile<2, kTiledThreads>(2, tt, g0.sbase, g0.b0, g0.na, g0.nb, tm, tiles);
+        }
         cp_async_commit();
         int it = 0;
         for (int64_t v = un.row_begin; v < un.row_end; v++, it++) {
             const bool next = v + 1 < un.row_end;
-            TileGeo<2> gn;
-            if (next) tile_bases<2>(sd, (uint32_t)(v + 1), gn.db, gn.sbase, gn.b0, gn.na, gn.nb);
-            if (stride > 0 && next) issue_tile<2, kTiledThreads>(2, tt, gn.sbase, gn.b0, gn.na, gn.nb, tiles + ((it + 1) & 1) * stride);
+            const TileGeo<2> &gn = ring[(it + 1) % 3];
+            if (stride > 0 && next) {
+                tm.update(gn.na, gn.nb);
+                issue_tile<2, kTiledThreads>(2, tt, gn.sbase, gn.b0, gn.na, gn.nb, tm, tiles + ((it + 1) & 1) * stride);
+            }
             cp_async_commit();
             cp_async_wait_pending(stride > 0);
             __syncthreads();
+            geo_ahead<2>(sd, v + 2, un.row_end, ring, (it + 2) % 3);
             const double *cur = tiles + (stride > 0 ? (it & 1) * stride : 0);
-            const int na = g.na, nb = g.nb;
-            const int da = kTiledThreads / nb;
-            const int a0 = threadIdx.x / nb, c = threadIdx.x - a0 * nb;
+            const TileGeo<2> &g = ring[it % 3];
+            const int na = g.na;
+            tm.update(na, g.nb);
+            const int da = tm.da, a0 = tm.a0, c = tm.c;
             if (a0 < da) {
                 const double *p[2];
                 int step[2];
@@ -427,8 +474,10 @@ dot_tiled_kernel(const DJob *__restrict__ jobs, const DTerm *__restrict__ terms,
                 }
             }
             __syncthreads();
-            if (stride == 0 && next) issue_tile<2, kTiledThreads>(2, tt, gn.sbase, gn.b0, gn.na, gn.nb, tiles);
-            g = gn;
+            if (stride == 0 && next) {
+                tm.update(gn.na, gn.nb);
+                issue_tile<2, kTiledThreads>(2, tt, gn.sbase, gn.b0, gn.na, gn.nb, tm, tiles);
+            }
         }
         red[threadIdx.x] = s;
         __syncthreads();
