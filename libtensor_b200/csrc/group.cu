@@ -3,9 +3,9 @@
 // see crt_groups in ltg_capi.cu).
 //  - gather_cells_kernel: every operand cell (a canonical block read through
 //    the pair's orbit transform, times its sign) copied into its place in a
-//    dense group panel (rows x k, k contiguous), the unit's (row, k) pairs
-//    spread over the CTA with k fastest; non-contiguous k offsets come from a
-//    shared-memory table built once per unit;
+//    dense group panel (rows x k, k contiguous), each thread on a fixed k
+//    (its offset found once) stepping over rows; non-contiguous k offsets
+//    come from a shared-memory table built once per unit;
 //  - scatter_groups_kernel: the dense group result (C rows x C columns of the
 //    group) written into the C blocks of the grid (assign or add), through
 //    the same placement tables as the modular mode's recombination.
@@ -47,16 +47,22 @@ gather_cells_kernel(const DGather *__restrict__ pieces, const int4 *__restrict__
         }
         const double *src = (P.src ? B : A) + P.src_off;
         const double coef = (double)P.coef;
-        // the unit's (row, k) pairs flattened over the CTA, k fastest
-        const int n = un.z * P.K;
-        int cur = -1;
-        const double *row = src;
-        for (int i = threadIdx.x; i < n; i += kGatherThreads) {
-            const int rl = i / P.K, k = i - rl * P.K;
-            const int r = un.y + rl;
-            if (r != cur) { cur = r; row = src + gmixed(r, P.nr, P.rext, P.rstr); }
-            const int64_t ko = contig ? k : (tab ? koff[k] : gmixed(k, P.nk, P.kext, P.kstr));
-            buf[P.dst_off + (int64_t)r * P.ld + k] = coef * row[ko];
+        if (P.K <= kGatherThreads) {
+            // a fixed k per thread (its offset found once), rows dr apart
+            const int dr = kGatherThreads / P.K, r0 = threadIdx.x / P.K, k = threadIdx.x - r0 * P.K;
+            if (r0 < dr) {
+                const int64_t ko = contig ? k : (tab ? koff[k] : gmixed(k, P.nk, P.kext, P.kstr));
+                double *d = buf + P.dst_off + (int64_t)(un.y + r0) * P.ld + k;
+                for (int r = un.y + r0; r < un.y + un.z; r += dr, d += (int64_t)dr * P.ld)
+                    *d = coef * src[gmixed(r, P.nr, P.rext, P.rstr) + ko];
+            }
+        } else {
+            for (int r = un.y; r < un.y + un.z; r++) {
+                const double *row = src + gmixed(r, P.nr, P.rext, P.rstr);
+                double *d = buf + P.dst_off + (int64_t)r * P.ld;
+                for (int k = threadIdx.x; k < P.K; k += kGatherThreads)
+                    d[k] = coef * row[contig ? k : (tab ? koff[k] : gmixed(k, P.nk, P.kext, P.kstr))];
+            }
         }
     }
 }
