@@ -2,6 +2,7 @@
 #include "ltg_host.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <list>
 #include <map>
 #include <set>
@@ -590,41 +591,63 @@ void contract2_result_space(const Contraction &c, const BlockTensorHost &a,
 namespace {
 
 // Coalescing of pairs with identical canonical blocks and identical permuted
-// contraction (btod_contract2_clst_optimize_impl.h:11-56).
-void coalesce(const Contraction &c, std::list<Pair> &lst) {
-    auto j1 = lst.begin();
-    while (j1 != lst.end()) {
-        auto j2 = j1; ++j2;
-        bool incj1 = true;
-        while (j2 != lst.end()) {
-            if (!(j1->acia == j2->acia && j1->acib == j2->acib)) { ++j2; continue; }
-            Contraction c1 = c, c2 = c;
-            c1.permute_a(j1->tra.perm); c1.permute_b(j1->trb.perm);
-            c2.permute_a(j2->tra.perm); c2.permute_b(j2->trb.perm);
-            if (!c1.same_conn(c2)) { ++j2; continue; }
-            double d1 = j1->tra.coeff * j1->trb.coeff;
-            double d2 = j2->tra.coeff * j2->trb.coeff;
-            if (d1 + d2 == 0) {
-                j1 = lst.erase(j1);
-                if (j1 == j2) { j1 = j2 = lst.erase(j2); }
-                else { j2 = lst.erase(j2); }
-                incj1 = false;
-                break;
-            } else {
-                j1->tra.coeff = d1 + d2;
-                j1->trb.coeff = 1.0;
-                j2 = lst.erase(j2);
-            }
-        }
-        if (incj1) ++j1;
+// contraction (btod_contract2_clst_optimize_impl.h:11-56): for every pair in
+// order, the later pairs with the same canonical A and B blocks (the only ones
+// that can merge) in order; a pair with the same permuted contraction is added
+// into it (coefficient d1 + d2), and when the sum is zero both go.  The same
+// result as comparing every pair with every later one, without the quadratic
+// scan of the whole list.
+void coalesce(const Contraction &c, std::vector<Pair> &v) {
+    const size_t n = v.size();
+    if (n < 2) return;
+    std::vector<uint32_t> order(n);
+    for (size_t i = 0; i < n; i++) order[i] = (uint32_t)i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+        return v[x].acia != v[y].acia ? v[x].acia < v[y].acia : v[x].acib < v[y].acib;
+    });
+    // next later pair with the same canonical blocks
+    std::vector<int64_t> next(n, -1);
+    for (size_t q = 0; q + 1 < n; q++) {
+        const Pair &x = v[order[q]], &y = v[order[q + 1]];
+        if (x.acia == y.acia && x.acib == y.acib) next[order[q]] = order[q + 1];
     }
+    std::vector<Contraction> conn(n);
+    std::vector<char> have(n, 0), alive(n, 1);
+    auto conn_of = [&](size_t i) -> const Contraction & {
+        if (!have[i]) {
+            conn[i] = c;
+            conn[i].permute_a(v[i].tra.perm);
+            conn[i].permute_b(v[i].trb.perm);
+            have[i] = 1;
+        }
+        return conn[i];
+    };
+    for (size_t i = 0; i < n; i++) {
+        if (!alive[i] || next[i] < 0) continue;
+        for (int64_t j = next[i]; j >= 0; j = next[j]) {
+            if (!alive[j]) continue;
+            if (!conn_of(i).same_conn(conn_of((size_t)j))) continue;
+            const double d1 = v[i].tra.coeff * v[i].trb.coeff;
+            const double d2 = v[j].tra.coeff * v[j].trb.coeff;
+            if (d1 + d2 == 0) {
+                alive[i] = alive[j] = 0;
+                break;
+            }
+            v[i].tra.coeff = d1 + d2;
+            v[i].trb.coeff = 1.0;
+            alive[j] = 0;
+        }
+    }
+    size_t w = 0;
+    for (size_t i = 0; i < n; i++)
+        if (alive[i]) v[w++] = v[i];
+    v.resize(w);
 }
 
 }  // namespace
 
 void contract2_schedule(const Contraction &c, const BlockTensorHost &a,
     const BlockTensorHost &b, ContractPlan &plan, int nthreads) {
-    (void)nthreads;
     plan.contr = c;
     contract2_result_space(c, a, b, plan.bisc, plan.symc);
     OrbitTable oc;
@@ -658,44 +681,79 @@ void contract2_schedule(const Contraction &c, const BlockTensorHost &a,
     plan.clst.clear();
     plan.flops = 0;
     plan.coalesced = false;
-    int64_t ic[kMaxOrder], ia[kMaxOrder], ib[kMaxOrder], ik[kMaxOrder];
-    int64_t da[kMaxOrder], dc[kMaxOrder];
-    std::list<Pair> lst;
-    for (int64_t cabs : oc.canon_list) {
-        plan.bisc.unabs(cabs, ic);
-        for (int i = 0; i < NA; i++) { int64_t s = c.conn[NC + i]; if (s < NC) ia[i] = ic[s]; }
-        for (int j = 0; j < NB; j++) { int64_t s = c.conn[NC + NA + j]; if (s < NC) ib[j] = ic[s]; }
-        lst.clear();
-        for (int64_t kk = 0; kk < nkb; kk++) {
-            int64_t rr = kk;
-            for (int q = nk - 1; q >= 0; q--) { ik[q] = rr % kbd[q]; rr /= kbd[q]; }
-            for (int q = 0; q < nk; q++) { ia[kda[q]] = ik[q]; ib[kdb[q]] = ik[q]; }
-            int64_t aia = a.bis.abs(ia), aib = b.bis.abs(ib);
-            if (!a_nz(aia) || !b_nz(aib)) continue;
-            Pair p;
-            p.aia = aia; p.acia = a.orbits.canon[aia]; p.tra = a.orbits.tr[aia];
-            p.aib = aib; p.acib = b.orbits.canon[aib]; p.trb = b.orbits.tr[aib];
-            if (p.tra.perm.n == 0) p.tra.perm.n = NA;
-            if (p.trb.perm.n == 0) p.trb.perm.n = NB;
-            lst.push_back(p);
+    // Canonical C blocks in chunks over host threads (the reference builds
+    // its lists in thread-pool tasks too); chunk results are joined in order,
+    // so the schedule is the same for any thread count.
+    struct Chunk {
+        std::vector<int64_t> schedule;
+        std::vector<std::vector<Pair> > clst;
+        double flops = 0;
+        bool coalesced = false;
+    };
+    const int64_t ncan = (int64_t)oc.canon_list.size();
+    const int64_t per = 64;
+    const int64_t nchunks = (ncan + per - 1) / per;
+    std::vector<Chunk> chunks((size_t)nchunks);
+    auto work = [&](int64_t ci) {
+        Chunk &ch = chunks[(size_t)ci];
+        int64_t ic[kMaxOrder], ia[kMaxOrder], ib[kMaxOrder], ik[kMaxOrder];
+        int64_t da[kMaxOrder], dc[kMaxOrder];
+        std::vector<Pair> lst;
+        for (int64_t e = ci * per; e < std::min(ncan, (ci + 1) * per); e++) {
+            const int64_t cabs = oc.canon_list[(size_t)e];
+            plan.bisc.unabs(cabs, ic);
+            for (int i = 0; i < NA; i++) { int64_t s = c.conn[NC + i]; if (s < NC) ia[i] = ic[s]; }
+            for (int j = 0; j < NB; j++) { int64_t s = c.conn[NC + NA + j]; if (s < NC) ib[j] = ic[s]; }
+            lst.clear();
+            for (int64_t kk = 0; kk < nkb; kk++) {
+                int64_t rr = kk;
+                for (int q = nk - 1; q >= 0; q--) { ik[q] = rr % kbd[q]; rr /= kbd[q]; }
+                for (int q = 0; q < nk; q++) { ia[kda[q]] = ik[q]; ib[kdb[q]] = ik[q]; }
+                int64_t aia = a.bis.abs(ia), aib = b.bis.abs(ib);
+                if (!a_nz(aia) || !b_nz(aib)) continue;
+                Pair p;
+                p.aia = aia; p.acia = a.orbits.canon[aia]; p.tra = a.orbits.tr[aia];
+                p.aib = aib; p.acib = b.orbits.canon[aib]; p.trb = b.orbits.tr[aib];
+                if (p.tra.perm.n == 0) p.tra.perm.n = NA;
+                if (p.trb.perm.n == 0) p.trb.perm.n = NB;
+                lst.push_back(p);
+            }
+            if (lst.empty()) continue;
+            const size_t before = lst.size();
+            coalesce(c, lst);
+            if (lst.size() != before) ch.coalesced = true;
+            if (lst.empty()) continue;
+            ch.schedule.push_back(cabs);
+            ch.clst.push_back(lst);
+            plan.bisc.block_dims(ic, dc);
+            int64_t csz = 1;
+            for (int i = 0; i < NC; i++) csz *= dc[i];
+            for (const Pair &p : lst) {
+                a.bis.unabs(p.aia, ia);
+                a.bis.block_dims(ia, da);
+                int64_t kext = 1;
+                for (int q = 0; q < nk; q++) kext *= da[kda[q]];
+                ch.flops += 2.0 * (double)csz * (double)kext;
+            }
         }
-        if (lst.empty()) continue;
-        const size_t before = lst.size();
-        coalesce(c, lst);
-        if (lst.size() != before) plan.coalesced = true;
-        if (lst.empty()) continue;
-        plan.schedule.push_back(cabs);
-        plan.clst.emplace_back(lst.begin(), lst.end());
-        plan.bisc.block_dims(ic, dc);
-        int64_t csz = 1;
-        for (int i = 0; i < NC; i++) csz *= dc[i];
-        for (const Pair &p : lst) {
-            a.bis.unabs(p.aia, ia);
-            a.bis.block_dims(ia, da);
-            int64_t kext = 1;
-            for (int q = 0; q < nk; q++) kext *= da[kda[q]];
-            plan.flops += 2.0 * (double)csz * (double)kext;
-        }
+    };
+    const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(1, nthreads), nchunks));
+    if (nt <= 1) {
+        for (int64_t ci = 0; ci < nchunks; ci++) work(ci);
+    } else {
+        std::atomic<int64_t> nextc(0);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; t++)
+            pool.emplace_back([&]() {
+                for (int64_t ci = nextc++; ci < nchunks; ci = nextc++) work(ci);
+            });
+        for (std::thread &th : pool) th.join();
+    }
+    for (Chunk &ch : chunks) {
+        plan.schedule.insert(plan.schedule.end(), ch.schedule.begin(), ch.schedule.end());
+        for (std::vector<Pair> &l : ch.clst) plan.clst.push_back(std::move(l));
+        plan.flops += ch.flops;
+        plan.coalesced = plan.coalesced || ch.coalesced;
     }
 }
 

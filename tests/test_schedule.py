@@ -90,3 +90,43 @@ def test_schedule_and_pairs_match_reference(hctx, case):
     for x in (C, A, B):
         x.close()
     op.close()
+
+
+def _fine_ladder_op(ctx, occ, vir):
+    from libtensor_b200 import spec as S
+    cfg = S.LadderConfig("fine", occ, vir)
+    A, B = block_tensor(ctx, cfg.t_spec()), block_tensor(ctx, cfg.v_spec())
+    A.mark_nonzero(); B.mark_nonzero()
+    c = cfg.contraction
+    contr = contraction2(c["n"], c["m"], c["k"], c["permc"])
+    for p in c["pairs"]:
+        contr.contract(*p)
+    return cfg, A, B, btod_contract2(contr, A, B, 1.0, 1.0, cfg.kc)
+
+
+def test_schedule_does_not_depend_on_host_threads():
+    """The schedule is built in chunks over host threads and joined in order."""
+    out = []
+    for nt in (1, 7):
+        ctx = Context(-1)
+        ctx.set_host_threads(nt)
+        _, A, B, op = _fine_ladder_op(ctx, [3, 3], [4] * 6)
+        sched = op.get_schedule()
+        out.append((sched, [op.pairs(i) for i in range(len(sched))], op.flops()))
+        ctx.close()
+    assert len(out[0][0]) > 64                        # several chunks
+    assert out[0] == out[1]
+
+
+def test_fine_blocking_schedule_matches_reference(hctx):
+    """Many blocks per index (long pair lists with coalescing): schedule and
+    coalesced pair lists as the reference builds them."""
+    cfg, A, B, op = _fine_ladder_op(hctx, [2, 2], [3] * 5)
+    ra = _ref_with_blocks(cfg.t_spec(), A)
+    rb = _ref_with_blocks(cfg.v_spec(), B)
+    c = cfg.contraction
+    rop = R.RefContract2(c["n"], c["m"], c["k"], c["permc"], c["pairs"], ra, rb, 1.0, 1.0, cfg.kc)
+    sched = op.get_schedule()
+    assert sched == rop.schedule()
+    for i, cabs in enumerate(sched):
+        assert op.pairs(i) == rop.pairs(cabs), cabs
