@@ -124,3 +124,38 @@ def test_crt_item_rows_are_bit_identical(gctx, case):
     (two MMA tiles per item) compute the same exact integers."""
     out = _crt_variants(gctx, case, (7, 8), [lambda op: op.set_crt_rows(128), lambda op: op.set_crt_rows(256)])
     assert np.array_equal(out[0], out[1])
+
+
+def test_grouped_products_with_zero_operand_blocks(gctx):
+    """Ring D2h with some t blocks zero: cells of the grouped products that no
+    pair uses stay zero; grouped and per-block products agree (bit-identical
+    in the modular mode, 1e-13 in FP64) and match the reference."""
+    from libtensor_b200 import spec as S
+    from libtensor_b200.core import MODE_PLAIN_FP64
+    case = next(c for c in CASES if c.name == "ring D2h small")
+    A, ra, _ = seeded_pair(gctx, case.a, 51, case.a_scale)
+    nz = A.nonzero()
+    zero = [tuple(A.block_index(a)) for a in nz[::3]]       # every third non-zero canonical block
+    A, ra, _ = seeded_pair(gctx, case.a, 51, case.a_scale, zero)
+    B, rb, _ = seeded_pair(gctx, case.b, 52, case.b_scale)
+    contr = contraction2(case.n, case.m, case.k, case.permc)
+    for p in case.pairs:
+        contr.contract(*p)
+    op = btod_contract2(contr, A, B, case.ka, case.kb, case.kc)
+    C = op.make_result()
+    assert op.group_info(C)[0] > 0
+    rop = R.RefContract2(case.n, case.m, case.k, case.permc, case.pairs, ra, rb, case.ka, case.kb, case.kc)
+    RC = rop.make_result()
+    rop.perform(RC)
+    for mode, S_, tol in ((MODE_PLAIN_FP64, 0, 1e-13), (MODE_OZAKI_CRT, 13, 1e-12)):
+        out = []
+        for grouped in (True, False):
+            op.set_grouping(grouped)
+            Cg = op.make_result()
+            op.perform(Cg, mode=mode, nslices=S_)
+            gctx.synchronize()
+            out.append(Cg.download())
+            assert max_rel_block_error(block_errors(Cg, out[-1], RC, None)) <= tol, (mode, grouped)
+        op.set_grouping(True)
+        if mode == MODE_OZAKI_CRT:
+            assert np.array_equal(out[0].view(np.uint64), out[1].view(np.uint64))
