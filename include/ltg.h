@@ -226,6 +226,42 @@ int ltg_contract2_autotune(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nsli
 int ltg_plan_tiles(ltg_plan *plan, int64_t *m, int64_t *n, int32_t *cfg, int64_t cap,
                    int64_t *count);
 
+/* ---- caller-built task lists ------------------------------------------ */
+/* One block-pair product C[c_off..] += coeff * A[a_off..] * B[b_off..] as
+ * LTG_TASK_WORDS int64 (element offsets into the tensors' arenas):
+ *   [0] c_off  [1] a_off  [2] b_off
+ *   [3] nm, [4..15]  up to four (extent, stride in A, stride in C)   (m)
+ *   [16] nn, [17..28] up to four (extent, stride in B, stride in C)  (n)
+ *   [29] nk, [30..41] up to four (extent, stride in A, stride in B)  (k)
+ *   [42] coeff as raw IEEE-754 bits.
+ * This is the product list that gen_bto_contract2_block::compute_block
+ * (libtensor/gen_block_tensor/impl/gen_bto_contract2_block_impl.h) hands to
+ * the dense kernel, one entry per (C block, pair); the record layout itself
+ * has no reference counterpart. */
+#define LTG_TASK_WORDS 43
+/* Writes the task list of plan for result c (coefficients ka = kb = kc = 1)
+ * into tasks (cap entries), *ntasks = the full count. */
+int ltg_plan_export_tasks(ltg_plan *plan, ltg_bt *c, int64_t *tasks, int64_t cap, int64_t *ntasks);
+/* Plan from a caller-built task list over a and b.  Consecutive tasks with
+ * the same c_off form one C block (same m and n extents; C strides from the
+ * first); a C block's first task assigns or accumulates as ltg_contract2's
+ * add says, the rest accumulate.  Runs in LTG_MODE_PLAIN_FP64 only; the
+ * result tensor must hold every c_off range.  Free with ltg_plan_free. */
+int ltg_plan_contract2_upload(ltg_ctx *ctx, ltg_bt *a, ltg_bt *b, const int64_t *tasks,
+                              int64_t ntasks, ltg_plan **out);
+
+/* ---- alternative names of the entry points above ----------------------- */
+int ltg_bt_alloc(ltg_ctx *ctx, const ltg_bt_spec *spec, ltg_bt **out);      /* ltg_bt_create */
+int ltg_bt_free(ltg_bt *bt);                                                /* ltg_bt_destroy */
+int ltg_bt_upload_blocks(ltg_bt *bt, const double *host);                   /* ltg_bt_upload */
+int ltg_bt_download_blocks(ltg_bt *bt, double *host);                       /* ltg_bt_download */
+int ltg_plan_free(ltg_plan *plan);                                          /* ltg_plan_destroy */
+int ltg_copy_perm(ltg_bt *a, const int32_t *perm, double c, ltg_bt *b,      /* ltg_copy */
+                  int32_t add, double d);
+int ltg_add_perm_n(int32_t nterms, ltg_bt *const *a, const int32_t *perms,  /* ltg_add */
+                   const double *coeffs, ltg_bt *b, int32_t add, double d);
+const char *ltg_last_error_string(void);                                    /* ltg_last_error */
+
 /* ---- btod_copy / btod_add / btod_dotprod ------------------------------ */
 /* b = c * perm(a)  or  b += d * c * perm(a)   (btod_copy.h:38-115) */
 int ltg_copy(ltg_bt *a, const int32_t *perm, double c, ltg_bt *b,

@@ -106,7 +106,20 @@ _SIGS = {
     "ltg_graph_end": (C.c_int, [c_vp, C.POINTER(c_vp)]),
     "ltg_graph_launch": (C.c_int, [c_vp]),
     "ltg_graph_destroy": (C.c_int, [c_vp]),
+    "ltg_plan_export_tasks": (C.c_int, [c_vp, c_vp, c_i64p, C.c_int64, c_i64p]),
+    "ltg_plan_contract2_upload": (C.c_int, [c_vp, c_vp, c_vp, c_i64p, C.c_int64, C.POINTER(c_vp)]),
+    "ltg_bt_alloc": (C.c_int, [c_vp, C.POINTER(ltg_bt_spec), C.POINTER(c_vp)]),
+    "ltg_bt_free": (C.c_int, [c_vp]),
+    "ltg_bt_upload_blocks": (C.c_int, [c_vp, c_dblp]),
+    "ltg_bt_download_blocks": (C.c_int, [c_vp, c_dblp]),
+    "ltg_plan_free": (C.c_int, [c_vp]),
+    "ltg_copy_perm": (C.c_int, [c_vp, c_i32p, C.c_double, c_vp, C.c_int32, C.c_double]),
+    "ltg_add_perm_n": (C.c_int, [C.c_int32, C.POINTER(c_vp), c_i32p, c_dblp, c_vp, C.c_int32, C.c_double]),
+    "ltg_last_error_string": (C.c_char_p, []),
 }
+
+# words per task record of ltg_plan_export_tasks / ltg_plan_contract2_upload
+LTG_TASK_WORDS = 43
 
 _lib = None
 

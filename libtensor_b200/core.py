@@ -345,6 +345,46 @@ class btod_contract2:
         check(lib().ltg_contract2(self.h, c.h, mode, nslices, self.ka, self.kb, self.kc,
                                   0 if d is None else 1, 0.0 if d is None else d))
 
+    def export_tasks(self, c: block_tensor) -> np.ndarray:
+        """Block-pair products of this contraction for result c, one row of
+        LTG_TASK_WORDS int64 per product (coefficients without ka, kb, kc)."""
+        n = C.c_int64()
+        check(lib().ltg_plan_export_tasks(self.h, c.h, None, 0, C.byref(n)))
+        buf = np.zeros((max(1, n.value), _capi.LTG_TASK_WORDS), np.int64)
+        check(lib().ltg_plan_export_tasks(self.h, c.h, buf.ctypes.data_as(_capi.c_i64p), n.value, C.byref(n)))
+        return buf[:n.value]
+
+
+class contract2_task_plan:
+    """A contraction given as a caller-built list of block-pair products over
+    the arenas of a, b and the result (rows of LTG_TASK_WORDS int64, as
+    btod_contract2.export_tasks writes them); plain FP64 mode only."""
+
+    def __init__(self, a: block_tensor, b: block_tensor, tasks: np.ndarray,
+                 ka: float = 1.0, kb: float = 1.0, kc: float = 1.0):
+        self.a, self.b = a, b
+        self.ka, self.kb, self.kc = ka, kb, kc
+        t = np.ascontiguousarray(tasks, dtype=np.int64).reshape(-1, _capi.LTG_TASK_WORDS)
+        h = C.c_void_p()
+        check(lib().ltg_plan_contract2_upload(a.ctx.h, a.h, b.h, t.ctypes.data_as(_capi.c_i64p), len(t),
+                                              C.byref(h)))
+        self.h = h
+        self.ntasks = len(t)
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(lib().ltg_plan_free(self.h))
+            self.h = None
+
+    def flops(self) -> float:
+        f = C.c_double()
+        check(lib().ltg_plan_flops(self.h, C.byref(f)))
+        return f.value
+
+    def perform(self, c: block_tensor, d: Optional[float] = None, mode: int = MODE_PLAIN_FP64):
+        check(lib().ltg_contract2(self.h, c.h, mode, 0, self.ka, self.kb, self.kc,
+                                  0 if d is None else 1, 0.0 if d is None else d))
+
 
 def decode_pairs(buf, na, nb):
     rec = 2 + na + 1 + 2 + nb + 1

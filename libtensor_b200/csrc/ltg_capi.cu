@@ -185,6 +185,10 @@ struct ltg_plan {
     ltg_bt *a = nullptr, *b = nullptr;
     int forced_tile = -1;         // >= 0: every C block uses this tile shape
     bool group_products = true;   // modular mode: small C blocks grouped into larger products
+    // caller-built task list (ltg_plan_contract2_upload): plain FP64 only,
+    // coefficients absolute, no schedule of its own
+    bool external = false;
+    std::vector<GemmTask> ext_tasks;
     int crt_rows = 0;             // modular mode: work-item rows (128, 256; 0 default)
     std::map<std::pair<int64_t, int64_t>, int> tile_override;   // autotuned (M, N) -> shape
     ContractPlan plan;
@@ -442,6 +446,12 @@ void pack_sub(const SubDims &s, int32_t &n, int32_t *ext, int32_t *str0, int32_t
     }
 }
 
+// Caller-built tasks as the per-C-block lists of the plain path: consecutive
+// tasks with the same c_off form one C block, whose C mapping is the first
+// task's (C strides of m and n, fused on C strides alone).
+void external_blocks(const ltg_plan *pl, double ka, double kb, double kc, std::vector<GemmTask> &tasks,
+                     std::vector<CBlockTask> &cbt);
+
 void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &cbt, double kabc, double post,
                         std::vector<int32_t> &group_of, PlainGroups &pg);
 std::vector<std::pair<int64_t, int64_t>> plain_group_shapes(ltg_plan *pl, ltg_bt *c,
@@ -456,7 +466,8 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     std::unique_ptr<ContractExec> ex(new ContractExec());
     std::vector<GemmTask> tasks;
     std::vector<CBlockTask> cbt;
-    contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    if (pl->external) external_blocks(pl, ka, kb, kc, tasks, cbt);
+    else contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
     // Every address a task can form must lie inside its arena.
     auto span = [](const SubDims &s, bool second) {
         int64_t m = 0;
@@ -470,6 +481,9 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
         if (t.a_off < 0 || amax >= pl->a->h.total_elems || t.b_off < 0 || bmax >= pl->b->h.total_elems ||
             t.c_off < 0 || cmax >= c->h.total_elems)
             throw error(kErrState, "contraction task addresses outside an operand arena");
+        if (t.m.total() * t.k.total() > pl->a->h.total_elems || t.n.total() * t.k.total() > pl->b->h.total_elems ||
+            t.m.total() * t.n.total() > c->h.total_elems)
+            throw error(kErrBadArg, "contraction task larger than its operands");
     }
     std::vector<DTask> dt(tasks.size());
     for (size_t i = 0; i < tasks.size(); i++) {
@@ -501,7 +515,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     }
     // small blocks computed as grouped products
     std::vector<int32_t> group_of(cbt.size(), -1);
-    if (pl->group_products && !pl->plan.coalesced) {
+    if (pl->group_products && !pl->plan.coalesced && !pl->external) {
         ex->groups.reset(new PlainGroups());
         build_plain_groups(pl, c, cbt, ka * kb * kc, post, group_of, *ex->groups);
         if (ex->groups->ngroups == 0) ex->groups.reset();
@@ -537,7 +551,21 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     upload_vec(ex->items, items, s);
     // blocks of C outside the schedule (zeroed in assign mode)
     std::vector<char> in_sched(c->h.blk_abs.size(), 0);
-    for (int64_t cabs : pl->plan.schedule) {
+    if (pl->external) {
+        std::map<int64_t, int64_t> slot_of_off;
+        for (size_t sl = 0; sl < c->h.blk_off.size(); sl++) slot_of_off[c->h.blk_off[sl]] = (int64_t)sl;
+        for (const CBlockTask &b : cbt) {
+            auto f = slot_of_off.find(b.c_off);
+            if (f == slot_of_off.end()) throw error(kErrBadArg, "a task's c_off is not the start of a block of C");
+            if (in_sched[f->second]) throw error(kErrBadArg, "the tasks of one C block must be consecutive");
+            if (b.c_off + span(b.cm, true) + span(b.cn, true) >= b.c_off + c->h.blk_size[f->second] ||
+                b.M * b.N > c->h.blk_size[f->second])
+                throw error(kErrBadArg, "a task's C range leaves its block");
+            ex->sched_slots.push_back(f->second);
+            in_sched[f->second] = 1;
+        }
+    }
+    for (int64_t cabs : pl->external ? std::vector<int64_t>() : pl->plan.schedule) {
         int64_t sl = c->h.slot_of[cabs];
         in_sched[sl] = 1;
         ex->sched_slots.push_back(sl);
@@ -1061,6 +1089,32 @@ std::vector<std::pair<int64_t, int64_t>> plain_group_shapes(ltg_plan *pl, ltg_bt
         shapes.push_back({lay.rows, lay.cols});
     }
     return shapes;
+}
+
+void external_blocks(const ltg_plan *pl, double ka, double kb, double kc, std::vector<GemmTask> &tasks,
+                     std::vector<CBlockTask> &cbt) {
+    tasks = pl->ext_tasks;
+    for (GemmTask &t : tasks) t.coeff = t.coeff * ka * kb * kc;   // the order contract2_tasks uses
+    cbt.clear();
+    for (size_t i = 0; i < tasks.size(); i++) {
+        if (cbt.empty() || tasks[i].c_off != cbt.back().c_off) {
+            CBlockTask b;
+            b.c_off = tasks[i].c_off;
+            b.t_begin = (int32_t)i;
+            b.cm = tasks[i].m; b.cn = tasks[i].n;
+            for (int q = 0; q < b.cm.n; q++) b.cm.s0[q] = b.cm.s1[q];
+            for (int q = 0; q < b.cn.n; q++) b.cn.s0[q] = b.cn.s1[q];
+            b.M = b.cm.total(); b.N = b.cn.total();
+            b.coeff0 = tasks[i].coeff;
+            cbt.push_back(b);
+        }
+        CBlockTask &b = cbt.back();
+        if (tasks[i].m.total() != b.M || tasks[i].n.total() != b.N)
+            throw error(kErrBadArg, "tasks of one C block must share its m and n extents");
+        tasks[i].cblk = (int32_t)(cbt.size() - 1);
+        b.kflops += (double)tasks[i].k.total();
+        b.t_end = (int32_t)i + 1;
+    }
 }
 
 void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &cbt, double kabc, double post,
@@ -1796,6 +1850,39 @@ void forget_dot(const ltg_bt *t) {
     }
 }
 
+// LTG_TASK_WORDS int64 per task (layout in ltg.h)
+void pack_task(const GemmTask &t, int64_t *w) {
+    std::memset(w, 0, LTG_TASK_WORDS * sizeof(int64_t));
+    w[0] = t.c_off; w[1] = t.a_off; w[2] = t.b_off;
+    const SubDims *sd[3] = {&t.m, &t.n, &t.k};
+    for (int g = 0; g < 3; g++) {
+        int64_t *x = w + 3 + 13 * g;
+        x[0] = sd[g]->n;
+        for (int i = 0; i < sd[g]->n; i++) { x[1 + 3 * i] = sd[g]->ext[i]; x[2 + 3 * i] = sd[g]->s0[i]; x[3 + 3 * i] = sd[g]->s1[i]; }
+    }
+    std::memcpy(&w[42], &t.coeff, sizeof(double));
+}
+GemmTask unpack_task(const int64_t *w) {
+    GemmTask t;
+    t.c_off = w[0]; t.a_off = w[1]; t.b_off = w[2];
+    SubDims *sd[3] = {&t.m, &t.n, &t.k};
+    for (int g = 0; g < 3; g++) {
+        const int64_t *x = w + 3 + 13 * g;
+        if (x[0] < 0 || x[0] > kMaxSub) throw error(kErrBadArg, "task: sub-dimension count out of range");
+        sd[g]->n = (int)x[0];
+        for (int i = 0; i < sd[g]->n; i++) {
+            if (x[1 + 3 * i] < 1 || x[1 + 3 * i] > ((int64_t)1 << 30)) throw error(kErrBadArg, "task: extent out of range");
+            if (x[2 + 3 * i] < 0 || x[3 + 3 * i] < 0 || x[2 + 3 * i] > ((int64_t)1 << 40) || x[3 + 3 * i] > ((int64_t)1 << 40))
+                throw error(kErrBadArg, "task: stride out of range");
+            sd[g]->ext[i] = (int32_t)x[1 + 3 * i]; sd[g]->s0[i] = x[2 + 3 * i]; sd[g]->s1[i] = x[3 + 3 * i];
+            if (sd[g]->total() > ((int64_t)1 << 31) - 1) throw error(kErrBadArg, "task: dimension too large");
+        }
+    }
+    std::memcpy(&t.coeff, &w[42], sizeof(double));
+    t.cblk = 0;
+    return t;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2142,6 +2229,7 @@ int ltg_contract2_create(ltg_ctx *ctx, int32_t n, int32_t m, int32_t k, const in
 int ltg_contract2_make_result(ltg_plan *plan, ltg_bt **c) {
     return guard([&] {
         if (!plan || !c) throw error(kErrBadArg, "null argument");
+        if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
         std::unique_ptr<ltg_bt> bt(new ltg_bt());
         bt->ctx = plan->ctx;
         bt->h.bis = plan->plan.bisc;
@@ -2189,13 +2277,66 @@ int ltg_plan_flops(ltg_plan *plan, double *flops) {
     return guard([&] { if (!plan || !flops) throw error(kErrBadArg, "null argument"); *flops = plan->plan.flops; });
 }
 
+
+
+int ltg_plan_export_tasks(ltg_plan *plan, ltg_bt *c, int64_t *tasks, int64_t cap, int64_t *ntasks) {
+    return guard([&] {
+        if (!plan || !ntasks) throw error(kErrBadArg, "null argument");
+        check_bt(c);
+        if (plan->external) throw error(kErrBadArg, "the plan holds caller-built tasks");
+        if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
+        std::vector<GemmTask> t;
+        std::vector<CBlockTask> cbt;
+        contract2_tasks(plan->plan, plan->a->h, plan->b->h, c->h, 1.0, 1.0, 1.0, t, cbt);
+        for (size_t i = 0; i < t.size() && (int64_t)i < cap; i++) pack_task(t[i], tasks + LTG_TASK_WORDS * i);
+        *ntasks = (int64_t)t.size();
+    });
+}
+
+int ltg_plan_contract2_upload(ltg_ctx *ctx, ltg_bt *a, ltg_bt *b, const int64_t *tasks, int64_t ntasks,
+                              ltg_plan **out) {
+    return guard([&] {
+        check_ctx(ctx); check_bt(a); check_bt(b);
+        if (!out || (ntasks > 0 && !tasks) || ntasks < 0) throw error(kErrBadArg, "invalid task list");
+        std::unique_ptr<ltg_plan> pl(new ltg_plan());
+        pl->ctx = ctx; pl->a = a; pl->b = b;
+        pl->external = true;
+        pl->plan.coalesced = true;
+        for (int64_t i = 0; i < ntasks; i++) {
+            pl->ext_tasks.push_back(unpack_task(tasks + LTG_TASK_WORDS * i));
+            const GemmTask &t = pl->ext_tasks.back();
+            pl->plan.flops += 2.0 * (double)t.m.total() * (double)t.n.total() * (double)t.k.total();
+        }
+        *out = pl.release();
+    });
+}
+
+// Names of the boundary as first specified (aliases of the entry points above).
+int ltg_bt_alloc(ltg_ctx *ctx, const ltg_bt_spec *spec, ltg_bt **out) { return ltg_bt_create(ctx, spec, out); }
+int ltg_bt_free(ltg_bt *bt) { return ltg_bt_destroy(bt); }
+int ltg_bt_upload_blocks(ltg_bt *bt, const double *host) { return ltg_bt_upload(bt, host); }
+int ltg_bt_download_blocks(ltg_bt *bt, double *host) { return ltg_bt_download(bt, host); }
+int ltg_plan_free(ltg_plan *plan) { return ltg_plan_destroy(plan); }
+int ltg_copy_perm(ltg_bt *a, const int32_t *perm, double c, ltg_bt *b, int32_t add, double d) {
+    return ltg_copy(a, perm, c, b, add, d);
+}
+int ltg_add_perm_n(int32_t nterms, ltg_bt *const *a, const int32_t *perms, const double *coeffs, ltg_bt *b,
+                   int32_t add, double d) {
+    return ltg_add(nterms, a, perms, coeffs, b, add, d);
+}
+const char *ltg_last_error_string(void) { return ltg_last_error(); }
+
 int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, double ka, double kb,
                   double kc, int32_t add, double d) {
     return guard([&] {
         if (!plan) throw error(kErrBadArg, "null plan");
         check_bt(c);
         need_dev(plan->ctx);
-        if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
+        if (plan->external) {
+            if (mode != LTG_MODE_PLAIN_FP64) throw error(kErrUnsupported, "a caller-built task plan runs in the plain FP64 mode only");
+        } else if (!c->h.bis.equals(plan->plan.bisc)) {
+            throw error(kErrBadDims, "result tensor has a different block index space");
+        }
         ltg_ctx *ctx = plan->ctx;
         cudaStream_t s = ctx->stream;
         if (mode == LTG_MODE_OZAKI_CRT) {
@@ -2320,6 +2461,7 @@ int ltg_contract2_split_bytes(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t n
                               double kc, int32_t add, double d, int64_t *read_bytes, int64_t *write_bytes) {
     return guard([&] {
         if (!plan || !read_bytes || !write_bytes) throw error(kErrBadArg, "null argument");
+        if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
         check_bt(c);
         need_dev(plan->ctx);
         if (mode == LTG_MODE_OZAKI_CRT) {
@@ -2377,6 +2519,7 @@ int ltg_contract2_group_info(ltg_plan *plan, ltg_bt *c, int64_t *ngroups, int64_
                              double *grouped_flops, double *block_flops) {
     return guard([&] {
         if (!plan) throw error(kErrBadArg, "null plan");
+        if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
         check_bt(c);
         if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
         std::vector<GemmTask> tasks;
@@ -2409,6 +2552,7 @@ int ltg_contract2_autotune(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nsli
                            double kb, double kc, int32_t reps) {
     return guard([&] {
         if (!plan) throw error(kErrBadArg, "null plan");
+        if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
         check_bt(c);
         need_dev(plan->ctx);
         if (plan->ctx->capturing) throw error(kErrState, "autotuning cannot run during graph capture");
