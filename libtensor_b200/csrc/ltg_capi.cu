@@ -438,6 +438,9 @@ int pick_tile(int64_t M, int64_t N) {
 
 void pack_sub(const SubDims &s, int32_t &n, int32_t *ext, int32_t *str0, int32_t *str1) {
     if (s.n > kDevMaxSub) throw error(kErrUnsupported, "too many sub-dimensions");
+    for (int i = 0; i < s.n; i++)
+        if (s.s0[i] < 0 || s.s0[i] > INT32_MAX || s.s1[i] < 0 || s.s1[i] > INT32_MAX)
+            throw error(kErrUnsupported, "stride beyond the 32-bit range of the kernels");
     n = s.n;
     for (int i = 0; i < kDevMaxSub; i++) {
         ext[i] = i < s.n ? s.ext[i] : 1;
@@ -1872,7 +1875,8 @@ GemmTask unpack_task(const int64_t *w) {
         sd[g]->n = (int)x[0];
         for (int i = 0; i < sd[g]->n; i++) {
             if (x[1 + 3 * i] < 1 || x[1 + 3 * i] > ((int64_t)1 << 30)) throw error(kErrBadArg, "task: extent out of range");
-            if (x[2 + 3 * i] < 0 || x[3 + 3 * i] < 0 || x[2 + 3 * i] > ((int64_t)1 << 40) || x[3 + 3 * i] > ((int64_t)1 << 40))
+            // the kernels hold strides as int32
+            if (x[2 + 3 * i] < 0 || x[3 + 3 * i] < 0 || x[2 + 3 * i] > INT32_MAX || x[3 + 3 * i] > INT32_MAX)
                 throw error(kErrBadArg, "task: stride out of range");
             sd[g]->ext[i] = (int32_t)x[1 + 3 * i]; sd[g]->s0[i] = x[2 + 3 * i]; sd[g]->s1[i] = x[3 + 3 * i];
             if (sd[g]->total() > ((int64_t)1 << 31) - 1) throw error(kErrBadArg, "task: dimension too large");

@@ -115,6 +115,9 @@ def test_malformed_task_records_are_rejected(hctx):
     assert _plan_upload(hctx, A, B, bad) == ERR_BAD_ARG
     assert "stride" in lib().ltg_last_error_string().decode()
     bad = tasks[:1].copy()
+    bad[0, 5] = 1 << 31                # stride beyond int32
+    assert _plan_upload(hctx, A, B, bad) == ERR_BAD_ARG
+    bad = tasks[:1].copy()
     bad[0, 4] = 1 << 20                # 2^20 x 2^20 rows: dimension too large
     bad[0, 3] = 2
     bad[0, 7] = 1 << 20
