@@ -303,16 +303,20 @@ using Cfg4 = TileCfg<80, 128, 32, 80, 16, 3>;
 using Cfg5 = TileCfg<96, 128, 32, 96, 16, 3>;
 using Cfg6 = TileCfg<48, 128, 32, 48, 16, 3>;
 using Cfg7 = TileCfg<112, 128, 16, 112, 16, 4>;
+// short shapes for C blocks of 16 or 32 rows (e.g. an occupied pair block
+// of 4 x 4 orbitals): wide in N so that each A row slab is reused 128 times
+using Cfg8 = TileCfg<16, 128, 32, 16, 16, 3>;
+using Cfg9 = TileCfg<32, 128, 32, 32, 16, 3>;
 
 }  // namespace
 
-int tile_cfg_count() { return 8; }
+int tile_cfg_count() { return 10; }
 int tile_cfg_bm(int cfg) {
-    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM};
+    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM, Cfg8::BM, Cfg9::BM};
     return v[cfg];
 }
 int tile_cfg_bn(int cfg) {
-    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN};
+    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN, Cfg8::BN, Cfg9::BN};
     return v[cfg];
 }
 
@@ -327,7 +331,9 @@ cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     case 4: return launch_cfg<Cfg4>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     case 5: return launch_cfg<Cfg5>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     case 6: return launch_cfg<Cfg6>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    default: return launch_cfg<Cfg7>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 7: return launch_cfg<Cfg7>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 8: return launch_cfg<Cfg8>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    default: return launch_cfg<Cfg9>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     }
 }
 

@@ -417,16 +417,18 @@ int32_t vec16_ok(int64_t off, const SubDims &rows, const SubDims &k, bool second
 // the shape (larger tiles reuse more data per load).  An autotuned table
 // (ltg_autotune) overrides the weights with measured rates.
 struct TileShape { int bm, bn; double eff; };
-const TileShape kShapes[8] = {
+constexpr int kNumShapes = 10;
+const TileShape kShapes[kNumShapes] = {
     {128, 128, 1.00}, {64, 64, 0.78}, {64, 128, 0.90}, {32, 32, 0.45},
     {80, 128, 0.97}, {96, 128, 0.98}, {48, 128, 0.85}, {112, 128, 0.99},
+    {16, 128, 0.50}, {32, 128, 0.70},
 };
-double g_tile_eff[8] = {1.00, 0.78, 0.90, 0.45, 0.97, 0.98, 0.85, 0.99};
+double g_tile_eff[kNumShapes] = {1.00, 0.78, 0.90, 0.45, 0.97, 0.98, 0.85, 0.99, 0.50, 0.70};
 
 int pick_tile(int64_t M, int64_t N) {
     int best = 0;
     double bestc = 1e300;
-    for (int c = 0; c < 8; c++) {
+    for (int c = 0; c < kNumShapes; c++) {
         const TileShape &s = kShapes[c];
         double pm = (double)((M + s.bm - 1) / s.bm) * s.bm;
         double pn = (double)((N + s.bn - 1) / s.bn) * s.bn;
@@ -525,7 +527,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     }
     // Work items per tile configuration, costliest first (LPT order for the
     // persistent work queue).
-    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(8);
+    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(kNumShapes);
     for (size_t e = 0; e < cbt.size(); e++) {
         if (group_of[e] >= 0) continue;
         int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(cbt[e].M, cbt[e].N);
@@ -540,7 +542,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
             }
     }
     std::vector<DItem> items;
-    for (int cfg = 0; cfg < 8; cfg++) {
+    for (int cfg = 0; cfg < kNumShapes; cfg++) {
         auto &v = per_cfg[cfg];
         if (v.empty()) continue;
         std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
@@ -1136,7 +1138,7 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
     std::vector<int64_t> res_off;
     std::vector<DTask> dt;
     std::vector<DCBlock> dc;
-    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(8);
+    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(kNumShapes);
     int64_t off = 0;
     PlainGroupLayout lay;
     // one tile shape for all groups (one launch, one tail): that of the
@@ -1215,7 +1217,7 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
         dc.push_back(b);
     }
     std::vector<DItem> items;
-    for (int cfg = 0; cfg < 8; cfg++) {
+    for (int cfg = 0; cfg < kNumShapes; cfg++) {
         auto &v = per_cfg[cfg];
         if (v.empty()) continue;
         std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
