@@ -307,16 +307,19 @@ using Cfg7 = TileCfg<112, 128, 16, 112, 16, 4>;
 // of 4 x 4 orbitals): wide in N so that each A row slab is reused 128 times
 using Cfg8 = TileCfg<16, 128, 32, 16, 16, 3>;
 using Cfg9 = TileCfg<32, 128, 32, 32, 16, 3>;
+// 80-row shapes with twelve warps (three per scheduler, 168 registers)
+using Cfg10 = TileCfg<80, 192, 16, 80, 16, 4>;
+using Cfg11 = TileCfg<80, 192, 32, 80, 16, 2>;
 
 }  // namespace
 
-int tile_cfg_count() { return 10; }
+int tile_cfg_count() { return 12; }
 int tile_cfg_bm(int cfg) {
-    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM, Cfg8::BM, Cfg9::BM};
+    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM, Cfg8::BM, Cfg9::BM, Cfg10::BM, Cfg11::BM};
     return v[cfg];
 }
 int tile_cfg_bn(int cfg) {
-    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN, Cfg8::BN, Cfg9::BN};
+    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN, Cfg8::BN, Cfg9::BN, Cfg10::BN, Cfg11::BN};
     return v[cfg];
 }
 
@@ -333,7 +336,9 @@ cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     case 6: return launch_cfg<Cfg6>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     case 7: return launch_cfg<Cfg7>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     case 8: return launch_cfg<Cfg8>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    default: return launch_cfg<Cfg9>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 9: return launch_cfg<Cfg9>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 10: return launch_cfg<Cfg10>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    default: return launch_cfg<Cfg11>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
     }
 }
 

@@ -417,13 +417,13 @@ int32_t vec16_ok(int64_t off, const SubDims &rows, const SubDims &k, bool second
 // the shape (larger tiles reuse more data per load).  An autotuned table
 // (ltg_autotune) overrides the weights with measured rates.
 struct TileShape { int bm, bn; double eff; };
-constexpr int kNumShapes = 10;
+constexpr int kNumShapes = 12;
 const TileShape kShapes[kNumShapes] = {
     {128, 128, 1.00}, {64, 64, 0.78}, {64, 128, 0.90}, {32, 32, 0.45},
     {80, 128, 0.97}, {96, 128, 0.98}, {48, 128, 0.85}, {112, 128, 0.99},
-    {16, 128, 0.50}, {32, 128, 0.70},
+    {16, 128, 0.50}, {32, 128, 0.70}, {80, 192, 0.96}, {80, 192, 0.95},
 };
-double g_tile_eff[kNumShapes] = {1.00, 0.78, 0.90, 0.45, 0.97, 0.98, 0.85, 0.99, 0.50, 0.70};
+double g_tile_eff[kNumShapes] = {1.00, 0.78, 0.90, 0.45, 0.97, 0.98, 0.85, 0.99, 0.50, 0.70, 0.96, 0.95};
 
 int pick_tile(int64_t M, int64_t N) {
     int best = 0;

@@ -61,7 +61,7 @@ def test_contract_add_matches_reference(gctx, case):
     assert max_rel_block_error(errs) <= TOL
 
 
-@pytest.mark.parametrize("cfg", range(10))
+@pytest.mark.parametrize("cfg", range(12))
 @pytest.mark.parametrize("case", [CASES[0], CASES[1], CASES[5]], ids=["ladder", "ring", "K=1"])
 def test_every_tile_shape_matches_reference(gctx, case, cfg):
     A, B, op, rop = _run(gctx, case)
