@@ -163,12 +163,15 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- reference
 
-def build_reference(a_spec, b_spec, cfg, A_host, A_bt, B_host, B_bt):
+def build_reference(a_spec, b_spec, cfg):
+    """The workload on the reference compiled from its sources: operands
+    filled with the seeded inputs inside the reference library (the same bits
+    the product generates on the device), the contraction and its result
+    tensor.  Nothing of the product library is loaded."""
     from oracle import refapi as R
     ra, rb = R.RefBT(a_spec), R.RefBT(b_spec)
-    for t, host, r in ((A_bt, A_host, ra), (B_bt, B_host, rb)):
-        for bidx, blk in t.blocks(host):
-            r.set_block(bidx, blk)
+    ra.fill_seeded(11, cfg.t_scale)
+    rb.fill_seeded(23, cfg.v_scale)
     c = cfg.contraction
     op = R.RefContract2(c["n"], c["m"], c["k"], c["permc"], c["pairs"], ra, rb, 1.0, 1.0, cfg.kc)
     rc = op.make_result()
@@ -196,21 +199,15 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from libtensor_b200.core import Context, block_tensor
     from oracle import refapi as R
     cfg, a_spec, b_spec = workload(args.workload)
     metric, unit = metric_name(), "TFLOP/s"
     if not R.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libltref.so was not built"}))
         return
-    hctx = Context(-1)
-    A, B = block_tensor(hctx, a_spec), block_tensor(hctx, b_spec)
-    ah, bh = A.fill_seeded_host(11, cfg.t_scale), B.fill_seeded_host(23, cfg.v_scale)
-    from libtensor_b200.core import btod_contract2
-    A.mark_nonzero(); B.mark_nonzero()
-    plan = btod_contract2(contraction_of(cfg), A, B, kc=cfg.kc)
-    flops = plan.flops()
-    ra, rb, op, rc = build_reference(a_spec, b_spec, cfg, ah, A, bh, B)
+    R.set_threads(os.cpu_count() or 1)
+    ra, rb, op, rc = build_reference(a_spec, b_spec, cfg)
+    flops = 2.0 * op.cost()[0]       # the reference's task cost of the schedule, before its /1000
     sec, runs = time_reference(op, rc, args.steps, min(args.warmup, 1), budget_s=120.0)
     v = flops / sec / 1e12
     out = {"metric": metric, "value": v, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
@@ -315,25 +312,15 @@ def ltg_arm(args):
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
 
-    # accuracy of the split-precision result against the plain FP64 path
-    # (which agrees with the reference CPU implementation to 1e-13 per block)
-    accuracy = None
-    if mode != 0:
-        got = C.download()
-        Cref = op.make_result()
-        op.perform(Cref, mode=0)
-        ref = Cref.download()
-        worst, num, den = 0.0, 0.0, 0.0
-        for (bidx, g), (_, r) in zip(C.blocks(got), Cref.blocks(ref)):
-            m = float(np.max(np.abs(r))) if r.size else 0.0
-            if m > 0:
-                worst = max(worst, float(np.max(np.abs(g - r))) / m)
-            num += float(np.sum((g - r) ** 2))
-            den += float(np.sum(r ** 2))
-        accuracy = {"max_block_rel_err": worst, "rms_rel_err": (num / den) ** 0.5 if den > 0 else 0.0,
-                    "against": "plain FP64 DMMA result of the same call (itself within 1e-13 of the "
-                               "reference CPU btod_contract2)"}
-        Cref.close()
+    # results kept for the accuracy check against the reference (below)
+    results = {}
+    if rank == 0:
+        results[args.mode] = C.download()
+        if mode != 0:
+            Cp = op.make_result()
+            op.perform(Cp, mode=0)
+            results["plain"] = Cp.download()
+            Cp.close()
 
     # plain FP64 DMMA companion on the same workload (the metric's denominator)
     plain = None
@@ -385,9 +372,9 @@ def ltg_arm(args):
         split = op.split_bytes(C, mode, args.nslices) if mode != 0 else None
         roofline = contraction_roofline(torch, dev, args, flops, ktimes, split)
 
-    cpu = None
+    cpu, accuracy = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(cfg, a_spec, b_spec, A, B, flops)
+        cpu, accuracy = cpu_baseline(cfg, a_spec, b_spec, C, results, flops, op.get_schedule())
 
     if world > 1:
         dist.barrier()
@@ -494,21 +481,46 @@ def contraction_roofline(torch, dev, args, flops, ktimes, split=None):
             "frac": None, "traffic": traffic, "avg_launch_ms": sec * 1e3}
 
 
-def cpu_baseline(cfg, a_spec, b_spec, A, B, flops):
+def block_accuracy(C, arena, rc):
+    """Block max-norm relative error (worst block) and RMS relative error of a
+    product result against the reference's result tensor."""
+    worst, num, den = 0.0, 0.0, 0.0
+    for bidx, g in C.blocks(arena):
+        r = rc.get_block(bidx, g.shape)
+        m = float(np.max(np.abs(r))) if r.size else 0.0
+        if m > 0:
+            worst = max(worst, float(np.max(np.abs(g - r))) / m)
+        num += float(np.sum((g - r) ** 2))
+        den += float(np.sum(r ** 2))
+    return {"max_block_rel_err": worst, "rms_rel_err": (num / den) ** 0.5 if den > 0 else 0.0}
+
+
+def cpu_baseline(cfg, a_spec, b_spec, C, results, flops, sched):
+    """The reference's perform() on the same seeded inputs, timed on the host
+    cores, and the product's results (this mode and the plain path) compared
+    block by block with the reference's result."""
     try:
         from oracle import refapi as R
         if not R.available():
-            return None
-        ah, bh = A.download(), B.download()
-        ra, rb, op, rc = build_reference(a_spec, b_spec, cfg, ah, A, bh, B)
+            return None, None
+        R.set_threads(os.cpu_count() or 1)
+        ra, rb, op, rc = build_reference(a_spec, b_spec, cfg)
         sec, runs = time_reference(op, rc, 2, 0, budget_s=30.0)
-        return {"value": flops / sec / 1e12, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": f"full workload, {runs} perform() call(s) of the reference built from its sources "
-                          f"(OpenBLAS, 1 BLAS thread x {os.cpu_count()} libutil threads, one batch per operand)",
-                "ms_per_step": sec * 1e3}
+        cpu = {"value": flops / sec / 1e12, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
+               "sample": f"full workload, {runs} perform() call(s) of the reference built from its sources "
+                         f"(OpenBLAS, 1 BLAS thread x {os.cpu_count()} libutil threads, one batch per operand)",
+               "ms_per_step": sec * 1e3}
+        acc = {k: block_accuracy(C, v, rc) for k, v in results.items()}
+        acc["against"] = ("the reference CPU btod_contract2 (built from its sources) on the same seeded "
+                          "inputs, per canonical C block")
+        acc["nonzero_blocks_identical"] = op.schedule() == list(sched)
+        for x in (rc, ra, rb):
+            x.close()
+        op.close()
+        return cpu, acc
     except Exception as e:   # the baseline is reported, never required
-        return {"value": None, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": f"failed: {e}"}
+        return ({"value": None, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
+                 "sample": f"failed: {e}"}, None)
 
 
 # ---------------------------------------------------------------- HBM-bound operations

@@ -16,8 +16,13 @@
  *   - the per-C-block contraction pair list exactly as the schedule builder
  *     makes it (gen_block_tensor/impl/gen_bto_contract2_nzorb_impl.h:455-463
  *     calls gen_bto_contract2_clst_builder::build_list(false, cbl));
+ *   - the schedule's work as the reference's task cost counts it
+ *     (gen_block_tensor/impl/gen_bto_contract2_block_impl.h:63-95);
  *   - btod_copy / btod_add / btod_dotprod (block_tensor/btod_copy.h:38,
- *     btod_add.h:38, btod_dotprod.h:35).
+ *     btod_add.h:38, btod_dotprod.h:35);
+ *   - seeded test inputs written straight into the reference's tensors (the
+ *     same distribution as the product's input generator, restated here), so
+ *     that a CPU-only caller needs nothing but this library.
  *
  * Tensor description ("spec") is a flat int64 array; the layout is documented
  * at parse_spec() and produced by oracle/refapi.py.
@@ -29,11 +34,13 @@
 #include <vector>
 #include <stdexcept>
 #include <sys/time.h>
+#include <thread>
 
 #include <libutil/thread_pool/thread_pool.h>
 #include <libtensor/core/allocator.h>
 #include <libtensor/core/abs_index.h>
 #include <libtensor/core/orbit.h>
+#include <libtensor/core/orbit_list.h>
 #include <libtensor/core/short_orbit.h>
 #include <libtensor/core/batching_policy_base.h>
 #include <libtensor/block_tensor/block_tensor.h>
@@ -312,6 +319,86 @@ int orbit_info(void *h, int64_t aidx, int64_t *canon, int32_t *perm,
     return o.is_allowed() ? 1 : 0;
 }
 
+/* ---------------- seeded test inputs ------------------------------------ */
+
+/* The test-input distribution, restated: splitmix64 (Steele, Lea & Flood,
+   OOPSLA 2014) keyed by the element's linear index in the full dense tensor,
+   six 64-bit draws giving twelve 32-bit uniforms, centred sum; symmetrised as
+   sum over the group (perm, sign) of sign * g(P x); one final multiply by
+   scale * 2^-32. */
+inline uint64_t sm64_mix(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+inline int64_t seeded_int(uint64_t seed, uint64_t lin) {
+    uint64_t key = sm64_mix(seed), s = 0;
+    for (int r = 0; r < 6; r++) {
+        uint64_t h = sm64_mix(key + lin * 6u + (uint64_t)r);
+        s += (h & 0xffffffffULL) + (h >> 32);
+    }
+    return (int64_t)s - (int64_t)(6ULL << 32);
+}
+
+/* Fills every canonical, allowed block of the tensor (the reference's own
+   orbit_list) with the seeded values; elements of a block are spread over
+   nthreads host threads. */
+template<size_t N>
+void fill_seeded(void *h, uint64_t seed, double scale, int ng,
+    const int32_t *perms, const int32_t *signs, int nthreads) {
+    bt_h<N> *t = as<N>(h);
+    block_tensor_wr_ctrl<N, double> ctrl(t->bt);
+    orbit_list<N, double> ol(ctrl.req_const_symmetry());
+    const dimensions<N> &dims = t->bis.get_dims();
+    const double sc = scale * 0x1p-32;
+    if (nthreads < 1) nthreads = 1;
+    for (typename orbit_list<N, double>::iterator it = ol.begin();
+         it != ol.end(); ++it) {
+        index<N> bi;
+        ol.get_index(it, bi);
+        index<N> start = t->bis.get_block_start(bi);
+        dimensions<N> bd = t->bis.get_block_dims(bi);
+        size_t n = bd.get_size();
+        dense_tensor_wr_i<N, double> &blk = ctrl.req_block(bi);
+        {
+            dense_tensor_wr_ctrl<N, double> tc(blk);
+            double *p = tc.req_dataptr();
+            auto work = [&](size_t e0, size_t e1) {
+                size_t x[N];
+                for (size_t e = e0; e < e1; e++) {
+                    size_t r = e;
+                    for (size_t d = N; d-- > 0;) {
+                        x[d] = start[d] + r % bd[d];
+                        r /= bd[d];
+                    }
+                    int64_t v = 0;
+                    for (int g = 0; g < ng; g++) {
+                        uint64_t lin = 0;
+                        for (size_t d = 0; d < N; d++)
+                            lin = lin * (uint64_t)dims[d] + (uint64_t)x[perms[g * N + d]];
+                        int64_t s = seeded_int(seed, lin);
+                        v += signs[g] > 0 ? s : -s;
+                    }
+                    p[e] = (double)v * sc;
+                }
+            };
+            size_t nt = std::min<size_t>((size_t)nthreads, (n + 4095) / 4096);
+            if (nt <= 1) {
+                work(0, n);
+            } else {
+                std::vector<std::thread> th;
+                for (size_t w = 0; w < nt; w++)
+                    th.emplace_back(work, n * w / nt, n * (w + 1) / nt);
+                for (auto &x : th) x.join();
+            }
+            tc.ret_dataptr(p);
+        }
+        ctrl.ret_block(bi);
+    }
+}
+
 /* ---------------- contraction ------------------------------------------ */
 
 struct c2_base {
@@ -320,6 +407,7 @@ struct c2_base {
     virtual void *make_result() = 0;
     virtual void perform(void *c, int add, double d) = 0;
     virtual size_t clst(int64_t cabs, int64_t *out, size_t cap) = 0;
+    virtual void cost(int64_t *exact, int64_t *ref_cost) = 0;
     virtual void result_bidims(int64_t *out) = 0;
 };
 
@@ -362,6 +450,41 @@ struct c2_h : c2_base {
         else op.perform(ch->bt);
     }
 
+    /* Unfolded non-zero block lists of A and B and the contraction block
+       list built from them: the inputs of every per-C-block pair list
+       (gen_bto_contract2_nzorb_impl.h:354-463).  Built on first use and kept,
+       so that pair lists of many C blocks cost one list build each. */
+    struct lists {
+        block_list<NA> blax;
+        block_list<NB> blbx;
+        std::unique_ptr< gen_bto_contract2_block_list<N, M, K> > cbl;
+        lists(const dimensions<NA> &da, const dimensions<NB> &db) :
+            blax(da), blbx(db) {}
+    };
+    std::unique_ptr<lists> m_lists;
+
+    lists &get_lists() {
+        if (m_lists) return *m_lists;
+        gen_block_tensor_rd_ctrl<NA, block_tensor_i_traits<double> > ca(a->bt);
+        gen_block_tensor_rd_ctrl<NB, block_tensor_i_traits<double> > cb(b->bt);
+        dimensions<NA> bidimsa = a->bis.get_block_index_dims();
+        dimensions<NB> bidimsb = b->bis.get_block_index_dims();
+        std::unique_ptr<lists> l(new lists(bidimsa, bidimsb));
+        std::vector<size_t> v;
+        block_list<NA> bla(bidimsa);
+        block_list<NB> blb(bidimsb);
+        ca.req_nonzero_blocks(v);
+        for (size_t i = 0; i < v.size(); i++) bla.add(v[i]);
+        cb.req_nonzero_blocks(v);
+        for (size_t i = 0; i < v.size(); i++) blb.add(v[i]);
+        gen_bto_unfold_block_list<NA, btod_traits>(ca.req_const_symmetry(), bla).build(l->blax);
+        gen_bto_unfold_block_list<NB, btod_traits>(cb.req_const_symmetry(), blb).build(l->blbx);
+        l->cbl.reset(new gen_bto_contract2_block_list<N, M, K>(contr, bidimsa,
+            l->blax, bidimsb, l->blbx));
+        m_lists = std::move(l);
+        return *m_lists;
+    }
+
     /* Pair list of one C block: the same call sequence the schedule builder
        makes (gen_bto_contract2_nzorb_impl.h:354-463).  Output per pair:
        aia, acia, perm_a[NA], coeff_a, aib, acib, perm_b[NB], coeff_b
@@ -372,25 +495,13 @@ struct c2_h : c2_base {
         gen_block_tensor_rd_ctrl<NB, block_tensor_i_traits<double> > cb(b->bt);
         const symmetry<NA, double> &syma = ca.req_const_symmetry();
         const symmetry<NB, double> &symb = cb.req_const_symmetry();
-        dimensions<NA> bidimsa = a->bis.get_block_index_dims();
-        dimensions<NB> bidimsb = b->bis.get_block_index_dims();
         dimensions<NC> bidimsc = op.get_bis().get_block_index_dims();
-        std::vector<size_t> v;
-        block_list<NA> bla(bidimsa), blax(bidimsa);
-        block_list<NB> blb(bidimsb), blbx(bidimsb);
-        ca.req_nonzero_blocks(v);
-        for (size_t i = 0; i < v.size(); i++) bla.add(v[i]);
-        cb.req_nonzero_blocks(v);
-        for (size_t i = 0; i < v.size(); i++) blb.add(v[i]);
-        gen_bto_unfold_block_list<NA, btod_traits>(syma, bla).build(blax);
-        gen_bto_unfold_block_list<NB, btod_traits>(symb, blb).build(blbx);
-        gen_bto_contract2_block_list<N, M, K> cbl(contr, bidimsa, blax,
-            bidimsb, blbx);
+        lists &l = get_lists();
         index<NC> ic;
         abs_index<NC>::get_index((size_t)cabs, bidimsc, ic);
         gen_bto_contract2_clst_builder<N, M, K, btod_traits> bld(contr, syma,
-            symb, blax, blbx, bidimsc, ic);
-        bld.build_list(false, cbl);
+            symb, l.blax, l.blbx, bidimsc, ic);
+        bld.build_list(false, *l.cbl);
         const typename gen_bto_contract2_clst<N, M, K, double>::list_type &lst =
             bld.get_clst();
         size_t rec = 2 + NA + 1 + 2 + NB + 1, k = 0;
@@ -413,6 +524,50 @@ struct c2_h : c2_base {
             std::memcpy(&q[2 + NB], &cb_, 8);
         }
         return k;
+    }
+
+    /* Work of the whole schedule as the reference's task cost counts it
+       (gen_bto_contract2_block_impl.h:63-95, applied to the coalesced pair
+       list of every scheduled C block): per pair, the product of A's block
+       extents on the indices contracted with B, times the C block's size.
+       exact = that sum without the reference's per-pair integer division by
+       1000; ref_cost = the sum of the reference's own per-pair summands. */
+    void cost(int64_t *exact, int64_t *ref_cost) {
+        gen_block_tensor_rd_ctrl<NA, block_tensor_i_traits<double> > ca(a->bt);
+        gen_block_tensor_rd_ctrl<NB, block_tensor_i_traits<double> > cb(b->bt);
+        const symmetry<NA, double> &syma = ca.req_const_symmetry();
+        const symmetry<NB, double> &symb = cb.req_const_symmetry();
+        const block_index_space<NC> &bisc = op.get_bis();
+        dimensions<NC> bidimsc = bisc.get_block_index_dims();
+        dimensions<NA> bidimsa = a->bis.get_block_index_dims();
+        const sequence<NA + NB + NC, size_t> &conn = contr.get_conn();
+        lists &l = get_lists();
+        const assignment_schedule<NC, double> &sch = op.get_schedule();
+        int64_t ex = 0, rc = 0;
+        for (typename assignment_schedule<NC, double>::iterator it = sch.begin();
+             it != sch.end(); ++it) {
+            index<NC> ic;
+            abs_index<NC>::get_index(sch.get_abs_index(it), bidimsc, ic);
+            gen_bto_contract2_clst_builder<N, M, K, btod_traits> bld(contr,
+                syma, symb, l.blax, l.blbx, bidimsc, ic);
+            bld.build_list(false, *l.cbl);
+            size_t szc = bisc.get_block_dims(ic).get_size();
+            const typename gen_bto_contract2_clst<N, M, K, double>::list_type
+                &lst = bld.get_clst();
+            for (typename gen_bto_contract2_clst<N, M, K, double>::list_type::
+                    const_iterator p = lst.begin(); p != lst.end(); ++p) {
+                index<NA> ia;
+                abs_index<NA>::get_index(p->get_aindex_a(), bidimsa, ia);
+                dimensions<NA> dimsa = a->bis.get_block_dims(ia);
+                size_t c = 1;
+                for (size_t j = 0; j < NA; j++)
+                    if (conn[NC + j] >= NA + NC) c *= dimsa[j];
+                ex += (int64_t)(c * szc);
+                rc += (int64_t)(c * szc / 1000);
+            }
+        }
+        *exact = ex;
+        *ref_cost = rc;
     }
 };
 
@@ -553,6 +708,20 @@ int ref_bt_orbit(void *h, int64_t aidx, int64_t *canon, int32_t *perm,
     catch (std::exception &e) { g_err = e.what(); return -1; }
 }
 
+/* Seeded test inputs in the reference tensor (see fill_seeded): the group
+   elements (perm[N] and sign per element, the full closure of the tensor's
+   se_perm generators) are passed by the caller. */
+int ref_bt_fill_seeded(void *h, uint64_t seed, double scale, int ngroup,
+    const int32_t *perms, const int32_t *signs, int nthreads) {
+    try {
+#define CALL(k) fill_seeded<k>(h, seed, scale, ngroup, perms, signs, nthreads)
+        DISPATCH_ORDER(static_cast<bt_base*>(h)->order, CALL)
+#undef CALL
+        return 0;
+    } catch (libtensor::exception &e) { g_err = e.what(); return -1; }
+    catch (std::exception &e) { g_err = e.what(); return -1; }
+}
+
 void *ref_contract2_create(int n, int m, int k, const int32_t *permc,
     const int32_t *pairs, void *a, double ka, void *b, double kb, double kc) {
     try {
@@ -597,6 +766,14 @@ int ref_contract2_perform(void *op, void *c, int add, double d) {
 
 int64_t ref_contract2_clst(void *op, int64_t cabs, int64_t *out, int64_t cap) {
     try { return (int64_t)static_cast<c2_base*>(op)->clst(cabs, out, (size_t)cap); }
+    catch (libtensor::exception &e) { g_err = e.what(); return -1; }
+    catch (std::exception &e) { g_err = e.what(); return -1; }
+}
+
+/* Work of the schedule as the reference's task cost counts it; see
+   c2_h::cost. */
+int ref_contract2_cost(void *op, int64_t *exact, int64_t *ref_cost) {
+    try { static_cast<c2_base*>(op)->cost(exact, ref_cost); return 0; }
     catch (libtensor::exception &e) { g_err = e.what(); return -1; }
     catch (std::exception &e) { g_err = e.what(); return -1; }
 }

@@ -40,6 +40,8 @@ _SIGS = {
     "ref_contract2_result_bidims": (C.c_int, [_vp, _i64p]),
     "ref_contract2_perform": (C.c_int, [_vp, _vp, C.c_int, C.c_double]),
     "ref_contract2_clst": (C.c_int64, [_vp, C.c_int64, _i64p, C.c_int64]),
+    "ref_contract2_cost": (C.c_int, [_vp, _i64p, _i64p]),
+    "ref_bt_fill_seeded": (C.c_int, [_vp, C.c_uint64, C.c_double, C.c_int, _i32p, _i32p, C.c_int]),
     "ref_copy": (C.c_int, [_vp, _i32p, C.c_double, _vp, C.c_int, C.c_double]),
     "ref_add": (C.c_int, [C.c_int, C.POINTER(_vp), _i32p, _dblp, _vp, C.c_int, C.c_double]),
     "ref_dotprod": (C.c_int, [_vp, _i32p, _vp, _i32p, _dblp]),
@@ -144,6 +146,18 @@ class RefBT:
         lib().ref_bt_nonzero(self.h, buf.ctypes.data_as(_i64p), len(buf))
         return [int(x) for x in buf[:n]]
 
+    def fill_seeded(self, seed: int, scale: float = 1.0, nthreads: Optional[int] = None):
+        """Seeded, symmetrised test inputs in every canonical allowed block
+        (the distribution of oracle/restate.seeded_dense, generated inside
+        the reference library; bit-identical to the product's generator)."""
+        from oracle.restate import perm_group
+        n = self.order
+        grp = perm_group(n, self.spec.perms)
+        perms = _i32([v for p, _ in grp for v in p])
+        signs = _i32([1 if c > 0 else -1 for _, c in grp])
+        _chk(lib().ref_bt_fill_seeded(self.h, seed, scale, len(grp), perms, signs,
+                                      nthreads or os.cpu_count() or 1))
+
     def orbit(self, aidx):
         canon, coeff, osz = C.c_int64(), C.c_double(), C.c_int64()
         perm = (C.c_int32 * self.order)()
@@ -195,6 +209,15 @@ class RefContract2:
             out.append((int(o[0]), int(o[1]), tuple(int(x) for x in o[2:2 + na]), ca,
                         int(q[0]), int(q[1]), tuple(int(x) for x in q[2:2 + nb]), cb))
         return out
+
+    def cost(self):
+        """(exact, ref_cost): the schedule's work as the reference's task cost
+        counts it -- sum over scheduled C blocks and coalesced pairs of
+        K * |C block| -- without and with the reference's per-pair integer
+        division by 1000.  2 * exact is the algorithmic FP64 flop count."""
+        ex, rc = C.c_int64(), C.c_int64()
+        _chk(lib().ref_contract2_cost(self.h, C.byref(ex), C.byref(rc)))
+        return ex.value, rc.value
 
     def make_result(self) -> RefBT:
         h = lib().ref_contract2_make_result(self.h)

@@ -64,3 +64,35 @@ def test_one_iteration_matches_dense_algebra(gctx):
     E = float(np.sum(Rd * t0))
     assert abs(it.energy() - E) <= 1e-12 * abs(E)
     it.close()
+
+
+def test_split_precision_iteration_at_full_size(gctx):
+    """CCD iteration o=30 v=300 (blocks 15 / 50,50,50 per spin) with both
+    contractions in split precision (modular INT8, 13 moduli): the energy
+    within 1e-11 relative of the plain FP64 iteration on the same inputs, and
+    the permuted copy X = P(0,2,1,3) t bit-identical to the reference's
+    btod_copy."""
+    from libtensor_b200 import spec as S
+    from libtensor_b200.spec import permuted_spec
+    from oracle import refapi as R
+    cfg = S.LADDER_CCD
+    energies = {}
+    for mode, nslices in ((MODE_PLAIN_FP64, 0), (MODE_OZAKI_CRT, 13)):
+        it = CCDIteration(gctx, cfg.occ_blocks, cfg.vir_blocks, mode, nslices)
+        it.step()
+        energies[mode] = it.energy()
+        if mode == MODE_PLAIN_FP64 and R.available():
+            perm = (0, 2, 1, 3)
+            rt = R.RefBT(it.t.spec)
+            rt.fill_seeded(7, 0.01)
+            rx = R.RefBT(permuted_spec(it.t.spec, perm))
+            R.ref_copy(rt, perm, 1.0, rx)
+            for bidx, blk in it.X.blocks(it.X.download()):
+                want = rx.get_block(bidx, blk.shape)
+                assert np.array_equal(blk.view(np.uint64), want.view(np.uint64)), bidx
+            rt.close()
+            rx.close()
+        it.close()
+    e64, e_split = energies[MODE_PLAIN_FP64], energies[MODE_OZAKI_CRT]
+    assert e64 != 0.0
+    assert abs(e_split - e64) <= 1e-11 * abs(e64), (e64, e_split)

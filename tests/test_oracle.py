@@ -45,6 +45,27 @@ def test_restated_generator_is_bit_identical(hctx, spec):
     assert list(t.abs_idx) == X.canonical_blocks(spec)
 
 
+@pytest.mark.parametrize("spec", [S.LADDER_SMALL.t_spec(), S.LADDER_SMALL.v_spec(),
+                                  S.RING_D2H_SMALL.t_spec(), S.RING_D2H_SMALL.w_spec()],
+                         ids=["t ladder", "V ladder", "t ring", "W ring"])
+def test_reference_side_generator_is_bit_identical(spec):
+    """The generator inside the reference library (seeded inputs for a
+    CPU-only caller) writes the restatement's bits into every canonical
+    allowed block, and only into those."""
+    r = R.RefBT(spec)
+    r.fill_seeded(99, 0.5, nthreads=3)
+    dense = X.seeded_dense(spec, 99, 0.5)
+    canon = X.canonical_blocks(spec)
+    assert sorted(r.nonzero()) == canon
+    bid = spec.bidims()
+    for a in canon:
+        bidx = X._unabs(a, bid)
+        want = X.block_view(spec, dense, bidx)
+        got = r.get_block(bidx, want.shape)
+        assert np.array_equal(got.view(np.uint64), np.ascontiguousarray(want).view(np.uint64))
+    r.close()
+
+
 def test_generator_symmetry():
     spec = S.LADDER_SMALL.t_spec()
     d = X.seeded_dense(spec, 7, 1.0)
