@@ -82,7 +82,19 @@ int ltg_version(void);
 /* ---- context --------------------------------------------------------- */
 int ltg_ctx_create(int device, ltg_ctx **out);
 int ltg_ctx_destroy(ltg_ctx *ctx);
+/* Waits for the context's stream.  Returns LTG_ERR_TIMEOUT (once) when a
+ * bounded device wait of a split-precision products kernel gave up since the
+ * last report; that call's results are invalid, the context stays usable. */
 int ltg_ctx_synchronize(ltg_ctx *ctx);
+/* Limit of one pipeline wait (mbarrier) inside the tcgen05 products kernels,
+ * in nanoseconds of wall time; default 2e9 (2 s).  When a wait runs out, the
+ * kernel stops its work, lets its bulk copies and MMAs in flight finish, frees
+ * its tensor memory and returns; the host reports LTG_ERR_TIMEOUT.  0 means no
+ * waiting at all (a wait whose phase has not completed at its first test gives
+ * up), which makes the unwind path testable.  No reference counterpart (the
+ * reference runs on the CPU and has no device waits). */
+int ltg_ctx_set_wait_limit(ltg_ctx *ctx, uint64_t ns);
+int ltg_ctx_wait_limit(ltg_ctx *ctx, uint64_t *ns);
 /* Underlying cudaStream_t of the context (for event timing by callers). */
 int ltg_ctx_stream(ltg_ctx *ctx, void **stream);
 /* Host threads used for schedule construction (libutil::thread_pool role). */
@@ -286,8 +298,12 @@ int ltg_dotprod_async(ltg_bt *a, const int32_t *perma, ltg_bt *b,
  * elements each): n is limited to 2^30 elements and larger n returns
  * LTG_ERR_BAD_ARG.  All calls on a device share that array, so calls that
  * overlap in time race and must be serialised by the caller.  The first call
- * on a device also looks up the array's address; make it before any stream
- * capture on that device.  The sum order depends only on n. */
+ * on a device is not allocation-free: it loads the library's module for this
+ * entry point (device memory for the array and the kernels) and looks up the
+ * array's address.  Make one call with n > 0 early on each device, while
+ * memory is free and before any stream capture on it; later calls allocate
+ * nothing.  Not usable after cudaDeviceReset.  The sum order depends only
+ * on n. */
 int ltg_dot_noalloc(const double *x, const double *y, int64_t n, void *stream,
                     double *out);
 /* a *= c  (btod_scale) */

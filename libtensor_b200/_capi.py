@@ -53,6 +53,8 @@ _SIGS = {
     "ltg_ctx_synchronize": (C.c_int, [c_vp]),
     "ltg_ctx_stream": (C.c_int, [c_vp, C.POINTER(c_vp)]),
     "ltg_ctx_set_host_threads": (C.c_int, [c_vp, C.c_int]),
+    "ltg_ctx_set_wait_limit": (C.c_int, [c_vp, C.c_uint64]),
+    "ltg_ctx_wait_limit": (C.c_int, [c_vp, C.POINTER(C.c_uint64)]),
     "ltg_ctx_launch_count": (C.c_int, [c_vp, c_i64p]),
     "ltg_bt_create": (C.c_int, [c_vp, C.POINTER(ltg_bt_spec), C.POINTER(c_vp)]),
     "ltg_bt_create_permuted": (C.c_int, [c_vp, c_i32p, C.POINTER(c_vp)]),

@@ -46,6 +46,7 @@ def _nvcc():
 
 def _compile(src, obj, verbose):
     path = os.path.join(CSRC, src)
+    t_src = os.path.getmtime(path)
     if src.endswith(".cpp"):
         cmd = [os.environ.get("CXX", "g++"), *CXX_FLAGS, "-I/usr/local/cuda/include", "-c", path, "-o", obj]
     else:
@@ -55,6 +56,8 @@ def _compile(src, obj, verbose):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"compile failed: {src}\n{r.stdout}\n{r.stderr}")
+    if os.path.getmtime(path) != t_src:          # edited while compiling: not up to date
+        os.utime(obj, (t_src, t_src))
     return obj
 
 
@@ -82,7 +85,9 @@ def build(verbose=False, force=False):
         for f in [ex.submit(_compile, s, o, verbose) for s, o in jobs]:
             f.result()
     if jobs or not os.path.exists(LIB):
-        cmd = [_nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"]
+        # --no-undefined: an object compiled from an older source (a changed
+        # launcher signature) fails the link instead of loading with a hole
+        cmd = [_nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart", "-Xlinker", "--no-undefined"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

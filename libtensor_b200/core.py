@@ -76,6 +76,17 @@ class Context:
         check(lib().ltg_ctx_kernel_times(self.h, ms, n))
         return {name: (ms[i], n[i]) for i, name in enumerate(self.KERNELS) if n[i]}
 
+    def set_wait_limit(self, ns: int):
+        """Limit of one pipeline wait inside the tcgen05 products kernels (ns;
+        default 2e9).  A wait that runs out makes the call's kernel unwind and
+        the next call or synchronize() raise LTG_ERR_TIMEOUT; 0 = no waiting."""
+        check(lib().ltg_ctx_set_wait_limit(self.h, int(ns)))
+
+    def wait_limit(self) -> int:
+        v = C.c_uint64()
+        check(lib().ltg_ctx_wait_limit(self.h, C.byref(v)))
+        return v.value
+
     def set_host_threads(self, n: int):
         check(lib().ltg_ctx_set_host_threads(self.h, n))
 

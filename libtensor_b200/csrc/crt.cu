@@ -46,7 +46,7 @@ constexpr int kStageBytes = kKbPerStage * kSubBytes;     // 32 KB
 constexpr int kMaxStages = 8;
 constexpr int kEpiWarps = 8;                        // two per TMEM lane quarter
 constexpr int kGemmThreads = 32 * (kEpiWarps + 2);  // + bulk-copy producer + MMA issuer
-constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s per barrier wait
+constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s: the drain waits after an abort
 constexpr double kMagicD = 6755399441055744.0;      // 1.5 * 2^52: round-to-integer constant
 constexpr float kMagicF = 12582912.0f;              // 1.5 * 2^23
 constexpr int32_t kNoExp = -1000000;                // exponent of a row with no non-zero element
@@ -365,9 +365,19 @@ __device__ __forceinline__ uint64_t global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded wait for the phase with the given parity (false on timeout or abort).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+// Bounded wait for the phase with the given parity: false when it has not
+// completed within limit_ns of wall time (try_wait itself may suspend the
+// thread, so the bound is on time, not on iterations) or when another role
+// aborted.  limit_ns == 0 tests the phase once and does not wait.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort,
+                                          uint64_t limit_ns) {
     const uint32_t a = smem_u32(bar);
+    if (limit_ns == 0) {                 // no time at all: one non-blocking test
+        uint32_t done;
+        asm volatile("{ .reg .pred p; mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        return done != 0;
+    }
     uint64_t t0 = 0;
     for (uint32_t i = 0;; i++) {
         uint32_t done;
@@ -378,7 +388,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
             if (*abort) return false;
             const uint64_t t = global_ns();
             if (t0 == 0) t0 = t;
-            else if (t - t0 > kWaitNs) return false;
+            else if (t - t0 > limit_ns) return false;
         }
     }
 }
@@ -426,7 +436,8 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 __global__ void __launch_bounds__(kGemmThreads, 1)
 crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict__ res,
                 const DCrtTask *__restrict__ tasks, const DCrtItem *__restrict__ items, int32_t nitems,
-                uint8_t *__restrict__ out, const CrtParams cp, int32_t stages, int32_t *err) {
+                uint8_t *__restrict__ out, const CrtParams cp, int32_t stages, int32_t *err,
+                uint64_t wait_ns) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], drain_bar;
@@ -472,7 +483,7 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                         const uint8_t *ga = res + t.xres + (int64_t)(item.x0 / kXRows) * xt;
                         const uint8_t *gb = res + t.yres + (int64_t)(item.y0 / item.nt) * nkb * L * ybytes;
                         for (int kb = 0; kb < nkb; kb += kKbPerStage) {
-                            if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s)) { ok = false; break; }
+                            if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s, wait_ns)) { ok = false; break; }
                             const int nsub = min(kKbPerStage, nkb - kb);
                             const uint32_t fb = smem_u32(&full_bar[st]);
                             mbar_expect_tx(&full_bar[st], (uint32_t)nsub * ((uint32_t)(item.nx * kXTile) + ybytes));
@@ -492,10 +503,13 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
             if (!ok) {
                 abort_s = 1;
                 atomicExch(err, 7);
-                volatile int never = 0;
-                for (int i = 0; i < stages; i++)
-                    if (armed[i] >= 0) (void)mbar_wait(&full_bar[i], (uint32_t)armed[i], &never);
             }
+            // Every issued copy has landed before the CTA leaves (after an
+            // abort the MMA warp no longer consumes them); in a normal run
+            // each stage's last phase has completed already.
+            volatile int never = 0;
+            for (int i = 0; i < stages; i++)
+                if (armed[i] >= 0) (void)mbar_wait(&full_bar[i], (uint32_t)armed[i], &never, kWaitNs);
         }
     } else if (warp == kEpiWarps + 1) {
         // ------------------------------------------------ MMA issuer
@@ -512,8 +526,8 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                     // a two-tile fill takes both slots, a one-tile fill slot rr
                     const int s0 = item.nx == 2 ? 0 : rr;
                     // the epilogue has read the slots' previous fills
-                    if (uses[s0] > 0 && !mbar_wait(&acce_bar[s0], (uses[s0] - 1) & 1, &abort_s)) { ok = false; break; }
-                    if (item.nx == 2 && uses[1] > 0 && !mbar_wait(&acce_bar[1], (uses[1] - 1) & 1, &abort_s)) {
+                    if (uses[s0] > 0 && !mbar_wait(&acce_bar[s0], (uses[s0] - 1) & 1, &abort_s, wait_ns)) { ok = false; break; }
+                    if (item.nx == 2 && uses[1] > 0 && !mbar_wait(&acce_bar[1], (uses[1] - 1) & 1, &abort_s, wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -523,7 +537,7 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                     for (int ti = item.t_begin; ti < item.t_end && ok; ti++) {
                         const int nkb = tasks[ti].nkb;
                         for (int kb = 0; kb < nkb; kb += kKbPerStage) {
-                            if (!mbar_wait(&full_bar[st], ph, &abort_s)) { ok = false; break; }
+                            if (!mbar_wait(&full_bar[st], ph, &abort_s, wait_ns)) { ok = false; break; }
                             tc_fence_after();
                             const int nsub = min(kKbPerStage, nkb - kb);
                             for (int j = 0; j < nsub; j++) {
@@ -549,7 +563,7 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                 atomicExch(err, 7);
                 volatile int never = 0;
                 umma_commit(&drain_bar);
-                (void)mbar_wait(&drain_bar, 0, &never);
+                (void)mbar_wait(&drain_bar, 0, &never, kWaitNs);
             }
         }
     } else {
@@ -565,8 +579,8 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
             const DCrtItem item = items[it];
             for (int l = 0; l < L; l++) {
                 const int s0 = item.nx == 2 ? 0 : rr;
-                ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[s0], uses[s0] & 1, &abort_s));
-                if (ok && item.nx == 2) ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[1], uses[1] & 1, &abort_s));
+                ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[s0], uses[s0] & 1, &abort_s, wait_ns));
+                if (ok && item.nx == 2) ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar[1], uses[1] & 1, &abort_s, wait_ns));
                 if (!ok) break;
                 tc_fence_after();
                 const double minv = cp.minv_d[l];
@@ -777,7 +791,7 @@ cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int3
 
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
                             const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp,
-                            int32_t *err, cudaStream_t s) {
+                            int32_t *err, uint64_t wait_ns, cudaStream_t s) {
     if (nitems <= 0) return cudaSuccess;
     int stages = (200 * 1024) / kStageBytes;
     if (stages > kMaxStages) stages = kMaxStages;
@@ -785,7 +799,8 @@ cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const D
     cudaError_t e = cudaFuncSetAttribute(crt_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = nitems < num_sms() ? nitems : num_sms();
-    crt_gemm_kernel<<<grid, kGemmThreads, smem, s>>>(panels, res, tasks, items, nitems, out, cp, stages, err);
+    crt_gemm_kernel<<<grid, kGemmThreads, smem, s>>>(panels, res, tasks, items, nitems, out, cp, stages, err,
+                                                      wait_ns);
     return cudaGetLastError();
 }
 

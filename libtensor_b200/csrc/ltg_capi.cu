@@ -113,6 +113,12 @@ struct ltg_ctx {
     DevBuf scratch_counter;      // work-queue counters of persistent launches
     DevBuf dot_out;              // device scalar for synchronous dot products
     KernelTiming timing;
+    // Bounded device waits of the tcgen05 kernels: the limit of one pipeline
+    // wait, and the error word a kernel sets when a wait gave up (copied to
+    // the pinned host word after every such launch and at synchronisation).
+    uint64_t wait_ns = 2000000000ull;
+    DevBuf wait_err;
+    int32_t *wait_err_host = nullptr;
 };
 
 static std::atomic<uint64_t> g_bt_uid{1};
@@ -156,11 +162,10 @@ struct ContractExec {
 struct OzExec {
     int kind = 0, S = 0, chunk_kb = 1, npanels = 0, max_rows_pad = 0, nitems = 0;
     int64_t src_elems = 0, slice_bytes = 0;   // operand elements read, slice bytes written
-    DevBuf panels, slices, exps, tasks, cblks, items, err;
+    DevBuf panels, slices, exps, tasks, cblks, items;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
-    int32_t *err_host = nullptr;     // pinned copy of the device error word
-    ~OzExec() { if (err_host) cudaFreeHost(err_host); }
+
 };
 
 // Device arrays of one modular split-precision contraction (crt.cu).
@@ -169,11 +174,10 @@ struct CrtExec {
     int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0, ngroups = 0, nunits = 0;
     int64_t src_elems = 0, res_bytes = 0;   // operand elements read per pass, residue bytes written
     double scale = 1.0;                     // kc (and d in add mode) times the pair coefficients' scale
-    DevBuf panels, units, tasks, items, cblks, comps, ctab, cells, gidx, ex, ey, res, out, err;
+    DevBuf panels, units, tasks, items, cblks, comps, ctab, cells, gidx, ex, ey, res, out;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
-    int32_t *err_host = nullptr;
-    ~CrtExec() { if (err_host) cudaFreeHost(err_host); }
+
 };
 
 struct ltg_plan {
@@ -692,10 +696,6 @@ OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, doubl
     upload_vec(ex->tasks, dt, s);
     upload_vec(ex->cblks, dc, s);
     upload_vec(ex->items, items, s);
-    ex->err.alloc(sizeof(int32_t));
-    LTG_CUDA(cudaMemsetAsync(ex->err.p, 0, sizeof(int32_t), s));
-    LTG_CUDA(cudaMallocHost(&ex->err_host, sizeof(int32_t)));
-    *ex->err_host = 0;
     // blocks of C outside the schedule (zeroed in assign mode)
     std::vector<char> in_sched(c->h.blk_abs.size(), 0);
     for (int64_t cabs : pl->plan.schedule) {
@@ -1557,10 +1557,6 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     upload_vec(ex->ctab, ctab, s);
     upload_vec(ex->cells, cells, s);
     ex->scale = post;
-    ex->err.alloc(sizeof(int32_t));
-    LTG_CUDA(cudaMemsetAsync(ex->err.p, 0, sizeof(int32_t), s));
-    LTG_CUDA(cudaMallocHost(&ex->err_host, sizeof(int32_t)));
-    *ex->err_host = 0;
     std::vector<char> in_sched(c->h.blk_abs.size(), 0);
     for (int64_t cabs : pl->plan.schedule) {
         int64_t sl = c->h.slot_of[cabs];
@@ -1896,6 +1892,28 @@ extern "C" {
 const char *ltg_last_error(void) { return g_last_error.c_str(); }
 int ltg_version(void) { return 100; }
 
+// Device-wait errors.  A tcgen05 kernel whose pipeline wait gave up sets the
+// context's error word (7) and unwinds; the word is copied to pinned host
+// memory after each such launch (outside graph capture) and reported as
+// LTG_ERR_TIMEOUT by the next contraction call or by ltg_ctx_synchronize,
+// which then clear it.
+static void fetch_device_wait(ltg_ctx *ctx) {
+    if (!ctx->capturing)
+        LTG_CUDA(cudaMemcpyAsync(ctx->wait_err_host, ctx->wait_err.p, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+}
+
+static void report_device_wait(ltg_ctx *ctx) {
+    if (*ctx->wait_err_host == 0) return;
+    // every copy of the word still in flight lands before it is cleared
+    LTG_CUDA(cudaStreamSynchronize(ctx->stream));
+    LTG_CUDA(cudaMemsetAsync(ctx->wait_err.p, 0, sizeof(int32_t), ctx->stream));
+    LTG_CUDA(cudaStreamSynchronize(ctx->stream));
+    *ctx->wait_err_host = 0;
+    throw error(kErrTimeout, "a bounded device wait of a split-precision products kernel gave up (limit " +
+                                 std::to_string(ctx->wait_ns) + " ns); its results are invalid");
+}
+
 int ltg_ctx_create(int device, ltg_ctx **out) {
     return guard([&] {
         if (!out) throw error(kErrBadArg, "null output");
@@ -1909,6 +1927,10 @@ int ltg_ctx_create(int device, ltg_ctx **out) {
             LTG_CUDA(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
             c->scratch_counter.alloc(64 * sizeof(int32_t));
             c->dot_out.alloc(sizeof(double));
+            c->wait_err.alloc(sizeof(int32_t));
+            LTG_CUDA(cudaMemset(c->wait_err.p, 0, sizeof(int32_t)));
+            LTG_CUDA(cudaMallocHost(&c->wait_err_host, sizeof(int32_t)));
+            *c->wait_err_host = 0;
         }
         unsigned hc = std::thread::hardware_concurrency();
         c->host_threads = hc ? (int)hc : 1;
@@ -1927,13 +1949,28 @@ int ltg_ctx_destroy(ltg_ctx *ctx) {
             }
             for (cudaEvent_t e : ctx->timing.pool) cudaEventDestroy(e);
             cudaStreamDestroy(ctx->stream);
+            if (ctx->wait_err_host) cudaFreeHost(ctx->wait_err_host);
         }
         delete ctx;
     });
 }
 
 int ltg_ctx_synchronize(ltg_ctx *ctx) {
-    return guard([&] { check_ctx(ctx); if (ctx->device >= 0) LTG_CUDA(cudaStreamSynchronize(ctx->stream)); });
+    return guard([&] {
+        check_ctx(ctx);
+        if (ctx->device < 0) return;
+        fetch_device_wait(ctx);
+        LTG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (!ctx->capturing) report_device_wait(ctx);
+    });
+}
+
+int ltg_ctx_set_wait_limit(ltg_ctx *ctx, uint64_t ns) {
+    return guard([&] { check_ctx(ctx); ctx->wait_ns = ns; });
+}
+
+int ltg_ctx_wait_limit(ltg_ctx *ctx, uint64_t *ns) {
+    return guard([&] { check_ctx(ctx); if (!ns) throw error(kErrBadArg, "null output"); *ns = ctx->wait_ns; });
 }
 
 int ltg_ctx_stream(ltg_ctx *ctx, void **stream) {
@@ -2347,12 +2384,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
         cudaStream_t s = ctx->stream;
         if (mode == LTG_MODE_OZAKI_CRT) {
             CrtExec *cx = prepare_crt(plan, c, nslices > 0 ? nslices : 13, ka, kb, kc, add, d);
-            if (*cx->err_host != 0) {
-                int code = *cx->err_host;
-                *cx->err_host = 0;
-                throw error(code == kErrTimeout ? kErrTimeout : kErrCuda,
-                            "a bounded device wait of the modular split-precision kernel gave up");
-            }
+            report_device_wait(ctx);
             if (!add)
                 for (auto &r : cx->zero_ranges)
                     LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
@@ -2368,7 +2400,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
             LTG_CUDA(launch_crt_gemm(cx->panels.as<DCrtPanel>(), cx->res.as<uint8_t>(), cx->tasks.as<DCrtTask>(),
                                      cx->items.as<DCrtItem>(), cx->nitems, cx->out.as<uint8_t>(), cx->cp,
-                                     cx->err.as<int32_t>(), s));
+                                     ctx->wait_err.as<int32_t>(), ctx->wait_ns, s));
             t_gemm.done();
             TimedLaunch t_comb(ctx, LTG_KERNEL_OZ_COMBINE);
             LTG_CUDA(launch_crt_combine(cx->panels.as<DCrtPanel>(), cx->items.as<DCrtItem>(), cx->nitems,
@@ -2378,8 +2410,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                                         cx->scale, cx->cp, s));
             t_comb.done();
             ctx->launches += 2 + (cx->nunits > 0 ? 2 : 0) + (cx->nitems > 0 ? 2 : 0);
-            if (!ctx->capturing)
-                LTG_CUDA(cudaMemcpyAsync(cx->err_host, cx->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            fetch_device_wait(ctx);
             if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
             for (int64_t sl : cx->sched_slots) c->h.nonzero[sl] = 1;
             return;
@@ -2388,12 +2419,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             if (mode < LTG_MODE_OZAKI_BF16 || mode > LTG_MODE_OZAKI_INT8) throw error(kErrBadArg, "unknown mode");
             int S = nslices > 0 ? nslices : (mode == LTG_MODE_OZAKI_FP8 ? 8 : 7);
             OzExec *ox = prepare_ozaki(plan, c, mode, S, ka, kb, kc, add, d);
-            if (*ox->err_host != 0) {
-                int code = *ox->err_host;
-                *ox->err_host = 0;
-                throw error(code == kErrTimeout ? kErrTimeout : kErrCuda,
-                            "a bounded device wait of the split-precision kernel gave up");
-            }
+            report_device_wait(ctx);
             if (!add)
                 for (auto &r : ox->zero_ranges)
                     LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
@@ -2406,11 +2432,10 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             LTG_CUDA(launch_oz_gemm(ox->kind, ox->panels.as<DPanel>(), ox->slices.as<uint8_t>(), ox->tasks.as<DOzTask>(),
                                     ox->cblks.as<DCBlock>(), ox->items.as<DItem>(), ox->nitems,
                                     ox->exps.as<int32_t>(), c->arena.as<double>(), add, ox->S, ox->chunk_kb,
-                                    ox->err.as<int32_t>(), s));
+                                    ctx->wait_err.as<int32_t>(), ctx->wait_ns, s));
             t_gemm.done();
             ctx->launches += 2;
-            if (!ctx->capturing)
-                LTG_CUDA(cudaMemcpyAsync(ox->err_host, ox->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            fetch_device_wait(ctx);
             if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
             for (int64_t sl : ox->sched_slots) c->h.nonzero[sl] = 1;
             return;

@@ -271,7 +271,7 @@ cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int
     const double *a, const double *b, uint8_t *slices, int32_t *exps, int32_t S, cudaStream_t s);
 cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices, const DOzTask *tasks,
     const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps, double *c,
-    int32_t add, int32_t S, int32_t chunk_kb, int32_t *err, cudaStream_t s);
+    int32_t add, int32_t S, int32_t chunk_kb, int32_t *err, uint64_t wait_ns, cudaStream_t s);
 // Per kind: first-slice bits, further-slice bits, element bytes, k elements
 // per 64-byte k block, bound of one slice product.
 void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod);
@@ -288,7 +288,7 @@ cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int3
     uint8_t *res, const CrtParams &cp, cudaStream_t s);
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
     const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp, int32_t *err,
-    cudaStream_t s);
+    uint64_t wait_ns, cudaStream_t s);
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
     const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab, const DCrtCell *cells,
     const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey, double *c,

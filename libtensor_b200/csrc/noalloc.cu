@@ -2,9 +2,9 @@
 //
 // Variant of the dot kernel of elementwise.cu (per-unit partial sums followed
 // by one fixed-order reduction) whose partial sums and result live in a
-// file-scope device array instead of memory obtained from cudaMalloc.  The
-// call allocates nothing, on the device or through any library, so it can be
-// used by callers that must not allocate:
+// file-scope device array instead of memory obtained from cudaMalloc.  After
+// the first call on a device, a call allocates nothing, on the device or
+// through any library, so it can be used by callers that must not allocate:
 //   - error paths after an out-of-memory failure (for example computing a
 //     residual norm to decide whether an iteration may continue), where a new
 //     allocation would fail again;
@@ -25,9 +25,15 @@
 //   - nothing in the array has to start at zero: every partial a call reads
 //     was written earlier in the same call, and the result slot is written by
 //     the reduction (or set to zero by cudaMemsetAsync when n == 0);
-//   - the first call on a device looks the array's address up with
-//     cudaGetSymbolAddress, with that device current; make that first call
-//     before any stream capture on the device.
+//   - the first call on a device is not allocation-free: with CUDA's lazy
+//     module loading it loads this file's module (the array and the two
+//     kernels' code take device memory then), and it looks the array's
+//     address up with cudaGetSymbolAddress, with that device current.  Make
+//     one call with n > 0 early on each device, while memory is still free
+//     and before any stream capture on the device;
+//   - the address is kept per device ordinal for the life of the process;
+//     after cudaDeviceReset the module may be loaded at another address, so
+//     the entry point must not be used after a device reset.
 //
 // The summation order depends only on n (units in index order, a fixed tree
 // inside each CTA), so repeated calls give bit-identical results.
@@ -144,8 +150,10 @@ extern "C" int ltg_dot_noalloc(const double *x, const double *y, int64_t n, void
         e = cudaMemsetAsync(result, 0, sizeof(double), s);
         if (e != cudaSuccess) return cuda_fail("cudaMemsetAsync", e);
     } else {
-        int nsm = 148;
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        int nsm = 0;
+        e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return cuda_fail("cudaDeviceGetAttribute", e);
+        if (nsm < 1) nsm = 1;
         const int64_t grid = nunits < 8LL * nsm ? nunits : 8LL * nsm;
         dot_units_kernel<<<(unsigned)grid, kThreads, 0, s>>>(x, y, n, nunits);
         e = cudaGetLastError();

@@ -25,9 +25,12 @@
 // Only levels l <= S-1 are formed: S(S+1)/2 slice products per k step.
 //
 // Warp roles (192 threads): warps 0-3 epilogue (TMEM lanes 0-127, one C row
-// per thread), warp 4 TMA producer, warp 5 MMA issuer.  Operand tiles move
-// with cp.async.bulk.tensor in 32-byte swizzled k blocks (one MMA k step per
-// pipeline stage, so even 8 slices leave room for 4 stages); no multicast.
+// per thread), warp 4 bulk-copy producer, warp 5 MMA issuer.  Operand tiles
+// are stored in global memory as the exact shared-memory images the MMA reads
+// (K-major core matrices, no swizzle), so each one moves with a single 1-D
+// cp.async.bulk copy completing on the stage's mbarrier (no tensor maps, no
+// multicast); one MMA k step per pipeline stage, so even 8 slices leave room
+// for 4 stages.
 // Every mbarrier wait is bounded in time and reports through *err.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -54,7 +57,7 @@ constexpr int kATile = kBM * kRowBytes;   // 4 KB per A slice per stage
 constexpr int kBTile = kBN * kRowBytes;   // 2 KB per B slice per stage
 constexpr int kThreads = 192;
 constexpr int kMaxStages = 8;
-constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s per barrier wait
+constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s: the drain waits after an abort
 
 __device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_t *ext,
                                                 const int32_t *str) {
@@ -204,11 +207,18 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // Wait for the phase with the given parity to complete, for at most
-// kWaitNs of wall time (try_wait itself may suspend the thread, so the bound
+// limit_ns of wall time (try_wait itself may suspend the thread, so the bound
 // is on time, not on iterations); false on timeout or when another role
-// aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+// aborted.  limit_ns == 0 tests the phase once and does not wait.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort,
+                                          uint64_t limit_ns) {
     const uint32_t a = smem_u32(bar);
+    if (limit_ns == 0) {                 // no time at all: one non-blocking test
+        uint32_t done;
+        asm volatile("{ .reg .pred p; mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        return done != 0;
+    }
     uint64_t t0 = 0;
     for (uint32_t i = 0;; i++) {
         uint32_t done;
@@ -219,7 +229,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
             if (*abort) return false;
             const uint64_t t = global_ns();
             if (t0 == 0) t0 = t;
-            else if (t - t0 > kWaitNs) return false;
+            else if (t - t0 > limit_ns) return false;
         }
     }
 }
@@ -321,7 +331,7 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
                const DOzTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
                const DItem *__restrict__ items, int32_t nitems, const int32_t *__restrict__ exps,
                double *__restrict__ Cp, int32_t add, int32_t stages, int32_t chunk_kb,
-               int32_t beta0, int32_t beta, int32_t kbe, int32_t *err) {
+               int32_t beta0, int32_t beta, int32_t kbe, int32_t *err, uint64_t wait_ns) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte aligned stage buffers: [stage][A slices | B slices]
     uint8_t *smem = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -375,7 +385,7 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
                     const uint8_t *ga = slices + panels[t.pa].slice_off + (int64_t)(item.m0 / kBM) * nkb * S * kATile;
                     const uint8_t *gb = slices + panels[t.pb].slice_off + (int64_t)(item.n0 / kBN) * nkb * S * kBTile;
                     for (int kb = 0; kb < nkb; kb++) {
-                        if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s)) { ok = false; break; }
+                        if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s, wait_ns)) { ok = false; break; }
                         const uint32_t sa = smem0 + st * kStageBytes;
                         const uint32_t sb = sa + S * kATile;
                         const uint32_t fb = smem_u32(&full_bar[st]);
@@ -390,11 +400,13 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
             if (!ok) {
                 abort_s = 1;
                 atomicExch(err, 7);
-                // let the copies already in flight land before the CTA exits
-                volatile int never = 0;
-                for (int i = 0; i < stages; i++)
-                    if (armed_parity[i] >= 0) (void)mbar_wait(&full_bar[i], (uint32_t)armed_parity[i], &never);
             }
+            // let the copies already in flight land before the CTA exits (after
+            // an abort the MMA warp no longer consumes them; in a normal run
+            // each stage's last phase has completed already)
+            volatile int never = 0;
+            for (int i = 0; i < stages; i++)
+                if (armed_parity[i] >= 0) (void)mbar_wait(&full_bar[i], (uint32_t)armed_parity[i], &never, kWaitNs);
         }
     } else if (warp == 5) {
         // ------------------------------------------------ MMA issuer
@@ -412,13 +424,13 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
                     for (int kb0 = 0; kb0 < nkb && ok; kb0 += chunk_kb) {
                         // the accumulators are free once the previous drain was read
                         if (ndrain > 0) {
-                            if (!mbar_wait(&acce_bar, accph, &abort_s)) { ok = false; break; }
+                            if (!mbar_wait(&acce_bar, accph, &abort_s, wait_ns)) { ok = false; break; }
                             accph ^= 1;
                         }
                         tc_fence_after();
                         const int kb1 = min(nkb, kb0 + chunk_kb);
                         for (int kb = kb0; kb < kb1; kb++) {
-                            if (!mbar_wait(&full_bar[st], ph, &abort_s)) { ok = false; break; }
+                            if (!mbar_wait(&full_bar[st], ph, &abort_s, wait_ns)) { ok = false; break; }
                             tc_fence_after();
                             const uint32_t a0 = smem0 + st * kStageBytes;
                             const uint32_t b0 = a0 + S * kATile;
@@ -463,7 +475,7 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
                 // the MMAs already issued must finish before TMEM is freed
                 volatile int never = 0;
                 umma_commit(&drain_bar);
-                (void)mbar_wait(&drain_bar, 0, &never);
+                (void)mbar_wait(&drain_bar, 0, &never, kWaitNs);
             }
         }
     } else {
@@ -492,7 +504,7 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
                 const int32_t *eb = exps + pb.exp_off + item.n0;
                 for (int kb0 = 0; kb0 < nkb; kb0 += chunk_kb) {
                     // warp-uniform outcome: tcgen05.ld below is .sync.aligned
-                    ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar, accph, &abort_s));
+                    ok = __all_sync(0xffffffffu, mbar_wait(&accf_bar, accph, &abort_s, wait_ns));
                     if (!ok) break;
                     accph ^= 1;
                     tc_fence_after();
@@ -551,7 +563,7 @@ int g_nsm = 0;
 template<int KIND, int S>
 cudaError_t launch_gemm_s(const DPanel *panels, const uint8_t *slices, const DOzTask *tasks, const DCBlock *cblks,
                           const DItem *items, int32_t nitems, const int32_t *exps, double *c, int32_t add,
-                          int32_t chunk_kb, int32_t *err, cudaStream_t s) {
+                          int32_t chunk_kb, int32_t *err, uint64_t wait_ns, cudaStream_t s) {
     int beta0, beta, esz, kbe;
     int64_t mp;
     oz_kind_params(KIND, &beta0, &beta, &esz, &kbe, &mp);
@@ -574,16 +586,16 @@ cudaError_t launch_gemm_s(const DPanel *panels, const uint8_t *slices, const DOz
     int grid = nitems < g_nsm ? nitems : g_nsm;
     if (grid < 1) return cudaSuccess;
     oz_gemm_kernel<KIND, S><<<grid, kThreads, smem, s>>>(panels, slices, tasks, cblks, items, nitems, exps, c, add,
-                                                        stages, chunk_kb, beta0, beta, kbe, err);
+                                                        stages, chunk_kb, beta0, beta, kbe, err, wait_ns);
     return cudaGetLastError();
 }
 
 template<int KIND>
 cudaError_t launch_gemm_k(int S, const DPanel *panels, const uint8_t *slices, const DOzTask *tasks,
                           const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps, double *c,
-                          int32_t add, int32_t chunk_kb, int32_t *err, cudaStream_t s) {
+                          int32_t add, int32_t chunk_kb, int32_t *err, uint64_t wait_ns, cudaStream_t s) {
     switch (S) {
-#define CASE_S(n) case n: return launch_gemm_s<KIND, n>(panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
+#define CASE_S(n) case n: return launch_gemm_s<KIND, n>(panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, wait_ns, s);
     CASE_S(1) CASE_S(2) CASE_S(3) CASE_S(4) CASE_S(5) CASE_S(6) CASE_S(7) CASE_S(8)
 #undef CASE_S
     default: return cudaErrorInvalidValue;
@@ -612,13 +624,16 @@ cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int
 cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices, const DOzTask *tasks,
                            const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps,
                            double *c, int32_t add, int32_t S, int32_t chunk_kb, int32_t *err,
-                           cudaStream_t s) {
+                           uint64_t wait_ns, cudaStream_t s) {
     if (S < 1 || S > 8) return cudaErrorInvalidValue;
     if (kind == kOzInt8)
-        return launch_gemm_k<kOzInt8>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
+        return launch_gemm_k<kOzInt8>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err,
+                                      wait_ns, s);
     if (kind == kOzBf16)
-        return launch_gemm_k<kOzBf16>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
-    return launch_gemm_k<kOzE4m3>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err, s);
+        return launch_gemm_k<kOzBf16>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err,
+                                      wait_ns, s);
+    return launch_gemm_k<kOzE4m3>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err,
+                                  wait_ns, s);
 }
 
 }  // namespace ltg

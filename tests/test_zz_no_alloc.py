@@ -35,6 +35,12 @@ def _noalloc_dot(x_ptr: int, y_ptr: int, n: int, stream: int):
     return st, out.value
 
 
+def _free_device_bytes() -> int:
+    """Free memory of the current device (cudaMemGetInfo)."""
+    import torch
+    return int(torch.cuda.mem_get_info(0)[0])
+
+
 def test_noalloc_dot_matches_dotprod():
     ctx = Context(0)
     try:
@@ -50,11 +56,21 @@ def test_noalloc_dot_matches_dotprod():
         host = float(np.dot(a.download(), b.download()))
         assert abs(expected - host) <= REL_TOL * abs(host)
 
+        # The first call on a device loads the module (not allocation-free);
+        # after it, repeated calls leave the device's free memory unchanged.
+        st, _ = _noalloc_dot(a.device_ptr(), b.device_ptr(), n, ctx.stream())
+        assert st == _capi.LTG_OK, _last_error()
+        free_before = _free_device_bytes()
+
         results = []
         for _ in range(2):       # two calls in a row share the static array
             st, v = _noalloc_dot(a.device_ptr(), b.device_ptr(), n, ctx.stream())
             assert st == _capi.LTG_OK, _last_error()
             results.append(v)
+        for _ in range(3):
+            st, _ = _noalloc_dot(a.device_ptr(), b.device_ptr(), n, ctx.stream())
+            assert st == _capi.LTG_OK
+        assert _free_device_bytes() == free_before
         for v in results:
             assert abs(v - expected) <= REL_TOL * abs(expected), (v, expected)
         assert results[0] == results[1]          # fixed summation order
