@@ -665,23 +665,51 @@ def transfer_arm(args):
     print(json.dumps(out))
 
 
-def transfer_reference(name, w):
+def transfer_elems(name):
+    """Elements of the result (copy, add) or of each operand (dot): the
+    canonical allowed blocks of the tensor, counted on the description, each
+    block rounded up to 4 elements as the product's arenas store them."""
+    from oracle import restate as X
+    spec = transfer_inputs(name)[0][0]
+    if name == "copy-vvvv":
+        from libtensor_b200.spec import permuted_spec
+        spec = permuted_spec(spec, (0, 2, 1, 3))
+    bid = spec.bidims()
+    n = 0
+    for a in X.canonical_blocks(spec):
+        bidx = X._unabs(a, bid)
+        m = 1
+        for d, b in enumerate(bidx):
+            m *= spec.block_extent(d, b)
+        n += (m + 3) // 4 * 4
+    return n
+
+
+def transfer_inputs(name):
+    """(spec, seed) of each operand of a transfer workload (scale 1.0), as
+    transfer_setup fills them."""
+    from libtensor_b200 import spec as S
+    cfg = S.LADDER_CCD
+    return {"copy-vvvv": [(cfg.v_spec(), 31)], "add-x4": [(cfg.x_spec(), 32)],
+            "dot-vvvv": [(cfg.v_spec(), 33), (cfg.v_spec(), 34)]}[name]
+
+
+def transfer_reference(name):
     """The reference's own btod_copy / btod_add / btod_dotprod on the same
-    canonical blocks; returns (callable, tensors to close)."""
+    seeded inputs (generated inside the reference library); returns
+    (callable, tensors to close)."""
     from oracle import refapi as R
     refs = []
-    for t in w["srcs"]:
-        r = R.RefBT(t.spec)
-        host = t.download()
-        for bidx, blk in t.blocks(host):
-            r.set_block(bidx, blk)
+    for spec, seed in transfer_inputs(name):
+        r = R.RefBT(spec)
+        r.fill_seeded(seed, 1.0)
         refs.append(r)
     if name == "copy-vvvv":
         from libtensor_b200.spec import permuted_spec
-        rb = R.RefBT(permuted_spec(w["srcs"][0].spec, (0, 2, 1, 3)))
+        rb = R.RefBT(permuted_spec(refs[0].spec, (0, 2, 1, 3)))
         return (lambda: R.ref_copy(refs[0], (0, 2, 1, 3), 1.0, rb)), refs + [rb]
     if name == "add-x4":
-        rr = R.RefBT(w["dst"].spec)
+        rr = R.RefBT(refs[0].spec)
         x = refs[0]
         ops = [(x, None, 1.0), (x, (1, 0, 2, 3), -1.0), (x, (0, 1, 3, 2), -0.5), (x, (1, 0, 3, 2), 0.5)]
         return (lambda: R.ref_add(ops, rr)), refs + [rr]
@@ -694,7 +722,7 @@ def transfer_cpu_baseline(name, w, steps=2, budget_s=30.0):
         if not R.available():
             return None
         R.set_threads(os.cpu_count() or 1)
-        fn, refs = transfer_reference(name, w)
+        fn, refs = transfer_reference(name)
         ts = []
         t_start = time.perf_counter()
         for _ in range(steps):
@@ -730,9 +758,11 @@ def ccd_arm(args):
     ctx = Context(local)
     mode = MODES[args.mode]
     it = CCDIteration(ctx, [15], [50, 50, 50], mode, args.nslices)
-    # per-operation device times of one eager iteration
+    # per-operation device times of one eager iteration (the first
+    # iteration's energy is compared with the reference's first iteration)
     it.step()
     ctx.synchronize()
+    energy0 = it.energy()
     ctx.set_timing(True)
     n0 = ctx.launch_count()
     it.step()
@@ -783,6 +813,19 @@ def ccd_arm(args):
         dist.destroy_process_group()
     if rank != 0:
         return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import refapi as R
+            if R.available():
+                sec, runs, rflops, e_ref = ccd_reference(1, 60.0)
+                cpu = {"value": rflops / sec / 1e12, "unit": "TFLOP/s", "cores": os.cpu_count(),
+                       "kind": "reference", "ms_per_step": sec * 1e3,
+                       "sample": f"full workload, {runs} iteration(s) of the reference's operations in sequence",
+                       "energy": e_ref, "energy_rel_diff": abs(energy0 - e_ref) / abs(e_ref) if e_ref else None}
+        except Exception as e:   # the baseline is reported, never required
+            cpu = {"value": None, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
     tot = sum(v for v, _ in kt.values())
     out = {"metric": "CCD iteration (CUDA graph): contraction TFLOP/s eff. FP64",
            "value": replica_rate(flops, ms, world) / 1e12, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -796,16 +839,63 @@ def ccd_arm(args):
            "energy": energy,
            "e2e": {"value": replica_rate(flops, ems, world) / 1e12, "unit": "TFLOP/s",
                    "h2d_bytes_per_step": 8 * nt, "d2h_bytes_per_step": 8, "ms_per_step": ems},
-           "gpu_launches": per_iter * args.steps, "clocks": clk, "cpu_baseline": None, "roofline": None}
+           "gpu_launches": per_iter * args.steps, "clocks": clk, "cpu_baseline": cpu, "roofline": None,
+           "first_iteration_energy": energy0}
     print(json.dumps(out))
+
+
+def ccd_reference(steps, budget_s):
+    """The CCD iteration on the reference built from its sources, one
+    operation after the other (oracle/ref_ccd.py), on the host cores: each
+    timed step is the first iteration of freshly built tensors (the
+    reference's assigning add stores R with the add's own, spin-only,
+    symmetry, so later iterations would run on a less symmetric t).
+    Returns (seconds per step, steps run, flops, energy)."""
+    from oracle import refapi as R
+    from oracle.ref_ccd import RefCCDIteration
+    R.set_threads(os.cpu_count() or 1)
+    ts, flops, energy = [], None, None
+    t_start = time.perf_counter()
+    for _ in range(max(1, steps)):
+        it = RefCCDIteration([15], [50, 50, 50])
+        t0 = time.perf_counter()
+        it.step()
+        ts.append(time.perf_counter() - t0)
+        flops, energy = it.flops, it.energy
+        it.close()
+        if time.perf_counter() - t_start > budget_s:
+            break
+    return float(np.median(ts)), len(ts), flops, energy
+
+
+def ccd_reference_arm(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import refapi as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libltref.so was not built"}))
+        return
+    sec, runs, flops, energy = ccd_reference(args.steps, 120.0)
+    v = flops / sec / 1e12
+    print(json.dumps({
+        "metric": "CCD iteration (CUDA graph): contraction TFLOP/s eff. FP64", "value": v, "unit": "TFLOP/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": runs, "warmup": 0, "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, symmetrised)",
+        "config": {"workload": "ccd-iter: o=30 (15 per spin) v=300 (50,50,50 per spin); the reference's "
+                               "btod_copy, btod_contract2 (ladder, ring), btod_add, denominator, btod_dotprod, "
+                               "btod_copy in sequence", "algorithmic_flops": flops},
+        "energy": energy,
+        "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"full workload, {runs} iteration(s), median"},
+        "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
 def main():
     args = parse()
     if args.workload in GRAPH_WORKLOADS:
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the CCD iteration graph has no single reference "
-                              "operation; its steps are timed one by one by the other workloads"}))
+            ccd_reference_arm(args)
         else:
             ccd_arm(args)
         return
@@ -813,10 +903,12 @@ def main():
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) != 0:
                 return
-            import torch  # noqa: F401  (device context for the operand fill)
-            from libtensor_b200.core import Context
-            ctx = Context(0)
-            w = transfer_setup(args.workload, ctx)
+            nbytes = {"copy-vvvv": 16, "add-x4": 40, "dot-vvvv": 16}[args.workload]
+            from oracle import refapi as R
+            if not R.available():
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libltref.so was not built"}))
+                return
+            w = {"bytes": nbytes * transfer_elems(args.workload)}
             b = transfer_cpu_baseline(args.workload, w, steps=args.steps, budget_s=120.0)
             print(json.dumps({"metric": f"{args.workload}: algorithmic GB/s", "value": b["value"], "unit": "GB/s",
                               "impl": "reference", "n_gpus": args.gpus, "higher_is_better": True,

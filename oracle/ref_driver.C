@@ -399,6 +399,51 @@ void fill_seeded(void *h, uint64_t seed, double scale, int ng,
     }
 }
 
+/* Orbital-energy denominator, in place: every element of every canonical
+   block divided by sum_d (d < nocc ? +1 : -1) eps[eps_off[d] + x_d], the sum
+   taken from the last dimension to the first (as the product's kernel does,
+   so both divide by the same double).  This is caller code over the
+   reference's block access, as a coupled-cluster program writes it. */
+template<size_t N>
+void denominator(void *h, const double *eps, int nocc) {
+    bt_h<N> *t = as<N>(h);
+    std::vector<size_t> nz;
+    {
+        gen_block_tensor_rd_ctrl<N, block_tensor_i_traits<double> > rc(t->bt);
+        rc.req_nonzero_blocks(nz);
+    }
+    block_tensor_wr_ctrl<N, double> ctrl(t->bt);
+    const dimensions<N> &dims = t->bis.get_dims();
+    const dimensions<N> bidims = t->bis.get_block_index_dims();
+    size_t eoff[N];
+    for (size_t d = 0, o = 0; d < N; d++) { eoff[d] = o; o += dims[d]; }
+    for (size_t k = 0; k < nz.size(); k++) {
+        index<N> bi;
+        abs_index<N>::get_index(nz[k], bidims, bi);
+        index<N> start = t->bis.get_block_start(bi);
+        dimensions<N> bd = t->bis.get_block_dims(bi);
+        dense_tensor_wr_i<N, double> &blk = ctrl.req_block(bi);
+        {
+            dense_tensor_wr_ctrl<N, double> tc(blk);
+            double *p = tc.req_dataptr();
+            const size_t n = bd.get_size();
+            for (size_t e = 0; e < n; e++) {
+                size_t r = e;
+                double den = 0.0;
+                for (size_t d = N; d-- > 0;) {
+                    const size_t x = start[d] + r % bd[d];
+                    r /= bd[d];
+                    const double v = eps[eoff[d] + x];
+                    den += (int)d < nocc ? v : -v;
+                }
+                p[e] /= den;
+            }
+            tc.ret_dataptr(p);
+        }
+        ctrl.ret_block(bi);
+    }
+}
+
 /* ---------------- contraction ------------------------------------------ */
 
 struct c2_base {
@@ -715,6 +760,16 @@ int ref_bt_fill_seeded(void *h, uint64_t seed, double scale, int ngroup,
     const int32_t *perms, const int32_t *signs, int nthreads) {
     try {
 #define CALL(k) fill_seeded<k>(h, seed, scale, ngroup, perms, signs, nthreads)
+        DISPATCH_ORDER(static_cast<bt_base*>(h)->order, CALL)
+#undef CALL
+        return 0;
+    } catch (libtensor::exception &e) { g_err = e.what(); return -1; }
+    catch (std::exception &e) { g_err = e.what(); return -1; }
+}
+
+int ref_denominator(void *h, const double *eps, int nocc) {
+    try {
+#define CALL(k) denominator<k>(h, eps, nocc)
         DISPATCH_ORDER(static_cast<bt_base*>(h)->order, CALL)
 #undef CALL
         return 0;

@@ -41,6 +41,7 @@ _SIGS = {
     "ref_contract2_perform": (C.c_int, [_vp, _vp, C.c_int, C.c_double]),
     "ref_contract2_clst": (C.c_int64, [_vp, C.c_int64, _i64p, C.c_int64]),
     "ref_contract2_cost": (C.c_int, [_vp, _i64p, _i64p]),
+    "ref_denominator": (C.c_int, [_vp, _dblp, C.c_int]),
     "ref_bt_fill_seeded": (C.c_int, [_vp, C.c_uint64, C.c_double, C.c_int, _i32p, _i32p, C.c_int]),
     "ref_copy": (C.c_int, [_vp, _i32p, C.c_double, _vp, C.c_int, C.c_double]),
     "ref_add": (C.c_int, [C.c_int, C.POINTER(_vp), _i32p, _dblp, _vp, C.c_int, C.c_double]),
@@ -242,6 +243,13 @@ def ref_add(ops, b: RefBT, d=None):
         perms += list(p) if p is not None else list(range(n))
     cs = (C.c_double * len(ops))(*[o[2] for o in ops])
     _chk(lib().ref_add(len(ops), hs, _i32(perms), cs, b.h, 0 if d is None else 1, 0.0 if d is None else d))
+
+
+def ref_denominator(a: RefBT, eps: np.ndarray, nocc: int):
+    """a /= (sum of eps over the first nocc dims - sum over the others), per
+    element; eps holds each dimension's values one after the other."""
+    e = np.ascontiguousarray(eps, np.float64)
+    _chk(lib().ref_denominator(a.h, e.ctypes.data_as(_dblp), nocc))
 
 
 def ref_dotprod(a: RefBT, pa, b: RefBT, pb) -> float:

@@ -66,33 +66,48 @@ def test_one_iteration_matches_dense_algebra(gctx):
     it.close()
 
 
-def test_split_precision_iteration_at_full_size(gctx):
-    """CCD iteration o=30 v=300 (blocks 15 / 50,50,50 per spin) with both
-    contractions in split precision (modular INT8, 13 moduli): the energy
-    within 1e-11 relative of the plain FP64 iteration on the same inputs, and
-    the permuted copy X = P(0,2,1,3) t bit-identical to the reference's
-    btod_copy."""
+def test_iteration_at_full_size_matches_reference(gctx):
+    """CCD iteration o=30 v=300 (blocks 15 / 50,50,50 per spin) against the
+    same iteration on the reference built from its sources (btod_copy,
+    btod_contract2 x 2, btod_add, the denominator, btod_dotprod; one
+    operation after the other, oracle/ref_ccd.py):
+      - the permuted copy X = P(0,2,1,3) t bit-identical;
+      - plain FP64: new amplitudes within 1e-12 per block and the energy
+        within 1e-12 relative;
+      - both contractions in split precision (modular INT8, 13 moduli): the
+        energy within 1e-11 relative of the plain FP64 iteration and of the
+        reference."""
     from libtensor_b200 import spec as S
-    from libtensor_b200.spec import permuted_spec
     from oracle import refapi as R
+    from oracle.ref_ccd import RefCCDIteration
+    if not R.available():
+        pytest.skip("oracle/_ref not built")
     cfg = S.LADDER_CCD
+    R.set_threads(__import__("os").cpu_count() or 1)
+    ref = RefCCDIteration(cfg.occ_blocks, cfg.vir_blocks)
+    ref.step()
+    e_ref = ref.energy
+    assert e_ref != 0.0
     energies = {}
     for mode, nslices in ((MODE_PLAIN_FP64, 0), (MODE_OZAKI_CRT, 13)):
         it = CCDIteration(gctx, cfg.occ_blocks, cfg.vir_blocks, mode, nslices)
+        assert it.flops == ref.flops
         it.step()
         energies[mode] = it.energy()
-        if mode == MODE_PLAIN_FP64 and R.available():
-            perm = (0, 2, 1, 3)
-            rt = R.RefBT(it.t.spec)
-            rt.fill_seeded(7, 0.01)
-            rx = R.RefBT(permuted_spec(it.t.spec, perm))
-            R.ref_copy(rt, perm, 1.0, rx)
+        if mode == MODE_PLAIN_FP64:
             for bidx, blk in it.X.blocks(it.X.download()):
-                want = rx.get_block(bidx, blk.shape)
+                want = ref.X.get_block(bidx, blk.shape)
                 assert np.array_equal(blk.view(np.uint64), want.view(np.uint64)), bidx
-            rt.close()
-            rx.close()
+            worst = 0.0
+            for bidx, blk in it.t.blocks(it.t.download()):
+                want = ref.t.get_block(bidx, blk.shape)
+                m = float(np.max(np.abs(want))) if want.size else 0.0
+                if m > 0:
+                    worst = max(worst, float(np.max(np.abs(blk - want))) / m)
+            assert worst <= 1e-12, worst
         it.close()
+    ref.close()
     e64, e_split = energies[MODE_PLAIN_FP64], energies[MODE_OZAKI_CRT]
-    assert e64 != 0.0
+    assert abs(e64 - e_ref) <= 1e-12 * abs(e_ref), (e64, e_ref)
     assert abs(e_split - e64) <= 1e-11 * abs(e64), (e64, e_split)
+    assert abs(e_split - e_ref) <= 1e-11 * abs(e_ref), (e_ref, e_split)

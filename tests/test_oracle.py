@@ -140,3 +140,36 @@ def test_reference_copy_add_dot_match_dense():
     dot = R.ref_dotprod(r1, None, r2, (1, 0, 2, 3))
     ddot = float(np.sum(d1 * X.dense_permute(d2, (1, 0, 2, 3))))
     assert abs(dot - ddot) <= 1e-12 * max(1.0, abs(ddot))
+
+
+def test_reference_ccd_iteration_matches_dense_algebra():
+    """The reference-side CCD iteration (oracle/ref_ccd.py: the reference's
+    operations one after the other) against the dense numpy algebra."""
+    from oracle.ref_ccd import RefCCDIteration
+    it = RefCCDIteration([3], [4, 3])
+    t0 = X.seeded_dense(it.t.spec, 7, 0.01)
+    V = X.seeded_dense(it.V.spec, 8, 0.01)
+    W = X.seeded_dense(it.W.spec, 9, 0.01)
+    it.step()
+    L = 0.5 * np.einsum("ijcd,abcd->ijab", t0, V)
+    G = np.einsum("ikac,kbcj->ijab", t0, W)
+    Rm = L + 0.5 * (G - G.transpose(1, 0, 2, 3) - G.transpose(0, 1, 3, 2) + G.transpose(1, 0, 3, 2))
+    o, v, e = it.o, it.v, it.eps
+    D = e[:o, None, None, None] + e[o:2 * o][None, :, None, None] - e[2 * o:2 * o + v][None, None, :, None] \
+        - e[2 * o + v:][None, None, None, :]
+    Rd = np.where(X.allowed_element_mask(it.R.spec if it.R.spec else it.t.spec), Rm / D, 0.0)
+    for a in X.canonical_blocks(it.t.spec):
+        bidx = X._unabs(a, it.t.spec.bidims())
+        want = X.block_view(it.t.spec, Rd, bidx)
+        got = it.t.get_block(bidx, want.shape)
+        assert np.max(np.abs(got - want)) <= 1e-13 * max(1e-300, np.max(np.abs(want)))
+    E = float(np.sum(Rd * t0))
+    assert abs(it.energy - E) <= 1e-12 * abs(E)
+    Xd = np.transpose(t0, (0, 2, 1, 3))
+    from libtensor_b200.spec import permuted_spec
+    xs = permuted_spec(it.t.spec, (0, 2, 1, 3))
+    for a in X.canonical_blocks(xs):
+        bidx = X._unabs(a, xs.bidims())
+        want = X.block_view(xs, Xd, bidx)
+        assert np.array_equal(it.X.get_block(bidx, want.shape), want)
+    it.close()
