@@ -207,6 +207,13 @@ int ltg_plan_destroy(ltg_plan *plan);
  * automatic choice (-1).  No reference counterpart: the reference hands each
  * block pair to BLAS. */
 int ltg_contract2_set_tile(ltg_plan *plan, int32_t cfg);
+/* Plain FP64 mode: k chunks per output tile.  0 (default) cuts the k range of
+ * the last work items of a launch into 2-4 chunks when that evens out the end
+ * of the launch; 1 never cuts; 2-4 cut every tile into that many chunks.  The
+ * chunks' partial tiles are summed in k order by a second kernel, so results
+ * do not depend on scheduling (they differ from the uncut sum in rounding
+ * only).  No reference counterpart. */
+int ltg_contract2_set_split_k(ltg_plan *plan, int32_t k);
 /* Modular mode (LTG_MODE_OZAKI_CRT): enables (default) or disables grouped
  * products.  When no pair list was shortened by coalescing, C blocks whose row
  * blocks (C dims taken from A) and column blocks (C dims taken from B) are

@@ -313,6 +313,10 @@ class btod_contract2:
     def set_tile(self, cfg: int):
         check(lib().ltg_contract2_set_tile(self.h, cfg))
 
+    def set_split_k(self, k: int):
+        """Plain FP64 mode: k chunks per output tile (0 automatic, 1 never, 2-4 always)."""
+        check(lib().ltg_contract2_set_split_k(self.h, k))
+
     def set_grouping(self, enable: bool):
         """Modular mode: grouped products of small C blocks (default on)."""
         check(lib().ltg_contract2_set_grouping(self.h, 1 if enable else 0))

@@ -61,10 +61,23 @@ __device__ __forceinline__ void dmma_16x8x8(double *d, const double *a, const do
         : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
+// m16n8k16 (sm_90 and later): the A fragment is the two m16n8k8 fragments of
+// k 0-7 and 8-15 one after the other (registers a0-a3, a4-a7), the B
+// fragment likewise (b0-b1, b2-b3).
+__device__ __forceinline__ void dmma_16x8x16(double *d, const double *a0, const double *a1, const double *b0,
+                                             const double *b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a0[0]), "d"(a0[1]), "d"(a0[2]), "d"(a0[3]), "d"(a1[0]), "d"(a1[1]), "d"(a1[2]), "d"(a1[3]),
+          "d"(b0[0]), "d"(b0[1]), "d"(b1[0]), "d"(b1[1]));
+}
 
-template<int BM_, int BN_, int BK_, int WM_, int WN_, int STAGES_>
+template<int BM_, int BN_, int BK_, int WM_, int WN_, int STAGES_, bool K16_ = false>
 struct TileCfg {
     static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_, STAGES = STAGES_;
+    static constexpr bool K16 = K16_;            // one m16n8k16 DMMA per two k8 steps
     static constexpr int kWarpsM = BM / WM, kWarpsN = BN / WN;
     static constexpr int kThreads = kWarpsM * kWarpsN * 32;
     static constexpr int kLd = BK + 8;          // padded row stride in doubles (conflict-free 16B reads)
@@ -129,7 +142,7 @@ __global__ void __launch_bounds__(C::kThreads, 1)
 contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
                      const DItem *__restrict__ items, int32_t nitems, int32_t *counter,
                      const double *__restrict__ A, const double *__restrict__ B,
-                     double *__restrict__ Cp, int32_t add) {
+                     double *__restrict__ Cp, double *__restrict__ ws, int32_t add) {
     extern __shared__ __align__(16) double smem[];
     double *sA = smem;
     double *sB = smem + C::STAGES * C::kStageA;
@@ -161,7 +174,14 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
 #pragma unroll
                 for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
 
-        for (int ti = cb.t_begin; ti < cb.t_end; ti++) {
+        int kt_base = 0;                       // k tiles of the tasks before ti
+        for (int ti = cb.t_begin; ti < cb.t_end && kt_base < item.kt1; ti++) {
+            // this item's k tiles of the task (a k chunk may cover part of it)
+            const int nkt_task = (tasks[ti].K + C::BK - 1) / C::BK;
+            const int kt_lo = max(item.kt0 - kt_base, 0);
+            const int kt_hi = min(item.kt1 - kt_base, nkt_task);
+            kt_base += nkt_task;
+            if (kt_lo >= kt_hi) continue;
             static_assert(sizeof(DTask) % 8 == 0, "task copy granularity");
             if (tid < (int)(sizeof(DTask) / 8))
                 reinterpret_cast<int64_t *>(&s_task)[tid] =
@@ -179,12 +199,13 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
             __syncthreads();
             const double coef = t.coeff;
             const bool scale_b = coef != 1.0;
-            const int nkt = (t.K + C::BK - 1) / C::BK;
+            const int nkt = kt_hi - kt_lo;          // k tiles kt_lo + kt, kt = 0 .. nkt-1
 
 #pragma unroll
             for (int s = 0; s < C::STAGES - 1; s++) {
                 if (s < nkt)
-                    load_stage<C>(sA + s * C::kStageA, sB + s * C::kStageB, rowA, rowB, A, B, t, s * C::BK);
+                    load_stage<C>(sA + s * C::kStageA, sB + s * C::kStageB, rowA, rowB, A, B, t,
+                                  (kt_lo + s) * C::BK);
                 cp_async_commit();
             }
             for (int kt = 0; kt < nkt; kt++) {
@@ -194,7 +215,8 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
                     int nk = kt + C::STAGES - 1;
                     if (nk < nkt) {
                         int st = nk % C::STAGES;
-                        load_stage<C>(sA + st * C::kStageA, sB + st * C::kStageB, rowA, rowB, A, B, t, nk * C::BK);
+                        load_stage<C>(sA + st * C::kStageA, sB + st * C::kStageB, rowA, rowB, A, B, t,
+                                      (kt_lo + nk) * C::BK);
                     }
                     cp_async_commit();
                 }
@@ -216,23 +238,60 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
                         bf[buf][j][1] = v.y;
                     }
                 };
-                load_frags(0, 0);
+                if constexpr (C::K16) {
+                    // both fragment buffers hold one k16 step
 #pragma unroll
-                for (int ks = 0; ks < C::BK; ks += 8) {
-                    const int cur = (ks / 8) & 1;
-                    if (ks + 8 < C::BK) load_frags(cur ^ 1, ks + 8);
-                    if (scale_b) {
+                    for (int ks = 0; ks < C::BK; ks += 16) {
+                        load_frags(0, ks);
+                        load_frags(1, ks + 8);
+                        if (scale_b) {
 #pragma unroll
-                        for (int j = 0; j < C::kNT; j++) { bf[cur][j][0] *= coef; bf[cur][j][1] *= coef; }
+                            for (int j = 0; j < C::kNT; j++)
+#pragma unroll
+                                for (int h = 0; h < 2; h++) { bf[h][j][0] *= coef; bf[h][j][1] *= coef; }
+                        }
+#pragma unroll
+                        for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+                            for (int j = 0; j < C::kNT; j++)
+                                dmma_16x8x16(acc[i][j], af[0][i], af[1][i], bf[0][j], bf[1][j]);
                     }
+                } else {
+                    load_frags(0, 0);
 #pragma unroll
-                    for (int i = 0; i < C::kMT; i++)
+                    for (int ks = 0; ks < C::BK; ks += 8) {
+                        const int cur = (ks / 8) & 1;
+                        if (ks + 8 < C::BK) load_frags(cur ^ 1, ks + 8);
+                        if (scale_b) {
 #pragma unroll
-                        for (int j = 0; j < C::kNT; j++) dmma_16x8x8(acc[i][j], af[cur][i], bf[cur][j]);
+                            for (int j = 0; j < C::kNT; j++) { bf[cur][j][0] *= coef; bf[cur][j][1] *= coef; }
+                        }
+#pragma unroll
+                        for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+                            for (int j = 0; j < C::kNT; j++) dmma_16x8x8(acc[i][j], af[cur][i], bf[cur][j]);
+                    }
                 }
             }
             cp_async_wait<0>();
             __syncthreads();
+        }
+
+        if (item.slot >= 0) {
+            // k chunk: the unscaled partial tile, dense BM x BN, to its slot
+            double *P = ws + (int64_t)item.slot * (C::BM * C::BN);
+#pragma unroll
+            for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+                for (int j = 0; j < C::kNT; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int r = wm * C::WM + i * 16 + g + 8 * h;
+                        const int cc = wn * C::WN + j * 8 + 2 * t4;
+                        *reinterpret_cast<double2 *>(P + r * C::BN + cc) =
+                            make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
+                    }
+            continue;
         }
 
         // Epilogue: scaled store (assign) or scaled accumulate (add) into the
@@ -270,10 +329,38 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
     }
 }
 
+// Split tiles: element e of tile x sums its nparts partials in chunk order
+// (fixed order: the result does not depend on which CTA ran which chunk).
+__global__ void __launch_bounds__(256)
+split_reduce_kernel(const DSplit *__restrict__ splits, int32_t nsplits, const DCBlock *__restrict__ cblks,
+                    const double *__restrict__ ws, int32_t bm, int32_t bn, double *__restrict__ Cp,
+                    int32_t add) {
+    const int64_t tile = (int64_t)bm * bn;
+    const int64_t total = (int64_t)nsplits * tile;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t x = (int32_t)(e / tile);
+        const int32_t r = (int32_t)((e - (int64_t)x * tile) / bn);
+        const int32_t cc = (int32_t)(e - (int64_t)x * tile - (int64_t)r * bn);
+        const DSplit sp = splits[x];
+        const DCBlock &cb = cblks[sp.cblk];
+        const int m = sp.m0 + r, n = sp.n0 + cc;
+        if (m >= cb.M || n >= cb.N) continue;
+        const double *p = ws + (int64_t)sp.slot0 * tile + (int64_t)r * bn + cc;
+        double v = 0.0;
+        for (int q = 0; q < sp.nparts; q++) v += p[(int64_t)q * tile];
+        v *= cb.scale;
+        double *dst = Cp + cb.c_off + mixed_offset(m, cb.nm, cb.mext, cb.mc_str) +
+                      mixed_offset(n, cb.nn, cb.next, cb.nc_str);
+        if (add) *dst += v;
+        else *dst = v;
+    }
+}
+
 template<class C>
 cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *items,
                        int32_t nitems, int32_t *counter, const double *a, const double *b,
-                       double *c, int32_t add, cudaStream_t s) {
+                       double *c, double *ws, int32_t add, cudaStream_t s) {
     static int configured_dev = -1;
     cudaError_t e;
     int dev = 0, nsm = 0;
@@ -290,7 +377,7 @@ cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *it
     e = cudaMemsetAsync(counter, 0, sizeof(int32_t), s);
     if (e != cudaSuccess) return e;
     contract_fp64_kernel<C><<<grid, C::kThreads, C::kSmem, s>>>(tasks, cblks, items, nitems, counter,
-                                                               a, b, c, add);
+                                                               a, b, c, ws, add);
     return cudaGetLastError();
 }
 
@@ -310,35 +397,60 @@ using Cfg9 = TileCfg<32, 128, 32, 32, 16, 3>;
 // 80-row shapes with twelve warps (three per scheduler, 168 registers)
 using Cfg10 = TileCfg<80, 192, 16, 80, 16, 4>;
 using Cfg11 = TileCfg<80, 192, 32, 80, 16, 2>;
+// m16n8k16 DMMA forms of shapes 11 and 4, and a squarer warp tile (48 x 32:
+// 12 DMMAs per 10 fragment loads instead of 10 per 12)
+using Cfg12 = TileCfg<80, 192, 32, 80, 16, 2, true>;
+using Cfg13 = TileCfg<80, 128, 32, 80, 16, 3, true>;
+using Cfg14 = TileCfg<96, 128, 32, 48, 32, 3>;
 
 }  // namespace
 
-int tile_cfg_count() { return 12; }
+int tile_cfg_count() { return 15; }
 int tile_cfg_bm(int cfg) {
-    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM, Cfg8::BM, Cfg9::BM, Cfg10::BM, Cfg11::BM};
+    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM, Cfg8::BM, Cfg9::BM, Cfg10::BM, Cfg11::BM, Cfg12::BM, Cfg13::BM, Cfg14::BM};
+    return v[cfg];
+}
+int tile_cfg_bk(int cfg) {
+    const int v[] = {Cfg0::BK, Cfg1::BK, Cfg2::BK, Cfg3::BK, Cfg4::BK, Cfg5::BK, Cfg6::BK, Cfg7::BK, Cfg8::BK, Cfg9::BK, Cfg10::BK, Cfg11::BK, Cfg12::BK, Cfg13::BK, Cfg14::BK};
     return v[cfg];
 }
 int tile_cfg_bn(int cfg) {
-    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN, Cfg8::BN, Cfg9::BN, Cfg10::BN, Cfg11::BN};
+    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN, Cfg8::BN, Cfg9::BN, Cfg10::BN, Cfg11::BN, Cfg12::BN, Cfg13::BN, Cfg14::BN};
     return v[cfg];
+}
+
+cudaError_t launch_split_reduce(const DSplit *splits, int32_t nsplits, const DCBlock *cblks,
+    const double *ws, int32_t bm, int32_t bn, double *c, int32_t add, cudaStream_t s) {
+    if (nsplits <= 0) return cudaSuccess;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t total = (int64_t)nsplits * bm * bn;
+    const int64_t want = (total + 255) / 256;
+    const int grid = (int)(want < 8LL * nsm ? want : 8LL * nsm);
+    split_reduce_kernel<<<grid, 256, 0, s>>>(splits, nsplits, cblks, ws, bm, bn, c, add);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     const DItem *items, int32_t nitems, int32_t *counter, const double *a,
-    const double *b, double *c, int32_t add, int32_t tile_cfg, cudaStream_t s) {
+    const double *b, double *c, double *ws, int32_t add, int32_t tile_cfg, cudaStream_t s) {
     switch (tile_cfg) {
-    case 0: return launch_cfg<Cfg0>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 1: return launch_cfg<Cfg1>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 2: return launch_cfg<Cfg2>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 3: return launch_cfg<Cfg3>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 4: return launch_cfg<Cfg4>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 5: return launch_cfg<Cfg5>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 6: return launch_cfg<Cfg6>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 7: return launch_cfg<Cfg7>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 8: return launch_cfg<Cfg8>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 9: return launch_cfg<Cfg9>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    case 10: return launch_cfg<Cfg10>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
-    default: return launch_cfg<Cfg11>(tasks, cblks, items, nitems, counter, a, b, c, add, s);
+    case 0: return launch_cfg<Cfg0>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 1: return launch_cfg<Cfg1>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 2: return launch_cfg<Cfg2>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 3: return launch_cfg<Cfg3>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 4: return launch_cfg<Cfg4>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 5: return launch_cfg<Cfg5>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 6: return launch_cfg<Cfg6>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 7: return launch_cfg<Cfg7>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 8: return launch_cfg<Cfg8>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 9: return launch_cfg<Cfg9>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 10: return launch_cfg<Cfg10>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 11: return launch_cfg<Cfg11>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 12: return launch_cfg<Cfg12>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 13: return launch_cfg<Cfg13>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    default: return launch_cfg<Cfg14>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
     }
 }
 

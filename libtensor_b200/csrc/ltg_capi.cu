@@ -8,9 +8,11 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <queue>
 #include <string>
 #include <thread>
 #include <tuple>
@@ -137,6 +139,16 @@ struct ltg_bt {
     DevBuf denom_dev, denom_off;
 };
 
+// One launch of the plain DMMA kernel: a tile shape, its work items, and the
+// tiles whose k range was cut into chunks (summed by the split reduction;
+// their partial tiles at ws_off in the workspace).
+struct DmmaLaunch {
+    int32_t cfg = 0;
+    int32_t item0 = 0, nitems = 0;
+    int32_t split0 = 0, nsplits = 0;
+    int64_t ws_off = 0;
+};
+
 // Grouped products of the plain FP64 path (the groups of crt_groups): the
 // operand cells of every group gathered into dense panels in buf, one DMMA
 // product per group into a dense result in buf, scattered into the C blocks.
@@ -144,15 +156,15 @@ struct PlainGroups {
     int32_t ngroups = 0, nunits = 0, nsunits = 0;
     double scale = 1.0;                       // ka kb kc (and d in add mode)
     DevBuf buf, pieces, units, sunits, comps, res_off, ctab, cells;
-    DevBuf tasks, cblks, items;               // DMMA work over buf
-    std::vector<std::pair<int32_t, std::pair<int32_t, int32_t>>> launches;   // cfg -> item range
+    DevBuf tasks, cblks, items, splits, ws;   // DMMA work over buf
+    std::vector<DmmaLaunch> launches;
 };
 
 struct ContractExec {
     // device task arrays bound to one output tensor and coefficient set
-    DevBuf tasks, cblks, items;
+    DevBuf tasks, cblks, items, splits, ws;
     std::unique_ptr<PlainGroups> groups;      // grouped small blocks, if any
-    std::vector<std::pair<int32_t, std::pair<int32_t, int32_t>>> launches;  // cfg -> item range
+    std::vector<DmmaLaunch> launches;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;  // assign mode: blocks not in the schedule
     std::vector<int64_t> sched_slots;
 };
@@ -188,6 +200,7 @@ struct ltg_plan {
              std::unique_ptr<CrtExec>> crt;
     ltg_bt *a = nullptr, *b = nullptr;
     int forced_tile = -1;         // >= 0: every C block uses this tile shape
+    int split_k = 0;              // plain DMMA k chunks per tile: 0 automatic, 1 never, 2-4 always
     bool group_products = true;   // modular mode: small C blocks grouped into larger products
     // caller-built task list (ltg_plan_contract2_upload): plain FP64 only,
     // coefficients absolute, no schedule of its own
@@ -421,13 +434,15 @@ int32_t vec16_ok(int64_t off, const SubDims &rows, const SubDims &k, bool second
 // the shape (larger tiles reuse more data per load).  An autotuned table
 // (ltg_autotune) overrides the weights with measured rates.
 struct TileShape { int bm, bn; double eff; };
-constexpr int kNumShapes = 12;
+constexpr int kNumShapes = 15;
 const TileShape kShapes[kNumShapes] = {
     {128, 128, 1.00}, {64, 64, 0.78}, {64, 128, 0.90}, {32, 32, 0.45},
     {80, 128, 0.97}, {96, 128, 0.98}, {48, 128, 0.85}, {112, 128, 0.99},
     {16, 128, 0.50}, {32, 128, 0.70}, {80, 192, 0.96}, {80, 192, 0.95},
+    {80, 192, 0.94}, {80, 128, 0.93}, {96, 128, 0.92},
 };
-double g_tile_eff[kNumShapes] = {1.00, 0.78, 0.90, 0.45, 0.97, 0.98, 0.85, 0.99, 0.50, 0.70, 0.96, 0.95};
+double g_tile_eff[kNumShapes] = {1.00, 0.78, 0.90, 0.45, 0.97, 0.98, 0.85, 0.99, 0.50, 0.70, 0.96, 0.95,
+                                 0.94, 0.93, 0.92};
 
 int pick_tile(int64_t M, int64_t N) {
     int best = 0;
@@ -440,6 +455,97 @@ int pick_tile(int64_t M, int64_t N) {
         if (cost < bestc) { bestc = cost; best = c; }
     }
     return best;
+}
+
+// Work items of one tile shape, appended to `items` costliest first (LPT
+// order for the persistent work queue).  The tail of a launch is uneven when
+// its items are few and long; cutting the k range of the last items into
+// equal chunks (partial tiles summed in chunk order by the split reduction,
+// so results do not depend on scheduling) evens it out at the price of the
+// partial tiles' traffic.  split_k 0 picks, among "no split" and the last
+// 1, 2 or 4 waves' items (or all) in 2-4 chunks, the shortest launch:
+// the slowest SM's work in a simulated greedy assignment (the device's
+// work-queue order) at the nominal per-SM DMMA rate, plus the partial tiles'
+// bytes at HBM speed; 1 never splits; 2-4 split every item in that many.
+void append_launch(int cfg, std::vector<std::pair<double, DItem>> &v, const std::vector<DTask> &dt,
+                   const std::vector<DCBlock> &dc, int nsm, int split_k, std::vector<DItem> &items,
+                   std::vector<DSplit> &splits, int64_t &ws_elems, std::vector<DmmaLaunch> &launches) {
+    if (v.empty()) return;
+    std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) {
+        return x.first > y.first;
+    });
+    const int bm = tile_cfg_bm(cfg), bn = tile_cfg_bn(cfg), bk = tile_cfg_bk(cfg);
+    const size_t n = v.size();
+    std::vector<int32_t> nkt(n, 0);
+    for (size_t i = 0; i < n; i++) {
+        const DCBlock &b = dc[v[i].second.cblk];
+        for (int32_t t = b.t_begin; t < b.t_end; t++) nkt[i] += (dt[t].K + bk - 1) / bk;
+    }
+    const double kFmaPerSmSec = 40e12 / 2 / 148, kBytesPerSec = 6e12, kReduceLaunchSec = 4e-6;
+    auto evaluate = [&](size_t first_split, int sk) {
+        std::vector<double> w;
+        double bytes = 0;
+        for (size_t i = 0; i < n; i++) {
+            const int parts = i >= first_split ? std::max(1, std::min(sk, nkt[i])) : 1;
+            for (int p = 0; p < parts; p++) w.push_back(v[i].first / parts);
+            if (parts > 1) bytes += (double)(2 * parts + 1) * bm * bn * 8;
+        }
+        std::sort(w.rbegin(), w.rend());
+        std::priority_queue<double, std::vector<double>, std::greater<double>> load;
+        for (int k = 0; k < std::max(1, nsm); k++) load.push(0.0);
+        double mk = 0;
+        for (double x : w) {
+            double t = load.top() + x;
+            load.pop();
+            load.push(t);
+            mk = std::max(mk, t);
+        }
+        return mk / kFmaPerSmSec + (bytes > 0 ? bytes / kBytesPerSec + kReduceLaunchSec : 0.0);
+    };
+    size_t first_split = n;
+    int sk = 1;
+    if (split_k >= 2) {
+        first_split = 0;
+        sk = std::min(split_k, 4);
+    } else if (split_k == 0 && n > 0) {
+        double best = evaluate(n, 1);
+        for (int waves : {1, 2, 4, 0})
+            for (int k = 2; k <= 4; k++) {
+                const size_t fs = waves == 0 ? 0 : (n > (size_t)waves * nsm ? n - (size_t)waves * nsm : 0);
+                const double t = evaluate(fs, k);
+                if (t < best * 0.995) { best = t; first_split = fs; sk = k; }
+            }
+    }
+    DmmaLaunch L;
+    L.cfg = cfg;
+    L.item0 = (int32_t)items.size();
+    L.split0 = (int32_t)splits.size();
+    L.ws_off = ws_elems;
+    std::vector<std::pair<double, DItem>> out;
+    int32_t slot = 0;
+    for (size_t i = 0; i < n; i++) {
+        const int parts = i >= first_split ? std::max(1, std::min(sk, nkt[i])) : 1;
+        if (parts == 1) { out.push_back(v[i]); continue; }
+        DSplit sp;
+        sp.cblk = v[i].second.cblk; sp.m0 = v[i].second.m0; sp.n0 = v[i].second.n0;
+        sp.nparts = parts; sp.slot0 = slot; sp.pad = 0;
+        splits.push_back(sp);
+        for (int p = 0; p < parts; p++) {
+            DItem it = v[i].second;
+            it.slot = slot++;
+            it.kt0 = (int32_t)((int64_t)p * nkt[i] / parts);
+            it.kt1 = (int32_t)((int64_t)(p + 1) * nkt[i] / parts);
+            out.push_back({v[i].first / parts, it});
+        }
+    }
+    std::stable_sort(out.begin(), out.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) {
+        return x.first > y.first;
+    });
+    for (auto &q : out) items.push_back(q.second);
+    L.nitems = (int32_t)out.size();
+    L.nsplits = (int32_t)splits.size() - L.split0;
+    ws_elems += (int64_t)slot * bm * bn;
+    launches.push_back(L);
 }
 
 void pack_sub(const SubDims &s, int32_t &n, int32_t *ext, int32_t *str0, int32_t *str1) {
@@ -540,24 +646,24 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
         int bm = tile_cfg_bm(cfg), bn = tile_cfg_bn(cfg);
         for (int64_t m0 = 0; m0 < cbt[e].M; m0 += bm)
             for (int64_t n0 = 0; n0 < cbt[e].N; n0 += bn) {
-                DItem it; it.cblk = (int32_t)e; it.m0 = (int32_t)m0; it.n0 = (int32_t)n0; it.pad = 0;
+                DItem it = make_item((int32_t)e, (int32_t)m0, (int32_t)n0);
                 double cost = (double)bm * bn * (cbt[e].kflops + 8.0 * (cbt[e].t_end - cbt[e].t_begin));
                 per_cfg[cfg].push_back({cost, it});
             }
     }
     std::vector<DItem> items;
-    for (int cfg = 0; cfg < kNumShapes; cfg++) {
-        auto &v = per_cfg[cfg];
-        if (v.empty()) continue;
-        std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
-        int32_t start = (int32_t)items.size();
-        for (auto &p : v) items.push_back(p.second);
-        ex->launches.push_back({cfg, {start, (int32_t)v.size()}});
-    }
+    std::vector<DSplit> splits;
+    int64_t ws_elems = 0;
+    for (int cfg = 0; cfg < kNumShapes; cfg++)
+        append_launch(cfg, per_cfg[cfg], dt, dc, pl->ctx->nsm, pl->split_k, items, splits, ws_elems, ex->launches);
     cudaStream_t s = pl->ctx->stream;
     upload_vec(ex->tasks, dt, s);
     upload_vec(ex->cblks, dc, s);
     upload_vec(ex->items, items, s);
+    if (!splits.empty()) {
+        upload_vec(ex->splits, splits, s);
+        ex->ws.alloc(ws_elems * (int64_t)sizeof(double));
+    }
     // blocks of C outside the schedule (zeroed in assign mode)
     std::vector<char> in_sched(c->h.blk_abs.size(), 0);
     if (pl->external) {
@@ -675,7 +781,7 @@ OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, doubl
     for (size_t e = 0; e < cbt.size(); e++)
         for (int64_t m0 = 0; m0 < cbt[e].M; m0 += 128)
             for (int64_t n0 = 0; n0 < cbt[e].N; n0 += 64) {
-                DItem it; it.cblk = (int32_t)e; it.m0 = (int32_t)m0; it.n0 = (int32_t)n0; it.pad = 0;
+                DItem it = make_item((int32_t)e, (int32_t)m0, (int32_t)n0);
                 iv.push_back({cbt[e].kflops + 64.0 * (cbt[e].t_end - cbt[e].t_begin), it});
             }
     std::stable_sort(iv.begin(), iv.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
@@ -1211,20 +1317,16 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
         const int bm = tile_cfg_bm(cfg), bn = tile_cfg_bn(cfg);
         for (int64_t m0 = 0; m0 < lay.rows; m0 += bm)
             for (int64_t n0 = 0; n0 < lay.cols; n0 += bn) {
-                DItem it; it.cblk = (int32_t)dc.size(); it.m0 = (int32_t)m0; it.n0 = (int32_t)n0; it.pad = 0;
+                DItem it = make_item((int32_t)dc.size(), (int32_t)m0, (int32_t)n0);
                 per_cfg[cfg].push_back({(double)bm * bn * (double)lay.kt, it});
             }
         dc.push_back(b);
     }
     std::vector<DItem> items;
-    for (int cfg = 0; cfg < kNumShapes; cfg++) {
-        auto &v = per_cfg[cfg];
-        if (v.empty()) continue;
-        std::stable_sort(v.begin(), v.end(), [](const std::pair<double, DItem> &x, const std::pair<double, DItem> &y) { return x.first > y.first; });
-        const int32_t start = (int32_t)items.size();
-        for (auto &q : v) items.push_back(q.second);
-        pg.launches.push_back({cfg, {start, (int32_t)v.size()}});
-    }
+    std::vector<DSplit> splits;
+    int64_t ws_elems = 0;
+    for (int cfg = 0; cfg < kNumShapes; cfg++)
+        append_launch(cfg, per_cfg[cfg], dt, dc, pl->ctx->nsm, pl->split_k, items, splits, ws_elems, pg.launches);
     cudaStream_t s = pl->ctx->stream;
     pg.ngroups = (int32_t)groups.size();
     pg.nunits = (int32_t)units.size();
@@ -1244,6 +1346,10 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
     upload_vec(pg.tasks, dt, s);
     upload_vec(pg.cblks, dc, s);
     upload_vec(pg.items, items, s);
+    if (!splits.empty()) {
+        upload_vec(pg.splits, splits, s);
+        pg.ws.alloc(ws_elems * (int64_t)sizeof(double));
+    }
 }
 
 CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, double kc, int add, double d) {
@@ -2456,10 +2562,16 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             for (auto &l : pg->launches) {
                 TimedLaunch tl(ctx, LTG_KERNEL_CONTRACT_FP64);
                 LTG_CUDA(launch_contract_fp64(pg->tasks.as<DTask>(), pg->cblks.as<DCBlock>(),
-                                              pg->items.as<DItem>() + l.second.first, l.second.second,
+                                              pg->items.as<DItem>() + l.item0, l.nitems,
                                               ctx->scratch_counter.as<int32_t>() + (slot++ % 64),
                                               pg->buf.as<double>(), pg->buf.as<double>(), pg->buf.as<double>(),
-                                              0, l.first, s));
+                                              pg->ws.as<double>() + l.ws_off, 0, l.cfg, s));
+                if (l.nsplits > 0) {
+                    LTG_CUDA(launch_split_reduce(pg->splits.as<DSplit>() + l.split0, l.nsplits, pg->cblks.as<DCBlock>(),
+                                                 pg->ws.as<double>() + l.ws_off, tile_cfg_bm(l.cfg),
+                                                 tile_cfg_bn(l.cfg), pg->buf.as<double>(), 0, s));
+                    ctx->launches++;
+                }
                 tl.done();
                 ctx->launches++;
             }
@@ -2467,10 +2579,16 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
         for (auto &l : ex->launches) {
             TimedLaunch tl(ctx, LTG_KERNEL_CONTRACT_FP64);
             LTG_CUDA(launch_contract_fp64(ex->tasks.as<DTask>(), ex->cblks.as<DCBlock>(),
-                                          ex->items.as<DItem>() + l.second.first, l.second.second,
+                                          ex->items.as<DItem>() + l.item0, l.nitems,
                                           ctx->scratch_counter.as<int32_t>() + (slot++ % 64),
                                           plan->a->arena.as<double>(), plan->b->arena.as<double>(),
-                                          c->arena.as<double>(), add, l.first, s));
+                                          c->arena.as<double>(), ex->ws.as<double>() + l.ws_off, add, l.cfg, s));
+            if (l.nsplits > 0) {
+                LTG_CUDA(launch_split_reduce(ex->splits.as<DSplit>() + l.split0, l.nsplits, ex->cblks.as<DCBlock>(),
+                                             ex->ws.as<double>() + l.ws_off, tile_cfg_bm(l.cfg), tile_cfg_bn(l.cfg),
+                                             c->arena.as<double>(), add, s));
+                ctx->launches++;
+            }
             tl.done();
             ctx->launches++;
         }
@@ -2523,6 +2641,15 @@ int ltg_contract2_set_tile(ltg_plan *plan, int32_t cfg) {
         if (!plan) throw error(kErrBadArg, "null plan");
         if (cfg < -1 || cfg >= tile_cfg_count()) throw error(kErrBadArg, "tile configuration out of range");
         plan->forced_tile = cfg;
+        plan->exec.clear();
+    });
+}
+
+int ltg_contract2_set_split_k(ltg_plan *plan, int32_t k) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (k < 0 || k > 4) throw error(kErrBadArg, "k chunks per tile must be 0 (automatic) or 1-4");
+        plan->split_k = k;
         plan->exec.clear();
     });
 }

@@ -37,12 +37,34 @@ struct DCBlock {
     int32_t t_begin, t_end;       // task range
 };
 
-// One CTA work item: an (m, n) tile of a C block.
+// One CTA work item: an (m, n) tile of a C block, over the k tiles
+// [kt0, kt1) of the C block's task sequence (every task's k tiles in task
+// order).  slot < 0: the item covers all k tiles and writes C itself;
+// slot >= 0: a k chunk whose partial tile goes to workspace slot `slot`,
+// summed in chunk order by the split reduction.
 struct DItem {
     int32_t cblk;
     int32_t m0, n0;
+    int32_t slot;
+    int32_t kt0, kt1;
+};
+
+// A tile whose k range was split into nparts chunks (workspace slots
+// slot0 .. slot0 + nparts - 1, in k order).
+struct DSplit {
+    int32_t cblk;
+    int32_t m0, n0;
+    int32_t nparts;
+    int32_t slot0;
     int32_t pad;
 };
+
+inline DItem make_item(int32_t cblk, int32_t m0, int32_t n0) {
+    DItem it;
+    it.cblk = cblk; it.m0 = m0; it.n0 = n0;
+    it.slot = -1; it.kt0 = 0; it.kt1 = INT32_MAX;
+    return it;
+}
 
 // ---------------------------------------------------------------- split precision
 
@@ -260,10 +282,16 @@ __host__ __device__ inline double seeded_value(const DGenGroup &g, uint64_t seed
 
 // ---------------------------------------------------------------- launchers
 
-// Plain FP64 DMMA grouped contraction over all work items.
+// Plain FP64 DMMA grouped contraction over all work items; partial tiles of
+// k-split items go to ws (BM x BN doubles per slot).
 cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     const DItem *items, int32_t nitems, int32_t *counter, const double *a,
-    const double *b, double *c, int32_t add, int32_t tile_cfg, cudaStream_t s);
+    const double *b, double *c, double *ws, int32_t add, int32_t tile_cfg, cudaStream_t s);
+// Sums the partial tiles of every split tile in chunk order and writes (or
+// adds) the scaled result into its C block.
+cudaError_t launch_split_reduce(const DSplit *splits, int32_t nsplits, const DCBlock *cblks,
+    const double *ws, int32_t bm, int32_t bn, double *c, int32_t add, cudaStream_t s);
+int tile_cfg_bk(int cfg);
 
 // Split-precision contraction: FP64 -> slice tile images, then the tcgen05
 // grouped slice-product kernel with FP64 recombination.
