@@ -33,6 +33,7 @@ WORKLOADS = {
     "ladder-prof": "LADDER_PROF",
     "ring": "RING_D2H",
     "ring-small": "RING_D2H_SMALL",
+    "dense": "DENSE_6144",
 }
 # HBM-bound operations (btod_copy / btod_add / btod_dotprod) on the CCD
 # iteration's tensors, o=30 v=300 (blocks 15 / 50,50,50 per spin).
@@ -80,7 +81,11 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-DMMA companion timing")
+    p.add_argument("--no-fused-split", action="store_true",
+                   help="modular mode: exponent pass and residue pass instead of the one-read split")
     p.add_argument("--tile", type=int, default=-1, help="force one tile shape (debug)")
+    p.add_argument("--split-k", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                   help="plain mode: k chunks per tile (0 automatic, 1 never)")
     p.add_argument("--crt-rows", type=int, default=0, choices=[0, 128, 256],
                    help="modular mode: rows of the products kernel's work items (0: default, 256)")
     a = p.parse_args()
@@ -227,7 +232,7 @@ def metric_name():
 def config_of(args, cfg, flops):
     return {"workload": f"{cfg.name} ({args.workload})", "mode": args.mode, "nslices": args.nslices,
             "o": cfg.o, "v": cfg.v, "algorithmic_flops": flops,
-            "l2": "inputs larger than L2 (no flush)" if args.workload in ("ladder-large", "ladder-split", "ring", "ladder-ccd") else "small inputs, L2-resident"}
+            "l2": "inputs larger than L2 (no flush)" if args.workload in ("ladder-large", "ladder-split", "ring", "ladder-ccd", "dense") else "small inputs, L2-resident"}
 
 
 # ---------------------------------------------------------------- ltg arm
@@ -285,6 +290,10 @@ def ltg_arm(args):
     tiles = None
     if args.crt_rows:
         op.set_crt_rows(args.crt_rows)
+    if args.split_k:
+        op.set_split_k(args.split_k)
+    if args.no_fused_split:
+        op.set_fused_split(False)
     if args.tile >= 0:
         op.set_tile(args.tile)
     elif not args.no_autotune:

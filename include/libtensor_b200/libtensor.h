@@ -35,6 +35,8 @@
 #define LIBTENSOR_B200_LIBTENSOR_H
 
 #include <array>
+#include <functional>
+#include <initializer_list>
 #include <cstddef>
 #include <cstdint>
 #include <map>
@@ -538,8 +540,19 @@ public:
 
 // ---------------------------------------------------------------- operations
 
+// An operation whose result can be assigned to or added into a block tensor
+// (the role of libtensor's additive_gen_bto, gen_block_tensor/additive_gen_bto.h):
+// what the symmetrizers wrap.
+template<size_t N>
+class additive_bto {
+public:
+    virtual ~additive_bto() { }
+    virtual void perform(block_tensor<N, double> &btb) = 0;
+    virtual void perform(block_tensor<N, double> &btb, double d) = 0;
+};
+
 template<size_t N, size_t M, size_t K>
-class btod_contract2 {
+class btod_contract2 : public additive_bto<N + M> {
     ltg_plan *m_plan = nullptr;
     double m_ka, m_kb, m_kc;
     int32_t m_mode = LTG_MODE_PLAIN_FP64, m_nslices = 0;
@@ -580,9 +593,9 @@ public:
     }
     ~btod_contract2() { if (m_plan) ltg_plan_destroy(m_plan); }
     // C = contraction (assign)
-    void perform(block_tensor<N + M, double> &btc) { run(btc, 0, 0.0); }
+    void perform(block_tensor<N + M, double> &btc) override { run(btc, 0, 0.0); }
     // C += d * contraction
-    void perform(block_tensor<N + M, double> &btc, double d) { run(btc, 1, d); }
+    void perform(block_tensor<N + M, double> &btc, double d) override { run(btc, 1, d); }
     void perform(block_tensor<N + M, double> &btc, const scalar_transf<double> &d) { run(btc, 1, d.get_coeff()); }
     // non-zero canonical result blocks (get_schedule), as absolute indices
     std::vector<int64_t> get_schedule() const {
@@ -604,7 +617,7 @@ public:
 };
 
 template<size_t N>
-class btod_copy {
+class btod_copy : public additive_bto<N> {
     block_tensor<N, double> &m_a;
     permutation<N> m_perm;
     double m_c;
@@ -614,7 +627,7 @@ public:
     btod_copy(block_tensor<N, double> &bta, const permutation<N> &perm, double c = 1.0)
         : m_a(bta), m_perm(perm), m_c(c) { }
     // B = c P(A): B takes the permuted space and symmetry of A
-    void perform(block_tensor<N, double> &btb) {
+    void perform(block_tensor<N, double> &btb) override {
         const std::vector<int32_t> p = m_perm.to_vector();
         if (!(btb.is_bound() && btb.handle() == m_adopted)) {
             ltg_bt *b = nullptr;
@@ -625,14 +638,14 @@ public:
         b200::check(ltg_copy(m_a.handle(), p.data(), m_c, btb.handle(), 0, 0.0));
     }
     // B += d c P(A)
-    void perform(block_tensor<N, double> &btb, double d) {
+    void perform(block_tensor<N, double> &btb, double d) override {
         const std::vector<int32_t> p = m_perm.to_vector();
         b200::check(ltg_copy(m_a.handle(), p.data(), m_c, btb.handle(), 1, d));
     }
 };
 
 template<size_t N>
-class btod_add {
+class btod_add : public additive_bto<N> {
     std::vector<block_tensor<N, double> *> m_ops;
     std::vector<permutation<N> > m_perms;
     std::vector<double> m_coeffs;
@@ -655,8 +668,8 @@ public:
         m_perms.push_back(perm);
         m_coeffs.push_back(c);
     }
-    void perform(block_tensor<N, double> &btb) { call(btb, 0, 0.0); }
-    void perform(block_tensor<N, double> &btb, double d) { call(btb, 1, d); }
+    void perform(block_tensor<N, double> &btb) override { call(btb, 0, 0.0); }
+    void perform(block_tensor<N, double> &btb, double d) override { call(btb, 1, d); }
 };
 
 template<size_t N>
@@ -760,6 +773,39 @@ label<N + 1> operator|(const label<N> &e, const letter &l) {
 template<size_t N, typename T = double>
 using btensor = block_tensor<N, T>;
 
+namespace b200 {
+
+// CUDA graph of a sequence of operations (ltg_graph_begin/end/launch): run
+// every operation once before the capture (their plans are built then), capture
+// the sequence, then launch it as often as needed.
+class graph {
+    ltg_graph *m_g = nullptr;
+public:
+    explicit graph(ltg_graph *g) : m_g(g) { }
+    graph(graph &&o) noexcept : m_g(o.m_g) { o.m_g = nullptr; }
+    graph(const graph &) = delete;
+    graph &operator=(const graph &) = delete;
+    ~graph() { if (m_g) ltg_graph_destroy(m_g); }
+    void launch() { check(ltg_graph_launch(m_g)); }
+};
+inline void begin_capture() { check(ltg_graph_begin(context())); }
+inline graph end_capture() {
+    ltg_graph *g = nullptr;
+    check(ltg_graph_end(context(), &g));
+    return graph(g);
+}
+inline void synchronize() { check(ltg_ctx_synchronize(context())); }
+
+// Arithmetic of the letter interface's contractions (ltg.h modes; default
+// LTG_MODE_PLAIN_FP64, the FP64 drop-in path).
+struct expr_precision { int32_t mode = LTG_MODE_PLAIN_FP64, nslices = 0; };
+inline expr_precision &letter_precision() { static expr_precision p; return p; }
+inline void set_letter_precision(int32_t mode, int32_t nslices) {
+    letter_precision().mode = mode;
+    letter_precision().nslices = nslices;
+}
+}  // namespace b200
+
 namespace expr_detail {
 
 // Permutation taking a tensor labelled `from` to the order of `to`:
@@ -790,6 +836,49 @@ label<N> relabel(const label<N> &l, const letter_swap &sw) {
     return r;
 }
 
+// One dimension of a block index space: its extent and split points.
+struct dim_space {
+    size_t dim = 0;
+    std::vector<size_t> splits;
+};
+template<size_t N>
+dim_space dim_of(const block_index_space<N> &b, size_t i) {
+    dim_space d;
+    d.dim = b.get_dims()[i];
+    d.splits = b.get_splits(i);
+    return d;
+}
+template<size_t N>
+block_index_space<N> make_space(const std::vector<dim_space> &d) {
+    index<N> i1;
+    for (size_t i = 0; i < N; i++) i1[i] = d[i].dim - 1;
+    block_index_space<N> bis(dimensions<N>(index_range<N>(index<N>(), i1)));
+    for (size_t i = 0; i < N; i++) {
+        mask<N> m;
+        m[i] = true;
+        for (size_t x : d[i].splits) bis.split(m, x);
+    }
+    return bis;
+}
+
+// The operations of one assignment in order, each run as it is added (later
+// operations use the tensors earlier ones created), with the operation
+// objects and intermediates kept, so that the sequence can run again and be
+// captured as one CUDA graph (b200::assignment).
+struct program {
+    std::vector<std::function<void()> > steps;
+    std::vector<std::shared_ptr<void> > keep;
+    void add(std::function<void()> f) {
+        f();
+        steps.push_back(std::move(f));
+    }
+    void run() const {
+        for (const auto &f : steps) f();
+    }
+};
+
+template<size_t N> struct tensor_term;
+
 // One term of an expression of order N.
 template<size_t N>
 struct term {
@@ -799,9 +888,16 @@ struct term {
     virtual term *scaled(double f) const = 0;
     // the term with the letters of sw exchanged (the permuted term P E)
     virtual term *swapped(const letter_swap &sw) const = 0;
-    // contraction terms: evaluate into c (assign, or add d times the term)
+    // its letters in their natural order (an operand's own order; a
+    // contraction's: A's free letters, then B's)
+    virtual label<N> natural_label() const = 0;
+    // contraction terms: the operations that write the term into c (assign,
+    // or add d times the term), appended to pg
     virtual bool is_contraction() const = 0;
-    virtual void contract_into(block_tensor<N, double> &c, const label<N> &lc, bool add, double d) const = 0;
+    virtual void contract_into(program &pg, block_tensor<N, double> &c, const label<N> &lc, bool add,
+                               double d) const = 0;
+    // contraction terms: the term as an intermediate labelled l
+    virtual tensor_term<N> contract_temp(program &pg, const label<N> &l) const = 0;
 };
 
 template<size_t N>
@@ -820,15 +916,20 @@ struct tensor_term : term<N> {
         r->lab = relabel(lab, sw);
         return r;
     }
+    label<N> natural_label() const override { return lab; }
     bool is_contraction() const override { return false; }
-    void contract_into(block_tensor<N, double> &, const label<N> &, bool, double) const override {
+    void contract_into(program &, block_tensor<N, double> &, const label<N> &, bool, double) const override {
+        throw exception("tensor term evaluated as a contraction");
+    }
+    tensor_term<N> contract_temp(program &, const label<N> &) const override {
         throw exception("tensor term evaluated as a contraction");
     }
 };
 
 }  // namespace expr_detail
 
-// Right-hand side of order N: a sum of (scaled) tensor and contraction terms.
+// Right-hand side of order N: a sum of (scaled) tensor, contraction and
+// symmetrizer terms.
 template<size_t N, typename T = double>
 class expr_rhs {
     static_assert(sizeof(T) == 8, "expressions of double");
@@ -843,6 +944,22 @@ public:
         if (!t) throw bad_parameter(std::string(what) + ": operands must be (scaled) tensors");
         return *t;
     }
+    bool uses(const void *p) const {
+        for (const auto &t : terms) if (t->uses(p)) return true;
+        return false;
+    }
+    // the letters of the expression: those of its first term, which every
+    // other term must have too (in any order)
+    label<N> natural_label() const {
+        if (terms.empty()) throw bad_parameter("empty expression");
+        const label<N> l = terms[0]->natural_label();
+        for (const auto &t : terms) {
+            const label<N> m = t->natural_label();
+            for (size_t i = 0; i < N; i++)
+                if (!l.contains(m.letter_at(i))) throw bad_parameter("terms of a sum with different letters");
+        }
+        return l;
+    }
 };
 
 namespace expr_detail {
@@ -855,10 +972,7 @@ struct symm_term : term<N> {
     letter_swap sw;
     double sign;
     symm_term(const expr_rhs<N> &e, const letter_swap &s, double sg) : sub(e), sw(s), sign(sg) { }
-    bool uses(const void *p) const override {
-        for (const auto &t : sub.terms) if (t->uses(p)) return true;
-        return false;
-    }
+    bool uses(const void *p) const override { return sub.uses(p); }
     term<N> *scaled(double f) const override {
         symm_term *r = new symm_term(*this);
         r->coeff *= f;
@@ -873,11 +987,90 @@ struct symm_term : term<N> {
         r->coeff = this->coeff;
         return r;
     }
+    label<N> natural_label() const override { return sub.natural_label(); }
     bool is_contraction() const override { return false; }
-    void contract_into(block_tensor<N, double> &, const label<N> &, bool, double) const override {
+    void contract_into(program &, block_tensor<N, double> &, const label<N> &, bool, double) const override {
+        throw exception("symmetrizer evaluated as a contraction");
+    }
+    tensor_term<N> contract_temp(program &, const label<N> &) const override {
         throw exception("symmetrizer evaluated as a contraction");
     }
 };
+
+// The terms of e (times f) as contraction terms and (scaled) tensor terms;
+// symmetrizers are expanded, the contraction terms inside them evaluated once
+// into intermediates labelled l.
+template<size_t N>
+void flatten(const expr_rhs<N> &e, double f, const label<N> &l, program &pg,
+             std::vector<std::shared_ptr<term<N> > > &contr, std::vector<tensor_term<N> > &tens) {
+    for (const auto &t : e.terms) {
+        if (t->is_contraction()) { contr.emplace_back(t->scaled(f)); continue; }
+        if (const tensor_term<N> *x = dynamic_cast<const tensor_term<N> *>(t.get())) {
+            tens.push_back(*x);
+            tens.back().coeff *= f;
+            continue;
+        }
+        const symm_term<N> &y = dynamic_cast<const symm_term<N> &>(*t);
+        std::vector<std::shared_ptr<term<N> > > sc;
+        std::vector<tensor_term<N> > st;
+        flatten(y.sub, 1.0, l, pg, sc, st);
+        for (const auto &c : sc) st.push_back(c->contract_temp(pg, l));
+        for (const tensor_term<N> &x : st) {
+            tens.push_back(x);
+            tens.back().coeff *= f * y.coeff;
+            tens.push_back(x);
+            tens.back().lab = relabel(x.lab, y.sw);
+            tens.back().coeff *= f * y.coeff * y.sign;
+        }
+    }
+}
+
+// An intermediate holding the sum of tensor terms, labelled l: the block
+// index space of the terms and the symmetry common to all of them
+// (ltg_bt_create_sum_space), assigned with one btod_add.
+template<size_t N>
+tensor_term<N> sum_temp(program &pg, const std::vector<tensor_term<N> > &tens, const label<N> &l) {
+    std::vector<ltg_bt *> hs;
+    std::vector<int32_t> perms;
+    for (const tensor_term<N> &x : tens) {
+        hs.push_back(x.bt->handle());
+        const std::vector<int32_t> p = align(x.lab, l).to_vector();
+        perms.insert(perms.end(), p.begin(), p.end());
+    }
+    const permutation<N> p0 = align(tens[0].lab, l);
+    std::vector<dim_space> d(N);
+    for (size_t i = 0; i < N; i++) d[i] = dim_of(tens[0].bt->get_bis(), p0.to_vector()[i]);
+    std::shared_ptr<block_tensor<N, double> > tmp(new block_tensor<N, double>(make_space<N>(d)));
+    ltg_bt *h = nullptr;
+    b200::check(ltg_bt_create_sum_space((int32_t)hs.size(), hs.data(), perms.data(), &h));
+    tmp->adopt(h);
+    std::shared_ptr<btod_add<N> > op;
+    for (const tensor_term<N> &x : tens) {
+        if (!op) op.reset(new btod_add<N>(*x.bt, align(x.lab, l), x.coeff));
+        else op->add_op(*x.bt, align(x.lab, l), x.coeff);
+    }
+    pg.keep.push_back(tmp);
+    pg.keep.push_back(op);
+    block_tensor<N, double> *t = tmp.get();
+    btod_add<N> *o = op.get();
+    pg.add([o, t] { o->perform(*t); });
+    return tensor_term<N>(*t, l);
+}
+
+// The expression as one (scaled) tensor: itself when it is one, else an
+// intermediate labelled with its natural letters.
+template<size_t N>
+tensor_term<N> materialize(const expr_rhs<N> &e, program &pg) {
+    if (e.terms.size() == 1)
+        if (const tensor_term<N> *x = dynamic_cast<const tensor_term<N> *>(e.terms[0].get())) return *x;
+    const label<N> l = e.natural_label();
+    std::vector<std::shared_ptr<term<N> > > contr;
+    std::vector<tensor_term<N> > tens;
+    flatten(e, 1.0, l, pg, contr, tens);
+    for (const auto &c : contr) tens.push_back(c->contract_temp(pg, l));
+    if (tens.size() == 1) return tens[0];
+    return sum_temp(pg, tens, l);
+}
 
 }  // namespace expr_detail
 
@@ -885,76 +1078,59 @@ template<size_t N>
 class labeled_btensor {
     block_tensor<N, double> &m_bt;
     label<N> m_label;
-    // The terms as contractions into the result and a flat list of (scaled)
-    // tensor terms; symmetrizers are expanded, their contraction terms
-    // evaluated once into temporaries kept in `temps`.
-    void flatten(const expr_rhs<N> &e, double f, std::vector<std::shared_ptr<expr_detail::term<N> > > &contr,
-                 std::vector<expr_detail::tensor_term<N> > &tens,
-                 std::vector<std::unique_ptr<block_tensor<N, double> > > &temps) {
-        for (const auto &t : e.terms) {
-            if (t->is_contraction()) { contr.emplace_back(t->scaled(f)); continue; }
-            if (const expr_detail::tensor_term<N> *x = dynamic_cast<const expr_detail::tensor_term<N> *>(t.get())) {
-                tens.push_back(*x);
-                tens.back().coeff *= f;
-                continue;
-            }
-            const expr_detail::symm_term<N> &y = dynamic_cast<const expr_detail::symm_term<N> &>(*t);
-            std::vector<std::shared_ptr<expr_detail::term<N> > > sc;
-            std::vector<expr_detail::tensor_term<N> > st;
-            flatten(y.sub, 1.0, sc, st, temps);
-            if (!sc.empty()) {
-                temps.emplace_back(new block_tensor<N, double>(m_bt.get_bis()));
-                block_tensor<N, double> &tmp = *temps.back();
-                for (size_t k = 0; k < sc.size(); k++) sc[k]->contract_into(tmp, m_label, k > 0, 1.0);
-                st.push_back(expr_detail::tensor_term<N>(tmp, m_label));
-            }
-            for (const expr_detail::tensor_term<N> &x : st) {
-                tens.push_back(x);
-                tens.back().coeff *= f * y.coeff;
-                tens.push_back(x);
-                tens.back().lab = expr_detail::relabel(x.lab, y.sw);
-                tens.back().coeff *= f * y.coeff * y.sign;
-            }
+public:
+    // The operations of  this = e  (add: this += sign e) appended to pg.
+    void evaluate(expr_detail::program &pg, const expr_rhs<N> &e, bool add, double sign) {
+        if (e.uses(&m_bt)) {
+            // the result on the right-hand side: the whole expression into an
+            // intermediate first, then into the result
+            const expr_detail::tensor_term<N> x = expr_detail::materialize(e, pg);
+            std::shared_ptr<btod_add<N> > op(new btod_add<N>(*x.bt, expr_detail::align(x.lab, m_label), x.coeff));
+            pg.keep.push_back(op);
+            btod_add<N> *o = op.get();
+            block_tensor<N, double> *r = &m_bt;
+            if (add) pg.add([o, r, sign] { o->perform(*r, sign); });
+            else if (sign == 1.0) pg.add([o, r] { o->perform(*r); });
+            else pg.add([o, r, sign] { b200::check(ltg_bt_set_zero(r->handle())); o->perform(*r, sign); });
+            return;
         }
-    }
-    void evaluate(const expr_rhs<N> &e, bool add, double sign) {
-        for (const auto &t : e.terms)
-            if (t->uses(&m_bt)) throw bad_parameter("letter interface: the result appears on the right-hand side");
         std::vector<std::shared_ptr<expr_detail::term<N> > > contr;
         std::vector<expr_detail::tensor_term<N> > tens;
-        std::vector<std::unique_ptr<block_tensor<N, double> > > temps;
-        flatten(e, 1.0, contr, tens, temps);
+        expr_detail::flatten(e, 1.0, m_label, pg, contr, tens);
         bool written = add;
         for (const auto &t : contr) {
-            t->contract_into(m_bt, m_label, written, sign);
+            t->contract_into(pg, m_bt, m_label, written, sign);
             written = true;
         }
-        std::unique_ptr<btod_add<N> > sum;
+        std::shared_ptr<btod_add<N> > sum;
         for (const expr_detail::tensor_term<N> &x : tens) {
             const permutation<N> p = expr_detail::align(x.lab, m_label);
             if (!sum) sum.reset(new btod_add<N>(*x.bt, p, x.coeff));
             else sum->add_op(*x.bt, p, x.coeff);
         }
-        if (!sum && !written) b200::check(ltg_bt_set_zero(m_bt.handle()));
-        if (sum) {
-            if (written) sum->perform(m_bt, sign);
-            else if (sign == 1.0) sum->perform(m_bt);
-            else {
-                // assignment of a negated sum: C = 0 - ... is C += -sum after zeroing
-                b200::check(ltg_bt_set_zero(m_bt.handle()));
-                sum->perform(m_bt, sign);
-            }
+        block_tensor<N, double> *r = &m_bt;
+        if (!sum) {
+            if (!written) pg.add([r] { b200::check(ltg_bt_set_zero(r->handle())); });
+            return;
         }
+        pg.keep.push_back(sum);
+        btod_add<N> *o = sum.get();
+        if (written) pg.add([o, r, sign] { o->perform(*r, sign); });
+        else if (sign == 1.0) pg.add([o, r] { o->perform(*r); });
+        else pg.add([o, r, sign] {
+            // assignment of a negated sum: C = 0 - ... is C += -sum after zeroing
+            b200::check(ltg_bt_set_zero(r->handle()));
+            o->perform(*r, sign);
+        });
     }
-public:
     labeled_btensor(block_tensor<N, double> &bt, const label<N> &l) : m_bt(bt), m_label(l) { }
     block_tensor<N, double> &get_btensor() const { return m_bt; }
     const label<N> &get_label() const { return m_label; }
     operator expr_rhs<N>() const { return expr_rhs<N>(new expr_detail::tensor_term<N>(m_bt, m_label)); }
-    labeled_btensor &operator=(const expr_rhs<N> &e) { evaluate(e, false, 1.0); return *this; }
-    labeled_btensor &operator=(const labeled_btensor &o) { evaluate(expr_rhs<N>(o), false, 1.0); return *this; }
-    labeled_btensor &operator+=(const expr_rhs<N> &e) { evaluate(e, true, 1.0); return *this; }
-    labeled_btensor &operator-=(const expr_rhs<N> &e) { evaluate(e, true, -1.0); return *this; }
+    labeled_btensor &operator=(const expr_rhs<N> &e) { expr_detail::program pg; evaluate(pg, e, false, 1.0); return *this; }
+    labeled_btensor &operator=(const labeled_btensor &o) { return *this = expr_rhs<N>(o); }
+    labeled_btensor &operator+=(const expr_rhs<N> &e) { expr_detail::program pg; evaluate(pg, e, true, 1.0); return *this; }
+    labeled_btensor &operator-=(const expr_rhs<N> &e) { expr_detail::program pg; evaluate(pg, e, true, -1.0); return *this; }
 };
 
 template<size_t N, typename T>
@@ -992,56 +1168,57 @@ template<size_t N> expr_rhs<N> operator-(const labeled_btensor<N> &a) { return -
 
 namespace b200 {
 
-// CUDA graph of a sequence of operations (ltg_graph_begin/end/launch): run
-// every operation once before the capture (their plans are built then), capture
-// the sequence, then launch it as often as needed.
-class graph {
-    ltg_graph *m_g = nullptr;
+// One letter-interface assignment kept for repeated runs: constructing it
+// evaluates  lhs = rhs  (mode 0; +1: +=, -1: -=) once, keeping every
+// operation and intermediate (nested contractions, contractions of sums,
+// symmetrizers); run() evaluates it again with the same operations, and
+// after capture() run() launches the whole assignment as one CUDA graph.
+// The tensors named in the expression must outlive the object.
+template<size_t N>
+class assignment {
+    std::shared_ptr<expr_detail::program> m_pg;
+    std::unique_ptr<graph> m_graph;
 public:
-    explicit graph(ltg_graph *g) : m_g(g) { }
-    graph(graph &&o) noexcept : m_g(o.m_g) { o.m_g = nullptr; }
-    graph(const graph &) = delete;
-    graph &operator=(const graph &) = delete;
-    ~graph() { if (m_g) ltg_graph_destroy(m_g); }
-    void launch() { check(ltg_graph_launch(m_g)); }
+    assignment(labeled_btensor<N> lhs, const expr_rhs<N> &rhs, int mode = 0) : m_pg(new expr_detail::program()) {
+        lhs.evaluate(*m_pg, rhs, mode != 0, mode < 0 ? -1.0 : 1.0);
+    }
+    void run() {
+        if (m_graph) m_graph->launch();
+        else m_pg->run();
+    }
+    void capture() {
+        begin_capture();
+        try {
+            m_pg->run();
+        } catch (...) {
+            end_capture();
+            throw;
+        }
+        m_graph.reset(new graph(end_capture()));
+    }
+    size_t operations() const { return m_pg->steps.size(); }
 };
-inline void begin_capture() { check(ltg_graph_begin(context())); }
-inline graph end_capture() {
-    ltg_graph *g = nullptr;
-    check(ltg_graph_end(context(), &g));
-    return graph(g);
-}
-inline void synchronize() { check(ltg_ctx_synchronize(context())); }
-
-// Arithmetic of the letter interface's contractions (ltg.h modes; default
-// LTG_MODE_PLAIN_FP64, the FP64 drop-in path).
-struct expr_precision { int32_t mode = LTG_MODE_PLAIN_FP64, nslices = 0; };
-inline expr_precision &letter_precision() { static expr_precision p; return p; }
-inline void set_letter_precision(int32_t mode, int32_t nslices) {
-    letter_precision().mode = mode;
-    letter_precision().nslices = nslices;
-}
 }  // namespace b200
 
 namespace expr_detail {
 
-// contraction of A (order NA) and B (order NB) over K letters
+// contraction of A (order NA) and B (order NB) over K letters; A and B are
+// expressions (intermediates evaluated first when they are not tensors)
 template<size_t NA, size_t NB, size_t K>
 struct contract_term : term<NA + NB - 2 * K> {
     static constexpr size_t NC = NA + NB - 2 * K;
-    block_tensor<NA, double> *a;
-    block_tensor<NB, double> *b;
+    expr_rhs<NA> ea;
+    expr_rhs<NB> eb;
     label<NA> la;
     label<NB> lb;
     label<K> lk;
-    contract_term(const tensor_term<NA> &x, const tensor_term<NB> &y, const label<K> &k)
-        : a(x.bt), b(y.bt), la(x.lab), lb(y.lab), lk(k) {
-        this->coeff = x.coeff * y.coeff;
+    contract_term(const expr_rhs<NA> &x, const expr_rhs<NB> &y, const label<K> &k)
+        : ea(x), eb(y), la(x.natural_label()), lb(y.natural_label()), lk(k) {
         for (size_t i = 0; i < K; i++)
             if (!la.contains(lk.letter_at(i)) || !lb.contains(lk.letter_at(i)))
                 throw bad_parameter("contract: a contracted letter is missing from an operand");
     }
-    bool uses(const void *p) const override { return p == (const void *)a || p == (const void *)b; }
+    bool uses(const void *p) const override { return ea.uses(p) || eb.uses(p); }
     term<NC> *scaled(double f) const override {
         contract_term *r = new contract_term(*this);
         r->coeff *= f;
@@ -1050,17 +1227,31 @@ struct contract_term : term<NA + NB - 2 * K> {
     term<NC> *swapped(const letter_swap &sw) const override {
         for (size_t i = 0; i < K; i++)
             if (sw.map(lk.ptr(i)) != lk.ptr(i)) throw bad_parameter("symm/asymm: a contracted letter is exchanged");
-        contract_term *r = new contract_term(*this);
-        r->la = relabel(la, sw);
-        r->lb = relabel(lb, sw);
+        expr_rhs<NA> xa;
+        expr_rhs<NB> xb;
+        for (const auto &t : ea.terms) xa.terms.emplace_back(t->swapped(sw));
+        for (const auto &t : eb.terms) xb.terms.emplace_back(t->swapped(sw));
+        contract_term *r = new contract_term(xa, xb, lk);
+        r->coeff = this->coeff;
         return r;
     }
+    label<NC> natural_label() const override {
+        label<NC> l;
+        size_t k = 0;
+        for (size_t i = 0; i < NA; i++) if (!lk.contains(la.letter_at(i))) l.set(k++, la.ptr(i));
+        for (size_t i = 0; i < NB; i++) if (!lk.contains(lb.letter_at(i))) l.set(k++, lb.ptr(i));
+        if (k != NC) throw bad_parameter("contract: uncontracted letters do not match the result");
+        return l;
+    }
     bool is_contraction() const override { return true; }
-    void contract_into(block_tensor<NC, double> &c, const label<NC> &lc, bool add, double d) const override {
+    void contract_into(program &pg, block_tensor<NC, double> &c, const label<NC> &lc, bool add,
+                       double d) const override {
+        const tensor_term<NA> x = materialize(ea, pg);
+        const tensor_term<NB> y = materialize(eb, pg);
         // natural result order: A's free letters, then B's (contraction2)
         std::vector<const letter *> nat;
-        for (size_t i = 0; i < NA; i++) if (!lk.contains(la.letter_at(i))) nat.push_back(la.ptr(i));
-        for (size_t i = 0; i < NB; i++) if (!lk.contains(lb.letter_at(i))) nat.push_back(lb.ptr(i));
+        for (size_t i = 0; i < NA; i++) if (!lk.contains(x.lab.letter_at(i))) nat.push_back(x.lab.ptr(i));
+        for (size_t i = 0; i < NB; i++) if (!lk.contains(y.lab.letter_at(i))) nat.push_back(y.lab.ptr(i));
         if (nat.size() != NC) throw bad_parameter("contract: uncontracted letters do not match the result");
         std::vector<size_t> pc(NC);
         for (size_t dd = 0; dd < NC; dd++) {
@@ -1070,26 +1261,54 @@ struct contract_term : term<NA + NB - 2 * K> {
             pc[dd] = k;
         }
         contraction2<NA - K, NB - K, K> contr{permutation<NC>(pc)};
-        for (size_t i = 0; i < K; i++) contr.contract(la.index_of(lk.letter_at(i)), lb.index_of(lk.letter_at(i)));
-        btod_contract2<NA - K, NB - K, K> op(contr, *a, 1.0, *b, 1.0, this->coeff);
-        op.set_split_precision(b200::letter_precision().mode, b200::letter_precision().nslices);
-        if (add) op.perform(c, d);
-        else if (d == 1.0) op.perform(c);
-        else {
-            op.perform(c);
-            b200::check(ltg_scale(c.handle(), d));
+        for (size_t i = 0; i < K; i++) contr.contract(x.lab.index_of(lk.letter_at(i)), y.lab.index_of(lk.letter_at(i)));
+        std::shared_ptr<btod_contract2<NA - K, NB - K, K> > op(
+            new btod_contract2<NA - K, NB - K, K>(contr, *x.bt, 1.0, *y.bt, 1.0, this->coeff * x.coeff * y.coeff));
+        op->set_split_precision(b200::letter_precision().mode, b200::letter_precision().nslices);
+        pg.keep.push_back(op);
+        btod_contract2<NA - K, NB - K, K> *o = op.get();
+        block_tensor<NC, double> *t = &c;
+        if (add) pg.add([o, t, d] { o->perform(*t, d); });
+        else if (d == 1.0) pg.add([o, t] { o->perform(*t); });
+        else pg.add([o, t, d] {
+            o->perform(*t);
+            b200::check(ltg_scale(t->handle(), d));
+        });
+    }
+    tensor_term<NC> contract_temp(program &pg, const label<NC> &l) const override {
+        // the intermediate's index space from the operands' dims (their
+        // letters' dims); its symmetry is the contraction's result symmetry,
+        // taken on by the assignment
+        const tensor_term<NA> x = materialize(ea, pg);
+        const tensor_term<NB> y = materialize(eb, pg);
+        std::vector<dim_space> d(NC);
+        for (size_t i = 0; i < NC; i++) {
+            const letter &w = l.letter_at(i);
+            if (x.lab.contains(w)) d[i] = dim_of(x.bt->get_bis(), x.lab.index_of(w));
+            else d[i] = dim_of(y.bt->get_bis(), y.lab.index_of(w));
         }
+        std::shared_ptr<block_tensor<NC, double> > tmp(new block_tensor<NC, double>(make_space<NC>(d)));
+        pg.keep.push_back(tmp);
+        expr_rhs<NA> xa;
+        xa.terms.emplace_back(new tensor_term<NA>(x));
+        expr_rhs<NB> xb;
+        xb.terms.emplace_back(new tensor_term<NB>(y));
+        contract_term done(xa, xb, lk);
+        done.coeff = this->coeff;
+        done.contract_into(pg, *tmp, l, false, 1.0);
+        return tensor_term<NC>(*tmp, l);
     }
 };
 
 }  // namespace expr_detail
 
-// contract(letters, A(...), B(...)) (libtensor/expr/operators/contract.h)
+// contract(letters, A(...), B(...)) (libtensor/expr/operators/contract.h);
+// A and B may be any expressions (sums, contractions, symmetrizers), which
+// are evaluated into intermediates first
 template<size_t K, size_t NA, size_t NB>
 expr_rhs<NA + NB - 2 * K> contract(const label<K> &lk, const expr_rhs<NA> &a, const expr_rhs<NB> &b) {
     static_assert(K >= 1 && K <= NA && K <= NB && NA + NB > 2 * K, "contraction orders");
-    return expr_rhs<NA + NB - 2 * K>(new expr_detail::contract_term<NA, NB, K>(a.as_tensor("contract"),
-                                                                               b.as_tensor("contract"), lk));
+    return expr_rhs<NA + NB - 2 * K>(new expr_detail::contract_term<NA, NB, K>(a, b, lk));
 }
 template<size_t NA, size_t NB>
 expr_rhs<NA + NB - 2> contract(const letter &l, const expr_rhs<NA> &a, const expr_rhs<NB> &b) {
@@ -1099,15 +1318,34 @@ template<size_t K, size_t NA, size_t NB>
 expr_rhs<NA + NB - 2 * K> contract(const label<K> &lk, const labeled_btensor<NA> &a, const labeled_btensor<NB> &b) {
     return contract(lk, expr_rhs<NA>(a), expr_rhs<NB>(b));
 }
+template<size_t K, size_t NA, size_t NB>
+expr_rhs<NA + NB - 2 * K> contract(const label<K> &lk, const expr_rhs<NA> &a, const labeled_btensor<NB> &b) {
+    return contract(lk, a, expr_rhs<NB>(b));
+}
+template<size_t K, size_t NA, size_t NB>
+expr_rhs<NA + NB - 2 * K> contract(const label<K> &lk, const labeled_btensor<NA> &a, const expr_rhs<NB> &b) {
+    return contract(lk, expr_rhs<NA>(a), b);
+}
 template<size_t NA, size_t NB>
 expr_rhs<NA + NB - 2> contract(const letter &l, const labeled_btensor<NA> &a, const labeled_btensor<NB> &b) {
     return contract(label<1>(l), expr_rhs<NA>(a), expr_rhs<NB>(b));
 }
+template<size_t NA, size_t NB>
+expr_rhs<NA + NB - 2> contract(const letter &l, const expr_rhs<NA> &a, const labeled_btensor<NB> &b) {
+    return contract(label<1>(l), a, expr_rhs<NB>(b));
+}
+template<size_t NA, size_t NB>
+expr_rhs<NA + NB - 2> contract(const letter &l, const labeled_btensor<NA> &a, const expr_rhs<NB> &b) {
+    return contract(label<1>(l), expr_rhs<NA>(a), b);
+}
 
-// dot_product(A(...), B(...)) (libtensor/expr/operators/dot_product.h)
+// dot_product(A(...), B(...)) (libtensor/expr/operators/dot_product.h);
+// operands that are not tensors are evaluated into intermediates first
 template<size_t N>
 double dot_product(const expr_rhs<N> &a, const expr_rhs<N> &b) {
-    const expr_detail::tensor_term<N> &x = a.as_tensor("dot_product"), &y = b.as_tensor("dot_product");
+    expr_detail::program pg;
+    const expr_detail::tensor_term<N> x = expr_detail::materialize(a, pg);
+    const expr_detail::tensor_term<N> y = expr_detail::materialize(b, pg);
     return x.coeff * y.coeff *
            btod_dotprod<N>(*x.bt, permutation<N>(), *y.bt, expr_detail::align(y.lab, x.lab)).calculate();
 }
@@ -1115,6 +1353,10 @@ template<size_t N>
 double dot_product(const labeled_btensor<N> &a, const labeled_btensor<N> &b) {
     return dot_product(expr_rhs<N>(a), expr_rhs<N>(b));
 }
+template<size_t N>
+double dot_product(const expr_rhs<N> &a, const labeled_btensor<N> &b) { return dot_product(a, expr_rhs<N>(b)); }
+template<size_t N>
+double dot_product(const labeled_btensor<N> &a, const expr_rhs<N> &b) { return dot_product(expr_rhs<N>(a), b); }
 
 // symm / asymm (libtensor/expr/operators/symm_asymm.h): E + P E and E - P E,
 // P exchanging the letters of l1 with those of l2 (pairwise, simultaneously)
@@ -1143,27 +1385,84 @@ expr_rhs<N> symm(const letter &l1, const letter &l2, const labeled_btensor<N> &e
 template<size_t N>
 expr_rhs<N> asymm(const letter &l1, const letter &l2, const labeled_btensor<N> &e) { return asymm(l1, l2, expr_rhs<N>(e)); }
 
-// btod_symmetrize2 (libtensor/block_tensor/btod_symmetrize2.h:19-60) over a
-// tensor: B = A + P(A) (symm) or A - P(A), P exchanging indexes i1 and i2.
-// The reference wraps another operation; here the operand is its result.
+namespace b200 {
+
+// Symmetrizer of a tensor or of an operation's result (ltg_symmetrize): the
+// group of the exchange of two indexes, of a unitary permutation, or of the
+// 24 permutations of four indexes.  An operation is evaluated into a result
+// tensor the object keeps (its own result space), then summed over the
+// group; assigning gives B the symmetrized space (as the reference's
+// perform does), repeated assignments reuse it.
 template<size_t N>
-class btod_symmetrize2 {
-    block_tensor<N, double> &m_a;
-    permutation<N> m_p;
-    double m_sign;
+class symmetrizer : public additive_bto<N> {
+    block_tensor<N, double> *m_a = nullptr;          // a tensor, or
+    additive_bto<N> *m_op = nullptr;                 // an operation evaluated into m_tmp
+    std::unique_ptr<block_tensor<N, double> > m_tmp;
+    int32_t m_nidx;
+    std::vector<int32_t> m_idx;
+    bool m_symm;
+    ltg_bt *m_adopted = nullptr;
+    block_tensor<N, double> &source(block_tensor<N, double> &btb) {
+        if (m_a) return *m_a;
+        if (!m_tmp) m_tmp.reset(new block_tensor<N, double>(btb.get_bis()));
+        m_op->perform(*m_tmp);
+        return *m_tmp;
+    }
+protected:
+    symmetrizer(block_tensor<N, double> *a, additive_bto<N> *op, int32_t nidx, std::vector<int32_t> idx, bool symm)
+        : m_a(a), m_op(op), m_nidx(nidx), m_idx(std::move(idx)), m_symm(symm) { }
 public:
+    void perform(block_tensor<N, double> &btb) override {
+        block_tensor<N, double> &a = source(btb);
+        if (!(btb.is_bound() && btb.handle() == m_adopted)) {
+            ltg_bt *b = nullptr;
+            check(ltg_bt_create_symmetrized(a.handle(), m_nidx, m_idx.data(), m_symm ? 1 : 0, &b));
+            btb.adopt(b);
+            m_adopted = b;
+        }
+        check(ltg_symmetrize(a.handle(), 1.0, m_nidx, m_idx.data(), m_symm ? 1 : 0, btb.handle(), 0, 0.0));
+    }
+    void perform(block_tensor<N, double> &btb, double d) override {
+        block_tensor<N, double> &a = source(btb);
+        check(ltg_symmetrize(a.handle(), 1.0, m_nidx, m_idx.data(), m_symm ? 1 : 0, btb.handle(), 1, d));
+    }
+};
+
+inline std::vector<int32_t> idx_vec(std::initializer_list<size_t> l) {
+    std::vector<int32_t> v;
+    for (size_t x : l) v.push_back((int32_t)x);
+    return v;
+}
+template<size_t N>
+std::vector<int32_t> perm_vec(const permutation<N> &p) { return p.to_vector(); }
+}  // namespace b200
+
+// btod_symmetrize2 (libtensor/block_tensor/btod_symmetrize2.h:19-60):
+// B = A + P(A) (symm) or A - P(A) for the exchange of indexes i1 and i2 or a
+// unitary permutation P, A an operation's result or a tensor.
+template<size_t N>
+class btod_symmetrize2 : public b200::symmetrizer<N> {
+public:
+    btod_symmetrize2(additive_bto<N> &op, size_t i1, size_t i2, bool symm)
+        : b200::symmetrizer<N>(nullptr, &op, 2, b200::idx_vec({i1, i2}), symm) { }
+    btod_symmetrize2(additive_bto<N> &op, const permutation<N> &perm, bool symm)
+        : b200::symmetrizer<N>(nullptr, &op, -1, b200::perm_vec(perm), symm) { }
     btod_symmetrize2(block_tensor<N, double> &bta, size_t i1, size_t i2, bool symm)
-        : m_a(bta), m_sign(symm ? 1.0 : -1.0) { m_p.permute(i1, i2); }
-    void perform(block_tensor<N, double> &btb) {
-        btod_add<N> op(m_a, 1.0);
-        op.add_op(m_a, m_p, m_sign);
-        op.perform(btb);
-    }
-    void perform(block_tensor<N, double> &btb, double d) {
-        btod_add<N> op(m_a, 1.0);
-        op.add_op(m_a, m_p, m_sign);
-        op.perform(btb, d);
-    }
+        : b200::symmetrizer<N>(&bta, nullptr, 2, b200::idx_vec({i1, i2}), symm) { }
+    btod_symmetrize2(block_tensor<N, double> &bta, const permutation<N> &perm, bool symm)
+        : b200::symmetrizer<N>(&bta, nullptr, -1, b200::perm_vec(perm), symm) { }
+};
+
+// btod_symmetrize4 (libtensor/block_tensor/btod_symmetrize4.h:27-60): the sum
+// over the 24 permutations of indexes i1..i4 (with the permutation's parity
+// as sign when not symm) of A, an operation's result or a tensor.
+template<size_t N>
+class btod_symmetrize4 : public b200::symmetrizer<N> {
+public:
+    btod_symmetrize4(additive_bto<N> &op, size_t i1, size_t i2, size_t i3, size_t i4, bool symm)
+        : b200::symmetrizer<N>(nullptr, &op, 4, b200::idx_vec({i1, i2, i3, i4}), symm) { }
+    btod_symmetrize4(block_tensor<N, double> &bta, size_t i1, size_t i2, size_t i3, size_t i4, bool symm)
+        : b200::symmetrizer<N>(&bta, nullptr, 4, b200::idx_vec({i1, i2, i3, i4}), symm) { }
 };
 
 }  // namespace libtensor

@@ -127,6 +127,30 @@ int ltg_bt_create(ltg_ctx *ctx, const ltg_bt_spec *spec, ltg_bt **out);
 /* New tensor with the block index space and symmetry of `a` permuted by
  * `perm` (so_permute; the result space of btod_copy(a, perm)). */
 int ltg_bt_create_permuted(ltg_bt *a, const int32_t *perm, ltg_bt **out);
+/* A block tensor for the sum of the terms P_t(a_t) (perms[t*order ..], NULL =
+ * identities): the block index space of P_0(a_0) (all terms must have it) and
+ * the symmetry every term has -- the permutational (anti)symmetry elements
+ * common to all terms' groups, and the partition and label rules when all
+ * terms carry the same ones (otherwise none, every block allowed).  The
+ * intermediate of a sum in the letter interface; the reference derives the
+ * symmetry of btod_add's result with so_dirsum/so_merge
+ * (libtensor/gen_block_tensor/impl/gen_bto_add_impl.h:225-274), which this
+ * never exceeds. */
+int ltg_bt_create_sum_space(int32_t nterms, ltg_bt *const *a, const int32_t *perms, ltg_bt **out);
+/* Symmetrizers (libtensor/block_tensor/btod_symmetrize2.h:19,
+ * btod_symmetrize4.h:27) over a tensor: the symmetrizer's group S is
+ * nidx = 2: {e, (i1 i2)} with idx = (i1, i2); nidx = -1: {e, P} with idx the
+ * unitary permutation P (P P = e, e.g. a pair exchange); nidx = 4: the 24
+ * permutations of the indexes idx[0..3].  Signs: +1 with symm, else -1 for
+ * the exchange (the parity of the permutation for four indexes).
+ * ltg_bt_create_symmetrized: a block tensor for S-sums of a: a's block index
+ * space with S's generators, the elements of a's group that map S onto
+ * itself, and a's partition and label rules if S leaves them unchanged.
+ * ltg_symmetrize: b = c sum_{s in S} sign(s) P_s(a) (add: b += d c ...),
+ * asynchronous on the context stream. */
+int ltg_bt_create_symmetrized(ltg_bt *a, int32_t nidx, const int32_t *idx, int32_t symm, ltg_bt **out);
+int ltg_symmetrize(ltg_bt *a, double c, int32_t nidx, const int32_t *idx, int32_t symm, ltg_bt *b,
+                   int32_t add, double d);
 int ltg_bt_destroy(ltg_bt *bt);
 /* Canonical allowed blocks: count and packed arena size in elements. */
 int ltg_bt_info(const ltg_bt *bt, int32_t *order, int64_t *nblocks, int64_t *nelems);
@@ -179,6 +203,15 @@ int ltg_bt_device_ptr(ltg_bt *bt, double **ptr);
 int ltg_contract2_create(ltg_ctx *ctx, int32_t n, int32_t m, int32_t k,
                          const int32_t *permc, const int32_t *pairs,
                          ltg_bt *a, ltg_bt *b, ltg_plan **out);
+/* Schedules are cached process-wide: ltg_contract2_create with a contraction
+ * and operands of a description seen before (block index spaces, symmetry
+ * elements, non-zero blocks) reuses the earlier schedule instead of building
+ * it again (the reference builds it in every btod_contract2 constructor,
+ * libtensor/gen_block_tensor/impl/gen_bto_contract2_nzorb_impl.h:354-477).
+ * Capacity in schedules (default 64, least recently used dropped; 0 turns
+ * the cache off) and its hit/miss counts: */
+int ltg_schedule_cache_set_capacity(int64_t entries);
+int ltg_schedule_cache_stats(int64_t *hits, int64_t *misses, int64_t *entries);
 /* Creates an empty result tensor with the derived block index space and
  * symmetry (btod_contract2::get_bis / get_symmetry). */
 int ltg_contract2_make_result(ltg_plan *plan, ltg_bt **c);
@@ -224,6 +257,13 @@ int ltg_contract2_set_split_k(ltg_plan *plan, int32_t k);
  * a few rows, as under point-group symmetry, fill whole tiles).  No reference
  * counterpart. */
 int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable);
+/* Modular mode: enables (default) or disables the one-read split of row
+ * families -- panels whose rows feed the same rows of C and nothing else does
+ * -- which forms each row's exponent and its residues in one pass over the
+ * operand (the second read of each tile hits L2) instead of an exponent pass
+ * and a residue pass.  Both forms give identical bits.  No reference
+ * counterpart. */
+int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable);
 /* Modular mode: rows of the products kernel's work items, 256 (two MMA
  * tiles sharing each operand tile of the other side; also 0, the default) or
  * 128 (one MMA tile; the epilogue of one modulus overlaps the products of the

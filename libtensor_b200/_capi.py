@@ -58,6 +58,9 @@ _SIGS = {
     "ltg_ctx_launch_count": (C.c_int, [c_vp, c_i64p]),
     "ltg_bt_create": (C.c_int, [c_vp, C.POINTER(ltg_bt_spec), C.POINTER(c_vp)]),
     "ltg_bt_create_permuted": (C.c_int, [c_vp, c_i32p, C.POINTER(c_vp)]),
+    "ltg_bt_create_sum_space": (C.c_int, [C.c_int32, C.POINTER(c_vp), c_i32p, C.POINTER(c_vp)]),
+    "ltg_bt_create_symmetrized": (C.c_int, [c_vp, C.c_int32, c_i32p, C.c_int32, C.POINTER(c_vp)]),
+    "ltg_symmetrize": (C.c_int, [c_vp, C.c_double, C.c_int32, c_i32p, C.c_int32, c_vp, C.c_int32, C.c_double]),
     "ltg_bt_destroy": (C.c_int, [c_vp]),
     "ltg_bt_info": (C.c_int, [c_vp, c_i32p, c_i64p, c_i64p]),
     "ltg_bt_blocks": (C.c_int, [c_vp, c_i64p, c_i64p, c_i64p]),
@@ -87,8 +90,11 @@ _SIGS = {
                                 C.c_double, C.c_int32, C.c_double]),
     "ltg_plan_destroy": (C.c_int, [c_vp]),
     "ltg_contract2_set_tile": (C.c_int, [c_vp, C.c_int32]),
+    "ltg_schedule_cache_set_capacity": (C.c_int, [C.c_int64]),
+    "ltg_schedule_cache_stats": (C.c_int, [c_i64p, c_i64p, c_i64p]),
     "ltg_contract2_set_split_k": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_set_grouping": (C.c_int, [c_vp, C.c_int32]),
+    "ltg_contract2_set_fused_split": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_group_info": (C.c_int, [c_vp, c_vp, c_i64p, c_i64p, c_dblp, c_dblp]),
     "ltg_contract2_set_crt_rows": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_autotune": (C.c_int, [c_vp, c_vp, C.c_int32, C.c_int32, C.c_double, C.c_double,

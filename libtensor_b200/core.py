@@ -317,6 +317,10 @@ class btod_contract2:
         """Plain FP64 mode: k chunks per output tile (0 automatic, 1 never, 2-4 always)."""
         check(lib().ltg_contract2_set_split_k(self.h, k))
 
+    def set_fused_split(self, enable: bool):
+        """Modular mode: one-read split of row families (default on)."""
+        check(lib().ltg_contract2_set_fused_split(self.h, 1 if enable else 0))
+
     def set_grouping(self, enable: bool):
         """Modular mode: grouped products of small C blocks (default on)."""
         check(lib().ltg_contract2_set_grouping(self.h, 1 if enable else 0))
@@ -457,3 +461,32 @@ class btod_dotprod:
         check(lib().ltg_dotprod(self.a.h, _perm(self.pa, self.a.order), self.b.h,
                                 _perm(self.pb, self.b.order), C.byref(out)))
         return out.value
+
+
+def _symm_args(n, idx, perm):
+    if perm is not None:
+        return -1, _i32(list(perm))
+    return len(idx), _i32(list(idx))
+
+
+class btod_symmetrize:
+    """Symmetrizer of a tensor (btod_symmetrize2 / btod_symmetrize4,
+    libtensor/block_tensor/btod_symmetrize2.h:19, btod_symmetrize4.h:27):
+    B = sum over the group of sign * P(A) -- the exchange of two indexes
+    (idx of length 2), a unitary permutation (perm), or the 24 permutations
+    of four indexes (idx of length 4); sign +1 with symm, else the parity."""
+
+    def __init__(self, a: block_tensor, symm: bool, idx=(), perm=None, c: float = 1.0):
+        self.a, self.symm, self.c = a, symm, c
+        self.nidx, self.idx = _symm_args(a.order if hasattr(a, "order") else len(a.bidims), idx, perm)
+
+    def make_result(self) -> block_tensor:
+        """A tensor with the symmetrized space (ltg_bt_create_symmetrized)."""
+        h = C.c_void_p()
+        check(lib().ltg_bt_create_symmetrized(self.a.h, self.nidx, self.idx, 1 if self.symm else 0, C.byref(h)))
+        return block_tensor(self.a.ctx, None, _handle=h)
+
+    def perform(self, b: block_tensor, d: Optional[float] = None):
+        check(lib().ltg_symmetrize(self.a.h, self.c, self.nidx, self.idx, 1 if self.symm else 0, b.h,
+                                   0 if d is None else 1, 0.0 if d is None else d))
+

@@ -64,6 +64,11 @@ __device__ __forceinline__ void dmma_16x8x8(double *d, const double *a, const do
 // m16n8k16 (sm_90 and later): the A fragment is the two m16n8k8 fragments of
 // k 0-7 and 8-15 one after the other (registers a0-a3, a4-a7), the B
 // fragment likewise (b0-b1, b2-b3).
+// m8n8k4: lane (g, t) holds A[g][t], B[t][g] (k = t) and C[g][2t], C[g][2t+1].
+__device__ __forceinline__ void dmma_8x8x4(double *d, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b));
+}
 __device__ __forceinline__ void dmma_16x8x16(double *d, const double *a0, const double *a1, const double *b0,
                                              const double *b1) {
     asm volatile(
@@ -74,19 +79,27 @@ __device__ __forceinline__ void dmma_16x8x16(double *d, const double *a0, const 
           "d"(b0[0]), "d"(b0[1]), "d"(b1[0]), "d"(b1[1]));
 }
 
-template<int BM_, int BN_, int BK_, int WM_, int WN_, int STAGES_, bool K16_ = false>
+// DMMA instruction shapes of a tile configuration
+constexpr int kMma16x8x8 = 0, kMma16x8x16 = 1, kMma8x8x4 = 2;
+
+template<int BM_, int BN_, int BK_, int WM_, int WN_, int STAGES_, int MMA_ = kMma16x8x8, int MINB_ = 1>
 struct TileCfg {
     static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_, STAGES = STAGES_;
-    static constexpr bool K16 = K16_;            // one m16n8k16 DMMA per two k8 steps
+    static constexpr int MMA = MMA_, MINB = MINB_;     // DMMA shape, CTAs per SM the registers allow
+    static constexpr bool K16 = MMA == kMma16x8x16;     // one m16n8k16 DMMA per two k8 steps
     static constexpr int kWarpsM = BM / WM, kWarpsN = BN / WN;
     static constexpr int kThreads = kWarpsM * kWarpsN * 32;
-    static constexpr int kLd = BK + 8;          // padded row stride in doubles (conflict-free 16B reads)
-    static constexpr int kMT = WM / 16, kNT = WN / 8;
+    // padded row stride in doubles: conflict-free 16-byte fragment reads
+    // (rows 64 bytes apart mod 128) or 8-byte reads (rows 32 bytes apart)
+    static constexpr int kLd = MMA == kMma8x8x4 ? BK + 4 : BK + 8;
+    // accumulator fragment: rows per fragment (16 or 8) and doubles per lane
+    static constexpr int kFragRows = MMA == kMma8x8x4 ? 8 : 16, kQ = MMA == kMma8x8x4 ? 2 : 4;
+    static constexpr int kMT = WM / kFragRows, kNT = WN / 8;
     static constexpr int kStageA = BM * kLd, kStageB = BN * kLd;
     static constexpr size_t kSmem = (size_t)STAGES * (kStageA + kStageB) * sizeof(double)
                                   + (size_t)(BM + BN) * sizeof(int64_t);
     static_assert(kThreads % BK == 0 && kThreads % (BK / 2) == 0, "loader assumes a fixed k column per thread");
-    static_assert(BM % WM == 0 && BN % WN == 0 && WM % 16 == 0 && WN % 8 == 0, "warp tiling");
+    static_assert(BM % WM == 0 && BN % WN == 0 && WM % kFragRows == 0 && WN % 8 == 0, "warp tiling");
     static_assert(BK % 8 == 0, "k step");
 };
 
@@ -138,7 +151,7 @@ __device__ __forceinline__ void load_stage(double *sA, double *sB, const int64_t
 }
 
 template<class C>
-__global__ void __launch_bounds__(C::kThreads, 1)
+__global__ void __launch_bounds__(C::kThreads, C::MINB)
 contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
                      const DItem *__restrict__ items, int32_t nitems, int32_t *counter,
                      const double *__restrict__ A, const double *__restrict__ B,
@@ -166,13 +179,15 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
         const DCBlock &cb = cblks[item.cblk];
         const int M = cb.M, N = cb.N;
 
-        double acc[C::kMT][C::kNT][4];
+        // lane fragment q of tile (i, j): row i * kFragRows + g + 8 (q >> 1),
+        // column j * 8 + 2 t4 + (q & 1) of the warp tile
+        double acc[C::kMT][C::kNT][C::kQ];
 #pragma unroll
         for (int i = 0; i < C::kMT; i++)
 #pragma unroll
             for (int j = 0; j < C::kNT; j++)
 #pragma unroll
-                for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
+                for (int q = 0; q < C::kQ; q++) acc[i][j][q] = 0.0;
 
         int kt_base = 0;                       // k tiles of the tasks before ti
         for (int ti = cb.t_begin; ti < cb.t_end && kt_base < item.kt1; ti++) {
@@ -221,6 +236,32 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
                     cp_async_commit();
                 }
                 const int st = kt % C::STAGES;
+                if constexpr (C::MMA == kMma8x8x4) {
+                    // one double per fragment: A[g][k], B[n = g][k], k = ks + t4
+                    const double *tA = sA + st * C::kStageA + (wm * C::WM + g) * C::kLd + t4;
+                    const double *tB = sB + st * C::kStageB + (wn * C::WN + g) * C::kLd + t4;
+                    double af[2][C::kMT], bf[2][C::kNT];
+                    auto load8 = [&](int buf, int ks) {
+#pragma unroll
+                        for (int i = 0; i < C::kMT; i++) af[buf][i] = tA[(i * 8) * C::kLd + ks];
+#pragma unroll
+                        for (int j = 0; j < C::kNT; j++) bf[buf][j] = tB[(j * 8) * C::kLd + ks];
+                    };
+                    load8(0, 0);
+#pragma unroll
+                    for (int ks = 0; ks < C::BK; ks += 4) {
+                        const int cur = (ks / 4) & 1;
+                        if (ks + 4 < C::BK) load8(cur ^ 1, ks + 4);
+                        if (scale_b) {
+#pragma unroll
+                            for (int j = 0; j < C::kNT; j++) bf[cur][j] *= coef;
+                        }
+#pragma unroll
+                        for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+                            for (int j = 0; j < C::kNT; j++) dmma_8x8x4(acc[i][j], af[cur][i], bf[cur][j]);
+                    }
+                } else {
                 const double *tA = sA + st * C::kStageA + (wm * C::WM + g) * C::kLd + 2 * t4;
                 const double *tB = sB + st * C::kStageB + (wn * C::WN + g) * C::kLd + 2 * t4;
                 double af[2][C::kMT][4], bf[2][C::kNT][2];
@@ -272,6 +313,7 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
                             for (int j = 0; j < C::kNT; j++) dmma_16x8x8(acc[i][j], af[cur][i], bf[cur][j]);
                     }
                 }
+                }
             }
             cp_async_wait<0>();
             __syncthreads();
@@ -285,8 +327,8 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
 #pragma unroll
                 for (int j = 0; j < C::kNT; j++)
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int r = wm * C::WM + i * 16 + g + 8 * h;
+                    for (int h = 0; h < C::kQ / 2; h++) {
+                        const int r = wm * C::WM + i * C::kFragRows + g + 8 * h;
                         const int cc = wn * C::WN + j * 8 + 2 * t4;
                         *reinterpret_cast<double2 *>(P + r * C::BN + cc) =
                             make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
@@ -297,13 +339,13 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
         // Epilogue: scaled store (assign) or scaled accumulate (add) into the
         // canonical C block through its own index mapping.
         const double scale = cb.scale;
-        int64_t coff_m[C::kMT][2];
+        int64_t coff_m[C::kMT][C::kQ / 2];
         int64_t coff_n[C::kNT][2];
 #pragma unroll
         for (int i = 0; i < C::kMT; i++)
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                int m = item.m0 + wm * C::WM + i * 16 + g + 8 * h;
+            for (int h = 0; h < C::kQ / 2; h++) {
+                int m = item.m0 + wm * C::WM + i * C::kFragRows + g + 8 * h;
                 coff_m[i][h] = m < M ? mixed_offset(m, cb.nm, cb.mext, cb.mc_str) : -1;
             }
 #pragma unroll
@@ -319,7 +361,7 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
 #pragma unroll
             for (int j = 0; j < C::kNT; j++)
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
+                for (int q = 0; q < C::kQ; q++) {
                     int64_t om = coff_m[i][q >> 1], on = coff_n[j][q & 1];
                     if (om < 0 || on < 0) continue;
                     double v = scale * acc[i][j][q];
@@ -372,7 +414,7 @@ cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *it
         configured_dev = dev;
     }
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    int grid = nitems < nsm ? nitems : nsm;
+    int grid = nitems < nsm * C::MINB ? nitems : nsm * C::MINB;       // persistent: resident CTAs
     if (grid < 1) return cudaSuccess;
     e = cudaMemsetAsync(counter, 0, sizeof(int32_t), s);
     if (e != cudaSuccess) return e;
@@ -402,20 +444,31 @@ using Cfg11 = TileCfg<80, 192, 32, 80, 16, 2>;
 using Cfg12 = TileCfg<80, 192, 32, 80, 16, 2, true>;
 using Cfg13 = TileCfg<80, 128, 32, 80, 16, 3, true>;
 using Cfg14 = TileCfg<96, 128, 32, 48, 32, 3>;
+// m8n8k4 DMMA (one double per fragment): 40 x 32 warp tiles (80-row C
+// tiles), and a 64 x 128 tile of 32 x 64 warp tiles, two CTAs per SM
+using Cfg15 = TileCfg<80, 128, 32, 40, 32, 3, kMma8x8x4>;
+using Cfg16 = TileCfg<80, 192, 32, 40, 32, 2, kMma8x8x4>;
+using Cfg17 = TileCfg<64, 128, 16, 32, 64, 3, kMma8x8x4, 2>;
+// more m8n8k4 shapes with two CTAs per SM: 80-row tiles of 40 x 64 and
+// 40 x 32 warp tiles, BK 32 with two stages, and 128 x 64
+using Cfg18 = TileCfg<80, 128, 16, 40, 64, 3, kMma8x8x4, 2>;
+using Cfg19 = TileCfg<80, 128, 16, 40, 32, 3, kMma8x8x4, 2>;
+using Cfg20 = TileCfg<64, 128, 32, 32, 64, 2, kMma8x8x4, 2>;
+using Cfg21 = TileCfg<128, 64, 16, 64, 32, 3, kMma8x8x4, 2>;
 
 }  // namespace
 
-int tile_cfg_count() { return 15; }
+int tile_cfg_count() { return 22; }
 int tile_cfg_bm(int cfg) {
-    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM, Cfg8::BM, Cfg9::BM, Cfg10::BM, Cfg11::BM, Cfg12::BM, Cfg13::BM, Cfg14::BM};
+    const int v[] = {Cfg0::BM, Cfg1::BM, Cfg2::BM, Cfg3::BM, Cfg4::BM, Cfg5::BM, Cfg6::BM, Cfg7::BM, Cfg8::BM, Cfg9::BM, Cfg10::BM, Cfg11::BM, Cfg12::BM, Cfg13::BM, Cfg14::BM, Cfg15::BM, Cfg16::BM, Cfg17::BM, Cfg18::BM, Cfg19::BM, Cfg20::BM, Cfg21::BM};
     return v[cfg];
 }
 int tile_cfg_bk(int cfg) {
-    const int v[] = {Cfg0::BK, Cfg1::BK, Cfg2::BK, Cfg3::BK, Cfg4::BK, Cfg5::BK, Cfg6::BK, Cfg7::BK, Cfg8::BK, Cfg9::BK, Cfg10::BK, Cfg11::BK, Cfg12::BK, Cfg13::BK, Cfg14::BK};
+    const int v[] = {Cfg0::BK, Cfg1::BK, Cfg2::BK, Cfg3::BK, Cfg4::BK, Cfg5::BK, Cfg6::BK, Cfg7::BK, Cfg8::BK, Cfg9::BK, Cfg10::BK, Cfg11::BK, Cfg12::BK, Cfg13::BK, Cfg14::BK, Cfg15::BK, Cfg16::BK, Cfg17::BK, Cfg18::BK, Cfg19::BK, Cfg20::BK, Cfg21::BK};
     return v[cfg];
 }
 int tile_cfg_bn(int cfg) {
-    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN, Cfg8::BN, Cfg9::BN, Cfg10::BN, Cfg11::BN, Cfg12::BN, Cfg13::BN, Cfg14::BN};
+    const int v[] = {Cfg0::BN, Cfg1::BN, Cfg2::BN, Cfg3::BN, Cfg4::BN, Cfg5::BN, Cfg6::BN, Cfg7::BN, Cfg8::BN, Cfg9::BN, Cfg10::BN, Cfg11::BN, Cfg12::BN, Cfg13::BN, Cfg14::BN, Cfg15::BN, Cfg16::BN, Cfg17::BN, Cfg18::BN, Cfg19::BN, Cfg20::BN, Cfg21::BN};
     return v[cfg];
 }
 
@@ -450,7 +503,14 @@ cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     case 11: return launch_cfg<Cfg11>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
     case 12: return launch_cfg<Cfg12>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
     case 13: return launch_cfg<Cfg13>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    default: return launch_cfg<Cfg14>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 14: return launch_cfg<Cfg14>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 15: return launch_cfg<Cfg15>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 16: return launch_cfg<Cfg16>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 17: return launch_cfg<Cfg17>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 18: return launch_cfg<Cfg18>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 19: return launch_cfg<Cfg19>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 20: return launch_cfg<Cfg20>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    default: return launch_cfg<Cfg21>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
     }
 }
 

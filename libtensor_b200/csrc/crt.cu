@@ -31,7 +31,11 @@
 // bounded in time and reports through *err.
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "ltg_device.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace ltg {
 namespace {
@@ -342,6 +346,130 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
             if (rl >= un.z || r >= P.wrows || k0 >= P.wk) continue;
             if (r != cur) set_row(r);
             put4(r, k0);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- fused split of row families
+//
+// The two passes above read every operand element twice from HBM (once for
+// the row maxima, once for the residues).  For a row family (DCrtFamily) the
+// exponent of a row needs only that family's rows, so a unit of 8 rows is
+// split completely by one cluster of kFuseCs CTAs: each CTA takes an equal
+// share of the family's 16-wide k tiles, pass 1 forms its row maxima, the
+// cluster combines them through distributed shared memory, and pass 2 reads
+// the same share again -- from L2 (8 rows x its share, a few hundred KB per
+// CTA, read moments before) -- and writes the residue images.  Thread
+// mapping of both passes: a warp takes one core tile (the unit's 8 rows x 16
+// k; lane l row l / 4 and the 4 consecutive k of group l % 4), so that every
+// residue store of a warp is one whole 128-byte core matrix.  Family panels
+// have one contiguous k run (k offset = k).
+
+constexpr int kFuseCs = 8;                          // CTAs per unit (cluster size)
+constexpr int kFuseThreads = 256;
+constexpr int kFuseWarps = kFuseThreads / 32;
+constexpr int kFuseCtasPerSm = 4;
+
+template<int L>
+__global__ void __cluster_dims__(kFuseCs, 1, 1) __launch_bounds__(kFuseThreads, kFuseCtasPerSm)
+crt_fused_kernel(const DCrtPanel *__restrict__ panels, const DCrtFamily *__restrict__ fams,
+                 const int32_t *__restrict__ famp, const int32_t *__restrict__ famt,
+                 const int4 *__restrict__ units, int32_t nunits, const double *__restrict__ A,
+                 const double *__restrict__ B, const int32_t *__restrict__ gidx, int32_t *ex, int32_t *ey,
+                 uint8_t *__restrict__ res, const CrtParams cp) {
+    __shared__ int32_t rexp[8];          // this CTA's row maxima (exponents)
+    __shared__ int32_t rfin[8];          // the cluster's
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lrow = lane >> 2, kq = lane & 3;
+    const int nclusters = gridDim.x / kFuseCs, cid = blockIdx.x / kFuseCs;
+    for (int u = cid; u < nunits; u += nclusters) {
+        const int4 un = units[u];
+        const DCrtFamily F = fams[un.x];
+        if (threadIdx.x < 8) rexp[threadIdx.x] = kNoExp;
+        __syncthreads();
+        // this CTA's share of the family's k tiles
+        const int t0 = (int)((int64_t)crank * F.ntiles / kFuseCs);
+        const int t1 = (int)((int64_t)(crank + 1) * F.ntiles / kFuseCs);
+        const int r = un.y + lrow;
+        const bool rvalid = lrow < un.z;
+        // pass 1: row maxima, panel by panel (a lane keeps one row: a running
+        // maximum over its tiles, reduced once)
+        double mx = 0.0;
+        for (int q = F.p_begin; q < F.p_end; q++) {
+            const int qa = famt[q], qb = q + 1 < F.p_end ? famt[q + 1] : F.ntiles;
+            const int lo = max(qa, t0), hi = min(qb, t1);
+            if (lo >= hi || !rvalid) continue;
+            const DCrtPanel &P = panels[famp[q]];
+            const double *row = (P.src ? B : A) + P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
+#pragma unroll 4
+            for (int t = lo + warp; t < hi; t += kFuseWarps) {
+                const int k0 = (t - qa) * 16 + kq * 4;
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (k0 + j < P.K) mx = fmax(mx, fabs(row[k0 + j]));
+            }
+        }
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+        if (rvalid && kq == 0 && mx > 0.0) {
+            int e;
+            frexp(mx, &e);                                     // mx = f * 2^e, f in [0.5, 1)
+            atomicMax(&rexp[lrow], e);
+        }
+        cluster.sync();                                        // every CTA's maxima are complete
+        if (threadIdx.x < 8) {
+            int m = kNoExp;
+            for (int c = 0; c < kFuseCs; c++) m = max(m, cluster.map_shared_rank(rexp, c)[threadIdx.x]);
+            rfin[threadIdx.x] = m;
+        }
+        cluster.sync();                                        // the peers have read rexp; rfin is visible
+        if (crank == 0 && threadIdx.x < un.z) {
+            const DCrtPanel &P0 = panels[famp[F.p_begin]];
+            int32_t *tab = P0.side == 0 ? ex : ey;
+            tab[gidx[P0.g_off + un.y + threadIdx.x]] = rfin[threadIdx.x];
+        }
+        // pass 2: residues (the reads hit L2)
+        const int e = rvalid ? rfin[lrow] : kNoExp;
+        const int sh = e > kNoExp ? cp.P - e : 0;
+        const double s1 = ldexp(1.0, sh / 2), s2 = ldexp(1.0, sh - sh / 2);   // 2^(P - e), two finite factors
+        const bool live = rvalid && e > kNoExp;
+        for (int q = F.p_begin; q < F.p_end; q++) {
+            const int qa = famt[q], qb = q + 1 < F.p_end ? famt[q + 1] : F.ntiles;
+            const int lo = max(qa, t0), hi = min(qb, t1);
+            if (lo >= hi || !rvalid) continue;
+            const DCrtPanel &P = panels[famp[q]];
+            const double *row = (P.src ? B : A) + P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
+            const double coef = (double)P.coef;
+            const uint32_t icoef = (uint32_t)P.coef;
+            const int nkb = P.K_pad / kKB;
+            const int64_t lstride = (int64_t)P.tr * kKB;
+            uint8_t *pbase = res + P.res_off;
+            for (int t = lo + warp; t < hi; t += kFuseWarps) {
+                const int k0 = (t - qa) * 16 + kq * 4;
+                if (k0 >= P.wk) continue;
+                double x[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) x[j] = (live && k0 + j < P.K) ? row[k0 + j] : 0.0;
+                uint32_t packed[L];
+#pragma unroll
+                for (int l = 0; l < L; l++) packed[l] = 0;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const double tt = (x[j] * s1) * s2 + kMagicD;         // 1.5 * 2^52 + rint(x 2^(P-e))
+                    const double X = (tt - kMagicD) * coef;               // the integer coefficient folded in
+                    const uint32_t xlo = (uint32_t)__double2loint(tt) * icoef;   // X mod 2^32
+                    const uint32_t sel = 0x3210u ^ ((0x4u ^ (uint32_t)j) << (4 * j));
+                    StaticFor<0, L>::run([&](auto ic) {
+                        constexpr int l = decltype(ic)::value;
+                        packed[l] = __byte_perm(packed[l], residue_byte<l>(X, xlo), sel);
+                    });
+                }
+                const int kk = P.k0 + k0;
+                uint8_t *dst0 = pbase + image_offset(P.r0 + r, P.tr, nkb, kk / kKB, 0, L, kk % kKB);
+#pragma unroll
+                for (int l = 0; l < L; l++) *reinterpret_cast<uint32_t *>(dst0 + l * lstride) = packed[l];
+            }
         }
     }
 }
@@ -767,11 +895,34 @@ int num_sms() {
 cudaError_t launch_crt_exponents(const DCrtPanel *panels, const int4 *units, int32_t nunits, int32_t nx,
                                  int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
                                  int32_t *ey, cudaStream_t s) {
-    crt_fill_kernel<<<64, 256, 0, s>>>(ex, nx, kNoExp);
-    crt_fill_kernel<<<64, 256, 0, s>>>(ey, ny, kNoExp);
-    if (nunits <= 0) return cudaGetLastError();
+    if (nunits <= 0) return cudaSuccess;
     const int grid = nunits;                               // one unit per CTA
     crt_exp_kernel<<<grid, kSplitThreads, 0, s>>>(panels, units, nunits, a, b, gidx, ex, ey);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_fill(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, cudaStream_t s) {
+    crt_fill_kernel<<<64, 256, 0, s>>>(ex, nx, kNoExp);
+    crt_fill_kernel<<<64, 256, 0, s>>>(ey, ny, kNoExp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_fused(const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
+                             const int32_t *famt, const int4 *units, int32_t nunits, const double *a,
+                             const double *b, const int32_t *gidx, int32_t *ex, int32_t *ey, uint8_t *res,
+                             const CrtParams &cp, cudaStream_t s) {
+    if (nunits <= 0) return cudaSuccess;
+    // kFuseCtasPerSm CTAs per SM: what the resident clusters read in pass 1
+    // (8 rows of a family each) must still be in L2 for pass 2
+    const int maxc = kFuseCtasPerSm * num_sms() / kFuseCs;
+    const int nclusters = nunits < maxc ? nunits : maxc;
+    const int grid = kFuseCs * (nclusters > 0 ? nclusters : 1);
+    switch (cp.L) {
+#define CASE_L(n) case n: crt_fused_kernel<n><<<grid, kFuseThreads, 0, s>>>(panels, fams, famp, famt, units, nunits, a, b, gidx, ex, ey, res, cp); break;
+    CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
+#undef CASE_L
+    default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

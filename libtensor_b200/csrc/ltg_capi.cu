@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -185,8 +186,13 @@ struct CrtExec {
     CrtParams cp{};
     int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0, ngroups = 0, nunits = 0;
     int64_t src_elems = 0, res_bytes = 0;   // operand elements read per pass, residue bytes written
+    int64_t fused_elems = 0;                // of those, elements of row families (read once from HBM)
     double scale = 1.0;                     // kc (and d in add mode) times the pair coefficients' scale
     DevBuf panels, units, tasks, items, cblks, comps, ctab, cells, gidx, ex, ey, res, out;
+    // row families split in one read (launch_crt_fused): families, their
+    // panels and tile offsets, and the 8-row units
+    DevBuf fams, famp, famt, funits;
+    int32_t nfunits = 0;
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
 
@@ -202,13 +208,16 @@ struct ltg_plan {
     int forced_tile = -1;         // >= 0: every C block uses this tile shape
     int split_k = 0;              // plain DMMA k chunks per tile: 0 automatic, 1 never, 2-4 always
     bool group_products = true;   // modular mode: small C blocks grouped into larger products
+    bool fused_split = true;      // modular mode: row families split in one read of the operand
     // caller-built task list (ltg_plan_contract2_upload): plain FP64 only,
     // coefficients absolute, no schedule of its own
     bool external = false;
     std::vector<GemmTask> ext_tasks;
     int crt_rows = 0;             // modular mode: work-item rows (128, 256; 0 default)
     std::map<std::pair<int64_t, int64_t>, int> tile_override;   // autotuned (M, N) -> shape
-    ContractPlan plan;
+    // the schedule (shared with the process-wide schedule cache)
+    std::shared_ptr<const ContractPlan> planp = std::make_shared<const ContractPlan>();
+    const ContractPlan &plan() const { return *planp; }
     // cache of device task arrays keyed by (C tensor, ka, kb, kc, add, d)
     std::map<std::tuple<uint64_t, double, double, double, int, double>,
              std::unique_ptr<ContractExec>> exec;
@@ -434,15 +443,20 @@ int32_t vec16_ok(int64_t off, const SubDims &rows, const SubDims &k, bool second
 // the shape (larger tiles reuse more data per load).  An autotuned table
 // (ltg_autotune) overrides the weights with measured rates.
 struct TileShape { int bm, bn; double eff; };
-constexpr int kNumShapes = 15;
+constexpr int kNumShapes = 22;
 const TileShape kShapes[kNumShapes] = {
     {128, 128, 1.00}, {64, 64, 0.78}, {64, 128, 0.90}, {32, 32, 0.45},
     {80, 128, 0.97}, {96, 128, 0.98}, {48, 128, 0.85}, {112, 128, 0.99},
     {16, 128, 0.50}, {32, 128, 0.70}, {80, 192, 0.96}, {80, 192, 0.95},
     {80, 192, 0.94}, {80, 128, 0.93}, {96, 128, 0.92},
+    {80, 128, 0.91}, {80, 192, 0.91}, {64, 128, 1.10},
+    {80, 128, 1.00}, {80, 128, 0.95}, {64, 128, 1.05}, {128, 64, 1.05},
 };
+// relative rates (the m8n8k4 shapes with two CTAs per SM measured fastest:
+// 64 x 128 at 30.1 TFLOP/s on a dense 6144^3 product against 26.1 for the
+// best m16n8k8 shape)
 double g_tile_eff[kNumShapes] = {1.00, 0.78, 0.90, 0.45, 0.97, 0.98, 0.85, 0.99, 0.50, 0.70, 0.96, 0.95,
-                                 0.94, 0.93, 0.92};
+                                 0.94, 0.93, 0.92, 0.91, 0.91, 1.10, 1.00, 0.95, 1.05, 1.05};
 
 int pick_tile(int64_t M, int64_t N) {
     int best = 0;
@@ -582,7 +596,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     std::vector<GemmTask> tasks;
     std::vector<CBlockTask> cbt;
     if (pl->external) external_blocks(pl, ka, kb, kc, tasks, cbt);
-    else contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    else contract2_tasks(pl->plan(), pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
     // Every address a task can form must lie inside its arena.
     auto span = [](const SubDims &s, bool second) {
         int64_t m = 0;
@@ -630,7 +644,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     }
     // small blocks computed as grouped products
     std::vector<int32_t> group_of(cbt.size(), -1);
-    if (pl->group_products && !pl->plan.coalesced && !pl->external) {
+    if (pl->group_products && !pl->plan().coalesced && !pl->external) {
         ex->groups.reset(new PlainGroups());
         build_plain_groups(pl, c, cbt, ka * kb * kc, post, group_of, *ex->groups);
         if (ex->groups->ngroups == 0) ex->groups.reset();
@@ -680,7 +694,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
             in_sched[f->second] = 1;
         }
     }
-    for (int64_t cabs : pl->external ? std::vector<int64_t>() : pl->plan.schedule) {
+    for (int64_t cabs : pl->external ? std::vector<int64_t>() : pl->plan().schedule) {
         int64_t sl = c->h.slot_of[cabs];
         in_sched[sl] = 1;
         ex->sched_slots.push_back(sl);
@@ -721,7 +735,7 @@ OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, doubl
 
     std::vector<GemmTask> tasks;
     std::vector<CBlockTask> cbt;
-    contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    contract2_tasks(pl->plan(), pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
     // panels, de-duplicated by (operand, block, row mapping, k mapping)
     std::map<std::vector<int64_t>, int32_t> pidx;
     std::vector<DPanel> panels;
@@ -804,7 +818,7 @@ OzExec *prepare_ozaki(ltg_plan *pl, ltg_bt *c, int mode, int S, double ka, doubl
     upload_vec(ex->items, items, s);
     // blocks of C outside the schedule (zeroed in assign mode)
     std::vector<char> in_sched(c->h.blk_abs.size(), 0);
-    for (int64_t cabs : pl->plan.schedule) {
+    for (int64_t cabs : pl->plan().schedule) {
         int64_t sl = c->h.slot_of[cabs];
         in_sched[sl] = 1;
         ex->sched_slots.push_back(sl);
@@ -960,7 +974,7 @@ void crt_side_maps(const Contraction &ct, const BlockTensorHost &ch, CrtSideMap 
 void crt_groups(const ltg_plan *pl, const BlockTensorHost &ch, const CrtSideMap *sm,
                 const std::vector<CBlockTask> &cbt, std::vector<CrtGroupHost> &groups,
                 std::vector<int32_t> &group_of) {
-    const ContractPlan &P = pl->plan;
+    const ContractPlan &P = pl->plan();
     const Contraction &c0 = P.contr;
     const BlockTensorHost &ah = pl->a->h, &bh = pl->b->h;
     const int NC = c0.NC(), NA = c0.NA(), NB = c0.NB();
@@ -1128,7 +1142,7 @@ DCrtComp crt_group_tables(const ltg_plan *pl, const BlockTensorHost &ch, const C
     auto side_entries = [&](int cside, const std::vector<int64_t> &ext, const std::vector<int32_t> &ce) {
         const std::vector<int> &dims = sm[cside].dims;
         for (size_t b = 0; b < ext.size(); b++) {
-            ch.bis.unabs(pl->plan.schedule[ce[b]], ic);
+            ch.bis.unabs(pl->plan().schedule[ce[b]], ic);
             ch.bis.block_dims(ic, dcb);
             for (int64_t i = 0; i < ext[b]; i++) {
                 int32_t co[kCrtSideDims] = {0, 0, 0, 0};
@@ -1149,7 +1163,7 @@ DCrtComp crt_group_tables(const ltg_plan *pl, const BlockTensorHost &ch, const C
         DCrtCell cl;
         std::memset(&cl, 0, sizeof(cl));
         cl.c_off = cbt[e].c_off;
-        ch.bis.unabs(pl->plan.schedule[e], ic);
+        ch.bis.unabs(pl->plan().schedule[e], ic);
         ch.bis.block_dims(ic, dcb);
         int64_t x = 1;
         for (int d = ch.bis.n - 1; d >= 0; d--) { scb[d] = x; x *= dcb[d]; }
@@ -1188,9 +1202,9 @@ std::vector<std::pair<int64_t, int64_t>> plain_group_shapes(ltg_plan *pl, ltg_bt
                                                            std::vector<int32_t> &group_of) {
     std::vector<std::pair<int64_t, int64_t>> shapes;
     group_of.assign(cbt.size(), -1);
-    if (!pl->group_products || pl->plan.coalesced) return shapes;
+    if (!pl->group_products || pl->plan().coalesced) return shapes;
     CrtSideMap sm[2];
-    crt_side_maps(pl->plan.contr, c->h, sm);
+    crt_side_maps(pl->plan().contr, c->h, sm);
     std::vector<CrtGroupHost> groups;
     crt_groups(pl, c->h, sm, cbt, groups, group_of);
     int64_t off = 0;
@@ -1231,7 +1245,7 @@ void external_blocks(const ltg_plan *pl, double ka, double kb, double kc, std::v
 void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &cbt, double kabc, double post,
                         std::vector<int32_t> &group_of, PlainGroups &pg) {
     CrtSideMap sm[2];
-    crt_side_maps(pl->plan.contr, c->h, sm);
+    crt_side_maps(pl->plan().contr, c->h, sm);
     std::vector<CrtGroupHost> groups;
     crt_groups(pl, c->h, sm, cbt, groups, group_of);
     if (groups.empty()) return;
@@ -1363,10 +1377,10 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
 
     std::vector<GemmTask> tasks;
     std::vector<CBlockTask> cbt;
-    contract2_tasks(pl->plan, pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    contract2_tasks(pl->plan(), pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
     const BlockTensorHost &ch = c->h;
     CrtSideMap sm[2];
-    crt_side_maps(pl->plan.contr, ch, sm);
+    crt_side_maps(pl->plan().contr, ch, sm);
     std::map<int64_t, int64_t> slot_of_off;
     for (size_t sl = 0; sl < ch.blk_off.size(); sl++) slot_of_off[ch.blk_off[sl]] = (int64_t)sl;
 
@@ -1387,7 +1401,7 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     // grouped products of small blocks (their pairs carry coefficients +-1)
     std::vector<CrtGroupHost> groups;
     std::vector<int32_t> group_of(cbt.size(), -1);
-    if (pl->group_products && !pl->plan.coalesced) crt_groups(pl, ch, sm, cbt, groups, group_of);
+    if (pl->group_products && !pl->plan().coalesced) crt_groups(pl, ch, sm, cbt, groups, group_of);
 
     // panels by (operand, block, row and k mappings, coefficient); one key can
     // hold several panels when the same rows feed different rows of C
@@ -1606,6 +1620,7 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
                 out_bytes += (int64_t)L * it.nx * 128 * q.nt;
                 iv.push_back({q.kw * q.nt * it.nx, it});
             }
+    const int32_t nplain = (int32_t)panels.size();                      // panels of their own
     const int32_t nsplit = (int32_t)(panels.size() + pieces.size());   // panels the split passes process
     panels.insert(panels.end(), pieces.begin(), pieces.end());
     panels.insert(panels.end(), records.begin(), records.end());
@@ -1633,10 +1648,61 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
         ex->src_elems += (int64_t)q.rows * q.K;
         ex->res_bytes += (int64_t)L * q.wrows * q.wk;
     }
-    // split-pass units: 32 rows of a panel with long k (8 threads per row), or
-    // about 64 core tiles (8 rows x 16 k, at most 256 rows) of one with short k
+    // Row families (DCrtFamily): panels of their own (not pieces of grouped
+    // images) with one contiguous k run whose global row arrays are equal,
+    // such that no other panel feeds those rows.  They are split in one read
+    // of the operand (launch_crt_fused); the other panels by the two passes.
+    std::vector<char> fused(nsplit, 0);
+    std::vector<DCrtFamily> fams;
+    std::vector<int32_t> famp, famt;
+    std::vector<int4> funits;
+    {
+        std::vector<int32_t> cnt[2];
+        cnt[0].assign(std::max<int32_t>(ex->nx, 1), 0);
+        cnt[1].assign(std::max<int32_t>(ex->ny, 1), 0);
+        for (int32_t i = 0; i < nsplit; i++) {
+            const DCrtPanel &q = panels[i];
+            for (int32_t r = 0; r < q.rows; r++) cnt[q.side][gidx[q.g_off + r]]++;
+        }
+        std::map<std::pair<int32_t, std::vector<int32_t>>, std::vector<int32_t>> byrows;
+        for (int32_t i = 0; i < (pl->fused_split ? nplain : 0); i++) {
+            const DCrtPanel &q = panels[i];
+            if (q.nk != 1 || q.kstr[0] != 1 || q.r0 != 0 || q.k0 != 0 || q.rows <= 0) continue;
+            std::vector<int32_t> g(gidx.begin() + q.g_off, gidx.begin() + q.g_off + q.rows);
+            byrows[{q.side, g}].push_back(i);
+        }
+        for (auto &f : byrows) {
+            const std::vector<int32_t> &g = f.first.second;
+            const int32_t n = (int32_t)f.second.size();
+            bool clean = true;
+            for (int32_t x : g) if (cnt[f.first.first][x] != n) { clean = false; break; }
+            if (!clean) continue;
+            DCrtFamily F;
+            F.p_begin = (int32_t)famp.size();
+            F.rows = (int32_t)g.size();
+            int32_t tiles = 0;
+            for (int32_t i : f.second) {
+                famp.push_back(i);
+                famt.push_back(tiles);
+                tiles += (panels[i].wk + 15) / 16;
+                fused[i] = 1;
+                ex->fused_elems += (int64_t)panels[i].rows * panels[i].K;
+            }
+            F.p_end = (int32_t)famp.size();
+            F.ntiles = tiles;
+            const int32_t fid = (int32_t)fams.size();
+            fams.push_back(F);
+            for (int32_t r0 = 0; r0 < F.rows; r0 += 8)
+                funits.push_back(make_int4(fid, r0, std::min<int32_t>(8, F.rows - r0), 0));
+        }
+        famt.push_back(0);      // famt[p_end] of the last family is read as a bound only when q + 1 < p_end
+    }
+    // the other panels' split-pass units: 32 rows of a panel with long k (8
+    // threads per row), or about 64 core tiles (8 rows x 16 k, at most 256
+    // rows) of one with short k
     std::vector<int4> units;
     for (int32_t i = 0; i < nsplit; i++) {
+        if (fused[i]) continue;
         const bool rowmap = panels[i].wk >= 128;
         const int32_t nkt = (panels[i].wk + 15) / 16;
         const int32_t ru = rowmap ? 32 : 8 * std::max(1, std::min(32, 64 / std::max(1, nkt)));
@@ -1645,6 +1711,13 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     }
     ex->nunits = (int32_t)units.size();
     upload_vec(ex->units, units, s);
+    ex->nfunits = (int32_t)funits.size();
+    if (!funits.empty()) {
+        upload_vec(ex->fams, fams, s);
+        upload_vec(ex->famp, famp, s);
+        upload_vec(ex->famt, famt, s);
+        upload_vec(ex->funits, funits, s);
+    }
     ex->res.alloc(std::max<int64_t>(res_bytes, 1024));
     // cells of grouped images that no piece writes stay zero
     LTG_CUDA(cudaMemsetAsync(ex->res.p, 0, std::max<int64_t>(res_bytes, 1024), s));
@@ -1664,7 +1737,7 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     upload_vec(ex->cells, cells, s);
     ex->scale = post;
     std::vector<char> in_sched(c->h.blk_abs.size(), 0);
-    for (int64_t cabs : pl->plan.schedule) {
+    for (int64_t cabs : pl->plan().schedule) {
         int64_t sl = c->h.slot_of[cabs];
         in_sched[sl] = 1;
         ex->sched_slots.push_back(sl);
@@ -2137,6 +2210,204 @@ int ltg_bt_create_permuted(ltg_bt *a, const int32_t *perm, ltg_bt **out) {
     });
 }
 
+namespace {
+bool same_part(const SePart &x, const SePart &y, int n) {
+    for (int d = 0; d < n; d++)
+        if (x.pdims[d] != y.pdims[d] || x.bipdims[d] != y.bipdims[d]) return false;
+    return x.forbidden == y.forbidden;
+}
+bool same_label(const SeLabel &x, const SeLabel &y, int n) {
+    if (x.nirrep != y.nirrep || x.rule.size() != y.rule.size()) return false;
+    for (int d = 0; d < n; d++) if (x.labels[d] != y.labels[d]) return false;
+    for (size_t i = 0; i < x.rule.size(); i++) {
+        if (x.rule[i].size() != y.rule[i].size()) return false;
+        for (size_t k = 0; k < x.rule[i].size(); k++) {
+            if (x.rule[i][k].intr != y.rule[i][k].intr) return false;
+            for (int d = 0; d < n; d++) if (x.rule[i][k].seq[d] != y.rule[i][k].seq[d]) return false;
+        }
+    }
+    return true;
+}
+}  // namespace
+
+int ltg_bt_create_sum_space(int32_t nterms, ltg_bt *const *a, const int32_t *perms, ltg_bt **out) {
+    return guard([&] {
+        if (nterms < 1 || !a || !out) throw error(kErrBadArg, "a sum needs at least one term");
+        for (int32_t t = 0; t < nterms; t++) check_bt(a[t]);
+        const int n = a[0]->h.bis.n;
+        std::vector<Bis> bis(nterms);
+        std::vector<Symmetry> sym(nterms);
+        for (int32_t t = 0; t < nterms; t++) {
+            if (a[t]->h.bis.n != n) throw error(kErrBadDims, "terms of different order");
+            permute_space(a[t]->h.bis, a[t]->h.sym, perm_from(n, perms ? perms + (size_t)t * n : nullptr),
+                          bis[t], sym[t]);
+            if (!bis[t].equals(bis[0])) throw error(kErrBadDims, "terms of a sum with different block index spaces");
+        }
+        std::unique_ptr<ltg_bt> bt(new ltg_bt());
+        bt->ctx = a[0]->ctx;
+        bt->h.bis = bis[0];
+        // permutational elements in every term's group (with the same sign)
+        std::vector<SePerm> common = perm_group_closure(n, sym[0].perm);
+        for (int32_t t = 1; t < nterms; t++) {
+            const std::vector<SePerm> g = perm_group_closure(n, sym[t].perm);
+            std::vector<SePerm> keep;
+            for (const SePerm &e : common)
+                for (const SePerm &f : g)
+                    if (e.perm == f.perm && e.coeff == f.coeff) { keep.push_back(e); break; }
+            common.swap(keep);
+        }
+        for (const SePerm &e : common)
+            if (!e.perm.is_identity()) bt->h.sym.perm.push_back(e);
+        // partition and label rules shared by all terms
+        bool parts = true, labels = true;
+        for (int32_t t = 1; t < nterms; t++) {
+            parts = parts && sym[t].part.size() == sym[0].part.size();
+            for (size_t i = 0; parts && i < sym[0].part.size(); i++) parts = same_part(sym[0].part[i], sym[t].part[i], n);
+            labels = labels && sym[t].label.size() == sym[0].label.size();
+            for (size_t i = 0; labels && i < sym[0].label.size(); i++)
+                labels = same_label(sym[0].label[i], sym[t].label[i], n);
+        }
+        if (parts) bt->h.sym.part = sym[0].part;
+        if (labels) bt->h.sym.label = sym[0].label;
+        alloc_arena(bt.get());
+        *out = bt.release();
+    });
+}
+
+namespace {
+// The symmetrizer's group: nidx 2, indexes idx[0] and idx[1]: {e, (i1 i2)};
+// nidx -1, a unitary permutation idx[0..n): {e, P}; nidx 4: the 24
+// permutations of indexes idx[0..3].  Signs: +1 (symm), else the parity.
+std::vector<SePerm> symmetrizer_group(int n, int32_t nidx, const int32_t *idx, bool symm) {
+    if (!idx) throw error(kErrBadArg, "null symmetrizer indexes");
+    std::vector<SePerm> g;
+    SePerm e;
+    e.perm = Perm::identity(n);
+    e.coeff = 1.0;
+    if (nidx == 2 || nidx == -1) {
+        SePerm q = e;
+        if (nidx == 2) {
+            if (idx[0] < 0 || idx[0] >= n || idx[1] < 0 || idx[1] >= n || idx[0] == idx[1])
+                throw error(kErrBadArg, "symmetrizer indexes out of range");
+            std::swap(q.perm.p[idx[0]], q.perm.p[idx[1]]);
+        } else {
+            q.perm = perm_from(n, idx);
+            Perm sq = q.perm;
+            sq.permute(q.perm);
+            if (!sq.is_identity() || q.perm.is_identity())
+                throw error(kErrBadArg, "the symmetrizer permutation must be its own inverse");
+        }
+        q.coeff = symm ? 1.0 : -1.0;
+        g.push_back(e);
+        g.push_back(q);
+        return g;
+    }
+    if (nidx != 4) throw error(kErrBadArg, "a symmetrizer takes 2 or 4 indexes or a permutation");
+    for (int k = 0; k < 4; k++) {
+        if (idx[k] < 0 || idx[k] >= n) throw error(kErrBadArg, "symmetrizer indexes out of range");
+        for (int l = 0; l < k; l++) if (idx[k] == idx[l]) throw error(kErrBadArg, "repeated symmetrizer index");
+    }
+    int pi[4] = {0, 1, 2, 3};
+    do {
+        SePerm q = e;
+        for (int k = 0; k < 4; k++) q.perm.p[idx[k]] = (int8_t)idx[pi[k]];
+        int inv = 0;
+        for (int a = 0; a < 4; a++) for (int b = a + 1; b < 4; b++) if (pi[a] > pi[b]) inv++;
+        q.coeff = symm || inv % 2 == 0 ? 1.0 : -1.0;
+        g.push_back(q);
+    } while (std::next_permutation(pi, pi + 4));
+    return g;
+}
+
+// Every block's allowedness is unchanged by the permutation.
+bool allowed_invariant(const Bis &bis, const Symmetry &sym, const Perm &p) {
+    int64_t bidx[kMaxOrder], pb[kMaxOrder];
+    const int64_t nb = bis.nblocks();
+    for (int64_t a = 0; a < nb; a++) {
+        bis.unabs(a, bidx);
+        for (int d = 0; d < bis.n; d++) pb[d] = bidx[p.p[d]];
+        if (sym.is_allowed(bis.n, bidx) != sym.is_allowed(bis.n, pb)) return false;
+    }
+    return true;
+}
+}  // namespace
+
+int ltg_bt_create_symmetrized(ltg_bt *a, int32_t nidx, const int32_t *idx, int32_t symm, ltg_bt **out) {
+    return guard([&] {
+        check_bt(a);
+        if (!out) throw error(kErrBadArg, "null output");
+        const int n = a->h.bis.n;
+        const std::vector<SePerm> S = symmetrizer_group(n, nidx, idx, symm != 0);
+        for (const SePerm &g : S)
+            if (!a->h.bis.permuted(g.perm).equals(a->h.bis))
+                throw error(kErrBadDims, "symmetrized indexes with different block structure");
+        std::unique_ptr<ltg_bt> bt(new ltg_bt());
+        bt->ctx = a->ctx;
+        bt->h.bis = a->h.bis;
+        // generators of the symmetrizer's group
+        if (nidx == 4) {
+            for (int k = 1; k < 4; k++) {
+                SePerm q;
+                q.perm = Perm::identity(n);
+                std::swap(q.perm.p[idx[0]], q.perm.p[idx[k]]);
+                q.coeff = symm ? 1.0 : -1.0;
+                bt->h.sym.perm.push_back(q);
+            }
+        } else {
+            bt->h.sym.perm.push_back(S[1]);
+        }
+        // the operand's elements that map the symmetrizer's group onto itself
+        // (h S h^-1 = S) remain symmetries of the sum over S
+        for (const SePerm &h : perm_group_closure(n, a->h.sym.perm)) {
+            if (h.perm.is_identity()) continue;
+            const Perm hi = h.perm.inverse();
+            bool normal = true;
+            for (const SePerm &g : S) {
+                Perm c = hi;
+                c.permute(g.perm).permute(h.perm);
+                bool found = false;
+                for (const SePerm &f : S) if (f.perm == c) { found = true; break; }
+                if (!found) { normal = false; break; }
+            }
+            if (normal) bt->h.sym.perm.push_back(h);
+        }
+        // partition and label rules the symmetrizer leaves unchanged
+        bool keep = true;
+        for (const SePerm &g : S) keep = keep && allowed_invariant(a->h.bis, a->h.sym, g.perm);
+        if (keep) {
+            bt->h.sym.part = a->h.sym.part;
+            bt->h.sym.label = a->h.sym.label;
+        }
+        alloc_arena(bt.get());
+        *out = bt.release();
+    });
+}
+
+int ltg_symmetrize(ltg_bt *a, double c, int32_t nidx, const int32_t *idx, int32_t symm, ltg_bt *b, int32_t add,
+                   double d) {
+    return guard([&] {
+        check_bt(a);
+        check_bt(b);
+        need_dev(a->ctx);
+        if (!b->h.bis.equals(a->h.bis)) throw error(kErrBadDims, "symmetrizer result of another index space");
+        const std::vector<SePerm> S = symmetrizer_group(a->h.bis.n, nidx, idx, symm != 0);
+        // passes of at most kMaxTerms_host permuted terms: the first assigns
+        // (or adds d times), the others add
+        for (size_t t0 = 0; t0 < S.size(); t0 += kMaxTerms_host) {
+            std::vector<ltg_bt *> srcs;
+            std::vector<Perm> ps;
+            std::vector<double> cs;
+            for (size_t t = t0; t < std::min(S.size(), t0 + kMaxTerms_host); t++) {
+                srcs.push_back(a);
+                ps.push_back(S[t].perm);
+                cs.push_back(c * S[t].coeff);
+            }
+            const bool first = t0 == 0;
+            run_transfer(a->ctx, srcs, ps, cs, b, first ? add != 0 : true, first ? d : (add ? d : 1.0));
+        }
+    });
+}
+
 int ltg_bt_destroy(ltg_bt *bt) {
     return guard([&] {
         check_bt(bt);
@@ -2358,6 +2629,92 @@ int ltg_bt_device_ptr(ltg_bt *bt, double **ptr) {
     return guard([&] { check_bt(bt); if (!ptr) throw error(kErrBadArg, "null output"); *ptr = bt->arena.as<double>(); });
 }
 
+namespace {
+// Process-wide cache of contraction schedules.  The schedule (non-zero C
+// blocks, coalesced pair lists, result space) depends only on the
+// contraction and on both operands' block index spaces, symmetries and
+// non-zero block sets, so operations built again from tensors of the same
+// description -- every iteration of a coupled-cluster program, every
+// letter-interface assignment -- reuse it.  Keyed by all of that, least
+// recently used entries dropped beyond the capacity.
+struct ScheduleCache {
+    std::mutex mtx;
+    std::list<std::pair<std::string, std::shared_ptr<const ContractPlan>>> lru;   // most recent first
+    std::map<std::string, decltype(lru)::iterator> index;
+    size_t capacity = 64;
+    int64_t hits = 0, misses = 0;
+};
+ScheduleCache &schedule_cache() {
+    static ScheduleCache c;
+    return c;
+}
+
+void key_put(std::string &k, int64_t v) { k.append(reinterpret_cast<const char *>(&v), sizeof(v)); }
+void key_putd(std::string &k, double v) { k.append(reinterpret_cast<const char *>(&v), sizeof(v)); }
+
+void key_tensor(std::string &k, const BlockTensorHost &h) {
+    const Bis &b = h.bis;
+    key_put(k, (int64_t)b.n);
+    for (int d = 0; d < b.n; d++) {
+        key_put(k, b.dims[d]);
+        key_put(k, (int64_t)b.starts[d].size());
+        for (int64_t x : b.starts[d]) key_put(k, x);
+    }
+    key_put(k, (int64_t)h.sym.perm.size());
+    for (const SePerm &e : h.sym.perm) {
+        for (int d = 0; d < b.n; d++) key_put(k, (int64_t)e.perm.p[d]);
+        key_putd(k, e.coeff);
+    }
+    key_put(k, (int64_t)h.sym.part.size());
+    for (const SePart &q : h.sym.part) {
+        for (int d = 0; d < b.n; d++) { key_put(k, q.pdims[d]); key_put(k, q.bipdims[d]); }
+        key_put(k, (int64_t)q.forbidden.size());
+        k.append(q.forbidden.begin(), q.forbidden.end());
+    }
+    key_put(k, (int64_t)h.sym.label.size());
+    for (const SeLabel &l : h.sym.label) {
+        key_put(k, (int64_t)l.nirrep);
+        for (int d = 0; d < b.n; d++) {
+            key_put(k, (int64_t)l.labels[d].size());
+            for (int x : l.labels[d]) key_put(k, (int64_t)x);
+        }
+        key_put(k, (int64_t)l.rule.size());
+        for (const auto &prod : l.rule) {
+            key_put(k, (int64_t)prod.size());
+            for (const LabelTerm &t : prod) {
+                for (int d = 0; d < b.n; d++) key_put(k, (int64_t)t.seq[d]);
+                key_put(k, (int64_t)t.intr);
+            }
+        }
+    }
+    key_put(k, (int64_t)h.nonzero.size());
+    k.append(h.nonzero.begin(), h.nonzero.end());
+}
+}  // namespace
+
+int ltg_schedule_cache_set_capacity(int64_t entries) {
+    return guard([&] {
+        if (entries < 0) throw error(kErrBadArg, "negative capacity");
+        ScheduleCache &c = schedule_cache();
+        std::lock_guard<std::mutex> lk(c.mtx);
+        c.capacity = (size_t)entries;
+        while (c.lru.size() > c.capacity) {
+            c.index.erase(c.lru.back().first);
+            c.lru.pop_back();
+        }
+    });
+}
+
+int ltg_schedule_cache_stats(int64_t *hits, int64_t *misses, int64_t *entries) {
+    return guard([&] {
+        ScheduleCache &c = schedule_cache();
+        std::lock_guard<std::mutex> lk(c.mtx);
+        if (hits) *hits = c.hits;
+        if (misses) *misses = c.misses;
+        if (entries) *entries = (int64_t)c.lru.size();
+    });
+}
+
 int ltg_contract2_create(ltg_ctx *ctx, int32_t n, int32_t m, int32_t k, const int32_t *permc,
                          const int32_t *pairs, ltg_bt *a, ltg_bt *b, ltg_plan **out) {
     return guard([&] {
@@ -2370,7 +2727,40 @@ int ltg_contract2_create(ltg_ctx *ctx, int32_t n, int32_t m, int32_t k, const in
         Contraction c;
         c.init(n, m, k, perm_from(n + m, permc));
         for (int q = 0; q < k; q++) c.contract(pairs[2 * q], pairs[2 * q + 1]);
-        contract2_schedule(c, a->h, b->h, pl->plan, ctx->host_threads);
+        std::string key;
+        key_put(key, (int64_t)n); key_put(key, (int64_t)m); key_put(key, (int64_t)k);
+        const Perm pc = perm_from(n + m, permc);
+        for (int d = 0; d < n + m; d++) key_put(key, (int64_t)pc.p[d]);
+        for (int q = 0; q < 2 * k; q++) key_put(key, (int64_t)pairs[q]);
+        key_tensor(key, a->h);
+        key_tensor(key, b->h);
+        ScheduleCache &sc = schedule_cache();
+        {
+            std::lock_guard<std::mutex> lk(sc.mtx);
+            auto f = sc.index.find(key);
+            if (f != sc.index.end()) {
+                sc.lru.splice(sc.lru.begin(), sc.lru, f->second);
+                pl->planp = f->second->second;
+                sc.hits++;
+                *out = pl.release();
+                return;
+            }
+            sc.misses++;
+        }
+        std::shared_ptr<ContractPlan> cp = std::make_shared<ContractPlan>();
+        contract2_schedule(c, a->h, b->h, *cp, ctx->host_threads);
+        pl->planp = cp;
+        {
+            std::lock_guard<std::mutex> lk(sc.mtx);
+            if (sc.capacity > 0 && sc.index.find(key) == sc.index.end()) {
+                sc.lru.emplace_front(key, pl->planp);
+                sc.index[key] = sc.lru.begin();
+                while (sc.lru.size() > sc.capacity) {
+                    sc.index.erase(sc.lru.back().first);
+                    sc.lru.pop_back();
+                }
+            }
+        }
         *out = pl.release();
     });
 }
@@ -2381,8 +2771,8 @@ int ltg_contract2_make_result(ltg_plan *plan, ltg_bt **c) {
         if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
         std::unique_ptr<ltg_bt> bt(new ltg_bt());
         bt->ctx = plan->ctx;
-        bt->h.bis = plan->plan.bisc;
-        bt->h.sym = plan->plan.symc;
+        bt->h.bis = plan->plan().bisc;
+        bt->h.sym = plan->plan().symc;
         alloc_arena(bt.get());
         *c = bt.release();
     });
@@ -2391,7 +2781,7 @@ int ltg_contract2_make_result(ltg_plan *plan, ltg_bt **c) {
 int ltg_plan_schedule(ltg_plan *plan, int64_t *abs_idx, int64_t cap, int64_t *n) {
     return guard([&] {
         if (!plan) throw error(kErrBadArg, "null plan");
-        const auto &s = plan->plan.schedule;
+        const auto &s = plan->plan().schedule;
         for (size_t i = 0; i < s.size() && (int64_t)i < cap; i++) abs_idx[i] = s[i];
         if (n) *n = (int64_t)s.size();
     });
@@ -2400,9 +2790,9 @@ int ltg_plan_schedule(ltg_plan *plan, int64_t *abs_idx, int64_t cap, int64_t *n)
 int ltg_plan_pairs(ltg_plan *plan, int64_t i, int64_t *out, int64_t cap, int64_t *npairs) {
     return guard([&] {
         if (!plan) throw error(kErrBadArg, "null plan");
-        if (i < 0 || i >= (int64_t)plan->plan.clst.size()) throw error(kErrBadArg, "schedule index out of range");
-        const auto &lst = plan->plan.clst[i];
-        const int NA = plan->plan.contr.NA(), NB = plan->plan.contr.NB();
+        if (i < 0 || i >= (int64_t)plan->plan().clst.size()) throw error(kErrBadArg, "schedule index out of range");
+        const auto &lst = plan->plan().clst[i];
+        const int NA = plan->plan().contr.NA(), NB = plan->plan().contr.NB();
         const int64_t rec = 2 + NA + 1 + 2 + NB + 1;
         int64_t k = 0;
         for (const Pair &p : lst) {
@@ -2423,7 +2813,7 @@ int ltg_plan_pairs(ltg_plan *plan, int64_t i, int64_t *out, int64_t cap, int64_t
 }
 
 int ltg_plan_flops(ltg_plan *plan, double *flops) {
-    return guard([&] { if (!plan || !flops) throw error(kErrBadArg, "null argument"); *flops = plan->plan.flops; });
+    return guard([&] { if (!plan || !flops) throw error(kErrBadArg, "null argument"); *flops = plan->plan().flops; });
 }
 
 
@@ -2433,10 +2823,10 @@ int ltg_plan_export_tasks(ltg_plan *plan, ltg_bt *c, int64_t *tasks, int64_t cap
         if (!plan || !ntasks) throw error(kErrBadArg, "null argument");
         check_bt(c);
         if (plan->external) throw error(kErrBadArg, "the plan holds caller-built tasks");
-        if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
+        if (!c->h.bis.equals(plan->plan().bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
         std::vector<GemmTask> t;
         std::vector<CBlockTask> cbt;
-        contract2_tasks(plan->plan, plan->a->h, plan->b->h, c->h, 1.0, 1.0, 1.0, t, cbt);
+        contract2_tasks(plan->plan(), plan->a->h, plan->b->h, c->h, 1.0, 1.0, 1.0, t, cbt);
         for (size_t i = 0; i < t.size() && (int64_t)i < cap; i++) pack_task(t[i], tasks + LTG_TASK_WORDS * i);
         *ntasks = (int64_t)t.size();
     });
@@ -2450,12 +2840,14 @@ int ltg_plan_contract2_upload(ltg_ctx *ctx, ltg_bt *a, ltg_bt *b, const int64_t 
         std::unique_ptr<ltg_plan> pl(new ltg_plan());
         pl->ctx = ctx; pl->a = a; pl->b = b;
         pl->external = true;
-        pl->plan.coalesced = true;
+        std::shared_ptr<ContractPlan> cp = std::make_shared<ContractPlan>();
+        cp->coalesced = true;
         for (int64_t i = 0; i < ntasks; i++) {
             pl->ext_tasks.push_back(unpack_task(tasks + LTG_TASK_WORDS * i));
             const GemmTask &t = pl->ext_tasks.back();
-            pl->plan.flops += 2.0 * (double)t.m.total() * (double)t.n.total() * (double)t.k.total();
+            cp->flops += 2.0 * (double)t.m.total() * (double)t.n.total() * (double)t.k.total();
         }
+        pl->planp = cp;
         *out = pl.release();
     });
 }
@@ -2483,7 +2875,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
         need_dev(plan->ctx);
         if (plan->external) {
             if (mode != LTG_MODE_PLAIN_FP64) throw error(kErrUnsupported, "a caller-built task plan runs in the plain FP64 mode only");
-        } else if (!c->h.bis.equals(plan->plan.bisc)) {
+        } else if (!c->h.bis.equals(plan->plan().bisc)) {
             throw error(kErrBadDims, "result tensor has a different block index space");
         }
         ltg_ctx *ctx = plan->ctx;
@@ -2496,6 +2888,11 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                     LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
             const double *pa = plan->a->arena.as<double>(), *pb = plan->b->arena.as<double>();
             TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
+            LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), s));
+            LTG_CUDA(launch_crt_fused(cx->panels.as<DCrtPanel>(), cx->fams.as<DCrtFamily>(), cx->famp.as<int32_t>(),
+                                      cx->famt.as<int32_t>(), cx->funits.as<int4>(), cx->nfunits, pa, pb,
+                                      cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
+                                      cx->res.as<uint8_t>(), cx->cp, s));
             LTG_CUDA(launch_crt_exponents(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, cx->nx,
                                           cx->ny, pa, pb, cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(),
                                           cx->ey.as<int32_t>(), s));
@@ -2515,7 +2912,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                                         cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), c->arena.as<double>(), add,
                                         cx->scale, cx->cp, s));
             t_comb.done();
-            ctx->launches += 2 + (cx->nunits > 0 ? 2 : 0) + (cx->nitems > 0 ? 2 : 0);
+            ctx->launches += 2 + (cx->nfunits > 0 ? 1 : 0) + (cx->nunits > 0 ? 2 : 0) + (cx->nitems > 0 ? 2 : 0);
             fetch_device_wait(ctx);
             if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
             for (int64_t sl : cx->sched_slots) c->h.nonzero[sl] = 1;
@@ -2615,7 +3012,9 @@ int ltg_contract2_split_bytes(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t n
         need_dev(plan->ctx);
         if (mode == LTG_MODE_OZAKI_CRT) {
             CrtExec *cx = prepare_crt(plan, c, nslices > 0 ? nslices : 13, ka, kb, kc, add, d);
-            *read_bytes = 2 * 8 * cx->src_elems;          // exponent pass and residue pass
+            // row families: one HBM read (the second pass reads L2); the other
+            // panels: the exponent pass and the residue pass
+            *read_bytes = 8 * (2 * cx->src_elems - cx->fused_elems);
             *write_bytes = cx->res_bytes;
         } else if (mode >= LTG_MODE_OZAKI_BF16 && mode <= LTG_MODE_OZAKI_INT8) {
             const int S = nslices > 0 ? nslices : (mode == LTG_MODE_OZAKI_FP8 ? 8 : 7);
@@ -2663,6 +3062,15 @@ int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable) {
     });
 }
 
+int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
+        plan->fused_split = enable != 0;
+        plan->crt.clear();
+    });
+}
+
 int ltg_contract2_set_crt_rows(ltg_plan *plan, int32_t rows) {
     return guard([&] {
         if (!plan) throw error(kErrBadArg, "null plan");
@@ -2679,15 +3087,15 @@ int ltg_contract2_group_info(ltg_plan *plan, ltg_bt *c, int64_t *ngroups, int64_
         if (!plan) throw error(kErrBadArg, "null plan");
         if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
         check_bt(c);
-        if (!c->h.bis.equals(plan->plan.bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
+        if (!c->h.bis.equals(plan->plan().bisc)) throw error(kErrBadDims, "result tensor has a different block index space");
         std::vector<GemmTask> tasks;
         std::vector<CBlockTask> cbt;
-        contract2_tasks(plan->plan, plan->a->h, plan->b->h, c->h, 1.0, 1.0, 1.0, tasks, cbt);
+        contract2_tasks(plan->plan(), plan->a->h, plan->b->h, c->h, 1.0, 1.0, 1.0, tasks, cbt);
         CrtSideMap sm[2];
-        crt_side_maps(plan->plan.contr, c->h, sm);
+        crt_side_maps(plan->plan().contr, c->h, sm);
         std::vector<CrtGroupHost> groups;
         std::vector<int32_t> group_of(cbt.size(), -1);
-        if (plan->group_products && !plan->plan.coalesced) crt_groups(plan, c->h, sm, cbt, groups, group_of);
+        if (plan->group_products && !plan->plan().coalesced) crt_groups(plan, c->h, sm, cbt, groups, group_of);
         int64_t nb = 0;
         double bf = 0, gf = 0;
         for (size_t e = 0; e < cbt.size(); e++)
@@ -2718,7 +3126,7 @@ int ltg_contract2_autotune(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nsli
         // Distinct C-block shapes, costliest bucket first.
         std::vector<GemmTask> tasks;
         std::vector<CBlockTask> cbt;
-        contract2_tasks(plan->plan, plan->a->h, plan->b->h, c->h, ka, kb, kc, tasks, cbt);
+        contract2_tasks(plan->plan(), plan->a->h, plan->b->h, c->h, ka, kb, kc, tasks, cbt);
         std::map<std::pair<int64_t, int64_t>, double> work;
         std::vector<int32_t> group_of;
         const std::vector<std::pair<int64_t, int64_t>> gshapes =

@@ -119,6 +119,17 @@ struct DCrtPanel {
     int32_t r0, k0, wrows, wk;
 };
 
+// A row family of the modular split: panels whose rows feed the same global
+// rows of C, row r of every panel the same global row, and nothing else
+// feeds those rows (so a row's exponent is the maximum over the family's
+// rows r alone).  Panels famp[p_begin .. p_end); famt[q] = first 16-wide k
+// tile of panel famp[q] in the family's tile sequence (famt[p_end] = ntiles).
+struct DCrtFamily {
+    int32_t p_begin, p_end;
+    int32_t rows;
+    int32_t ntiles;
+};
+
 struct DCrtTask {
     int32_t px, py;               // MMA M-side and N-side panels of one pair
     int64_t xres, yres;           // byte offsets of their tile images
@@ -311,6 +322,13 @@ void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t
 cudaError_t launch_crt_exponents(const DCrtPanel *panels, const int4 *units, int32_t nunits,
     int32_t nx, int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
     int32_t *ey, cudaStream_t s);
+// Sets both exponent tables to "no element" (before the passes below).
+cudaError_t launch_crt_fill(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, cudaStream_t s);
+// Exponents and residues of the row families in one HBM read (units: 8 rows
+// of one family, {family, first row, rows, 0}); ex/ey hold kNoExp before.
+cudaError_t launch_crt_fused(const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
+    const int32_t *famt, const int4 *units, int32_t nunits, const double *a, const double *b,
+    const int32_t *gidx, int32_t *ex, int32_t *ey, uint8_t *res, const CrtParams &cp, cudaStream_t s);
 cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int32_t nunits,
     const double *a, const double *b, const int32_t *gidx, const int32_t *ex, const int32_t *ey,
     uint8_t *res, const CrtParams &cp, cudaStream_t s);

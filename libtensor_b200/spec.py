@@ -257,3 +257,34 @@ class RingConfig:
 
 RING_D2H = RingConfig("ring D2h o=46 v=296", D2H_OCC, D2H_VIR)
 RING_D2H_SMALL = RingConfig("ring D2h small", [2, 1, 1, 1, 2, 1, 1, 1], [5, 2, 3, 1, 4, 2, 3, 1])
+
+
+@dataclass
+class DenseConfig:
+    """C(i,j) = sum_k A(i,k) B(j,k) with one block per tensor and no symmetry:
+    the DMMA kernel on one long product, without a schedule's uneven end."""
+    name: str
+    n: int
+
+    @property
+    def o(self):
+        return self.n
+
+    @property
+    def v(self):
+        return self.n
+
+    def t_spec(self) -> BTSpec:
+        return BTSpec(dims=[self.n, self.n], splits=[[], []])
+
+    def v_spec(self) -> BTSpec:
+        return BTSpec(dims=[self.n, self.n], splits=[[], []])
+
+    contraction = dict(n=1, m=1, k=1, permc=None, pairs=[(1, 1)])
+    kc = 1.0
+    t_scale = 1.0
+    v_scale = 1.0
+
+
+DENSE_6144 = DenseConfig("dense 6144^3", 6144)
+

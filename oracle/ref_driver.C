@@ -49,6 +49,8 @@
 #include <libtensor/block_tensor/btod_add.h>
 #include <libtensor/block_tensor/btod_copy.h>
 #include <libtensor/block_tensor/btod_dotprod.h>
+#include <libtensor/block_tensor/btod_symmetrize2.h>
+#include <libtensor/block_tensor/btod_symmetrize4.h>
 #include <libtensor/dense_tensor/dense_tensor_ctrl.h>
 #include <libtensor/symmetry/so_copy.h>
 #include <libtensor/symmetry/se_perm.h>
@@ -444,6 +446,63 @@ void denominator(void *h, const double *eps, int nocc) {
     }
 }
 
+/* ---------------- symmetrizers ----------------------------------------- */
+
+/* b = op + s P(op) for a unitary permutation P (btod_symmetrize2,
+   block_tensor/btod_symmetrize2.h:54), or the sum over the 24 permutations
+   of four indexes with the parity sign (btod_symmetrize4,
+   block_tensor/btod_symmetrize4.h:53), of any additive operation op. */
+// The reference instantiates btod_symmetrize2 for orders >= 2 and
+// btod_symmetrize4 for orders >= 4 (block_tensor/impl/btod_symmetrize2.C,
+// btod_symmetrize4.C).
+template<size_t N, bool Two = (N >= 2), bool Four = (N >= 4)>
+struct symm_impl {
+    static void run(additive_gen_bto<N, btod_traits::bti_traits> &, int, const int32_t *, int, void *, int,
+                    double) {
+        throw std::runtime_error("symmetrize: tensor order too small");
+    }
+};
+template<size_t N, bool Four>
+struct symm_impl<N, true, Four> {
+    static void run(additive_gen_bto<N, btod_traits::bti_traits> &op, int nidx, const int32_t *idx, int symm,
+                    void *b, int add, double d) {
+        block_tensor<N, double, alloc_t> &bt = as<N>(b)->bt;
+        if (nidx == 2 || nidx == -1) {
+            permutation<N> p;
+            if (nidx == 2) p.permute((size_t)idx[0], (size_t)idx[1]);
+            else p = perm_from<N>(idx);
+            btod_symmetrize2<N> s(op, p, symm != 0);
+            if (add) s.perform(bt, d);
+            else s.perform(bt);
+        } else {
+            symm_impl<N, false, Four>::run(op, nidx, idx, symm, b, add, d);
+        }
+    }
+};
+template<size_t N>
+struct symm_impl<N, false, true> {
+    static void run(additive_gen_bto<N, btod_traits::bti_traits> &op, int nidx, const int32_t *idx, int symm,
+                    void *b, int add, double d) {
+        if (nidx != 4) throw std::runtime_error("symmetrize: 2 or 4 indexes, or a permutation");
+        block_tensor<N, double, alloc_t> &bt = as<N>(b)->bt;
+        btod_symmetrize4<N> s(op, (size_t)idx[0], (size_t)idx[1], (size_t)idx[2], (size_t)idx[3], symm != 0);
+        if (add) s.perform(bt, d);
+        else s.perform(bt);
+    }
+};
+
+template<size_t N>
+void symmetrize_op(additive_gen_bto<N, btod_traits::bti_traits> &op, int nidx, const int32_t *idx, int symm,
+    void *b, int add, double d) {
+    symm_impl<N>::run(op, nidx, idx, symm, b, add, d);
+}
+
+template<size_t N>
+void symmetrize_copy(void *a, double c, int nidx, const int32_t *idx, int symm, void *b, int add, double d) {
+    btod_copy<N> cp(as<N>(a)->bt, c);
+    symmetrize_op<N>(cp, nidx, idx, symm, b, add, d);
+}
+
 /* ---------------- contraction ------------------------------------------ */
 
 struct c2_base {
@@ -453,6 +512,7 @@ struct c2_base {
     virtual void perform(void *c, int add, double d) = 0;
     virtual size_t clst(int64_t cabs, int64_t *out, size_t cap) = 0;
     virtual void cost(int64_t *exact, int64_t *ref_cost) = 0;
+    virtual void symmetrize(int nidx, const int32_t *idx, int symm, void *b, int add, double d) = 0;
     virtual void result_bidims(int64_t *out) = 0;
 };
 
@@ -475,6 +535,10 @@ struct c2_h : c2_base {
             if (i < cap) out[i] = (int64_t)sch.get_abs_index(it);
         }
         return i;
+    }
+
+    void symmetrize(int nidx, const int32_t *idx, int symm, void *b, int add, double d) {
+        symmetrize_op<NC>(op, nidx, idx, symm, b, add, d);
     }
 
     void *make_result() {
@@ -829,6 +893,25 @@ int64_t ref_contract2_clst(void *op, int64_t cabs, int64_t *out, int64_t cap) {
    c2_h::cost. */
 int ref_contract2_cost(void *op, int64_t *exact, int64_t *ref_cost) {
     try { static_cast<c2_base*>(op)->cost(exact, ref_cost); return 0; }
+    catch (libtensor::exception &e) { g_err = e.what(); return -1; }
+    catch (std::exception &e) { g_err = e.what(); return -1; }
+}
+
+/* Symmetrizer of a tensor (wrapping btod_copy with coefficient c) or of a
+   contraction.  nidx 2: indexes idx[0], idx[1]; -1: the unitary permutation
+   idx[0..N); 4: the four indexes idx[0..3]. */
+int ref_symmetrize(void *a, double c, int nidx, const int32_t *idx, int symm, void *b, int add, double d) {
+    try {
+#define CALL(k) symmetrize_copy<k>(a, c, nidx, idx, symm, b, add, d)
+        DISPATCH_ORDER(static_cast<bt_base*>(a)->order, CALL)
+#undef CALL
+        return 0;
+    } catch (libtensor::exception &e) { g_err = e.what(); return -1; }
+    catch (std::exception &e) { g_err = e.what(); return -1; }
+}
+
+int ref_contract2_symmetrize(void *op, int nidx, const int32_t *idx, int symm, void *b, int add, double d) {
+    try { static_cast<c2_base*>(op)->symmetrize(nidx, idx, symm, b, add, d); return 0; }
     catch (libtensor::exception &e) { g_err = e.what(); return -1; }
     catch (std::exception &e) { g_err = e.what(); return -1; }
 }

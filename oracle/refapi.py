@@ -42,6 +42,8 @@ _SIGS = {
     "ref_contract2_clst": (C.c_int64, [_vp, C.c_int64, _i64p, C.c_int64]),
     "ref_contract2_cost": (C.c_int, [_vp, _i64p, _i64p]),
     "ref_denominator": (C.c_int, [_vp, _dblp, C.c_int]),
+    "ref_symmetrize": (C.c_int, [_vp, C.c_double, C.c_int, _i32p, C.c_int, _vp, C.c_int, C.c_double]),
+    "ref_contract2_symmetrize": (C.c_int, [_vp, C.c_int, _i32p, C.c_int, _vp, C.c_int, C.c_double]),
     "ref_bt_fill_seeded": (C.c_int, [_vp, C.c_uint64, C.c_double, C.c_int, _i32p, _i32p, C.c_int]),
     "ref_copy": (C.c_int, [_vp, _i32p, C.c_double, _vp, C.c_int, C.c_double]),
     "ref_add": (C.c_int, [C.c_int, C.POINTER(_vp), _i32p, _dblp, _vp, C.c_int, C.c_double]),
@@ -220,6 +222,13 @@ class RefContract2:
         _chk(lib().ref_contract2_cost(self.h, C.byref(ex), C.byref(rc)))
         return ex.value, rc.value
 
+    def symmetrize(self, b: RefBT, symm: bool, idx=(), perm=None, d=None):
+        """The contraction symmetrized (btod_symmetrize2/4 wrapping this
+        btod_contract2) into b."""
+        n, arr = _symm_args(idx, perm)
+        _chk(lib().ref_contract2_symmetrize(self.h, n, arr, 1 if symm else 0, b.h, 0 if d is None else 1,
+                                            0.0 if d is None else d))
+
     def make_result(self) -> RefBT:
         h = lib().ref_contract2_make_result(self.h)
         if not h:
@@ -243,6 +252,22 @@ def ref_add(ops, b: RefBT, d=None):
         perms += list(p) if p is not None else list(range(n))
     cs = (C.c_double * len(ops))(*[o[2] for o in ops])
     _chk(lib().ref_add(len(ops), hs, _i32(perms), cs, b.h, 0 if d is None else 1, 0.0 if d is None else d))
+
+
+def _symm_args(idx, perm):
+    if perm is not None:
+        return -1, _i32(list(perm))
+    return len(idx), _i32(list(idx))
+
+
+def ref_symmetrize(a: RefBT, c, b: RefBT, symm: bool, idx=(), perm=None, d=None):
+    """b = c (A + s P A) (btod_symmetrize2 over indexes idx[0], idx[1] or the
+    unitary permutation perm) or the 24-term sum over four indexes idx
+    (btod_symmetrize4); s = +1 symmetric, -1 antisymmetric (and the
+    permutation's parity for four indexes)."""
+    n, arr = _symm_args(idx, perm)
+    _chk(lib().ref_symmetrize(a.h, c, n, arr, 1 if symm else 0, b.h, 0 if d is None else 1,
+                              0.0 if d is None else d))
 
 
 def ref_denominator(a: RefBT, eps: np.ndarray, nocc: int):

@@ -179,6 +179,54 @@ int main(int argc, char **argv) {
         ys(i|j|a|b) = symm(i|a, j|b, r(i|j|a|b));             // = 2 r
         gs(i|j|a|b) = asymm(a, b, contract(c1, t(i|j|a|c1), fl(c1|b)));
         btod_symmetrize2<4>(ge, 2, 3, false).perform(gse);
+        // intermediates: a contraction of a contraction, a contraction of a sum
+        // (terms with the same symmetry, and with a spin-only term, whose sum
+        // keeps only the common symmetry), the result on the right-hand side,
+        // a dot product of a sum -- against the operations written out
+        block_tensor<4, double> nl(bis_r), ne(bis_r);
+        nl(i|j|a|b) = contract(c1, contract(d1, t(i|j|a|d1), fl(d1|c1)), fl(c1|b));
+        btod_contract2<3, 1, 1>(c1c, ge, fe).perform(ne);
+        block_tensor<4, double> ql(bis_r), qe(bis_r), u(bis_t);
+        add_symmetry(u, bis_t);
+        ql(i|j|a|b) = contract(c1, t(i|j|a|c1) + s(i|j|a|c1), fl(c1|b));
+        btod_add<4> tu(t, 1.0);
+        tu.add_op(s, 1.0);
+        tu.perform(u);
+        btod_contract2<3, 1, 1>(c1c, u, fe).perform(qe);
+        block_tensor<4, double> w(bis_t), wl(bis_r), we(bis_r), uw(bis_t);
+        {
+            block_tensor_ctrl<4, double> cw(w);
+            symmetry<4, double> &sym = cw.req_symmetry();
+            mask<4> all;
+            for (size_t k = 0; k < 4; k++) all[k] = true;
+            se_part<4, double> part(bis_t, all, 2);
+            for (size_t x = 0; x < 16; x++) {
+                index<4> pp;
+                for (size_t k = 0; k < 4; k++) pp[k] = (x >> (3 - k)) & 1;
+                if (pp[0] + pp[1] != pp[2] + pp[3]) part.mark_forbidden(pp);
+            }
+            sym.insert(part);
+            cw.fill_seeded(29, 0.01);
+            block_tensor_ctrl<4, double> cu(uw);
+            cu.req_symmetry().insert(part);
+        }
+        wl(i|j|a|b) = contract(c1, t(i|j|a|c1) - 2.0 * w(i|j|a|c1), fl(c1|b));
+        btod_add<4> twu(t, 1.0);
+        twu.add_op(w, -2.0);
+        twu.perform(uw);
+        btod_contract2<3, 1, 1>(c1c, uw, fe).perform(we);
+        block_tensor<4, double> hr(bis_r);
+        hr(i|j|a|b) = r(i|j|a|b);
+        hr(i|j|a|b) = hr(i|j|a|b) + r(i|j|a|b);               // = 2 r
+        const double dl_sum = dot_product(t(i|j|a|b) + s(i|j|a|b), t(i|j|a|b));   // = <t,t> + <s,t>
+        // one assignment with intermediates kept and replayed as one graph
+        block_tensor<4, double> qg(bis_r);
+        b200::assignment<4> asg(qg(i|j|a|b), contract(c1, t(i|j|a|c1) + s(i|j|a|c1), fl(c1|b)));
+        asg.capture();
+        block_tensor_ctrl<4, double>(qg).fill_seeded(8, 1.0);
+        asg.run();
+        b200::synchronize();
+        const double asg_diff = max_diff(qg, ql, 1.0);
         // one CUDA graph of the contraction, the permuted copy and the add:
         // run once, captured, inputs overwritten, replayed
         block_tensor<4, double> r2(bis_r), tp2(bis_t), s2(bis_t);
@@ -203,7 +251,10 @@ int main(int argc, char **argv) {
                                 std::fabs(dl_tt - dot_tt), std::fabs(dl_tp + dot_tt),
                                 max_diff(fl, fe, 1.0), max_diff(gl, ge, 1.0),
                                 max_diff(hl, r, 0.5), max_diff(ys, r, 2.0),
-                                max_diff(gs, gse, 1.0), graph_diff};
+                                max_diff(gse, gs, 1.0), graph_diff,
+                                max_diff(nl, ne, 1.0), max_diff(ql, qe, 1.0), max_diff(wl, we, 1.0),
+                                max_diff(r, hr, 0.5), std::fabs(dl_sum - dot_tt - dot_ts), asg_diff,
+                                (double)asg.operations()};
 
         // the contraction's non-zero blocks in index order, then the dot products
         FILE *f = std::fopen(argv[2], "wb");

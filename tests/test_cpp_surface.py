@@ -61,7 +61,7 @@ def test_surface_compute_matches_golden(exe, tmp_path):
     assert abs(dot_pp - 0.25 * dot_tt) <= 1e-13 * dot_tt
     # letter interface against the operations written out: the ladder, an
     # antisymmetrising difference, dot products (one permuted), K = 3 and
-    # K = 1 contractions, assignment then -=, symmetrizers
+    # K = 1 contractions, assignment then -=, symmetrizers, intermediates
     d = [float(x) for x in lines[pos + 1].split()]
     rmax = max(float(np.max(np.abs(v))) for v in gold.values())
     assert d[0] == 0.0                                  # the same plan and kernels
@@ -72,3 +72,12 @@ def test_surface_compute_matches_golden(exe, tmp_path):
     assert d[7] <= 1e-15 * rmax                         # symm(i|a, j|b, r) = 2 r
     assert d[8] == 0.0                                  # asymm(a, b, contraction) = btod_symmetrize2
     assert d[9] == 0.0                                  # graph replay = eager operations
+    # intermediates: nested contraction, contraction of sums (same symmetry,
+    # and a spin-only term), result on the right-hand side, dot of a sum, and
+    # the assignment replayed as one graph (bit-identical to its eager run)
+    gmax = max(1.0, rmax)
+    assert d[10] <= 1e-13 * gmax and d[11] <= 1e-13 * gmax and d[12] <= 1e-13 * gmax
+    assert d[13] <= 1e-15 * rmax                        # r - hr / 2, hr = r + r
+    assert d[14] <= 1e-13 * dot_tt
+    assert d[15] == 0.0
+    assert d[16] >= 3                                   # the add into the intermediate, the contraction

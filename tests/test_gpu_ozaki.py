@@ -159,3 +159,37 @@ def test_grouped_products_with_zero_operand_blocks(gctx):
         op.set_grouping(True)
         if mode == MODE_OZAKI_CRT:
             assert np.array_equal(out[0].view(np.uint64), out[1].view(np.uint64))
+
+
+@pytest.mark.parametrize("which", ["ladder", "ring", "ladder o=40 v=160"])
+def test_fused_split_matches_two_pass(gctx, which):
+    """Row families split in one read of the operand (exponents and residues
+    in one kernel, the second read from L2) give the same bits as the
+    exponent pass followed by the residue pass, in assign and add mode."""
+    from libtensor_b200 import spec as S
+    from libtensor_b200.core import block_tensor, btod_contract2, contraction2
+    cfg = {"ladder": S.LADDER_SMALL, "ring": S.RING_D2H_SMALL, "ladder o=40 v=160": S.LADDER_PROF}[which]
+    a_spec = cfg.t_spec()
+    b_spec = cfg.v_spec() if hasattr(cfg, "v_spec") else cfg.w_spec()
+    A, B = block_tensor(gctx, a_spec), block_tensor(gctx, b_spec)
+    A.fill_seeded(11, cfg.t_scale)
+    B.fill_seeded(23, cfg.v_scale)
+    c = cfg.contraction
+    contr = contraction2(c["n"], c["m"], c["k"], c["permc"])
+    for p in c["pairs"]:
+        contr.contract(*p)
+    op = btod_contract2(contr, A, B, kc=cfg.kc)
+    out = []
+    for fused in (True, False):
+        op.set_fused_split(fused)
+        C = op.make_result()
+        op.perform(C, mode=MODE_OZAKI_CRT, nslices=13)
+        op.perform(C, 0.5, mode=MODE_OZAKI_CRT, nslices=13)
+        gctx.synchronize()
+        out.append(C.download())
+        C.close()
+    op.set_fused_split(True)
+    assert np.array_equal(out[0].view(np.uint64), out[1].view(np.uint64))
+    op.close()
+    A.close()
+    B.close()

@@ -1,0 +1,122 @@
+"""GPU parity of the symmetrizers (ltg_symmetrize; btod_symmetrize2 /
+btod_symmetrize4 of libtensor/block_tensor/btod_symmetrize2.h:19,
+btod_symmetrize4.h:27):
+
+* the exchange of two indexes and a unitary pair exchange P(01)P(23), symmetric
+  and antisymmetric, of a tensor and of a contraction's result (the ring
+  term), against the reference's btod_symmetrize2 wrapping btod_copy or the
+  btod_contract2 itself, assign and add;
+* the 24-term sum over four indexes against the dense numpy restatement (the
+  reference's btod_symmetrize4 leaves index i1 without a group in its
+  make_symmetry, gen_bto_symmetrize4_impl.h:219-249, and fails).
+The product's result space (ltg_bt_create_symmetrized) has the reference's
+canonical blocks in these cases, so results compare block by block."""
+from itertools import permutations
+
+import numpy as np
+import pytest
+
+from libtensor_b200 import spec as S
+from libtensor_b200.core import Context, block_tensor, btod_contract2, btod_symmetrize, contraction2
+from libtensor_b200.spec import BTSpec
+from oracle import refapi as R
+from oracle import restate as X
+from tests.helpers import block_errors, max_rel_block_error
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")]
+
+TOL = 1e-15
+
+
+@pytest.fixture(scope="module")
+def gctx():
+    c = Context(0)
+    yield c
+    c.close()
+
+
+CASES = [dict(symm=False, idx=(0, 1)), dict(symm=True, idx=(2, 3)), dict(symm=False, perm=(1, 0, 3, 2)),
+         dict(symm=True, perm=(1, 0, 3, 2))]
+IDS = ["asymm(0,1)", "symm(2,3)", "asymm P(01)P(23)", "symm P(01)P(23)"]
+
+
+@pytest.mark.parametrize("kw", CASES, ids=IDS)
+def test_symmetrize_tensor_matches_reference(gctx, kw):
+    spec = S.RING_D2H_SMALL.t_spec()
+    x_spec = BTSpec(dims=spec.dims, splits=spec.splits, part_pdims=spec.part_pdims,
+                    part_forbidden=spec.part_forbidden, labels=spec.labels, label_nirrep=spec.label_nirrep,
+                    label_intr=spec.label_intr)              # spin and labels, no permutational symmetry
+    a = block_tensor(gctx, x_spec)
+    a.fill_seeded(41, 1.0)
+    ra = R.RefBT(x_spec)
+    ra.fill_seeded(41, 1.0)
+    op = btod_symmetrize(a, c=0.5, **kw)
+    b = op.make_result()
+    op.perform(b)
+    rb = R.RefBT(x_spec)
+    R.ref_symmetrize(ra, 0.5, rb, **kw)
+    errs = block_errors(b, b.download(), rb, None)
+    assert max_rel_block_error(errs) <= TOL
+    op.perform(b, 2.0)                                       # b += 2 * (sum)
+    R.ref_symmetrize(ra, 0.5, rb, d=2.0, **kw)
+    assert max_rel_block_error(block_errors(b, b.download(), rb, None)) <= TOL
+
+
+@pytest.mark.parametrize("kw", [CASES[0], CASES[2]], ids=[IDS[0], IDS[2]])
+def test_symmetrize_contraction_matches_reference(gctx, kw):
+    """The ring term r(i,j,a,b) = sum_kc t(i,k,a,c) W(k,b,c,j) antisymmetrized
+    (the result of the product's contraction, symmetrized) against the
+    reference's btod_symmetrize2 wrapping its btod_contract2."""
+    cfg = S.RING_D2H_SMALL
+    c = cfg.contraction
+    A, B = block_tensor(gctx, cfg.t_spec()), block_tensor(gctx, cfg.w_spec())
+    A.fill_seeded(11, cfg.t_scale)
+    B.fill_seeded(23, cfg.v_scale)
+    contr = contraction2(c["n"], c["m"], c["k"], c["permc"])
+    for p in c["pairs"]:
+        contr.contract(*p)
+    op = btod_contract2(contr, A, B)
+    G = op.make_result()
+    op.perform(G)
+    sy = btod_symmetrize(G, **kw)
+    out = sy.make_result()
+    sy.perform(out)
+    ra, rb = R.RefBT(cfg.t_spec()), R.RefBT(cfg.w_spec())
+    ra.fill_seeded(11, cfg.t_scale)
+    rb.fill_seeded(23, cfg.v_scale)
+    rop = R.RefContract2(c["n"], c["m"], c["k"], c["permc"], c["pairs"], ra, rb)
+    rout = rop.make_result()
+    rop.symmetrize(rout, **kw)
+    errs = block_errors(out, out.download(), rout, None)
+    assert max_rel_block_error(errs) <= 1e-13
+
+
+def _parity(p):
+    p, s = list(p), 1
+    for i in range(len(p)):
+        while p[i] != i:
+            j = p[i]
+            p[i], p[j] = p[j], p[i]
+            s = -s
+    return s
+
+
+@pytest.mark.parametrize("symm", [True, False], ids=["symm", "asymm"])
+def test_symmetrize4_matches_dense(gctx, symm):
+    spec = BTSpec(dims=[12] * 4, splits=[[5]] * 4)
+    a = block_tensor(gctx, spec)
+    a.fill_seeded(6, 1.0)
+    d = X.seeded_dense(spec, 6, 1.0)
+    want = sum((1 if symm else _parity(p)) * np.transpose(d, p) for p in permutations(range(4)))
+    op = btod_symmetrize(a, symm, idx=(0, 1, 2, 3))
+    b = op.make_result()
+    op.perform(b)
+    got = b.download()
+    worst = 0.0
+    for bidx, blk in b.blocks(got):
+        w = X.block_view(spec, want, bidx)
+        worst = max(worst, float(np.max(np.abs(blk - w))) / max(1e-300, float(np.max(np.abs(want)))))
+    assert worst <= 1e-14
+    # the result space has the symmetric group of the four indexes: with two
+    # blocks per index, one canonical block per number of second blocks
+    assert len(b.abs_idx) == 5
