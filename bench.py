@@ -81,8 +81,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-DMMA companion timing")
-    p.add_argument("--no-fused-split", action="store_true",
-                   help="modular mode: exponent pass and residue pass instead of the one-read split")
+    p.add_argument("--fused-split", type=int, default=0, choices=[0, 1, 2],
+                   help="modular mode: one-read split of row families in kernel shape 1 or 2 (0: exponent and "
+                        "residue passes)")
     p.add_argument("--tile", type=int, default=-1, help="force one tile shape (debug)")
     p.add_argument("--split-k", type=int, default=0, choices=[0, 1, 2, 3, 4],
                    help="plain mode: k chunks per tile (0 automatic, 1 never)")
@@ -292,8 +293,8 @@ def ltg_arm(args):
         op.set_crt_rows(args.crt_rows)
     if args.split_k:
         op.set_split_k(args.split_k)
-    if args.no_fused_split:
-        op.set_fused_split(False)
+    if args.fused_split:
+        op.set_fused_split(args.fused_split)
     if args.tile >= 0:
         op.set_tile(args.tile)
     elif not args.no_autotune:

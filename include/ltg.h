@@ -257,12 +257,14 @@ int ltg_contract2_set_split_k(ltg_plan *plan, int32_t k);
  * a few rows, as under point-group symmetry, fill whole tiles).  No reference
  * counterpart. */
 int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable);
-/* Modular mode: enables (default) or disables the one-read split of row
- * families -- panels whose rows feed the same rows of C and nothing else does
- * -- which forms each row's exponent and its residues in one pass over the
- * operand (the second read of each tile hits L2) instead of an exponent pass
- * and a residue pass.  Both forms give identical bits.  No reference
- * counterpart. */
+/* Modular mode: the one-read split of row families -- panels whose rows feed
+ * the same rows of C and nothing else does -- which forms each row's exponent
+ * and its residues in one pass over the operand (the second read of each
+ * tile hits L2) instead of an exponent pass and a residue pass: shape 0 off
+ * (default), 1 or 2 (rows per CTA, threads, CTAs per SM: 2/512/2, 2/256/4).
+ * All forms give identical bits; on the ladder o=40 v=240 the two passes are
+ * faster (2.40 ms against 2.68 ms for shape 2, although the one-read form
+ * moves 9.6 GB through HBM against 13.2).  No reference counterpart. */
 int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable);
 /* Modular mode: rows of the products kernel's work items, 256 (two MMA
  * tiles sharing each operand tile of the other side; also 0, the default) or
@@ -270,6 +272,11 @@ int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable);
  * next, at twice the operand traffic per product).  Both give identical bits.
  * No reference counterpart. */
 int ltg_contract2_set_crt_rows(ltg_plan *plan, int32_t rows);
+/* Modular mode: 32-byte k blocks per pipeline stage of the products kernel
+ * (2, 3, 4 (default) or 6; the stages fill about 200 KB of shared memory,
+ * each stage's k blocks moved as one bulk copy per operand tile).  No
+ * reference counterpart. */
+int ltg_contract2_set_crt_stage(ltg_plan *plan, int32_t kblocks);
 /* Host-side summary of the grouped products the modular mode would use for
  * result c: number of groups, C blocks they cover, flops of the grouped
  * products (padding of the contracted blocks to 4 included) and algorithmic

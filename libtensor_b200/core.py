@@ -317,9 +317,14 @@ class btod_contract2:
         """Plain FP64 mode: k chunks per output tile (0 automatic, 1 never, 2-4 always)."""
         check(lib().ltg_contract2_set_split_k(self.h, k))
 
-    def set_fused_split(self, enable: bool):
-        """Modular mode: one-read split of row families (default on)."""
-        check(lib().ltg_contract2_set_fused_split(self.h, 1 if enable else 0))
+    def set_fused_split(self, shape: int):
+        """Modular mode: one-read split of row families in kernel shape 1 or 2,
+        or 0 (default) for the exponent and residue passes."""
+        check(lib().ltg_contract2_set_fused_split(self.h, int(shape)))
+
+    def set_crt_stage(self, kblocks: int):
+        """Modular mode: k blocks per pipeline stage of the products kernel."""
+        check(lib().ltg_contract2_set_crt_stage(self.h, kblocks))
 
     def set_grouping(self, enable: bool):
         """Modular mode: grouped products of small C blocks (default on)."""

@@ -31,11 +31,8 @@
 // bounded in time and reports through *err.
 #include <type_traits>
 
-#include <cooperative_groups.h>
-
 #include "ltg_device.cuh"
 
-namespace cg = cooperative_groups;
 
 namespace ltg {
 namespace {
@@ -45,8 +42,8 @@ constexpr int kKB = 32;                             // bytes (INT8 elements) per
 constexpr int kXTile = kXRows * kKB;                // 4 KB
 constexpr int kMaxNt = 256;
 constexpr int kSubBytes = 2 * kXTile + kMaxNt * kKB;    // one k block: two M tiles and one N tile (16 KB)
-constexpr int kKbPerStage = 4;                           // k blocks per pipeline stage
-constexpr int kStageBytes = kKbPerStage * kSubBytes;     // 32 KB
+// (a stage holds KB k blocks as [M tile 0][M tile 1][N tile] regions; KB is
+// the products kernel's template parameter, crt_stage_kb() at launch)
 constexpr int kMaxStages = 8;
 constexpr int kEpiWarps = 8;                        // two per TMEM lane quarter
 constexpr int kGemmThreads = 32 * (kEpiWarps + 2);  // + bulk-copy producer + MMA issuer
@@ -124,12 +121,13 @@ __device__ __forceinline__ int64_t mixed_offset(int32_t lin, int n, const int32_
 }
 
 // Byte offset of element (row r, k byte kb_byte of k block kb) of modulus l
-// in a panel's tile images: [row tile][k block][modulus] images of TR rows x
-// 32 bytes, K-major core matrices of 8 rows x 16 bytes (the two 16-byte k
-// halves 128 bytes apart, 8-row groups 256 bytes apart).
+// in a panel's tile images: [row tile][modulus][k block] images of TR rows x
+// 32 bytes (so that the k blocks of one pipeline stage are one contiguous
+// copy), K-major core matrices of 8 rows x 16 bytes (the two 16-byte k halves
+// 128 bytes apart, 8-row groups 256 bytes apart).
 __device__ __forceinline__ int64_t image_offset(int r, int TR, int nkb, int kb, int l, int L, int kb_byte) {
     const int tile = r / TR, rr = r - tile * TR;
-    return ((int64_t)(tile * nkb + kb) * L + l) * (int64_t)(TR * kKB) + (rr >> 3) * 256 +
+    return ((int64_t)(tile * L + l) * nkb + kb) * (int64_t)(TR * kKB) + (rr >> 3) * 256 +
            (kb_byte >> 4) * 128 + (rr & 7) * 16 + (kb_byte & 15);
 }
 
@@ -284,7 +282,7 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
         uint8_t *base = res + P.res_off;
         const int TR = P.tr, nkb = P.K_pad / kKB;
         const double coef = (double)P.coef;
-        const int64_t lstride = (int64_t)TR * kKB;            // next modulus image
+        const int64_t lstride = (int64_t)nkb * TR * kKB;      // the same k block of the next modulus
         int cur = -1;
         const double *row = src;
         double s1 = 0.0, s2 = 0.0;
@@ -301,14 +299,16 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
             s2 = ldexp(1.0, sh - sh / 2);
             live = valid && e > kNoExp;
         };
-        // residues of k0..k0+3 of row r (k0 % 4 == 0) into the images
-        auto put4 = [&](int r, int k0) {
-            double x[4];
+        // elements k0..k0+3 of the current row (zero past K)
+        auto load4 = [&](int k0, double *x) {
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int k = k0 + j;
                 x[j] = (live && k < P.K) ? row[koffset(P, mode, koff, k)] : 0.0;
             }
+        };
+        // residues of k0..k0+3 of row r (k0 % 4 == 0) into the images
+        auto put4x = [&](int r, int k0, const double *x) {
             uint32_t packed[L];
 #pragma unroll
             for (int l = 0; l < L; l++) packed[l] = 0;
@@ -328,6 +328,11 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
             uint8_t *dst0 = base + image_offset(P.r0 + r, TR, nkb, kk / kKB, 0, L, kk % kKB);
 #pragma unroll
             for (int l = 0; l < L; l++) *reinterpret_cast<uint32_t *>(dst0 + l * lstride) = packed[l];
+        };
+        auto put4 = [&](int r, int k0) {
+            double x[4];
+            load4(k0, x);
+            put4x(r, k0, x);
         };
         if (un.w == kUnitRowMap) {
             const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
@@ -354,99 +359,92 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
 //
 // The two passes above read every operand element twice from HBM (once for
 // the row maxima, once for the residues).  For a row family (DCrtFamily) the
-// exponent of a row needs only that family's rows, so a unit of 8 rows is
-// split completely by one cluster of kFuseCs CTAs: each CTA takes an equal
-// share of the family's 16-wide k tiles, pass 1 forms its row maxima, the
-// cluster combines them through distributed shared memory, and pass 2 reads
-// the same share again -- from L2 (8 rows x its share, a few hundred KB per
-// CTA, read moments before) -- and writes the residue images.  Thread
-// mapping of both passes: a warp takes one core tile (the unit's 8 rows x 16
-// k; lane l row l / 4 and the 4 consecutive k of group l % 4), so that every
-// residue store of a warp is one whole 128-byte core matrix.  Family panels
-// have one contiguous k run (k offset = k).
+// exponent of a row needs only that family's rows, so one CTA splits a unit
+// of kFuseRows rows of a family completely: pass 1 reads the rows (all of the
+// family's k) and forms their maxima, pass 2 reads them again -- from L2:
+// the resident CTAs hold kFuseRows rows of a family each, tens of MB in all
+// -- and writes the residue images.  HBM then sees the operand once.  Lane
+// mapping of both passes: kFuseRows rows x 16 groups of 4 consecutive k per
+// warp (a 64-wide k tile), so that pass-2 stores of a warp fill whole
+// 32-byte sectors of the core matrices (two rows x 16 bytes each).  Family
+// panels have one contiguous k run (k offset = k).
 
-constexpr int kFuseCs = 8;                          // CTAs per unit (cluster size)
-constexpr int kFuseThreads = 256;
-constexpr int kFuseWarps = kFuseThreads / 32;
-constexpr int kFuseCtasPerSm = 4;
+// Shapes of the one-read split (rows per unit, threads, CTAs per SM); the
+// resident CTAs' rows must stay well inside L2 (148 SMs x CTAs x rows x the
+// family's k x 8 bytes).
+template<int ROWS, int THREADS, int MINB>
+struct FuseCfg {
+    static constexpr int kRows = ROWS, kThreads = THREADS, kCtasPerSm = MINB;
+    static constexpr int kWarps = THREADS / 32;
+    static constexpr int kLanesPerRow = 32 / ROWS;     // 4-k groups per row in a warp tile
+    static constexpr int kTileK = 4 * kLanesPerRow;    // k per warp tile
+};
 
-template<int L>
-__global__ void __cluster_dims__(kFuseCs, 1, 1) __launch_bounds__(kFuseThreads, kFuseCtasPerSm)
+template<int L, class FC>
+__global__ void __launch_bounds__(FC::kThreads, FC::kCtasPerSm)
 crt_fused_kernel(const DCrtPanel *__restrict__ panels, const DCrtFamily *__restrict__ fams,
                  const int32_t *__restrict__ famp, const int32_t *__restrict__ famt,
                  const int4 *__restrict__ units, int32_t nunits, const double *__restrict__ A,
                  const double *__restrict__ B, const int32_t *__restrict__ gidx, int32_t *ex, int32_t *ey,
                  uint8_t *__restrict__ res, const CrtParams cp) {
-    __shared__ int32_t rexp[8];          // this CTA's row maxima (exponents)
-    __shared__ int32_t rfin[8];          // the cluster's
-    cg::cluster_group cluster = cg::this_cluster();
-    const int crank = (int)cluster.block_rank();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lrow = lane >> 2, kq = lane & 3;
-    const int nclusters = gridDim.x / kFuseCs, cid = blockIdx.x / kFuseCs;
-    for (int u = cid; u < nunits; u += nclusters) {
+    __shared__ int32_t rexp[FC::kRows];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lrow = lane / FC::kLanesPerRow, kq = lane % FC::kLanesPerRow;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const int4 un = units[u];
         const DCrtFamily F = fams[un.x];
-        if (threadIdx.x < 8) rexp[threadIdx.x] = kNoExp;
+        __syncthreads();                                       // the previous unit's readers of rexp are done
+        if (threadIdx.x < FC::kRows) rexp[threadIdx.x] = kNoExp;
         __syncthreads();
-        // this CTA's share of the family's k tiles
-        const int t0 = (int)((int64_t)crank * F.ntiles / kFuseCs);
-        const int t1 = (int)((int64_t)(crank + 1) * F.ntiles / kFuseCs);
         const int r = un.y + lrow;
         const bool rvalid = lrow < un.z;
         // pass 1: row maxima, panel by panel (a lane keeps one row: a running
         // maximum over its tiles, reduced once)
         double mx = 0.0;
-        for (int q = F.p_begin; q < F.p_end; q++) {
-            const int qa = famt[q], qb = q + 1 < F.p_end ? famt[q + 1] : F.ntiles;
-            const int lo = max(qa, t0), hi = min(qb, t1);
-            if (lo >= hi || !rvalid) continue;
-            const DCrtPanel &P = panels[famp[q]];
-            const double *row = (P.src ? B : A) + P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
+        if (rvalid) {
+            for (int q = F.p_begin; q < F.p_end; q++) {
+                const DCrtPanel &P = panels[famp[q]];
+                const double *row = (P.src ? B : A) + P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
+                const int nt = (P.K + FC::kTileK - 1) / FC::kTileK;
 #pragma unroll 4
-            for (int t = lo + warp; t < hi; t += kFuseWarps) {
-                const int k0 = (t - qa) * 16 + kq * 4;
+                for (int t = warp; t < nt; t += FC::kWarps) {
+                    const int k0 = t * FC::kTileK + kq * 4;
 #pragma unroll
-                for (int j = 0; j < 4; j++)
-                    if (k0 + j < P.K) mx = fmax(mx, fabs(row[k0 + j]));
+                    for (int j = 0; j < 4; j++)
+                        if (k0 + j < P.K) mx = fmax(mx, fabs(row[k0 + j]));
+                }
             }
         }
-        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
-        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+#pragma unroll
+        for (int o = 1; o < FC::kLanesPerRow; o <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         if (rvalid && kq == 0 && mx > 0.0) {
             int e;
             frexp(mx, &e);                                     // mx = f * 2^e, f in [0.5, 1)
             atomicMax(&rexp[lrow], e);
         }
-        cluster.sync();                                        // every CTA's maxima are complete
-        if (threadIdx.x < 8) {
-            int m = kNoExp;
-            for (int c = 0; c < kFuseCs; c++) m = max(m, cluster.map_shared_rank(rexp, c)[threadIdx.x]);
-            rfin[threadIdx.x] = m;
-        }
-        cluster.sync();                                        // the peers have read rexp; rfin is visible
-        if (crank == 0 && threadIdx.x < un.z) {
+        __syncthreads();
+        if (threadIdx.x < un.z) {
             const DCrtPanel &P0 = panels[famp[F.p_begin]];
             int32_t *tab = P0.side == 0 ? ex : ey;
-            tab[gidx[P0.g_off + un.y + threadIdx.x]] = rfin[threadIdx.x];
+            tab[gidx[P0.g_off + un.y + threadIdx.x]] = rexp[threadIdx.x];
         }
+        if (!rvalid) continue;
         // pass 2: residues (the reads hit L2)
-        const int e = rvalid ? rfin[lrow] : kNoExp;
+        const int e = rexp[lrow];
         const int sh = e > kNoExp ? cp.P - e : 0;
         const double s1 = ldexp(1.0, sh / 2), s2 = ldexp(1.0, sh - sh / 2);   // 2^(P - e), two finite factors
-        const bool live = rvalid && e > kNoExp;
+        const bool live = e > kNoExp;
         for (int q = F.p_begin; q < F.p_end; q++) {
-            const int qa = famt[q], qb = q + 1 < F.p_end ? famt[q + 1] : F.ntiles;
-            const int lo = max(qa, t0), hi = min(qb, t1);
-            if (lo >= hi || !rvalid) continue;
             const DCrtPanel &P = panels[famp[q]];
             const double *row = (P.src ? B : A) + P.src_off + mixed_offset(r, P.nr, P.rext, P.rstr);
             const double coef = (double)P.coef;
             const uint32_t icoef = (uint32_t)P.coef;
             const int nkb = P.K_pad / kKB;
-            const int64_t lstride = (int64_t)P.tr * kKB;
+            const int64_t lstride = (int64_t)nkb * P.tr * kKB;  // the same k block of the next modulus
             uint8_t *pbase = res + P.res_off;
-            for (int t = lo + warp; t < hi; t += kFuseWarps) {
-                const int k0 = (t - qa) * 16 + kq * 4;
+            const int nt = (P.wk + FC::kTileK - 1) / FC::kTileK;
+            for (int t = warp; t < nt; t += FC::kWarps) {
+                const int k0 = t * FC::kTileK + kq * 4;
                 if (k0 >= P.wk) continue;
                 double x[4];
 #pragma unroll
@@ -561,6 +559,7 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 
 // ---------------------------------------------------------------- modular products
 
+template<int KB>
 __global__ void __launch_bounds__(kGemmThreads, 1)
 crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict__ res,
                 const DCrtTask *__restrict__ tasks, const DCrtItem *__restrict__ items, int32_t nitems,
@@ -610,18 +609,18 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                         const int64_t xt = (int64_t)nkb * L * kXTile;          // one M tile's images
                         const uint8_t *ga = res + t.xres + (int64_t)(item.x0 / kXRows) * xt;
                         const uint8_t *gb = res + t.yres + (int64_t)(item.y0 / item.nt) * nkb * L * ybytes;
-                        for (int kb = 0; kb < nkb; kb += kKbPerStage) {
+                        for (int kb = 0; kb < nkb; kb += KB) {
                             if (!mbar_wait(&empty_bar[st], ph ^ 1, &abort_s, wait_ns)) { ok = false; break; }
-                            const int nsub = min(kKbPerStage, nkb - kb);
+                            const int nsub = min(KB, nkb - kb);
                             const uint32_t fb = smem_u32(&full_bar[st]);
                             mbar_expect_tx(&full_bar[st], (uint32_t)nsub * ((uint32_t)(item.nx * kXTile) + ybytes));
-                            for (int j = 0; j < nsub; j++) {
-                                const uint32_t sa = smem0 + st * kStageBytes + j * kSubBytes;
-                                const int64_t img = (int64_t)(kb + j) * L + l;
-                                bulk_load(sa, ga + img * kXTile, kXTile, fb);
-                                if (item.nx == 2) bulk_load(sa + kXTile, ga + xt + img * kXTile, kXTile, fb);
-                                bulk_load(sa + 2 * kXTile, gb + img * ybytes, ybytes, fb);
-                            }
+                            // the stage's k blocks of modulus l: one copy per tile
+                            const uint32_t sa = smem0 + st * (KB * kSubBytes);
+                            const int64_t img = (int64_t)l * nkb + kb;
+                            bulk_load(sa, ga + img * kXTile, (uint32_t)nsub * kXTile, fb);
+                            if (item.nx == 2)
+                                bulk_load(sa + KB * kXTile, ga + xt + img * kXTile, (uint32_t)nsub * kXTile, fb);
+                            bulk_load(sa + 2 * KB * kXTile, gb + img * ybytes, (uint32_t)nsub * ybytes, fb);
                             armed[st] = (int)ph;
                             if (++st == stages) { st = 0; ph ^= 1; }
                         }
@@ -664,15 +663,19 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
                     uint32_t acc = 0;
                     for (int ti = item.t_begin; ti < item.t_end && ok; ti++) {
                         const int nkb = tasks[ti].nkb;
-                        for (int kb = 0; kb < nkb; kb += kKbPerStage) {
+                        for (int kb = 0; kb < nkb; kb += KB) {
                             if (!mbar_wait(&full_bar[st], ph, &abort_s, wait_ns)) { ok = false; break; }
                             tc_fence_after();
-                            const int nsub = min(kKbPerStage, nkb - kb);
+                            const int nsub = min(KB, nkb - kb);
+                            // stage layout: [first M tile's k blocks][second's][N tile's]
+                            const uint32_t sbase = smem0 + st * (KB * kSubBytes);
+                            const uint32_t ybytes = (uint32_t)item.nt * kKB;
                             for (int j = 0; j < nsub; j++) {
-                                const uint32_t a0 = smem0 + st * kStageBytes + j * kSubBytes;
-                                const uint64_t db = smem_desc_kmajor(a0 + 2 * kXTile);
+                                const uint32_t a0 = sbase + j * kXTile;
+                                const uint64_t db = smem_desc_kmajor(sbase + 2 * KB * kXTile + j * ybytes);
                                 umma_i8(d0, smem_desc_kmajor(a0), db, idesc, acc);
-                                if (item.nx == 2) umma_i8(tmem + kMaxNt, smem_desc_kmajor(a0 + kXTile), db, idesc, acc);
+                                if (item.nx == 2)
+                                    umma_i8(tmem + kMaxNt, smem_desc_kmajor(a0 + KB * kXTile), db, idesc, acc);
                                 acc = 1;
                             }
                             umma_commit(&empty_bar[st]);
@@ -907,23 +910,46 @@ cudaError_t launch_crt_fill(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, cu
     return cudaGetLastError();
 }
 
-cudaError_t launch_crt_fused(const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
+template<int L, class FC>
+cudaError_t launch_fused_l(const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
+                           const int32_t *famt, const int4 *units, int32_t nunits, const double *a,
+                           const double *b, const int32_t *gidx, int32_t *ex, int32_t *ey, uint8_t *res,
+                           const CrtParams &cp, cudaStream_t s) {
+    const int maxg = FC::kCtasPerSm * num_sms();
+    const int grid = nunits < maxg ? nunits : maxg;
+    crt_fused_kernel<L, FC><<<grid, FC::kThreads, 0, s>>>(panels, fams, famp, famt, units, nunits, a, b, gidx, ex,
+                                                          ey, res, cp);
+    return cudaGetLastError();
+}
+
+template<class FC>
+cudaError_t launch_fused_cfg(const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
                              const int32_t *famt, const int4 *units, int32_t nunits, const double *a,
                              const double *b, const int32_t *gidx, int32_t *ex, int32_t *ey, uint8_t *res,
                              const CrtParams &cp, cudaStream_t s) {
-    if (nunits <= 0) return cudaSuccess;
-    // kFuseCtasPerSm CTAs per SM: what the resident clusters read in pass 1
-    // (8 rows of a family each) must still be in L2 for pass 2
-    const int maxc = kFuseCtasPerSm * num_sms() / kFuseCs;
-    const int nclusters = nunits < maxc ? nunits : maxc;
-    const int grid = kFuseCs * (nclusters > 0 ? nclusters : 1);
     switch (cp.L) {
-#define CASE_L(n) case n: crt_fused_kernel<n><<<grid, kFuseThreads, 0, s>>>(panels, fams, famp, famt, units, nunits, a, b, gidx, ex, ey, res, cp); break;
+#define CASE_L(n) case n: return launch_fused_l<n, FC>(panels, fams, famp, famt, units, nunits, a, b, gidx, ex, ey, res, cp, s);
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
 #undef CASE_L
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
+}
+
+int crt_fuse_rows(int shape) { return shape == 1 || shape == 2 ? 2 : 0; }
+
+cudaError_t launch_crt_fused(int shape, const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
+                             const int32_t *famt, const int4 *units, int32_t nunits, const double *a,
+                             const double *b, const int32_t *gidx, int32_t *ex, int32_t *ey, uint8_t *res,
+                             const CrtParams &cp, cudaStream_t s) {
+    if (nunits <= 0) return cudaSuccess;
+    // 1: 2 rows, 512 threads, 2 CTAs/SM; 2: 2 rows, 256 threads, 4/SM.
+    // (1-row units, whose residue stores fill half sectors, ran 3.5x slower
+    // than these; 4-row units with 2 CTAs/SM 20 % slower.)
+    switch (shape) {
+    case 1: return launch_fused_cfg<FuseCfg<2, 512, 2>>(panels, fams, famp, famt, units, nunits, a, b, gidx, ex, ey, res, cp, s);
+    case 2: return launch_fused_cfg<FuseCfg<2, 256, 4>>(panels, fams, famp, famt, units, nunits, a, b, gidx, ex, ey, res, cp, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int32_t nunits,
@@ -940,19 +966,34 @@ cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int3
     return cudaGetLastError();
 }
 
-cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
-                            const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp,
-                            int32_t *err, uint64_t wait_ns, cudaStream_t s) {
-    if (nitems <= 0) return cudaSuccess;
-    int stages = (200 * 1024) / kStageBytes;
+template<int KB>
+cudaError_t launch_gemm_kb(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
+                           const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp,
+                           int32_t *err, uint64_t wait_ns, cudaStream_t s) {
+    constexpr int stage_bytes = KB * kSubBytes;
+    int stages = (200 * 1024) / stage_bytes;
     if (stages > kMaxStages) stages = kMaxStages;
-    const size_t smem = (size_t)stages * kStageBytes + 1024;
-    cudaError_t e = cudaFuncSetAttribute(crt_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = (size_t)stages * stage_bytes + 1024;
+    cudaError_t e = cudaFuncSetAttribute(crt_gemm_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = nitems < num_sms() ? nitems : num_sms();
-    crt_gemm_kernel<<<grid, kGemmThreads, smem, s>>>(panels, res, tasks, items, nitems, out, cp, stages, err,
-                                                      wait_ns);
+    crt_gemm_kernel<KB><<<grid, kGemmThreads, smem, s>>>(panels, res, tasks, items, nitems, out, cp, stages, err,
+                                                         wait_ns);
     return cudaGetLastError();
+}
+
+cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
+                            const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp,
+                            int32_t *err, uint64_t wait_ns, int32_t stage_kb, cudaStream_t s) {
+    if (nitems <= 0) return cudaSuccess;
+    // k blocks per pipeline stage: 2 (6 stages of 32 KB), 3 (4 x 48 KB), 4
+    // (3 x 64 KB, the default), 6 (2 x 96 KB)
+    switch (stage_kb) {
+    case 2: return launch_gemm_kb<2>(panels, res, tasks, items, nitems, out, cp, err, wait_ns, s);
+    case 3: return launch_gemm_kb<3>(panels, res, tasks, items, nitems, out, cp, err, wait_ns, s);
+    case 6: return launch_gemm_kb<6>(panels, res, tasks, items, nitems, out, cp, err, wait_ns, s);
+    default: return launch_gemm_kb<4>(panels, res, tasks, items, nitems, out, cp, err, wait_ns, s);
+    }
 }
 
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,

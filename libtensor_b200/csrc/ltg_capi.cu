@@ -208,12 +208,13 @@ struct ltg_plan {
     int forced_tile = -1;         // >= 0: every C block uses this tile shape
     int split_k = 0;              // plain DMMA k chunks per tile: 0 automatic, 1 never, 2-4 always
     bool group_products = true;   // modular mode: small C blocks grouped into larger products
-    bool fused_split = true;      // modular mode: row families split in one read of the operand
+    int fused_split = 0;          // modular mode: row families split in one read (kernel shape 1, 2; 0 off)
     // caller-built task list (ltg_plan_contract2_upload): plain FP64 only,
     // coefficients absolute, no schedule of its own
     bool external = false;
     std::vector<GemmTask> ext_tasks;
     int crt_rows = 0;             // modular mode: work-item rows (128, 256; 0 default)
+    int crt_stage_kb = 4;         // modular mode: k blocks per pipeline stage of the products kernel
     std::map<std::pair<int64_t, int64_t>, int> tile_override;   // autotuned (M, N) -> shape
     // the schedule (shared with the process-wide schedule cache)
     std::shared_ptr<const ContractPlan> planp = std::make_shared<const ContractPlan>();
@@ -1692,8 +1693,9 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
             F.ntiles = tiles;
             const int32_t fid = (int32_t)fams.size();
             fams.push_back(F);
-            for (int32_t r0 = 0; r0 < F.rows; r0 += 8)
-                funits.push_back(make_int4(fid, r0, std::min<int32_t>(8, F.rows - r0), 0));
+            const int32_t fr = crt_fuse_rows(pl->fused_split);
+            for (int32_t r0 = 0; r0 < F.rows; r0 += fr)
+                funits.push_back(make_int4(fid, r0, std::min<int32_t>(fr, F.rows - r0), 0));
         }
         famt.push_back(0);      // famt[p_end] of the last family is read as a bound only when q + 1 < p_end
     }
@@ -2889,7 +2891,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             const double *pa = plan->a->arena.as<double>(), *pb = plan->b->arena.as<double>();
             TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
             LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), s));
-            LTG_CUDA(launch_crt_fused(cx->panels.as<DCrtPanel>(), cx->fams.as<DCrtFamily>(), cx->famp.as<int32_t>(),
+            LTG_CUDA(launch_crt_fused(plan->fused_split, cx->panels.as<DCrtPanel>(), cx->fams.as<DCrtFamily>(), cx->famp.as<int32_t>(),
                                       cx->famt.as<int32_t>(), cx->funits.as<int4>(), cx->nfunits, pa, pb,
                                       cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
                                       cx->res.as<uint8_t>(), cx->cp, s));
@@ -2903,7 +2905,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
             LTG_CUDA(launch_crt_gemm(cx->panels.as<DCrtPanel>(), cx->res.as<uint8_t>(), cx->tasks.as<DCrtTask>(),
                                      cx->items.as<DCrtItem>(), cx->nitems, cx->out.as<uint8_t>(), cx->cp,
-                                     ctx->wait_err.as<int32_t>(), ctx->wait_ns, s));
+                                     ctx->wait_err.as<int32_t>(), ctx->wait_ns, plan->crt_stage_kb, s));
             t_gemm.done();
             TimedLaunch t_comb(ctx, LTG_KERNEL_OZ_COMBINE);
             LTG_CUDA(launch_crt_combine(cx->panels.as<DCrtPanel>(), cx->items.as<DCrtItem>(), cx->nitems,
@@ -3066,8 +3068,18 @@ int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable) {
     return guard([&] {
         if (!plan) throw error(kErrBadArg, "null plan");
         if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
-        plan->fused_split = enable != 0;
+        if (enable < 0 || enable > 2) throw error(kErrBadArg, "one-read split shape must be 0 (off), 1 or 2");
+        plan->fused_split = enable;
         plan->crt.clear();
+    });
+}
+
+int ltg_contract2_set_crt_stage(ltg_plan *plan, int32_t kblocks) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (kblocks != 2 && kblocks != 3 && kblocks != 4 && kblocks != 6)
+            throw error(kErrBadArg, "k blocks per stage must be 2, 3, 4 or 6");
+        plan->crt_stage_kb = kblocks;
     });
 }
 

@@ -98,7 +98,7 @@ constexpr int kCrtMaxModuli = 16;
 // One operand panel of the modular contraction: the matricised view (rows x K)
 // of a canonical block, with the pair's integer coefficient folded in, scaled
 // row by row to integers and stored as its residues modulo each modulus, in
-// shared-memory tile images (per tile of tr rows, 32-byte k block, modulus).
+// shared-memory tile images (per tile of tr rows, modulus, 32-byte k block).
 struct DCrtPanel {
     int64_t src_off;              // FP64 source block offset (elements)
     int64_t res_off;              // byte offset of the tile images
@@ -324,9 +324,11 @@ cudaError_t launch_crt_exponents(const DCrtPanel *panels, const int4 *units, int
     int32_t *ey, cudaStream_t s);
 // Sets both exponent tables to "no element" (before the passes below).
 cudaError_t launch_crt_fill(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, cudaStream_t s);
-// Exponents and residues of the row families in one HBM read (units: 8 rows
-// of one family, {family, first row, rows, 0}); ex/ey hold kNoExp before.
-cudaError_t launch_crt_fused(const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
+// Exponents and residues of the row families in one HBM read, in kernel
+// shape 1-4 (units: crt_fuse_rows(shape) rows of one family, {family, first
+// row, rows, 0}); ex/ey hold kNoExp before.
+int crt_fuse_rows(int shape);
+cudaError_t launch_crt_fused(int shape, const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
     const int32_t *famt, const int4 *units, int32_t nunits, const double *a, const double *b,
     const int32_t *gidx, int32_t *ex, int32_t *ey, uint8_t *res, const CrtParams &cp, cudaStream_t s);
 cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int32_t nunits,
@@ -334,7 +336,7 @@ cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int3
     uint8_t *res, const CrtParams &cp, cudaStream_t s);
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
     const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp, int32_t *err,
-    uint64_t wait_ns, cudaStream_t s);
+    uint64_t wait_ns, int32_t stage_kb, cudaStream_t s);
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
     const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab, const DCrtCell *cells,
     const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey, double *c,

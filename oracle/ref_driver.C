@@ -209,13 +209,22 @@ bt_h<N> *make_bt(spec_reader &r) {
         std::string id = ensure_xor_table(nirrep);
         se_label<N, double> sl(bidims, id);
         block_labeling<N> &bl = sl.get_labeling();
+        std::vector< std::vector<int64_t> > labs(N);
         for (size_t d = 0; d < N; d++) {
             int64_t nb = r.next();
-            mask<N> m; m[d] = true;
-            for (int64_t b = 0; b < nb; b++) {
-                int64_t lab = r.next();
-                if (lab >= 0) bl.assign(m, (size_t)b, (size_t)lab);
-            }
+            for (int64_t b = 0; b < nb; b++) labs[d].push_back(r.next());
+        }
+        // dims with the same labels are labelled together (one mask), so that
+        // they keep one dimension type in the labeling (symmetrizers over
+        // them require it, so_symmetrize_se_label_impl.h:53-62)
+        std::vector<bool> done(N, false);
+        for (size_t d = 0; d < N; d++) {
+            if (done[d]) continue;
+            mask<N> m;
+            for (size_t e2 = d; e2 < N; e2++)
+                if (!done[e2] && labs[e2] == labs[d] && bidims[e2] == bidims[d]) { m[e2] = true; done[e2] = true; }
+            for (size_t b = 0; b < labs[d].size(); b++)
+                if (labs[d][b] >= 0) bl.assign(m, b, (size_t)labs[d][b]);
         }
         int64_t nintr = r.next();
         product_table_i::label_set_t ls;
