@@ -392,11 +392,12 @@ class block_tensor {
     block_tensor &operator=(const block_tensor &) = delete;
 public:
     explicit block_tensor(const block_index_space<N> &bis) : m_bis(bis) { }
-    ~block_tensor() { if (m_bt) ltg_bt_destroy(m_bt); }
+    virtual ~block_tensor() { if (m_bt) ltg_bt_destroy(m_bt); }
     const block_index_space<N> &get_bis() const { return m_bis; }
     bool is_bound() const { return m_bt != nullptr; }
-    // The device tensor, built from the index space and symmetry on first use.
-    ltg_bt *handle() {
+    // The device tensor, built from the index space and symmetry on first use
+    // (a direct block tensor first computes its operation's result).
+    virtual ltg_bt *handle() {
         if (m_bt) return m_bt;
         std::vector<int64_t> dims(N), splits;
         std::vector<int32_t> nsplit(N), perm, labels, intr;
@@ -1463,6 +1464,79 @@ public:
         : b200::symmetrizer<N>(nullptr, &op, 4, b200::idx_vec({i1, i2, i3, i4}), symm) { }
     btod_symmetrize4(block_tensor<N, double> &bta, size_t i1, size_t i2, size_t i3, size_t i4, bool symm)
         : b200::symmetrizer<N>(&bta, nullptr, 4, b200::idx_vec({i1, i2, i3, i4}), symm) { }
+};
+
+// Result block index space of a contraction: A's uncontracted dims, then
+// B's, permuted by the contraction's permc.
+template<size_t N, size_t M, size_t K>
+block_index_space<N + M> contraction_space(const contraction2<N, M, K> &contr,
+                                           const block_index_space<N + K> &bisa,
+                                           const block_index_space<M + K> &bisb) {
+    std::vector<bool> ca(N + K, false), cb(M + K, false);
+    for (const std::pair<size_t, size_t> &p : contr.get_pairs()) {
+        ca[p.first] = true;
+        cb[p.second] = true;
+    }
+    std::vector<expr_detail::dim_space> nat;
+    for (size_t i = 0; i < N + K; i++) if (!ca[i]) nat.push_back(expr_detail::dim_of(bisa, i));
+    for (size_t i = 0; i < M + K; i++) if (!cb[i]) nat.push_back(expr_detail::dim_of(bisb, i));
+    const std::vector<int32_t> pc = contr.get_permc().to_vector();
+    std::vector<expr_detail::dim_space> d(N + M);
+    for (size_t i = 0; i < N + M; i++) d[i] = nat[(size_t)pc[i]];
+    return expr_detail::make_space<N + M>(d);
+}
+
+// btod_contract3 (libtensor/block_tensor/btod_contract3.h:36): D = kd (AB) C
+// with AB = contr1(A, B) and D = contr2(AB, C).  The intermediate AB is one
+// device tensor the operation keeps (it is formed whole: the reference forms
+// it in batches of B's blocks to bound host memory, which 180 GB of HBM
+// makes unnecessary at these sizes); the second contraction is built on the
+// first perform, when AB's non-zero blocks are known, and reused.
+template<size_t N1, size_t N2, size_t N3, size_t K1, size_t K2>
+class btod_contract3 : public additive_bto<N1 + N2 + N3> {
+    static constexpr size_t NAB = N1 + N2 + K2;
+    contraction2<N1 + N2, N3, K2> m_contr2;
+    btod_contract2<N1, N2 + K2, K1> m_op1;
+    block_tensor<NAB, double> m_ab;
+    block_tensor<N3 + K2, double> &m_c;
+    double m_kd;
+    std::unique_ptr<btod_contract2<N1 + N2, N3, K2> > m_op2;
+    btod_contract2<N1 + N2, N3, K2> &second() {
+        m_op1.perform(m_ab);
+        if (!m_op2) m_op2.reset(new btod_contract2<N1 + N2, N3, K2>(m_contr2, m_ab, 1.0, m_c, 1.0, m_kd));
+        return *m_op2;
+    }
+public:
+    btod_contract3(const contraction2<N1, N2 + K2, K1> &contr1, const contraction2<N1 + N2, N3, K2> &contr2,
+                   block_tensor<N1 + K1, double> &bta, block_tensor<N2 + K1 + K2, double> &btb,
+                   block_tensor<N3 + K2, double> &btc, double kd = 1.0)
+        : m_contr2(contr2), m_op1(contr1, bta, btb),
+          m_ab(contraction_space(contr1, bta.get_bis(), btb.get_bis())), m_c(btc), m_kd(kd) { }
+    void perform(block_tensor<N1 + N2 + N3, double> &btd) override { second().perform(btd); }
+    void perform(block_tensor<N1 + N2 + N3, double> &btd, double d) override { second().perform(btd, d); }
+};
+
+// direct_block_tensor (libtensor/block_tensor/direct_block_tensor.h:22): a
+// block tensor holding an operation's result, computed when an operation
+// first reads it, so that it needs no separate perform.  The whole result is
+// formed on the device at that first read (the reference forms each block
+// when it is requested); refresh() forms it again at the next read, after the
+// operation's inputs changed.
+template<size_t N>
+class direct_block_tensor : public block_tensor<N, double> {
+    additive_bto<N> &m_op;
+    bool m_ready = false;
+public:
+    direct_block_tensor(additive_bto<N> &op, const block_index_space<N> &bis)
+        : block_tensor<N, double>(bis), m_op(op) { }
+    ltg_bt *handle() override {
+        if (!m_ready) {
+            m_ready = true;                  // the operation's own handle() calls land below
+            m_op.perform(*this);
+        }
+        return block_tensor<N, double>::handle();
+    }
+    void refresh() { m_ready = false; }
 };
 
 }  // namespace libtensor

@@ -318,8 +318,9 @@ class btod_contract2:
         check(lib().ltg_contract2_set_split_k(self.h, k))
 
     def set_fused_split(self, shape: int):
-        """Modular mode: one-read split of row families in kernel shape 1 or 2,
-        or 0 (default) for the exponent and residue passes."""
+        """Modular mode: one-read split of row families in kernel shape 1-4
+        (3, 4: rows staged in shared memory by bulk copies), or 0 (default)
+        for the exponent and residue passes."""
         check(lib().ltg_contract2_set_fused_split(self.h, int(shape)))
 
     def set_crt_stage(self, kblocks: int):
@@ -494,4 +495,125 @@ class btod_symmetrize:
     def perform(self, b: block_tensor, d: Optional[float] = None):
         check(lib().ltg_symmetrize(self.a.h, self.c, self.nidx, self.idx, 1 if self.symm else 0, b.h,
                                    0 if d is None else 1, 0.0 if d is None else d))
+
+
+class btod_contract3:
+    """btod_contract3<N1,N2,N3,K1,K2>(contr1, contr2, A, B, C, kd)
+    (libtensor/block_tensor/btod_contract3.h:36): D = kd * contr2(contr1(A, B), C),
+    the intermediate AB formed in batches of B's non-zero canonical blocks,
+    AB = sum_i A B_i (gen_bto_contract3_impl.h:51-260), each batch's
+    intermediate kept on the device and contracted with C into D.  One batch
+    (the default) forms the whole intermediate once; more batches bound its
+    size by contracting A with a copy of B holding only that batch's blocks.
+    The operations (and their schedules) are built on the first perform and
+    reused."""
+
+    def __init__(self, contr1: contraction2, contr2: contraction2, a: block_tensor, b: block_tensor,
+                 c: block_tensor, kd: float = 1.0, batches: int = 1):
+        if batches < 1:
+            raise ValueError("batches must be >= 1")
+        self.contr1, self.contr2 = contr1, contr2
+        self.a, self.b, self.c, self.kd = a, b, c, kd
+        self.batches = batches
+        self._stages = None           # [(B_i, op1_i, AB, op2_i)]
+
+    def _build(self):
+        ctx = self.a.ctx
+        nz = set(self.b.nonzero())
+        slots = [s for s in range(self.b.nblocks) if int(self.b.abs_idx[s]) in nz]
+        nb = max(1, min(self.batches, len(slots)))
+        # batches of about equal size, canonical blocks in order
+        sizes = [int(self.b.sizes[s]) for s in slots]
+        total, acc, cut = sum(sizes), 0, [0]
+        for i, x in enumerate(sizes):
+            acc += x
+            if len(cut) < nb and acc >= total * len(cut) / nb:
+                cut.append(i + 1)
+        cut.append(len(slots))
+        self._stages = []
+        ab = None
+        for i in range(len(cut) - 1):
+            if nb == 1:
+                bi = self.b
+            else:
+                bi = self.b.permuted(list(range(self.b.order)))
+                btod_copy(self.b).perform(bi)
+                keep = set(slots[cut[i]:cut[i + 1]])
+                for s in range(bi.nblocks):
+                    if s not in keep:
+                        bi.zero_block(bi.block_index(bi.abs_idx[s]))
+            op1 = btod_contract2(self.contr1, self.a, bi)
+            if ab is None:
+                ab = op1.make_result()
+            self._stages.append([bi, op1, ab, None])
+
+    def perform(self, d: block_tensor, dd: Optional[float] = None, mode: int = MODE_PLAIN_FP64,
+                nslices: int = 0):
+        """D = kd (AB) C (assign), or D += dd kd (AB) C."""
+        if self._stages is None:
+            self._build()
+        for i, st in enumerate(self._stages):
+            bi, op1, ab, op2 = st
+            op1.perform(ab, mode=mode, nslices=nslices)
+            if op2 is None:
+                # the second contraction's schedule follows AB's non-zero blocks
+                op2 = st[3] = btod_contract2(self.contr2, ab, self.c, kc=self.kd)
+            if i == 0 and dd is None:
+                op2.perform(d, mode=mode, nslices=nslices)
+            else:
+                op2.perform(d, 1.0 if dd is None else dd, mode=mode, nslices=nslices)
+
+    def make_result(self) -> block_tensor:
+        if self._stages is None:
+            self._build()
+        # the result space does not depend on AB's non-zero blocks: a throwaway
+        # operation gives it (the stages' own second operations are built after
+        # AB is formed, so that their schedules see its blocks)
+        tmp = btod_contract2(self.contr2, self._stages[0][2], self.c, kc=self.kd)
+        try:
+            return tmp.make_result()
+        finally:
+            tmp.close()
+
+    def close(self):
+        for bi, op1, ab, op2 in self._stages or []:
+            op1.close()
+            if op2 is not None:
+                op2.close()
+            if bi is not self.b:
+                bi.close()
+        if self._stages:
+            self._stages[0][2].close()
+        self._stages = None
+
+
+class direct_block_tensor(block_tensor):
+    """A block tensor holding an operation's result, computed when it is
+    first read (libtensor/block_tensor/direct_block_tensor.h:22): as an
+    operand of another operation it needs no separate perform.  The whole
+    result is formed on the device at the first read (the reference forms
+    each block when it is requested); refresh() forms it again at the next
+    read, after the operation's inputs changed."""
+
+    def __init__(self, op):
+        t = op.make_result()
+        self._op, self._t, self._ready = op, t, False
+        self.ctx, self.spec = t.ctx, t.spec
+        self.order, self.nblocks, self.nelems = t.order, t.nblocks, t.nelems
+        self.abs_idx, self.offsets, self.sizes, self.bidims = t.abs_idx, t.offsets, t.sizes, t.bidims
+
+    @property
+    def h(self):
+        if not self._ready:
+            self._ready = True
+            self._op.perform(self._t)
+        return self._t.h
+
+    def refresh(self):
+        self._ready = False
+
+    def close(self):
+        if self._t is not None:
+            self._t.close()
+            self._t = None
 

@@ -227,6 +227,24 @@ int main(int argc, char **argv) {
         asg.run();
         b200::synchronize();
         const double asg_diff = max_diff(qg, ql, 1.0);
+        // a three-tensor contraction and a direct block tensor as an operand,
+        // against the two contractions written out:
+        //   D(i,j,k,l) = 1/4 sum_ab [sum_cd t(i,j,c,d) v(a,b,c,d)] t(k,l,a,b)
+        contraction2<2, 2, 2> cA, cB;
+        cA.contract(2, 2);
+        cA.contract(3, 3);
+        cB.contract(2, 2);
+        cB.contract(3, 3);
+        block_index_space<4> bis_d = make_bis(10, 10, occ, occ);
+        block_tensor<4, double> abx(bis_r), dx(bis_d), d3(bis_d), d4(bis_d);
+        btod_contract2<2, 2, 2>(cA, t, v).perform(abx);
+        btod_contract2<2, 2, 2>(cB, abx, 1.0, t, 1.0, 0.25).perform(dx);
+        btod_contract3<2, 0, 2, 2, 2> c3op(cA, cB, t, v, t, 0.25);
+        c3op.perform(d3);
+        btod_contract2<2, 2, 2> first(cA, t, v);
+        direct_block_tensor<4> dab(first, bis_r);
+        btod_contract2<2, 2, 2>(cB, dab, 1.0, t, 1.0, 0.25).perform(d4);
+        const double c3_diff = std::max(max_diff(d3, dx, 1.0), max_diff(d4, dx, 1.0));
         // one CUDA graph of the contraction, the permuted copy and the add:
         // run once, captured, inputs overwritten, replayed
         block_tensor<4, double> r2(bis_r), tp2(bis_t), s2(bis_t);
@@ -254,7 +272,7 @@ int main(int argc, char **argv) {
                                 max_diff(gse, gs, 1.0), graph_diff,
                                 max_diff(nl, ne, 1.0), max_diff(ql, qe, 1.0), max_diff(wl, we, 1.0),
                                 max_diff(r, hr, 0.5), std::fabs(dl_sum - dot_tt - dot_ts), asg_diff,
-                                (double)asg.operations()};
+                                (double)asg.operations(), c3_diff};
 
         // the contraction's non-zero blocks in index order, then the dot products
         FILE *f = std::fopen(argv[2], "wb");

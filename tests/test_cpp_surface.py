@@ -81,3 +81,4 @@ def test_surface_compute_matches_golden(exe, tmp_path):
     assert d[14] <= 1e-13 * dot_tt
     assert d[15] == 0.0
     assert d[16] == 2                                   # the add into the intermediate, the contraction
+    assert d[17] == 0.0                                 # btod_contract3, direct_block_tensor = explicit ops
