@@ -81,6 +81,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-DMMA companion timing")
+    p.add_argument("--no-slices", action="store_true",
+                   help="skip the companion timing of the BF16 x7 and FP8 x8 slice modes")
     p.add_argument("--fused-split", type=int, default=0, choices=[0, 1, 2],
                    help="modular mode: one-read split of row families in kernel shape 1 or 2 (0: exponent and "
                         "residue passes)")
@@ -346,6 +348,28 @@ def ltg_arm(args):
         barrier()
         pms = max_over_ranks([p0.elapsed_time(p1) / args.steps], dev, world)[0]
         plain = {"value": replica_rate(flops, pms, world) / 1e12, "unit": "TFLOP/s", "ms_per_step": pms}
+    # slice split-precision companions (Ozaki BF16 / FP8 slices, FP32
+    # accumulation) on the same workload: throughput, and their results for
+    # the accuracy check against the reference
+    slices = None
+    if args.mode == "ozaki-crt" and not args.no_slices:
+        slices = {}
+        for sname, S in (("ozaki-bf16", 7), ("ozaki-fp8", 8)):
+            sm = MODES[sname]
+            for _ in range(3):
+                op.perform(C, mode=sm, nslices=S)
+            barrier()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for _ in range(args.steps):
+                op.perform(C, mode=sm, nslices=S)
+            s1.record(stream)
+            barrier()
+            sms = max_over_ranks([s0.elapsed_time(s1) / args.steps], dev, world)[0]
+            slices[sname] = {"value": replica_rate(flops, sms, world) / 1e12, "unit": "TFLOP/s", "slices": S,
+                             "ms_per_step": sms}
+            if rank == 0:
+                results[sname] = C.download()
     ms = max_over_ranks([ms], dev, world)[0]
     value = replica_rate(flops, ms, world) / 1e12
 
@@ -403,6 +427,8 @@ def ltg_arm(args):
     if plain:
         out["plain_fp64_dmma"] = plain
         out["split_vs_plain"] = value / plain["value"]
+    if slices:
+        out["slice_modes"] = slices
     if accuracy:
         out["accuracy"] = accuracy
     print(json.dumps(out))

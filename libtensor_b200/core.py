@@ -318,9 +318,8 @@ class btod_contract2:
         check(lib().ltg_contract2_set_split_k(self.h, k))
 
     def set_fused_split(self, shape: int):
-        """Modular mode: one-read split of row families in kernel shape 1-4
-        (3, 4: rows staged in shared memory by bulk copies), or 0 (default)
-        for the exponent and residue passes."""
+        """Modular mode: one-read split of row families in kernel shape 1 or 2,
+        or 0 (default) for the exponent and residue passes."""
         check(lib().ltg_contract2_set_fused_split(self.h, int(shape)))
 
     def set_crt_stage(self, kblocks: int):
