@@ -266,6 +266,17 @@ int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable);
  * faster (2.40 ms against 2.68 ms for shape 2, although the one-read form
  * moves 9.6 GB through HBM against 13.2).  No reference counterpart. */
 int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable);
+/* Modular mode: how the row exponents (the scale of each operand row) are
+ * found.  1 (default): rows of at least 1024 k words read one 32-element run
+ * in 16 for a bound one binade above the sampled maximum; the residue
+ * pass forms their exact maxima while it reads them, and redoes the rows whose
+ * bound was too small with the exact exponent -- so every row's integers stay
+ * within 2^P, at most one bit of the P-bit operands is given up, and the
+ * exponent pass reads about 1/16 of those operands.  0: an exponent pass
+ * over every element (exact maxima).  Both give results within the mode's
+ * error bound; their bits differ where the bound is a binade above the
+ * maximum.  No reference counterpart. */
+int ltg_contract2_set_crt_bound(ltg_plan *plan, int32_t sampled);
 /* Modular mode: rows of the products kernel's work items, 256 (two MMA
  * tiles sharing each operand tile of the other side; also 0, the default) or
  * 128 (one MMA tile; the epilogue of one modulus overlaps the products of the

@@ -95,6 +95,7 @@ _SIGS = {
     "ltg_contract2_set_split_k": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_set_grouping": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_set_fused_split": (C.c_int, [c_vp, C.c_int32]),
+    "ltg_contract2_set_crt_bound": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_set_crt_stage": (C.c_int, [c_vp, C.c_int32]),
     "ltg_contract2_group_info": (C.c_int, [c_vp, c_vp, c_i64p, c_i64p, c_dblp, c_dblp]),
     "ltg_contract2_set_crt_rows": (C.c_int, [c_vp, C.c_int32]),

@@ -322,6 +322,11 @@ class btod_contract2:
         or 0 (default) for the exponent and residue passes."""
         check(lib().ltg_contract2_set_fused_split(self.h, int(shape)))
 
+    def set_crt_bound(self, sampled: bool):
+        """Modular mode: row exponents from sampled bounds checked by the
+        residue pass (True, the default) or from an exact exponent pass."""
+        check(lib().ltg_contract2_set_crt_bound(self.h, 1 if sampled else 0))
+
     def set_crt_stage(self, kblocks: int):
         """Modular mode: k blocks per pipeline stage of the products kernel."""
         check(lib().ltg_contract2_set_crt_stage(self.h, kblocks))

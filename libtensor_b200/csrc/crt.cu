@@ -6,7 +6,11 @@
 //   1. exponents (crt_exp_kernel): for every operand row, the exponent of its
 //      largest magnitude, combined over all panels that feed the same global
 //      row of C (atomicMax into one table per side of C), so that every pair
-//      of a C block shares the row and column scaling;
+//      of a C block shares the row and column scaling.  Long rows may be
+//      sampled instead (one 32-element run in kSampleGroups, one binade of
+//      headroom): the residue pass then forms their exact maxima as it reads
+//      them, and rows whose sampled bound was too small are redone with the
+//      exact exponent (see crt_res_kernel);
 //   2. residues (crt_res_kernel): X = c_p * rint(x * 2^(P - e_row)) (the
 //      pair's integer coefficient c_p folded in on one side), stored as its
 //      balanced residues mod m_l (INT8) in shared-memory tile images;
@@ -149,9 +153,23 @@ constexpr int kSplitWarps = kSplitThreads / 32;
 constexpr int kKoffMax = 4096;                      // k offsets tabulated per unit
 constexpr int kUnitRowsMax = 256;                   // rows per unit (bound of the host's units)
 constexpr int kUnitRowMap = 0, kUnitTileMap = 1;    // thread mapping of a unit (units[].w)
+// Sampled exponents: rows of row-mapped units with at least kSampleMinK
+// k words read one 32-element run in kSampleGroups (the 8 threads of the
+// row one 4-element group each, so that a run is one 256-byte read) for
+// their bound.
+constexpr int kSampleMinK = 1024;
+constexpr int kSampleGroups = 16;
+__host__ __device__ __forceinline__ bool sampled_panel(const DCrtPanel &P, int unit_map) {
+    return unit_map == kUnitRowMap && P.wk >= kSampleMinK;
+}
 
 __global__ void crt_fill_kernel(int32_t *p, int32_t n, int32_t v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+// After the residue pass and its redo: the exponent each row's residues were
+// formed with, max(bound, exact).
+__global__ void crt_merge_kernel(int32_t *e, const int32_t *et, int32_t n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) e[i] = max(e[i], et[i]);
 }
 
 // k offset mode of a panel: 0 contiguous, 1 tabulated in koff, 2 computed.
@@ -168,7 +186,7 @@ __device__ __forceinline__ int64_t koffset(const DCrtPanel &P, int mode, const i
 __global__ void __launch_bounds__(kSplitThreads)
 crt_exp_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ units, int32_t nunits,
                const double *__restrict__ A, const double *__restrict__ B, const int32_t *__restrict__ gidx,
-               int32_t *ex, int32_t *ey) {
+               int32_t *ex, int32_t *ey, int32_t sample) {
     __shared__ int32_t koff[kKoffMax];
     __shared__ int32_t rexp[kUnitRowsMax];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lrow = lane >> 2, kq = lane & 3;
@@ -191,9 +209,13 @@ crt_exp_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
             const int r = un.y + lr;
             const bool valid = lr < un.z && r < P.rows;
             const double *row = src + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
+            // sampled: group c of every kSampleGroups-th run of 32 elements;
+            // else group c of every run
+            const bool smp = sample && sampled_panel(P, un.w);
+            const int step = smp ? 32 * kSampleGroups : 32, first = 4 * c;
             double mx = 0.0;
             if (valid)
-                for (int k0 = 4 * c; k0 < P.K; k0 += 32)
+                for (int k0 = first; k0 < P.K; k0 += step)
 #pragma unroll
                     for (int j = 0; j < 4; j++)
                         if (k0 + j < P.K) mx = fmax(mx, fabs(row[koffset(P, mode, koff, k0 + j)]));
@@ -203,7 +225,7 @@ crt_exp_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
             if (valid && c == 0 && mx > 0.0) {
                 int e;
                 frexp(mx, &e);
-                atomicMax(&tab[gidx[P.g_off + r]], e);
+                atomicMax(&tab[gidx[P.g_off + r]], smp ? e + 1 : e);   // one binade of headroom
             }
             continue;
         }
@@ -262,12 +284,18 @@ __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, ui
     return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
+// Sampled rows (sampled_panel): their residues are formed with the sampled
+// bound e (|x| < 2^e unless the sample missed the row's largest elements),
+// and the row's exact exponent goes to the side's second table (ext / eyt).
+// With redo set, only those rows run again, and only where the exact
+// exponent exceeds the bound: with the exact exponent, overwriting the
+// residues formed before (whose integers may have exceeded 2^P).
 template<int L>
-__global__ void __launch_bounds__(kSplitThreads)
+__global__ void __launch_bounds__(kSplitThreads, 4)
 crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ units, int32_t nunits,
                const double *__restrict__ A, const double *__restrict__ B, const int32_t *__restrict__ gidx,
-               const int32_t *__restrict__ ex, const int32_t *__restrict__ ey, uint8_t *__restrict__ res,
-               const CrtParams cp) {
+               const int32_t *__restrict__ ex, const int32_t *__restrict__ ey, int32_t *ext, int32_t *eyt,
+               int32_t sample, int32_t redo, uint8_t *__restrict__ res, const CrtParams cp) {
     __shared__ int32_t koff[kKoffMax];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lrow = lane >> 2, kq = lane & 3;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
@@ -279,6 +307,7 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
         if (shared) __syncthreads();
         const double *src = (P.src ? B : A) + P.src_off;
         const int32_t *tab = P.side == 0 ? ex : ey;
+        int32_t *tabt = P.side == 0 ? ext : eyt;
         uint8_t *base = res + P.res_off;
         const int TR = P.tr, nkb = P.K_pad / kKB;
         const double coef = (double)P.coef;
@@ -286,37 +315,65 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
         int cur = -1;
         const double *row = src;
         double s1 = 0.0, s2 = 0.0;
-        bool live = false;
-        // row r's offset and scaling, kept while the thread stays on it
-        auto set_row = [&](int r) {
+        bool live = false, rowok = false, fast = false, vec = false;
+        // row r's offset and scaling (exponent e_over, or the side table's),
+        // kept while the thread stays on it
+        auto set_row = [&](int r, int e_over) {
             cur = r;
             const bool valid = r < P.rows;
             row = src + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
-            const int e = valid ? tab[gidx[P.g_off + r]] : kNoExp;
+            const int e = !valid ? kNoExp : (e_over > kNoExp ? e_over : tab[gidx[P.g_off + r]]);
             // 2^(P - e) as two finite factors
             const int sh = e > kNoExp ? cp.P - e : 0;
             s1 = ldexp(1.0, sh / 2);
             s2 = ldexp(1.0, sh - sh / 2);
             live = valid && e > kNoExp;
+            rowok = valid;
+            vec = mode == 0 && ((uintptr_t)row & 15) == 0;
+            // one finite factor and no coefficient: one FMA forms the integer
+            fast = sh <= 1000 && P.coef == 1;
+            if (fast) { s1 = ldexp(1.0, sh); s2 = 1.0; }
         };
-        // elements k0..k0+3 of the current row (zero past K)
-        auto load4 = [&](int k0, double *x) {
+        // elements k0..k0+3 of the current row (zero past K, and zero for a
+        // row without elements unless any: a sampled row's exact maximum is
+        // formed from them, and a non-zero row whose bound said "no element"
+        // is redone)
+        auto load4_if = [&](int k0, double *x, bool any) {
+            const bool ok = any ? rowok : live;
+            if (ok && vec && k0 + 3 < P.K) {
+                // contiguous, 16-byte aligned row: two 16-byte loads
+                const double2 a = *reinterpret_cast<const double2 *>(row + k0);
+                const double2 b = *reinterpret_cast<const double2 *>(row + k0 + 2);
+                x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+                return;
+            }
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int k = k0 + j;
-                x[j] = (live && k < P.K) ? row[koffset(P, mode, koff, k)] : 0.0;
+                x[j] = (ok && k < P.K) ? row[koffset(P, mode, koff, k)] : 0.0;
             }
         };
-        // residues of k0..k0+3 of row r (k0 % 4 == 0) into the images
-        auto put4x = [&](int r, int k0, const double *x) {
+        // residues of k0..k0+3 of row r (k0 % 4 == 0) into the images; the
+        // fast form (fast_c true: one scale factor, coefficient 1) needs the
+        // row's fast flag
+        auto put4g = [&](auto fast_c, int r, int k0, const double *x) {
+            constexpr bool kFast = decltype(fast_c)::value;
             uint32_t packed[L];
 #pragma unroll
             for (int l = 0; l < L; l++) packed[l] = 0;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                const double tt = (x[j] * s1) * s2 + kMagicD;         // 1.5 * 2^52 + rint(x 2^(P-e))
-                const double X = (tt - kMagicD) * coef;               // the integer coefficient folded in
-                const uint32_t xlo = (uint32_t)__double2loint(tt) * (uint32_t)P.coef;   // X mod 2^32
+                double tt, X;
+                uint32_t xlo;                                         // X mod 2^32
+                if (kFast) {
+                    tt = fma(x[j], s1, kMagicD);                      // 1.5 * 2^52 + rint(x 2^(P-e))
+                    X = tt - kMagicD;
+                    xlo = (uint32_t)__double2loint(tt);
+                } else {
+                    tt = (x[j] * s1) * s2 + kMagicD;
+                    X = (tt - kMagicD) * coef;                        // the integer coefficient folded in
+                    xlo = (uint32_t)__double2loint(tt) * (uint32_t)P.coef;
+                }
                 // byte j of each modulus word takes this element's residue
                 const uint32_t sel = 0x3210u ^ ((0x4u ^ (uint32_t)j) << (4 * j));
                 StaticFor<0, L>::run([&](auto ic) {
@@ -331,17 +388,60 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
         };
         auto put4 = [&](int r, int k0) {
             double x[4];
-            load4(k0, x);
-            put4x(r, k0, x);
+            load4_if(k0, x, false);
+            put4g(std::false_type(), r, k0, x);
         };
         if (un.w == kUnitRowMap) {
             const int lr = threadIdx.x >> 3, c = threadIdx.x & 7;
             const int r = un.y + lr;
-            if (lr >= un.z || r >= P.wrows) continue;
-            set_row(r);
-            for (int k0 = 4 * c; k0 < P.wk; k0 += 32) put4(r, k0);
+            const bool smp = sample && sampled_panel(P, un.w);       // uniform over the CTA
+            if (redo && !smp) continue;
+            const bool rv = lr < un.z && r < P.wrows;
+            // largest |x| of the row as the largest high word without its
+            // sign bit (ordered as |x|; its exponent field is that of the maximum)
+            uint32_t mx = 0;
+            if (rv) {
+                bool act = true;
+                int e_over = kNoExp;
+                if (redo) {
+                    // the exact exponent against the bound the residues used
+                    const int g = gidx[P.g_off + r];
+                    e_over = tabt[g];
+                    act = e_over > tab[g];
+                }
+                if (act) {
+                    set_row(r, e_over);
+                    const bool track = smp && !redo;
+                    auto run = [&](auto fast_c) {
+                        for (int k0 = 4 * c; k0 < P.wk; k0 += 32) {
+                            double x[4];
+                            load4_if(k0, x, track);
+                            if (track)
+#pragma unroll
+                                for (int j = 0; j < 4; j++)
+                                    mx = max(mx, (uint32_t)__double2hiint(x[j]) & 0x7fffffffu);
+                            put4g(fast_c, r, k0, x);
+                        }
+                    };
+                    if (fast) run(std::true_type());
+                    else run(std::false_type());
+                }
+            }
+            if (smp && !redo) {
+                // the row's exact exponent (all 8 threads of every row of the warp take part)
+                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+                if (rv && c == 0 && mx != 0) {
+                    // frexp's exponent of a normal number with biased exponent b is
+                    // b - 1022; subnormals (b = 0) take -1022, above their own
+                    const int b = (int)(mx >> 20);
+                    atomicMax(&tabt[gidx[P.g_off + r]], (b > 0 ? b : 1) - 1022);
+                }
+            }
             continue;
         }
+        if (redo) continue;                                  // tile-mapped units read every element
         const int nkt = (P.wk + 15) >> 4;
         const int ntile = ((un.z + 7) >> 3) * nkt;
         for (int t = warp; t < ntile; t += kSplitWarps) {
@@ -349,7 +449,7 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
             const int rl = rg * 8 + lrow, r = un.y + rl;
             const int k0 = kt * 16 + kq * 4;
             if (rl >= un.z || r >= P.wrows || k0 >= P.wk) continue;
-            if (r != cur) set_row(r);
+            if (r != cur) set_row(r, kNoExp);
             put4(r, k0);
         }
     }
@@ -897,10 +997,10 @@ int num_sms() {
 
 cudaError_t launch_crt_exponents(const DCrtPanel *panels, const int4 *units, int32_t nunits, int32_t nx,
                                  int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
-                                 int32_t *ey, cudaStream_t s) {
+                                 int32_t *ey, int32_t sample, cudaStream_t s) {
     if (nunits <= 0) return cudaSuccess;
     const int grid = nunits;                               // one unit per CTA
-    crt_exp_kernel<<<grid, kSplitThreads, 0, s>>>(panels, units, nunits, a, b, gidx, ex, ey);
+    crt_exp_kernel<<<grid, kSplitThreads, 0, s>>>(panels, units, nunits, a, b, gidx, ex, ey, sample);
     return cudaGetLastError();
 }
 
@@ -908,6 +1008,20 @@ cudaError_t launch_crt_fill(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, cu
     crt_fill_kernel<<<64, 256, 0, s>>>(ex, nx, kNoExp);
     crt_fill_kernel<<<64, 256, 0, s>>>(ey, ny, kNoExp);
     return cudaGetLastError();
+}
+
+cudaError_t launch_crt_merge(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, const int32_t *ext,
+                             const int32_t *eyt, cudaStream_t s) {
+    crt_merge_kernel<<<64, 256, 0, s>>>(ex, ext, nx);
+    crt_merge_kernel<<<64, 256, 0, s>>>(ey, eyt, ny);
+    return cudaGetLastError();
+}
+
+bool crt_unit_sampled(const DCrtPanel &p, int unit_map) { return sampled_panel(p, unit_map); }
+int64_t crt_sampled_elems(const DCrtPanel &p) {
+    // elements the sampled exponent pass reads of one row
+    const int64_t runs = ((int64_t)p.K + 32 * kSampleGroups - 1) / (32 * kSampleGroups);
+    return std::min<int64_t>(32 * runs, p.K);
 }
 
 template<int L, class FC>
@@ -954,11 +1068,12 @@ cudaError_t launch_crt_fused(int shape, const DCrtPanel *panels, const DCrtFamil
 
 cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int32_t nunits,
                                 const double *a, const double *b, const int32_t *gidx, const int32_t *ex,
-                                const int32_t *ey, uint8_t *res, const CrtParams &cp, cudaStream_t s) {
+                                const int32_t *ey, int32_t *ext, int32_t *eyt, int32_t sample, int32_t redo,
+                                uint8_t *res, const CrtParams &cp, cudaStream_t s) {
     if (nunits <= 0) return cudaSuccess;
     const int grid = nunits;                               // one unit per CTA
     switch (cp.L) {
-#define CASE_L(n) case n: crt_res_kernel<n><<<grid, kSplitThreads, 0, s>>>(panels, units, nunits, a, b, gidx, ex, ey, res, cp); break;
+#define CASE_L(n) case n: crt_res_kernel<n><<<grid, kSplitThreads, 0, s>>>(panels, units, nunits, a, b, gidx, ex, ey, ext, eyt, sample, redo, res, cp); break;
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
 #undef CASE_L
     default: return cudaErrorInvalidValue;

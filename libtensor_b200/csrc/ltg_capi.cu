@@ -187,8 +187,11 @@ struct CrtExec {
     int32_t npanels = 0, nitems = 0, max_rows = 0, nx = 0, ny = 0, ngroups = 0, nunits = 0;
     int64_t src_elems = 0, res_bytes = 0;   // operand elements read per pass, residue bytes written
     int64_t fused_elems = 0;                // of those, elements of row families (read once from HBM)
+    int64_t exp_elems = 0;                  // elements the exponent pass reads (the others: per pass)
+    int32_t sampled = 0;                    // sampled exponent bounds, checked by the residue pass
     double scale = 1.0;                     // kc (and d in add mode) times the pair coefficients' scale
     DevBuf panels, units, tasks, items, cblks, comps, ctab, cells, gidx, ex, ey, res, out;
+    DevBuf ext, eyt;                        // exact exponents of the sampled rows
     // row families split in one read (launch_crt_fused): families, their
     // panels and tile offsets, and the 8-row units
     DevBuf fams, famp, famt, funits;
@@ -209,6 +212,7 @@ struct ltg_plan {
     int split_k = 0;              // plain DMMA k chunks per tile: 0 automatic, 1 never, 2-4 always
     bool group_products = true;   // modular mode: small C blocks grouped into larger products
     int fused_split = 0;          // modular mode: row families split in one read (kernel shape 1, 2; 0 off)
+    int crt_sampled = 1;          // modular mode: sampled exponent bounds of long rows (0: exact pass)
     // caller-built task list (ltg_plan_contract2_upload): plain FP64 only,
     // coefficients absolute, no schedule of its own
     bool external = false;
@@ -1712,6 +1716,11 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
             units.push_back(make_int4(i, r0, std::min(ru, panels[i].wrows - r0), rowmap ? 0 : 1));
     }
     ex->nunits = (int32_t)units.size();
+    ex->sampled = pl->crt_sampled ? 1 : 0;
+    for (const int4 &u : units) {
+        const DCrtPanel &q = panels[u.x];
+        ex->exp_elems += (int64_t)u.z * (ex->sampled && crt_unit_sampled(q, u.w) ? crt_sampled_elems(q) : q.K);
+    }
     upload_vec(ex->units, units, s);
     ex->nfunits = (int32_t)funits.size();
     if (!funits.empty()) {
@@ -1726,6 +1735,10 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     ex->out.alloc(std::max<int64_t>(out_bytes, 1024));
     ex->ex.alloc(std::max<int64_t>(ex->nx, 1) * sizeof(int32_t));
     ex->ey.alloc(std::max<int64_t>(ex->ny, 1) * sizeof(int32_t));
+    if (ex->sampled) {
+        ex->ext.alloc(std::max<int64_t>(ex->nx, 1) * sizeof(int32_t));
+        ex->eyt.alloc(std::max<int64_t>(ex->ny, 1) * sizeof(int32_t));
+    }
     upload_vec(ex->panels, panels, s);
     upload_vec(ex->tasks, dt, s);
     upload_vec(ex->items, items, s);
@@ -2891,16 +2904,22 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             const double *pa = plan->a->arena.as<double>(), *pb = plan->b->arena.as<double>();
             TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
             LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), s));
+            if (cx->sampled) LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), s));
             LTG_CUDA(launch_crt_fused(plan->fused_split, cx->panels.as<DCrtPanel>(), cx->fams.as<DCrtFamily>(), cx->famp.as<int32_t>(),
                                       cx->famt.as<int32_t>(), cx->funits.as<int4>(), cx->nfunits, pa, pb,
                                       cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
                                       cx->res.as<uint8_t>(), cx->cp, s));
             LTG_CUDA(launch_crt_exponents(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, cx->nx,
                                           cx->ny, pa, pb, cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(),
-                                          cx->ey.as<int32_t>(), s));
-            LTG_CUDA(launch_crt_residues(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, pa, pb,
-                                         cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
-                                         cx->res.as<uint8_t>(), cx->cp, s));
+                                          cx->ey.as<int32_t>(), cx->sampled, s));
+            for (int redo = 0; redo <= cx->sampled; redo++)
+                LTG_CUDA(launch_crt_residues(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, pa, pb,
+                                             cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
+                                             cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), cx->sampled, redo,
+                                             cx->res.as<uint8_t>(), cx->cp, s));
+            if (cx->sampled)
+                LTG_CUDA(launch_crt_merge(cx->nx, cx->ny, cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
+                                          cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), s));
             t_split.done();
             TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
             LTG_CUDA(launch_crt_gemm(cx->panels.as<DCrtPanel>(), cx->res.as<uint8_t>(), cx->tasks.as<DCrtTask>(),
@@ -2914,7 +2933,8 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                                         cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), c->arena.as<double>(), add,
                                         cx->scale, cx->cp, s));
             t_comb.done();
-            ctx->launches += 2 + (cx->nfunits > 0 ? 1 : 0) + (cx->nunits > 0 ? 2 : 0) + (cx->nitems > 0 ? 2 : 0);
+            ctx->launches += 2 + (cx->nfunits > 0 ? 1 : 0) + (cx->nunits > 0 ? 2 : 0) + (cx->nitems > 0 ? 2 : 0) +
+                             (cx->sampled ? 4 + (cx->nunits > 0 ? 1 : 0) : 0);
             fetch_device_wait(ctx);
             if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
             for (int64_t sl : cx->sched_slots) c->h.nonzero[sl] = 1;
@@ -3016,7 +3036,7 @@ int ltg_contract2_split_bytes(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t n
             CrtExec *cx = prepare_crt(plan, c, nslices > 0 ? nslices : 13, ka, kb, kc, add, d);
             // row families: one HBM read (the second pass reads L2); the other
             // panels: the exponent pass and the residue pass
-            *read_bytes = 8 * (2 * cx->src_elems - cx->fused_elems);
+            *read_bytes = 8 * (cx->exp_elems + cx->src_elems);
             *write_bytes = cx->res_bytes;
         } else if (mode >= LTG_MODE_OZAKI_BF16 && mode <= LTG_MODE_OZAKI_INT8) {
             const int S = nslices > 0 ? nslices : (mode == LTG_MODE_OZAKI_FP8 ? 8 : 7);
@@ -3070,6 +3090,16 @@ int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable) {
         if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
         if (enable < 0 || enable > 2) throw error(kErrBadArg, "one-read split shape must be 0 (off), 1 or 2");
         plan->fused_split = enable;
+        plan->crt.clear();
+    });
+}
+
+int ltg_contract2_set_crt_bound(ltg_plan *plan, int32_t sampled) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
+        if (sampled != 0 && sampled != 1) throw error(kErrBadArg, "exponent bound must be 0 (exact) or 1 (sampled)");
+        plan->crt_sampled = sampled;
         plan->crt.clear();
     });
 }

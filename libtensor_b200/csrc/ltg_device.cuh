@@ -319,11 +319,19 @@ void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t
 // Garner recombination into FP64 C.
 // Split passes work on units (panel, first row, rows, unused): at most 256
 // rows of one panel.
+// sample != 0: long rows of row-mapped units (crt_unit_sampled) contribute
+// a sampled bound, one binade above the largest sampled magnitude.
 cudaError_t launch_crt_exponents(const DCrtPanel *panels, const int4 *units, int32_t nunits,
     int32_t nx, int32_t ny, const double *a, const double *b, const int32_t *gidx, int32_t *ex,
-    int32_t *ey, cudaStream_t s);
+    int32_t *ey, int32_t sample, cudaStream_t s);
+bool crt_unit_sampled(const DCrtPanel &p, int unit_map);
+int64_t crt_sampled_elems(const DCrtPanel &p);        // elements of one row the sampled pass reads
 // Sets both exponent tables to "no element" (before the passes below).
 cudaError_t launch_crt_fill(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, cudaStream_t s);
+// ex = max(ex, ext), ey = max(ey, eyt): after the residue pass's redo, the
+// exponents the residues were formed with.
+cudaError_t launch_crt_merge(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, const int32_t *ext,
+    const int32_t *eyt, cudaStream_t s);
 // Exponents and residues of the row families in one HBM read, in kernel
 // shape 1-4 (units: crt_fuse_rows(shape) rows of one family, {family, first
 // row, rows, 0}); ex/ey hold kNoExp before.
@@ -331,9 +339,13 @@ int crt_fuse_rows(int shape);
 cudaError_t launch_crt_fused(int shape, const DCrtPanel *panels, const DCrtFamily *fams, const int32_t *famp,
     const int32_t *famt, const int4 *units, int32_t nunits, const double *a, const double *b,
     const int32_t *gidx, int32_t *ex, int32_t *ey, uint8_t *res, const CrtParams &cp, cudaStream_t s);
+// sample != 0: sampled rows also form their exact exponents into ext / eyt
+// (set to "no element" before); redo != 0: only the sampled rows whose exact
+// exponent exceeds their bound run, with the exact exponent.
 cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int32_t nunits,
     const double *a, const double *b, const int32_t *gidx, const int32_t *ex, const int32_t *ey,
-    uint8_t *res, const CrtParams &cp, cudaStream_t s);
+    int32_t *ext, int32_t *eyt, int32_t sample, int32_t redo, uint8_t *res, const CrtParams &cp,
+    cudaStream_t s);
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
     const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp, int32_t *err,
     uint64_t wait_ns, int32_t stage_kb, cudaStream_t s);

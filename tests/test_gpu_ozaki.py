@@ -179,6 +179,7 @@ def test_fused_split_matches_two_pass(gctx, which):
     for p in c["pairs"]:
         contr.contract(*p)
     op = btod_contract2(contr, A, B, kc=cfg.kc)
+    op.set_crt_bound(False)                  # exact exponents on both sides of the comparison
     out = []
     for fused in (1, 2, 0):
         op.set_fused_split(fused)
@@ -193,3 +194,82 @@ def test_fused_split_matches_two_pass(gctx, which):
     op.close()
     A.close()
     B.close()
+
+
+def _ladder_prof(gctx):
+    from libtensor_b200 import spec as S
+    from libtensor_b200.core import block_tensor
+    cfg = S.LADDER_PROF
+    A, B = block_tensor(gctx, cfg.t_spec()), block_tensor(gctx, cfg.v_spec())
+    A.fill_seeded(11, cfg.t_scale)
+    B.fill_seeded(23, cfg.v_scale)
+    c = cfg.contraction
+    contr = contraction2(c["n"], c["m"], c["k"], c["permc"])
+    for p in c["pairs"]:
+        contr.contract(*p)
+    return cfg, A, B, btod_contract2(contr, A, B, kc=cfg.kc)
+
+
+def _modes_against_plain(gctx, op):
+    """Block-relative error of the modular result (sampled and exact row
+    exponents) against the plain FP64 result of the same call."""
+    P = op.make_result()
+    op.perform(P)
+    gctx.synchronize()
+    want = P.download()
+    errs = {}
+    for sampled in (True, False):
+        op.set_crt_bound(sampled)
+        C = op.make_result()
+        op.perform(C, mode=MODE_OZAKI_CRT, nslices=13)
+        op.perform(C, 0.5, mode=MODE_OZAKI_CRT, nslices=13)           # C += 0.5 (...): 1.5 x
+        gctx.synchronize()
+        got = C.download()
+        worst = 0.0
+        for (bidx, g), (_, w) in zip(C.blocks(got), P.blocks(want)):
+            m = float(np.max(np.abs(w))) if w.size else 0.0
+            if m > 0:
+                worst = max(worst, float(np.max(np.abs(g - 1.5 * w))) / (1.5 * m))
+        errs[sampled] = worst
+        C.close()
+    op.set_crt_bound(True)
+    P.close()
+    return errs
+
+
+def test_sampled_row_bounds_within_error():
+    """Ladder o=40 v=160 (rows of 1024-2304 k words, so the long rows take
+    sampled exponent bounds): both ways of finding the row exponents stay
+    within 1e-12 of the plain FP64 result, assign and add."""
+    ctx = Context(0)
+    cfg, A, B, op = _ladder_prof(ctx)
+    errs = _modes_against_plain(ctx, op)
+    assert errs[True] <= 1e-12 and errs[False] <= 1e-12, errs
+    op.close(); A.close(); B.close(); ctx.close()
+
+
+def test_rows_whose_sample_misses_the_maximum_are_redone():
+    """Large elements placed between the sampled groups of many operand rows
+    (k = 40 and k = 300 of row 0 of every V block, outside the sampled runs
+    k = 0..31, 512..543, ...; 1e4 times the block's magnitude) make the
+    sampled bounds too small for those rows; the residue pass must find it
+    and redo them.  Residues formed with a bound 2^13 too small would exceed
+    the CRT range and give errors of order one; redone, the error against the
+    plain FP64 result is that of exact exponents within the one binade of
+    headroom the sampled bounds of the other side's rows may take (the large
+    elements cost the other elements of their rows about 13 of their P bits,
+    hence the looser bound)."""
+    ctx = Context(0)
+    cfg, A, B, op = _ladder_prof(ctx)
+    arena = B.download().copy()
+    for bidx, blk in B.blocks(arena):
+        flat = blk.reshape(-1)
+        if flat.size > 300:
+            m = float(np.max(np.abs(flat))) or 1.0
+            flat[40] = 1e4 * m
+            flat[300] = -1e4 * m
+    B.upload(arena)
+    errs = _modes_against_plain(ctx, op)
+    assert errs[True] <= 1e-10 and errs[False] <= 1e-10, errs
+    assert errs[True] <= 4.0 * errs[False], errs
+    op.close(); A.close(); B.close(); ctx.close()
