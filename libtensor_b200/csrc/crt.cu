@@ -166,11 +166,7 @@ __host__ __device__ __forceinline__ bool sampled_panel(const DCrtPanel &P, int u
 __global__ void crt_fill_kernel(int32_t *p, int32_t n, int32_t v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
-// After the residue pass and its redo: the exponent each row's residues were
-// formed with, max(bound, exact).
-__global__ void crt_merge_kernel(int32_t *e, const int32_t *et, int32_t n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) e[i] = max(e[i], et[i]);
-}
+
 
 // k offset mode of a panel: 0 contiguous, 1 tabulated in koff, 2 computed.
 __device__ __forceinline__ int koff_setup(const DCrtPanel &P, int32_t *koff) {
@@ -882,7 +878,8 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
                    const DCBlock *__restrict__ cblks, const DCrtComp *__restrict__ comps,
                    const int32_t *__restrict__ ctab, const DCrtCell *__restrict__ cells,
                    const uint8_t *__restrict__ out, const int32_t *__restrict__ gidx,
-                   const int32_t *__restrict__ ex, const int32_t *__restrict__ ey, double *__restrict__ C,
+                   const int32_t *__restrict__ ex, const int32_t *__restrict__ ey,
+                   const int32_t *__restrict__ ext, const int32_t *__restrict__ eyt, double *__restrict__ C,
                    int32_t add, double scale, const CrtParams cp) {
     __shared__ __align__(16) uint8_t sres[L][kXRows][kCombCols];
     __shared__ int64_t soff[kXRows + kCombCols];               // one C block: row / column offsets
@@ -909,7 +906,10 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
             const int j = isx ? i : i - kXRows;
             if (isx ? j >= xr : c0 + j >= yc) continue;
             const int idx = isx ? xb + j : item.y0 + c0 + j;           // tile row / column
-            sexp[i] = isx ? ex[gidx[panels[item.gx].g_off + idx]] : ey[gidx[panels[item.gy].g_off + idx]];
+            // the exponent the residues were formed with: the bound, or the
+            // exact exponent of a row the residue pass redid
+            const int g = isx ? gidx[panels[item.gx].g_off + idx] : gidx[panels[item.gy].g_off + idx];
+            sexp[i] = isx ? max(ex[g], ext[g]) : max(ey[g], eyt[g]);
             const bool crow = isx != (cp.swap != 0);                  // a row of C (side of A)
             if (cc) {
                 const int32_t *e = ctab + (crow ? cc->row_off : cc->col_off) + (1 + kCrtSideDims) * idx;
@@ -1010,13 +1010,6 @@ cudaError_t launch_crt_fill(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, cu
     return cudaGetLastError();
 }
 
-cudaError_t launch_crt_merge(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, const int32_t *ext,
-                             const int32_t *eyt, cudaStream_t s) {
-    crt_merge_kernel<<<64, 256, 0, s>>>(ex, ext, nx);
-    crt_merge_kernel<<<64, 256, 0, s>>>(ey, eyt, ny);
-    return cudaGetLastError();
-}
-
 bool crt_unit_sampled(const DCrtPanel &p, int unit_map) { return sampled_panel(p, unit_map); }
 int64_t crt_sampled_elems(const DCrtPanel &p) {
     // elements the sampled exponent pass reads of one row
@@ -1114,12 +1107,12 @@ cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const D
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
                                const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab,
                                const DCrtCell *cells, const uint8_t *out, const int32_t *gidx,
-                               const int32_t *ex, const int32_t *ey, double *c, int32_t add, double scale,
+                               const int32_t *ex, const int32_t *ey, const int32_t *ext, const int32_t *eyt, double *c, int32_t add, double scale,
                                const CrtParams &cp, cudaStream_t s) {
     if (nitems <= 0) return cudaSuccess;
     const int grid = 32 * nitems < 8 * num_sms() ? 32 * nitems : 8 * num_sms();
     switch (cp.L) {
-#define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, c, add, scale, cp); break;
+#define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, ext, eyt, c, add, scale, cp); break;
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
 #undef CASE_L
     default: return cudaErrorInvalidValue;

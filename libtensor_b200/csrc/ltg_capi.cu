@@ -1735,10 +1735,8 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     ex->out.alloc(std::max<int64_t>(out_bytes, 1024));
     ex->ex.alloc(std::max<int64_t>(ex->nx, 1) * sizeof(int32_t));
     ex->ey.alloc(std::max<int64_t>(ex->ny, 1) * sizeof(int32_t));
-    if (ex->sampled) {
-        ex->ext.alloc(std::max<int64_t>(ex->nx, 1) * sizeof(int32_t));
-        ex->eyt.alloc(std::max<int64_t>(ex->ny, 1) * sizeof(int32_t));
-    }
+    ex->ext.alloc(std::max<int64_t>(ex->nx, 1) * sizeof(int32_t));
+    ex->eyt.alloc(std::max<int64_t>(ex->ny, 1) * sizeof(int32_t));
     upload_vec(ex->panels, panels, s);
     upload_vec(ex->tasks, dt, s);
     upload_vec(ex->items, items, s);
@@ -2904,7 +2902,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             const double *pa = plan->a->arena.as<double>(), *pb = plan->b->arena.as<double>();
             TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
             LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), s));
-            if (cx->sampled) LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), s));
+            LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), s));
             LTG_CUDA(launch_crt_fused(plan->fused_split, cx->panels.as<DCrtPanel>(), cx->fams.as<DCrtFamily>(), cx->famp.as<int32_t>(),
                                       cx->famt.as<int32_t>(), cx->funits.as<int4>(), cx->nfunits, pa, pb,
                                       cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
@@ -2917,9 +2915,6 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
                                              cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
                                              cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), cx->sampled, redo,
                                              cx->res.as<uint8_t>(), cx->cp, s));
-            if (cx->sampled)
-                LTG_CUDA(launch_crt_merge(cx->nx, cx->ny, cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
-                                          cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), s));
             t_split.done();
             TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
             LTG_CUDA(launch_crt_gemm(cx->panels.as<DCrtPanel>(), cx->res.as<uint8_t>(), cx->tasks.as<DCrtTask>(),
@@ -2930,11 +2925,12 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
             LTG_CUDA(launch_crt_combine(cx->panels.as<DCrtPanel>(), cx->items.as<DCrtItem>(), cx->nitems,
                                         cx->cblks.as<DCBlock>(), cx->comps.as<DCrtComp>(), cx->ctab.as<int32_t>(),
                                         cx->cells.as<DCrtCell>(), cx->out.as<uint8_t>(), cx->gidx.as<int32_t>(),
-                                        cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), c->arena.as<double>(), add,
+                                        cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), cx->ext.as<int32_t>(),
+                                        cx->eyt.as<int32_t>(), c->arena.as<double>(), add,
                                         cx->scale, cx->cp, s));
             t_comb.done();
-            ctx->launches += 2 + (cx->nfunits > 0 ? 1 : 0) + (cx->nunits > 0 ? 2 : 0) + (cx->nitems > 0 ? 2 : 0) +
-                             (cx->sampled ? 4 + (cx->nunits > 0 ? 1 : 0) : 0);
+            ctx->launches += 4 + (cx->nfunits > 0 ? 1 : 0) + (cx->nunits > 0 ? 2 + cx->sampled : 0) +
+                             (cx->nitems > 0 ? 2 : 0);
             fetch_device_wait(ctx);
             if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
             for (int64_t sl : cx->sched_slots) c->h.nonzero[sl] = 1;

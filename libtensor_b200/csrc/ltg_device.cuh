@@ -328,10 +328,7 @@ bool crt_unit_sampled(const DCrtPanel &p, int unit_map);
 int64_t crt_sampled_elems(const DCrtPanel &p);        // elements of one row the sampled pass reads
 // Sets both exponent tables to "no element" (before the passes below).
 cudaError_t launch_crt_fill(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, cudaStream_t s);
-// ex = max(ex, ext), ey = max(ey, eyt): after the residue pass's redo, the
-// exponents the residues were formed with.
-cudaError_t launch_crt_merge(int32_t nx, int32_t ny, int32_t *ex, int32_t *ey, const int32_t *ext,
-    const int32_t *eyt, cudaStream_t s);
+
 // Exponents and residues of the row families in one HBM read, in kernel
 // shape 1-4 (units: crt_fuse_rows(shape) rows of one family, {family, first
 // row, rows, 0}); ex/ey hold kNoExp before.
@@ -349,9 +346,11 @@ cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int3
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
     const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp, int32_t *err,
     uint64_t wait_ns, int32_t stage_kb, cudaStream_t s);
+// Garner recombination into C; each row's exponent is max(ex, ext) (the
+// bound, or the exact exponent of a row the residue pass redid).
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
     const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab, const DCrtCell *cells,
-    const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey, double *c,
+    const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey, const int32_t *ext, const int32_t *eyt, double *c,
     int32_t add, double scale, const CrtParams &cp, cudaStream_t s);
 
 // Grouped plain products: operand cells into dense group panels (units:
