@@ -185,6 +185,7 @@ crt_exp_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
                int32_t *ex, int32_t *ey, int32_t sample) {
     __shared__ int32_t koff[kKoffMax];
     __shared__ int32_t rexp[kUnitRowsMax];
+    __shared__ int64_t roff[kUnitRowsMax];                  // tile mapping: the unit's row offsets
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lrow = lane >> 2, kq = lane & 3;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const int4 un = units[u];
@@ -196,7 +197,10 @@ crt_exp_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
         if (shared) __syncthreads();
         const int mode = koff_setup(P, koff);
         if (un.w == kUnitTileMap)
-            for (int i = threadIdx.x; i < un.z; i += blockDim.x) rexp[i] = kNoExp;
+            for (int i = threadIdx.x; i < un.z; i += blockDim.x) {
+                rexp[i] = kNoExp;
+                roff[i] = un.y + i < P.rows ? mixed_offset(un.y + i, P.nr, P.rext, P.rstr) : 0;
+            }
         if (shared) __syncthreads();
         const double *src = (P.src ? B : A) + P.src_off;
         int32_t *tab = P.side == 0 ? ex : ey;
@@ -227,15 +231,13 @@ crt_exp_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
         }
         const int nkt = (P.K + 15) >> 4;
         const int ntile = ((un.z + 7) >> 3) * nkt;
-        int cur = -1;
-        const double *row = src;
         for (int t = warp; t < ntile; t += kSplitWarps) {
             const int rg = t / nkt, kt = t - rg * nkt;
             const int rl = rg * 8 + lrow, r = un.y + rl;
             const bool valid = rl < un.z && r < P.rows;
             double mx = 0.0;
             if (valid) {
-                if (r != cur) { row = src + mixed_offset(r, P.nr, P.rext, P.rstr); cur = r; }
+                const double *row = src + roff[rl];
                 const int k0 = kt * 16 + kq * 4;
 #pragma unroll
                 for (int j = 0; j < 4; j++)
@@ -293,13 +295,23 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
                const int32_t *__restrict__ ex, const int32_t *__restrict__ ey, int32_t *ext, int32_t *eyt,
                int32_t sample, int32_t redo, uint8_t *__restrict__ res, const CrtParams cp) {
     __shared__ int32_t koff[kKoffMax];
+    __shared__ int64_t roff[kUnitRowsMax];                  // tile mapping: the unit's row offsets
+    __shared__ int32_t rexp[kUnitRowsMax];                  //   and exponents
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lrow = lane >> 2, kq = lane & 3;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const int4 un = units[u];
         const DCrtPanel &P = panels[un.x];
-        const bool shared = P.nk != 1 || P.kstr[0] != 1;      // tabulated k offsets (uniform)
+        // tabulated k offsets and the tile mapping's row tables (uniform)
+        const bool shared = P.nk != 1 || P.kstr[0] != 1 || (un.w == kUnitTileMap && !redo);
         if (shared) __syncthreads();                         // the previous unit's readers are done
         const int mode = koff_setup(P, koff);
+        if (un.w == kUnitTileMap && !redo)
+            for (int i = threadIdx.x; i < un.z; i += blockDim.x) {
+                const int r = un.y + i;
+                const bool valid = r < P.rows;
+                roff[i] = valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0;
+                rexp[i] = valid ? (P.side == 0 ? ex : ey)[gidx[P.g_off + r]] : kNoExp;
+            }
         if (shared) __syncthreads();
         const double *src = (P.src ? B : A) + P.src_off;
         const int32_t *tab = P.side == 0 ? ex : ey;
@@ -312,12 +324,13 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
         const double *row = src;
         double s1 = 0.0, s2 = 0.0;
         bool live = false, rowok = false, fast = false, vec = false;
-        // row r's offset and scaling (exponent e_over, or the side table's),
-        // kept while the thread stays on it
-        auto set_row = [&](int r, int e_over) {
+        // row r's offset and scaling (exponent e_over, or the side table's;
+        // the tile mapping passes both from its row tables), kept while the
+        // thread stays on it
+        auto set_row = [&](int r, int e_over, int64_t off = -1) {
             cur = r;
             const bool valid = r < P.rows;
-            row = src + (valid ? mixed_offset(r, P.nr, P.rext, P.rstr) : 0);
+            row = src + (!valid ? 0 : off >= 0 ? off : mixed_offset(r, P.nr, P.rext, P.rstr));
             const int e = !valid ? kNoExp : (e_over > kNoExp ? e_over : tab[gidx[P.g_off + r]]);
             // 2^(P - e) as two finite factors
             const int sh = e > kNoExp ? cp.P - e : 0;
@@ -445,7 +458,7 @@ crt_res_kernel(const DCrtPanel *__restrict__ panels, const int4 *__restrict__ un
             const int rl = rg * 8 + lrow, r = un.y + rl;
             const int k0 = kt * 16 + kq * 4;
             if (rl >= un.z || r >= P.wrows || k0 >= P.wk) continue;
-            if (r != cur) set_row(r, kNoExp);
+            if (r != cur) set_row(r, rexp[rl], roff[rl]);
             put4(r, k0);
         }
     }

@@ -1716,7 +1716,11 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
             units.push_back(make_int4(i, r0, std::min(ru, panels[i].wrows - r0), rowmap ? 0 : 1));
     }
     ex->nunits = (int32_t)units.size();
-    ex->sampled = pl->crt_sampled ? 1 : 0;
+    // sampled bounds only where some unit samples (else the exact pass, and
+    // no redo launch)
+    bool any_sampled = false;
+    for (const int4 &u : units) any_sampled = any_sampled || crt_unit_sampled(panels[u.x], u.w);
+    ex->sampled = pl->crt_sampled && any_sampled ? 1 : 0;
     for (const int4 &u : units) {
         const DCrtPanel &q = panels[u.x];
         ex->exp_elems += (int64_t)u.z * (ex->sampled && crt_unit_sampled(q, u.w) ? crt_sampled_elems(q) : q.K);
