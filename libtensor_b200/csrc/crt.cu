@@ -671,9 +671,12 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 template<int KB>
 __global__ void __launch_bounds__(kGemmThreads, 1)
 crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict__ res,
-                const DCrtTask *__restrict__ tasks, const DCrtItem *__restrict__ items, int32_t nitems,
-                uint8_t *__restrict__ out, const CrtParams cp, int32_t stages, int32_t *err,
-                uint64_t wait_ns) {
+                const DCrtTask *__restrict__ tasks, const DCrtItem *__restrict__ items,
+                const int32_t *__restrict__ cta_items, uint8_t *__restrict__ out, const CrtParams cp,
+                int32_t stages, int32_t *err, uint64_t wait_ns) {
+    // this CTA's items: cta_items[j], j in [cta_items[b], cta_items[b + 1])
+    // (every role walks the same list)
+    const int j0 = cta_items[blockIdx.x], j1 = cta_items[blockIdx.x + 1];
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], accf_bar[2], acce_bar[2], drain_bar;
@@ -708,7 +711,8 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
             bool ok = true;
             int armed[kMaxStages];
             for (int i = 0; i < kMaxStages; i++) armed[i] = -1;
-            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+            for (int j = j0; j < j1 && ok; j++) {
+                const int it = cta_items[j];
                 const DCrtItem item = items[it];
                 const uint32_t ybytes = (uint32_t)item.nt * kKB;
                 for (int l = 0; l < L && ok; l++) {
@@ -755,7 +759,8 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
             uint32_t uses[2] = {0, 0};               // fills of each accumulator slot so far
             int rr = 0;                              // slot of the next one-tile fill
             bool ok = true;
-            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+            for (int j = j0; j < j1 && ok; j++) {
+                const int it = cta_items[j];
                 const DCrtItem item = items[it];
                 const uint32_t idesc = instr_desc_i8(item.nt);
                 for (int l = 0; l < L && ok; l++) {
@@ -815,7 +820,8 @@ crt_gemm_kernel(const DCrtPanel *__restrict__ panels, const uint8_t *__restrict_
         uint32_t uses[2] = {0, 0};                                // same slot sequence as the MMA warp
         int rr = 0;
         bool ok = true;
-        for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+        for (int j = j0; j < j1 && ok; j++) {
+            const int it = cta_items[j];
             const DCrtItem item = items[it];
             for (int l = 0; l < L; l++) {
                 const int s0 = item.nx == 2 ? 0 : rr;
@@ -1089,7 +1095,7 @@ cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int3
 
 template<int KB>
 cudaError_t launch_gemm_kb(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
-                           const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp,
+                           const DCrtItem *items, const int32_t *cta_items, int32_t ncta, uint8_t *out, const CrtParams &cp,
                            int32_t *err, uint64_t wait_ns, cudaStream_t s) {
     constexpr int stage_bytes = KB * kSubBytes;
     int stages = (200 * 1024) / stage_bytes;
@@ -1097,23 +1103,22 @@ cudaError_t launch_gemm_kb(const DCrtPanel *panels, const uint8_t *res, const DC
     const size_t smem = (size_t)stages * stage_bytes + 1024;
     cudaError_t e = cudaFuncSetAttribute(crt_gemm_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int grid = nitems < num_sms() ? nitems : num_sms();
-    crt_gemm_kernel<KB><<<grid, kGemmThreads, smem, s>>>(panels, res, tasks, items, nitems, out, cp, stages, err,
+    crt_gemm_kernel<KB><<<ncta, kGemmThreads, smem, s>>>(panels, res, tasks, items, cta_items, out, cp, stages, err,
                                                          wait_ns);
     return cudaGetLastError();
 }
 
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
-                            const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp,
+                            const DCrtItem *items, const int32_t *cta_items, int32_t ncta, uint8_t *out, const CrtParams &cp,
                             int32_t *err, uint64_t wait_ns, int32_t stage_kb, cudaStream_t s) {
-    if (nitems <= 0) return cudaSuccess;
+    if (ncta <= 0) return cudaSuccess;
     // k blocks per pipeline stage: 2 (6 stages of 32 KB), 3 (4 x 48 KB), 4
     // (3 x 64 KB, the default), 6 (2 x 96 KB)
     switch (stage_kb) {
-    case 2: return launch_gemm_kb<2>(panels, res, tasks, items, nitems, out, cp, err, wait_ns, s);
-    case 3: return launch_gemm_kb<3>(panels, res, tasks, items, nitems, out, cp, err, wait_ns, s);
-    case 6: return launch_gemm_kb<6>(panels, res, tasks, items, nitems, out, cp, err, wait_ns, s);
-    default: return launch_gemm_kb<4>(panels, res, tasks, items, nitems, out, cp, err, wait_ns, s);
+    case 2: return launch_gemm_kb<2>(panels, res, tasks, items, cta_items, ncta, out, cp, err, wait_ns, s);
+    case 3: return launch_gemm_kb<3>(panels, res, tasks, items, cta_items, ncta, out, cp, err, wait_ns, s);
+    case 6: return launch_gemm_kb<6>(panels, res, tasks, items, cta_items, ncta, out, cp, err, wait_ns, s);
+    default: return launch_gemm_kb<4>(panels, res, tasks, items, cta_items, ncta, out, cp, err, wait_ns, s);
     }
 }
 

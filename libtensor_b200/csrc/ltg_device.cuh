@@ -343,8 +343,10 @@ cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int3
     const double *a, const double *b, const int32_t *gidx, const int32_t *ex, const int32_t *ey,
     int32_t *ext, int32_t *eyt, int32_t sample, int32_t redo, uint8_t *res, const CrtParams &cp,
     cudaStream_t s);
+// Products: ncta persistent CTAs, CTA b working through the items
+// cta_items[j], j in [cta_items[b], cta_items[b + 1]).
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
-    const DCrtItem *items, int32_t nitems, uint8_t *out, const CrtParams &cp, int32_t *err,
+    const DCrtItem *items, const int32_t *cta_items, int32_t ncta, uint8_t *out, const CrtParams &cp, int32_t *err,
     uint64_t wait_ns, int32_t stage_kb, cudaStream_t s);
 // Garner recombination into C; each row's exponent is max(ex, ext) (the
 // bound, or the exact exponent of a row the residue pass redid).
