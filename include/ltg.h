@@ -258,13 +258,14 @@ int ltg_contract2_set_split_k(ltg_plan *plan, int32_t k);
  * counterpart. */
 int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable);
 /* Modular mode: the one-read split of row families -- panels whose rows feed
- * the same rows of C and nothing else does -- which forms each row's exponent
- * and its residues in one pass over the operand (the second read of each
- * tile hits L2) instead of an exponent pass and a residue pass: shape 0 off
+ * the same rows of C and nothing else does -- which forms each row's exact
+ * exponent and its residues in one kernel (the second read of each tile hits
+ * L2) instead of the exponent pass and the residue pass: shape 0 off
  * (default), 1 or 2 (rows per CTA, threads, CTAs per SM: 2/512/2, 2/256/4).
- * All forms give identical bits; on the ladder o=40 v=240 the two passes are
- * faster (2.40 ms against 2.68 ms for shape 2, although the one-read form
- * moves 9.6 GB through HBM against 13.2).  No reference counterpart. */
+ * Identical bits to the two passes with exact exponents; on the ladder
+ * o=40 v=240 slower than the two passes (2.68 ms for shape 2 against 2.40
+ * with an exact exponent pass, 1.79 with sampled bounds).  No reference
+ * counterpart. */
 int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable);
 /* Modular mode: how the row exponents (the scale of each operand row) are
  * found.  1 (default): rows of at least 1024 k words read one 32-element run
