@@ -86,6 +86,8 @@ def parse():
     p.add_argument("--fused-split", type=int, default=0, choices=[0, 1, 2],
                    help="modular mode: one-read split of row families in kernel shape 1 or 2 (0: exponent and "
                         "residue passes)")
+    p.add_argument("--crt-stage", type=int, default=0, choices=[0, 2, 3, 4, 6],
+                   help="modular mode: k blocks per products pipeline stage (0: default)")
     p.add_argument("--tile", type=int, default=-1, help="force one tile shape (debug)")
     p.add_argument("--split-k", type=int, default=0, choices=[0, 1, 2, 3, 4],
                    help="plain mode: k chunks per tile (0 automatic, 1 never)")
@@ -297,6 +299,8 @@ def ltg_arm(args):
         op.set_split_k(args.split_k)
     if args.fused_split:
         op.set_fused_split(args.fused_split)
+    if args.crt_stage:
+        op.set_crt_stage(args.crt_stage)
     if args.tile >= 0:
         op.set_tile(args.tile)
     elif not args.no_autotune:
