@@ -368,7 +368,7 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
     const uint32_t smem0 = smem_u32(smem);
 
     if (warp == 4) {
-        // ------------------------------------------------ TMA producer
+        // ------------------------------------------------ bulk-copy producer (1-D cp.async.bulk)
         if (lane == 0) {
             int st = 0;
             uint32_t ph = 0;
