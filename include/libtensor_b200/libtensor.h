@@ -550,6 +550,15 @@ public:
     virtual ~additive_bto() { }
     virtual void perform(block_tensor<N, double> &btb) = 0;
     virtual void perform(block_tensor<N, double> &btb, double d) = 0;
+    // btb = sum over the two-element symmetrizer group {e, P} of sign * P(this
+    // operation's result), formed without the result itself where the
+    // operation can (a plain FP64 contraction writes both terms from its
+    // epilogue); false: not supported here, nothing done.
+    virtual bool perform_symmetrized(block_tensor<N, double> &btb, int32_t nidx, const int32_t *idx, bool symm,
+                                     ltg_bt **adopted) {
+        (void)btb; (void)nidx; (void)idx; (void)symm; (void)adopted;
+        return false;
+    }
 };
 
 template<size_t N, size_t M, size_t K>
@@ -615,6 +624,18 @@ public:
     // LTG_MODE_OZAKI_* of ltg.h with its slice (or modulus) count; the
     // default LTG_MODE_PLAIN_FP64 is the FP64 drop-in path.
     void set_split_precision(int32_t mode, int32_t nslices) { m_mode = mode; m_nslices = nslices; }
+    bool perform_symmetrized(block_tensor<N + M, double> &btb, int32_t nidx, const int32_t *idx, bool symm,
+                             ltg_bt **adopted) override {
+        if (m_mode != LTG_MODE_PLAIN_FP64 || (nidx != 2 && nidx != -1)) return false;
+        if (!(btb.is_bound() && btb.handle() == *adopted)) {
+            ltg_bt *r = nullptr;
+            b200::check(ltg_contract2_make_symmetrized(m_plan, nidx, idx, symm ? 1 : 0, &r));
+            btb.adopt(r);
+            *adopted = r;
+        }
+        b200::check(ltg_contract2_symmetrized(m_plan, btb.handle(), 1.0, nidx, idx, symm ? 1 : 0, m_ka, m_kb, m_kc));
+        return true;
+    }
 };
 
 template<size_t N>
@@ -1414,6 +1435,9 @@ protected:
         : m_a(a), m_op(op), m_nidx(nidx), m_idx(std::move(idx)), m_symm(symm) { }
 public:
     void perform(block_tensor<N, double> &btb) override {
+        // an operation that forms the symmetrized sum itself (a contraction
+        // writing both terms from its epilogue) needs no temporary
+        if (m_op && m_op->perform_symmetrized(btb, m_nidx, m_idx.data(), m_symm, &m_adopted)) return;
         block_tensor<N, double> &a = source(btb);
         if (!(btb.is_bound() && btb.handle() == m_adopted)) {
             ltg_bt *b = nullptr;

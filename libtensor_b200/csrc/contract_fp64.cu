@@ -150,12 +150,18 @@ __device__ __forceinline__ void load_stage(double *sA, double *sB, const int64_t
     load_operand<C, C::BN>(sB, rowB, B, k0, t.K, t.nk, t.kext, t.kb_str, t.vec_b != 0);
 }
 
-template<class C>
+// SCATTER: the epilogue writes each C block's tile to the destinations
+// dests[drange[cblk].x .. drange[cblk].y) instead of the block itself --
+// blocks of another tensor, each through its own index mapping and scale
+// (the terms of a symmetrizer over the contraction) -- by atomic adds into
+// a zeroed result.
+template<class C, bool SCATTER>
 __global__ void __launch_bounds__(C::kThreads, C::MINB)
 contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
                      const DItem *__restrict__ items, int32_t nitems, int32_t *counter,
                      const double *__restrict__ A, const double *__restrict__ B,
-                     double *__restrict__ Cp, double *__restrict__ ws, int32_t add) {
+                     double *__restrict__ Cp, double *__restrict__ ws, int32_t add,
+                     const int2 *__restrict__ drange, const DCBlock *__restrict__ dests) {
     extern __shared__ __align__(16) double smem[];
     double *sA = smem;
     double *sB = smem + C::STAGES * C::kStageA;
@@ -336,6 +342,41 @@ contract_fp64_kernel(const DTask *__restrict__ tasks, const DCBlock *__restrict_
             continue;
         }
 
+        if constexpr (SCATTER) {
+            const int2 dr = drange[item.cblk];
+            for (int d = dr.x; d < dr.y; d++) {
+                const DCBlock &db = dests[d];
+                int64_t dm[C::kMT][C::kQ / 2];
+                int64_t dn[C::kNT][2];
+#pragma unroll
+                for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+                    for (int h = 0; h < C::kQ / 2; h++) {
+                        int m = item.m0 + wm * C::WM + i * C::kFragRows + g + 8 * h;
+                        dm[i][h] = m < M ? mixed_offset(m, db.nm, db.mext, db.mc_str) : -1;
+                    }
+#pragma unroll
+                for (int j = 0; j < C::kNT; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        int n = item.n0 + wn * C::WN + j * 8 + 2 * t4 + h;
+                        dn[j][h] = n < N ? mixed_offset(n, db.nn, db.next, db.nc_str) : -1;
+                    }
+                double *Db = Cp + db.c_off;
+#pragma unroll
+                for (int i = 0; i < C::kMT; i++)
+#pragma unroll
+                    for (int j = 0; j < C::kNT; j++)
+#pragma unroll
+                        for (int q = 0; q < C::kQ; q++) {
+                            int64_t om = dm[i][q >> 1], on = dn[j][q & 1];
+                            if (om < 0 || on < 0) continue;
+                            atomicAdd(Db + om + on, db.scale * acc[i][j][q]);
+                        }
+            }
+            continue;
+        }
+
         // Epilogue: scaled store (assign) or scaled accumulate (add) into the
         // canonical C block through its own index mapping.
         const double scale = cb.scale;
@@ -399,16 +440,17 @@ split_reduce_kernel(const DSplit *__restrict__ splits, int32_t nsplits, const DC
     }
 }
 
-template<class C>
-cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *items,
-                       int32_t nitems, int32_t *counter, const double *a, const double *b,
-                       double *c, double *ws, int32_t add, cudaStream_t s) {
+template<class C, bool SCATTER>
+cudaError_t launch_cfg_s(const DTask *tasks, const DCBlock *cblks, const DItem *items,
+                         int32_t nitems, int32_t *counter, const double *a, const double *b,
+                         double *c, double *ws, int32_t add, const int2 *drange, const DCBlock *dests,
+                         cudaStream_t s) {
     static int configured_dev = -1;
     cudaError_t e;
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     if (configured_dev != dev) {
-        e = cudaFuncSetAttribute(contract_fp64_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(contract_fp64_kernel<C, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)C::kSmem);
         if (e != cudaSuccess) return e;
         configured_dev = dev;
@@ -418,9 +460,19 @@ cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *it
     if (grid < 1) return cudaSuccess;
     e = cudaMemsetAsync(counter, 0, sizeof(int32_t), s);
     if (e != cudaSuccess) return e;
-    contract_fp64_kernel<C><<<grid, C::kThreads, C::kSmem, s>>>(tasks, cblks, items, nitems, counter,
-                                                               a, b, c, ws, add);
+    contract_fp64_kernel<C, SCATTER><<<grid, C::kThreads, C::kSmem, s>>>(tasks, cblks, items, nitems, counter,
+                                                                        a, b, c, ws, add, drange, dests);
     return cudaGetLastError();
+}
+
+template<class C>
+cudaError_t launch_cfg(const DTask *tasks, const DCBlock *cblks, const DItem *items,
+                       int32_t nitems, int32_t *counter, const double *a, const double *b,
+                       double *c, double *ws, int32_t add, const int2 *drange, const DCBlock *dests,
+                       cudaStream_t s) {
+    if (dests)
+        return launch_cfg_s<C, true>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    return launch_cfg_s<C, false>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, nullptr, nullptr, s);
 }
 
 // Tile configurations (BM, BN, BK, warp tile M, warp tile N, stages).
@@ -487,30 +539,31 @@ cudaError_t launch_split_reduce(const DSplit *splits, int32_t nsplits, const DCB
 
 cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     const DItem *items, int32_t nitems, int32_t *counter, const double *a,
-    const double *b, double *c, double *ws, int32_t add, int32_t tile_cfg, cudaStream_t s) {
+    const double *b, double *c, double *ws, int32_t add, int32_t tile_cfg, cudaStream_t s,
+    const int2 *drange, const DCBlock *dests) {
     switch (tile_cfg) {
-    case 0: return launch_cfg<Cfg0>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 1: return launch_cfg<Cfg1>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 2: return launch_cfg<Cfg2>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 3: return launch_cfg<Cfg3>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 4: return launch_cfg<Cfg4>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 5: return launch_cfg<Cfg5>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 6: return launch_cfg<Cfg6>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 7: return launch_cfg<Cfg7>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 8: return launch_cfg<Cfg8>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 9: return launch_cfg<Cfg9>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 10: return launch_cfg<Cfg10>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 11: return launch_cfg<Cfg11>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 12: return launch_cfg<Cfg12>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 13: return launch_cfg<Cfg13>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 14: return launch_cfg<Cfg14>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 15: return launch_cfg<Cfg15>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 16: return launch_cfg<Cfg16>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 17: return launch_cfg<Cfg17>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 18: return launch_cfg<Cfg18>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 19: return launch_cfg<Cfg19>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    case 20: return launch_cfg<Cfg20>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
-    default: return launch_cfg<Cfg21>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, s);
+    case 0: return launch_cfg<Cfg0>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 1: return launch_cfg<Cfg1>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 2: return launch_cfg<Cfg2>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 3: return launch_cfg<Cfg3>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 4: return launch_cfg<Cfg4>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 5: return launch_cfg<Cfg5>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 6: return launch_cfg<Cfg6>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 7: return launch_cfg<Cfg7>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 8: return launch_cfg<Cfg8>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 9: return launch_cfg<Cfg9>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 10: return launch_cfg<Cfg10>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 11: return launch_cfg<Cfg11>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 12: return launch_cfg<Cfg12>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 13: return launch_cfg<Cfg13>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 14: return launch_cfg<Cfg14>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 15: return launch_cfg<Cfg15>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 16: return launch_cfg<Cfg16>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 17: return launch_cfg<Cfg17>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 18: return launch_cfg<Cfg18>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 19: return launch_cfg<Cfg19>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    case 20: return launch_cfg<Cfg20>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
+    default: return launch_cfg<Cfg21>(tasks, cblks, items, nitems, counter, a, b, c, ws, add, drange, dests, s);
     }
 }
 

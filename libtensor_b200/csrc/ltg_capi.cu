@@ -170,6 +170,18 @@ struct ContractExec {
     std::vector<int64_t> sched_slots;
 };
 
+// A symmetrizer of two terms fused into the plain contraction's epilogue:
+// the contraction's own tasks and items (no k chunks, no grouped products),
+// and per scheduled C block the destinations in the symmetrized result (its
+// canonical blocks that take a term of the block, each with the term's index
+// mapping and sign), added atomically into the zeroed result.
+struct SymExec {
+    DevBuf tasks, cblks, items, drange, dests;
+    std::vector<DmmaLaunch> launches;
+    std::vector<int64_t> nonzero_slots;      // result blocks some term reaches
+    int64_t ndests = 0;
+};
+
 // Device arrays of the split-precision path for one (C tensor, coefficients,
 // mode, slice count).
 struct OzExec {
@@ -228,6 +240,9 @@ struct ltg_plan {
     // cache of device task arrays keyed by (C tensor, ka, kb, kc, add, d)
     std::map<std::tuple<uint64_t, double, double, double, int, double>,
              std::unique_ptr<ContractExec>> exec;
+    // fused symmetrizers keyed by (result tensor, symmetrizer, c, ka, kb, kc)
+    std::map<std::tuple<uint64_t, std::vector<int32_t>, double, double, double, double>,
+             std::unique_ptr<struct SymExec>> sym;
 };
 
 struct ltg_graph {
@@ -594,34 +609,31 @@ std::vector<std::pair<int64_t, int64_t>> plain_group_shapes(ltg_plan *pl, ltg_bt
                                                            const std::vector<CBlockTask> &cbt,
                                                            std::vector<int32_t> &group_of);
 
-ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double kc, int add, double d) {
-    auto key = std::make_tuple(c->uid, ka, kb, kc, add, add ? d : 0.0);
-    auto it = pl->exec.find(key);
-    if (it != pl->exec.end()) return it->second.get();
-    if (pl->ctx->capturing) throw error(kErrState, "contraction not prepared before graph capture: call it once outside the capture");
-    std::unique_ptr<ContractExec> ex(new ContractExec());
-    std::vector<GemmTask> tasks;
-    std::vector<CBlockTask> cbt;
-    if (pl->external) external_blocks(pl, ka, kb, kc, tasks, cbt);
-    else contract2_tasks(pl->plan(), pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
-    // Every address a task can form must lie inside its arena.
-    auto span = [](const SubDims &s, bool second) {
-        int64_t m = 0;
-        for (int i = 0; i < s.n; i++) m += (int64_t)(s.ext[i] - 1) * (second ? s.s1[i] : s.s0[i]);
-        return m;
-    };
+// Largest offset a sub-dimension group can add (strides s0, or s1).
+int64_t sub_span(const SubDims &s, bool second) {
+    int64_t m = 0;
+    for (int i = 0; i < s.n; i++) m += (int64_t)(s.ext[i] - 1) * (second ? s.s1[i] : s.s0[i]);
+    return m;
+}
+
+// Device task and C-block arrays of the plain path (post: d in add mode,
+// else 1); every address a task can form must lie inside its arena (c_elems:
+// the C arena's size).
+void plain_task_arrays(const ltg_plan *pl, int64_t c_elems, const std::vector<GemmTask> &tasks,
+                       const std::vector<CBlockTask> &cbt, double post, std::vector<DTask> &dt,
+                       std::vector<DCBlock> &dc) {
     for (const GemmTask &t : tasks) {
-        int64_t amax = t.a_off + span(t.m, false) + span(t.k, false);
-        int64_t bmax = t.b_off + span(t.n, false) + span(t.k, true);
-        int64_t cmax = t.c_off + span(t.m, true) + span(t.n, true);
+        int64_t amax = t.a_off + sub_span(t.m, false) + sub_span(t.k, false);
+        int64_t bmax = t.b_off + sub_span(t.n, false) + sub_span(t.k, true);
+        int64_t cmax = t.c_off + sub_span(t.m, true) + sub_span(t.n, true);
         if (t.a_off < 0 || amax >= pl->a->h.total_elems || t.b_off < 0 || bmax >= pl->b->h.total_elems ||
-            t.c_off < 0 || cmax >= c->h.total_elems)
+            t.c_off < 0 || cmax >= c_elems)
             throw error(kErrState, "contraction task addresses outside an operand arena");
         if (t.m.total() * t.k.total() > pl->a->h.total_elems || t.n.total() * t.k.total() > pl->b->h.total_elems ||
-            t.m.total() * t.n.total() > c->h.total_elems)
+            t.m.total() * t.n.total() > c_elems)
             throw error(kErrBadArg, "contraction task larger than its operands");
     }
-    std::vector<DTask> dt(tasks.size());
+    dt.assign(tasks.size(), DTask());
     for (size_t i = 0; i < tasks.size(); i++) {
         const GemmTask &t = tasks[i];
         DTask &x = dt[i];
@@ -634,8 +646,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
         x.vec_a = vec16_ok(t.a_off, t.m, t.k, false);
         x.vec_b = vec16_ok(t.b_off, t.n, t.k, true);
     }
-    std::vector<DCBlock> dc(cbt.size());
-    double post = add ? d : 1.0;
+    dc.assign(cbt.size(), DCBlock());
     for (size_t e = 0; e < cbt.size(); e++) {
         const CBlockTask &b = cbt[e];
         DCBlock &x = dc[e];
@@ -649,6 +660,22 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
         x.t_begin = b.t_begin; x.t_end = b.t_end;
         for (int32_t t = b.t_begin; t < b.t_end; t++) dt[t].coeff = tasks[t].coeff / c0;
     }
+}
+
+ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double kc, int add, double d) {
+    auto key = std::make_tuple(c->uid, ka, kb, kc, add, add ? d : 0.0);
+    auto it = pl->exec.find(key);
+    if (it != pl->exec.end()) return it->second.get();
+    if (pl->ctx->capturing) throw error(kErrState, "contraction not prepared before graph capture: call it once outside the capture");
+    std::unique_ptr<ContractExec> ex(new ContractExec());
+    std::vector<GemmTask> tasks;
+    std::vector<CBlockTask> cbt;
+    if (pl->external) external_blocks(pl, ka, kb, kc, tasks, cbt);
+    else contract2_tasks(pl->plan(), pl->a->h, pl->b->h, c->h, ka, kb, kc, tasks, cbt);
+    const double post = add ? d : 1.0;
+    std::vector<DTask> dt;
+    std::vector<DCBlock> dc;
+    plain_task_arrays(pl, c->h.total_elems, tasks, cbt, post, dt, dc);
     // small blocks computed as grouped products
     std::vector<int32_t> group_of(cbt.size(), -1);
     if (pl->group_products && !pl->plan().coalesced && !pl->external) {
@@ -694,7 +721,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
             auto f = slot_of_off.find(b.c_off);
             if (f == slot_of_off.end()) throw error(kErrBadArg, "a task's c_off is not the start of a block of C");
             if (in_sched[f->second]) throw error(kErrBadArg, "the tasks of one C block must be consecutive");
-            if (b.c_off + span(b.cm, true) + span(b.cn, true) >= b.c_off + c->h.blk_size[f->second] ||
+            if (b.c_off + sub_span(b.cm, true) + sub_span(b.cn, true) >= b.c_off + c->h.blk_size[f->second] ||
                 b.M * b.N > c->h.blk_size[f->second])
                 throw error(kErrBadArg, "a task's C range leaves its block");
             ex->sched_slots.push_back(f->second);
@@ -2394,52 +2421,208 @@ bool allowed_invariant(const Bis &bis, const Symmetry &sym, const Perm &p) {
 }
 }  // namespace
 
+namespace {
+
+// The space of S-sums of a tensor with block index space bis and symmetry
+// sym: bis with S's generators, the elements of sym's group that map S onto
+// itself, and sym's partition and label rules if S leaves them unchanged.
+void symmetrized_space(const Bis &bis, const Symmetry &sym, int32_t nidx, const int32_t *idx, int32_t symm,
+                       BlockTensorHost &h) {
+    const int n = bis.n;
+    const std::vector<SePerm> S = symmetrizer_group(n, nidx, idx, symm != 0);
+    for (const SePerm &g : S)
+        if (!bis.permuted(g.perm).equals(bis))
+            throw error(kErrBadDims, "symmetrized indexes with different block structure");
+    h.bis = bis;
+    // generators of the symmetrizer's group
+    if (nidx == 4) {
+        for (int k = 1; k < 4; k++) {
+            SePerm q;
+            q.perm = Perm::identity(n);
+            std::swap(q.perm.p[idx[0]], q.perm.p[idx[k]]);
+            q.coeff = symm ? 1.0 : -1.0;
+            h.sym.perm.push_back(q);
+        }
+    } else {
+        h.sym.perm.push_back(S[1]);
+    }
+    // the operand's elements that map the symmetrizer's group onto itself
+    // (h S h^-1 = S) remain symmetries of the sum over S
+    for (const SePerm &x : perm_group_closure(n, sym.perm)) {
+        if (x.perm.is_identity()) continue;
+        const Perm xi = x.perm.inverse();
+        bool normal = true;
+        for (const SePerm &g : S) {
+            Perm c = xi;
+            c.permute(g.perm).permute(x.perm);
+            bool found = false;
+            for (const SePerm &f : S) if (f.perm == c) { found = true; break; }
+            if (!found) { normal = false; break; }
+        }
+        if (normal) h.sym.perm.push_back(x);
+    }
+    // partition and label rules the symmetrizer leaves unchanged
+    bool keep = true;
+    for (const SePerm &g : S) keep = keep && allowed_invariant(bis, sym, g.perm);
+    if (keep) {
+        h.sym.part = sym.part;
+        h.sym.label = sym.label;
+    }
+}
+
+// Sub-dimension groups of one tile axis over the C dims `dims` (in the order
+// the axis enumerates them) with extents ext and strides str: unit extents
+// dropped, neighbours contiguous in str merged.
+SubDims axis_dims(const std::vector<int> &dims, const int64_t *ext, const int64_t *str) {
+    SubDims r;
+    for (int i : dims) {
+        if (ext[i] == 1) continue;
+        if (r.n > 0 && r.s0[r.n - 1] == str[i] * ext[i]) {
+            r.ext[r.n - 1] *= (int32_t)ext[i];
+            r.s0[r.n - 1] = r.s1[r.n - 1] = str[i];
+            continue;
+        }
+        if (r.n == kMaxSub) throw error(kErrUnsupported, "too many sub-dimensions in a symmetrizer term");
+        r.ext[r.n] = (int32_t)ext[i];
+        r.s0[r.n] = r.s1[r.n] = str[i];
+        r.n++;
+    }
+    return r;
+}
+
+// The fused symmetrizer r = c sum_{s in S} sign(s) P_s(T) of the contraction
+// T (coefficients ka, kb, kc) in the plain path, for S of two elements.  The
+// destinations are the terms of plan_transfer's symmetrizer pass read the
+// other way round: result block y and term t read element x_q = y_d, q =
+// T.perm[t.perm[d]], of the canonical contraction block behind t^-1(y), so
+// that block's element x goes to y with the result block's stride of d on
+// its dim q and coefficient c sign(t) (orbit sign).  Each result element has
+// one source per term, so it takes at most two atomic adds onto zero, whose
+// sum does not depend on their order.
+SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int32_t *idx, int32_t symm,
+                     double ka, double kb, double kc) {
+    const int n = pl->plan().bisc.n;
+    const std::vector<SePerm> S = symmetrizer_group(n, nidx, idx, symm != 0);
+    if (S.size() != 2)
+        throw error(kErrUnsupported, "the fused symmetrizer takes an index pair or a unitary permutation");
+    std::vector<int32_t> skey = {nidx, symm != 0 ? 1 : 0};
+    for (int i = 0; i < (nidx < 0 ? n : nidx); i++) skey.push_back(idx[i]);
+    auto key = std::make_tuple(r->uid, skey, c, ka, kb, kc);
+    auto it = pl->sym.find(key);
+    if (it != pl->sym.end()) return it->second.get();
+    if (pl->ctx->capturing) throw error(kErrState, "symmetrizer not prepared before graph capture: call it once outside the capture");
+    // the contraction's result space (no arena: its offsets are not used)
+    BlockTensorHost th;
+    th.bis = pl->plan().bisc;
+    th.sym = pl->plan().symc;
+    th.build_directory();
+    std::vector<GemmTask> tasks;
+    std::vector<CBlockTask> cbt;
+    contract2_tasks(pl->plan(), pl->a->h, pl->b->h, th, ka, kb, kc, tasks, cbt);
+    std::vector<DTask> dt;
+    std::vector<DCBlock> dc;
+    plain_task_arrays(pl, th.total_elems, tasks, cbt, 1.0, dt, dc);
+    // the tile axes: C dims taken from A (m) and from B (n), in C order
+    const Contraction &ct = pl->plan().contr;
+    const int NC = ct.NC(), NA = ct.NA();
+    std::vector<int> mdims, ndims;
+    for (int i = 0; i < NC; i++) (ct.conn[i] < NC + NA ? mdims : ndims).push_back(i);
+    std::map<int64_t, int32_t> e_of;
+    for (size_t e = 0; e < pl->plan().schedule.size(); e++) e_of[pl->plan().schedule[e]] = (int32_t)e;
+    const BlockTensorHost &rh = r->h;
+    std::unique_ptr<SymExec> ex(new SymExec());
+    std::vector<std::vector<DCBlock>> per(cbt.size());
+    int64_t yb[kMaxOrder], xb[kMaxOrder], ext[kMaxOrder], rstr[kMaxOrder], cbi[kMaxOrder], sext[kMaxOrder],
+        dstr[kMaxOrder];
+    for (size_t sl = 0; sl < rh.blk_abs.size(); sl++) {
+        rh.bis.unabs(rh.blk_abs[sl], yb);
+        rh.bis.block_dims(yb, ext);
+        int64_t st = 1;
+        for (int d = n - 1; d >= 0; d--) { rstr[d] = st; st *= ext[d]; }
+        bool any = false;
+        for (const SePerm &t : S) {
+            for (int d = 0; d < n; d++) xb[t.perm.p[d]] = yb[d];
+            const int64_t xa = th.bis.abs(xb);
+            if (!th.orbits.allowed[xa]) continue;
+            const int64_t ca = th.orbits.canon[xa];
+            auto f = e_of.find(ca);
+            if (f == e_of.end()) continue;                       // a zero block of the contraction
+            const int32_t e = f->second;
+            if (cbt[e].t_end <= cbt[e].t_begin) continue;
+            const Transf &T = th.orbits.tr[xa];
+            th.bis.unabs(ca, cbi);
+            th.bis.block_dims(cbi, sext);
+            for (int d = 0; d < n; d++) {
+                const int q = T.perm.p[t.perm.p[d]];
+                if (sext[q] != ext[d]) throw error(kErrState, "symmetrizer term extent mismatch");
+                dstr[q] = rstr[d];
+            }
+            DCBlock y;
+            std::memset(&y, 0, sizeof(y));
+            y.c_off = rh.blk_off[sl];
+            y.scale = dc[e].scale * (c * t.coeff * T.coeff);
+            y.M = dc[e].M;
+            y.N = dc[e].N;
+            const SubDims sm = axis_dims(mdims, sext, dstr), sn = axis_dims(ndims, sext, dstr);
+            if (sm.total() != y.M || sn.total() != y.N) throw error(kErrState, "symmetrizer term shape");
+            pack_sub(sm, y.nm, y.mext, y.mc_str, nullptr);
+            pack_sub(sn, y.nn, y.next, y.nc_str, nullptr);
+            per[e].push_back(y);
+            any = true;
+        }
+        if (any) ex->nonzero_slots.push_back((int64_t)sl);
+    }
+    std::vector<int2> drange(std::max<size_t>(cbt.size(), 1), make_int2(0, 0));
+    std::vector<DCBlock> dests;
+    for (size_t e = 0; e < cbt.size(); e++) {
+        drange[e].x = (int32_t)dests.size();
+        dests.insert(dests.end(), per[e].begin(), per[e].end());
+        drange[e].y = (int32_t)dests.size();
+    }
+    ex->ndests = (int64_t)dests.size();
+    // work items of the C blocks that reach the result, each over its whole
+    // k range (tile shapes as in the plain path)
+    std::vector<std::vector<std::pair<double, DItem>>> per_cfg(kNumShapes);
+    for (size_t e = 0; e < cbt.size(); e++) {
+        if (per[e].empty()) continue;
+        int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(cbt[e].M, cbt[e].N);
+        auto ov = pl->tile_override.find({cbt[e].M, cbt[e].N});
+        if (pl->forced_tile < 0 && ov != pl->tile_override.end()) cfg = ov->second;
+        const int bm = tile_cfg_bm(cfg), bn = tile_cfg_bn(cfg);
+        for (int64_t m0 = 0; m0 < cbt[e].M; m0 += bm)
+            for (int64_t n0 = 0; n0 < cbt[e].N; n0 += bn) {
+                DItem di = make_item((int32_t)e, (int32_t)m0, (int32_t)n0);
+                const double cost = (double)bm * bn * (cbt[e].kflops + 8.0 * (cbt[e].t_end - cbt[e].t_begin));
+                per_cfg[cfg].push_back({cost, di});
+            }
+    }
+    std::vector<DItem> items;
+    std::vector<DSplit> splits;
+    int64_t ws_elems = 0;
+    for (int cfg = 0; cfg < kNumShapes; cfg++)
+        append_launch(cfg, per_cfg[cfg], dt, dc, pl->ctx->nsm, 1, items, splits, ws_elems, ex->launches);
+    if (!splits.empty()) throw error(kErrState, "k chunks in a fused symmetrizer");
+    if (dests.empty()) dests.resize(1);
+    cudaStream_t s = pl->ctx->stream;
+    upload_vec(ex->tasks, dt, s);
+    upload_vec(ex->cblks, dc, s);
+    upload_vec(ex->items, items, s);
+    upload_vec(ex->drange, drange, s);
+    upload_vec(ex->dests, dests, s);
+    SymExec *raw = ex.get();
+    pl->sym[key] = std::move(ex);
+    return raw;
+}
+
+}  // namespace
+
 int ltg_bt_create_symmetrized(ltg_bt *a, int32_t nidx, const int32_t *idx, int32_t symm, ltg_bt **out) {
     return guard([&] {
         check_bt(a);
         if (!out) throw error(kErrBadArg, "null output");
-        const int n = a->h.bis.n;
-        const std::vector<SePerm> S = symmetrizer_group(n, nidx, idx, symm != 0);
-        for (const SePerm &g : S)
-            if (!a->h.bis.permuted(g.perm).equals(a->h.bis))
-                throw error(kErrBadDims, "symmetrized indexes with different block structure");
         std::unique_ptr<ltg_bt> bt(new ltg_bt());
         bt->ctx = a->ctx;
-        bt->h.bis = a->h.bis;
-        // generators of the symmetrizer's group
-        if (nidx == 4) {
-            for (int k = 1; k < 4; k++) {
-                SePerm q;
-                q.perm = Perm::identity(n);
-                std::swap(q.perm.p[idx[0]], q.perm.p[idx[k]]);
-                q.coeff = symm ? 1.0 : -1.0;
-                bt->h.sym.perm.push_back(q);
-            }
-        } else {
-            bt->h.sym.perm.push_back(S[1]);
-        }
-        // the operand's elements that map the symmetrizer's group onto itself
-        // (h S h^-1 = S) remain symmetries of the sum over S
-        for (const SePerm &h : perm_group_closure(n, a->h.sym.perm)) {
-            if (h.perm.is_identity()) continue;
-            const Perm hi = h.perm.inverse();
-            bool normal = true;
-            for (const SePerm &g : S) {
-                Perm c = hi;
-                c.permute(g.perm).permute(h.perm);
-                bool found = false;
-                for (const SePerm &f : S) if (f.perm == c) { found = true; break; }
-                if (!found) { normal = false; break; }
-            }
-            if (normal) bt->h.sym.perm.push_back(h);
-        }
-        // partition and label rules the symmetrizer leaves unchanged
-        bool keep = true;
-        for (const SePerm &g : S) keep = keep && allowed_invariant(a->h.bis, a->h.sym, g.perm);
-        if (keep) {
-            bt->h.sym.part = a->h.sym.part;
-            bt->h.sym.label = a->h.sym.label;
-        }
+        symmetrized_space(a->h.bis, a->h.sym, nidx, idx, symm, bt->h);
         alloc_arena(bt.get());
         *out = bt.release();
     });
@@ -2467,6 +2650,49 @@ int ltg_symmetrize(ltg_bt *a, double c, int32_t nidx, const int32_t *idx, int32_
             const bool first = t0 == 0;
             run_transfer(a->ctx, srcs, ps, cs, b, first ? add != 0 : true, first ? d : (add ? d : 1.0));
         }
+    });
+}
+
+int ltg_contract2_make_symmetrized(ltg_plan *plan, int32_t nidx, const int32_t *idx, int32_t symm, ltg_bt **out) {
+    return guard([&] {
+        if (!plan || !out) throw error(kErrBadArg, "null argument");
+        if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
+        std::unique_ptr<ltg_bt> bt(new ltg_bt());
+        bt->ctx = plan->ctx;
+        symmetrized_space(plan->plan().bisc, plan->plan().symc, nidx, idx, symm, bt->h);
+        alloc_arena(bt.get());
+        *out = bt.release();
+    });
+}
+
+int ltg_contract2_symmetrized(ltg_plan *plan, ltg_bt *r, double c, int32_t nidx, const int32_t *idx, int32_t symm,
+                              double ka, double kb, double kc) {
+    return guard([&] {
+        if (!plan) throw error(kErrBadArg, "null plan");
+        if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
+        check_bt(r);
+        need_dev(plan->ctx);
+        if (!r->h.bis.equals(plan->plan().bisc)) throw error(kErrBadDims, "symmetrizer result of another index space");
+        SymExec *ex = prepare_sym(plan, r, c, nidx, idx, symm, ka, kb, kc);
+        ltg_ctx *ctx = plan->ctx;
+        cudaStream_t s = ctx->stream;
+        // the result starts at zero: every element then takes at most two adds
+        LTG_CUDA(cudaMemsetAsync(r->arena.p, 0, (size_t)std::max<int64_t>(r->h.total_elems, 1) * sizeof(double), s));
+        int slot = 0;
+        for (auto &l : ex->launches) {
+            TimedLaunch tl(ctx, LTG_KERNEL_CONTRACT_FP64);
+            LTG_CUDA(launch_contract_fp64(ex->tasks.as<DTask>(), ex->cblks.as<DCBlock>(),
+                                          ex->items.as<DItem>() + l.item0, l.nitems,
+                                          ctx->scratch_counter.as<int32_t>() + (slot++ % 64),
+                                          plan->a->arena.as<double>(), plan->b->arena.as<double>(),
+                                          r->arena.as<double>(), nullptr, 0, l.cfg, s, ex->drange.as<int2>(),
+                                          ex->dests.as<DCBlock>()));
+            tl.done();
+            ctx->launches++;
+        }
+        std::fill(r->h.nonzero.begin(), r->h.nonzero.end(), 0);
+        for (int64_t sl : ex->nonzero_slots) r->h.nonzero[sl] = 1;
+        if (!ctx->capturing) LTG_CUDA(cudaGetLastError());
     });
 }
 
@@ -3109,6 +3335,7 @@ int ltg_contract2_set_tile(ltg_plan *plan, int32_t cfg) {
         if (cfg < -1 || cfg >= tile_cfg_count()) throw error(kErrBadArg, "tile configuration out of range");
         plan->forced_tile = cfg;
         plan->exec.clear();
+        plan->sym.clear();
     });
 }
 
@@ -3118,6 +3345,7 @@ int ltg_contract2_set_split_k(ltg_plan *plan, int32_t k) {
         if (k < 0 || k > 4) throw error(kErrBadArg, "k chunks per tile must be 0 (automatic) or 1-4");
         plan->split_k = k;
         plan->exec.clear();
+        plan->sym.clear();
     });
 }
 
@@ -3234,6 +3462,7 @@ int ltg_contract2_autotune(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nsli
         LTG_CUDA(cudaEventCreate(&e1));
         auto timed = [&]() {
             plan->exec.clear();
+            plan->sym.clear();
             int st = ltg_contract2(plan, c, mode, nslices, ka, kb, kc, 0, 0.0);   // warm + upload
             if (st != kOk) throw error(st, g_last_error);
             LTG_CUDA(cudaEventRecord(e0, s));
@@ -3259,6 +3488,7 @@ int ltg_contract2_autotune(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nsli
             plan->tile_override[key] = bestc;
         }
         plan->exec.clear();
+        plan->sym.clear();
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     });

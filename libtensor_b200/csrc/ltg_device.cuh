@@ -295,9 +295,13 @@ __host__ __device__ inline double seeded_value(const DGenGroup &g, uint64_t seed
 
 // Plain FP64 DMMA grouped contraction over all work items; partial tiles of
 // k-split items go to ws (BM x BN doubles per slot).
+// With dests (and drange, one index range of dests per C block), every C
+// block's tile is added atomically to its destinations instead of being
+// written (no k chunks: every item covers its whole k range).
 cudaError_t launch_contract_fp64(const DTask *tasks, const DCBlock *cblks,
     const DItem *items, int32_t nitems, int32_t *counter, const double *a,
-    const double *b, double *c, double *ws, int32_t add, int32_t tile_cfg, cudaStream_t s);
+    const double *b, double *c, double *ws, int32_t add, int32_t tile_cfg, cudaStream_t s,
+    const int2 *drange = nullptr, const DCBlock *dests = nullptr);
 // Sums the partial tiles of every split tile in chunk order and writes (or
 // adds) the scaled result into its C block.
 cudaError_t launch_split_reduce(const DSplit *splits, int32_t nsplits, const DCBlock *cblks,

@@ -179,6 +179,11 @@ int main(int argc, char **argv) {
         ys(i|j|a|b) = symm(i|a, j|b, r(i|j|a|b));             // = 2 r
         gs(i|j|a|b) = asymm(a, b, contract(c1, t(i|j|a|c1), fl(c1|b)));
         btod_symmetrize2<4>(ge, 2, 3, false).perform(gse);
+        // the same symmetrizer over the contraction itself: both terms written
+        // by the contraction's epilogue, no temporary
+        block_tensor<4, double> gsf(bis_r);
+        btod_contract2<3, 1, 1> gop(c1c, t, fe);
+        btod_symmetrize2<4>(gop, 2, 3, false).perform(gsf);
         // intermediates: a contraction of a contraction, a contraction of a sum
         // (terms with the same symmetry, and with a spin-only term, whose sum
         // keeps only the common symmetry), the result on the right-hand side,
@@ -272,7 +277,7 @@ int main(int argc, char **argv) {
                                 max_diff(gse, gs, 1.0), graph_diff,
                                 max_diff(nl, ne, 1.0), max_diff(ql, qe, 1.0), max_diff(wl, we, 1.0),
                                 max_diff(r, hr, 0.5), std::fabs(dl_sum - dot_tt - dot_ts), asg_diff,
-                                (double)asg.operations(), c3_diff};
+                                (double)asg.operations(), c3_diff, max_diff(gsf, gse, 1.0)};
 
         // the contraction's non-zero blocks in index order, then the dot products
         FILE *f = std::fopen(argv[2], "wb");

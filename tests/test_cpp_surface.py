@@ -82,3 +82,7 @@ def test_surface_compute_matches_golden(exe, tmp_path):
     assert d[15] == 0.0
     assert d[16] == 2                                   # the add into the intermediate, the contraction
     assert d[17] == 0.0                                 # btod_contract3, direct_block_tensor = explicit ops
+    # btod_symmetrize2 over the contraction (fused into its epilogue) against
+    # the symmetrizer over the contraction's result (same terms; the k
+    # summation of the contraction may be cut differently)
+    assert d[18] <= 1e-15 * gmax

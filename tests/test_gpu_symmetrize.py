@@ -120,3 +120,86 @@ def test_symmetrize4_matches_dense(gctx, symm):
     # the result space has the symmetric group of the four indexes: with two
     # blocks per index, one canonical block per number of second blocks
     assert len(b.abs_idx) == 5
+
+
+def _ring_op(gctx, cfg):
+    c = cfg.contraction
+    A, B = block_tensor(gctx, cfg.t_spec()), block_tensor(gctx, cfg.w_spec())
+    A.fill_seeded(11, cfg.t_scale)
+    B.fill_seeded(23, cfg.v_scale)
+    contr = contraction2(c["n"], c["m"], c["k"], c["permc"])
+    for p in c["pairs"]:
+        contr.contract(*p)
+    return A, B, btod_contract2(contr, A, B)
+
+
+@pytest.mark.parametrize("kw", [CASES[0], CASES[2]], ids=[IDS[0], IDS[2]])
+def test_fused_symmetrize_contraction_matches_reference(gctx, kw):
+    """The ring term antisymmetrized with both terms written by the
+    contraction kernel's epilogue (ltg_contract2_symmetrized, no temporary)
+    against the reference's btod_symmetrize2 wrapping its btod_contract2:
+    the same non-zero blocks, every block within 1e-13; two calls give the
+    same bits (two adds per element onto zero)."""
+    cfg = S.RING_D2H_SMALL
+    A, B, op = _ring_op(gctx, cfg)
+    out = op.make_symmetrized(**kw)
+    op.perform_symmetrized(out, **kw)
+    gctx.synchronize()
+    got = out.download().copy()
+    op.perform_symmetrized(out, **kw)
+    gctx.synchronize()
+    assert np.array_equal(out.download(), got)
+    c = cfg.contraction
+    ra, rb = R.RefBT(cfg.t_spec()), R.RefBT(cfg.w_spec())
+    ra.fill_seeded(11, cfg.t_scale)
+    rb.fill_seeded(23, cfg.v_scale)
+    rop = R.RefContract2(c["n"], c["m"], c["k"], c["permc"], c["pairs"], ra, rb)
+    rout = rop.make_result()
+    rop.symmetrize(rout, **kw)
+    assert out.nonzero() == rout.nonzero()
+    assert max_rel_block_error(block_errors(out, got, rout, None)) <= 1e-13
+    out.close(); op.close(); A.close(); B.close()
+
+
+@pytest.mark.parametrize("kw", CASES, ids=IDS)
+def test_fused_symmetrize_equals_symmetrizer_of_result(gctx, kw):
+    """Fused and unfused forms of the same symmetrizer over the ring term and
+    over the ladder (whose result is antisymmetric already, so its orbit
+    signs enter every term) agree to rounding; a scale c applies to both
+    terms."""
+    for cfg in (S.RING_D2H_SMALL, S.LADDER_SMALL):
+        if cfg is S.RING_D2H_SMALL:
+            A, B, op = _ring_op(gctx, cfg)
+        else:
+            c = cfg.contraction
+            A, B = block_tensor(gctx, cfg.t_spec()), block_tensor(gctx, cfg.v_spec())
+            A.fill_seeded(11, cfg.t_scale)
+            B.fill_seeded(23, cfg.v_scale)
+            contr = contraction2(c["n"], c["m"], c["k"], c["permc"])
+            for p in c["pairs"]:
+                contr.contract(*p)
+            op = btod_contract2(contr, A, B, kc=cfg.kc)
+        G = op.make_result()
+        op.perform(G)
+        sy = btod_symmetrize(G, c=0.5, **kw)
+        want_t = sy.make_result()
+        sy.perform(want_t)
+        out = op.make_symmetrized(**kw)
+        op.perform_symmetrized(out, c=0.5, **kw)
+        gctx.synchronize()
+        got, want = out.download(), want_t.download()
+        assert np.array_equal(out.abs_idx, want_t.abs_idx)
+        assert out.nonzero() == want_t.nonzero()
+        scale = max(1e-300, float(np.max(np.abs(want))))
+        assert float(np.max(np.abs(got - want))) <= 1e-14 * scale, cfg.name
+        for t in (out, want_t, G, op, A, B):
+            t.close()
+
+
+def test_fused_symmetrize_rejects_four_indexes(gctx):
+    cfg = S.RING_D2H_SMALL
+    A, B, op = _ring_op(gctx, cfg)
+    out = op.make_symmetrized(True, idx=(0, 1))
+    with pytest.raises(Exception):
+        op.perform_symmetrized(out, True, idx=(0, 1, 2, 3))
+    out.close(); op.close(); A.close(); B.close()
