@@ -86,6 +86,10 @@ def parse():
     p.add_argument("--fused-split", type=int, default=0, choices=[0, 1, 2],
                    help="modular mode: one-read split of row families in kernel shape 1 or 2 (0: exponent and "
                         "residue passes)")
+    p.add_argument("--symmetrize", default="", choices=["", "asymm01", "asymm-p0123"],
+                   help="plain mode: also time the result antisymmetrized over indexes (0,1) or the pair "
+                        "exchange (0 1)(2 3), fused into the contraction's epilogue against the contraction "
+                        "followed by the symmetrizer pass")
     p.add_argument("--crt-stage", type=int, default=0, choices=[0, 2, 3, 4, 6],
                    help="modular mode: k blocks per products pipeline stage (0: default)")
     p.add_argument("--tile", type=int, default=-1, help="force one tile shape (debug)")
@@ -374,6 +378,45 @@ def ltg_arm(args):
                              "ms_per_step": sms}
             if rank == 0:
                 results[sname] = C.download()
+    # symmetrizer companion (plain mode): fused into the contraction epilogue
+    # against the contraction into a temporary followed by the symmetrizer
+    symm = None
+    if mode == 0 and args.symmetrize:
+        from libtensor_b200.core import btod_symmetrize
+        kw = dict(symm=False, idx=(0, 1)) if args.symmetrize == "asymm01" else dict(symm=False, perm=(1, 0, 3, 2))
+        Rf = op.make_symmetrized(**kw)
+        G = op.make_result()
+        sy = btod_symmetrize(G, **kw)
+        Ru = sy.make_result()
+
+        def timed(fn):
+            for _ in range(3):
+                fn()
+            barrier()
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record(stream)
+            for _ in range(args.steps):
+                fn()
+            q1.record(stream)
+            barrier()
+            return max_over_ranks([q0.elapsed_time(q1) / args.steps], dev, world)[0]
+
+        def unfused():
+            op.perform(G)
+            sy.perform(Ru)
+        fms = timed(lambda: op.perform_symmetrized(Rf, **kw))
+        ums = timed(unfused)
+        diff = None
+        if rank == 0:
+            # relative to the contraction's largest element (a symmetrizer
+            # whose terms cancel leaves a result of rounding size)
+            a, b = Rf.download(), Ru.download()
+            diff = float(np.max(np.abs(a - b))) / max(1e-300, float(np.max(np.abs(G.download()))))
+        symm = {"terms": args.symmetrize, "fused_ms": fms, "unfused_ms": ums,
+                "fused_vs_unfused": ums / fms, "max_diff_rel_to_contraction": diff,
+                "temporary_bytes_saved": 8 * G.nelems}
+        for t in (Rf, Ru, G):
+            t.close()
     ms = max_over_ranks([ms], dev, world)[0]
     value = replica_rate(flops, ms, world) / 1e12
 
@@ -433,6 +476,8 @@ def ltg_arm(args):
         out["split_vs_plain"] = value / plain["value"]
     if slices:
         out["slice_modes"] = slices
+    if symm:
+        out["symmetrizer"] = symm
     if accuracy:
         out["accuracy"] = accuracy
     print(json.dumps(out))

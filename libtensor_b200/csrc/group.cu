@@ -95,6 +95,40 @@ scatter_groups_kernel(const DCrtComp *__restrict__ comps, const int64_t *__restr
     }
 }
 
+// The same rows, each element added (atomically, into a zeroed result) to
+// the destinations of its cell: dcells[drange[cell].x .. drange[cell].y),
+// each a block of another tensor with its own strides, times dcoef (the
+// terms of a symmetrizer over the contraction).
+__global__ void __launch_bounds__(256)
+scatter_groups_dest_kernel(const DCrtComp *__restrict__ comps, const int64_t *__restrict__ res_off,
+                           const int32_t *__restrict__ ctab, const int2 *__restrict__ drange,
+                           const DCrtCell *__restrict__ dcells, const double *__restrict__ dcoef,
+                           const int2 *__restrict__ units, int32_t nunits, const double *__restrict__ buf,
+                           double *__restrict__ R, double scale) {
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int2 un = units[u];
+        const DCrtComp cc = comps[un.x];
+        const int m = un.y;
+        const int32_t *re = ctab + cc.row_off + (1 + kCrtSideDims) * m;
+        const int rb = re[0];
+        const double *src = buf + res_off[un.x] + (int64_t)m * cc.cols;
+        for (int n = threadIdx.x; n < cc.cols; n += blockDim.x) {
+            const int32_t *ce = ctab + cc.col_off + (1 + kCrtSideDims) * n;
+            const int cell = ctab[cc.cell_off + rb * cc.ncb + ce[0]];
+            if (cell < 0) continue;
+            const int2 dr = drange[cell];
+            const double v = scale * src[n];
+            for (int d = dr.x; d < dr.y; d++) {
+                const DCrtCell &dl = dcells[d];
+                int64_t off = dl.c_off;
+#pragma unroll
+                for (int k = 0; k < kCrtSideDims; k++) off += (int64_t)re[1 + k] * dl.ms[k] + (int64_t)ce[1 + k] * dl.ns[k];
+                atomicAdd(R + off, dcoef[d] * v);
+            }
+        }
+    }
+}
+
 int g_group_nsm = 0;
 
 int group_sms() {
@@ -122,6 +156,17 @@ cudaError_t launch_scatter_groups(const DCrtComp *comps, const int64_t *res_off,
     if (nunits <= 0) return cudaSuccess;
     const int grid = nunits < 8 * group_sms() ? nunits : 8 * group_sms();
     scatter_groups_kernel<<<grid, 256, 0, s>>>(comps, res_off, ctab, cells, units, nunits, buf, c, scale, add);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_groups_dest(const DCrtComp *comps, const int64_t *res_off, const int32_t *ctab,
+                                       const int2 *drange, const DCrtCell *dcells, const double *dcoef,
+                                       const int2 *units, int32_t nunits, const double *buf, double *r,
+                                       double scale, cudaStream_t s) {
+    if (nunits <= 0) return cudaSuccess;
+    const int grid = nunits < 8 * group_sms() ? nunits : 8 * group_sms();
+    scatter_groups_dest_kernel<<<grid, 256, 0, s>>>(comps, res_off, ctab, drange, dcells, dcoef, units, nunits, buf,
+                                                    r, scale);
     return cudaGetLastError();
 }
 

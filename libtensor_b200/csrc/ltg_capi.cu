@@ -178,6 +178,10 @@ struct ContractExec {
 struct SymExec {
     DevBuf tasks, cblks, items, drange, dests;
     std::vector<DmmaLaunch> launches;
+    // small blocks as the plain path's grouped products, their results
+    // scattered from the group buffer to each cell's destinations
+    std::unique_ptr<PlainGroups> groups;
+    DevBuf gdrange, gdcells, gdcoef;
     std::vector<int64_t> nonzero_slots;      // result blocks some term reaches
     int64_t ndests = 0;
 };
@@ -603,8 +607,9 @@ void pack_sub(const SubDims &s, int32_t &n, int32_t *ext, int32_t *str0, int32_t
 void external_blocks(const ltg_plan *pl, double ka, double kb, double kc, std::vector<GemmTask> &tasks,
                      std::vector<CBlockTask> &cbt);
 
-void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &cbt, double kabc, double post,
-                        std::vector<int32_t> &group_of, PlainGroups &pg);
+void build_plain_groups(ltg_plan *pl, const BlockTensorHost &ch, const std::vector<CBlockTask> &cbt, double kabc,
+                        double post, std::vector<int32_t> &group_of, PlainGroups &pg,
+                        std::vector<DCrtCell> *cells_out = nullptr);
 std::vector<std::pair<int64_t, int64_t>> plain_group_shapes(ltg_plan *pl, ltg_bt *c,
                                                            const std::vector<CBlockTask> &cbt,
                                                            std::vector<int32_t> &group_of);
@@ -680,7 +685,7 @@ ContractExec *prepare_exec(ltg_plan *pl, ltg_bt *c, double ka, double kb, double
     std::vector<int32_t> group_of(cbt.size(), -1);
     if (pl->group_products && !pl->plan().coalesced && !pl->external) {
         ex->groups.reset(new PlainGroups());
-        build_plain_groups(pl, c, cbt, ka * kb * kc, post, group_of, *ex->groups);
+        build_plain_groups(pl, c->h, cbt, ka * kb * kc, post, group_of, *ex->groups);
         if (ex->groups->ngroups == 0) ex->groups.reset();
     }
     // Work items per tile configuration, costliest first (LPT order for the
@@ -1276,12 +1281,15 @@ void external_blocks(const ltg_plan *pl, double ka, double kb, double kc, std::v
     }
 }
 
-void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &cbt, double kabc, double post,
-                        std::vector<int32_t> &group_of, PlainGroups &pg) {
+// ch: the result's space (its block offsets go into the cells); cells_out:
+// the cells' host copy, in cell order.
+void build_plain_groups(ltg_plan *pl, const BlockTensorHost &ch, const std::vector<CBlockTask> &cbt, double kabc,
+                        double post, std::vector<int32_t> &group_of, PlainGroups &pg,
+                        std::vector<DCrtCell> *cells_out) {
     CrtSideMap sm[2];
-    crt_side_maps(pl->plan().contr, c->h, sm);
+    crt_side_maps(pl->plan().contr, ch, sm);
     std::vector<CrtGroupHost> groups;
-    crt_groups(pl, c->h, sm, cbt, groups, group_of);
+    crt_groups(pl, ch, sm, cbt, groups, group_of);
     if (groups.empty()) return;
     std::vector<DGather> pieces;
     std::vector<int4> units;
@@ -1339,7 +1347,7 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
         for (const auto &x : G.bc)
             piece(1, x.second, lay.boff + lay.sofs[x.first.second] * lay.kt + lay.kofs[x.first.first],
                   G.sn[x.first.second], G.kn[x.first.first]);
-        comps.push_back(crt_group_tables(pl, c->h, sm, cbt, G, ctab, cells));
+        comps.push_back(crt_group_tables(pl, ch, sm, cbt, G, ctab, cells));
         res_off.push_back(lay.coff);
         for (int64_t m = 0; m < lay.rows; m++) sunits.push_back(make_int2((int32_t)gi, (int32_t)m));
         // the dense product: result[m][n] = sum_k A[m][k] B[n][k]
@@ -1383,6 +1391,7 @@ void build_plain_groups(ltg_plan *pl, ltg_bt *c, const std::vector<CBlockTask> &
     pg.buf.alloc(std::max<int64_t>(off, 4) * (int64_t)sizeof(double));
     // cells that no pair uses stay zero
     LTG_CUDA(cudaMemsetAsync(pg.buf.p, 0, std::max<int64_t>(off, 4) * sizeof(double), s));
+    if (cells_out) *cells_out = cells;
     if (cells.empty()) cells.resize(1);
     upload_vec(pg.pieces, pieces, s);
     upload_vec(pg.units, units, s);
@@ -2532,6 +2541,14 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int3
     const BlockTensorHost &rh = r->h;
     std::unique_ptr<SymExec> ex(new SymExec());
     std::vector<std::vector<DCBlock>> per(cbt.size());
+    // the same destinations per dim (result block offset, stride of each
+    // contraction dim, coefficient), for the grouped products' cells
+    struct DestRec {
+        int64_t off;
+        int64_t dstr[kMaxOrder];
+        double coef;
+    };
+    std::vector<std::vector<DestRec>> praw(cbt.size());
     int64_t yb[kMaxOrder], xb[kMaxOrder], ext[kMaxOrder], rstr[kMaxOrder], cbi[kMaxOrder], sext[kMaxOrder],
         dstr[kMaxOrder];
     for (size_t sl = 0; sl < rh.blk_abs.size(); sl++) {
@@ -2568,6 +2585,11 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int3
             pack_sub(sm, y.nm, y.mext, y.mc_str, nullptr);
             pack_sub(sn, y.nn, y.next, y.nc_str, nullptr);
             per[e].push_back(y);
+            DestRec q;
+            q.off = rh.blk_off[sl];
+            for (int d = 0; d < kMaxOrder; d++) q.dstr[d] = d < n ? dstr[d] : 0;
+            q.coef = c * t.coeff * T.coeff;
+            praw[e].push_back(q);
             any = true;
         }
         if (any) ex->nonzero_slots.push_back((int64_t)sl);
@@ -2580,11 +2602,50 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int3
         drange[e].y = (int32_t)dests.size();
     }
     ex->ndests = (int64_t)dests.size();
-    // work items of the C blocks that reach the result, each over its whole
-    // k range (tile shapes as in the plain path)
+    // small blocks grouped as in the plain path (products into the group
+    // buffer; each cell's elements then go to its C block's destinations)
+    std::vector<int32_t> group_of(cbt.size(), -1);
+    if (pl->group_products && !pl->plan().coalesced) {
+        std::vector<DCrtCell> gcells;
+        ex->groups.reset(new PlainGroups());
+        build_plain_groups(pl, th, cbt, ka * kb * kc, 1.0, group_of, *ex->groups, &gcells);
+        if (ex->groups->ngroups == 0) {
+            ex->groups.reset();
+        } else {
+            std::map<int64_t, int32_t> e_of_off;
+            for (size_t e = 0; e < cbt.size(); e++) e_of_off[cbt[e].c_off] = (int32_t)e;
+            CrtSideMap sm[2];
+            crt_side_maps(ct, th, sm);
+            std::vector<int2> gdr(std::max<size_t>(gcells.size(), 1), make_int2(0, 0));
+            std::vector<DCrtCell> gdc;
+            std::vector<double> gco;
+            for (size_t ci = 0; ci < gcells.size(); ci++) {
+                auto f = e_of_off.find(gcells[ci].c_off);
+                if (f == e_of_off.end() || group_of[f->second] < 0) throw error(kErrState, "grouped cell without its C block");
+                gdr[ci].x = (int32_t)gdc.size();
+                for (const DestRec &q : praw[f->second]) {
+                    DCrtCell d;
+                    std::memset(&d, 0, sizeof(d));
+                    d.c_off = q.off;
+                    for (size_t k = 0; k < sm[0].dims.size(); k++) d.ms[k] = (int32_t)q.dstr[sm[0].dims[k]];
+                    for (size_t k = 0; k < sm[1].dims.size(); k++) d.ns[k] = (int32_t)q.dstr[sm[1].dims[k]];
+                    gdc.push_back(d);
+                    gco.push_back(q.coef);
+                }
+                gdr[ci].y = (int32_t)gdc.size();
+            }
+            if (gdc.empty()) { gdc.resize(1); gco.resize(1); }
+            cudaStream_t gs = pl->ctx->stream;
+            upload_vec(ex->gdrange, gdr, gs);
+            upload_vec(ex->gdcells, gdc, gs);
+            upload_vec(ex->gdcoef, gco, gs);
+        }
+    }
+    // work items of the other C blocks that reach the result, each over its
+    // whole k range (tile shapes as in the plain path)
     std::vector<std::vector<std::pair<double, DItem>>> per_cfg(kNumShapes);
     for (size_t e = 0; e < cbt.size(); e++) {
-        if (per[e].empty()) continue;
+        if (per[e].empty() || group_of[e] >= 0) continue;
         int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(cbt[e].M, cbt[e].N);
         auto ov = pl->tile_override.find({cbt[e].M, cbt[e].N});
         if (pl->forced_tile < 0 && ov != pl->tile_override.end()) cfg = ov->second;
@@ -2679,6 +2740,38 @@ int ltg_contract2_symmetrized(ltg_plan *plan, ltg_bt *r, double c, int32_t nidx,
         // the result starts at zero: every element then takes at most two adds
         LTG_CUDA(cudaMemsetAsync(r->arena.p, 0, (size_t)std::max<int64_t>(r->h.total_elems, 1) * sizeof(double), s));
         int slot = 0;
+        if (PlainGroups *pg = ex->groups.get()) {
+            TimedLaunch tg(ctx, LTG_KERNEL_TRANSFER);
+            LTG_CUDA(launch_gather_cells(pg->pieces.as<DGather>(), pg->units.as<int4>(), pg->nunits,
+                                         plan->a->arena.as<double>(), plan->b->arena.as<double>(),
+                                         pg->buf.as<double>(), s));
+            tg.done();
+            ctx->launches++;
+            for (auto &l : pg->launches) {
+                TimedLaunch tl(ctx, LTG_KERNEL_CONTRACT_FP64);
+                LTG_CUDA(launch_contract_fp64(pg->tasks.as<DTask>(), pg->cblks.as<DCBlock>(),
+                                              pg->items.as<DItem>() + l.item0, l.nitems,
+                                              ctx->scratch_counter.as<int32_t>() + (slot++ % 64),
+                                              pg->buf.as<double>(), pg->buf.as<double>(), pg->buf.as<double>(),
+                                              pg->ws.as<double>() + l.ws_off, 0, l.cfg, s));
+                if (l.nsplits > 0) {
+                    LTG_CUDA(launch_split_reduce(pg->splits.as<DSplit>() + l.split0, l.nsplits, pg->cblks.as<DCBlock>(),
+                                                 pg->ws.as<double>() + l.ws_off, tile_cfg_bm(l.cfg),
+                                                 tile_cfg_bn(l.cfg), pg->buf.as<double>(), 0, s));
+                    ctx->launches++;
+                }
+                tl.done();
+                ctx->launches++;
+            }
+            TimedLaunch ts(ctx, LTG_KERNEL_TRANSFER);
+            LTG_CUDA(launch_scatter_groups_dest(pg->comps.as<DCrtComp>(), pg->res_off.as<int64_t>(),
+                                                pg->ctab.as<int32_t>(), ex->gdrange.as<int2>(),
+                                                ex->gdcells.as<DCrtCell>(), ex->gdcoef.as<double>(),
+                                                pg->sunits.as<int2>(), pg->nsunits, pg->buf.as<double>(),
+                                                r->arena.as<double>(), pg->scale, s));
+            ts.done();
+            ctx->launches++;
+        }
         for (auto &l : ex->launches) {
             TimedLaunch tl(ctx, LTG_KERNEL_CONTRACT_FP64);
             LTG_CUDA(launch_contract_fp64(ex->tasks.as<DTask>(), ex->cblks.as<DCBlock>(),

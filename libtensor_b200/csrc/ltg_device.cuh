@@ -367,6 +367,11 @@ cudaError_t launch_gather_cells(const DGather *pieces, const int4 *units, int32_
 cudaError_t launch_scatter_groups(const DCrtComp *comps, const int64_t *res_off, const int32_t *ctab,
     const DCrtCell *cells, const int2 *units, int32_t nunits, const double *buf, double *c,
     double scale, int32_t add, cudaStream_t s);
+// The group results added atomically (into a zeroed r) to the destinations
+// of each cell: dcells[drange[cell].x .. .y) times dcoef.
+cudaError_t launch_scatter_groups_dest(const DCrtComp *comps, const int64_t *res_off, const int32_t *ctab,
+    const int2 *drange, const DCrtCell *dcells, const double *dcoef, const int2 *units, int32_t nunits,
+    const double *buf, double *r, double scale, cudaStream_t s);
 
 // Element-wise transfer kernels.  max_terms bounds nterms and tile_bytes the
 // shared-memory tiles of any tiled-mode job.
