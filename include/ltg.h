@@ -155,16 +155,18 @@ int ltg_symmetrize(ltg_bt *a, double c, int32_t nidx, const int32_t *idx, int32_
  * btod_contract2, libtensor/block_tensor/btod_symmetrize2.h:19,
  * gen_block_tensor/impl/gen_bto_symmetrize2_impl.h): r = c (T + sign P(T)),
  * T the plan's contraction with coefficients ka, kb, kc, S = {e, P} as in
- * ltg_symmetrize (nidx 2 or -1).  The plain FP64 kernel's epilogue adds each
- * tile of T straight into the canonical blocks of r that its two terms
- * reach (no temporary T); r is zeroed first, so every element takes at most
- * two adds and the result does not depend on their order.  Assignment only
- * (ltg_symmetrize over a formed T adds).  ltg_contract2_make_symmetrized:
- * a tensor with the space of such sums (as ltg_bt_create_symmetrized over
- * the contraction's result). */
+ * ltg_symmetrize (nidx 2 or -1), in mode LTG_MODE_PLAIN_FP64 or
+ * LTG_MODE_OZAKI_CRT (nslices moduli, 0: 13).  The kernel that writes T's
+ * elements -- the plain DMMA epilogue, the grouped products' scatter, or the
+ * modular recombination -- adds each of them straight into the canonical
+ * blocks of r that its two terms reach (no temporary T); r is zeroed first,
+ * so every element takes at most two adds and the result does not depend on
+ * their order.  Assignment only (ltg_symmetrize over a formed T adds).
+ * ltg_contract2_make_symmetrized: a tensor with the space of such sums (as
+ * ltg_bt_create_symmetrized over the contraction's result). */
 int ltg_contract2_make_symmetrized(ltg_plan *plan, int32_t nidx, const int32_t *idx, int32_t symm, ltg_bt **out);
-int ltg_contract2_symmetrized(ltg_plan *plan, ltg_bt *r, double c, int32_t nidx, const int32_t *idx, int32_t symm,
-                              double ka, double kb, double kc);
+int ltg_contract2_symmetrized(ltg_plan *plan, ltg_bt *r, int32_t mode, int32_t nslices, double c, int32_t nidx,
+                              const int32_t *idx, int32_t symm, double ka, double kb, double kc);
 int ltg_bt_destroy(ltg_bt *bt);
 /* Canonical allowed blocks: count and packed arena size in elements. */
 int ltg_bt_info(const ltg_bt *bt, int32_t *order, int64_t *nblocks, int64_t *nelems);

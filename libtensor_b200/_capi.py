@@ -62,8 +62,8 @@ _SIGS = {
     "ltg_bt_create_symmetrized": (C.c_int, [c_vp, C.c_int32, c_i32p, C.c_int32, C.POINTER(c_vp)]),
     "ltg_symmetrize": (C.c_int, [c_vp, C.c_double, C.c_int32, c_i32p, C.c_int32, c_vp, C.c_int32, C.c_double]),
     "ltg_contract2_make_symmetrized": (C.c_int, [c_vp, C.c_int32, c_i32p, C.c_int32, C.POINTER(c_vp)]),
-    "ltg_contract2_symmetrized": (C.c_int, [c_vp, c_vp, C.c_double, C.c_int32, c_i32p, C.c_int32, C.c_double,
-                                            C.c_double, C.c_double]),
+    "ltg_contract2_symmetrized": (C.c_int, [c_vp, c_vp, C.c_int32, C.c_int32, C.c_double, C.c_int32, c_i32p,
+                                            C.c_int32, C.c_double, C.c_double, C.c_double]),
     "ltg_bt_destroy": (C.c_int, [c_vp]),
     "ltg_bt_info": (C.c_int, [c_vp, c_i32p, c_i64p, c_i64p]),
     "ltg_bt_blocks": (C.c_int, [c_vp, c_i64p, c_i64p, c_i64p]),

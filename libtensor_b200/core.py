@@ -318,12 +318,14 @@ class btod_contract2:
         check(lib().ltg_contract2_make_symmetrized(self.h, nidx, arr, 1 if symm else 0, C.byref(h)))
         return block_tensor(self.a.ctx, None, _handle=h)
 
-    def perform_symmetrized(self, r: block_tensor, symm: bool, idx=(), perm=None, c: float = 1.0):
-        """r = c (T + sign P(T)) with T this contraction (plain FP64), the
-        two terms written by the contraction kernel's epilogue straight into
-        r (ltg_contract2_symmetrized; btod_symmetrize2 over btod_contract2)."""
+    def perform_symmetrized(self, r: block_tensor, symm: bool, idx=(), perm=None, c: float = 1.0,
+                            mode: int = 0, nslices: int = 0):
+        """r = c (T + sign P(T)) with T this contraction (plain FP64, or the
+        modular mode), both terms written by the kernel that forms T's
+        elements straight into r (ltg_contract2_symmetrized; btod_symmetrize2
+        over btod_contract2)."""
         nidx, arr = _symm_args(self.contr.n + self.contr.m, idx, perm)
-        check(lib().ltg_contract2_symmetrized(self.h, r.h, c, nidx, arr, 1 if symm else 0,
+        check(lib().ltg_contract2_symmetrized(self.h, r.h, mode, nslices, c, nidx, arr, 1 if symm else 0,
                                               self.ka, self.kb, self.kc))
 
     def set_tile(self, cfg: int):

@@ -891,7 +891,13 @@ constexpr int kCombCols = 16;                       // tile columns staged per p
 // and column; grouped products: the block and coordinates, combined with the
 // C block's strides per element); then one thread per element runs Garner
 // and writes C.
-template<int L>
+// SCATTER: each element goes, by atomic adds into a zeroed result, to its C
+// block's destinations instead -- blocks of another tensor with their own
+// index mappings and coefficients (the terms of a symmetrizer over the
+// contraction): dests[drange[cblk]] for a C block of its own (their row and
+// column offsets staged like soff), gdcells[gdrange[cell]] with gdcoef for
+// a cell of a grouped product.
+template<int L, bool SCATTER>
 __global__ void __launch_bounds__(256)
 crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restrict__ items, int32_t nitems,
                    const DCBlock *__restrict__ cblks, const DCrtComp *__restrict__ comps,
@@ -899,8 +905,12 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
                    const uint8_t *__restrict__ out, const int32_t *__restrict__ gidx,
                    const int32_t *__restrict__ ex, const int32_t *__restrict__ ey,
                    const int32_t *__restrict__ ext, const int32_t *__restrict__ eyt, double *__restrict__ C,
-                   int32_t add, double scale, const CrtParams cp) {
+                   int32_t add, double scale, const CrtParams cp, const int2 *__restrict__ drange,
+                   const DCBlock *__restrict__ dests, const int2 *__restrict__ gdrange,
+                   const DCrtCell *__restrict__ gdcells, const double *__restrict__ gdcoef) {
+    constexpr int kTab = kXRows + kCombCols;
     __shared__ __align__(16) uint8_t sres[L][kXRows][kCombCols];
+    __shared__ int64_t sdoff[SCATTER ? kCrtMaxDests * kTab : 1];  // SCATTER: each destination's offsets
     __shared__ int64_t soff[kXRows + kCombCols];               // one C block: row / column offsets
     __shared__ int32_t sexp[kXRows + kCombCols];               // exponents of tile rows / columns
     __shared__ int32_t sco[kXRows + kCombCols][1 + kCrtSideDims];   // grouped: block, coordinates
@@ -915,6 +925,14 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
         if (xh >= item.nx || c0 >= yc) continue;                     // uniform over the CTA
         const int xb = item.x0 + xh * kXRows;                        // first row of this half
         const int xr = min(kXRows, xext - xb);
+        int d0 = 0, nd = 0;                                          // SCATTER: the C block's destinations
+        if constexpr (SCATTER) {
+            if (!cc) {
+                const int2 dr = drange[item.cblk];
+                d0 = dr.x;
+                nd = min(dr.y - dr.x, kCrtMaxDests);
+            }
+        }
         __syncthreads();                                             // the previous unit is done
         for (int i = threadIdx.x; i < L * kXRows; i += blockDim.x) {
             const int l = i / kXRows, r = i - l * kXRows;
@@ -937,6 +955,12 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
             } else {
                 soff[i] = crow ? mixed_offset(idx, cb1->nm, cb1->mext, cb1->mc_str)
                                : mixed_offset(idx, cb1->nn, cb1->next, cb1->nc_str);
+                if constexpr (SCATTER)
+                    for (int d = 0; d < nd; d++) {
+                        const DCBlock &db = dests[d0 + d];
+                        sdoff[d * kTab + i] = crow ? mixed_offset(idx, db.nm, db.mext, db.mc_str)
+                                                   : mixed_offset(idx, db.nn, db.next, db.nc_str);
+                    }
             }
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -946,17 +970,22 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
             if (cp.swap) { r = e & (kXRows - 1); c = e >> 7; }      // C rows along the tile columns
             else { c = e & (kCombCols - 1); r = e >> 4; }
             if (r >= xr || c0 + c >= yc) continue;
-            int64_t off;
+            int64_t off = 0;
+            int cell = -1;
+            const int32_t *cm = nullptr, *cn = nullptr;
             if (cc) {                                                // grouped: the C block of (r, c)
                 const int32_t *cx = sco[r], *cy = sco[kXRows + c];
-                const int32_t *cm = cp.swap ? cy : cx, *cn = cp.swap ? cx : cy;
-                const int cell = ctab[cc->cell_off + cm[0] * cc->ncb + cn[0]];
+                cm = cp.swap ? cy : cx;
+                cn = cp.swap ? cx : cy;
+                cell = ctab[cc->cell_off + cm[0] * cc->ncb + cn[0]];
                 if (cell < 0) continue;
-                const DCrtCell &cl = cells[cell];
-                off = cl.c_off;
+                if constexpr (!SCATTER) {
+                    const DCrtCell &cl = cells[cell];
+                    off = cl.c_off;
 #pragma unroll
-                for (int k = 0; k < kCrtSideDims; k++) off += (int64_t)cm[1 + k] * cl.ms[k] + (int64_t)cn[1 + k] * cl.ns[k];
-            } else {
+                    for (int k = 0; k < kCrtSideDims; k++) off += (int64_t)cm[1 + k] * cl.ms[k] + (int64_t)cn[1 + k] * cl.ns[k];
+                }
+            } else if constexpr (!SCATTER) {
                 off = cb1->c_off + soff[r] + soff[kXRows + c];
             }
             // Garner: balanced mixed-radix digits v_i of the residues.  Every
@@ -994,9 +1023,26 @@ crt_combine_kernel(const DCrtPanel *__restrict__ panels, const DCrtItem *__restr
             const int e2 = sexp[r] + sexp[kXRows + c] - 2 * cp.P;
             const double p2 = e2 < -1022 ? 0.0 : __hiloint2double((min(e2, 1023) + 1023) << 20, 0);
             const double val = scale * (X * p2);
-            double *dst = C + off;
-            if (add) *dst += val;
-            else *dst = val;
+            if constexpr (SCATTER) {
+                if (cc) {
+                    const int2 dr = gdrange[cell];
+                    for (int d = dr.x; d < dr.y; d++) {
+                        const DCrtCell &dl = gdcells[d];
+                        int64_t o = dl.c_off;
+#pragma unroll
+                        for (int k = 0; k < kCrtSideDims; k++) o += (int64_t)cm[1 + k] * dl.ms[k] + (int64_t)cn[1 + k] * dl.ns[k];
+                        atomicAdd(C + o, gdcoef[d] * val);
+                    }
+                } else {
+                    for (int d = 0; d < nd; d++)
+                        atomicAdd(C + dests[d0 + d].c_off + sdoff[d * kTab + r] + sdoff[d * kTab + kXRows + c],
+                                  dests[d0 + d].scale * val);
+                }
+            } else {
+                double *dst = C + off;
+                if (add) *dst += val;
+                else *dst = val;
+            }
         }
     }
 }
@@ -1126,11 +1172,14 @@ cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, i
                                const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab,
                                const DCrtCell *cells, const uint8_t *out, const int32_t *gidx,
                                const int32_t *ex, const int32_t *ey, const int32_t *ext, const int32_t *eyt, double *c, int32_t add, double scale,
-                               const CrtParams &cp, cudaStream_t s) {
+                               const CrtParams &cp, cudaStream_t s, const CrtDests *dd) {
     if (nitems <= 0) return cudaSuccess;
     const int grid = 32 * nitems < 8 * num_sms() ? 32 * nitems : 8 * num_sms();
     switch (cp.L) {
-#define CASE_L(n) case n: crt_combine_kernel<n><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, ext, eyt, c, add, scale, cp); break;
+#define CASE_L(n) case n: \
+        if (dd) crt_combine_kernel<n, true><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, ext, eyt, c, 0, scale, cp, dd->drange, dd->dests, dd->gdrange, dd->gdcells, dd->gdcoef); \
+        else crt_combine_kernel<n, false><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, ext, eyt, c, add, scale, cp, nullptr, nullptr, nullptr, nullptr, nullptr); \
+        break;
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
 #undef CASE_L
     default: return cudaErrorInvalidValue;

@@ -182,6 +182,11 @@ struct SymExec {
     // scattered from the group buffer to each cell's destinations
     std::unique_ptr<PlainGroups> groups;
     DevBuf gdrange, gdcells, gdcoef;
+    // modular mode: the contraction's modular exec over a host-only view of
+    // its result space (kept: the exec is cached by the view's identity);
+    // dests and gd* then hold the recombination's destinations
+    std::unique_ptr<ltg_bt> tview;
+    struct CrtExec *crt = nullptr;
     std::vector<int64_t> nonzero_slots;      // result blocks some term reaches
     int64_t ndests = 0;
 };
@@ -214,6 +219,7 @@ struct CrtExec {
     // panels and tile offsets, and the 8-row units
     DevBuf fams, famp, famt, funits;
     int32_t nfunits = 0;
+    std::vector<DCrtCell> cells_host;       // the grouped products' cells, in cell order
     std::vector<std::pair<int64_t, int64_t>> zero_ranges;
     std::vector<int64_t> sched_slots;
 
@@ -1827,6 +1833,7 @@ CrtExec *prepare_crt(ltg_plan *pl, ltg_bt *c, int L, double ka, double kb, doubl
     upload_vec(ex->cta_items, cta_items, s);
     upload_vec(ex->cblks, dc, s);
     upload_vec(ex->gidx, gidx, s);
+    ex->cells_host = cells;
     if (comps.empty()) comps.resize(1);
     if (ctab.empty()) ctab.resize(1);
     if (cells.empty()) cells.resize(1);
@@ -2479,6 +2486,52 @@ void symmetrized_space(const Bis &bis, const Symmetry &sym, int32_t nidx, const 
     }
 }
 
+// The launches of one modular contraction (split passes, products,
+// recombination) into the arena carena, or, with dd, added to the
+// destinations dd names (the caller zeroes their tensor).
+void run_crt(ltg_plan *plan, CrtExec *cx, double *carena, int add, const CrtDests *dd) {
+    ltg_ctx *ctx = plan->ctx;
+    cudaStream_t s = ctx->stream;
+    report_device_wait(ctx);
+    if (!add && !dd)
+        for (auto &r : cx->zero_ranges)
+            LTG_CUDA(cudaMemsetAsync(carena + r.first, 0, (r.second - r.first) * sizeof(double), s));
+    const double *pa = plan->a->arena.as<double>(), *pb = plan->b->arena.as<double>();
+    TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
+    LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), s));
+    LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), s));
+    LTG_CUDA(launch_crt_fused(plan->fused_split, cx->panels.as<DCrtPanel>(), cx->fams.as<DCrtFamily>(), cx->famp.as<int32_t>(),
+                              cx->famt.as<int32_t>(), cx->funits.as<int4>(), cx->nfunits, pa, pb,
+                              cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
+                              cx->res.as<uint8_t>(), cx->cp, s));
+    LTG_CUDA(launch_crt_exponents(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, cx->nx,
+                                  cx->ny, pa, pb, cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(),
+                                  cx->ey.as<int32_t>(), cx->sampled, s));
+    for (int redo = 0; redo <= cx->sampled; redo++)
+        LTG_CUDA(launch_crt_residues(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, pa, pb,
+                                     cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
+                                     cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), cx->sampled, redo,
+                                     cx->res.as<uint8_t>(), cx->cp, s));
+    t_split.done();
+    TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
+    LTG_CUDA(launch_crt_gemm(cx->panels.as<DCrtPanel>(), cx->res.as<uint8_t>(), cx->tasks.as<DCrtTask>(),
+                             cx->items.as<DCrtItem>(), cx->cta_items.as<int32_t>(), cx->ncta,
+                             cx->out.as<uint8_t>(), cx->cp,
+                             ctx->wait_err.as<int32_t>(), ctx->wait_ns, plan->crt_stage_kb, s));
+    t_gemm.done();
+    TimedLaunch t_comb(ctx, LTG_KERNEL_OZ_COMBINE);
+    LTG_CUDA(launch_crt_combine(cx->panels.as<DCrtPanel>(), cx->items.as<DCrtItem>(), cx->nitems,
+                                cx->cblks.as<DCBlock>(), cx->comps.as<DCrtComp>(), cx->ctab.as<int32_t>(),
+                                cx->cells.as<DCrtCell>(), cx->out.as<uint8_t>(), cx->gidx.as<int32_t>(),
+                                cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), cx->ext.as<int32_t>(),
+                                cx->eyt.as<int32_t>(), carena, add,
+                                cx->scale, cx->cp, s, dd));
+    t_comb.done();
+    ctx->launches += 4 + (cx->nfunits > 0 ? 1 : 0) + (cx->nunits > 0 ? 2 + cx->sampled : 0) +
+                     (cx->nitems > 0 ? 2 : 0);
+    fetch_device_wait(ctx);
+}
+
 // Sub-dimension groups of one tile axis over the C dims `dims` (in the order
 // the axis enumerates them) with extents ext and strides str: unit extents
 // dropped, neighbours contiguous in str merged.
@@ -2508,13 +2561,16 @@ SubDims axis_dims(const std::vector<int> &dims, const int64_t *ext, const int64_
 // its dim q and coefficient c sign(t) (orbit sign).  Each result element has
 // one source per term, so it takes at most two atomic adds onto zero, whose
 // sum does not depend on their order.
-SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int32_t *idx, int32_t symm,
-                     double ka, double kb, double kc) {
+SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, int32_t mode, int32_t L, double c, int32_t nidx, const int32_t *idx,
+                     int32_t symm, double ka, double kb, double kc) {
+    if (mode != LTG_MODE_PLAIN_FP64 && mode != LTG_MODE_OZAKI_CRT)
+        throw error(kErrUnsupported, "the fused symmetrizer runs in the plain FP64 and modular modes");
+    const bool crt = mode == LTG_MODE_OZAKI_CRT;
     const int n = pl->plan().bisc.n;
     const std::vector<SePerm> S = symmetrizer_group(n, nidx, idx, symm != 0);
     if (S.size() != 2)
         throw error(kErrUnsupported, "the fused symmetrizer takes an index pair or a unitary permutation");
-    std::vector<int32_t> skey = {nidx, symm != 0 ? 1 : 0};
+    std::vector<int32_t> skey = {mode, crt ? L : 0, nidx, symm != 0 ? 1 : 0};
     for (int i = 0; i < (nidx < 0 ? n : nidx); i++) skey.push_back(idx[i]);
     auto key = std::make_tuple(r->uid, skey, c, ka, kb, kc);
     auto it = pl->sym.find(key);
@@ -2577,7 +2633,9 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int3
             DCBlock y;
             std::memset(&y, 0, sizeof(y));
             y.c_off = rh.blk_off[sl];
-            y.scale = dc[e].scale * (c * t.coeff * T.coeff);
+            // plain: the C block's own scale folded in; modular: the
+            // coefficient alone (the recombination applies the global scale)
+            y.scale = (crt ? 1.0 : dc[e].scale) * (c * t.coeff * T.coeff);
             y.M = dc[e].M;
             y.N = dc[e].N;
             const SubDims sm = axis_dims(mdims, sext, dstr), sn = axis_dims(ndims, sext, dstr);
@@ -2594,6 +2652,15 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int3
         }
         if (any) ex->nonzero_slots.push_back((int64_t)sl);
     }
+    if (crt) {
+        for (size_t e = 0; e < cbt.size(); e++)
+            if (per[e].size() > (size_t)kCrtMaxDests)
+                throw error(kErrUnsupported, "too many symmetrizer destinations per block for the modular recombination");
+        ex->tview.reset(new ltg_bt());
+        ex->tview->ctx = pl->ctx;
+        ex->tview->h = th;
+        ex->crt = prepare_crt(pl, ex->tview.get(), L, ka, kb, kc, 0, 0.0);
+    }
     std::vector<int2> drange(std::max<size_t>(cbt.size(), 1), make_int2(0, 0));
     std::vector<DCBlock> dests;
     for (size_t e = 0; e < cbt.size(); e++) {
@@ -2605,13 +2672,27 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int3
     // small blocks grouped as in the plain path (products into the group
     // buffer; each cell's elements then go to its C block's destinations)
     std::vector<int32_t> group_of(cbt.size(), -1);
-    if (pl->group_products && !pl->plan().coalesced) {
+    if (crt || (pl->group_products && !pl->plan().coalesced)) {
         std::vector<DCrtCell> gcells;
-        ex->groups.reset(new PlainGroups());
-        build_plain_groups(pl, th, cbt, ka * kb * kc, 1.0, group_of, *ex->groups, &gcells);
-        if (ex->groups->ngroups == 0) {
-            ex->groups.reset();
+        bool grouped = false;
+        if (crt) {
+            gcells = ex->crt->cells_host;
+            grouped = ex->crt->ngroups > 0;
+            if (grouped) {
+                std::map<int64_t, int32_t> e_of_off;
+                for (size_t e = 0; e < cbt.size(); e++) e_of_off[cbt[e].c_off] = (int32_t)e;
+                for (const DCrtCell &cl : gcells) {
+                    auto f = e_of_off.find(cl.c_off);
+                    if (f != e_of_off.end()) group_of[f->second] = 0;
+                }
+            }
         } else {
+            ex->groups.reset(new PlainGroups());
+            build_plain_groups(pl, th, cbt, ka * kb * kc, 1.0, group_of, *ex->groups, &gcells);
+            grouped = ex->groups->ngroups > 0;
+            if (!grouped) ex->groups.reset();
+        }
+        if (grouped) {
             std::map<int64_t, int32_t> e_of_off;
             for (size_t e = 0; e < cbt.size(); e++) e_of_off[cbt[e].c_off] = (int32_t)e;
             CrtSideMap sm[2];
@@ -2644,7 +2725,7 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, double c, int32_t nidx, const int3
     // work items of the other C blocks that reach the result, each over its
     // whole k range (tile shapes as in the plain path)
     std::vector<std::vector<std::pair<double, DItem>>> per_cfg(kNumShapes);
-    for (size_t e = 0; e < cbt.size(); e++) {
+    for (size_t e = 0; e < cbt.size() && !crt; e++) {
         if (per[e].empty() || group_of[e] >= 0) continue;
         int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(cbt[e].M, cbt[e].N);
         auto ov = pl->tile_override.find({cbt[e].M, cbt[e].N});
@@ -2726,19 +2807,27 @@ int ltg_contract2_make_symmetrized(ltg_plan *plan, int32_t nidx, const int32_t *
     });
 }
 
-int ltg_contract2_symmetrized(ltg_plan *plan, ltg_bt *r, double c, int32_t nidx, const int32_t *idx, int32_t symm,
-                              double ka, double kb, double kc) {
+int ltg_contract2_symmetrized(ltg_plan *plan, ltg_bt *r, int32_t mode, int32_t nslices, double c, int32_t nidx,
+                              const int32_t *idx, int32_t symm, double ka, double kb, double kc) {
     return guard([&] {
         if (!plan) throw error(kErrBadArg, "null plan");
         if (plan->external) throw error(kErrUnsupported, "a caller-built task plan has no schedule of its own");
         check_bt(r);
         need_dev(plan->ctx);
         if (!r->h.bis.equals(plan->plan().bisc)) throw error(kErrBadDims, "symmetrizer result of another index space");
-        SymExec *ex = prepare_sym(plan, r, c, nidx, idx, symm, ka, kb, kc);
+        SymExec *ex = prepare_sym(plan, r, mode, nslices > 0 ? nslices : 13, c, nidx, idx, symm, ka, kb, kc);
         ltg_ctx *ctx = plan->ctx;
         cudaStream_t s = ctx->stream;
         // the result starts at zero: every element then takes at most two adds
         LTG_CUDA(cudaMemsetAsync(r->arena.p, 0, (size_t)std::max<int64_t>(r->h.total_elems, 1) * sizeof(double), s));
+        if (ex->crt) {
+            const CrtDests dd{ex->drange.as<int2>(), ex->dests.as<DCBlock>(), ex->gdrange.as<int2>(),
+                              ex->gdcells.as<DCrtCell>(), ex->gdcoef.as<double>()};
+            run_crt(plan, ex->crt, r->arena.as<double>(), 0, &dd);
+            std::fill(r->h.nonzero.begin(), r->h.nonzero.end(), 0);
+            for (int64_t sl : ex->nonzero_slots) r->h.nonzero[sl] = 1;
+            return;
+        }
         int slot = 0;
         if (PlainGroups *pg = ex->groups.get()) {
             TimedLaunch tg(ctx, LTG_KERNEL_TRANSFER);
@@ -3263,44 +3352,7 @@ int ltg_contract2(ltg_plan *plan, ltg_bt *c, int32_t mode, int32_t nslices, doub
         cudaStream_t s = ctx->stream;
         if (mode == LTG_MODE_OZAKI_CRT) {
             CrtExec *cx = prepare_crt(plan, c, nslices > 0 ? nslices : 13, ka, kb, kc, add, d);
-            report_device_wait(ctx);
-            if (!add)
-                for (auto &r : cx->zero_ranges)
-                    LTG_CUDA(cudaMemsetAsync(c->arena.as<double>() + r.first, 0, (r.second - r.first) * sizeof(double), s));
-            const double *pa = plan->a->arena.as<double>(), *pb = plan->b->arena.as<double>();
-            TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
-            LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), s));
-            LTG_CUDA(launch_crt_fill(cx->nx, cx->ny, cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), s));
-            LTG_CUDA(launch_crt_fused(plan->fused_split, cx->panels.as<DCrtPanel>(), cx->fams.as<DCrtFamily>(), cx->famp.as<int32_t>(),
-                                      cx->famt.as<int32_t>(), cx->funits.as<int4>(), cx->nfunits, pa, pb,
-                                      cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
-                                      cx->res.as<uint8_t>(), cx->cp, s));
-            LTG_CUDA(launch_crt_exponents(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, cx->nx,
-                                          cx->ny, pa, pb, cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(),
-                                          cx->ey.as<int32_t>(), cx->sampled, s));
-            for (int redo = 0; redo <= cx->sampled; redo++)
-                LTG_CUDA(launch_crt_residues(cx->panels.as<DCrtPanel>(), cx->units.as<int4>(), cx->nunits, pa, pb,
-                                             cx->gidx.as<int32_t>(), cx->ex.as<int32_t>(), cx->ey.as<int32_t>(),
-                                             cx->ext.as<int32_t>(), cx->eyt.as<int32_t>(), cx->sampled, redo,
-                                             cx->res.as<uint8_t>(), cx->cp, s));
-            t_split.done();
-            TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
-            LTG_CUDA(launch_crt_gemm(cx->panels.as<DCrtPanel>(), cx->res.as<uint8_t>(), cx->tasks.as<DCrtTask>(),
-                                     cx->items.as<DCrtItem>(), cx->cta_items.as<int32_t>(), cx->ncta,
-                                     cx->out.as<uint8_t>(), cx->cp,
-                                     ctx->wait_err.as<int32_t>(), ctx->wait_ns, plan->crt_stage_kb, s));
-            t_gemm.done();
-            TimedLaunch t_comb(ctx, LTG_KERNEL_OZ_COMBINE);
-            LTG_CUDA(launch_crt_combine(cx->panels.as<DCrtPanel>(), cx->items.as<DCrtItem>(), cx->nitems,
-                                        cx->cblks.as<DCBlock>(), cx->comps.as<DCrtComp>(), cx->ctab.as<int32_t>(),
-                                        cx->cells.as<DCrtCell>(), cx->out.as<uint8_t>(), cx->gidx.as<int32_t>(),
-                                        cx->ex.as<int32_t>(), cx->ey.as<int32_t>(), cx->ext.as<int32_t>(),
-                                        cx->eyt.as<int32_t>(), c->arena.as<double>(), add,
-                                        cx->scale, cx->cp, s));
-            t_comb.done();
-            ctx->launches += 4 + (cx->nfunits > 0 ? 1 : 0) + (cx->nunits > 0 ? 2 + cx->sampled : 0) +
-                             (cx->nitems > 0 ? 2 : 0);
-            fetch_device_wait(ctx);
+            run_crt(plan, cx, c->arena.as<double>(), add, nullptr);
             if (!add) std::fill(c->h.nonzero.begin(), c->h.nonzero.end(), 0);
             for (int64_t sl : cx->sched_slots) c->h.nonzero[sl] = 1;
             return;

@@ -352,12 +352,27 @@ cudaError_t launch_crt_residues(const DCrtPanel *panels, const int4 *units, int3
 cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const DCrtTask *tasks,
     const DCrtItem *items, const int32_t *cta_items, int32_t ncta, uint8_t *out, const CrtParams &cp, int32_t *err,
     uint64_t wait_ns, int32_t stage_kb, cudaStream_t s);
+// Destinations of a contraction's C blocks in another tensor (a two-term
+// symmetrizer fused into the recombination): per C block of its own a range
+// of dests (offset, index mapping; scale = the coefficient), at most
+// kCrtMaxDests; per cell of a grouped product a range of gdcells with
+// coefficients gdcoef.
+constexpr int kCrtMaxDests = 8;
+struct CrtDests {
+    const int2 *drange;
+    const DCBlock *dests;
+    const int2 *gdrange;
+    const DCrtCell *gdcells;
+    const double *gdcoef;
+};
 // Garner recombination into C; each row's exponent is max(ex, ext) (the
-// bound, or the exact exponent of a row the residue pass redid).
+// bound, or the exact exponent of a row the residue pass redid).  With dd,
+// each element is added atomically to its destinations instead (c zeroed
+// before; add ignored).
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
     const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab, const DCrtCell *cells,
     const uint8_t *out, const int32_t *gidx, const int32_t *ex, const int32_t *ey, const int32_t *ext, const int32_t *eyt, double *c,
-    int32_t add, double scale, const CrtParams &cp, cudaStream_t s);
+    int32_t add, double scale, const CrtParams &cp, cudaStream_t s, const CrtDests *dd = nullptr);
 
 // Grouped plain products: operand cells into dense group panels (units:
 // piece, first row, rows), and the dense group results into the C blocks
