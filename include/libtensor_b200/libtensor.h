@@ -633,8 +633,10 @@ public:
             btb.adopt(r);
             *adopted = r;
         }
-        b200::check(ltg_contract2_symmetrized(m_plan, btb.handle(), m_mode, m_nslices, 1.0, nidx, idx, symm ? 1 : 0,
-                                              m_ka, m_kb, m_kc));
+        const int rc = ltg_contract2_symmetrized(m_plan, btb.handle(), m_mode, m_nslices, 1.0, nidx, idx,
+                                                 symm ? 1 : 0, m_ka, m_kb, m_kc);
+        if (rc == LTG_ERR_UNSUPPORTED) return false;   // e.g. too many destinations: through a temporary
+        b200::check(rc);
         return true;
     }
 };

@@ -216,3 +216,27 @@ def test_fused_symmetrize_rejects_four_indexes(gctx):
     with pytest.raises(Exception):
         op.perform_symmetrized(out, True, idx=(0, 1, 2, 3))
     out.close(); op.close(); A.close(); B.close()
+
+
+def test_fused_symmetrize_in_captured_graph(gctx):
+    """A fused symmetrizer call (zeroing the result, then the contraction's
+    kernels adding into it) captured as a CUDA graph replays to the eager
+    bits, plain and modular."""
+    cfg = S.RING_D2H_SMALL
+    A, B, op = _ring_op(gctx, cfg)
+    for mode in (0, 4):
+        out = op.make_symmetrized(False, idx=(0, 1))
+        op.perform_symmetrized(out, False, idx=(0, 1), mode=mode)      # prepared outside the capture
+        gctx.synchronize()
+        want = out.download().copy()
+        out.upload(np.zeros(out.nelems))
+        gctx.graph_begin()
+        op.perform_symmetrized(out, False, idx=(0, 1), mode=mode)
+        g = gctx.graph_end()
+        for _ in range(2):
+            g.launch()
+        gctx.synchronize()
+        assert np.array_equal(out.download(), want), mode
+        g.close()
+        out.close()
+    op.close(); A.close(); B.close()
