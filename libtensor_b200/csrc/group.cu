@@ -140,12 +140,23 @@ int group_sms() {
     return g_group_nsm;
 }
 
+// One wave of resident CTAs of a grid-striding kernel (256 threads, no
+// dynamic shared memory): more CTAs than fit leave a partial last wave that
+// sets the launch's time.
+template<class K>
+int resident_grid(K kernel) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 256, 0) != cudaSuccess || n < 1) n = 1;
+    return n * group_sms();
+}
+
 }  // namespace
 
 cudaError_t launch_gather_cells(const DGather *pieces, const int4 *units, int32_t nunits, const double *a,
                                 const double *b, double *buf, cudaStream_t s) {
     if (nunits <= 0) return cudaSuccess;
-    const int grid = nunits < 8 * group_sms() ? nunits : 8 * group_sms();
+    static const int resident = resident_grid(gather_cells_kernel);
+    const int grid = nunits < resident ? nunits : resident;
     gather_cells_kernel<<<grid, kGatherThreads, 0, s>>>(pieces, units, nunits, a, b, buf);
     return cudaGetLastError();
 }
@@ -154,7 +165,8 @@ cudaError_t launch_scatter_groups(const DCrtComp *comps, const int64_t *res_off,
                                   const DCrtCell *cells, const int2 *units, int32_t nunits, const double *buf,
                                   double *c, double scale, int32_t add, cudaStream_t s) {
     if (nunits <= 0) return cudaSuccess;
-    const int grid = nunits < 8 * group_sms() ? nunits : 8 * group_sms();
+    static const int resident = resident_grid(scatter_groups_kernel);
+    const int grid = nunits < resident ? nunits : resident;
     scatter_groups_kernel<<<grid, 256, 0, s>>>(comps, res_off, ctab, cells, units, nunits, buf, c, scale, add);
     return cudaGetLastError();
 }
@@ -164,7 +176,8 @@ cudaError_t launch_scatter_groups_dest(const DCrtComp *comps, const int64_t *res
                                        const int2 *units, int32_t nunits, const double *buf, double *r,
                                        double scale, cudaStream_t s) {
     if (nunits <= 0) return cudaSuccess;
-    const int grid = nunits < 8 * group_sms() ? nunits : 8 * group_sms();
+    static const int resident = resident_grid(scatter_groups_dest_kernel);
+    const int grid = nunits < resident ? nunits : resident;
     scatter_groups_dest_kernel<<<grid, 256, 0, s>>>(comps, res_off, ctab, drange, dcells, dcoef, units, nunits, buf,
                                                     r, scale);
     return cudaGetLastError();
