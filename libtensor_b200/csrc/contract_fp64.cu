@@ -533,12 +533,11 @@ cudaError_t launch_split_reduce(const DSplit *splits, int32_t nsplits, const DCB
     const int64_t total = (int64_t)nsplits * bm * bn;
     const int64_t want = (total + 255) / 256;
     // one wave of resident CTAs (a partial last wave would set the time)
-    static int per_sm = 0;
-    if (per_sm == 0) {
+    static const int per_sm = [] {
         int n = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, split_reduce_kernel, 256, 0) != cudaSuccess || n < 1) n = 1;
-        per_sm = n;
-    }
+        return n;
+    }();
     const int grid = (int)(want < (int64_t)per_sm * nsm ? want : (int64_t)per_sm * nsm);
     split_reduce_kernel<<<grid, 256, 0, s>>>(splits, nsplits, cblks, ws, bm, bn, c, add);
     return cudaGetLastError();

@@ -3500,6 +3500,7 @@ int ltg_contract2_set_grouping(ltg_plan *plan, int32_t enable) {
         if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
         plan->group_products = enable != 0;
         plan->crt.clear();
+        plan->sym.clear();              // modular symmetrizers point into plan->crt
     });
 }
 
@@ -3510,6 +3511,7 @@ int ltg_contract2_set_fused_split(ltg_plan *plan, int32_t enable) {
         if (enable < 0 || enable > 2) throw error(kErrBadArg, "one-read split shape must be 0 (off), 1 or 2");
         plan->fused_split = enable;
         plan->crt.clear();
+        plan->sym.clear();              // modular symmetrizers point into plan->crt
     });
 }
 
@@ -3520,6 +3522,7 @@ int ltg_contract2_set_crt_bound(ltg_plan *plan, int32_t sampled) {
         if (sampled != 0 && sampled != 1) throw error(kErrBadArg, "exponent bound must be 0 (exact) or 1 (sampled)");
         plan->crt_sampled = sampled;
         plan->crt.clear();
+        plan->sym.clear();              // modular symmetrizers point into plan->crt
     });
 }
 
@@ -3539,6 +3542,7 @@ int ltg_contract2_set_crt_rows(ltg_plan *plan, int32_t rows) {
         if (plan->ctx->capturing) throw error(kErrState, "cannot change a plan during graph capture");
         plan->crt_rows = rows;
         plan->crt.clear();
+        plan->sym.clear();              // modular symmetrizers point into plan->crt
     });
 }
 

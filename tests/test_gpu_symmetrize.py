@@ -240,3 +240,23 @@ def test_fused_symmetrize_in_captured_graph(gctx):
         g.close()
         out.close()
     op.close(); A.close(); B.close()
+
+
+def test_fused_modular_symmetrizer_after_plan_change(gctx):
+    """Changing the plan's modular settings drops the prepared modular
+    contractions and the fused symmetrizers built on them together: the next
+    fused call prepares again and gives the same result within the mode's
+    bound (exact instead of sampled row exponents)."""
+    cfg = S.RING_D2H_SMALL
+    A, B, op = _ring_op(gctx, cfg)
+    out = op.make_symmetrized(False, idx=(0, 1))
+    op.perform_symmetrized(out, False, idx=(0, 1), mode=4)
+    gctx.synchronize()
+    first = out.download().copy()
+    op.set_crt_bound(False)
+    op.perform_symmetrized(out, False, idx=(0, 1), mode=4)
+    gctx.synchronize()
+    second = out.download()
+    scale = max(1e-300, float(np.max(np.abs(first))))
+    assert float(np.max(np.abs(second - first))) <= 1e-12 * scale
+    out.close(); op.close(); A.close(); B.close()
