@@ -87,9 +87,9 @@ def parse():
                    help="modular mode: one-read split of row families in kernel shape 1 or 2 (0: exponent and "
                         "residue passes)")
     p.add_argument("--symmetrize", default="", choices=["", "asymm01", "asymm-p0123"],
-                   help="plain or modular mode: also time the result antisymmetrized over indexes (0,1) or "
-                        "the pair exchange (0 1)(2 3), fused into the contraction's kernels against the "
-                        "contraction followed by the symmetrizer pass")
+                   help="also time the result antisymmetrized over indexes (0,1) or the pair exchange "
+                        "(0 1)(2 3), fused into the contraction's kernels against the contraction followed by "
+                        "the symmetrizer pass (slice modes at their default slice counts)")
     p.add_argument("--crt-stage", type=int, default=0, choices=[0, 2, 3, 4, 6],
                    help="modular mode: k blocks per products pipeline stage (0: default)")
     p.add_argument("--tile", type=int, default=-1, help="force one tile shape (debug)")
@@ -384,7 +384,7 @@ def ltg_arm(args):
     # symmetrizer companion (plain mode): fused into the contraction epilogue
     # against the contraction into a temporary followed by the symmetrizer
     symm = None
-    if mode in (0, 4) and args.symmetrize:
+    if args.symmetrize:
         from libtensor_b200.core import btod_symmetrize
         kw = dict(symm=False, idx=(0, 1)) if args.symmetrize == "asymm01" else dict(symm=False, perm=(1, 0, 3, 2))
         Rf = op.make_symmetrized(**kw)

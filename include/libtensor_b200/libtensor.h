@@ -626,7 +626,7 @@ public:
     void set_split_precision(int32_t mode, int32_t nslices) { m_mode = mode; m_nslices = nslices; }
     bool perform_symmetrized(block_tensor<N + M, double> &btb, int32_t nidx, const int32_t *idx, bool symm,
                              ltg_bt **adopted) override {
-        if ((m_mode != LTG_MODE_PLAIN_FP64 && m_mode != LTG_MODE_OZAKI_CRT) || (nidx != 2 && nidx != -1)) return false;
+        if (nidx != 2 && nidx != -1) return false;
         if (!(btb.is_bound() && btb.handle() == *adopted)) {
             ltg_bt *r = nullptr;
             b200::check(ltg_contract2_make_symmetrized(m_plan, nidx, idx, symm ? 1 : 0, &r));

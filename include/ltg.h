@@ -155,10 +155,12 @@ int ltg_symmetrize(ltg_bt *a, double c, int32_t nidx, const int32_t *idx, int32_
  * btod_contract2, libtensor/block_tensor/btod_symmetrize2.h:19,
  * gen_block_tensor/impl/gen_bto_symmetrize2_impl.h): r = c (T + sign P(T)),
  * T the plan's contraction with coefficients ka, kb, kc, S = {e, P} as in
- * ltg_symmetrize (nidx 2 or -1), in mode LTG_MODE_PLAIN_FP64 or
- * LTG_MODE_OZAKI_CRT (nslices moduli, 0: 13).  The kernel that writes T's
- * elements -- the plain DMMA epilogue, the grouped products' scatter, or the
- * modular recombination -- adds each of them straight into the canonical
+ * ltg_symmetrize (nidx 2 or -1), in any mode: plain FP64, modular (nslices
+ * moduli, 0: 13) or a slice mode at its default slice count (0, or 7 for
+ * BF16 and INT8, 8 for FP8; other counts LTG_ERR_UNSUPPORTED).  The kernel
+ * that writes T's elements -- the plain DMMA epilogue, the grouped products'
+ * scatter, the modular recombination or the slice products' epilogue --
+ * adds each of them straight into the canonical
  * blocks of r that its two terms reach (no temporary T); r is zeroed first,
  * so every element takes at most two adds and the result does not depend on
  * their order.  Assignment only (ltg_symmetrize over a formed T adds).

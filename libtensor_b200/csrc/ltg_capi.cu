@@ -187,6 +187,7 @@ struct SymExec {
     // dests and gd* then hold the recombination's destinations
     std::unique_ptr<ltg_bt> tview;
     struct CrtExec *crt = nullptr;
+    struct OzExec *oz = nullptr;               // slice modes: the slice exec over the same view
     std::vector<int64_t> nonzero_slots;      // result blocks some term reaches
     int64_t ndests = 0;
 };
@@ -2563,14 +2564,16 @@ SubDims axis_dims(const std::vector<int> &dims, const int64_t *ext, const int64_
 // sum does not depend on their order.
 SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, int32_t mode, int32_t L, double c, int32_t nidx, const int32_t *idx,
                      int32_t symm, double ka, double kb, double kc) {
-    if (mode != LTG_MODE_PLAIN_FP64 && mode != LTG_MODE_OZAKI_CRT)
-        throw error(kErrUnsupported, "the fused symmetrizer runs in the plain FP64 and modular modes");
     const bool crt = mode == LTG_MODE_OZAKI_CRT;
+    const bool slice = mode >= LTG_MODE_OZAKI_BF16 && mode <= LTG_MODE_OZAKI_INT8;
+    if (mode != LTG_MODE_PLAIN_FP64 && !crt && !slice) throw error(kErrBadArg, "unknown mode");
+    if (slice && L != (mode == LTG_MODE_OZAKI_FP8 ? 8 : 7))
+        throw error(kErrUnsupported, "the fused symmetrizer in a slice mode takes its default slice count");
     const int n = pl->plan().bisc.n;
     const std::vector<SePerm> S = symmetrizer_group(n, nidx, idx, symm != 0);
     if (S.size() != 2)
         throw error(kErrUnsupported, "the fused symmetrizer takes an index pair or a unitary permutation");
-    std::vector<int32_t> skey = {mode, crt ? L : 0, nidx, symm != 0 ? 1 : 0};
+    std::vector<int32_t> skey = {mode, mode != LTG_MODE_PLAIN_FP64 ? L : 0, nidx, symm != 0 ? 1 : 0};
     for (int i = 0; i < (nidx < 0 ? n : nidx); i++) skey.push_back(idx[i]);
     auto key = std::make_tuple(r->uid, skey, c, ka, kb, kc);
     auto it = pl->sym.find(key);
@@ -2661,6 +2664,12 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, int32_t mode, int32_t L, double c,
         ex->tview->h = th;
         ex->crt = prepare_crt(pl, ex->tview.get(), L, ka, kb, kc, 0, 0.0);
     }
+    if (slice) {
+        ex->tview.reset(new ltg_bt());
+        ex->tview->ctx = pl->ctx;
+        ex->tview->h = th;
+        ex->oz = prepare_ozaki(pl, ex->tview.get(), mode, L, ka, kb, kc, 0, 0.0);
+    }
     std::vector<int2> drange(std::max<size_t>(cbt.size(), 1), make_int2(0, 0));
     std::vector<DCBlock> dests;
     for (size_t e = 0; e < cbt.size(); e++) {
@@ -2672,7 +2681,7 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, int32_t mode, int32_t L, double c,
     // small blocks grouped as in the plain path (products into the group
     // buffer; each cell's elements then go to its C block's destinations)
     std::vector<int32_t> group_of(cbt.size(), -1);
-    if (crt || (pl->group_products && !pl->plan().coalesced)) {
+    if (!slice && (crt || (pl->group_products && !pl->plan().coalesced))) {
         std::vector<DCrtCell> gcells;
         bool grouped = false;
         if (crt) {
@@ -2725,7 +2734,7 @@ SymExec *prepare_sym(ltg_plan *pl, ltg_bt *r, int32_t mode, int32_t L, double c,
     // work items of the other C blocks that reach the result, each over its
     // whole k range (tile shapes as in the plain path)
     std::vector<std::vector<std::pair<double, DItem>>> per_cfg(kNumShapes);
-    for (size_t e = 0; e < cbt.size() && !crt; e++) {
+    for (size_t e = 0; e < cbt.size() && !crt && !slice; e++) {
         if (per[e].empty() || group_of[e] >= 0) continue;
         int cfg = pl->forced_tile >= 0 ? pl->forced_tile : pick_tile(cbt[e].M, cbt[e].N);
         auto ov = pl->tile_override.find({cbt[e].M, cbt[e].N});
@@ -2815,11 +2824,33 @@ int ltg_contract2_symmetrized(ltg_plan *plan, ltg_bt *r, int32_t mode, int32_t n
         check_bt(r);
         need_dev(plan->ctx);
         if (!r->h.bis.equals(plan->plan().bisc)) throw error(kErrBadDims, "symmetrizer result of another index space");
-        SymExec *ex = prepare_sym(plan, r, mode, nslices > 0 ? nslices : 13, c, nidx, idx, symm, ka, kb, kc);
+        const int L = nslices > 0 ? nslices
+                                  : (mode == LTG_MODE_OZAKI_CRT ? 13 : mode == LTG_MODE_OZAKI_FP8 ? 8 : 7);
+        SymExec *ex = prepare_sym(plan, r, mode, L, c, nidx, idx, symm, ka, kb, kc);
         ltg_ctx *ctx = plan->ctx;
         cudaStream_t s = ctx->stream;
         // the result starts at zero: every element then takes at most two adds
         LTG_CUDA(cudaMemsetAsync(r->arena.p, 0, (size_t)std::max<int64_t>(r->h.total_elems, 1) * sizeof(double), s));
+        if (OzExec *ox = ex->oz) {
+            report_device_wait(ctx);
+            TimedLaunch t_split(ctx, LTG_KERNEL_OZ_SPLIT);
+            LTG_CUDA(launch_oz_split(ox->kind, ox->panels.as<DPanel>(), ox->npanels, ox->max_rows_pad,
+                                     plan->a->arena.as<double>(), plan->b->arena.as<double>(),
+                                     ox->slices.as<uint8_t>(), ox->exps.as<int32_t>(), ox->S, s));
+            t_split.done();
+            TimedLaunch t_gemm(ctx, LTG_KERNEL_OZ_GEMM);
+            LTG_CUDA(launch_oz_gemm(ox->kind, ox->panels.as<DPanel>(), ox->slices.as<uint8_t>(), ox->tasks.as<DOzTask>(),
+                                    ox->cblks.as<DCBlock>(), ox->items.as<DItem>(), ox->nitems,
+                                    ox->exps.as<int32_t>(), r->arena.as<double>(), 0, ox->S, ox->chunk_kb,
+                                    ctx->wait_err.as<int32_t>(), ctx->wait_ns, s, ex->drange.as<int2>(),
+                                    ex->dests.as<DCBlock>()));
+            t_gemm.done();
+            ctx->launches += 2;
+            fetch_device_wait(ctx);
+            std::fill(r->h.nonzero.begin(), r->h.nonzero.end(), 0);
+            for (int64_t sl : ex->nonzero_slots) r->h.nonzero[sl] = 1;
+            return;
+        }
         if (ex->crt) {
             const CrtDests dd{ex->drange.as<int2>(), ex->dests.as<DCBlock>(), ex->gdrange.as<int2>(),
                               ex->gdcells.as<DCrtCell>(), ex->gdcoef.as<double>()};

@@ -312,9 +312,13 @@ int tile_cfg_bk(int cfg);
 // grouped slice-product kernel with FP64 recombination.
 cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int32_t max_rows_pad,
     const double *a, const double *b, uint8_t *slices, int32_t *exps, int32_t S, cudaStream_t s);
+// With dests (one range drange[cblk] per C block), each C block's tile is
+// added atomically to its destinations (c zeroed before; add ignored); only
+// for each kind's default slice count (INT8 and BF16 7, FP8 8).
 cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices, const DOzTask *tasks,
     const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps, double *c,
-    int32_t add, int32_t S, int32_t chunk_kb, int32_t *err, uint64_t wait_ns, cudaStream_t s);
+    int32_t add, int32_t S, int32_t chunk_kb, int32_t *err, uint64_t wait_ns, cudaStream_t s,
+    const int2 *drange = nullptr, const DCBlock *dests = nullptr);
 // Per kind: first-slice bits, further-slice bits, element bytes, k elements
 // per 64-byte k block, bound of one slice product.
 void oz_kind_params(int kind, int *beta0, int *beta, int *esz, int *kbe, int64_t *maxprod);

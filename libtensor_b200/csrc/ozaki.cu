@@ -325,13 +325,18 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 
 // ---------------------------------------------------------------- slice products
 
-template<int KIND, int S>
+// SCATTER: each finished tile row goes, by atomic adds into a zeroed
+// result, to the destinations dests[drange[cblk]] of its C block (blocks of
+// another tensor with their own index mappings and scales: the terms of a
+// symmetrizer over the contraction) instead of the C block itself.
+template<int KIND, int S, bool SCATTER = false>
 __global__ void __launch_bounds__(kThreads, 1)
 oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ slices,
                const DOzTask *__restrict__ tasks, const DCBlock *__restrict__ cblks,
                const DItem *__restrict__ items, int32_t nitems, const int32_t *__restrict__ exps,
                double *__restrict__ Cp, int32_t add, int32_t stages, int32_t chunk_kb,
-               int32_t beta0, int32_t beta, int32_t kbe, int32_t *err, uint64_t wait_ns) {
+               int32_t beta0, int32_t beta, int32_t kbe, int32_t *err, uint64_t wait_ns,
+               const int2 *__restrict__ drange = nullptr, const DCBlock *__restrict__ dests = nullptr) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte aligned stage buffers: [stage][A slices | B slices]
     uint8_t *smem = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -533,7 +538,21 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
             }
             if (!ok) break;
             // FP64 write of the finished tile row
-            if (m < cb.M) {
+            if constexpr (SCATTER) {
+                if (m < cb.M) {
+                    const int2 dr = drange[item.cblk];
+                    for (int d = dr.x; d < dr.y; d++) {
+                        const DCBlock &db = dests[d];
+                        const int64_t drow = db.c_off + mixed_offset(m, db.nm, db.mext, db.mc_str);
+#pragma unroll
+                        for (int j = 0; j < kBN; j++) {
+                            const int n = item.n0 + j;
+                            if (n < cb.N)
+                                atomicAdd(Cp + drow + mixed_offset(n, db.nn, db.next, db.nc_str), db.scale * acc[j]);
+                        }
+                    }
+                }
+            } else if (m < cb.M) {
                 const int64_t orow = cb.c_off + mixed_offset(m, cb.nm, cb.mext, cb.mc_str);
 #pragma unroll
                 for (int j = 0; j < kBN; j++) {
@@ -560,10 +579,11 @@ oz_gemm_kernel(const DPanel *__restrict__ panels, const uint8_t *__restrict__ sl
 
 int g_nsm = 0;
 
-template<int KIND, int S>
+template<int KIND, int S, bool SCATTER = false>
 cudaError_t launch_gemm_s(const DPanel *panels, const uint8_t *slices, const DOzTask *tasks, const DCBlock *cblks,
                           const DItem *items, int32_t nitems, const int32_t *exps, double *c, int32_t add,
-                          int32_t chunk_kb, int32_t *err, uint64_t wait_ns, cudaStream_t s) {
+                          int32_t chunk_kb, int32_t *err, uint64_t wait_ns, cudaStream_t s,
+                          const int2 *drange = nullptr, const DCBlock *dests = nullptr) {
     int beta0, beta, esz, kbe;
     int64_t mp;
     oz_kind_params(KIND, &beta0, &beta, &esz, &kbe, &mp);
@@ -575,8 +595,8 @@ cudaError_t launch_gemm_s(const DPanel *panels, const uint8_t *slices, const DOz
     // holds all 512 TMEM columns.
     size_t smem = (size_t)stages * stage_bytes + 1024;
     if (smem < 120 * 1024) smem = 120 * 1024;
-    cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<KIND, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(oz_gemm_kernel<KIND, S, SCATTER>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (g_nsm == 0) {
         int dev = 0;
@@ -585,8 +605,9 @@ cudaError_t launch_gemm_s(const DPanel *panels, const uint8_t *slices, const DOz
     }
     int grid = nitems < g_nsm ? nitems : g_nsm;
     if (grid < 1) return cudaSuccess;
-    oz_gemm_kernel<KIND, S><<<grid, kThreads, smem, s>>>(panels, slices, tasks, cblks, items, nitems, exps, c, add,
-                                                        stages, chunk_kb, beta0, beta, kbe, err, wait_ns);
+    oz_gemm_kernel<KIND, S, SCATTER><<<grid, kThreads, smem, s>>>(panels, slices, tasks, cblks, items, nitems, exps,
+                                                                 c, add, stages, chunk_kb, beta0, beta, kbe, err,
+                                                                 wait_ns, drange, dests);
     return cudaGetLastError();
 }
 
@@ -624,8 +645,21 @@ cudaError_t launch_oz_split(int kind, const DPanel *panels, int32_t npanels, int
 cudaError_t launch_oz_gemm(int kind, const DPanel *panels, const uint8_t *slices, const DOzTask *tasks,
                            const DCBlock *cblks, const DItem *items, int32_t nitems, const int32_t *exps,
                            double *c, int32_t add, int32_t S, int32_t chunk_kb, int32_t *err,
-                           uint64_t wait_ns, cudaStream_t s) {
+                           uint64_t wait_ns, cudaStream_t s, const int2 *drange, const DCBlock *dests) {
     if (S < 1 || S > 8) return cudaErrorInvalidValue;
+    if (dests) {
+        // the scattering form for each kind's default slice count only
+        if (kind == kOzInt8 && S == 7)
+            return launch_gemm_s<kOzInt8, 7, true>(panels, slices, tasks, cblks, items, nitems, exps, c, 0, chunk_kb,
+                                                   err, wait_ns, s, drange, dests);
+        if (kind == kOzBf16 && S == 7)
+            return launch_gemm_s<kOzBf16, 7, true>(panels, slices, tasks, cblks, items, nitems, exps, c, 0, chunk_kb,
+                                                   err, wait_ns, s, drange, dests);
+        if (kind == kOzE4m3 && S == 8)
+            return launch_gemm_s<kOzE4m3, 8, true>(panels, slices, tasks, cblks, items, nitems, exps, c, 0, chunk_kb,
+                                                   err, wait_ns, s, drange, dests);
+        return cudaErrorNotSupported;
+    }
     if (kind == kOzInt8)
         return launch_gemm_k<kOzInt8>(S, panels, slices, tasks, cblks, items, nitems, exps, c, add, chunk_kb, err,
                                       wait_ns, s);

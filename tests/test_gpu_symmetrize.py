@@ -170,7 +170,7 @@ def test_fused_symmetrize_contraction_matches_reference(gctx, kw, mode, tol, gto
     out.close(); op.close(); A.close(); B.close()
 
 
-@pytest.mark.parametrize("mode", [0, 4], ids=["plain", "modular13"])
+@pytest.mark.parametrize("mode", [0, 4, 1, 2], ids=["plain", "modular13", "bf16x7", "fp8x8"])
 @pytest.mark.parametrize("kw", CASES, ids=IDS)
 def test_fused_symmetrize_equals_symmetrizer_of_result(gctx, kw, mode):
     """Fused and unfused forms of the same symmetrizer over the ring term and
@@ -259,4 +259,17 @@ def test_fused_modular_symmetrizer_after_plan_change(gctx):
     second = out.download()
     scale = max(1e-300, float(np.max(np.abs(first))))
     assert float(np.max(np.abs(second - first))) <= 1e-12 * scale
+    out.close(); op.close(); A.close(); B.close()
+
+
+def test_fused_slice_symmetrizer_takes_default_slice_count(gctx):
+    """The slice modes' fused symmetrizer runs at their default slice counts;
+    another count is refused (LTG_ERR_UNSUPPORTED) before anything runs."""
+    cfg = S.RING_D2H_SMALL
+    A, B, op = _ring_op(gctx, cfg)
+    out = op.make_symmetrized(False, idx=(0, 1))
+    with pytest.raises(Exception):
+        op.perform_symmetrized(out, False, idx=(0, 1), mode=1, nslices=4)
+    op.perform_symmetrized(out, False, idx=(0, 1), mode=1)
+    gctx.synchronize()
     out.close(); op.close(); A.close(); B.close()
