@@ -163,7 +163,8 @@ int ltg_symmetrize(ltg_bt *a, double c, int32_t nidx, const int32_t *idx, int32_
  * adds each of them straight into the canonical
  * blocks of r that its two terms reach (no temporary T); r is zeroed first,
  * so every element takes at most two adds and the result does not depend on
- * their order.  Assignment only (ltg_symmetrize over a formed T adds).
+ * their order.  Assignment only (ltg_symmetrize over a formed T adds); r
+ * must not be an operand of the contraction (LTG_ERR_UNSUPPORTED).
  * ltg_contract2_make_symmetrized: a tensor with the space of such sums (as
  * ltg_bt_create_symmetrized over the contraction's result). */
 int ltg_contract2_make_symmetrized(ltg_plan *plan, int32_t nidx, const int32_t *idx, int32_t symm, ltg_bt **out);

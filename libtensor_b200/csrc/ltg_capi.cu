@@ -2824,6 +2824,9 @@ int ltg_contract2_symmetrized(ltg_plan *plan, ltg_bt *r, int32_t mode, int32_t n
         check_bt(r);
         need_dev(plan->ctx);
         if (!r->h.bis.equals(plan->plan().bisc)) throw error(kErrBadDims, "symmetrizer result of another index space");
+        // the result is zeroed before the contraction reads its operands
+        if (r == plan->a || r == plan->b)
+            throw error(kErrUnsupported, "the fused symmetrizer's result is an operand of the contraction");
         const int L = nslices > 0 ? nslices
                                   : (mode == LTG_MODE_OZAKI_CRT ? 13 : mode == LTG_MODE_OZAKI_FP8 ? 8 : 7);
         SymExec *ex = prepare_sym(plan, r, mode, L, c, nidx, idx, symm, ka, kb, kc);

@@ -273,3 +273,14 @@ def test_fused_slice_symmetrizer_takes_default_slice_count(gctx):
     op.perform_symmetrized(out, False, idx=(0, 1), mode=1)
     gctx.synchronize()
     out.close(); op.close(); A.close(); B.close()
+
+
+def test_fused_symmetrizer_refuses_an_operand_as_result(gctx):
+    """The fused form zeroes its result before the contraction reads the
+    operands, so a result that is an operand is refused (the C++ class then
+    goes through a temporary)."""
+    cfg = S.RING_D2H_SMALL
+    A, B, op = _ring_op(gctx, cfg)
+    with pytest.raises(Exception):
+        op.perform_symmetrized(A, False, idx=(0, 1))
+    op.close(); A.close(); B.close()
