@@ -1168,17 +1168,38 @@ cudaError_t launch_crt_gemm(const DCrtPanel *panels, const uint8_t *res, const D
     }
 }
 
+// Resident CTAs per SM of a recombination instantiation (its registers and
+// shared memory), found once.
+template<int L, bool SCATTER>
+int combine_ctas_per_sm() {
+    static const int v = [] {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, crt_combine_kernel<L, SCATTER>, 256, 0) != cudaSuccess ||
+            n < 1)
+            n = 1;
+        return n;
+    }();
+    return v;
+}
+
 cudaError_t launch_crt_combine(const DCrtPanel *panels, const DCrtItem *items, int32_t nitems,
                                const DCBlock *cblks, const DCrtComp *comps, const int32_t *ctab,
                                const DCrtCell *cells, const uint8_t *out, const int32_t *gidx,
                                const int32_t *ex, const int32_t *ey, const int32_t *ext, const int32_t *eyt, double *c, int32_t add, double scale,
                                const CrtParams &cp, cudaStream_t s, const CrtDests *dd) {
     if (nitems <= 0) return cudaSuccess;
-    const int grid = 32 * nitems < 8 * num_sms() ? 32 * nitems : 8 * num_sms();
+    // 8 CTAs per SM (6 resident) striding over the units; with fewer than 16
+    // units per CTA the partial second wave of that grid sets the time, and
+    // one wave of resident CTAs is used instead
+    const int units = 32 * nitems;
+    auto grid_of = [&](int resident) {
+        const int g = units < 16 * 8 * num_sms() ? resident * num_sms() : 8 * num_sms();
+        return units < g ? units : g;
+    };
     switch (cp.L) {
 #define CASE_L(n) case n: \
-        if (dd) crt_combine_kernel<n, true><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, ext, eyt, c, 0, scale, cp, dd->drange, dd->dests, dd->gdrange, dd->gdcells, dd->gdcoef); \
-        else crt_combine_kernel<n, false><<<grid, 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, ext, eyt, c, add, scale, cp, nullptr, nullptr, nullptr, nullptr, nullptr); \
+        if (dd) crt_combine_kernel<n, true><<<grid_of(combine_ctas_per_sm<n, true>()), 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, ext, eyt, c, 0, scale, cp, dd->drange, dd->dests, dd->gdrange, dd->gdcells, dd->gdcoef); \
+        else crt_combine_kernel<n, false><<<grid_of(combine_ctas_per_sm<n, false>()), 256, 0, s>>>(panels, items, nitems, cblks, comps, ctab, cells, out, gidx, ex, ey, ext, eyt, c, add, scale, cp, nullptr, nullptr, nullptr, nullptr, nullptr); \
         break;
     CASE_L(8) CASE_L(9) CASE_L(10) CASE_L(11) CASE_L(12) CASE_L(13) CASE_L(14) CASE_L(15) CASE_L(16)
 #undef CASE_L
