@@ -181,9 +181,14 @@ int main(int argc, char **argv) {
         btod_symmetrize2<4>(ge, 2, 3, false).perform(gse);
         // the same symmetrizer over the contraction itself: both terms written
         // by the contraction's epilogue, no temporary
-        block_tensor<4, double> gsf(bis_r);
+        block_tensor<4, double> gsf(bis_r), gsm(bis_r);
         btod_contract2<3, 1, 1> gop(c1c, t, fe);
         btod_symmetrize2<4>(gop, 2, 3, false).perform(gsf);
+        // and with the contraction in the modular split-precision mode (the
+        // recombination adds each element to both terms)
+        btod_contract2<3, 1, 1> gopm(c1c, t, fe);
+        gopm.set_split_precision(LTG_MODE_OZAKI_CRT, 13);
+        btod_symmetrize2<4>(gopm, 2, 3, false).perform(gsm);
         // intermediates: a contraction of a contraction, a contraction of a sum
         // (terms with the same symmetry, and with a spin-only term, whose sum
         // keeps only the common symmetry), the result on the right-hand side,
@@ -277,7 +282,8 @@ int main(int argc, char **argv) {
                                 max_diff(gse, gs, 1.0), graph_diff,
                                 max_diff(nl, ne, 1.0), max_diff(ql, qe, 1.0), max_diff(wl, we, 1.0),
                                 max_diff(r, hr, 0.5), std::fabs(dl_sum - dot_tt - dot_ts), asg_diff,
-                                (double)asg.operations(), c3_diff, max_diff(gsf, gse, 1.0)};
+                                (double)asg.operations(), c3_diff, max_diff(gsf, gse, 1.0),
+                                max_diff(gsm, gse, 1.0)};
 
         // the contraction's non-zero blocks in index order, then the dot products
         FILE *f = std::fopen(argv[2], "wb");

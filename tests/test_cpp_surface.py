@@ -86,3 +86,4 @@ def test_surface_compute_matches_golden(exe, tmp_path):
     # the symmetrizer over the contraction's result (same terms; the k
     # summation of the contraction may be cut differently)
     assert d[18] <= 1e-15 * gmax
+    assert d[19] <= 1e-12 * gmax                        # the same in the modular mode (13 moduli)
